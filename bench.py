@@ -1,0 +1,296 @@
+#!/usr/bin/env python
+"""Headline benchmark: simulated days per second of the 2048 x 2048 x 2-layer wind-driven
+double gyre (rigid lid, AB3, FP64 state, multigrid pressure), one model step per step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm runs the CUDA path through the C ABI (``pawsim_b200``). ``value`` is device-timed
+throughput with the state resident in HBM; ``e2e`` is the same metric through the public
+API with the initial state uploaded from pinned host memory, the per-step solve report read
+back every step and the final state read back, all inside the timed region. The roofline
+object times the dominant kernel (the fused tendency + AB3 kernel) alone with CUDA events.
+The reference arm (``--impl reference``) times the reference's own serial build of the same
+step (``oracle/_ref/ref_harness``, built from the reference sources) on the host cores.
+
+Multi-GPU runs (torchrun, one rank per GPU) advance independent replicas: the model does not
+shard in this build, so there is no data-path collective; only the timing uses a MAX
+all-reduce. Inputs are seeded synthetic fields of the headline configuration; dt is 60 s,
+the AB3 stability limit of this grid being about 64 s (120 s blows up).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "sim-days/s at 2048^2 2-layer (double gyre, rigid lid, AB3, MG pressure)"
+N_GRID = int(os.environ.get("PAWSIM_BENCH_N", "2048"))
+DT = 60.0
+TOL = 1e-10
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def make_inputs(d):
+    from pawsim_b200 import inputs
+    return inputs.gyre(d, N=N_GRID, dt=DT, Nt=1000, solver=1, tol=TOL, seed=0)
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region (median SM clock, throttle reasons)."""
+
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.out.flush()
+        rows = []
+        with open(self.out.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 6:
+                    rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[2 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_reference(param, steps, label):
+    """Time the reference's serial step with ref_harness; returns (s/step, sample text)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    if not os.path.exists(exe):
+        return None, "oracle/_ref/ref_harness not built"
+    r = subprocess.run([exe, param, str(steps)], capture_output=True, text=True, timeout=1800)
+    if r.returncode != 0:
+        return None, "ref_harness failed: " + r.stderr.strip()[-200:]
+    secs = [json.loads(l)["seconds"] for l in r.stdout.splitlines() if '"phase": "step"' in l]
+    if not secs:
+        return None, "no steps timed"
+    return secs, f"{len(secs)} {label} steps of the {N_GRID}x{N_GRID}x2 gyre after set-up, 1 thread"
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    with tempfile.TemporaryDirectory() as d:
+        param = make_inputs(d)
+        nsteps = args.warmup + min(args.steps, 8)
+        secs, sample = cpu_reference(param, nsteps, "reference")
+    line = {"metric": METRIC, "unit": "sim-days/s", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": f"double gyre {N_GRID}x{N_GRID}x2, dt={DT} s, MG tol={TOL}"}}
+    if secs is None:
+        line.update({"unavailable": sample})
+    else:
+        timed = secs[args.warmup:] or secs
+        per = float(np.mean(timed))
+        v = DT / 86400.0 / per
+        line.update({"value": v, "ms_per_step": per * 1e3,
+                     "cpu_baseline": {"value": v, "unit": "sim-days/s", "cores": 1,
+                                      "kind": "reference", "sample": sample},
+                     "e2e": {"value": v, "unit": "sim-days/s", "h2d_bytes_per_step": 0,
+                             "d2h_bytes_per_step": 0}})
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mg-fp32", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    import torch
+    import pawsim_b200
+    from pawsim_b200 import inputs
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    tmp = tempfile.TemporaryDirectory()
+    param = make_inputs(tmp.name)
+    cfg = inputs.read_config(param)
+    fields = inputs.load_fields(cfg)
+    model = pawsim_b200.Model(cfg, fields, mg_fp32=args.mg_fp32)
+    model.set_stream(stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        model.prelim()
+        n = 1
+        for _ in range(args.warmup):
+            model.step(n)
+            n += 1
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        launches0 = model.launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        iters = []
+        solve_ms = []
+        with Clocks(local) as clk:
+            e0.record(stream)
+            for _ in range(args.steps):
+                st = model.step(n)
+                iters.append(st["iters"])
+                solve_ms.append(st["solve_ms"])
+                n += 1
+            e1.record(stream)
+            torch.cuda.synchronize()
+        launches = model.launch_count() - launches0
+        ms = e0.elapsed_time(e1)
+
+        # roofline of the dominant kernel: the fused tendency + AB3 kernel, one launch per call
+        k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 10
+        torch.cuda.synchronize()
+        k0.record(stream)
+        for _ in range(reps):
+            model.integrator_step(n)
+            n += 1
+        k1.record(stream)
+        torch.cuda.synchronize()
+        k_ms = k0.elapsed_time(k1) / reps
+
+    t_all = torch.tensor([ms], dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(t_all, op=dist.ReduceOp.MAX)
+    ms_max = float(t_all[0])
+    sec = ms_max / 1e3
+    value = world * args.steps * DT / 86400.0 / sec
+
+    # e2e through the public API: upload the state from pinned host memory, step, read the
+    # per-step report, download the final state -- all inside the timed region
+    L = cfg.Nlay
+    pinned = {k: torch.from_numpy(np.ascontiguousarray(fields[k])).pin_memory() for k in ("u", "v", "h")}
+    model2 = pawsim_b200.Model(cfg, fields, mg_fp32=args.mg_fp32)
+    model2.set_stream(stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        model2.prelim()
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for k in range(L):
+            for name in ("u", "v", "h"):
+                model2.set(name, k, pinned[name][k].numpy())
+        h2d = 3 * L * cfg.Nx * cfg.Ny * 8
+        nn = 1
+        for _ in range(args.steps):
+            model2.step(nn)
+            nn += 1
+        out = model2.state()
+        pi = model2.get("pi")
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+    d2h = out["u"].nbytes * 3 + pi.nbytes + args.steps * 7 * 8
+    t_e2e = torch.tensor([e2e_s], dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
+    e2e_value = world * args.steps * DT / 86400.0 / float(t_e2e[0])
+
+    peak, peak_kind = peaks()
+    ncell = cfg.Nx * cfg.Ny
+    alg_bytes = ncell * (120 * L + 24)
+    achieved = alg_bytes / (k_ms / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "sim-days/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded double-gyre inputs of the headline configuration)",
+        "config": {"workload": f"double gyre {N_GRID}x{N_GRID}x2, dt={DT} s, MG tol={TOL}",
+                   "pressure": "GPU multigrid, " + ("FP32 V-cycles in FP64 defect correction"
+                                                    if args.mg_fp32 else "FP64 V-cycles"),
+                   "l2": "inputs larger than L2 (state 201 MB + history 403 MB)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "pressure_ms_per_step": float(np.mean(solve_ms)),
+        "vcycles_per_step": float(np.mean(iters)),
+        "gpu_launches": int(launches),
+        "e2e": {"value": e2e_value, "unit": "sim-days/s", "h2d_bytes_per_step": h2d // args.steps,
+                "d2h_bytes_per_step": d2h // args.steps},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "tendency_kernel (fused tendency + AB3)", "kernel_ms": k_ms,
+                     "algorithmic_bytes": alg_bytes, "peak_kind": peak_kind},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        secs, sample = cpu_reference(param, 2, "reference")
+        if secs is not None:
+            line["cpu_baseline"] = {"value": DT / 86400.0 / float(np.mean(secs)), "unit": "sim-days/s",
+                                    "cores": 1, "kind": "reference", "sample": sample}
+        else:
+            line["cpu_baseline"] = {"value": None, "unit": "sim-days/s", "cores": 1,
+                                    "kind": "reference", "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    model.close()
+    model2.close()
+    tmp.cleanup()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,134 @@
+/*
+ * pawsim_b200.h -- C ABI of the B200 implementation of PAWSIM's timestep hot path.
+ *
+ * The library keeps one model's layered fields resident on one GPU and replaces the
+ * reference's hot-path entry points (paths are within the reference project):
+ *
+ *   pawsim_gpu_tendency_eval       <- pawsim_tendency_eval        model_code/tendency.c:81-115
+ *                                                                  (model_code/tendency.h:20-22)
+ *   pawsim_gpu_integrator_step     <- pawsim_integrator_step      model_code/integrator.c:138-198
+ *                                                                  (model_code/integrator.h:20)
+ *   pawsim_gpu_pressure_correct    <- pawsim_pressure_correct_rigid_lid
+ *                                                                  model_code/pressure.c:2254-2300
+ *                                                                  (model_code/pressure.h:16)
+ *   pawsim_gpu_prelim              <- timeSteppingPreliminaries   model_code/pawsim.c:266-304
+ *   pawsim_gpu_step                <- one pass of the main loop   model_code/pawsim.c:471-492
+ *   pawsim_gpu_solve_mg            <- solve_MG                     model_code/multigrid.c:1304-1343
+ *                                                                  (model_code/multigrid.h:12-24)
+ *
+ * Conventions: plain pointers and sizes, no library types in the signatures. Host arrays
+ * are float64, x fastest (the AWSIM disk order), Nx*Ny values per 2-D field. Return codes
+ * are 0 on success and negative PAWSIM_GPU_E* values on failure; the text of the last
+ * failure is available from pawsim_gpu_last_error(). A handle is not thread-safe; its work
+ * runs on one CUDA stream (the default stream unless pawsim_gpu_set_stream is called).
+ */
+#ifndef PAWSIM_B200_H
+#define PAWSIM_B200_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define PAWSIM_API __attribute__((visibility("default")))
+#else
+#define PAWSIM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PAWSIM_GPU_OK 0
+#define PAWSIM_GPU_EBADCONFIG (-1)
+#define PAWSIM_GPU_ECUDA (-2)
+#define PAWSIM_GPU_ENOTCONVERGED (-3)
+#define PAWSIM_GPU_ENONFINITE (-4)
+#define PAWSIM_GPU_EUNSUPPORTED (-5)
+#define PAWSIM_GPU_EBADNAME (-6)
+
+/* Solver identifiers (model_code/config.h:12-15). */
+#define PAWSIM_GPU_SOLVER_SOR 0
+#define PAWSIM_GPU_SOLVER_MG 1
+#define PAWSIM_GPU_SOLVER_MG_DISTRIBUTED 2
+
+/* Mirrors the parsed parameters of pawsim_config (model_code/config.h:17-130) that the hot
+ * path reads; derived feature flags are passed as parsed (config.c:285-312). */
+typedef struct pawsim_gpu_config
+{
+  int Nx, Ny, Nlay;
+  int wall_ew, wall_ns;
+  int ts_scheme;            /* 3 AB1, 4 AB2, 5 AB3 */
+  int mom_scheme;           /* 0 AL81, 1 HK83, 2 S75e, 3 TW81 */
+  int thick_scheme;         /* 0 AL81, 1 HK83, 2 UP3, 3 KT00 */
+  int use_rl, ocean_surf_drag, wind_feedback;
+  int use_wind, use_fbaro, use_relax, use_wdia, use_diavisc, use_wdia_file;
+  int tau_nrecs, wdia_nrecs;
+  int solver;               /* PAWSIM_GPU_SOLVER_* (pressureSolver, or use_MG 0/1) */
+  int use_full_mg, maxiters, pressure_timing;
+  double Lx, Ly, dt, tmin;
+  double A2, A4, A2smag, A4smag, h0, hsml, hmin_surf, hbbl, hmin_bot, KT00_sigma;
+  double lin_drag, quad_drag, lin_drag_surf, quad_drag_surf;
+  double tau_period, wdia_period, conv_diff;
+  double pi_tol, sor_rp, omega_mg;
+  /* GPU multigrid controls: 0 FP64 V-cycles, 1 FP32 V-cycles inside FP64 defect
+   * correction; red-black sweeps before/after the coarse correction and their weight
+   * (0 selects the defaults 1, 1, 1.0). */
+  int mg_fp32, mg_pre, mg_post;
+  double mg_omega;
+  /* 1: sums in the reference's serial order (bitwise parity), 0: fixed pairwise tree,
+   * -1: serial order for grids of at most 65536 cells. */
+  int serial_sums;
+} pawsim_gpu_config;
+
+/* Per-solve report, the numbers of the "PAWSIM pressure solve" line (pawsim.c:100-108). */
+typedef struct pawsim_gpu_stats
+{
+  int iters;                 /* SOR iterations or V-cycles */
+  double residual_max, residual_rms;   /* rhs - L(pi), pressure.c:652-690 (pressure_timing) */
+  double div_max, div_rms;             /* sum_k div(h u) after projection, pressure.c:693-737 */
+  double stop_measure;       /* value of the solver's own stopping test at exit */
+  double solve_ms;           /* device time of the solve alone */
+} pawsim_gpu_stats;
+
+typedef struct pawsim_gpu pawsim_gpu;
+
+PAWSIM_API int pawsim_gpu_create (const pawsim_gpu_config * cfg, pawsim_gpu ** out);
+PAWSIM_API void pawsim_gpu_destroy (pawsim_gpu * m);
+
+/* Upload or read one input/state field by name. Names and shapes:
+ *   u v h uRelax vRelax hRelax eRelax uTime vTime eTime nu_u_dia nu_v_dia  (k = layer)
+ *   hhs hhb uLid vLid Fbaro_x Fbaro_y hTime                                 (k = 0)
+ *   omegaz (Nx+1)*(Ny+1), taux tauy (k = record), wdia_ff (k = record*(Nlay+1)+interface)
+ *   gg (vector of Nlay, n = Nlay)
+ * Readable only: pi, pi_rhs, dt_u dt_v dt_h (last tendency), wdia (k <= Nlay), Hc.
+ * n is the number of doubles in host. */
+PAWSIM_API int pawsim_gpu_set_field (pawsim_gpu * m, const char * name, int k, const double * host, size_t n);
+PAWSIM_API int pawsim_gpu_get_field (pawsim_gpu * m, const char * name, int k, double * host, size_t n);
+
+/* Finish set-up after the uploads: wall faces, pressure operator, multigrid hierarchy. */
+PAWSIM_API int pawsim_gpu_init (pawsim_gpu * m);
+
+PAWSIM_API int pawsim_gpu_tendency_eval (pawsim_gpu * m);
+PAWSIM_API int pawsim_gpu_integrator_step (pawsim_gpu * m, unsigned n);
+PAWSIM_API int pawsim_gpu_pressure_correct (pawsim_gpu * m, int update_diags, pawsim_gpu_stats * st);
+PAWSIM_API int pawsim_gpu_prelim (pawsim_gpu * m, pawsim_gpu_stats * st);
+/* integrator step n followed by the rigid-lid correction (one pass of pawsim.c:471-492) */
+PAWSIM_API int pawsim_gpu_step (pawsim_gpu * m, unsigned n, pawsim_gpu_stats * st);
+/* nsteps passes starting at step n0; st receives the last step's report */
+PAWSIM_API int pawsim_gpu_run (pawsim_gpu * m, unsigned n0, unsigned nsteps, pawsim_gpu_stats * st);
+
+/* Solve L(pi) = rhs on the resident pi/pi_rhs with the GPU multigrid (no projection). */
+PAWSIM_API int pawsim_gpu_solve_mg (pawsim_gpu * m, pawsim_gpu_stats * st);
+
+/* Use the caller's CUDA stream (a cudaStream_t passed as void*) for all later work. */
+PAWSIM_API int pawsim_gpu_set_stream (pawsim_gpu * m, void * stream);
+PAWSIM_API int pawsim_gpu_synchronize (pawsim_gpu * m);
+PAWSIM_API double pawsim_gpu_time (const pawsim_gpu * m);
+/* kernels this library launched since creation (the launch counter) */
+PAWSIM_API long long pawsim_gpu_launch_count (const pawsim_gpu * m);
+PAWSIM_API const char * pawsim_gpu_last_error (void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,262 @@
+"""pawsim_b200 -- B200-native timestep hot path of PAWSIM behind a C ABI.
+
+The compute path is ``libpawsim_b200.so`` (hand-written sm_100a CUDA, see
+``include/pawsim_b200.h``). This module is the Python mirror of the reference's
+interface for that path: :class:`Model` is created from an AWSIM parameter file and
+exposes ``tendency_eval``, ``integrator_step``, ``pressure_correct``, ``prelim`` and
+``step`` with the meaning of ``pawsim_tendency_eval`` (model_code/tendency.c:81-115),
+``pawsim_integrator_step`` (model_code/integrator.c:138-198) and
+``pawsim_pressure_correct_rigid_lid`` (model_code/pressure.c:2254-2300). There is no CPU
+fallback: importing works anywhere, but creating a model needs the built library and a
+CUDA device, and fails loudly otherwise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import inputs
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpawsim_b200.so")
+
+SOLVER_SOR, SOLVER_MG, SOLVER_MG_DISTRIBUTED = 0, 1, 2
+
+
+class PawsimError(RuntimeError):
+    """A negative return code of the C ABI, with the library's last error text."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"pawsim_b200 error {code}: {msg}")
+        self.code = code
+
+
+class GpuConfig(ctypes.Structure):
+    """``pawsim_gpu_config`` of include/pawsim_b200.h (field order matters)."""
+    _fields_ = [(n, ctypes.c_int) for n in (
+        "Nx", "Ny", "Nlay", "wall_ew", "wall_ns", "ts_scheme", "mom_scheme", "thick_scheme",
+        "use_rl", "ocean_surf_drag", "wind_feedback", "use_wind", "use_fbaro", "use_relax",
+        "use_wdia", "use_diavisc", "use_wdia_file", "tau_nrecs", "wdia_nrecs", "solver",
+        "use_full_mg", "maxiters", "pressure_timing")] + [(n, ctypes.c_double) for n in (
+        "Lx", "Ly", "dt", "tmin", "A2", "A4", "A2smag", "A4smag", "h0", "hsml", "hmin_surf",
+        "hbbl", "hmin_bot", "KT00_sigma", "lin_drag", "quad_drag", "lin_drag_surf",
+        "quad_drag_surf", "tau_period", "wdia_period", "conv_diff", "pi_tol", "sor_rp",
+        "omega_mg")] + [("mg_fp32", ctypes.c_int), ("mg_pre", ctypes.c_int),
+                        ("mg_post", ctypes.c_int), ("mg_omega", ctypes.c_double),
+                        ("serial_sums", ctypes.c_int)]
+
+
+class GpuStats(ctypes.Structure):
+    _fields_ = [("iters", ctypes.c_int), ("residual_max", ctypes.c_double),
+                ("residual_rms", ctypes.c_double), ("div_max", ctypes.c_double),
+                ("div_rms", ctypes.c_double), ("stop_measure", ctypes.c_double),
+                ("solve_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+EXPORTS = (
+    "pawsim_gpu_create", "pawsim_gpu_destroy", "pawsim_gpu_set_field", "pawsim_gpu_get_field",
+    "pawsim_gpu_init", "pawsim_gpu_tendency_eval", "pawsim_gpu_integrator_step",
+    "pawsim_gpu_pressure_correct", "pawsim_gpu_prelim", "pawsim_gpu_step", "pawsim_gpu_run",
+    "pawsim_gpu_solve_mg", "pawsim_gpu_set_stream", "pawsim_gpu_synchronize",
+    "pawsim_gpu_time", "pawsim_gpu_launch_count", "pawsim_gpu_last_error",
+)
+
+_LIB = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the CUDA library (no compute happens here). Raises if it was not built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise PawsimError(-2, f"{path} is missing: run `python -m pawsim_b200.build` first")
+    lib = ctypes.CDLL(path)
+    P = ctypes.c_void_p
+    lib.pawsim_gpu_create.argtypes = [ctypes.POINTER(GpuConfig), ctypes.POINTER(P)]
+    lib.pawsim_gpu_destroy.argtypes = [P]
+    lib.pawsim_gpu_destroy.restype = None
+    for fn in ("pawsim_gpu_set_field", "pawsim_gpu_get_field"):
+        getattr(lib, fn).argtypes = [P, ctypes.c_char_p, ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_double), ctypes.c_size_t]
+    lib.pawsim_gpu_init.argtypes = [P]
+    lib.pawsim_gpu_tendency_eval.argtypes = [P]
+    lib.pawsim_gpu_integrator_step.argtypes = [P, ctypes.c_uint]
+    lib.pawsim_gpu_pressure_correct.argtypes = [P, ctypes.c_int, ctypes.POINTER(GpuStats)]
+    lib.pawsim_gpu_prelim.argtypes = [P, ctypes.POINTER(GpuStats)]
+    lib.pawsim_gpu_step.argtypes = [P, ctypes.c_uint, ctypes.POINTER(GpuStats)]
+    lib.pawsim_gpu_run.argtypes = [P, ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(GpuStats)]
+    lib.pawsim_gpu_solve_mg.argtypes = [P, ctypes.POINTER(GpuStats)]
+    lib.pawsim_gpu_set_stream.argtypes = [P, P]
+    lib.pawsim_gpu_synchronize.argtypes = [P]
+    lib.pawsim_gpu_time.argtypes = [P]
+    lib.pawsim_gpu_time.restype = ctypes.c_double
+    lib.pawsim_gpu_launch_count.argtypes = [P]
+    lib.pawsim_gpu_launch_count.restype = ctypes.c_longlong
+    lib.pawsim_gpu_last_error.argtypes = []
+    lib.pawsim_gpu_last_error.restype = ctypes.c_char_p
+    _LIB = lib
+    return lib
+
+
+def _check(rc):
+    if rc < 0:
+        raise PawsimError(rc, load_library().pawsim_gpu_last_error().decode())
+    return rc
+
+
+def gpu_config(cfg: inputs.Config, **over) -> GpuConfig:
+    """Translate a parsed AWSIM configuration into the C ABI's struct."""
+    v = cfg.values
+    g = GpuConfig()
+    g.Nx, g.Ny, g.Nlay = v["Nx"], v["Ny"], v["Nlay"]
+    g.wall_ew, g.wall_ns = int(v["useWallEW"]), int(v["useWallNS"])
+    g.ts_scheme, g.mom_scheme, g.thick_scheme = (v["timeSteppingScheme"], v["momentumScheme"],
+                                                 v["thicknessScheme"])
+    g.use_rl, g.ocean_surf_drag, g.wind_feedback = (int(v["useRL"]), int(v["oceanSurfDrag"]),
+                                                    int(v["windFeedback"]))
+    g.use_wind, g.use_fbaro, g.use_relax = int(v["useWind"]), int(v["useFbaro"]), int(v["useRelax"])
+    g.use_wdia, g.use_diavisc = int(v["useWDia"]), int(v["useDiaVisc"])
+    g.use_wdia_file = int(bool(cfg.files.get("wDiaFile")))
+    g.tau_nrecs, g.wdia_nrecs = v["tauNrecs"], v["wDiaNrecs"]
+    g.solver, g.use_full_mg, g.maxiters = v["pressureSolver"], int(v["use_fullMG"]), v["maxiters"]
+    g.pressure_timing = int(v["pressureTiming"])
+    g.Lx, g.Ly, g.dt, g.tmin = v["Lx"], v["Ly"], v["dt"], v["tmin"]
+    for a, b in (("A2", "A2"), ("A4", "A4"), ("A2smag", "A2smag"), ("A4smag", "A4smag"),
+                 ("h0", "h0"), ("hsml", "hsml"), ("hmin_surf", "hmin_surf"), ("hbbl", "hbbl"),
+                 ("hmin_bot", "hmin_bot"), ("KT00_sigma", "KT00_sigma"),
+                 ("lin_drag", "linDragCoeff"), ("quad_drag", "quadDragCoeff"),
+                 ("lin_drag_surf", "linDragSurf"), ("quad_drag_surf", "quadDragSurf"),
+                 ("tau_period", "tauPeriod"), ("wdia_period", "wDiaPeriod"),
+                 ("conv_diff", "convDiff"), ("pi_tol", "tol"), ("sor_rp", "SOR_rp"),
+                 ("omega_mg", "omega_MG")):
+        setattr(g, a, float(v[b]))
+    g.mg_fp32, g.mg_pre, g.mg_post, g.mg_omega = 0, 1, 1, 1.0
+    g.serial_sums = -1
+    for k, val in over.items():
+        setattr(g, k, val)
+    return g
+
+
+class Model:
+    """One model resident on the GPU (the drop-in for the reference's hot path)."""
+
+    def __init__(self, cfg: inputs.Config, fields: dict | None = None, **options):
+        if cfg.values["useTracer"]:
+            raise PawsimError(-5, "the tracer equation is not part of this path yet")
+        self.lib = load_library()
+        self.cfg = cfg
+        self.L, self.Nx, self.Ny = cfg.values["Nlay"], cfg.values["Nx"], cfg.values["Ny"]
+        self._gc = gpu_config(cfg, **options)
+        h = ctypes.c_void_p()
+        _check(self.lib.pawsim_gpu_create(ctypes.byref(self._gc), ctypes.byref(h)))
+        self._h = h
+        if fields is None:
+            fields = inputs.load_fields(cfg)
+        self.upload(fields)
+        _check(self.lib.pawsim_gpu_init(self._h))
+
+    @classmethod
+    def from_param_file(cls, path: str, **options) -> "Model":
+        return cls(inputs.read_config(path), **options)
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self.lib.pawsim_gpu_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------------ fields
+    def set(self, name: str, k: int, arr) -> None:
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        _check(self.lib.pawsim_gpu_set_field(self._h, name.encode(), k,
+                                             a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                             a.size))
+
+    def get(self, name: str, k: int = 0) -> np.ndarray:
+        if name == "omegaz":
+            out = np.empty((self.Ny + 1, self.Nx + 1))
+        elif name == "gg":
+            out = np.empty(self.L)
+        else:
+            out = np.empty((self.Ny, self.Nx))
+        _check(self.lib.pawsim_gpu_get_field(self._h, name.encode(), k,
+                                             out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                             out.size))
+        return out
+
+    def upload(self, f: dict) -> None:
+        L = self.L
+        for name in ("u", "v", "h", "uRelax", "vRelax", "hRelax", "eRelax", "uTime", "vTime",
+                     "eTime", "nu_u_dia", "nu_v_dia"):
+            for k in range(L):
+                self.set(name, k, f[name][k])
+        for name in ("hhs", "hhb", "uLid", "vLid", "Fbaro_x", "Fbaro_y", "hTime", "omegaz"):
+            self.set(name, 0, f[name])
+        for r in range(f["taux"].shape[0]):
+            self.set("taux", r, f["taux"][r])
+            self.set("tauy", r, f["tauy"][r])
+        for r in range(f["wdia_ff"].shape[0]):
+            for k in range(L + 1):
+                self.set("wdia_ff", r * (L + 1) + k, f["wdia_ff"][r, k])
+        self.set("gg", 0, f["gg"])
+
+    def state(self) -> dict:
+        return {n: np.stack([self.get(n, k) for k in range(self.L)]) for n in ("u", "v", "h")}
+
+    # ----------------------------------------------------------------- hot path
+    def tendency_eval(self) -> dict:
+        _check(self.lib.pawsim_gpu_tendency_eval(self._h))
+        return {n: np.stack([self.get("dt_" + n, k) for k in range(self.L)]) for n in ("u", "v", "h")}
+
+    def integrator_step(self, n: int) -> None:
+        _check(self.lib.pawsim_gpu_integrator_step(self._h, n))
+
+    def pressure_correct(self, update_diags: bool = True) -> dict:
+        st = GpuStats()
+        _check(self.lib.pawsim_gpu_pressure_correct(self._h, int(update_diags), ctypes.byref(st)))
+        return st.as_dict()
+
+    def prelim(self) -> dict:
+        st = GpuStats()
+        _check(self.lib.pawsim_gpu_prelim(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def step(self, n: int) -> dict:
+        st = GpuStats()
+        _check(self.lib.pawsim_gpu_step(self._h, n, ctypes.byref(st)))
+        return st.as_dict()
+
+    def run(self, n0: int, nsteps: int) -> dict:
+        st = GpuStats()
+        _check(self.lib.pawsim_gpu_run(self._h, n0, nsteps, ctypes.byref(st)))
+        return st.as_dict()
+
+    def solve_mg(self) -> dict:
+        st = GpuStats()
+        _check(self.lib.pawsim_gpu_solve_mg(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def synchronize(self) -> None:
+        _check(self.lib.pawsim_gpu_synchronize(self._h))
+
+    def set_stream(self, stream_ptr: int) -> None:
+        _check(self.lib.pawsim_gpu_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    @property
+    def t(self) -> float:
+        return self.lib.pawsim_gpu_time(self._h)
+
+    def launch_count(self) -> int:
+        return self.lib.pawsim_gpu_launch_count(self._h)

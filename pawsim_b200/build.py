@@ -1,0 +1,55 @@
+"""Build recipe for the CUDA library (sm_100a) and the drop-in host driver.
+
+``python -m pawsim_b200.build`` (or ``pawsim_b200.build.build()``) compiles every
+``csrc/*.cu`` into ``pawsim_b200/libpawsim_b200.so`` with nvcc for sm_100a. The tendency
+and pressure kernels are compiled with ``-fmad=false`` so that no multiply-add is fused,
+as in the reference's x86-64 build; this is what makes the FP64 path bit-identical.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libpawsim_b200.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC,-O3",
+         "-Xcompiler", "-fvisibility=hidden"]
+SOURCES = ["api.cu", "tendency.cu", "pressure.cu", "mg.cu"]
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    srcs = [os.path.join(CSRC, s) for s in SOURCES]
+    deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    deps.append(os.path.join(os.path.dirname(HERE), "include", "pawsim_b200.h"))
+    if not force and not _stale(LIB, deps):
+        return LIB
+    objs = []
+    for s in srcs:
+        o = os.path.join(CSRC, os.path.basename(s).replace(".cu", ".o"))
+        cmd = [NVCC, *ARCH, *FLAGS, "-c", s, "-o", o]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        objs.append(o)
+    cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    for o in objs:
+        os.remove(o)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

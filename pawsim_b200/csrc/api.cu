@@ -1,0 +1,631 @@
+// api.cu -- the model object behind the C ABI of include/pawsim_b200.h.
+//
+// Owns the resident device fields of one model and sequences the hot path exactly as the
+// reference's driver does (model_code/pawsim.c:266-304, 471-492): tendency + AB update
+// (integrator.c:138-198), then the rigid-lid correction (pressure.c:2254-2300).
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/pawsim_b200.h"
+#include "common.cuh"
+#include "mg.cuh"
+#include "pressure.cuh"
+#include "tendency.cuh"
+
+namespace pawsim {
+
+static thread_local char g_err[512] = "";
+long long g_launches = 0;
+
+int set_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
+  snprintf(g_err, sizeof(g_err), "CUDA error %s (%s) in %s at %s:%d", cudaGetErrorName(e),
+           cudaGetErrorString(e), what, file, line);
+  return PAWSIM_GPU_ECUDA;
+}
+
+static int fail(int code, const char* msg) {
+  snprintf(g_err, sizeof(g_err), "%s", msg);
+  return code;
+}
+
+// rigid-lid column constraint (pressure.c:525-561) when it is not fused into K-tend
+__global__ void thickness_fix_kernel(double* h, const double* Hc, int Nx, int Ny, int pitch, size_t ls, int L) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= Nx || j >= Ny) return;
+  size_t c = (size_t)j * pitch + i;
+  double tot = 0;
+  for (int k = 0; k < L; ++k) tot += h[k * ls + c];
+  if (tot == 0) return;
+  double err = tot - Hc[c];
+  for (int k = 0; k < L; ++k) h[k * ls + c] *= (1 - err / tot);
+}
+
+__global__ void hc_kernel(const double* hhs, const double* hhb, double* Hc, int Nx, int Ny, int pitch) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= Nx || j >= Ny) return;
+  size_t c = (size_t)j * pitch + i;
+  Hc[c] = hhs[c] - hhb[c];
+}
+
+struct Model {
+  pawsim_gpu_config c;
+  int Nx, Ny, L, pitch, qpitch;
+  size_t lstride, plane;
+  double dx, dy, t;
+  cudaStream_t s = 0;
+  std::vector<void*> allocs;
+  double *u[2], *v[2], *h[2];
+  int cur = 0;
+  double *fu[2], *fv[2], *fh[2];
+  int h1 = 0;   // history buffer holding the newest stored tendency
+  double *dtu, *dtv, *dth, *wdia;
+  double *hhs, *hhb, *Hc, *omz, *taux, *tauy, *fbx, *fby, *uLid, *vLid;
+  double *uRelax, *vRelax, *hRelax, *eRelax, *uTime, *vTime, *eTime, *hTime, *wdff, *nu_u, *nu_v;
+  double *pi, *rhs, *work, *scratch, *dsum;
+  unsigned long long* slots;
+  int* diters;
+  Operator op;
+  double gg[LMAX], geff[LMAX];
+  std::vector<double> hhs_host, hhb_host;
+  Multigrid* mg = nullptr;
+  bool thickness_fixed = false;
+  bool ready = false;
+  cudaEvent_t ev0, ev1;
+
+  template <typename T> T* alloc(size_t n) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+    cudaMemset(p, 0, n * sizeof(T));
+    allocs.push_back(p);
+    return (T*)p;
+  }
+  ~Model() {
+    delete mg;
+    for (void* p : allocs) cudaFree(p);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+  }
+  bool serial() const {
+    if (c.serial_sums == 1) return true;
+    if (c.serial_sums == 0) return false;
+    return (long long)Nx * Ny <= 65536;
+  }
+  Grid2 grid2() const {
+    Grid2 g;
+    g.Nx = Nx; g.Ny = Ny; g.pitch = pitch; g.L = L; g.lstride = lstride;
+    g.wall_ew = c.wall_ew; g.wall_ns = c.wall_ns; g.dx = dx; g.dy = dy; g.dt = c.dt;
+    g.thick_scheme = c.thick_scheme;
+    return g;
+  }
+};
+
+static void fill_d(double* d, size_t n, double v) {
+  std::vector<double> tmp(n, v);
+  cudaMemcpy(d, tmp.data(), n * sizeof(double), cudaMemcpyHostToDevice);
+}
+
+static int create(const pawsim_gpu_config* cfg, Model** out) {
+  const pawsim_gpu_config& c = *cfg;
+  if (c.Nlay < 1 || c.Nlay > LMAX) return fail(PAWSIM_GPU_EBADCONFIG, "Nlay must be in 1..8");
+  if (c.Nx < 4 || c.Ny < 4) return fail(PAWSIM_GPU_EBADCONFIG, "Nx and Ny must be at least 4");
+  if (c.Ly <= 0 || c.Lx <= 0 || c.dt <= 0) return fail(PAWSIM_GPU_EBADCONFIG, "Lx, Ly and dt must be positive");
+  if (c.ts_scheme < 3 || c.ts_scheme > 5)
+    return fail(PAWSIM_GPU_EBADCONFIG, "PAWSIM only supports AB1, AB2 and AB3 time stepping so far");
+  if (c.mom_scheme < 0 || c.mom_scheme > 3 || c.thick_scheme < 0 || c.thick_scheme > 3)
+    return fail(PAWSIM_GPU_EBADCONFIG, "Unknown or unsupported numerical scheme identifier");
+  if (c.thick_scheme > 1) return fail(PAWSIM_GPU_EUNSUPPORTED, "UP3/KT00 thickness schemes are not built yet");
+  if (c.A2smag > 0 || c.A4smag > 0) return fail(PAWSIM_GPU_EUNSUPPORTED, "Smagorinsky viscosity is not built yet");
+  if (c.quad_drag > 0 || c.quad_drag_surf > 0) return fail(PAWSIM_GPU_EUNSUPPORTED, "quadratic drag is not built yet");
+  if (c.hsml > 0 || c.hbbl > 0) return fail(PAWSIM_GPU_EUNSUPPORTED, "hsml/hbbl layer fractions are not built yet");
+  if (c.tau_nrecs < 1 || c.wdia_nrecs < 1) return fail(PAWSIM_GPU_EBADCONFIG, "record counts must be positive");
+  if (c.solver < 0 || c.solver > 2) return fail(PAWSIM_GPU_EBADCONFIG, "Unknown pressureSolver identifier");
+  Model* m = new Model();
+  m->c = c;
+  m->Nx = c.Nx; m->Ny = c.Ny; m->L = c.Nlay;
+  m->pitch = round_up(c.Nx, 32);
+  m->qpitch = round_up(c.Nx + 1, 32);
+  m->lstride = (size_t)c.Ny * m->pitch;
+  m->plane = m->lstride;
+  m->dx = c.Lx / c.Nx;
+  m->dy = c.Ly / c.Ny;
+  m->t = c.tmin;
+  cudaEventCreate(&m->ev0);
+  cudaEventCreate(&m->ev1);
+  size_t Ls = m->L * m->lstride;
+  bool ok = true;
+  for (int b = 0; b < 2; ++b) {
+    ok &= (m->u[b] = m->alloc<double>(Ls)) && (m->v[b] = m->alloc<double>(Ls)) && (m->h[b] = m->alloc<double>(Ls));
+    ok &= (m->fu[b] = m->alloc<double>(Ls)) && (m->fv[b] = m->alloc<double>(Ls)) && (m->fh[b] = m->alloc<double>(Ls));
+  }
+  ok &= (m->dtu = m->alloc<double>(Ls)) && (m->dtv = m->alloc<double>(Ls)) && (m->dth = m->alloc<double>(Ls));
+  ok &= (m->wdia = m->alloc<double>((m->L + 1) * m->lstride)) != nullptr;
+  ok &= (m->hhs = m->alloc<double>(m->plane)) && (m->hhb = m->alloc<double>(m->plane)) && (m->Hc = m->alloc<double>(m->plane));
+  ok &= (m->omz = m->alloc<double>((size_t)(c.Ny + 1) * m->qpitch)) != nullptr;
+  ok &= (m->taux = m->alloc<double>(c.tau_nrecs * m->plane)) && (m->tauy = m->alloc<double>(c.tau_nrecs * m->plane));
+  ok &= (m->fbx = m->alloc<double>(m->plane)) && (m->fby = m->alloc<double>(m->plane));
+  ok &= (m->uLid = m->alloc<double>(m->plane)) && (m->vLid = m->alloc<double>(m->plane));
+  ok &= (m->uRelax = m->alloc<double>(Ls)) && (m->vRelax = m->alloc<double>(Ls)) && (m->hRelax = m->alloc<double>(Ls));
+  ok &= (m->eRelax = m->alloc<double>(Ls)) && (m->uTime = m->alloc<double>(Ls)) && (m->vTime = m->alloc<double>(Ls));
+  ok &= (m->eTime = m->alloc<double>(Ls)) && (m->hTime = m->alloc<double>(m->plane));
+  ok &= (m->wdff = m->alloc<double>((size_t)c.wdia_nrecs * (m->L + 1) * m->lstride)) != nullptr;
+  ok &= (m->nu_u = m->alloc<double>(Ls)) && (m->nu_v = m->alloc<double>(Ls));
+  ok &= (m->pi = m->alloc<double>(m->plane)) && (m->rhs = m->alloc<double>(m->plane)) && (m->work = m->alloc<double>(m->plane));
+  ok &= (m->scratch = m->alloc<double>(reduce_scratch_elems(c.Nx, c.Ny))) != nullptr;
+  ok &= (m->dsum = m->alloc<double>(8)) != nullptr;
+  ok &= (m->slots = m->alloc<unsigned long long>(2)) != nullptr;
+  ok &= (m->diters = m->alloc<int>(1)) != nullptr;
+  m->op.opitch = round_up(c.Nx + 1, 32);
+  ok &= (m->op.Ow = m->alloc<double>((size_t)(c.Ny + 1) * m->op.opitch)) != nullptr;
+  ok &= (m->op.Os = m->alloc<double>((size_t)(c.Ny + 1) * m->op.opitch)) != nullptr;
+  ok &= (m->op.csor = m->alloc<double>(m->plane)) != nullptr;
+  if (!ok) {
+    delete m;
+    return fail(PAWSIM_GPU_ECUDA, "device allocation failed");
+  }
+  // defaults of model_code/state.c:968-1006
+  for (int k = 0; k < m->L; ++k) {
+    fill_d(m->hRelax + k * m->lstride, m->lstride, 1000.0 / m->L);
+    fill_d(m->eRelax + k * m->lstride, m->lstride, 1000.0 * k / m->L);
+    fill_d(m->uTime + k * m->lstride, m->lstride, -1);
+    fill_d(m->vTime + k * m->lstride, m->lstride, -1);
+    fill_d(m->eTime + k * m->lstride, m->lstride, -1);
+    m->gg[k] = 9.81;
+  }
+  fill_d(m->hTime, m->plane, -1);
+  m->hhs_host.assign((size_t)c.Nx * c.Ny, 0.0);
+  m->hhb_host.assign((size_t)c.Nx * c.Ny, 0.0);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    delete m;
+    return set_cuda_error(e, "create", __FILE__, __LINE__);
+  }
+  *out = m;
+  return 0;
+}
+
+// resolve a field name to (device base, rows, cols, pitch, count of k)
+struct FieldRef {
+  double* base;
+  int rows, cols, pitch;
+  size_t kstride;
+  int nk;
+  bool writable;
+};
+
+static bool lookup(Model* m, const std::string& n, FieldRef& f) {
+  int L = m->L;
+  f = FieldRef{nullptr, m->Ny, m->Nx, m->pitch, m->lstride, 1, true};
+  if (n == "u") { f.base = m->u[m->cur]; f.nk = L; }
+  else if (n == "v") { f.base = m->v[m->cur]; f.nk = L; }
+  else if (n == "h") { f.base = m->h[m->cur]; f.nk = L; }
+  else if (n == "uRelax") { f.base = m->uRelax; f.nk = L; }
+  else if (n == "vRelax") { f.base = m->vRelax; f.nk = L; }
+  else if (n == "hRelax") { f.base = m->hRelax; f.nk = L; }
+  else if (n == "eRelax") { f.base = m->eRelax; f.nk = L; }
+  else if (n == "uTime") { f.base = m->uTime; f.nk = L; }
+  else if (n == "vTime") { f.base = m->vTime; f.nk = L; }
+  else if (n == "eTime") { f.base = m->eTime; f.nk = L; }
+  else if (n == "nu_u_dia") { f.base = m->nu_u; f.nk = L; }
+  else if (n == "nu_v_dia") { f.base = m->nu_v; f.nk = L; }
+  else if (n == "hhs") f.base = m->hhs;
+  else if (n == "hhb") f.base = m->hhb;
+  else if (n == "uLid") f.base = m->uLid;
+  else if (n == "vLid") f.base = m->vLid;
+  else if (n == "Fbaro_x") f.base = m->fbx;
+  else if (n == "Fbaro_y") f.base = m->fby;
+  else if (n == "hTime") f.base = m->hTime;
+  else if (n == "taux") { f.base = m->taux; f.nk = m->c.tau_nrecs; }
+  else if (n == "tauy") { f.base = m->tauy; f.nk = m->c.tau_nrecs; }
+  else if (n == "wdia_ff") { f.base = m->wdff; f.nk = m->c.wdia_nrecs * (L + 1); }
+  else if (n == "omegaz") { f.base = m->omz; f.rows = m->Ny + 1; f.cols = m->Nx + 1; f.pitch = m->qpitch;
+                            f.kstride = 0; }
+  else {
+    f.writable = false;
+    if (n == "pi") f.base = m->pi;
+    else if (n == "pi_rhs") f.base = m->rhs;
+    else if (n == "Hc") f.base = m->Hc;
+    else if (n == "dt_u") { f.base = m->dtu; f.nk = L; }
+    else if (n == "dt_v") { f.base = m->dtv; f.nk = L; }
+    else if (n == "dt_h") { f.base = m->dth; f.nk = L; }
+    else if (n == "wdia") { f.base = m->wdia; f.nk = L + 1; }
+    else if (n == "tend_u") { f.base = m->fu[m->h1]; f.nk = L; }
+    else if (n == "tend_v") { f.base = m->fv[m->h1]; f.nk = L; }
+    else if (n == "tend_h") { f.base = m->fh[m->h1]; f.nk = L; }
+    else return false;
+  }
+  return true;
+}
+
+static int set_field(Model* m, const char* name, int k, const double* host, size_t n) {
+  std::string nm(name ? name : "");
+  if (nm == "gg") {
+    if ((int)n != m->L) return fail(PAWSIM_GPU_EBADNAME, "gg needs Nlay values");
+    for (int q = 0; q < m->L; ++q) {
+      if (host[q] < 0) return fail(PAWSIM_GPU_EBADCONFIG, "gFile may contain only non-negative values");
+      m->gg[q] = host[q];
+    }
+    return 0;
+  }
+  FieldRef f;
+  if (!lookup(m, nm, f) || !f.writable) return fail(PAWSIM_GPU_EBADNAME, "unknown or read-only field name");
+  if (k < 0 || k >= f.nk) return fail(PAWSIM_GPU_EBADNAME, "field index out of range");
+  if (n != (size_t)f.rows * f.cols) return fail(PAWSIM_GPU_EBADNAME, "wrong element count for field");
+  PAWSIM_CUDA_OK(cudaMemcpy2DAsync(f.base + k * f.kstride, f.pitch * sizeof(double), host, f.cols * sizeof(double),
+                                   f.cols * sizeof(double), f.rows, cudaMemcpyHostToDevice, m->s));
+  // the state halo fill (state.c:1052-1057) puts +0 on wall faces of the normal velocity
+  if (nm == "u" && m->c.wall_ew)
+    PAWSIM_CUDA_OK(cudaMemset2DAsync(f.base + k * f.kstride, f.pitch * sizeof(double), 0, sizeof(double), f.rows, m->s));
+  if (nm == "v" && m->c.wall_ns)
+    PAWSIM_CUDA_OK(cudaMemsetAsync(f.base + k * f.kstride, 0, f.cols * sizeof(double), m->s));
+  if (nm == "hhs" || nm == "hhb") {
+    std::vector<double>& dst = nm == "hhs" ? m->hhs_host : m->hhb_host;
+    memcpy(dst.data(), host, n * sizeof(double));
+    m->ready = false;   // the pressure operator and hierarchy depend on Hc
+  }
+  PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
+  return 0;
+}
+
+static int get_field(Model* m, const char* name, int k, double* host, size_t n) {
+  std::string nm(name ? name : "");
+  if (nm == "gg") {
+    if ((int)n != m->L) return fail(PAWSIM_GPU_EBADNAME, "gg needs Nlay values");
+    memcpy(host, m->gg, m->L * sizeof(double));
+    return 0;
+  }
+  FieldRef f;
+  if (!lookup(m, nm, f)) return fail(PAWSIM_GPU_EBADNAME, "unknown field name");
+  if (k < 0 || k >= f.nk) return fail(PAWSIM_GPU_EBADNAME, "field index out of range");
+  if (n != (size_t)f.rows * f.cols) return fail(PAWSIM_GPU_EBADNAME, "wrong element count for field");
+  PAWSIM_CUDA_OK(cudaMemcpy2DAsync(host, f.cols * sizeof(double), f.base + k * f.kstride, f.pitch * sizeof(double),
+                                   f.cols * sizeof(double), f.rows, cudaMemcpyDeviceToHost, m->s));
+  PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
+  return 0;
+}
+
+static int init(Model* m) {
+  // state halo fill of state.c:1052-1057: wall-normal velocity is zero on the wall face
+  for (int k = 0; k < m->L; ++k) {
+    if (m->c.wall_ew)
+      PAWSIM_CUDA_OK(cudaMemset2DAsync(m->u[m->cur] + k * m->lstride, m->pitch * sizeof(double), 0, sizeof(double),
+                                       m->Ny, m->s));
+    if (m->c.wall_ns)
+      PAWSIM_CUDA_OK(cudaMemsetAsync(m->v[m->cur] + k * m->lstride, 0, m->Nx * sizeof(double), m->s));
+  }
+  m->geff[0] = m->gg[0];
+  for (int k = 1; k < m->L; ++k) m->geff[k] = m->geff[k - 1] + m->gg[k];
+  dim3 b(32, 8), g((m->Nx + 31) / 32, (m->Ny + 7) / 8);
+  hc_kernel<<<g, b, 0, m->s>>>(m->hhs, m->hhb, m->Hc, m->Nx, m->Ny, m->pitch);
+  ++g_launches;
+  launch_operator(m->grid2(), m->Hc, m->op, m->c.sor_rp, m->s);
+  g_launches += 2;
+  PAWSIM_CUDA_OK(cudaGetLastError());
+  if (m->c.use_rl && m->c.solver != PAWSIM_GPU_SOLVER_SOR) {
+    delete m->mg;
+    m->mg = nullptr;
+    std::vector<double> Hc(m->hhs_host.size());
+    for (size_t q = 0; q < Hc.size(); ++q) Hc[q] = m->hhs_host[q] - m->hhb_host[q];
+    MGOptions o;
+    o.fp32_cycles = m->c.mg_fp32;
+    o.pre = m->c.mg_pre > 0 ? m->c.mg_pre : 1;
+    o.post = m->c.mg_post > 0 ? m->c.mg_post : 1;
+    o.omega_rb = m->c.mg_omega > 0 ? m->c.mg_omega : 1.0;
+    o.full_mg = m->c.use_full_mg;
+    m->mg = new Multigrid(m->Nx, m->Ny, m->c.Lx, m->c.Ly, m->c.wall_ew, m->c.wall_ns, Hc.data(), o, m->s);
+    if (!m->mg->ok()) return fail(PAWSIM_GPU_ECUDA, "multigrid allocation failed");
+  }
+  PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
+  m->ready = true;
+  return 0;
+}
+
+// wind / wDia record interpolation weights (forcing.c:49-68, restoring.c:56-70)
+static void record_weights(int nrecs, double period, double t, int* n0, int* n1, double* w0, double* w1) {
+  *n0 = 0; *n1 = 0; *w0 = 1; *w1 = 0;
+  if (nrecs > 1 && period > 0) {
+    double nflt = (fmod(t, period) / period) * nrecs;
+    unsigned nm1 = (unsigned)floor(nflt), np1 = (unsigned)ceil(nflt);
+    if (np1 == nm1) np1 = nm1 + 1;
+    *n0 = (int)nm1;
+    *n1 = (int)(np1 % (unsigned)nrecs);
+    *w0 = np1 - nflt;
+    *w1 = nflt - nm1;
+  }
+}
+
+static TendParams base_params(Model* m) {
+  TendParams p;
+  memset(&p, 0, sizeof(p));
+  const pawsim_gpu_config& c = m->c;
+  p.Nx = m->Nx; p.Ny = m->Ny; p.L = m->L; p.pitch = m->pitch; p.qpitch = m->qpitch; p.lstride = m->lstride;
+  p.wall_ew = c.wall_ew; p.wall_ns = c.wall_ns; p.use_rl = c.use_rl;
+  p.dx = m->dx; p.dy = m->dy;
+  p.u = m->u[m->cur]; p.v = m->v[m->cur]; p.h = m->h[m->cur];
+  p.hhb = m->hhb; p.hhs = m->hhs; p.Hc = m->Hc; p.omz = m->omz;
+  for (int k = 0; k < m->L; ++k) { p.gg[k] = m->gg[k]; p.geff[k] = m->geff[k]; }
+  p.h0 = c.h0;
+  p.useA2 = (c.A2 > 0) || (c.A2smag > 0);
+  p.useA4 = (c.A4 > 0) || (c.A4smag > 0);
+  p.A2 = c.A2;
+  p.A4sqrt = sqrt(c.A4);
+  p.use_wind = c.use_wind; p.use_fbaro = c.use_fbaro;
+  int n0, n1;
+  record_weights(c.tau_nrecs, c.tau_period, m->t, &n0, &n1, &p.tw0, &p.tw1);
+  p.taux0 = m->taux + n0 * m->plane; p.taux1 = m->taux + n1 * m->plane;
+  p.tauy0 = m->tauy + n0 * m->plane; p.tauy1 = m->tauy + n1 * m->plane;
+  p.fbx = m->fbx; p.fby = m->fby;
+  p.lin_drag = c.lin_drag; p.lin_drag_surf = c.lin_drag_surf; p.ocean_surf_drag = c.ocean_surf_drag;
+  p.uLid = m->uLid; p.vLid = m->vLid;
+  p.use_relax = c.use_relax; p.use_wdia = c.use_wdia; p.use_wdia_file = c.use_wdia_file;
+  p.use_diavisc = c.use_diavisc;
+  record_weights(c.wdia_nrecs, c.wdia_period, m->t, &n0, &n1, &p.ww0, &p.ww1);
+  p.wd0 = m->wdff + (size_t)n0 * (m->L + 1) * m->lstride;
+  p.wd1 = m->wdff + (size_t)n1 * (m->L + 1) * m->lstride;
+  p.hRelax = m->hRelax; p.eRelax = m->eRelax; p.eTime = m->eTime; p.hTime = m->hTime;
+  p.uRelax = m->uRelax; p.vRelax = m->vRelax; p.uTime = m->uTime; p.vTime = m->vTime;
+  p.nu_u = m->nu_u; p.nu_v = m->nu_v;
+  p.wdia_out = m->wdia;
+  return p;
+}
+
+static int tendency_eval(Model* m) {
+  if (!m->ready) return fail(PAWSIM_GPU_EBADCONFIG, "pawsim_gpu_init must follow the uploads");
+  TendParams p = base_params(m);
+  p.ab_mode = 0;
+  p.fu_out = m->dtu; p.fv_out = m->dtv; p.fh_out = m->dth;
+  if (launch_tendency(p, m->c.mom_scheme, m->c.thick_scheme, m->s) != 0)
+    return fail(PAWSIM_GPU_EUNSUPPORTED, "scheme combination not available");
+  ++g_launches;
+  PAWSIM_CUDA_OK(cudaGetLastError());
+  return 0;
+}
+
+static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
+  if (!m->ready) return fail(PAWSIM_GPU_EBADCONFIG, "pawsim_gpu_init must follow the uploads");
+  const pawsim_gpu_config& c = m->c;
+  TendParams p = base_params(m);
+  double dt = c.dt;
+  bool shift = true;
+  if (c.ts_scheme == 3 || n == 1) {
+    p.ab_mode = 1; p.c0 = dt;
+    if (c.ts_scheme == 5) shift = false;   // AB3 start-up keeps no history (integrator.c:169-172)
+  } else if (c.ts_scheme == 4 || n == 2) {
+    p.ab_mode = 2; p.c0 = 3 * dt / 2; p.c1 = dt / 2;
+  } else {
+    p.ab_mode = 3; p.c0 = 23 * dt / 12; p.c1 = 4 * dt / 3; p.c2 = 5 * dt / 12;
+  }
+  int h2 = 1 - m->h1;
+  p.f1u = m->fu[m->h1]; p.f1v = m->fv[m->h1]; p.f1h = m->fh[m->h1];
+  p.f2u = m->fu[h2]; p.f2v = m->fv[h2]; p.f2h = m->fh[h2];
+  p.fu_out = m->fu[h2]; p.fv_out = m->fv[h2]; p.fh_out = m->fh[h2];
+  p.write_hist = shift ? 1 : 0;
+  int nb = 1 - m->cur;
+  p.u_out = m->u[nb]; p.v_out = m->v[nb]; p.h_out = m->h[nb];
+  p.fuse_thickness_fix = (fuse_fix && c.use_rl) ? 1 : 0;
+  if (launch_tendency(p, c.mom_scheme, c.thick_scheme, m->s) != 0)
+    return fail(PAWSIM_GPU_EUNSUPPORTED, "scheme combination not available");
+  ++g_launches;
+  PAWSIM_CUDA_OK(cudaGetLastError());
+  if (shift) m->h1 = h2;
+  m->cur = nb;
+  m->t += dt;
+  m->thickness_fixed = p.fuse_thickness_fix != 0;
+  return 0;
+}
+
+static int finish_norms(Model* m, const double* field, double* mx, double* rms) {
+  launch_norms(field, m->Nx, m->Ny, m->pitch, m->serial(), m->scratch, m->dsum, m->s);
+  g_launches += 3;
+  double hbuf[2];
+  PAWSIM_CUDA_OK(cudaMemcpyAsync(hbuf, m->dsum, 2 * sizeof(double), cudaMemcpyDeviceToHost, m->s));
+  PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
+  *mx = hbuf[0];
+  *rms = sqrt(hbuf[1] / ((double)m->Nx * (double)m->Ny));
+  return 0;
+}
+
+static int pressure_correct(Model* m, int update_diags, pawsim_gpu_stats* st) {
+  (void)update_diags;
+  pawsim_gpu_stats local;
+  memset(&local, 0, sizeof(local));
+  if (!m->ready) return fail(PAWSIM_GPU_EBADCONFIG, "pawsim_gpu_init must follow the uploads");
+  if (!m->c.use_rl) {
+    if (st) *st = local;
+    return 0;
+  }
+  const int cur = m->cur;
+  Grid2 g = m->grid2();
+  dim3 b(32, 8), gr((m->Nx + 31) / 32, (m->Ny + 7) / 8);
+  if (!m->thickness_fixed) {
+    thickness_fix_kernel<<<gr, b, 0, m->s>>>(m->h[cur], m->Hc, m->Nx, m->Ny, m->pitch, m->lstride, m->L);
+    ++g_launches;
+  }
+  m->thickness_fixed = false;
+  launch_pressure_rhs(g, m->u[cur], m->v[cur], m->h[cur], m->rhs, m->s);
+  launch_sum(m->rhs, m->Nx, m->Ny, m->pitch, m->serial(), m->scratch, m->dsum, m->s);
+  launch_subtract_mean(m->rhs, m->Nx, m->Ny, m->pitch, m->dsum, m->s);
+  g_launches += m->serial() ? 3 : 4;
+  PAWSIM_CUDA_OK(cudaGetLastError());
+  PAWSIM_CUDA_OK(cudaEventRecord(m->ev0, m->s));
+  int iters = 0;
+  if (m->c.solver == PAWSIM_GPU_SOLVER_SOR) {
+    if (launch_sor(g, m->pi, m->rhs, m->op, m->c.sor_rp, m->c.pi_tol, m->c.maxiters, m->slots, m->diters, m->s) != 0)
+      return fail(PAWSIM_GPU_ECUDA, "cooperative SOR launch failed");
+    ++g_launches;
+    launch_sum(m->pi, m->Nx, m->Ny, m->pitch, m->serial(), m->scratch, m->dsum, m->s);
+    launch_subtract_mean(m->pi, m->Nx, m->Ny, m->pitch, m->dsum, m->s);
+    g_launches += m->serial() ? 2 : 3;
+    PAWSIM_CUDA_OK(cudaMemcpyAsync(&iters, m->diters, sizeof(int), cudaMemcpyDeviceToHost, m->s));
+    PAWSIM_CUDA_OK(cudaEventRecord(m->ev1, m->s));
+    PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
+  } else if (m->c.solver == PAWSIM_GPU_SOLVER_MG) {
+    double mres = 0;
+    iters = m->mg->solve(m->pi, m->pitch, m->rhs, m->pitch, m->c.pi_tol, m->c.maxiters, &mres);
+    local.stop_measure = mres;
+    PAWSIM_CUDA_OK(cudaEventRecord(m->ev1, m->s));
+    PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
+  } else {
+    return fail(PAWSIM_GPU_EUNSUPPORTED, "pressureSolver 2 is not built yet");
+  }
+  float ms = 0;
+  cudaEventElapsedTime(&ms, m->ev0, m->ev1);
+  local.solve_ms = ms;
+  local.iters = iters;
+  PAWSIM_CUDA_OK(cudaGetLastError());
+  if (m->c.pressure_timing) {
+    launch_residual_field(g, m->pi, m->rhs, m->op, m->work, m->s);
+    ++g_launches;
+    int r = finish_norms(m, m->work, &local.residual_max, &local.residual_rms);
+    if (r) return r;
+  }
+  launch_projection(g, m->pi, m->u[cur], m->v[cur], m->s);
+  ++g_launches;
+  if (m->c.pressure_timing) {
+    launch_divergence_field(g, m->u[cur], m->v[cur], m->h[cur], m->work, m->s);
+    ++g_launches;
+    int r = finish_norms(m, m->work, &local.div_max, &local.div_rms);
+    if (r) return r;
+  }
+  PAWSIM_CUDA_OK(cudaGetLastError());
+  if (st) *st = local;
+  return iters;
+}
+
+}  // namespace pawsim
+
+using namespace pawsim;
+
+struct pawsim_gpu {
+  Model* m;
+};
+
+extern "C" {
+
+int pawsim_gpu_create(const pawsim_gpu_config* cfg, pawsim_gpu** out) {
+  if (!cfg || !out) return fail(PAWSIM_GPU_EBADCONFIG, "null argument");
+  Model* m = nullptr;
+  int r = create(cfg, &m);
+  if (r) return r;
+  *out = new pawsim_gpu{m};
+  return 0;
+}
+
+void pawsim_gpu_destroy(pawsim_gpu* h) {
+  if (!h) return;
+  delete h->m;
+  delete h;
+}
+
+int pawsim_gpu_set_field(pawsim_gpu* h, const char* name, int k, const double* host, size_t n) {
+  if (!h || !host) return fail(PAWSIM_GPU_EBADNAME, "null argument");
+  return set_field(h->m, name, k, host, n);
+}
+
+int pawsim_gpu_get_field(pawsim_gpu* h, const char* name, int k, double* host, size_t n) {
+  if (!h || !host) return fail(PAWSIM_GPU_EBADNAME, "null argument");
+  return get_field(h->m, name, k, host, n);
+}
+
+int pawsim_gpu_init(pawsim_gpu* h) { return h ? init(h->m) : PAWSIM_GPU_EBADCONFIG; }
+
+int pawsim_gpu_tendency_eval(pawsim_gpu* h) {
+  if (!h) return PAWSIM_GPU_EBADCONFIG;
+  int r = tendency_eval(h->m);
+  if (r) return r;
+  PAWSIM_CUDA_OK(cudaStreamSynchronize(h->m->s));
+  return 0;
+}
+
+int pawsim_gpu_integrator_step(pawsim_gpu* h, unsigned n) {
+  if (!h) return PAWSIM_GPU_EBADCONFIG;
+  return integrator_step(h->m, n, false);
+}
+
+int pawsim_gpu_pressure_correct(pawsim_gpu* h, int update_diags, pawsim_gpu_stats* st) {
+  if (!h) return PAWSIM_GPU_EBADCONFIG;
+  int r = pressure_correct(h->m, update_diags, st);
+  return r < 0 ? r : 0;
+}
+
+int pawsim_gpu_prelim(pawsim_gpu* h, pawsim_gpu_stats* st) {
+  if (!h) return PAWSIM_GPU_EBADCONFIG;
+  Model* m = h->m;
+  if (!m->ready) {
+    int r = init(m);
+    if (r) return r;
+  }
+  m->thickness_fixed = false;
+  int r = pressure_correct(m, 0, st);
+  if (r < 0) return r;
+  r = tendency_eval(m);   // rebuilds wdia for the n = 0 output, as pawsim.c:296-300 does
+  if (r) return r;
+  PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
+  return 0;
+}
+
+int pawsim_gpu_step(pawsim_gpu* h, unsigned n, pawsim_gpu_stats* st) {
+  if (!h) return PAWSIM_GPU_EBADCONFIG;
+  int r = integrator_step(h->m, n, true);
+  if (r) return r;
+  r = pressure_correct(h->m, 1, st);
+  return r < 0 ? r : 0;
+}
+
+int pawsim_gpu_run(pawsim_gpu* h, unsigned n0, unsigned nsteps, pawsim_gpu_stats* st) {
+  if (!h) return PAWSIM_GPU_EBADCONFIG;
+  for (unsigned n = n0; n < n0 + nsteps; ++n) {
+    int r = pawsim_gpu_step(h, n, st);
+    if (r) return r;
+  }
+  return 0;
+}
+
+int pawsim_gpu_solve_mg(pawsim_gpu* h, pawsim_gpu_stats* st) {
+  if (!h) return PAWSIM_GPU_EBADCONFIG;
+  Model* m = h->m;
+  if (!m->mg) return fail(PAWSIM_GPU_EBADCONFIG, "multigrid not configured");
+  double mres = 0;
+  PAWSIM_CUDA_OK(cudaEventRecord(m->ev0, m->s));
+  int it = m->mg->solve(m->pi, m->pitch, m->rhs, m->pitch, m->c.pi_tol, m->c.maxiters, &mres);
+  PAWSIM_CUDA_OK(cudaEventRecord(m->ev1, m->s));
+  PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
+  if (st) {
+    memset(st, 0, sizeof(*st));
+    st->iters = it;
+    st->stop_measure = mres;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, m->ev0, m->ev1);
+    st->solve_ms = ms;
+  }
+  return 0;
+}
+
+int pawsim_gpu_set_stream(pawsim_gpu* h, void* stream) {
+  if (!h) return PAWSIM_GPU_EBADCONFIG;
+  h->m->s = (cudaStream_t)stream;
+  if (h->m->mg) h->m->mg->set_stream(h->m->s);
+  return 0;
+}
+
+int pawsim_gpu_synchronize(pawsim_gpu* h) {
+  if (!h) return PAWSIM_GPU_EBADCONFIG;
+  PAWSIM_CUDA_OK(cudaStreamSynchronize(h->m->s));
+  return 0;
+}
+
+double pawsim_gpu_time(const pawsim_gpu* h) { return h ? h->m->t : 0.0; }
+
+long long pawsim_gpu_launch_count(const pawsim_gpu* h) {
+  (void)h;
+  return g_launches;
+}
+
+const char* pawsim_gpu_last_error(void) { return g_err; }
+
+}  // extern "C"

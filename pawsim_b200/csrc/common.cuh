@@ -1,0 +1,87 @@
+// common.cuh -- device-side layout, boundary mapping and launch helpers.
+//
+// Layout: every 2-D field is FP64 (or FP32 inside the multigrid preconditioner), x fastest
+// (the AWSIM disk order), rows of `pitch` elements (a multiple of 32, so every row starts on
+// a 256-byte boundary), layers `lstride = Ny*pitch` apart. Only owned cells are stored; the
+// reference's 3-cell ghost ring (model_code/pawsim.c:28) and its halo exchanges
+// (model_code/field.c:121-241) are replaced by the index maps below, applied at load time.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pawsim {
+
+// Boundary behaviour of a field along one axis (model_code/field.c:158-241):
+//   MAP_S  scalar and wall-parallel velocity: mirror about the wall (F(-1) = F(0))
+//   MAP_N  wall-normal velocity: zero on the wall face, odd mirror beyond it
+//          (F(0) = +0, F(-i) = -F(i), F(N) = -0, F(N+i) = -F(N-i))
+//   MAP_Q  q-grid: nearest of the N+1 stored lines
+enum MapKind { MAP_S = 0, MAP_N = 1, MAP_Q = 2 };
+
+struct AxisMap {
+  int idx;      // source index in [0, N) (or [0, N] for MAP_Q)
+  double sgn;   // +1 or -1
+  bool zero;    // value is a signed zero (sgn carries the sign)
+};
+
+__host__ __device__ inline int wrap_index(int i, int n) {
+  int r = i % n;
+  return r < 0 ? r + n : r;
+}
+
+// Map a raw coordinate i (any integer within a few cells of [0, N)) to storage.
+__host__ __device__ inline AxisMap map_axis(int i, int n, bool wall, int kind) {
+  AxisMap m;
+  m.sgn = 1.0;
+  m.zero = false;
+  if (!wall) {
+    m.idx = wrap_index(i, n);
+    return m;
+  }
+  if (kind == MAP_Q) {
+    m.idx = i < 0 ? 0 : (i > n ? n : i);
+    return m;
+  }
+  if (kind == MAP_S) {
+    if (i < 0) m.idx = -i - 1;
+    else if (i >= n) m.idx = 2 * n - i - 1;
+    else m.idx = i;
+    return m;
+  }
+  // MAP_N
+  if (i == 0) { m.idx = 0; m.zero = true; return m; }
+  if (i == n) { m.idx = 0; m.zero = true; m.sgn = -1.0; return m; }
+  if (i < 0) { m.idx = -i; m.sgn = -1.0; return m; }
+  if (i > n) { m.idx = 2 * n - i; m.sgn = -1.0; return m; }
+  m.idx = i;
+  return m;
+}
+
+// Read a field at raw (i, j) with the x and y boundary kinds of that field. The sign of
+// a wall zero follows the reference exactly (+0 on the west/south face, -0 on east/north).
+__host__ __device__ inline double load_mapped(const double* __restrict__ f, int pitch, int i, int j,
+                                              int nx, int ny, bool wx, bool wy, int kx, int ky) {
+  AxisMap ax = map_axis(i, nx, wx, kx);
+  if (ax.zero) return ax.sgn * 0.0;
+  AxisMap ay = map_axis(j, ny, wy, ky);
+  if (ay.zero) return ay.sgn * 0.0;
+  double v = f[(size_t)ay.idx * pitch + ax.idx];
+  return (ax.sgn * ay.sgn < 0) ? -v : v;
+}
+
+inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+}  // namespace pawsim
+
+#define PAWSIM_CUDA_OK(call)                                     \
+  do {                                                           \
+    cudaError_t _e = (call);                                     \
+    if (_e != cudaSuccess) return ::pawsim::set_cuda_error(_e, #call, __FILE__, __LINE__); \
+  } while (0)
+
+namespace pawsim {
+int set_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+// kernels launched by this library since load (reported by pawsim_gpu_launch_count)
+extern long long g_launches;
+}

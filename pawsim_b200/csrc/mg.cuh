@@ -1,0 +1,72 @@
+// mg.cuh -- geometric multigrid for the rigid-lid pressure equation on the GPU.
+//
+// Same hierarchy, operator, restriction and prolongation as the reference's serial AWSIM
+// multigrid (model_code/multigrid.c:196-446, 651-932): levels (N+1)/2 down to 1 x 1,
+// Ow = Hw/dx^2 and Os = Hs/dy^2 with wall faces zeroed, 2x2 means (area-weighted for
+// uneven pairs) and bilinear prolongation with the wall and corner weights. The smoother
+// is red-black Gauss-Seidel (weight `omega_rb`) instead of the reference's in-place
+// lexicographic sweep, which has no parallel form; convergence is judged by the
+// reference's own test, max |pi - Jacobi(pi)| <= tol (multigrid.c:1123-1156).
+// Two precisions: plain FP64 V-cycles on pi, or FP32 V-cycles on the correction inside an
+// FP64 defect-correction loop (the residual, the update of pi and the test stay FP64).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+namespace pawsim {
+
+struct MGOptions {
+  int fp32_cycles = 0;     // 0: FP64 V-cycles, 1: FP32 V-cycles in FP64 defect correction
+  int pre = 1, post = 1;   // red-black sweeps before and after the coarse correction
+  double omega_rb = 1.0;   // smoother weight
+  int full_mg = 0;         // use_fullMG: nested iteration from the coarsest level
+};
+
+class Multigrid {
+ public:
+  // Hc: host array Nx*Ny (x fastest) of the water-column thickness
+  Multigrid(int Nx, int Ny, double Lx, double Ly, bool wall_ew, bool wall_ns, const double* Hc_host,
+            const MGOptions& opt, cudaStream_t s);
+  ~Multigrid();
+  bool ok() const { return ok_; }
+  // Solve in place on the fine pi (pitched FP64); returns the V-cycle count.
+  // maxres_out receives max |pi - Jacobi(pi)| of the last check.
+  int solve(double* pi, int pi_pitch, const double* rhs, int rhs_pitch, double tol, int maxiters,
+            double* maxres_out);
+  // one evaluation of the stopping measure (for diagnostics and warm-start decisions)
+  double max_residual(const double* pi, int pi_pitch, const double* rhs, int rhs_pitch);
+  void set_options(const MGOptions& o) { opt_ = o; }
+  const MGOptions& options() const { return opt_; }
+  int levels() const { return (int)lv_.size(); }
+  cudaStream_t stream() const { return s_; }
+  void set_stream(cudaStream_t s) { s_ = s; }
+
+  struct Level {
+    int Nx, Ny, pitch;
+    bool power2;          // transfer to the next coarser level is exactly 2:1
+    double *Ow, *Os, *Osum, *rOsum;     // FP64 operator
+    float *Ow32, *Os32, *Osum32, *rOsum32;
+    double *e, *rhs, *res;              // FP64 work
+    float *e32, *rhs32, *res32;         // FP32 work
+  };
+
+ private:
+  template <typename T> void vcycle(int n);
+  template <typename T> void smooth(int n, int sweeps);
+  void set_fine(double* pi, int pitch, const double* rhs, int rhs_pitch);
+  bool ok_ = false;
+  int Nx_, Ny_;
+  bool wew_, wns_;
+  MGOptions opt_;
+  cudaStream_t s_;
+  std::vector<Level> lv_;   // index 0 is the coarsest
+  double* dmax_ = nullptr;  // device scalar
+  unsigned long long* dbits_ = nullptr;
+  double* fine_pi_ = nullptr;
+  const double* fine_rhs_ = nullptr;
+  int fine_pitch_ = 0, fine_rhs_pitch_ = 0;
+};
+
+}  // namespace pawsim

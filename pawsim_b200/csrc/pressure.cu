@@ -1,0 +1,399 @@
+// pressure.cu -- rigid-lid pressure kernels (RHS, mean, SOR, projection, diagnostics).
+//
+// Compiled with -fmad=false; every expression keeps the association order of
+// model_code/pressure.c so the SOR path reproduces the reference bit for bit.
+#include <cooperative_groups.h>
+
+#include "common.cuh"
+#include "pressure.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace pawsim {
+
+namespace {
+
+__device__ inline double ld_s(const double* f, const Grid2& g, int i, int j) {
+  return load_mapped(f, g.pitch, i, j, g.Nx, g.Ny, g.wall_ew, g.wall_ns, MAP_S, MAP_S);
+}
+
+// Gathered face thickness with wrapped indices (work.c:865-1030), at an owned cell.
+__device__ inline double hw_gathered(const Grid2& g, const double* h, int i, int j) {
+  int Nx = g.Nx, Ny = g.Ny;
+  int im1 = wrap_index(i - 1, Nx), ip1 = wrap_index(i + 1, Nx);
+  int jm1 = wrap_index(j - 1, Ny), jp1 = wrap_index(j + 1, Ny);
+  const int P = g.pitch;
+#define H(ii, jj) h[(size_t)(jj) * P + (ii)]
+  if (g.thick_scheme == 1) {
+    if (g.wall_ns && j == 0)
+      return (1.0 / 3) * (1.25 * (H(i, j) + H(im1, j)) + 0.25 * (H(i, jp1) + H(im1, jp1)));
+    if (g.wall_ns && j == Ny - 1)
+      return (1.0 / 3) * (1.25 * (H(i, j) + H(im1, j)) + 0.25 * (H(i, jm1) + H(im1, jm1)));
+    return (1.0 / 3) * (H(i, j) + H(im1, j) + 0.25 * (H(i, jp1) + H(im1, jp1) + H(i, jm1) + H(im1, jm1)));
+  }
+  (void)ip1;
+  return 0.5 * (H(i, j) + H(im1, j));
+}
+
+__device__ inline double hs_gathered(const Grid2& g, const double* h, int i, int j) {
+  int Nx = g.Nx, Ny = g.Ny;
+  int im1 = wrap_index(i - 1, Nx), ip1 = wrap_index(i + 1, Nx);
+  int jm1 = wrap_index(j - 1, Ny);
+  const int P = g.pitch;
+  if (g.thick_scheme == 1) {
+    if (g.wall_ew && i == 0)
+      return (1.0 / 3) * (1.25 * (H(i, j) + H(i, jm1)) + 0.25 * (H(ip1, j) + H(ip1, jm1)));
+    if (g.wall_ew && i == Nx - 1)
+      return (1.0 / 3) * (1.25 * (H(i, j) + H(i, jm1)) + 0.25 * (H(im1, j) + H(im1, jm1)));
+    return (1.0 / 3) * (H(i, j) + H(i, jm1) + 0.25 * (H(ip1, j) + H(im1, j) + H(ip1, jm1) + H(im1, jm1)));
+  }
+  return 0.5 * (H(i, j) + H(i, jm1));
+#undef H
+}
+
+// the gathered face arrays are scalar-filled afterwards: a face one past the last cell
+// copies the last face on a wall and the first face when periodic (field.c:121-241)
+__device__ inline double hw_face(const Grid2& g, const double* h, int i, int j) {
+  if (i >= g.Nx) i = g.wall_ew ? 2 * g.Nx - i - 1 : i - g.Nx;
+  return hw_gathered(g, h, i, j);
+}
+__device__ inline double hs_face(const Grid2& g, const double* h, int i, int j) {
+  if (j >= g.Ny) j = g.wall_ns ? 2 * g.Ny - j - 1 : j - g.Ny;
+  return hs_gathered(g, h, i, j);
+}
+
+__device__ inline double ld_u(const Grid2& g, const double* u, int i, int j) {
+  return load_mapped(u, g.pitch, i, j, g.Nx, g.Ny, g.wall_ew, g.wall_ns, MAP_N, MAP_S);
+}
+__device__ inline double ld_v(const Grid2& g, const double* v, int i, int j) {
+  return load_mapped(v, g.pitch, i, j, g.Nx, g.Ny, g.wall_ew, g.wall_ns, MAP_S, MAP_N);
+}
+
+__global__ void rhs_kernel(const Grid2 g, const double* __restrict__ u, const double* __restrict__ v,
+                           const double* __restrict__ h, double* __restrict__ rhs, int with_dt) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.Nx || j >= g.Ny) return;
+  double acc = 0;
+  double dxdt = g.dx * g.dt, dydt = g.dy * g.dt;
+  for (int k = 0; k < g.L; ++k) {
+    const double* uk = u + k * g.lstride;
+    const double* vk = v + k * g.lstride;
+    const double* hk = h + k * g.lstride;
+    double hu_w = ld_u(g, uk, i, j) * hw_face(g, hk, i, j);
+    double hu_e = ld_u(g, uk, i + 1, j) * hw_face(g, hk, i + 1, j);
+    double hv_s = ld_v(g, vk, i, j) * hs_face(g, hk, i, j);
+    double hv_n = ld_v(g, vk, i, j + 1) * hs_face(g, hk, i, j + 1);
+    if (with_dt)
+      acc += (hu_e - hu_w) / dxdt + (hv_n - hv_s) / dydt;
+    else
+      acc += (hu_e - hu_w) / g.dx + (hv_n - hv_s) / g.dy;
+  }
+  rhs[(size_t)j * g.pitch + i] = acc;
+}
+
+// ---------------------------------------------------------------- reductions
+
+constexpr int RED_BLOCK = 256;
+constexpr int RED_ROWS = 8;   // rows per partial in the tree sum
+
+// serial order of pressure.c:62-69: x outer, y inner. One thread; loads are batched so
+// that the dependent additions, not the memory latency, set the pace.
+__global__ void serial_sum_kernel(const double* __restrict__ f, int Nx, int Ny, int pitch,
+                                  double* out, int squares) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double s = 0;
+  for (int i = 0; i < Nx; ++i) {
+    int j = 0;
+    for (; j + 8 <= Ny; j += 8) {
+      double a[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) a[q] = f[(size_t)(j + q) * pitch + i];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) s += squares ? a[q] * a[q] : a[q];
+    }
+    for (; j < Ny; ++j) {
+      double a = f[(size_t)j * pitch + i];
+      s += squares ? a * a : a;
+    }
+  }
+  out[0] = s;
+}
+
+// fixed-shape tree: each block sums RED_ROWS rows (one column per thread, looping over
+// columns), then a fixed shuffle tree; a second pass adds the partials in index order.
+__global__ void tree_partial_kernel(const double* __restrict__ f, int Nx, int Ny, int pitch,
+                                    double* partials, int squares) {
+  __shared__ double ws[RED_BLOCK / 32];
+  int r0 = blockIdx.x * RED_ROWS;
+  double s = 0;
+  for (int r = r0; r < r0 + RED_ROWS && r < Ny; ++r)
+    for (int i = threadIdx.x; i < Nx; i += RED_BLOCK) {
+      double a = f[(size_t)r * pitch + i];
+      s += squares ? a * a : a;
+    }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < RED_BLOCK / 32; ++w) t += ws[w];
+    partials[blockIdx.x] = t;
+  }
+}
+
+__global__ void tree_final_kernel(const double* partials, int n, double* out) {
+  __shared__ double ws[RED_BLOCK / 32];
+  double s = 0;
+  for (int i = threadIdx.x; i < n; i += RED_BLOCK) s += partials[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < RED_BLOCK / 32; ++w) t += ws[w];
+    out[0] = t;
+  }
+}
+
+__global__ void max_abs_kernel(const double* __restrict__ f, int Nx, int Ny, int pitch,
+                               unsigned long long* out) {
+  // fmax semantics: NaN entries are ignored, as C's fmax does
+  double m = 0;
+  int n = Nx * Ny;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    double a = fabs(f[(size_t)(q / Nx) * pitch + (q % Nx)]);
+    m = fmax(m, a);
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+__global__ void store_max_kernel(const unsigned long long* bits, double* out) {
+  out[0] = __longlong_as_double((long long)bits[0]);
+}
+
+__global__ void subtract_mean_kernel(double* f, int Nx, int Ny, int pitch, const double* sum) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= Nx || j >= Ny) return;
+  double mean = sum[0] / ((double)Nx * (double)Ny);
+  f[(size_t)j * pitch + i] -= mean;
+}
+
+// ------------------------------------------------------------------ operator
+
+__global__ void operator_kernel(const Grid2 g, const double* __restrict__ Hc, Operator op, double sor_rp) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  // Ow on faces i in [0, Nx], Os on faces j in [0, Ny] (pressure.c:609-637): Hw, Hs are the
+  // centered averages of Hc (work.c:1160-1166), scalar-filled past the last cell.
+  if (i <= g.Nx && j < g.Ny) {
+    double Hw = 0.5 * (ld_s(Hc, g, i, j) + ld_s(Hc, g, i - 1, j));
+    if (i == g.Nx) {
+      int ii = g.wall_ew ? g.Nx - 1 : 0;
+      Hw = 0.5 * (ld_s(Hc, g, ii, j) + ld_s(Hc, g, ii - 1, j));
+    }
+    double o = Hw / (g.dx * g.dx);
+    if (g.wall_ew && (i == 0 || i == g.Nx)) o = 0;
+    op.Ow[(size_t)j * op.opitch + i] = o;
+  }
+  if (i < g.Nx && j <= g.Ny) {
+    double Hs = 0.5 * (ld_s(Hc, g, i, j) + ld_s(Hc, g, i, j - 1));
+    if (j == g.Ny) {
+      int jj = g.wall_ns ? g.Ny - 1 : 0;
+      Hs = 0.5 * (ld_s(Hc, g, i, jj) + ld_s(Hc, g, i, jj - 1));
+    }
+    double o = Hs / (g.dy * g.dy);
+    if (g.wall_ns && (j == 0 || j == g.Ny)) o = 0;
+    op.Os[(size_t)j * op.opitch + i] = o;
+  }
+}
+
+__global__ void sor_factor_kernel(const Grid2 g, Operator op, double sor_rp) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.Nx || j >= g.Ny) return;
+  double Ow = op.Ow[(size_t)j * op.opitch + i], Oe = op.Ow[(size_t)j * op.opitch + i + 1];
+  double Os = op.Os[(size_t)j * op.opitch + i], On = op.Os[(size_t)(j + 1) * op.opitch + i];
+  double Osum = Ow + Oe + Os + On;
+  op.csor[(size_t)j * g.pitch + i] = (Osum == 0) ? 0.0 : sor_rp / Osum;
+}
+
+// ----------------------------------------------------------------------- SOR
+
+__device__ inline double sor_point(const Grid2& g, double* pi, const double* rhs, const Operator& op,
+                                   double one_minus_w, int i, int j) {
+  size_t c = (size_t)j * g.pitch + i;
+  double cs = op.csor[c];
+  if (cs == 0) return 0;   // Osum == 0: the reference skips the cell
+  double Ow = op.Ow[(size_t)j * op.opitch + i], Oe = op.Ow[(size_t)j * op.opitch + i + 1];
+  double Os = op.Os[(size_t)j * op.opitch + i], On = op.Os[(size_t)(j + 1) * op.opitch + i];
+  double pn = ld_s(pi, g, i, j + 1), ps = ld_s(pi, g, i, j - 1);
+  double pe = ld_s(pi, g, i + 1, j), pw = ld_s(pi, g, i - 1, j);
+  double prev = pi[c];
+  double nw = one_minus_w * prev + cs * (On * pn + Os * ps + Oe * pe + Ow * pw - rhs[c]);
+  pi[c] = nw;
+  double d = fabs(nw - prev);
+  return d;
+}
+
+__global__ void __launch_bounds__(512) sor_kernel(const Grid2 g, double* pi, const double* __restrict__ rhs,
+                                                  const Operator op, double sor_rp, double tol, int maxiters,
+                                                  unsigned long long* slots, int* iters_out) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double wmax[16];
+  const double one_minus_w = 1 - sor_rp;
+  const int n = g.Nx * g.Ny;
+  const int stride = gridDim.x * blockDim.x;
+  int iters = 0;
+  double gmax = tol + 1;
+  if (blockIdx.x == 0 && threadIdx.x == 0) { slots[0] = 0; slots[1] = 0; }
+  grid.sync();
+  while ((gmax > tol) && (iters < maxiters)) {
+    double lmax = 0;
+    for (int color = 0; color < 2; ++color) {
+      for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
+        int j = q / g.Nx, i = q % g.Nx;
+        if (((i + j) & 1) != color) continue;
+        double d = sor_point(g, pi, rhs, op, one_minus_w, i, j);
+        lmax = fmax(lmax, d);
+      }
+      grid.sync();
+    }
+    for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_down_sync(0xffffffffu, lmax, o));
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = lmax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double b = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b = fmax(b, wmax[w]);
+      atomicMax(&slots[iters & 1], (unsigned long long)__double_as_longlong(b));
+    }
+    grid.sync();
+    gmax = __longlong_as_double((long long)slots[iters & 1]);
+    if (blockIdx.x == 0 && threadIdx.x == 0) slots[(iters + 1) & 1] = 0;
+    ++iters;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) iters_out[0] = iters;
+}
+
+// ---------------------------------------------------------------- projection
+
+__global__ void projection_kernel(const Grid2 g, const double* __restrict__ pi, double* u, double* v) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.Nx || j >= g.Ny) return;
+  size_t c = (size_t)j * g.pitch + i;
+  double pc = pi[c];
+  double pw = ld_s(pi, g, i - 1, j), ps = ld_s(pi, g, i, j - 1);
+  bool skip_u = g.wall_ew && i == 0;
+  bool skip_v = g.wall_ns && j == 0;
+  for (int k = 0; k < g.L; ++k) {
+    size_t o = k * g.lstride + c;
+    if (!skip_u) u[o] += -g.dt * (pc - pw) / g.dx;
+    if (!skip_v) v[o] += -g.dt * (pc - ps) / g.dy;
+  }
+}
+
+__global__ void residual_field_kernel(const Grid2 g, const double* __restrict__ pi, const double* __restrict__ rhs,
+                                      const Operator op, double* out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.Nx || j >= g.Ny) return;
+  size_t c = (size_t)j * g.pitch + i;
+  double Ow = op.Ow[(size_t)j * op.opitch + i], Oe = op.Ow[(size_t)j * op.opitch + i + 1];
+  double Os = op.Os[(size_t)j * op.opitch + i], On = op.Os[(size_t)(j + 1) * op.opitch + i];
+  double pc = pi[c];
+  double Lp = Oe * (ld_s(pi, g, i + 1, j) - pc) + Ow * (ld_s(pi, g, i - 1, j) - pc)
+            + On * (ld_s(pi, g, i, j + 1) - pc) + Os * (ld_s(pi, g, i, j - 1) - pc);
+  out[c] = rhs[c] - Lp;
+}
+
+inline dim3 grid2(int Nx, int Ny, dim3 b) { return dim3((Nx + b.x - 1) / b.x, (Ny + b.y - 1) / b.y); }
+
+}  // namespace
+
+void launch_pressure_rhs(const Grid2& g, const double* u, const double* v, const double* h, double* rhs,
+                         cudaStream_t s) {
+  dim3 b(32, 8);
+  rhs_kernel<<<grid2(g.Nx, g.Ny, b), b, 0, s>>>(g, u, v, h, rhs, 1);
+}
+
+void launch_divergence_field(const Grid2& g, const double* u, const double* v, const double* h, double* out,
+                             cudaStream_t s) {
+  dim3 b(32, 8);
+  rhs_kernel<<<grid2(g.Nx, g.Ny, b), b, 0, s>>>(g, u, v, h, out, 0);
+}
+
+size_t reduce_scratch_elems(int Nx, int Ny) { (void)Nx; return (size_t)(Ny + RED_ROWS - 1) / RED_ROWS + 4; }
+
+void launch_sum(const double* f, int Nx, int Ny, int pitch, bool serial, double* partials, double* out,
+                cudaStream_t s) {
+  if (serial) {
+    serial_sum_kernel<<<1, 32, 0, s>>>(f, Nx, Ny, pitch, out, 0);
+    return;
+  }
+  int nb = (Ny + RED_ROWS - 1) / RED_ROWS;
+  tree_partial_kernel<<<nb, RED_BLOCK, 0, s>>>(f, Nx, Ny, pitch, partials, 0);
+  tree_final_kernel<<<1, RED_BLOCK, 0, s>>>(partials, nb, out);
+}
+
+void launch_subtract_mean(double* f, int Nx, int Ny, int pitch, const double* sum, cudaStream_t s) {
+  dim3 b(32, 8);
+  subtract_mean_kernel<<<grid2(Nx, Ny, b), b, 0, s>>>(f, Nx, Ny, pitch, sum);
+}
+
+void launch_norms(const double* f, int Nx, int Ny, int pitch, bool serial, double* partials, double* out,
+                  cudaStream_t s) {
+  // out[0] = max |f| (via an integer max on the bit pattern, in out[2] as scratch), out[1] = sum f^2
+  unsigned long long* bits = reinterpret_cast<unsigned long long*>(out + 2);
+  cudaMemsetAsync(bits, 0, sizeof(unsigned long long), s);
+  max_abs_kernel<<<148, 256, 0, s>>>(f, Nx, Ny, pitch, bits);
+  store_max_kernel<<<1, 1, 0, s>>>(bits, out);
+  if (serial) {
+    serial_sum_kernel<<<1, 32, 0, s>>>(f, Nx, Ny, pitch, out + 1, 1);
+  } else {
+    int nb = (Ny + RED_ROWS - 1) / RED_ROWS;
+    tree_partial_kernel<<<nb, RED_BLOCK, 0, s>>>(f, Nx, Ny, pitch, partials, 1);
+    tree_final_kernel<<<1, RED_BLOCK, 0, s>>>(partials, nb, out + 1);
+  }
+}
+
+void launch_operator(const Grid2& g, const double* Hc, const Operator& op, double sor_rp, cudaStream_t s) {
+  dim3 b(32, 8);
+  operator_kernel<<<grid2(g.Nx + 1, g.Ny + 1, b), b, 0, s>>>(g, Hc, op, sor_rp);
+  sor_factor_kernel<<<grid2(g.Nx, g.Ny, b), b, 0, s>>>(g, op, sor_rp);
+}
+
+int launch_sor(const Grid2& g, double* pi, const double* rhs, const Operator& op, double sor_rp, double tol,
+               int maxiters, unsigned long long* slots, int* iters, cudaStream_t s) {
+  int dev = 0, nsm = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int threads = 512;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sor_kernel, threads, 0);
+  int want = (g.Nx * g.Ny + threads - 1) / threads;
+  int cap = nsm * (per_sm < 1 ? 1 : per_sm);
+  int blocks = want < cap ? want : cap;
+  if (blocks < 1) blocks = 1;
+  Grid2 gg = g;
+  Operator oo = op;
+  double* ppi = pi;
+  const double* prhs = rhs;
+  void* args[] = {&gg, &ppi, &prhs, &oo, &sor_rp, &tol, &maxiters, &slots, &iters};
+  cudaError_t e = cudaLaunchCooperativeKernel((void*)sor_kernel, dim3(blocks), dim3(threads), args, 0, s);
+  return e == cudaSuccess ? 0 : -1;
+}
+
+void launch_projection(const Grid2& g, const double* pi, double* u, double* v, cudaStream_t s) {
+  dim3 b(32, 8);
+  projection_kernel<<<grid2(g.Nx, g.Ny, b), b, 0, s>>>(g, pi, u, v);
+}
+
+void launch_residual_field(const Grid2& g, const double* pi, const double* rhs, const Operator& op, double* out,
+                           cudaStream_t s) {
+  dim3 b(32, 8);
+  residual_field_kernel<<<grid2(g.Nx, g.Ny, b), b, 0, s>>>(g, pi, rhs, op, out);
+}
+
+}  // namespace pawsim

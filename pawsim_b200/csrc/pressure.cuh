@@ -1,0 +1,58 @@
+// pressure.cuh -- rigid-lid pressure kernels: RHS, mean removal, red-black SOR,
+// projection and the solve-quality diagnostics.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+namespace pawsim {
+
+struct Grid2 {
+  int Nx, Ny, pitch, L;
+  size_t lstride;
+  int wall_ew, wall_ns;
+  double dx, dy, dt;
+  int thick_scheme;
+};
+
+// rhs = sum_k div(h_k u_k) / dt with the gathered face thickness (pressure.c:570-606)
+void launch_pressure_rhs(const Grid2& g, const double* u, const double* v, const double* h,
+                         double* rhs, cudaStream_t s);
+
+// sum of the owned cells in the reference's serial order (x outer, y inner) or in a fixed
+// pairwise tree; the result is written to *out (device). `partials` needs
+// reduce_scratch_elems(n) doubles.
+size_t reduce_scratch_elems(int Nx, int Ny);
+void launch_sum(const double* f, int Nx, int Ny, int pitch, bool serial_order, double* partials,
+                double* out, cudaStream_t s);
+// f -= mean, mean = *sum / (Nx*Ny) (pressure.c:55-88)
+void launch_subtract_mean(double* f, int Nx, int Ny, int pitch, const double* sum, cudaStream_t s);
+
+// operator coefficients Ow, Os (pressure.c:609-637) and the SOR factor SOR_rp/Osum
+struct Operator {
+  double* Ow;    // (Nx+1) columns x Ny rows, pitch `opitch`
+  double* Os;    // Nx columns x (Ny+1) rows, pitch `opitch`
+  double* csor;  // Nx x Ny, pitch `pitch`; 0 marks a cell whose Osum is zero
+  int opitch;
+};
+void launch_operator(const Grid2& g, const double* Hc, const Operator& op, double sor_rp,
+                     cudaStream_t s);
+
+// red-black SOR (pressure.c:743-814) as one persistent cooperative kernel; the iteration
+// count is written to *iters (device int).
+int launch_sor(const Grid2& g, double* pi, const double* rhs, const Operator& op, double sor_rp,
+               double tol, int maxiters, unsigned long long* slots, int* iters, cudaStream_t s);
+
+// u -= dt dpi/dx, v -= dt dpi/dy on every layer, skipping wall faces (pressure.c:2182-2248)
+void launch_projection(const Grid2& g, const double* pi, double* u, double* v, cudaStream_t s);
+
+// per-cell residual rhs - L(pi) and barotropic divergence (pressure.c:652-737)
+void launch_residual_field(const Grid2& g, const double* pi, const double* rhs,
+                           const Operator& op, double* out, cudaStream_t s);
+void launch_divergence_field(const Grid2& g, const double* u, const double* v, const double* h,
+                             double* out, cudaStream_t s);
+// max |f| and sum f^2 (serial order or tree) into out[0], out[1]
+void launch_norms(const double* f, int Nx, int Ny, int pitch, bool serial_order,
+                  double* partials, double* out, cudaStream_t s);
+
+}  // namespace pawsim

@@ -1,0 +1,592 @@
+// tendency.cu -- fused layer tendency + Adams-Bashforth step (the K-tend kernel).
+//
+// One CTA owns a TX x TY tile of cells for every layer. It replaces, for that tile, the
+// reference's whole derivative evaluation and state update:
+//   model_code/tendency.c:81-115 (pawsim_tendency_eval) with the stages of work.c
+//   (face thickness :566-684, eta :1173-1203, PV :1231-1288, PV coefficients :1294-1404,
+//   Bernoulli :1410-1512, momentum :1520-1857, thickness :1864-1941), restoring.c:29-220,
+//   diapycnal.c:72-291, forcing.c:30-395, and the AB1/AB2/AB3 update of
+//   integrator.c:15-198, plus the rigid-lid column correction of pressure.c:525-561.
+// Every intermediate lives in shared memory over exactly the region later stages read.
+// The halo exchanges of field.c become index maps at load time (common.cuh), and each
+// derived field is evaluated either directly at a ghost position (fields the reference
+// computes over its ghost ring) or at the mirrored owned position (fields the reference
+// re-fills after computing them), so results equal the reference's bit for bit. This
+// file is compiled with -fmad=false: no multiply-add is contracted, as in the reference's
+// x86-64 build.
+#include "common.cuh"
+#include "tendency.cuh"
+
+namespace pawsim {
+
+namespace {
+
+constexpr int TX = 32;
+constexpr int TY = 8;
+constexpr int HALO = 2;
+constexpr int RW = TX + 2 * HALO;
+constexpr int RH = TY + 2 * HALO;
+constexpr int RN = RW * RH;
+constexpr int NT = TX * TY;
+enum { F_U, F_V, F_H, F_HW, F_HS, F_QQ, F_HQ, F_KE, F_HUU, F_HVV, F_DT, F_DS, F_U4, F_V4, F_NUM };
+
+struct Tile {
+  int X0, Y0;
+  int Nx, Ny;
+  bool wx, wy;
+  // raw coordinate of local index
+  __device__ int gx(int lx) const { return X0 - HALO + lx; }
+  __device__ int gy(int ly) const { return Y0 - HALO + ly; }
+  // raw position within the band that owned cells can reach (mirrors stay in the tile)
+  __device__ bool near(int lx, int ly) const {
+    int x = gx(lx), y = gy(ly);
+    return x >= -HALO && x < Nx + HALO && y >= -HALO && y < Ny + HALO;
+  }
+  // local index of the owned cell that a filled (mirror-symmetric) field copies at raw x
+  __device__ int mlx(int lx) const {
+    if (!wx) return lx;
+    int g = gx(lx);
+    if (g < 0) g = -g - 1;
+    else if (g >= Nx) g = 2 * Nx - g - 1;
+    return g - X0 + HALO;
+  }
+  __device__ int mly(int ly) const {
+    if (!wy) return ly;
+    int g = gy(ly);
+    if (g < 0) g = -g - 1;
+    else if (g >= Ny) g = 2 * Ny - g - 1;
+    return g - Y0 + HALO;
+  }
+};
+
+#define AT(arr, lx, ly) (arr)[(ly) * RW + (lx)]
+
+__device__ inline double sq(double x) { return x * x; }
+
+// PV interpolation coefficients (work.c:1294-1404) evaluated from qq in shared memory
+template <int MS> struct Coef {
+  const double* q;
+  __device__ double Q(int x, int y) const { return AT(q, x, y); }
+  __device__ double alpha(int i, int j) const {
+    if (MS == 3)
+      return (2 * Q(i + 1, j + 1) + 3 * Q(i, j + 1) + 2 * Q(i, j) + Q(i + 1, j) - Q(i, j + 2) - Q(i - 1, j + 1)) / 24;
+    return (2 * Q(i + 1, j + 1) + Q(i, j + 1) + 2 * Q(i, j) + Q(i + 1, j)) / 24;
+  }
+  __device__ double beta(int i, int j) const {
+    if (MS == 3)
+      return (3 * Q(i, j + 1) + 2 * Q(i - 1, j + 1) + Q(i - 1, j) + 2 * Q(i, j) - Q(i + 1, j + 1) - Q(i, j + 2)) / 24;
+    return (Q(i, j + 1) + 2 * Q(i - 1, j + 1) + Q(i - 1, j) + 2 * Q(i, j)) / 24;
+  }
+  __device__ double gamma(int i, int j) const {
+    if (MS == 3)
+      return (2 * Q(i, j + 1) + Q(i - 1, j + 1) + 2 * Q(i - 1, j) + 3 * Q(i, j) - Q(i, j - 1) - Q(i + 1, j)) / 24;
+    return (2 * Q(i, j + 1) + Q(i - 1, j + 1) + 2 * Q(i - 1, j) + Q(i, j)) / 24;
+  }
+  __device__ double delta(int i, int j) const {
+    if (MS == 3)
+      return (Q(i + 1, j + 1) + 2 * Q(i, j + 1) + 3 * Q(i, j) + 2 * Q(i + 1, j) - Q(i - 1, j) - Q(i, j - 1)) / 24;
+    return (Q(i + 1, j + 1) + 2 * Q(i, j + 1) + Q(i, j) + 2 * Q(i + 1, j)) / 24;
+  }
+  __device__ double epsilon(int i, int j) const {
+    return (Q(i + 1, j + 1) + Q(i, j + 1) - Q(i, j) - Q(i + 1, j)) / 24;
+  }
+  __device__ double phi(int i, int j) const {
+    return (-Q(i + 1, j + 1) + Q(i, j + 1) + Q(i, j) - Q(i + 1, j)) / 24;
+  }
+  __device__ double lambda(int i, int j) const { return (Q(i + 1, j) - Q(i - 1, j)) / 24; }
+  __device__ double mu(int i, int j) const { return (Q(i, j - 1) - Q(i, j + 1)) / 24; }
+};
+
+// face thickness of one layer at a local position (work.c:566-684, AL81 and HK83)
+template <int TS>
+__device__ inline double face_west(const double* h, int i, int j) {
+  if (TS == 1)
+    return (1.0 / 3) * (AT(h, i, j) + AT(h, i - 1, j)
+                        + 0.25 * (AT(h, i, j + 1) + AT(h, i - 1, j + 1) + AT(h, i, j - 1) + AT(h, i - 1, j - 1)));
+  return 0.5 * (AT(h, i, j) + AT(h, i - 1, j));
+}
+template <int TS>
+__device__ inline double face_south(const double* h, int i, int j) {
+  if (TS == 1)
+    return (1.0 / 3) * (AT(h, i, j) + AT(h, i, j - 1)
+                        + 0.25 * (AT(h, i + 1, j) + AT(h, i - 1, j) + AT(h, i + 1, j - 1) + AT(h, i - 1, j - 1)));
+  return 0.5 * (AT(h, i, j) + AT(h, i, j - 1));
+}
+
+// kinetic energy of the Bernoulli function (work.c:1437-1499)
+template <int MS>
+__device__ inline double kinetic(const double* u, const double* v, int i, int j) {
+  if (MS == 1) {
+    return (sq(AT(u, i + 1, j)) + sq(AT(u, i, j))
+            + 0.25 * (sq(AT(u, i + 1, j + 1)) + sq(AT(u, i, j + 1)) + sq(AT(u, i + 1, j - 1)) + sq(AT(u, i, j - 1)))
+            + sq(AT(v, i, j + 1)) + sq(AT(v, i, j))
+            + 0.25 * (sq(AT(v, i + 1, j + 1)) + sq(AT(v, i + 1, j)) + sq(AT(v, i - 1, j + 1)) + sq(AT(v, i - 1, j)))) / 6;
+  }
+  if (MS == 3) {
+    return 0.25 * ((2.0 / 3.0) * sq(AT(u, i, j))
+                   + (1.0 / 3.0) * sq(0.5 * (AT(u, i - 1, j) + AT(u, i + 1, j)))
+                   + (2.0 / 3.0) * sq(AT(u, i + 1, j))
+                   + (1.0 / 3.0) * sq(0.5 * (AT(u, i, j) + AT(u, i + 2, j)))
+                   + (2.0 / 3.0) * sq(AT(v, i, j))
+                   + (1.0 / 3.0) * sq(0.5 * (AT(v, i, j - 1) + AT(v, i, j + 1)))
+                   + (2.0 / 3.0) * sq(AT(v, i, j + 1))
+                   + (1.0 / 3.0) * sq(0.5 * (AT(v, i, j) + AT(v, i, j + 2))));
+  }
+  return (sq(AT(u, i + 1, j)) + sq(AT(u, i, j))) / 4 + (sq(AT(v, i, j + 1)) + sq(AT(v, i, j))) / 4;
+}
+
+__device__ inline double gload(const double* f, const TendParams& p, int gi, int gj, int kx, int ky) {
+  return load_mapped(f, p.pitch, gi, gj, p.Nx, p.Ny, p.wall_ew, p.wall_ns, kx, ky);
+}
+
+// face thickness of another layer at an owned cell, read from global memory
+template <int TS>
+__device__ inline double gface_west(const TendParams& p, const double* h, int i, int j) {
+  if (TS == 1)
+    return (1.0 / 3) * (gload(h, p, i, j, MAP_S, MAP_S) + gload(h, p, i - 1, j, MAP_S, MAP_S)
+                        + 0.25 * (gload(h, p, i, j + 1, MAP_S, MAP_S) + gload(h, p, i - 1, j + 1, MAP_S, MAP_S)
+                                  + gload(h, p, i, j - 1, MAP_S, MAP_S) + gload(h, p, i - 1, j - 1, MAP_S, MAP_S)));
+  return 0.5 * (gload(h, p, i, j, MAP_S, MAP_S) + gload(h, p, i - 1, j, MAP_S, MAP_S));
+}
+template <int TS>
+__device__ inline double gface_south(const TendParams& p, const double* h, int i, int j) {
+  if (TS == 1)
+    return (1.0 / 3) * (gload(h, p, i, j, MAP_S, MAP_S) + gload(h, p, i, j - 1, MAP_S, MAP_S)
+                        + 0.25 * (gload(h, p, i + 1, j, MAP_S, MAP_S) + gload(h, p, i - 1, j, MAP_S, MAP_S)
+                                  + gload(h, p, i + 1, j - 1, MAP_S, MAP_S) + gload(h, p, i - 1, j - 1, MAP_S, MAP_S)));
+  return 0.5 * (gload(h, p, i, j, MAP_S, MAP_S) + gload(h, p, i, j - 1, MAP_S, MAP_S));
+}
+
+template <int MS, int TS>
+__global__ void __launch_bounds__(NT)
+tendency_kernel(const __grid_constant__ TendParams p) {
+  extern __shared__ double smem[];
+  double* F[F_NUM];
+#pragma unroll
+  for (int f = 0; f < F_NUM; ++f) F[f] = smem + f * RN;
+  double* MMall = smem + F_NUM * RN;            // [L][RN]
+  double* WDall = MMall + p.L * RN;             // [L+1][RN] when use_wdia
+
+  const int tid = threadIdx.x;
+  Tile t;
+  t.X0 = blockIdx.x * TX;
+  t.Y0 = blockIdx.y * TY;
+  t.Nx = p.Nx;
+  t.Ny = p.Ny;
+  t.wx = p.wall_ew;
+  t.wy = p.wall_ns;
+  const int L = p.L;
+  const double dx = p.dx, dy = p.dy;
+
+  // ---- column prologue over the Bernoulli region: eta, pp, Montgomery MM, wdia ----
+  for (int q = tid; q < RN; q += NT) {
+    int lx = q % RW, ly = q / RW;
+    if (lx < 1 || lx > TX + 1 || ly < 1 || ly > TY + 1) continue;
+    if (!t.near(lx, ly)) {
+      for (int k = 0; k < L; ++k) MMall[k * RN + q] = 0;
+      if (p.use_wdia)
+        for (int k = 0; k <= L; ++k) WDall[k * RN + q] = 0;
+      continue;
+    }
+    int gi = t.gx(lx), gj = t.gy(ly);
+    double hk[LMAX], eta[LMAX + 1];
+    double hb = gload(p.hhb, p, gi, gj, MAP_S, MAP_S);
+    eta[L] = hb;
+    for (int k = L - 1; k >= 0; --k) {
+      hk[k] = gload(p.h + k * p.lstride, p, gi, gj, MAP_S, MAP_S);
+      eta[k] = eta[k + 1] + hk[k];
+    }
+    double pp = 0;
+    for (int k = 0; k < L; ++k) {
+      if (k == 0) pp = p.use_rl ? 0 : p.gg[0] * eta[0];
+      else pp = pp + p.gg[k] * eta[k];
+      double mm = pp;
+      if (p.h0 != 0) {
+        double h0 = p.h0, hc = hk[k];
+        mm -= p.geff[k] * (h0 * h0 * h0 * h0) / (hc * hc * hc) / 3;
+      }
+      MMall[k * RN + q] = mm;
+    }
+    if (p.use_wdia) {
+      double wd[LMAX + 1];
+      for (int k = 0; k <= L; ++k) {
+        if (p.use_wdia_file) {
+          wd[k] = p.ww0 * gload(p.wd0 + k * p.lstride, p, gi, gj, MAP_S, MAP_S)
+                + p.ww1 * gload(p.wd1 + k * p.lstride, p, gi, gj, MAP_S, MAP_S);
+        } else {
+          wd[k] = 0;
+        }
+      }
+      if (p.use_relax) {
+        double acc = 0;
+        double ht = gload(p.hTime, p, gi, gj, MAP_S, MAP_S);
+        for (int k = L - 1; k >= 0; --k) {
+          if (ht > 0) {
+            acc += (hk[k] - gload(p.hRelax + k * p.lstride, p, gi, gj, MAP_S, MAP_S)) / ht;
+            wd[k] += acc;
+          }
+          double et = gload(p.eTime + k * p.lstride, p, gi, gj, MAP_S, MAP_S);
+          if (et > 0) wd[k] += (eta[k] - gload(p.eRelax + k * p.lstride, p, gi, gj, MAP_S, MAP_S)) / et;
+        }
+      }
+      for (int k = 0; k <= L; ++k) WDall[k * RN + q] = wd[k];
+      if (p.wdia_out && lx >= HALO && lx < HALO + TX && ly >= HALO && ly < HALO + TY && gi < p.Nx && gj < p.Ny) {
+        for (int k = 0; k <= L; ++k) p.wdia_out[k * p.lstride + (size_t)gj * p.pitch + gi] = wd[k];
+      }
+    }
+  }
+
+  // per-thread output cell
+  const int tx = tid % TX, ty = tid / TX;
+  const int ox = tx + HALO, oy = ty + HALO;
+  const int gi = t.X0 + tx, gj = t.Y0 + ty;
+  const bool valid = gi < p.Nx && gj < p.Ny;
+  const size_t cell = (size_t)gj * p.pitch + gi;
+  double hnew[LMAX];
+
+  for (int k = 0; k < L; ++k) {
+    const double* uk = p.u + k * p.lstride;
+    const double* vk = p.v + k * p.lstride;
+    const double* hkp = p.h + k * p.lstride;
+    __syncthreads();
+    // ---- load the layer's u, v, h with the reference's ghost semantics ----
+    for (int q = tid; q < RN; q += NT) {
+      int lx = q % RW, ly = q / RW;
+      int gx = t.gx(lx), gy = t.gy(ly);
+      bool in = gx >= -HALO && gx < p.Nx + HALO && gy >= -HALO && gy < p.Ny + HALO;
+      F[F_U][q] = in ? gload(uk, p, gx, gy, MAP_N, MAP_S) : 0.0;
+      F[F_V][q] = in ? gload(vk, p, gx, gy, MAP_S, MAP_N) : 0.0;
+      F[F_H][q] = in ? gload(hkp, p, gx, gy, MAP_S, MAP_S) : 0.0;
+    }
+    __syncthreads();
+    const double* su = F[F_U];
+    const double* sv = F[F_V];
+    const double* sh = F[F_H];
+    // ---- face thickness, PV, kinetic energy, deformation rates ----
+    for (int q = tid; q < RN; q += NT) {
+      int lx = q % RW, ly = q / RW;
+      const bool nr = t.near(lx, ly);
+      if (lx >= 1 && lx <= TX + 2 && ly >= 1 && ly <= TY + 2 && nr) {
+        int mx = t.mlx(lx), my = t.mly(ly);
+        F[F_HW][q] = face_west<TS>(sh, mx, my);
+        F[F_HS][q] = face_south<TS>(sh, mx, my);
+      }
+      if (lx >= 1 && ly >= 1) {
+        // zeta, h on the q grid and q itself (work.c:1261-1270)
+        double z = (AT(su, lx, ly - 1) - AT(su, lx, ly)) / dy + (AT(sv, lx, ly) - AT(sv, lx - 1, ly)) / dx;
+        double hq = 0.25 * (AT(sh, lx, ly) + AT(sh, lx - 1, ly - 1) + AT(sh, lx - 1, ly) + AT(sh, lx, ly - 1));
+        double om = load_mapped(p.omz, p.qpitch, t.gx(lx), t.gy(ly), p.Nx, p.Ny, p.wall_ew, p.wall_ns, MAP_Q, MAP_Q);
+        F[F_QQ][q] = (2 * om + z) / hq;
+        F[F_HQ][q] = hq;
+      }
+      if (lx >= 1 && lx <= TX + 1 && ly >= 1 && ly <= TY + 1) {
+        F[F_KE][q] = nr ? kinetic<MS>(su, sv, t.mlx(lx), t.mly(ly)) : 0.0;
+      }
+      if (p.useA2 || p.useA4) {
+        if (lx <= TX + 2 && ly <= TY + 2)
+          F[F_DT][q] = (AT(su, lx + 1, ly) - AT(su, lx, ly)) / dx - (AT(sv, lx, ly + 1) - AT(sv, lx, ly)) / dy;
+        if (lx >= 1 && ly >= 1)
+          F[F_DS][q] = (AT(su, lx, ly) - AT(su, lx, ly - 1)) / dy + (AT(sv, lx, ly) - AT(sv, lx - 1, ly)) / dx;
+      }
+    }
+    __syncthreads();
+    // ---- mass fluxes and the biharmonic intermediate velocities ----
+    const double* hw = F[F_HW];
+    const double* hs = F[F_HS];
+    const double* hq = F[F_HQ];
+    const double* DT = F[F_DT];
+    const double* DS = F[F_DS];
+    for (int q = tid; q < RN; q += NT) {
+      int lx = q % RW, ly = q / RW;
+      if (lx >= 1 && lx <= TX + 2 && ly >= 1 && ly <= TY + 1) F[F_HUU][q] = su[q] * hw[q];
+      if (lx >= 1 && lx <= TX + 1 && ly >= 1 && ly <= TY + 2) F[F_HVV][q] = sv[q] * hs[q];
+      if (p.useA4 && lx >= 1 && lx <= TX + 2 && ly >= 1 && ly <= TY + 2) {
+        const double A = p.A4sqrt;
+        F[F_U4][q] = ((A * AT(sh, lx, ly) * AT(DT, lx, ly) - A * AT(sh, lx - 1, ly) * AT(DT, lx - 1, ly)) / dx
+                      + (A * AT(hq, lx, ly + 1) * AT(DS, lx, ly + 1) - A * AT(hq, lx, ly) * AT(DS, lx, ly)) / dy)
+                     / AT(hw, lx, ly);
+        F[F_V4][q] = ((A * AT(hq, lx + 1, ly) * AT(DS, lx + 1, ly) - A * AT(hq, lx, ly) * AT(DS, lx, ly)) / dx
+                      - (A * AT(sh, lx, ly) * AT(DT, lx, ly) - A * AT(sh, lx, ly - 1) * AT(DT, lx, ly - 1)) / dy)
+                     / AT(hs, lx, ly);
+      }
+    }
+    __syncthreads();
+    if (!valid) continue;
+
+    const double* huu = F[F_HUU];
+    const double* hvv = F[F_HVV];
+    const double* KE = F[F_KE];
+    const double* MM = MMall + k * RN;
+    const double* U4 = F[F_U4];
+    const double* V4 = F[F_V4];
+    Coef<MS> c{F[F_QQ]};
+    const double* qq = F[F_QQ];
+    const int i = ox, j = oy;
+    const double hwest = AT(hw, i, j), hsouth = AT(hs, i, j);
+    const double uc = AT(su, i, j), vc = AT(sv, i, j);
+
+    // ---- u momentum (work.c:1667-1752) ----
+    double ru;
+    {
+      double gM = -(AT(MM, i, j) - AT(MM, i - 1, j)) / dx;
+      double gK = -(AT(KE, i, j) - AT(KE, i - 1, j)) / dx;
+      double rq = 0;
+      if (MS == 0 || MS == 1) {
+        rq += c.alpha(i, j) * AT(hvv, i, j + 1) + c.beta(i, j) * AT(hvv, i - 1, j + 1)
+            + c.gamma(i, j) * AT(hvv, i - 1, j) + c.delta(i, j) * AT(hvv, i, j)
+            - c.epsilon(i, j) * AT(huu, i + 1, j) + c.epsilon(i - 1, j) * AT(huu, i - 1, j);
+      } else if (MS == 3) {
+        rq += c.alpha(i, j) * AT(hvv, i, j + 1) + c.beta(i, j) * AT(hvv, i - 1, j + 1)
+            + c.gamma(i, j) * AT(hvv, i - 1, j) + c.delta(i, j) * AT(hvv, i, j)
+            - c.epsilon(i, j) * AT(huu, i + 1, j) + c.epsilon(i - 1, j) * AT(huu, i - 1, j)
+            - c.lambda(i, j + 1) * AT(huu, i, j) + c.lambda(i, j) * AT(huu, i, j - 1);
+      } else {
+        rq += 0.25 * AT(qq, i, j) * (AT(hvv, i, j) + AT(hvv, i - 1, j))
+            + 0.25 * AT(qq, i, j + 1) * (AT(hvv, i, j + 1) + AT(hvv, i - 1, j + 1));
+      }
+      double a2 = 0, a4 = 0;
+      if (p.useA2) {
+        const double A = p.A2;
+        a2 = ((A * AT(sh, i, j) * AT(DT, i, j) - A * AT(sh, i - 1, j) * AT(DT, i - 1, j)) / dx
+              + (A * AT(hq, i, j + 1) * AT(DS, i, j + 1) - A * AT(hq, i, j) * AT(DS, i, j)) / dy);
+      }
+      if (p.useA4) {
+        const double A = p.A4sqrt;
+        double d4t0 = (AT(U4, i + 1, j) - AT(U4, i, j)) / dx - (AT(V4, i, j + 1) - AT(V4, i, j)) / dy;
+        double d4tm = (AT(U4, i, j) - AT(U4, i - 1, j)) / dx - (AT(V4, i - 1, j + 1) - AT(V4, i - 1, j)) / dy;
+        double d4s1 = (AT(U4, i, j + 1) - AT(U4, i, j)) / dy + (AT(V4, i, j + 1) - AT(V4, i - 1, j + 1)) / dx;
+        double d4s0 = (AT(U4, i, j) - AT(U4, i, j - 1)) / dy + (AT(V4, i, j) - AT(V4, i - 1, j)) / dx;
+        a4 = -((A * AT(sh, i, j) * d4t0 - A * AT(sh, i - 1, j) * d4tm) / dx
+               + (A * AT(hq, i, j + 1) * d4s1 - A * AT(hq, i, j) * d4s0) / dy);
+      }
+      ru = gM + gK + rq + ((hwest != 0) ? (a2 + a4 + 0.0) / hwest : 0);
+    }
+    // ---- v momentum (work.c:1759-1852) ----
+    double rv;
+    {
+      double gM = -(AT(MM, i, j) - AT(MM, i, j - 1)) / dy;
+      double gK = -(AT(KE, i, j) - AT(KE, i, j - 1)) / dy;
+      double rq = 0;
+      if (MS == 0 || MS == 1) {
+        rq += c.phi(i, j - 1) * AT(hvv, i, j - 1) - c.phi(i, j) * AT(hvv, i, j + 1)
+            - c.gamma(i + 1, j) * AT(huu, i + 1, j) - c.delta(i, j) * AT(huu, i, j)
+            - c.alpha(i, j - 1) * AT(huu, i, j - 1) - c.beta(i + 1, j - 1) * AT(huu, i + 1, j - 1);
+      } else if (MS == 3) {
+        rq += c.phi(i, j - 1) * AT(hvv, i, j - 1) - c.phi(i, j) * AT(hvv, i, j + 1)
+            - c.gamma(i + 1, j) * AT(huu, i + 1, j) - c.delta(i, j) * AT(huu, i, j)
+            - c.alpha(i, j - 1) * AT(huu, i, j - 1) - c.beta(i + 1, j - 1) * AT(huu, i + 1, j - 1)
+            - c.mu(i + 1, j) * AT(hvv, i, j) + c.mu(i, j) * AT(hvv, i - 1, j);
+      } else {
+        rq -= 0.25 * AT(qq, i, j) * (AT(huu, i, j) + AT(huu, i, j - 1))
+            + 0.25 * AT(qq, i + 1, j) * (AT(huu, i + 1, j) + AT(huu, i + 1, j - 1));
+      }
+      double a2 = 0, a4 = 0;
+      if (p.useA2) {
+        const double A = p.A2;
+        a2 = ((A * AT(hq, i + 1, j) * AT(DS, i + 1, j) - A * AT(hq, i, j) * AT(DS, i, j)) / dx
+              - (A * AT(sh, i, j) * AT(DT, i, j) - A * AT(sh, i, j - 1) * AT(DT, i, j - 1)) / dy);
+      }
+      if (p.useA4) {
+        const double A = p.A4sqrt;
+        double d4s1 = (AT(U4, i + 1, j) - AT(U4, i + 1, j - 1)) / dy + (AT(V4, i + 1, j) - AT(V4, i, j)) / dx;
+        double d4s0 = (AT(U4, i, j) - AT(U4, i, j - 1)) / dy + (AT(V4, i, j) - AT(V4, i - 1, j)) / dx;
+        double d4t0 = (AT(U4, i + 1, j) - AT(U4, i, j)) / dx - (AT(V4, i, j + 1) - AT(V4, i, j)) / dy;
+        double d4tm = (AT(U4, i + 1, j - 1) - AT(U4, i, j - 1)) / dx - (AT(V4, i, j) - AT(V4, i, j - 1)) / dy;
+        a4 = -((A * AT(hq, i + 1, j) * d4s1 - A * AT(hq, i, j) * d4s0) / dx
+               - (A * AT(sh, i, j) * d4t0 - A * AT(sh, i, j - 1) * d4tm) / dy);
+      }
+      rv = gM + gK + rq + ((hsouth != 0) ? (a2 + a4 + 0.0) / hsouth : 0);
+    }
+    // ---- diapycnal advection and viscosity (diapycnal.c:203-291) ----
+    if (p.use_wdia || p.use_diavisc) {
+      if (p.use_wdia) {
+        const double* W0 = WDall + k * RN;
+        const double* W1 = WDall + (k + 1) * RN;
+        double wu0 = 0.5 * (AT(W0, i, j) + AT(W0, i - 1, j));
+        double wu1 = 0.5 * (AT(W1, i, j) + AT(W1, i - 1, j));
+        double wv0 = 0.5 * (AT(W0, i, j) + AT(W0, i, j - 1));
+        double wv1 = 0.5 * (AT(W1, i, j) + AT(W1, i, j - 1));
+        double up = (k == 0) ? 0 : p.u[(k - 1) * p.lstride + cell];
+        double um = (k == L - 1) ? 0 : p.u[(k + 1) * p.lstride + cell];
+        double vp = (k == 0) ? 0 : p.v[(k - 1) * p.lstride + cell];
+        double vm = (k == L - 1) ? 0 : p.v[(k + 1) * p.lstride + cell];
+        // the wall face carries a zero tendency at the end, whatever is accumulated here
+        double dup = (wu0 > 0) ? 0 : up - uc;
+        double dum = (wu1 > 0) ? uc - um : 0;
+        double dvp = (wv0 > 0) ? 0 : vp - vc;
+        double dvm = (wv1 > 0) ? vc - vm : 0;
+        if (hwest != 0) ru += (-(wu0 * dup + wu1 * dum)) / hwest;
+        if (hsouth != 0) rv += (-(wv0 * dvp + wv1 * dvm)) / hsouth;
+      }
+      if (p.use_diavisc && L >= 2) {
+        double Fu[2] = {0, 0}, Fv[2] = {0, 0};
+        for (int s = 0; s < 2; ++s) {
+          int kk = k + s;                    // interface kk between layers kk-1 and kk
+          if (kk < 1 || kk > L - 1) continue;
+          double hwa = gface_west<TS>(p, p.h + (kk - 1) * p.lstride, gi, gj);
+          double hwb = gface_west<TS>(p, p.h + kk * p.lstride, gi, gj);
+          double hsa = gface_south<TS>(p, p.h + (kk - 1) * p.lstride, gi, gj);
+          double hsb = gface_south<TS>(p, p.h + kk * p.lstride, gi, gj);
+          double dzu = 0.5 * (hwb + hwa);
+          double dzv = 0.5 * (hsb + hsa);
+          double nuu = gload(p.nu_u + kk * p.lstride, p, gi, gj, MAP_N, MAP_S);
+          double nuv = gload(p.nu_v + kk * p.lstride, p, gi, gj, MAP_S, MAP_N);
+          double ua = gload(p.u + (kk - 1) * p.lstride, p, gi, gj, MAP_N, MAP_S);
+          double ub = gload(p.u + kk * p.lstride, p, gi, gj, MAP_N, MAP_S);
+          double va = gload(p.v + (kk - 1) * p.lstride, p, gi, gj, MAP_S, MAP_N);
+          double vb = gload(p.v + kk * p.lstride, p, gi, gj, MAP_S, MAP_N);
+          if (dzu != 0) Fu[s] = nuu * (ua - ub) / dzu;
+          if (dzv != 0) Fv[s] = nuv * (va - vb) / dzv;
+        }
+        if (hwest != 0) ru += (Fu[0] - Fu[1]) / hwest;
+        if (hsouth != 0) rv += (Fv[0] - Fv[1]) / hsouth;
+      }
+    }
+    // ---- forcing and drag (forcing.c:245-393); hsml = hbbl = 0 fractions ----
+    {
+      const bool wface_u = p.wall_ew && gi == 0;
+      const bool wface_v = p.wall_ns && gj == 0;
+      double fsw = (k == 0 && !wface_u) ? 1.0 : 0.0;
+      double fss = (k == 0 && !wface_v) ? 1.0 : 0.0;
+      double fbw = (k == L - 1 && !wface_u) ? 1.0 : 0.0;
+      double fbs = (k == L - 1 && !wface_v) ? 1.0 : 0.0;
+      if (p.use_wind) {
+        double tx_ = p.tw0 * p.taux0[cell] + p.tw1 * p.taux1[cell];
+        double ty_ = p.tw0 * p.tauy0[cell] + p.tw1 * p.tauy1[cell];
+        double r = tx_ * fsw;
+        if (hwest != 0) ru += r / hwest;
+        r = ty_ * fss;
+        if (hsouth != 0) rv += r / hsouth;
+      }
+      if (p.use_fbaro) {
+        ru += gload(p.fbx, p, gi, gj, MAP_N, MAP_S);
+        rv += gload(p.fby, p, gi, gj, MAP_S, MAP_N);
+      }
+      if (p.lin_drag > 0) {
+        if (hwest != 0) ru += (-p.lin_drag * uc * fbw) / hwest;
+        if (hsouth != 0) rv += (-p.lin_drag * vc * fbs) / hsouth;
+      }
+      if (p.lin_drag_surf > 0) {
+        if (hwest != 0) {
+          double r = -p.lin_drag_surf * (uc - gload(p.uLid, p, gi, gj, MAP_N, MAP_S)) * fsw;
+          double hsw = 0.5 * (gload(p.hhs, p, gi, gj, MAP_S, MAP_S) + gload(p.hhs, p, gi - 1, gj, MAP_S, MAP_S));
+          if (!p.ocean_surf_drag && p.use_rl && hsw >= 0) r = 0;
+          ru += r / hwest;
+        }
+        if (hsouth != 0) {
+          double r = -p.lin_drag_surf * (vc - gload(p.vLid, p, gi, gj, MAP_S, MAP_N)) * fss;
+          double hss = 0.5 * (gload(p.hhs, p, gi, gj, MAP_S, MAP_S) + gload(p.hhs, p, gi, gj - 1, MAP_S, MAP_S));
+          if (!p.ocean_surf_drag && p.use_rl && hss >= 0) r = 0;
+          rv += r / hsouth;
+        }
+      }
+    }
+    // ---- Newtonian velocity restoring (restoring.c:172-220) ----
+    if (p.use_relax) {
+      double ut = gload(p.uTime + k * p.lstride, p, gi, gj, MAP_N, MAP_S);
+      if (ut > 0) ru += (-(uc - gload(p.uRelax + k * p.lstride, p, gi, gj, MAP_N, MAP_S))) / ut;
+      double vt = gload(p.vTime + k * p.lstride, p, gi, gj, MAP_S, MAP_N);
+      if (vt > 0) rv += (-(vc - gload(p.vRelax + k * p.lstride, p, gi, gj, MAP_S, MAP_N))) / vt;
+    }
+    // the wall-normal tendency is zero on the wall face (field.c:173-176, 216-220)
+    if (p.wall_ew && gi == 0) ru = 0.0;
+    if (p.wall_ns && gj == 0) rv = 0.0;
+    // ---- thickness tendency (work.c:1875-1885) ----
+    double rh;
+    {
+      double adv = (AT(huu, i, j) - AT(huu, i + 1, j)) / dx + (AT(hvv, i, j) - AT(hvv, i, j + 1)) / dy;
+      double rel = 0;
+      if (p.use_wdia) {
+        const double* W0 = WDall + k * RN;
+        const double* W1 = WDall + (k + 1) * RN;
+        rel = -(AT(W0, i, j) - AT(W1, i, j));
+      } else {
+        rel = -(0.0 - 0.0);
+      }
+      rh = adv + rel;
+    }
+    // ---- Adams-Bashforth epilogue (integrator.c:15-69) ----
+    const size_t o = k * p.lstride + cell;
+    if (p.ab_mode == 0) {
+      p.fu_out[o] = ru;
+      p.fv_out[o] = rv;
+      p.fh_out[o] = rh;
+      continue;
+    }
+    double un, vn, hn;
+    const double hc = sh[j * RW + i];
+    if (p.ab_mode == 1) {
+      un = uc + p.c0 * ru;
+      vn = vc + p.c0 * rv;
+      hn = hc + p.c0 * rh;
+    } else if (p.ab_mode == 2) {
+      un = uc + (p.c0 * ru - p.c1 * p.f1u[o]);
+      vn = vc + (p.c0 * rv - p.c1 * p.f1v[o]);
+      hn = hc + (p.c0 * rh - p.c1 * p.f1h[o]);
+    } else {
+      un = uc + (p.c0 * ru - p.c1 * p.f1u[o] + p.c2 * p.f2u[o]);
+      vn = vc + (p.c0 * rv - p.c1 * p.f1v[o] + p.c2 * p.f2v[o]);
+      hn = hc + (p.c0 * rh - p.c1 * p.f1h[o] + p.c2 * p.f2h[o]);
+    }
+    // after the update the reference re-imposes the wall face (field.c:173-176, 216-220)
+    if (p.wall_ew && gi == 0) un = 0.0;
+    if (p.wall_ns && gj == 0) vn = 0.0;
+    if (p.write_hist) {
+      p.fu_out[o] = ru;
+      p.fv_out[o] = rv;
+      p.fh_out[o] = rh;
+    }
+    p.u_out[o] = un;
+    p.v_out[o] = vn;
+    hnew[k] = hn;
+    if (!p.fuse_thickness_fix) p.h_out[o] = hn;
+  }
+
+  // ---- rigid-lid column thickness constraint (pressure.c:525-561) ----
+  if (p.ab_mode != 0 && p.fuse_thickness_fix && valid) {
+    double tot = 0;
+    for (int k = 0; k < L; ++k) tot += hnew[k];
+    if (tot != 0) {
+      double err = tot - p.Hc[cell];
+      for (int k = 0; k < L; ++k) hnew[k] *= (1 - err / tot);
+    }
+    for (int k = 0; k < L; ++k) p.h_out[k * p.lstride + cell] = hnew[k];
+  }
+}
+
+template <int MS, int TS>
+int launch_t(const TendParams& p, cudaStream_t s) {
+  size_t shm = (size_t)(F_NUM + p.L + (p.use_wdia ? p.L + 1 : 0)) * RN * sizeof(double);
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaFuncSetAttribute(tendency_kernel<MS, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_done = true;
+  }
+  dim3 grid((p.Nx + TX - 1) / TX, (p.Ny + TY - 1) / TY);
+  tendency_kernel<MS, TS><<<grid, NT, shm, s>>>(p);
+  return 0;
+}
+
+}  // namespace
+
+int launch_tendency(const TendParams& p, int ms, int ts, cudaStream_t s) {
+  if (p.L < 1 || p.L > LMAX) return -1;
+  if (ts == 0) {
+    switch (ms) {
+      case 0: return launch_t<0, 0>(p, s);
+      case 1: return launch_t<1, 0>(p, s);
+      case 2: return launch_t<2, 0>(p, s);
+      case 3: return launch_t<3, 0>(p, s);
+    }
+  } else if (ts == 1) {
+    switch (ms) {
+      case 0: return launch_t<0, 1>(p, s);
+      case 1: return launch_t<1, 1>(p, s);
+      case 2: return launch_t<2, 1>(p, s);
+      case 3: return launch_t<3, 1>(p, s);
+    }
+  }
+  return -1;
+}
+
+}  // namespace pawsim

@@ -1,0 +1,55 @@
+// tendency.cuh -- parameters of the fused tendency + Adams-Bashforth kernel.
+#pragma once
+
+#include <stddef.h>
+
+namespace pawsim {
+
+constexpr int LMAX = 8;   // layers supported by the fused kernel
+
+struct TendParams {
+  int Nx, Ny, L, pitch, qpitch;
+  size_t lstride;                 // elements between layers
+  int wall_ew, wall_ns;
+  int use_rl;
+  double dx, dy;
+  // Adams-Bashforth epilogue. mode 0 writes the tendency itself to f_out.
+  int ab_mode;                    // 0: tendency only, 1: AB1, 2: AB2, 3: AB3
+  double c0, c1, c2;              // AB coefficients, computed on the host as the reference does
+  int write_hist;                 // store the new tendency into f_out
+  int fuse_thickness_fix;         // apply the rigid-lid column correction to the new h
+  // state and history
+  const double *u, *v, *h;        // S_n
+  double *u_out, *v_out, *h_out;  // S_{n+1} (or unused in mode 0)
+  const double *f1u, *f1v, *f1h;  // tendency one step back
+  const double *f2u, *f2v, *f2h;  // tendency two steps back (may alias f_out)
+  double *fu_out, *fv_out, *fh_out;
+  // statics
+  const double *hhb, *hhs, *Hc, *omz;
+  double gg[LMAX], geff[LMAX];
+  double h0;
+  double A2, A4sqrt;
+  int useA2, useA4;
+  // forcing (model_code/forcing.c)
+  int use_wind, use_fbaro;
+  const double *taux0, *taux1, *tauy0, *tauy1;
+  double tw0, tw1;
+  const double *fbx, *fby;
+  double lin_drag, lin_drag_surf;
+  int ocean_surf_drag;
+  const double *uLid, *vLid;
+  // restoring and diapycnal (model_code/restoring.c, diapycnal.c)
+  int use_relax, use_wdia, use_wdia_file, use_diavisc;
+  const double *wd0, *wd1;        // wDia records n0, n1 (L+1 interfaces each)
+  double ww0, ww1;
+  const double *hRelax, *eRelax, *eTime, *hTime;
+  const double *uRelax, *vRelax, *uTime, *vTime;
+  const double *nu_u, *nu_v;
+  // outputs for diagnostics
+  double *wdia_out;               // interface velocities [L+1] (nullable)
+};
+
+int launch_tendency(const TendParams& p, int momentum_scheme, int thickness_scheme,
+                    cudaStream_t stream);
+
+}  // namespace pawsim
