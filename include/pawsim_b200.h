@@ -127,6 +127,7 @@ PAWSIM_API double pawsim_gpu_time (const pawsim_gpu * m);
 PAWSIM_API long long pawsim_gpu_launch_count (const pawsim_gpu * m);
 PAWSIM_API const char * pawsim_gpu_last_error (void);
 
+
 #ifdef __cplusplus
 }
 #endif

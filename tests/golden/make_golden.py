@@ -1,0 +1,75 @@
+"""Regenerate the golden fixtures from the reference's own serial build.
+
+Run in a container where the reference sources exist (oracle/Makefile builds
+oracle/_ref/PAWSIM.exe from them):  python tests/golden/make_golden.py
+
+For each small seeded set-up this writes one ``<case>.npz`` holding the input files
+themselves (parameter text and raw data files, so the fixture does not depend on the
+generator), and what the reference printed and wrote: the init_* tendency dumps of
+``writeInitDiagnostics 1`` (model_code/diagnostics.c:914-972), U/V/H/P after each step
+(diagnostics.c:874-908) and the ``PAWSIM pressure solve`` lines of ``pressureTiming 1``
+(model_code/pawsim.c:100-108).
+"""
+import os
+import re
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from pawsim_b200 import inputs  # noqa: E402
+import oracle  # noqa: E402
+
+NSTEPS = 3
+CASES = {
+    "gyre_sor": (inputs.gyre, dict(N=16, dt=900.0, solver=0, tol=1e-10)),
+    "gyre_mg": (inputs.gyre, dict(N=16, dt=900.0, solver=1, tol=1e-10)),
+    "gyre_hk83_a4": (inputs.gyre, dict(N=20, Ny=12, dt=600.0, solver=0, A2=0.0, A4=1e9,
+                                       extra=dict(momentumScheme=1, thicknessScheme=1))),
+    "channel": (inputs.channel, dict(Nx=32, Ny=16, dt=150.0, solver=1)),
+    "jets": (inputs.jets, dict(N=16, dt=100.0, solver=1)),
+    "full": (inputs.full_physics, dict(N=16, dt=50.0, solver=1, Ly=320e3, bathy_len=20e3,
+                                       sponge=40e3)),
+}
+LINE = re.compile(r"iters=(\d+) walltime=\S+ s residual_max=(\S+) residual_rms=(\S+) "
+                  r"div_max=(\S+) div_rms=(\S+)")
+
+
+def make(name, fn, kw, outdir):
+    with tempfile.TemporaryDirectory() as d:
+        kw = dict(kw)
+        extra = dict(kw.pop("extra", {}) or {})
+        extra.update(writeInitDiagnostics=1, pressureTiming=1)
+        dt = kw["dt"]
+        p = fn(os.path.join(d, "in"), Nt=NSTEPS, savefrequency=dt, extra=extra, **kw)
+        cfg = inputs.read_config(p)
+        out = os.path.join(d, "out")
+        os.makedirs(out)
+        r = subprocess.run([oracle.reference_exe(), p, out], capture_output=True, text=True, check=True)
+        stats = np.array([[float(x) for x in m.groups()] for m in LINE.finditer(r.stdout)])
+        L, Nx, Ny = cfg.Nlay, cfg.Nx, cfg.Ny
+        rec = {"stats": stats, "param_text": np.array(open(p).read())}
+        for f in sorted(os.listdir(os.path.dirname(p))):
+            if f.endswith(".dat") and f != "params.dat":
+                rec["in_" + f] = np.fromfile(os.path.join(os.path.dirname(p), f), dtype="<f8")
+        for k in range(L):
+            for tag in ("dudt", "dvdt", "dhdt"):
+                rec[f"init_{tag}{k}"] = inputs.read_data(os.path.join(out, f"init_{tag}{k}_n=0.dat"), (Ny, Nx))
+            for n in range(1, NSTEPS + 1):
+                for v in ("U", "V", "H"):
+                    rec[f"{v}{k}_{n}"] = inputs.read_data(os.path.join(out, f"{v}{k}_n={n}.dat"), (Ny, Nx))
+        for n in range(1, NSTEPS + 1):
+            rec[f"P_{n}"] = inputs.read_data(os.path.join(out, f"P_n={n}.dat"), (Ny, Nx))
+        np.savez_compressed(os.path.join(outdir, name + ".npz"), **rec)
+
+
+if __name__ == "__main__":
+    oracle.build(ref=True)
+    for name, (fn, kw) in CASES.items():
+        make(name, fn, kw, HERE)
+        print("wrote", name)
