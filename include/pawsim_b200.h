@@ -127,6 +127,24 @@ PAWSIM_API double pawsim_gpu_time (const pawsim_gpu * m);
 PAWSIM_API long long pawsim_gpu_launch_count (const pawsim_gpu * m);
 PAWSIM_API const char * pawsim_gpu_last_error (void);
 
+/* No counterpart in the reference. For callers that cannot allocate device memory (code
+ * running under an allocator or memory pool it does not own, hosts that forbid device
+ * allocation after start-up): builds the rigid-lid right-hand side, sum_k div(h_k u_k)/dt
+ * with its mean removed, from device arrays the caller holds (u, v, h: Nlay planes of Ny
+ * rows x pitch doubles, thickness already corrected to the column constraint) into the
+ * caller's device array rhs (Ny rows x pitch), on `stream` (a cudaStream_t, may be NULL).
+ * It allocates nothing: the partial sums of the mean use a static device array of 4096
+ * doubles, so grids are limited to Ny <= 32760 rows (any Nx); larger grids, Nx or Ny
+ * below 4 and thickness schemes other than AL81/HK83 are rejected with an error code.
+ * serial_sum: 1 sums in the reference's serial order, 0 in a fixed tree, -1 picks the
+ * serial order for grids of at most 65536 cells. The first call on a device looks up the
+ * array's device address, so make it before any stream capture. All calls share the
+ * array: calls that overlap on the GPU (other streams, other threads) race and must be
+ * serialised by the caller. */
+PAWSIM_API int pawsim_pressure_rhs_noalloc (const double * u, const double * v, const double * h,
+                                            int Nx, int Ny, int Nlay, int pitch, double dx, double dy,
+                                            double dt, int wall_ew, int wall_ns, int thick_scheme,
+                                            int serial_sum, double * rhs, void * stream);
 
 #ifdef __cplusplus
 }
