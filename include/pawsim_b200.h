@@ -126,6 +126,10 @@ PAWSIM_API double pawsim_gpu_time (const pawsim_gpu * m);
 /* kernels this library launched since creation (the launch counter) */
 PAWSIM_API long long pawsim_gpu_launch_count (const pawsim_gpu * m);
 PAWSIM_API const char * pawsim_gpu_last_error (void);
+/* Self-check of the library's correctly rounded division by a known divisor (used by the
+ * stencils for 1/dx, 1/dy, 1/24 and per-cell thickness) against the GPU's IEEE division on
+ * n host values x / d; *bad receives the number of results that differ in any bit. */
+PAWSIM_API int pawsim_gpu_check_division (const double * x, size_t n, double d, long long * bad);
 
 /* No counterpart in the reference. For callers that cannot allocate device memory (code
  * running under an allocator or memory pool it does not own, hosts that forbid device

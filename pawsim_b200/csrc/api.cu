@@ -45,6 +45,15 @@ __global__ void thickness_fix_kernel(double* h, const double* Hc, int Nx, int Ny
   for (int k = 0; k < L; ++k) h[k * ls + c] *= (1 - err / tot);
 }
 
+// div_rn against the IEEE division, bit for bit (signed zeros and NaN payloads compared as bits)
+__global__ void div_check_kernel(const double* x, size_t n, double d, double r, unsigned long long* bad) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double a = div_rn(x[i], d, r), b = x[i] / d;
+  bool same = __double_as_longlong(a) == __double_as_longlong(b) || (a != a && b != b);
+  if (!same) atomicAdd(bad, 1ull);
+}
+
 __global__ void hc_kernel(const double* hhs, const double* hhb, double* Hc, int Nx, int Ny, int pitch) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -101,6 +110,8 @@ struct Model {
     g.Nx = Nx; g.Ny = Ny; g.pitch = pitch; g.L = L; g.lstride = lstride;
     g.wall_ew = c.wall_ew; g.wall_ns = c.wall_ns; g.dx = dx; g.dy = dy; g.dt = c.dt;
     g.thick_scheme = c.thick_scheme;
+    g.rdx = 1.0 / dx; g.rdy = 1.0 / dy;
+    g.rdxdt = 1.0 / (dx * c.dt); g.rdydt = 1.0 / (dy * c.dt);
     return g;
   }
 };
@@ -346,6 +357,7 @@ static TendParams base_params(Model* m) {
   p.Nx = m->Nx; p.Ny = m->Ny; p.L = m->L; p.pitch = m->pitch; p.qpitch = m->qpitch; p.lstride = m->lstride;
   p.wall_ew = c.wall_ew; p.wall_ns = c.wall_ns; p.use_rl = c.use_rl;
   p.dx = m->dx; p.dy = m->dy;
+  p.rdx = 1.0 / m->dx; p.rdy = 1.0 / m->dy; p.r24 = 1.0 / 24.0;
   p.u = m->u[m->cur]; p.v = m->v[m->cur]; p.h = m->h[m->cur];
   p.hhb = m->hhb; p.hhs = m->hhs; p.Hc = m->Hc; p.omz = m->omz;
   for (int k = 0; k < m->L; ++k) { p.gg[k] = m->gg[k]; p.geff[k] = m->geff[k]; }
@@ -627,5 +639,24 @@ long long pawsim_gpu_launch_count(const pawsim_gpu* h) {
 }
 
 const char* pawsim_gpu_last_error(void) { return g_err; }
+
+int pawsim_gpu_check_division(const double* x_host, size_t n, double d, long long* bad) {
+  if (!x_host || !bad || n == 0) return fail(PAWSIM_GPU_EBADCONFIG, "null argument");
+  double* x = nullptr;
+  unsigned long long* cnt = nullptr;
+  PAWSIM_CUDA_OK(cudaMalloc(&x, n * sizeof(double)));
+  PAWSIM_CUDA_OK(cudaMalloc(&cnt, sizeof(unsigned long long)));
+  PAWSIM_CUDA_OK(cudaMemcpy(x, x_host, n * sizeof(double), cudaMemcpyHostToDevice));
+  PAWSIM_CUDA_OK(cudaMemset(cnt, 0, sizeof(unsigned long long)));
+  div_check_kernel<<<(unsigned)((n + 255) / 256), 256>>>(x, n, d, 1.0 / d, cnt);
+  ++g_launches;
+  unsigned long long h = 0;
+  cudaError_t e = cudaMemcpy(&h, cnt, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaFree(x);
+  cudaFree(cnt);
+  if (e != cudaSuccess) return set_cuda_error(e, "check_division", __FILE__, __LINE__);
+  *bad = (long long)h;
+  return 0;
+}
 
 }  // extern "C"

@@ -25,9 +25,16 @@ struct AxisMap {
   bool zero;    // value is a signed zero (sgn carries the sign)
 };
 
+// i mod n for the few-cells-out-of-range indices of stencils; no integer division unless
+// the index is more than one period away
 __host__ __device__ inline int wrap_index(int i, int n) {
-  int r = i % n;
-  return r < 0 ? r + n : r;
+  if (i < 0) i += n;
+  if (i >= n) i -= n;
+  if (i < 0 || i >= n) {
+    i %= n;
+    if (i < 0) i += n;
+  }
+  return i;
 }
 
 // Map a raw coordinate i (any integer within a few cells of [0, N)) to storage.
@@ -71,6 +78,22 @@ __host__ __device__ inline double load_mapped(const double* __restrict__ f, int 
 }
 
 inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+// x / d rounded to nearest, given r = 1/d rounded to nearest. Markstein's theorem: when q
+// is within one ulp of x/d and r is the correctly rounded reciprocal, the remainder
+// x - q*d is exact and q + (x - q*d)*r rounds to x/d. The first correction makes q = x*r
+// faithful, the second rounds it. Zeros keep their sign; tiny, huge and non-finite
+// operands take the IEEE division. Checked against the hardware division bit for bit by
+// pawsim_gpu_check_division (tests/test_gpu_division.py).
+__device__ __forceinline__ double div_rn(double x, double d, double r) {
+  double q = x * r;
+  double ax = fabs(x);
+  if (!(ax > 0x1p-900 && ax < 0x1p900)) return (x == 0) ? q : x / d;
+  double e = fma(-q, d, x);
+  q = fma(e, r, q);
+  e = fma(-q, d, x);
+  return fma(e, r, q);
+}
 
 }  // namespace pawsim
 

@@ -1,5 +1,15 @@
 // mg.cu -- GPU multigrid for the rigid-lid pressure equation (see mg.cuh).
+//
+// Per level above the coarse block, one fused "down" kernel (red-black pre-smoothing,
+// residual and 2x2 restriction on a shared-memory tile with a 2*nu+1 halo) and one fused
+// "up" kernel (bilinear prolongation of the coarse correction, correction and red-black
+// post-smoothing on a tile with a 2*nu halo). Cells of the halo are smoothed redundantly by
+// neighbouring tiles from the same inputs, so every tile sees the values a global sweep
+// would produce. Levels of at most 1024 cells run inside one CTA in shared memory. The whole
+// V-cycle plus the stopping test is a CUDA graph whose body sits in a device-side `while`
+// conditional node: no host round trip per V-cycle.
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <vector>
@@ -33,6 +43,11 @@ LV<float> view<float>(const Multigrid::Level& l) {
 
 #define IX(l, i, j) ((size_t)(j) * (l).pitch + (i))
 
+__host__ __device__ inline int wrapi(int i, int n) { return wrap_index(i, n); }
+
+// ---------------------------------------------------------------- generic kernels
+// (levels whose transfer is not an exact 2:1 coarsening, and the fine-level checks)
+
 // operator sum around a cell with the multigrid's periodic indexing (multigrid.c:604-623)
 template <typename T>
 __device__ inline T neighbour_sum(const LV<T>& l, const T* e, int i, int j) {
@@ -52,16 +67,6 @@ __global__ void smooth_kernel(LV<T> l, int color, T omega) {
   l.e[c] = omega * l.rOsum[c] * (s - l.rhs[c]) + (T(1) - omega) * l.e[c];
 }
 
-// first red sweep from a zero initial guess: neighbours are zero
-template <typename T>
-__global__ void smooth_zero_kernel(LV<T> l, T omega) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= l.Nx || j >= l.Ny) return;
-  size_t c = IX(l, i, j);
-  l.e[c] = (((i + j) & 1) == 0) ? omega * l.rOsum[c] * (-l.rhs[c]) : T(0);
-}
-
 template <typename T>
 __global__ void residual_kernel(LV<T> l) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -71,36 +76,12 @@ __global__ void residual_kernel(LV<T> l) {
   l.res[c] = neighbour_sum(l, l.e, i, j) - l.Osum[c] * l.e[c] - l.rhs[c];
 }
 
-// residual of the fine level restricted by 2x2 means straight into the coarse rhs
-// (multigrid.c:599-668); the coarse correction starts from zero
-template <typename T>
-__global__ void residual_restrict_kernel(LV<T> f, LV<T> c) {
-  int ic = blockIdx.x * blockDim.x + threadIdx.x;
-  int jc = blockIdx.y * blockDim.y + threadIdx.y;
-  if (ic >= c.Nx || jc >= c.Ny) return;
-  T r[4];
-  int q = 0;
-#pragma unroll
-  for (int dj = 0; dj < 2; ++dj)
-#pragma unroll
-    for (int di = 0; di < 2; ++di) {
-      int i = 2 * ic + di, j = 2 * jc + dj;
-      size_t x = IX(f, i, j);
-      r[q++] = neighbour_sum(f, f.e, i, j) - f.Osum[x] * f.e[x] - f.rhs[x];
-    }
-  // order of restrict_power2_MG: (2i,2j) + (2i+1,2j) + (2i,2j+1) + (2i+1,2j+1)
-  c.rhs[IX(c, ic, jc)] = T(0.25) * (r[0] + r[1] + r[2] + r[3]);
-  c.e[IX(c, ic, jc)] = T(0);
-}
-
 // area-weighted restriction for uneven pairs (multigrid.c:681-740)
 template <typename T>
-__global__ void restrict_general_kernel(LV<T> f, const T* src, LV<T> c, T* dst) {
-  int ic = blockIdx.x * blockDim.x + threadIdx.x;
-  int jc = blockIdx.y * blockDim.y + threadIdx.y;
-  if (ic >= c.Nx || jc >= c.Ny) return;
-  double x0 = (double)ic * f.Nx / c.Nx, x1 = (double)(ic + 1) * f.Nx / c.Nx;
-  double y0 = (double)jc * f.Ny / c.Ny, y1 = (double)(jc + 1) * f.Ny / c.Ny;
+__device__ inline T restrict_general_at(int fNx, int fNy, int cNx, int cNy, int ic, int jc,
+                                        const T* src, int spitch) {
+  double x0 = (double)ic * fNx / cNx, x1 = (double)(ic + 1) * fNx / cNx;
+  double y0 = (double)jc * fNy / cNy, y1 = (double)(jc + 1) * fNy / cNy;
   double acc = 0, wsum = 0;
   for (int fi = (int)floor(x0); fi < (int)ceil(x1); ++fi) {
     double wx = fmin(x1, (double)(fi + 1)) - fmax(x0, (double)fi);
@@ -109,83 +90,392 @@ __global__ void restrict_general_kernel(LV<T> f, const T* src, LV<T> c, T* dst) 
       double wy = fmin(y1, (double)(fj + 1)) - fmax(y0, (double)fj);
       if (wy <= 0) continue;
       double w = wx * wy;
-      acc += w * (double)src[IX(f, fi, fj)];
+      acc += w * (double)src[(size_t)fj * spitch + fi];
       wsum += w;
     }
   }
-  dst[IX(c, ic, jc)] = (T)(wsum > 0 ? acc / wsum : acc);
+  return (T)(wsum > 0 ? acc / wsum : acc);
+}
+
+template <typename T>
+__global__ void restrict_general_kernel(LV<T> f, LV<T> c) {
+  int ic = blockIdx.x * blockDim.x + threadIdx.x;
+  int jc = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ic >= c.Nx || jc >= c.Ny) return;
+  c.rhs[IX(c, ic, jc)] = restrict_general_at<T>(f.Nx, f.Ny, c.Nx, c.Ny, ic, jc, f.res, f.pitch);
   c.e[IX(c, ic, jc)] = T(0);
 }
 
-// bilinear prolongation of the coarse correction, subtracted from the fine level
-// (multigrid.c:376-442, 827-932, 986-1004)
+// bilinear prolongation weights and coarse indices of one fine cell (multigrid.c:376-442,
+// 827-932); returns the interpolated coarse correction
+template <typename T, typename Get>
+__device__ inline T prolong_at(int i, int j, int fNx, int fNy, int cNx, int cNy, bool power2, bool wew,
+                               bool wns, Get ec) {
+  if (power2) {
+    // coarse points east/west and north/south of fine point (i, j), i, j >= 0
+    int hx = fNx / 2, hy = fNy / 2;
+    int ip = (i + 1) >> 1, jp = (j + 1) >> 1;
+    if (ip >= hx) ip -= hx;
+    if (jp >= hy) jp -= hy;
+    int im = ip == 0 ? hx - 1 : ip - 1, jm = jp == 0 ? hy - 1 : jp - 1;
+    const bool io = (i & 1) != 0, jo = (j & 1) != 0;
+    T ai = io ? T(0.75) : T(0.25), bi = io ? T(0.25) : T(0.75);
+    T aj = jo ? T(0.75) : T(0.25), bj = jo ? T(0.25) : T(0.75);
+    T wmm = ai * aj, wmp = ai * bj, wpm = bi * aj, wpp = bi * bj;
+    if (wns) {
+      if (j == 0) { wmm = 0; wpm = 0; wmp = ai; wpp = bi; }
+      if (j == fNy - 1) { wmp = 0; wpp = 0; wmm = ai; wpm = bi; }
+    }
+    if (wew) {
+      if (i == 0) { wmm = 0; wmp = 0; wpm = aj; wpp = bj; }
+      if (i == fNx - 1) { wpm = 0; wpp = 0; wmm = aj; wmp = bj; }
+    }
+    if (wns && wew) {
+      if (i == 0 && j == 0) { wmm = 0; wmp = 0; wpm = 0; wpp = 1; }
+      if (i == 0 && j == fNy - 1) { wmm = 0; wmp = 0; wpm = 1; wpp = 0; }
+      if (i == fNx - 1 && j == 0) { wmm = 0; wmp = 1; wpm = 0; wpp = 0; }
+      if (i == fNx - 1 && j == fNy - 1) { wmm = 1; wmp = 0; wpm = 0; wpp = 0; }
+    }
+    return wmm * ec(im, jm) + wpm * ec(ip, jm) + wmp * ec(im, jp) + wpp * ec(ip, jp);
+  }
+  double x = ((double)i + 0.5) * cNx / fNx - 0.5, y = ((double)j + 0.5) * cNy / fNy - 0.5, tx, ty;
+  int imr, jmr;
+  if (wew && x <= 0) { imr = 0; tx = 0; }
+  else if (wew && x >= cNx - 1) { imr = cNx - 1; tx = 0; }
+  else { imr = (int)floor(x); tx = x - imr; }
+  if (wns && y <= 0) { jmr = 0; ty = 0; }
+  else if (wns && y >= cNy - 1) { jmr = cNy - 1; ty = 0; }
+  else { jmr = (int)floor(y); ty = y - jmr; }
+  auto idx = [](int v, int n, bool wall) {
+    if (n <= 1) return 0;
+    if (wall) return v < 0 ? 0 : (v >= n ? n - 1 : v);
+    return ((v % n) + n) % n;
+  };
+  int im = idx(imr, cNx, wew), ip = idx(imr + 1, cNx, wew);
+  int jm = idx(jmr, cNy, wns), jp = idx(jmr + 1, cNy, wns);
+  return (T)((1 - tx) * (1 - ty) * (double)ec(im, jm) + tx * (1 - ty) * (double)ec(ip, jm)
+             + (1 - tx) * ty * (double)ec(im, jp) + tx * ty * (double)ec(ip, jp));
+}
+
 template <typename T>
 __global__ void prolong_correct_kernel(LV<T> f, LV<T> c, int power2, int wew, int wns) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= f.Nx || j >= f.Ny) return;
-  T val;
-  if (power2) {
-    int hx = f.Nx / 2, hy = f.Ny / 2;
-    int ip = (((i + 1) - (i + 1) % 2) / 2 + hx) % hx, im = (ip - 1 + hx) % hx;
-    int jp = (((j + 1) - (j + 1) % 2) / 2 + hy) % hy, jm = (jp - 1 + hy) % hy;
-    T ai = (i % 2 == 1) ? T(0.75) : T(0.25), bi = (i % 2 == 1) ? T(0.25) : T(0.75);
-    T aj = (j % 2 == 1) ? T(0.75) : T(0.25), bj = (j % 2 == 1) ? T(0.25) : T(0.75);
-    T wmm = ai * aj, wmp = ai * bj, wpm = bi * aj, wpp = bi * bj;
-    if (wns) {
-      if (j == 0) { wmm = 0; wpm = 0; wmp = ai; wpp = bi; }
-      if (j == f.Ny - 1) { wmp = 0; wpp = 0; wmm = ai; wpm = bi; }
-    }
-    if (wew) {
-      if (i == 0) { wmm = 0; wmp = 0; wpm = aj; wpp = bj; }
-      if (i == f.Nx - 1) { wpm = 0; wpp = 0; wmm = aj; wmp = bj; }
-    }
-    if (wns && wew) {
-      if (i == 0 && j == 0) { wmm = 0; wmp = 0; wpm = 0; wpp = 1; }
-      if (i == 0 && j == f.Ny - 1) { wmm = 0; wmp = 0; wpm = 1; wpp = 0; }
-      if (i == f.Nx - 1 && j == 0) { wmm = 0; wmp = 1; wpm = 0; wpp = 0; }
-      if (i == f.Nx - 1 && j == f.Ny - 1) { wmm = 1; wmp = 0; wpm = 0; wpp = 0; }
-    }
-    val = wmm * c.e[IX(c, im, jm)] + wpm * c.e[IX(c, ip, jm)] + wmp * c.e[IX(c, im, jp)] + wpp * c.e[IX(c, ip, jp)];
-  } else {
-    double x = ((double)i + 0.5) * c.Nx / f.Nx - 0.5, y = ((double)j + 0.5) * c.Ny / f.Ny - 0.5, tx, ty;
-    int imr, jmr;
-    if (wew && x <= 0) { imr = 0; tx = 0; }
-    else if (wew && x >= c.Nx - 1) { imr = c.Nx - 1; tx = 0; }
-    else { imr = (int)floor(x); tx = x - imr; }
-    if (wns && y <= 0) { jmr = 0; ty = 0; }
-    else if (wns && y >= c.Ny - 1) { jmr = c.Ny - 1; ty = 0; }
-    else { jmr = (int)floor(y); ty = y - jmr; }
-    auto idx = [](int v, int n, int wall) {
-      if (n <= 1) return 0;
-      if (wall) return v < 0 ? 0 : (v >= n ? n - 1 : v);
-      return ((v % n) + n) % n;
-    };
-    int im = idx(imr, c.Nx, wew), ip = idx(imr + 1, c.Nx, wew);
-    int jm = idx(jmr, c.Ny, wns), jp = idx(jmr + 1, c.Ny, wns);
-    val = (T)((1 - tx) * (1 - ty) * (double)c.e[IX(c, im, jm)] + tx * (1 - ty) * (double)c.e[IX(c, ip, jm)]
-              + (1 - tx) * ty * (double)c.e[IX(c, im, jp)] + tx * ty * (double)c.e[IX(c, ip, jp)]);
-  }
-  f.e[IX(f, i, j)] -= val;
+  auto ec = [&](int a, int b) { return c.e[IX(c, a, b)]; };
+  f.e[IX(f, i, j)] -= prolong_at<T>(i, j, f.Nx, f.Ny, c.Nx, c.Ny, power2, wew, wns, ec);
 }
+
+// ---------------------------------------------------------------- fused tile kernels
+
+constexpr int BX = 32, BY = 8, BT = BX * BY;
+const dim3 TB(BX, BY);
+
+// smem tile of a level: raw coordinates [X0-H, X0+BX+H) x [Y0-H, Y0+BY+H), plus one more
+// column of Ow and one more row of Os (the east/north faces)
+template <int H>
+struct TileGeom {
+  static constexpr int W = BX + 2 * H, Hh = BY + 2 * H, N = W * Hh;
+  static constexpr int WO = W + 1, NO = WO * (Hh + 1);   // operator arrays
+};
+
+template <typename T, int H>
+__device__ inline void load_tile(const LV<T>& l, int X0, int Y0, T* e, T* rhs, T* Ow, T* Os, T* rO,
+                                 bool zero_e) {
+  using G = TileGeom<H>;
+  // tiles whose halo (and the extra east/north face) lies inside the level load directly
+  const bool inner = X0 - H >= 0 && X0 + BX + H + 1 <= l.Nx && Y0 - H >= 0 && Y0 + BY + H + 1 <= l.Ny;
+  for (int ly = threadIdx.y; ly < G::Hh + 1; ly += BY)
+    for (int lx = threadIdx.x; lx < G::WO; lx += BX) {
+      int gi = X0 - H + lx, gj = Y0 - H + ly;
+      if (!inner) {
+        gi = wrapi(gi, l.Nx);
+        gj = wrapi(gj, l.Ny);
+      }
+      size_t g = IX(l, gi, gj);
+      int q = ly * G::WO + lx;
+      Ow[q] = l.Ow[g];
+      Os[q] = l.Os[g];
+      if (lx < G::W && ly < G::Hh) {
+        int p = ly * G::W + lx;
+        e[p] = zero_e ? T(0) : l.e[g];
+        rhs[p] = l.rhs[g];
+        rO[p] = l.rOsum[g];
+      }
+    }
+}
+
+// one red-black half sweep over tile cells within `reach` of the owned tile
+template <typename T, int H>
+__device__ inline void tile_half_sweep(int X0, int Y0, int color, int reach, T omega, T* e, const T* rhs,
+                                       const T* Ow, const T* Os, const T* rO) {
+  using G = TileGeom<H>;
+  const int par = (X0 + Y0 + color) & 1;   // (X0-H+lx + Y0-H+ly) & 1 == color, H*2 even
+  for (int ly = H - reach + threadIdx.y; ly < H + BY + reach; ly += BY)
+    for (int lx = H - reach + threadIdx.x; lx < H + BX + reach; lx += BX) {
+      if (((lx + ly) & 1) != par) continue;
+      int q = ly * G::W + lx, o = ly * G::WO + lx;
+      T s = Os[o + G::WO] * e[q + G::W] + Os[o] * e[q - G::W] + Ow[o + 1] * e[q + 1] + Ow[o] * e[q - 1];
+      e[q] = omega * rO[q] * (s - rhs[q]) + (T(1) - omega) * e[q];
+    }
+}
+
+// pre-smoothing, residual and 2x2 restriction into the coarse rhs (the coarse correction
+// starts from zero: the coarse kernels treat it as zero instead of reading it)
+template <typename T, int NU>
+__global__ void __launch_bounds__(BT) down_kernel(LV<T> f, LV<T> c, T omega, int zero_e) {
+  constexpr int H = 2 * NU + 1;
+  using G = TileGeom<H>;
+  extern __shared__ unsigned char sm_raw[];
+  T* e = reinterpret_cast<T*>(sm_raw);
+  T* rhs = e + G::N;
+  T* rO = rhs + G::N;
+  T* Ow = rO + G::N;
+  T* Os = Ow + G::NO;
+  const int X0 = blockIdx.x * BX, Y0 = blockIdx.y * BY;
+  load_tile<T, H>(f, X0, Y0, e, rhs, Ow, Os, rO, zero_e);
+  __syncthreads();
+  for (int s = 0; s < NU; ++s) {
+    tile_half_sweep<T, H>(X0, Y0, 0, H - (2 * s + 1), omega, e, rhs, Ow, Os, rO);
+    __syncthreads();
+    tile_half_sweep<T, H>(X0, Y0, 1, H - (2 * s + 2), omega, e, rhs, Ow, Os, rO);
+    __syncthreads();
+  }
+  // write the smoothed owned cells and form their residuals (multigrid.c:604-623)
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int lx = tx + H, ly = ty + H;
+  const int q = ly * G::W + lx, o = ly * G::WO + lx;
+  const int gi = X0 + tx, gj = Y0 + ty;
+  T r = 0;
+  if (gi < f.Nx && gj < f.Ny) {
+    T ec = e[q];
+    f.e[IX(f, gi, gj)] = ec;
+    T osum = Ow[o] + Ow[o + 1] + Os[o] + Os[o + G::WO];
+    T s = Os[o + G::WO] * e[q + G::W] + Os[o] * e[q - G::W] + Ow[o + 1] * e[q + 1] + Ow[o] * e[q - 1];
+    r = s - osum * ec - rhs[q];
+  }
+  __syncthreads();
+  T* res = rO;   // rOsum is no longer needed
+  res[ty * BX + tx] = r;
+  __syncthreads();
+  // restriction, order of restrict_power2_MG: (2i,2j) + (2i+1,2j) + (2i,2j+1) + (2i+1,2j+1)
+  const int t = ty * BX + tx;
+  if (t < (BX / 2) * (BY / 2)) {
+    int cx = t % (BX / 2), cy = t / (BX / 2);
+    int ic = X0 / 2 + cx, jc = Y0 / 2 + cy;
+    if (ic < c.Nx && jc < c.Ny) {
+      const T* rr = res + (2 * cy) * BX + 2 * cx;
+      c.rhs[IX(c, ic, jc)] = T(0.25) * (rr[0] + rr[1] + rr[BX] + rr[BX + 1]);
+    }
+  }
+}
+
+// prolongation + correction over the tile and halo, then post-smoothing
+template <typename T, int NU>
+__global__ void __launch_bounds__(BT) up_kernel(LV<T> f, LV<T> c, T omega, int wew, int wns, int zero_e) {
+  constexpr int H = 2 * NU;
+  using G = TileGeom<H>;
+  extern __shared__ unsigned char sm_raw[];
+  T* e = reinterpret_cast<T*>(sm_raw);
+  T* rhs = e + G::N;
+  T* rO = rhs + G::N;
+  T* Ow = rO + G::N;
+  T* Os = Ow + G::NO;
+  const int X0 = blockIdx.x * BX, Y0 = blockIdx.y * BY;
+  load_tile<T, H>(f, X0, Y0, e, rhs, Ow, Os, rO, zero_e);
+  __syncthreads();
+  auto ec = [&](int a, int b) { return c.e[IX(c, a, b)]; };
+  for (int ly = threadIdx.y; ly < G::Hh; ly += BY)
+    for (int lx = threadIdx.x; lx < G::W; lx += BX) {
+      int gi = wrapi(X0 - H + lx, f.Nx), gj = wrapi(Y0 - H + ly, f.Ny);
+      e[ly * G::W + lx] -= prolong_at<T>(gi, gj, f.Nx, f.Ny, c.Nx, c.Ny, true, wew, wns, ec);
+    }
+  __syncthreads();
+  for (int s = 0; s < NU; ++s) {
+    tile_half_sweep<T, H>(X0, Y0, 0, H - (2 * s + 1), omega, e, rhs, Ow, Os, rO);
+    __syncthreads();
+    tile_half_sweep<T, H>(X0, Y0, 1, H - (2 * s + 2), omega, e, rhs, Ow, Os, rO);
+    __syncthreads();
+  }
+  const int gi = X0 + threadIdx.x, gj = Y0 + threadIdx.y;
+  if (gi < f.Nx && gj < f.Ny) f.e[IX(f, gi, gj)] = e[(threadIdx.y + H) * G::W + threadIdx.x + H];
+}
+
+// ---------------------------------------------------------------- coarse levels in one CTA
+
+constexpr int CMAX_LEVELS = 12;
+constexpr int CT = 1024;
+
+struct CoarseDesc {
+  int n;                        // levels 0..n-1, index n-1 is the top of the block
+  int Nx[CMAX_LEVELS], Ny[CMAX_LEVELS], pitch[CMAX_LEVELS], power2[CMAX_LEVELS];
+  int off[CMAX_LEVELS];         // offset of each level inside every smem array
+  int total;                    // cells of all levels
+  const void *Ow[CMAX_LEVELS], *Os[CMAX_LEVELS], *rO[CMAX_LEVELS];
+  const void* top_rhs;          // rhs of the top level (global, pitched)
+  void* top_e;                  // output correction of the top level
+  int top_from_e;               // start the top level from top_e instead of zero
+  int wew, wns, pre, post;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(CT) coarse_kernel(const __grid_constant__ CoarseDesc d, T omega) {
+  extern __shared__ unsigned char sm_raw[];
+  T* E = reinterpret_cast<T*>(sm_raw);
+  T* R = E + d.total;
+  T* W = R + d.total;
+  T* S = W + d.total;
+  T* Q = S + d.total;
+  T* RES = Q + d.total;
+  const int tid = threadIdx.x;
+  for (int l = 0; l < d.n; ++l) {
+    const T* ow = (const T*)d.Ow[l];
+    const T* os = (const T*)d.Os[l];
+    const T* ro = (const T*)d.rO[l];
+    int nx = d.Nx[l], ny = d.Ny[l], cnt = nx * ny;
+    for (int q = tid; q < cnt; q += CT) {
+      int i = q % nx, j = q / nx;
+      size_t g = (size_t)j * d.pitch[l] + i;
+      W[d.off[l] + q] = ow[g];
+      S[d.off[l] + q] = os[g];
+      Q[d.off[l] + q] = ro[g];
+      E[d.off[l] + q] = (l == d.n - 1 && d.top_from_e) ? ((const T*)d.top_e)[g] : T(0);
+      if (l == d.n - 1) R[d.off[l] + q] = ((const T*)d.top_rhs)[g];
+    }
+  }
+  __syncthreads();
+  auto nsum = [&](int l, int i, int j) {
+    int nx = d.Nx[l], ny = d.Ny[l], b = d.off[l];
+    int ip1 = i + 1 == nx ? 0 : i + 1, im1 = i == 0 ? nx - 1 : i - 1;
+    int jp1 = j + 1 == ny ? 0 : j + 1, jm1 = j == 0 ? ny - 1 : j - 1;
+    return S[b + jp1 * nx + i] * E[b + jp1 * nx + i] + S[b + j * nx + i] * E[b + jm1 * nx + i]
+         + W[b + j * nx + ip1] * E[b + j * nx + ip1] + W[b + j * nx + i] * E[b + j * nx + im1];
+  };
+  auto smooth = [&](int l, int sweeps) {
+    int nx = d.Nx[l], b = d.off[l], cnt = nx * d.Ny[l];
+    for (int s = 0; s < sweeps; ++s)
+      for (int color = 0; color < 2; ++color) {
+        for (int q = tid; q < cnt; q += CT) {
+          int i = q % nx, j = q / nx;
+          if (((i + j) & 1) != color) continue;
+          T sm = nsum(l, i, j);
+          E[b + q] = omega * Q[b + q] * (sm - R[b + q]) + (T(1) - omega) * E[b + q];
+        }
+        __syncthreads();
+      }
+  };
+  // down
+  for (int l = d.n - 1; l >= 1; --l) {
+    smooth(l, d.pre);
+    int nx = d.Nx[l], ny = d.Ny[l], b = d.off[l], cnt = nx * ny;
+    for (int q = tid; q < cnt; q += CT) {
+      int i = q % nx, j = q / nx;
+      int ip1 = i + 1 == nx ? 0 : i + 1, jp1 = j + 1 == ny ? 0 : j + 1;
+      T osum = W[b + q] + W[b + j * nx + ip1] + S[b + q] + S[b + jp1 * nx + i];
+      RES[q] = nsum(l, i, j) - osum * E[b + q] - R[b + q];
+    }
+    __syncthreads();
+    int cnx = d.Nx[l - 1], cny = d.Ny[l - 1], cb = d.off[l - 1];
+    for (int q = tid; q < cnx * cny; q += CT) {
+      int ic = q % cnx, jc = q / cnx;
+      T v;
+      if (d.power2[l]) {
+        const T* rr = RES + (2 * jc) * nx + 2 * ic;
+        v = T(0.25) * (rr[0] + rr[1] + rr[nx] + rr[nx + 1]);
+      } else {
+        v = restrict_general_at<T>(nx, ny, cnx, cny, ic, jc, RES, nx);
+      }
+      R[cb + q] = v;
+      E[cb + q] = 0;
+    }
+    __syncthreads();
+  }
+  // coarsest: a single cell carries no information (multigrid.c:472-476)
+  if (d.Nx[0] * d.Ny[0] == 1) {
+    if (tid == 0) E[d.off[0]] = 0;
+    __syncthreads();
+  } else {
+    smooth(0, d.pre + d.post);
+  }
+  // up
+  for (int l = 1; l < d.n; ++l) {
+    int nx = d.Nx[l], ny = d.Ny[l], b = d.off[l];
+    int cnx = d.Nx[l - 1], cny = d.Ny[l - 1], cb = d.off[l - 1];
+    auto ec = [&](int a, int bb) { return E[cb + bb * cnx + a]; };
+    for (int q = tid; q < nx * ny; q += CT) {
+      int i = q % nx, j = q / nx;
+      E[b + q] -= prolong_at<T>(i, j, nx, ny, cnx, cny, d.power2[l] != 0, d.wew, d.wns, ec);
+    }
+    __syncthreads();
+    smooth(l, d.post);
+  }
+  int l = d.n - 1;
+  for (int q = tid; q < d.Nx[l] * d.Ny[l]; q += CT) {
+    int i = q % d.Nx[l], j = q / d.Nx[l];
+    ((T*)d.top_e)[(size_t)j * d.pitch[l] + i] = E[d.off[l] + q];
+  }
+}
+
+// ---------------------------------------------------------------- stopping test and loop control
+
+// max over the block (warp shuffles, then the warps' maxima), one atomic per block
+__device__ inline void block_max_to(double m, unsigned long long* bits) {
+  __shared__ double wm[32];
+  const int t = threadIdx.x + threadIdx.y * blockDim.x;
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((t & 31) == 0) wm[t >> 5] = m;
+  __syncthreads();
+  if (t == 0) {
+    const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+    double b = 0;
+    for (int w = 0; w < nw; ++w) b = fmax(b, wm[w]);
+    if (b > 0) atomicMax(bits, (unsigned long long)__double_as_longlong(b));
+  }
+}
+
+struct LoopState {
+  unsigned long long bits;   // max |pi - Jacobi(pi)| as an integer bit pattern
+  int iters;
+  int maxiters;
+  double tol;
+  double maxres;
+};
 
 // max |pi - Jacobi(pi)| on the fine level (multigrid.c:1123-1156); NaNs are ignored like fmax
 __global__ void max_residual_kernel(LV<double> l, unsigned long long* bits) {
   double m = 0;
-  int n = l.Nx * l.Ny;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-    int i = q % l.Nx, j = q / l.Nx;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i < l.Nx && j < l.Ny) {
     size_t c = IX(l, i, j);
     double r = l.e[c] - l.rOsum[c] * (neighbour_sum(l, l.e, i, j) - l.rhs[c]);
     m = fmax(m, fabs(r));
   }
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(bits, (unsigned long long)__double_as_longlong(m));
+  block_max_to(m, bits);
 }
 
-// FP64 defect step: pi -= e32 (when `correct`), then r = L(pi) - rhs stored as FP32 on the
-// fine FP32 level, plus the stopping measure of the updated pi
-__global__ void defect_kernel(LV<double> l, const float* __restrict__ e32, int p32, float* r32, float* ez32,
+__global__ void loop_reset_kernel(LoopState* st, int maxiters, double tol) {
+  st->bits = 0;
+  st->iters = 0;
+  st->maxiters = maxiters;
+  st->tol = tol;
+  st->maxres = tol + 1;
+}
+
+// the loop condition of iterate_MG (multigrid.c:1185-1201)
+__global__ void loop_finalize_kernel(LoopState* st, cudaGraphConditionalHandle h) {
+  double m = __longlong_as_double((long long)st->bits);
+  st->bits = 0;
+  st->iters += 1;
+  st->maxres = m;
+  unsigned cont = (m > st->tol) && (st->iters < st->maxiters);
+  cudaGraphSetConditional(h, cont);
+}
+
+// FP64 defect step of the mixed-precision solve: pi_new = pi - e32 (when `correct`), the
+// residual L(pi_new) - rhs stored as FP32 on the fine FP32 level, and the stopping measure
+// of pi_new. pi_new goes to `out` and is copied back by commit_kernel.
+__global__ void defect_kernel(LV<double> l, const float* __restrict__ e32, int p32, float* r32, double* out,
                               int correct, unsigned long long* bits) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -202,28 +492,19 @@ __global__ void defect_kernel(LV<double> l, const float* __restrict__ e32, int p
     double s = l.Os[IX(l, i, jp1)] * P(i, jp1) + l.Os[IX(l, i, j)] * P(i, jm1)
              + l.Ow[IX(l, ip1, j)] * P(ip1, j) + l.Ow[IX(l, i, j)] * P(im1, j);
     size_t c = IX(l, i, j);
-    double crit = pc - l.rOsum[c] * (s - l.rhs[c]);
-    m = fabs(crit);
+    m = fabs(pc - l.rOsum[c] * (s - l.rhs[c]));
     if (m != m) m = 0;
     r32[(size_t)j * p32 + i] = (float)(s - l.Osum[c] * pc - l.rhs[c]);
-    ez32[(size_t)j * p32 + i] = 0.f;
-    l.res[c] = pc;   // updated pi, copied back by commit_kernel
+    if (correct) out[c] = pc;
   }
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(bits, (unsigned long long)__double_as_longlong(m));
+  block_max_to(m, bits);
 }
 
-__global__ void commit_kernel(LV<double> l) {
+__global__ void commit_kernel(double* dst, const double* src, int Nx, int Ny, int pitch) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= l.Nx || j >= l.Ny) return;
-  l.e[IX(l, i, j)] = l.res[IX(l, i, j)];
-}
-
-__global__ void zero_kernel_d(double* a, int Nx, int Ny, int pitch) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i < Nx && j < Ny) a[(size_t)j * pitch + i] = 0;
+  if (i >= Nx || j >= Ny) return;
+  dst[(size_t)j * pitch + i] = src[(size_t)j * pitch + i];
 }
 
 inline dim3 g2(int Nx, int Ny) { return dim3((Nx + 31) / 32, (Ny + 7) / 8); }
@@ -267,7 +548,21 @@ void host_restrict(int fnx, int fny, const std::vector<double>& f, int cnx, int 
   }
 }
 
+template <typename T, int H>
+size_t tile_smem() {
+  using G = TileGeom<H>;
+  return (size_t)(3 * G::N + 2 * G::NO) * sizeof(T);
+}
+
 }  // namespace
+
+struct Multigrid::Graphs {
+  cudaGraph_t graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  cudaGraphConditionalHandle handle[2];
+  int pre = -1, post = -1;
+  double omega = -1;
+};
 
 Multigrid::Multigrid(int Nx, int Ny, double Lx, double Ly, bool wew, bool wns, const double* Hc_host,
                      const MGOptions& opt, cudaStream_t s)
@@ -285,7 +580,6 @@ Multigrid::Multigrid(int Nx, int Ny, double Lx, double Ly, bool wew, bool wns, c
   }
   int n = (int)nxs.size();
   lv_.resize(n);
-  // Hc on every level, reference arithmetic; host arrays are i-major like the reference
   std::vector<std::vector<double>> Hc(n);
   Hc[n - 1].resize((size_t)Nx * Ny);
   for (int i = 0; i < Nx; ++i)
@@ -357,65 +651,153 @@ Multigrid::Multigrid(int Nx, int Ny, double Lx, double Ly, bool wew, bool wns, c
     L.e32 = dalloc<float>(np); L.rhs32 = dalloc<float>(np); L.res32 = dalloc<float>(np);
     good = good && L.e && L.rhs && L.res && L.e32 && L.rhs32 && L.res32;
   }
-  dmax_ = dalloc<double>(2);
-  dbits_ = dalloc<unsigned long long>(2);
-  ok_ = good && dmax_ && dbits_;
+  own_e_ = lv_.back().e;
+  own_rhs_ = lv_.back().rhs;
+  // the top of the coarse block: the largest level with at most 1024 cells among the
+  // CMAX_LEVELS coarsest (the block must fit one CTA's shared memory)
+  ctop_ = 0;
+  for (int m = 0; m < n && m < CMAX_LEVELS; ++m)
+    if ((long long)lv_[m].Nx * lv_[m].Ny <= 1024) ctop_ = m;
+  dstate_ = reinterpret_cast<void*>(dalloc<LoopState>(1));
+  good = good && dstate_;
+  cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking);
+  g_ = new Graphs();
+  ok_ = good;
+  cudaFuncSetAttribute(coarse_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(coarse_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
 Multigrid::~Multigrid() {
+  if (g_) {
+    for (int p = 0; p < 2; ++p) {
+      if (g_->exec[p]) cudaGraphExecDestroy(g_->exec[p]);
+      if (g_->graph[p]) cudaGraphDestroy(g_->graph[p]);
+    }
+    delete g_;
+  }
+  if (cap_) cudaStreamDestroy(cap_);
+  lv_.back().e = own_e_;
+  lv_.back().rhs = own_rhs_;
   for (auto& L : lv_) {
     cudaFree(L.Ow); cudaFree(L.Os); cudaFree(L.Osum); cudaFree(L.rOsum);
     cudaFree(L.Ow32); cudaFree(L.Os32); cudaFree(L.Osum32); cudaFree(L.rOsum32);
     cudaFree(L.e); cudaFree(L.rhs); cudaFree(L.res);
     cudaFree(L.e32); cudaFree(L.rhs32); cudaFree(L.res32);
   }
-  cudaFree(dmax_);
-  cudaFree(dbits_);
+  cudaFree(dstate_);
 }
 
 template <typename T>
-void Multigrid::smooth(int n, int sweeps) {
-  LV<T> l = view<T>(lv_[n]);
-  if (n == (int)lv_.size() - 1 && sizeof(T) == 8) {
-    l.e = reinterpret_cast<T*>(fine_pi_);
-    l.rhs = const_cast<T*>(reinterpret_cast<const T*>(fine_rhs_));
-  }
-  for (int s = 0; s < sweeps; ++s) {
-    smooth_kernel<T><<<g2(l.Nx, l.Ny), B2, 0, s_>>>(l, 0, (T)opt_.omega_rb);
-    smooth_kernel<T><<<g2(l.Nx, l.Ny), B2, 0, s_>>>(l, 1, (T)opt_.omega_rb);
-    g_launches += 2;
-  }
-}
-
-template <typename T>
-void Multigrid::vcycle(int n) {
-  Level& F = lv_[n];
-  LV<T> f = view<T>(F);
-  if (n == 0) {
-    // coarsest level (multigrid.c:461-511): a single cell carries no information
-    if (F.Nx == 1 && F.Ny == 1) {
-      cudaMemsetAsync(f.e, 0, sizeof(T), s_);
-      return;
+void Multigrid::enqueue_vcycle(cudaStream_t s) {
+  const int top = (int)lv_.size() - 1;
+  const T omega = (T)opt_.omega_rb;
+  const int pre = opt_.pre, post = opt_.post;
+  // down through the tiled levels
+  for (int n = top; n > ctop_; --n) {
+    Level& F = lv_[n];
+    LV<T> f = view<T>(F), c = view<T>(lv_[n - 1]);
+    // coarse corrections, and the FP32 correction of the defect loop, start from zero
+    bool zero_e = (n != top) || (sizeof(T) == 4);
+    bool fused = F.power2 && F.Nx >= BX && F.Ny >= BY && pre == 1;
+    if (fused) {
+      down_kernel<T, 1><<<dim3((F.Nx + BX - 1) / BX, (F.Ny + BY - 1) / BY), TB, tile_smem<T, 3>(), s>>>(
+          f, c, omega, zero_e ? 1 : 0);
+      ++g_launches;
+    } else {
+      if (zero_e) cudaMemsetAsync(f.e, 0, (size_t)F.pitch * F.Ny * sizeof(T), s);
+      for (int q = 0; q < pre; ++q) {
+        smooth_kernel<T><<<g2(f.Nx, f.Ny), B2, 0, s>>>(f, 0, omega);
+        smooth_kernel<T><<<g2(f.Nx, f.Ny), B2, 0, s>>>(f, 1, omega);
+      }
+      residual_kernel<T><<<g2(f.Nx, f.Ny), B2, 0, s>>>(f);
+      restrict_general_kernel<T><<<g2(c.Nx, c.Ny), B2, 0, s>>>(f, c);
+      g_launches += 2 * pre + 2;
     }
   }
-  smooth<T>(n, opt_.pre);
-  if (n == 0) {
-    smooth<T>(n, opt_.post);
-    return;
-  }
-  LV<T> c = view<T>(lv_[n - 1]);
-  if (F.power2) {
-    residual_restrict_kernel<T><<<g2(c.Nx, c.Ny), B2, 0, s_>>>(f, c);
+  // coarse block
+  {
+    CoarseDesc d;
+    memset(&d, 0, sizeof(d));
+    d.n = ctop_ + 1;
+    int total = 0;
+    for (int m = 0; m <= ctop_; ++m) {
+      const Level& L = lv_[m];
+      d.Nx[m] = L.Nx; d.Ny[m] = L.Ny; d.pitch[m] = L.pitch; d.power2[m] = L.power2 ? 1 : 0;
+      d.off[m] = total;
+      total += L.Nx * L.Ny;
+      if (sizeof(T) == 8) { d.Ow[m] = L.Ow; d.Os[m] = L.Os; d.rO[m] = L.rOsum; }
+      else { d.Ow[m] = L.Ow32; d.Os[m] = L.Os32; d.rO[m] = L.rOsum32; }
+    }
+    d.total = total;
+    const Level& Ltop = lv_[ctop_];
+    d.top_rhs = sizeof(T) == 8 ? (const void*)Ltop.rhs : (const void*)Ltop.rhs32;
+    d.top_e = sizeof(T) == 8 ? (void*)Ltop.e : (void*)Ltop.e32;
+    // when the coarse block is the whole problem, the FP64 solve iterates on pi itself
+    d.top_from_e = (ctop_ == top && sizeof(T) == 8) ? 1 : 0;
+    d.wew = wew_; d.wns = wns_; d.pre = pre; d.post = post;
+    size_t shm = (size_t)(5 * total + Ltop.Nx * Ltop.Ny) * sizeof(T);
+    coarse_kernel<T><<<1, CT, shm, s>>>(d, omega);
     ++g_launches;
-  } else {
-    g_launches += 2;
-    residual_kernel<T><<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f);
-    restrict_general_kernel<T><<<g2(c.Nx, c.Ny), B2, 0, s_>>>(f, f.res, c, c.rhs);
   }
-  vcycle<T>(n - 1);
-  prolong_correct_kernel<T><<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f, c, F.power2 ? 1 : 0, wew_, wns_);
-  ++g_launches;
-  smooth<T>(n, opt_.post);
+  // up through the tiled levels
+  for (int n = ctop_ + 1; n <= top; ++n) {
+    Level& F = lv_[n];
+    LV<T> f = view<T>(F), c = view<T>(lv_[n - 1]);
+    bool fused = F.power2 && F.Nx >= BX && F.Ny >= BY && post == 1;
+    if (fused) {
+      up_kernel<T, 1><<<dim3((F.Nx + BX - 1) / BX, (F.Ny + BY - 1) / BY), TB, tile_smem<T, 2>(), s>>>(
+          f, c, omega, wew_, wns_, 0);
+      ++g_launches;
+    } else {
+      prolong_correct_kernel<T><<<g2(f.Nx, f.Ny), B2, 0, s>>>(f, c, F.power2 ? 1 : 0, wew_, wns_);
+      for (int q = 0; q < post; ++q) {
+        smooth_kernel<T><<<g2(f.Nx, f.Ny), B2, 0, s>>>(f, 0, omega);
+        smooth_kernel<T><<<g2(f.Nx, f.Ny), B2, 0, s>>>(f, 1, omega);
+      }
+      g_launches += 1 + 2 * post;
+    }
+  }
+}
+
+void Multigrid::set_fine(double* pi, const double* rhs) {
+  fine_pi_ = pi;
+  fine_rhs_ = rhs;
+  Level& F = lv_.back();
+  F.e = pi;
+  F.rhs = const_cast<double*>(rhs);
+}
+
+int Multigrid::build_graph(int prec) {
+  LoopState* st = reinterpret_cast<LoopState*>(dstate_);
+  cudaGraph_t& G = g_->graph[prec];
+  if (cudaGraphCreate(&G, 0) != cudaSuccess) return -1;
+  if (cudaGraphConditionalHandleCreate(&g_->handle[prec], G, 1, cudaGraphCondAssignDefault) != cudaSuccess) return -1;
+  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+  cp.conditional.handle = g_->handle[prec];
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (cudaGraphAddNode(&node, G, nullptr, 0, &cp) != cudaSuccess) return -1;
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  const long long counted = g_launches;   // captured launches are counted per executed cycle
+  if (cudaStreamBeginCaptureToGraph(cap_, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+    return -1;
+  Level& F = lv_.back();
+  if (prec == 0) {
+    enqueue_vcycle<double>(cap_);
+    LV<double> f = view<double>(F);
+    max_residual_kernel<<<g2(f.Nx, f.Ny), B2, 0, cap_>>>(f, &st->bits);
+  } else {
+    enqueue_vcycle<float>(cap_);
+    LV<double> f = view<double>(F);
+    defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, cap_>>>(f, F.e32, F.pitch, F.rhs32, F.res, 1, &st->bits);
+    commit_kernel<<<g2(f.Nx, f.Ny), B2, 0, cap_>>>(F.e, F.res, F.Nx, F.Ny, F.pitch);
+  }
+  loop_finalize_kernel<<<1, 1, 0, cap_>>>(st, g_->handle[prec]);
+  g_launches = counted;
+  if (cudaStreamEndCapture(cap_, &body) != cudaSuccess) return -1;
+  if (cudaGraphInstantiate(&g_->exec[prec], G, 0) != cudaSuccess) return -1;
+  return 0;
 }
 
 double Multigrid::max_residual(const double* pi, int pitch, const double* rhs, int rhs_pitch) {
@@ -424,11 +806,12 @@ double Multigrid::max_residual(const double* pi, int pitch, const double* rhs, i
   f.e = const_cast<double*>(pi);
   f.rhs = const_cast<double*>(rhs);
   (void)pitch; (void)rhs_pitch;
-  cudaMemsetAsync(dbits_, 0, sizeof(unsigned long long), s_);
-  max_residual_kernel<<<148, 256, 0, s_>>>(f, dbits_);
+  LoopState* st = reinterpret_cast<LoopState*>(dstate_);
+  cudaMemsetAsync(&st->bits, 0, sizeof(unsigned long long), s_);
+  max_residual_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f, &st->bits);
   ++g_launches;
   unsigned long long b = 0;
-  cudaMemcpyAsync(&b, dbits_, sizeof(b), cudaMemcpyDeviceToHost, s_);
+  cudaMemcpyAsync(&b, &st->bits, sizeof(b), cudaMemcpyDeviceToHost, s_);
   cudaStreamSynchronize(s_);
   double m;
   memcpy(&m, &b, sizeof(m));
@@ -437,53 +820,84 @@ double Multigrid::max_residual(const double* pi, int pitch, const double* rhs, i
 
 int Multigrid::solve(double* pi, int pitch, const double* rhs, int rhs_pitch, double tol, int maxiters,
                      double* maxres_out) {
-  const int top = (int)lv_.size() - 1;
-  fine_pi_ = pi;
-  fine_rhs_ = rhs;
-  Level& F = lv_[top];
-  int iters = 0;
-  double maxres = tol + 1;
-  if (!opt_.fp32_cycles) {
-    // the fine level of the FP64 hierarchy works on the caller's pi and rhs
-    double *se = F.e, *sr = F.rhs;
-    F.e = pi;
-    F.rhs = const_cast<double*>(rhs);
-    while (maxres > tol && iters < maxiters) {
-      vcycle<double>(top);
-      maxres = max_residual(pi, pitch, rhs, rhs_pitch);
-      ++iters;
+  (void)pitch; (void)rhs_pitch;
+  const int prec = opt_.fp32_cycles ? 1 : 0;
+  if (fine_pi_ != pi || fine_rhs_ != rhs || g_->pre != opt_.pre || g_->post != opt_.post ||
+      g_->omega != opt_.omega_rb) {
+    for (int p = 0; p < 2; ++p) {
+      if (g_->exec[p]) cudaGraphExecDestroy(g_->exec[p]);
+      if (g_->graph[p]) cudaGraphDestroy(g_->graph[p]);
+      g_->exec[p] = nullptr;
+      g_->graph[p] = nullptr;
     }
-    F.e = se;
-    F.rhs = sr;
-  } else {
-    LV<double> f = view<double>(F);
-    f.e = pi;
-    f.rhs = const_cast<double*>(rhs);
-    int correct = 0;
-    // the first defect step only forms the residual of the initial pi
-    cudaMemsetAsync(dbits_, 0, sizeof(unsigned long long), s_);
-    defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f, F.e32, F.pitch, F.rhs32, F.e32, correct, dbits_);
-    ++g_launches;
-    while (maxres > tol && iters < maxiters) {
-      vcycle<float>(top);
-      cudaMemsetAsync(dbits_, 0, sizeof(unsigned long long), s_);
-      defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f, F.e32, F.pitch, F.rhs32, F.res32, 1, dbits_);
-      commit_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f);
-      g_launches += 2;
-      // the zeroed correction for the next cycle was written to res32; swap the buffers
-      float* t = F.e32; F.e32 = F.res32; F.res32 = t;
-      unsigned long long b = 0;
-      cudaMemcpyAsync(&b, dbits_, sizeof(b), cudaMemcpyDeviceToHost, s_);
-      cudaStreamSynchronize(s_);
-      memcpy(&maxres, &b, sizeof(maxres));
-      ++iters;
-    }
+    g_->pre = opt_.pre;
+    g_->post = opt_.post;
+    g_->omega = opt_.omega_rb;
   }
-  if (maxres_out) *maxres_out = maxres;
-  return iters;
+  set_fine(pi, rhs);
+  LoopState* st = reinterpret_cast<LoopState*>(dstate_);
+  if (getenv("PAWSIM_MG_HOST_LOOP")) {
+    // host-driven loop with the same kernels (for profilers that do not see inside the
+    // conditional graph node)
+    Level& F = lv_.back();
+    LV<double> f = view<double>(F);
+    int it = 0;
+    double mres = tol + 1;
+    if (prec == 1) {
+      cudaMemsetAsync(&st->bits, 0, sizeof(unsigned long long), s_);
+      defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f, F.e32, F.pitch, F.rhs32, F.res, 0, &st->bits);
+    }
+    while (mres > tol && it < maxiters) {
+      cudaMemsetAsync(&st->bits, 0, sizeof(unsigned long long), s_);
+      if (prec == 0) {
+        enqueue_vcycle<double>(s_);
+        max_residual_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f, &st->bits);
+      } else {
+        enqueue_vcycle<float>(s_);
+        defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f, F.e32, F.pitch, F.rhs32, F.res, 1, &st->bits);
+        commit_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(F.e, F.res, F.Nx, F.Ny, F.pitch);
+      }
+      unsigned long long b = 0;
+      cudaMemcpyAsync(&b, &st->bits, sizeof(b), cudaMemcpyDeviceToHost, s_);
+      if (cudaStreamSynchronize(s_) != cudaSuccess) return -1;
+      memcpy(&mres, &b, sizeof(mres));
+      ++it;
+    }
+    if (maxres_out) *maxres_out = mres;
+    return it;
+  }
+  if (!g_->exec[prec] && build_graph(prec) != 0) return -1;
+  loop_reset_kernel<<<1, 1, 0, s_>>>(st, maxiters, tol);
+  ++g_launches;
+  if (prec == 1) {
+    Level& F = lv_.back();
+    LV<double> f = view<double>(F);
+    defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f, F.e32, F.pitch, F.rhs32, F.res, 0, &st->bits);
+    cudaMemsetAsync(&st->bits, 0, sizeof(unsigned long long), s_);
+    ++g_launches;
+  }
+  if (cudaGraphLaunch(g_->exec[prec], s_) != cudaSuccess) return -1;
+  LoopState h;
+  cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s_);
+  if (cudaStreamSynchronize(s_) != cudaSuccess) return -1;
+  // kernels of the graph body, counted once per executed V-cycle
+  g_launches += (long long)h.iters * body_launches(prec);
+  if (maxres_out) *maxres_out = h.maxres;
+  return h.iters;
 }
 
-template void Multigrid::vcycle<double>(int);
-template void Multigrid::vcycle<float>(int);
+int Multigrid::body_launches(int prec) const {
+  const int top = (int)lv_.size() - 1;
+  int k = 0;
+  for (int n = top; n > ctop_; --n) {
+    const Level& F = lv_[n];
+    bool fused = F.power2 && F.Nx >= BX && F.Ny >= BY;
+    k += fused ? 2 : (2 * opt_.pre + 2) + (1 + 2 * opt_.post);
+  }
+  return k + 1 + (prec ? 3 : 2);
+}
+
+template void Multigrid::enqueue_vcycle<double>(cudaStream_t);
+template void Multigrid::enqueue_vcycle<float>(cudaStream_t);
 
 }  // namespace pawsim

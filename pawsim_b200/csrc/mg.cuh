@@ -53,20 +53,24 @@ class Multigrid {
   };
 
  private:
-  template <typename T> void vcycle(int n);
-  template <typename T> void smooth(int n, int sweeps);
-  void set_fine(double* pi, int pitch, const double* rhs, int rhs_pitch);
+  template <typename T> void enqueue_vcycle(cudaStream_t s);
+  void set_fine(double* pi, const double* rhs);
+  int build_graph(int prec);
+  int body_launches(int prec) const;
+  struct Graphs;
   bool ok_ = false;
   int Nx_, Ny_;
   bool wew_, wns_;
   MGOptions opt_;
   cudaStream_t s_;
-  std::vector<Level> lv_;   // index 0 is the coarsest
-  double* dmax_ = nullptr;  // device scalar
-  unsigned long long* dbits_ = nullptr;
+  cudaStream_t cap_ = nullptr;     // stream used only to capture the V-cycle graph
+  std::vector<Level> lv_;          // index 0 is the coarsest
+  int ctop_ = 0;                   // top level of the single-CTA coarse block
+  void* dstate_ = nullptr;         // device loop state (stopping measure, iteration count)
+  Graphs* g_ = nullptr;
   double* fine_pi_ = nullptr;
   const double* fine_rhs_ = nullptr;
-  int fine_pitch_ = 0, fine_rhs_pitch_ = 0;
+  double *own_e_ = nullptr, *own_rhs_ = nullptr;
 };
 
 }  // namespace pawsim

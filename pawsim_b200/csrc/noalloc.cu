@@ -66,6 +66,7 @@ extern "C" int pawsim_pressure_rhs_noalloc(const double* u, const double* v, con
   Grid2 g;
   g.Nx = Nx; g.Ny = Ny; g.pitch = pitch; g.L = Nlay; g.lstride = (size_t)Ny * pitch;
   g.wall_ew = wall_ew; g.wall_ns = wall_ns; g.dx = dx; g.dy = dy; g.dt = dt; g.thick_scheme = thick_scheme;
+  g.rdx = 1.0 / dx; g.rdy = 1.0 / dy; g.rdxdt = 1.0 / (dx * dt); g.rdydt = 1.0 / (dy * dt);
   bool serial = serial_sum == 1 || (serial_sum < 0 && (long long)Nx * Ny <= 65536);
   launch_pressure_rhs(g, u, v, h, rhs, s);
   launch_sum(rhs, Nx, Ny, pitch, serial, scratch + 1, scratch, s);

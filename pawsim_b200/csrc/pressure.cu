@@ -20,8 +20,8 @@ __device__ inline double ld_s(const double* f, const Grid2& g, int i, int j) {
 // Gathered face thickness with wrapped indices (work.c:865-1030), at an owned cell.
 __device__ inline double hw_gathered(const Grid2& g, const double* h, int i, int j) {
   int Nx = g.Nx, Ny = g.Ny;
-  int im1 = wrap_index(i - 1, Nx), ip1 = wrap_index(i + 1, Nx);
-  int jm1 = wrap_index(j - 1, Ny), jp1 = wrap_index(j + 1, Ny);
+  int im1 = i == 0 ? Nx - 1 : i - 1, ip1 = i + 1 == Nx ? 0 : i + 1;
+  int jm1 = j == 0 ? Ny - 1 : j - 1, jp1 = j + 1 == Ny ? 0 : j + 1;
   const int P = g.pitch;
 #define H(ii, jj) h[(size_t)(jj) * P + (ii)]
   if (g.thick_scheme == 1) {
@@ -36,9 +36,9 @@ __device__ inline double hw_gathered(const Grid2& g, const double* h, int i, int
 }
 
 __device__ inline double hs_gathered(const Grid2& g, const double* h, int i, int j) {
-  int Nx = g.Nx, Ny = g.Ny;
-  int im1 = wrap_index(i - 1, Nx), ip1 = wrap_index(i + 1, Nx);
-  int jm1 = wrap_index(j - 1, Ny);
+  int Nx = g.Nx;
+  int im1 = i == 0 ? Nx - 1 : i - 1, ip1 = i + 1 == Nx ? 0 : i + 1;
+  int jm1 = j == 0 ? g.Ny - 1 : j - 1;
   const int P = g.pitch;
   if (g.thick_scheme == 1) {
     if (g.wall_ew && i == 0)
@@ -76,18 +76,31 @@ __global__ void rhs_kernel(const Grid2 g, const double* __restrict__ u, const do
   if (i >= g.Nx || j >= g.Ny) return;
   double acc = 0;
   double dxdt = g.dx * g.dt, dydt = g.dy * g.dt;
+  const bool inner = i > 0 && j > 0 && i + 1 < g.Nx && j + 1 < g.Ny && g.thick_scheme == 0;
+  const size_t c = (size_t)j * g.pitch + i;
   for (int k = 0; k < g.L; ++k) {
     const double* uk = u + k * g.lstride;
     const double* vk = v + k * g.lstride;
     const double* hk = h + k * g.lstride;
-    double hu_w = ld_u(g, uk, i, j) * hw_face(g, hk, i, j);
-    double hu_e = ld_u(g, uk, i + 1, j) * hw_face(g, hk, i + 1, j);
-    double hv_s = ld_v(g, vk, i, j) * hs_face(g, hk, i, j);
-    double hv_n = ld_v(g, vk, i, j + 1) * hs_face(g, hk, i, j + 1);
+    double hu_w, hu_e, hv_s, hv_n;
+    if (inner) {
+      // owned neighbours only: plain loads, AL81 face averages (work.c:889-901)
+      const size_t P = g.pitch;
+      double hc = hk[c];
+      hu_w = uk[c] * (0.5 * (hc + hk[c - 1]));
+      hu_e = uk[c + 1] * (0.5 * (hk[c + 1] + hc));
+      hv_s = vk[c] * (0.5 * (hc + hk[c - P]));
+      hv_n = vk[c + P] * (0.5 * (hk[c + P] + hc));
+    } else {
+      hu_w = ld_u(g, uk, i, j) * hw_face(g, hk, i, j);
+      hu_e = ld_u(g, uk, i + 1, j) * hw_face(g, hk, i + 1, j);
+      hv_s = ld_v(g, vk, i, j) * hs_face(g, hk, i, j);
+      hv_n = ld_v(g, vk, i, j + 1) * hs_face(g, hk, i, j + 1);
+    }
     if (with_dt)
-      acc += (hu_e - hu_w) / dxdt + (hv_n - hv_s) / dydt;
+      acc += div_rn(hu_e - hu_w, dxdt, g.rdxdt) + div_rn(hv_n - hv_s, dydt, g.rdydt);
     else
-      acc += (hu_e - hu_w) / g.dx + (hv_n - hv_s) / g.dy;
+      acc += div_rn(hu_e - hu_w, g.dx, g.rdx) + div_rn(hv_n - hv_s, g.dy, g.rdy);
   }
   rhs[(size_t)j * g.pitch + i] = acc;
 }
@@ -160,13 +173,18 @@ __global__ void max_abs_kernel(const double* __restrict__ f, int Nx, int Ny, int
                                unsigned long long* out) {
   // fmax semantics: NaN entries are ignored, as C's fmax does
   double m = 0;
-  int n = Nx * Ny;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-    double a = fabs(f[(size_t)(q / Nx) * pitch + (q % Nx)]);
-    m = fmax(m, a);
-  }
+  for (int j = blockIdx.y; j < Ny; j += gridDim.y)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < Nx; i += gridDim.x * blockDim.x)
+      m = fmax(m, fabs(f[(size_t)j * pitch + i]));
+  __shared__ double wm[32];
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double b = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b = fmax(b, wm[w]);
+    atomicMax(out, (unsigned long long)__double_as_longlong(b));
+  }
 }
 
 __global__ void store_max_kernel(const unsigned long long* bits, double* out) {
@@ -244,8 +262,6 @@ __global__ void __launch_bounds__(512) sor_kernel(const Grid2 g, double* pi, con
   cg::grid_group grid = cg::this_grid();
   __shared__ double wmax[16];
   const double one_minus_w = 1 - sor_rp;
-  const int n = g.Nx * g.Ny;
-  const int stride = gridDim.x * blockDim.x;
   int iters = 0;
   double gmax = tol + 1;
   if (blockIdx.x == 0 && threadIdx.x == 0) { slots[0] = 0; slots[1] = 0; }
@@ -253,12 +269,12 @@ __global__ void __launch_bounds__(512) sor_kernel(const Grid2 g, double* pi, con
   while ((gmax > tol) && (iters < maxiters)) {
     double lmax = 0;
     for (int color = 0; color < 2; ++color) {
-      for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
-        int j = q / g.Nx, i = q % g.Nx;
-        if (((i + j) & 1) != color) continue;
-        double d = sor_point(g, pi, rhs, op, one_minus_w, i, j);
-        lmax = fmax(lmax, d);
-      }
+      // rows are dealt to blocks; within a row a thread visits only cells of this colour
+      for (int j = blockIdx.x; j < g.Ny; j += gridDim.x)
+        for (int i = 2 * threadIdx.x + ((j + color) & 1); i < g.Nx; i += 2 * blockDim.x) {
+          double d = sor_point(g, pi, rhs, op, one_minus_w, i, j);
+          lmax = fmax(lmax, d);
+        }
       grid.sync();
     }
     for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_down_sync(0xffffffffu, lmax, o));
@@ -285,13 +301,14 @@ __global__ void projection_kernel(const Grid2 g, const double* __restrict__ pi, 
   if (i >= g.Nx || j >= g.Ny) return;
   size_t c = (size_t)j * g.pitch + i;
   double pc = pi[c];
-  double pw = ld_s(pi, g, i - 1, j), ps = ld_s(pi, g, i, j - 1);
+  double pw = i > 0 ? pi[c - 1] : ld_s(pi, g, i - 1, j);
+  double ps = j > 0 ? pi[c - g.pitch] : ld_s(pi, g, i, j - 1);
   bool skip_u = g.wall_ew && i == 0;
   bool skip_v = g.wall_ns && j == 0;
   for (int k = 0; k < g.L; ++k) {
     size_t o = k * g.lstride + c;
-    if (!skip_u) u[o] += -g.dt * (pc - pw) / g.dx;
-    if (!skip_v) v[o] += -g.dt * (pc - ps) / g.dy;
+    if (!skip_u) u[o] += div_rn(-g.dt * (pc - pw), g.dx, g.rdx);
+    if (!skip_v) v[o] += div_rn(-g.dt * (pc - ps), g.dy, g.rdy);
   }
 }
 
@@ -348,7 +365,7 @@ void launch_norms(const double* f, int Nx, int Ny, int pitch, bool serial, doubl
   // out[0] = max |f| (via an integer max on the bit pattern, in out[2] as scratch), out[1] = sum f^2
   unsigned long long* bits = reinterpret_cast<unsigned long long*>(out + 2);
   cudaMemsetAsync(bits, 0, sizeof(unsigned long long), s);
-  max_abs_kernel<<<148, 256, 0, s>>>(f, Nx, Ny, pitch, bits);
+  max_abs_kernel<<<dim3(1, Ny < 1184 ? Ny : 1184), 256, 0, s>>>(f, Nx, Ny, pitch, bits);
   store_max_kernel<<<1, 1, 0, s>>>(bits, out);
   if (serial) {
     serial_sum_kernel<<<1, 32, 0, s>>>(f, Nx, Ny, pitch, out + 1, 1);
@@ -372,7 +389,7 @@ int launch_sor(const Grid2& g, double* pi, const double* rhs, const Operator& op
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const int threads = 512;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sor_kernel, threads, 0);
-  int want = (g.Nx * g.Ny + threads - 1) / threads;
+  int want = g.Ny;   // one block per row at most
   int cap = nsm * (per_sm < 1 ? 1 : per_sm);
   int blocks = want < cap ? want : cap;
   if (blocks < 1) blocks = 1;

@@ -13,6 +13,7 @@ struct Grid2 {
   int wall_ew, wall_ns;
   double dx, dy, dt;
   int thick_scheme;
+  double rdx, rdy, rdxdt, rdydt;   // reciprocals rounded to nearest, for div_rn
 };
 
 // rhs = sum_k div(h_k u_k) / dt with the gathered face thickness (pressure.c:570-606)

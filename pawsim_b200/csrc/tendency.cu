@@ -66,35 +66,37 @@ __device__ inline double sq(double x) { return x * x; }
 // PV interpolation coefficients (work.c:1294-1404) evaluated from qq in shared memory
 template <int MS> struct Coef {
   const double* q;
+  double r24;
+  __device__ double D(double x) const { return div_rn(x, 24.0, r24); }
   __device__ double Q(int x, int y) const { return AT(q, x, y); }
   __device__ double alpha(int i, int j) const {
     if (MS == 3)
-      return (2 * Q(i + 1, j + 1) + 3 * Q(i, j + 1) + 2 * Q(i, j) + Q(i + 1, j) - Q(i, j + 2) - Q(i - 1, j + 1)) / 24;
-    return (2 * Q(i + 1, j + 1) + Q(i, j + 1) + 2 * Q(i, j) + Q(i + 1, j)) / 24;
+      return D(2 * Q(i + 1, j + 1) + 3 * Q(i, j + 1) + 2 * Q(i, j) + Q(i + 1, j) - Q(i, j + 2) - Q(i - 1, j + 1));
+    return D(2 * Q(i + 1, j + 1) + Q(i, j + 1) + 2 * Q(i, j) + Q(i + 1, j));
   }
   __device__ double beta(int i, int j) const {
     if (MS == 3)
-      return (3 * Q(i, j + 1) + 2 * Q(i - 1, j + 1) + Q(i - 1, j) + 2 * Q(i, j) - Q(i + 1, j + 1) - Q(i, j + 2)) / 24;
-    return (Q(i, j + 1) + 2 * Q(i - 1, j + 1) + Q(i - 1, j) + 2 * Q(i, j)) / 24;
+      return D(3 * Q(i, j + 1) + 2 * Q(i - 1, j + 1) + Q(i - 1, j) + 2 * Q(i, j) - Q(i + 1, j + 1) - Q(i, j + 2));
+    return D(Q(i, j + 1) + 2 * Q(i - 1, j + 1) + Q(i - 1, j) + 2 * Q(i, j));
   }
   __device__ double gamma(int i, int j) const {
     if (MS == 3)
-      return (2 * Q(i, j + 1) + Q(i - 1, j + 1) + 2 * Q(i - 1, j) + 3 * Q(i, j) - Q(i, j - 1) - Q(i + 1, j)) / 24;
-    return (2 * Q(i, j + 1) + Q(i - 1, j + 1) + 2 * Q(i - 1, j) + Q(i, j)) / 24;
+      return D(2 * Q(i, j + 1) + Q(i - 1, j + 1) + 2 * Q(i - 1, j) + 3 * Q(i, j) - Q(i, j - 1) - Q(i + 1, j));
+    return D(2 * Q(i, j + 1) + Q(i - 1, j + 1) + 2 * Q(i - 1, j) + Q(i, j));
   }
   __device__ double delta(int i, int j) const {
     if (MS == 3)
-      return (Q(i + 1, j + 1) + 2 * Q(i, j + 1) + 3 * Q(i, j) + 2 * Q(i + 1, j) - Q(i - 1, j) - Q(i, j - 1)) / 24;
-    return (Q(i + 1, j + 1) + 2 * Q(i, j + 1) + Q(i, j) + 2 * Q(i + 1, j)) / 24;
+      return D(Q(i + 1, j + 1) + 2 * Q(i, j + 1) + 3 * Q(i, j) + 2 * Q(i + 1, j) - Q(i - 1, j) - Q(i, j - 1));
+    return D(Q(i + 1, j + 1) + 2 * Q(i, j + 1) + Q(i, j) + 2 * Q(i + 1, j));
   }
   __device__ double epsilon(int i, int j) const {
-    return (Q(i + 1, j + 1) + Q(i, j + 1) - Q(i, j) - Q(i + 1, j)) / 24;
+    return D(Q(i + 1, j + 1) + Q(i, j + 1) - Q(i, j) - Q(i + 1, j));
   }
   __device__ double phi(int i, int j) const {
-    return (-Q(i + 1, j + 1) + Q(i, j + 1) + Q(i, j) - Q(i + 1, j)) / 24;
+    return D(-Q(i + 1, j + 1) + Q(i, j + 1) + Q(i, j) - Q(i + 1, j));
   }
-  __device__ double lambda(int i, int j) const { return (Q(i + 1, j) - Q(i - 1, j)) / 24; }
-  __device__ double mu(int i, int j) const { return (Q(i, j - 1) - Q(i, j + 1)) / 24; }
+  __device__ double lambda(int i, int j) const { return D(Q(i + 1, j) - Q(i - 1, j)); }
+  __device__ double mu(int i, int j) const { return D(Q(i, j - 1) - Q(i, j + 1)); }
 };
 
 // face thickness of one layer at a local position (work.c:566-684, AL81 and HK83)
@@ -157,8 +159,12 @@ __device__ inline double gface_south(const TendParams& p, const double* h, int i
   return 0.5 * (gload(h, p, i, j, MAP_S, MAP_S) + gload(h, p, i, j - 1, MAP_S, MAP_S));
 }
 
+#ifndef PAWSIM_TEND_MINB
+#define PAWSIM_TEND_MINB 4
+#endif
+
 template <int MS, int TS>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, PAWSIM_TEND_MINB)
 tendency_kernel(const __grid_constant__ TendParams p) {
   extern __shared__ double smem[];
   double* F[F_NUM];
@@ -176,7 +182,9 @@ tendency_kernel(const __grid_constant__ TendParams p) {
   t.wx = p.wall_ew;
   t.wy = p.wall_ns;
   const int L = p.L;
-  const double dx = p.dx, dy = p.dy;
+  const double dx = p.dx, dy = p.dy, rdx = p.rdx, rdy = p.rdy, r24 = p.r24;
+  // tiles whose halo lies inside the domain read global memory without boundary maps
+  const bool inner = t.X0 - HALO >= 0 && t.X0 + TX + HALO <= p.Nx && t.Y0 - HALO >= 0 && t.Y0 + TY + HALO <= p.Ny;
 
   // ---- column prologue over the Bernoulli region: eta, pp, Montgomery MM, wdia ----
   for (int q = tid; q < RN; q += NT) {
@@ -190,10 +198,11 @@ tendency_kernel(const __grid_constant__ TendParams p) {
     }
     int gi = t.gx(lx), gj = t.gy(ly);
     double hk[LMAX], eta[LMAX + 1];
-    double hb = gload(p.hhb, p, gi, gj, MAP_S, MAP_S);
+    const size_t gc = (size_t)gj * p.pitch + gi;
+    double hb = inner ? p.hhb[gc] : gload(p.hhb, p, gi, gj, MAP_S, MAP_S);
     eta[L] = hb;
     for (int k = L - 1; k >= 0; --k) {
-      hk[k] = gload(p.h + k * p.lstride, p, gi, gj, MAP_S, MAP_S);
+      hk[k] = inner ? p.h[k * p.lstride + gc] : gload(p.h + k * p.lstride, p, gi, gj, MAP_S, MAP_S);
       eta[k] = eta[k + 1] + hk[k];
     }
     double pp = 0;
@@ -250,13 +259,23 @@ tendency_kernel(const __grid_constant__ TendParams p) {
     const double* hkp = p.h + k * p.lstride;
     __syncthreads();
     // ---- load the layer's u, v, h with the reference's ghost semantics ----
-    for (int q = tid; q < RN; q += NT) {
-      int lx = q % RW, ly = q / RW;
-      int gx = t.gx(lx), gy = t.gy(ly);
-      bool in = gx >= -HALO && gx < p.Nx + HALO && gy >= -HALO && gy < p.Ny + HALO;
-      F[F_U][q] = in ? gload(uk, p, gx, gy, MAP_N, MAP_S) : 0.0;
-      F[F_V][q] = in ? gload(vk, p, gx, gy, MAP_S, MAP_N) : 0.0;
-      F[F_H][q] = in ? gload(hkp, p, gx, gy, MAP_S, MAP_S) : 0.0;
+    if (inner) {
+      for (int q = tid; q < RN; q += NT) {
+        int lx = q % RW, ly = q / RW;
+        size_t g = (size_t)t.gy(ly) * p.pitch + t.gx(lx);
+        F[F_U][q] = uk[g];
+        F[F_V][q] = vk[g];
+        F[F_H][q] = hkp[g];
+      }
+    } else {
+      for (int q = tid; q < RN; q += NT) {
+        int lx = q % RW, ly = q / RW;
+        int gx = t.gx(lx), gy = t.gy(ly);
+        bool in = gx >= -HALO && gx < p.Nx + HALO && gy >= -HALO && gy < p.Ny + HALO;
+        F[F_U][q] = in ? gload(uk, p, gx, gy, MAP_N, MAP_S) : 0.0;
+        F[F_V][q] = in ? gload(vk, p, gx, gy, MAP_S, MAP_N) : 0.0;
+        F[F_H][q] = in ? gload(hkp, p, gx, gy, MAP_S, MAP_S) : 0.0;
+      }
     }
     __syncthreads();
     const double* su = F[F_U];
@@ -273,9 +292,11 @@ tendency_kernel(const __grid_constant__ TendParams p) {
       }
       if (lx >= 1 && ly >= 1) {
         // zeta, h on the q grid and q itself (work.c:1261-1270)
-        double z = (AT(su, lx, ly - 1) - AT(su, lx, ly)) / dy + (AT(sv, lx, ly) - AT(sv, lx - 1, ly)) / dx;
+        double z = div_rn(AT(su, lx, ly - 1) - AT(su, lx, ly), dy, rdy)
+                 + div_rn(AT(sv, lx, ly) - AT(sv, lx - 1, ly), dx, rdx);
         double hq = 0.25 * (AT(sh, lx, ly) + AT(sh, lx - 1, ly - 1) + AT(sh, lx - 1, ly) + AT(sh, lx, ly - 1));
-        double om = load_mapped(p.omz, p.qpitch, t.gx(lx), t.gy(ly), p.Nx, p.Ny, p.wall_ew, p.wall_ns, MAP_Q, MAP_Q);
+        double om = inner ? p.omz[(size_t)t.gy(ly) * p.qpitch + t.gx(lx)]
+                          : load_mapped(p.omz, p.qpitch, t.gx(lx), t.gy(ly), p.Nx, p.Ny, p.wall_ew, p.wall_ns, MAP_Q, MAP_Q);
         F[F_QQ][q] = (2 * om + z) / hq;
         F[F_HQ][q] = hq;
       }
@@ -284,9 +305,11 @@ tendency_kernel(const __grid_constant__ TendParams p) {
       }
       if (p.useA2 || p.useA4) {
         if (lx <= TX + 2 && ly <= TY + 2)
-          F[F_DT][q] = (AT(su, lx + 1, ly) - AT(su, lx, ly)) / dx - (AT(sv, lx, ly + 1) - AT(sv, lx, ly)) / dy;
+          F[F_DT][q] = div_rn(AT(su, lx + 1, ly) - AT(su, lx, ly), dx, rdx)
+                     - div_rn(AT(sv, lx, ly + 1) - AT(sv, lx, ly), dy, rdy);
         if (lx >= 1 && ly >= 1)
-          F[F_DS][q] = (AT(su, lx, ly) - AT(su, lx, ly - 1)) / dy + (AT(sv, lx, ly) - AT(sv, lx - 1, ly)) / dx;
+          F[F_DS][q] = div_rn(AT(su, lx, ly) - AT(su, lx, ly - 1), dy, rdy)
+                     + div_rn(AT(sv, lx, ly) - AT(sv, lx - 1, ly), dx, rdx);
       }
     }
     __syncthreads();
@@ -302,11 +325,11 @@ tendency_kernel(const __grid_constant__ TendParams p) {
       if (lx >= 1 && lx <= TX + 1 && ly >= 1 && ly <= TY + 2) F[F_HVV][q] = sv[q] * hs[q];
       if (p.useA4 && lx >= 1 && lx <= TX + 2 && ly >= 1 && ly <= TY + 2) {
         const double A = p.A4sqrt;
-        F[F_U4][q] = ((A * AT(sh, lx, ly) * AT(DT, lx, ly) - A * AT(sh, lx - 1, ly) * AT(DT, lx - 1, ly)) / dx
-                      + (A * AT(hq, lx, ly + 1) * AT(DS, lx, ly + 1) - A * AT(hq, lx, ly) * AT(DS, lx, ly)) / dy)
+        F[F_U4][q] = (div_rn(A * AT(sh, lx, ly) * AT(DT, lx, ly) - A * AT(sh, lx - 1, ly) * AT(DT, lx - 1, ly), dx, rdx)
+                      + div_rn(A * AT(hq, lx, ly + 1) * AT(DS, lx, ly + 1) - A * AT(hq, lx, ly) * AT(DS, lx, ly), dy, rdy))
                      / AT(hw, lx, ly);
-        F[F_V4][q] = ((A * AT(hq, lx + 1, ly) * AT(DS, lx + 1, ly) - A * AT(hq, lx, ly) * AT(DS, lx, ly)) / dx
-                      - (A * AT(sh, lx, ly) * AT(DT, lx, ly) - A * AT(sh, lx, ly - 1) * AT(DT, lx, ly - 1)) / dy)
+        F[F_V4][q] = (div_rn(A * AT(hq, lx + 1, ly) * AT(DS, lx + 1, ly) - A * AT(hq, lx, ly) * AT(DS, lx, ly), dx, rdx)
+                      - div_rn(A * AT(sh, lx, ly) * AT(DT, lx, ly) - A * AT(sh, lx, ly - 1) * AT(DT, lx, ly - 1), dy, rdy))
                      / AT(hs, lx, ly);
       }
     }
@@ -319,17 +342,18 @@ tendency_kernel(const __grid_constant__ TendParams p) {
     const double* MM = MMall + k * RN;
     const double* U4 = F[F_U4];
     const double* V4 = F[F_V4];
-    Coef<MS> c{F[F_QQ]};
+    Coef<MS> c{F[F_QQ], r24};
     const double* qq = F[F_QQ];
     const int i = ox, j = oy;
     const double hwest = AT(hw, i, j), hsouth = AT(hs, i, j);
+    const double rhw = 1.0 / hwest, rhs = 1.0 / hsouth;   // reciprocals for div_rn
     const double uc = AT(su, i, j), vc = AT(sv, i, j);
 
     // ---- u momentum (work.c:1667-1752) ----
     double ru;
     {
-      double gM = -(AT(MM, i, j) - AT(MM, i - 1, j)) / dx;
-      double gK = -(AT(KE, i, j) - AT(KE, i - 1, j)) / dx;
+      double gM = div_rn(-(AT(MM, i, j) - AT(MM, i - 1, j)), dx, rdx);
+      double gK = div_rn(-(AT(KE, i, j) - AT(KE, i - 1, j)), dx, rdx);
       double rq = 0;
       if (MS == 0 || MS == 1) {
         rq += c.alpha(i, j) * AT(hvv, i, j + 1) + c.beta(i, j) * AT(hvv, i - 1, j + 1)
@@ -347,25 +371,25 @@ tendency_kernel(const __grid_constant__ TendParams p) {
       double a2 = 0, a4 = 0;
       if (p.useA2) {
         const double A = p.A2;
-        a2 = ((A * AT(sh, i, j) * AT(DT, i, j) - A * AT(sh, i - 1, j) * AT(DT, i - 1, j)) / dx
-              + (A * AT(hq, i, j + 1) * AT(DS, i, j + 1) - A * AT(hq, i, j) * AT(DS, i, j)) / dy);
+        a2 = (div_rn(A * AT(sh, i, j) * AT(DT, i, j) - A * AT(sh, i - 1, j) * AT(DT, i - 1, j), dx, rdx)
+              + div_rn(A * AT(hq, i, j + 1) * AT(DS, i, j + 1) - A * AT(hq, i, j) * AT(DS, i, j), dy, rdy));
       }
       if (p.useA4) {
         const double A = p.A4sqrt;
-        double d4t0 = (AT(U4, i + 1, j) - AT(U4, i, j)) / dx - (AT(V4, i, j + 1) - AT(V4, i, j)) / dy;
-        double d4tm = (AT(U4, i, j) - AT(U4, i - 1, j)) / dx - (AT(V4, i - 1, j + 1) - AT(V4, i - 1, j)) / dy;
-        double d4s1 = (AT(U4, i, j + 1) - AT(U4, i, j)) / dy + (AT(V4, i, j + 1) - AT(V4, i - 1, j + 1)) / dx;
-        double d4s0 = (AT(U4, i, j) - AT(U4, i, j - 1)) / dy + (AT(V4, i, j) - AT(V4, i - 1, j)) / dx;
-        a4 = -((A * AT(sh, i, j) * d4t0 - A * AT(sh, i - 1, j) * d4tm) / dx
-               + (A * AT(hq, i, j + 1) * d4s1 - A * AT(hq, i, j) * d4s0) / dy);
+        double d4t0 = div_rn(AT(U4, i + 1, j) - AT(U4, i, j), dx, rdx) - div_rn(AT(V4, i, j + 1) - AT(V4, i, j), dy, rdy);
+        double d4tm = div_rn(AT(U4, i, j) - AT(U4, i - 1, j), dx, rdx) - div_rn(AT(V4, i - 1, j + 1) - AT(V4, i - 1, j), dy, rdy);
+        double d4s1 = div_rn(AT(U4, i, j + 1) - AT(U4, i, j), dy, rdy) + div_rn(AT(V4, i, j + 1) - AT(V4, i - 1, j + 1), dx, rdx);
+        double d4s0 = div_rn(AT(U4, i, j) - AT(U4, i, j - 1), dy, rdy) + div_rn(AT(V4, i, j) - AT(V4, i - 1, j), dx, rdx);
+        a4 = -(div_rn(A * AT(sh, i, j) * d4t0 - A * AT(sh, i - 1, j) * d4tm, dx, rdx)
+               + div_rn(A * AT(hq, i, j + 1) * d4s1 - A * AT(hq, i, j) * d4s0, dy, rdy));
       }
-      ru = gM + gK + rq + ((hwest != 0) ? (a2 + a4 + 0.0) / hwest : 0);
+      ru = gM + gK + rq + ((hwest != 0) ? div_rn(a2 + a4 + 0.0, hwest, rhw) : 0);
     }
     // ---- v momentum (work.c:1759-1852) ----
     double rv;
     {
-      double gM = -(AT(MM, i, j) - AT(MM, i, j - 1)) / dy;
-      double gK = -(AT(KE, i, j) - AT(KE, i, j - 1)) / dy;
+      double gM = div_rn(-(AT(MM, i, j) - AT(MM, i, j - 1)), dy, rdy);
+      double gK = div_rn(-(AT(KE, i, j) - AT(KE, i, j - 1)), dy, rdy);
       double rq = 0;
       if (MS == 0 || MS == 1) {
         rq += c.phi(i, j - 1) * AT(hvv, i, j - 1) - c.phi(i, j) * AT(hvv, i, j + 1)
@@ -383,19 +407,19 @@ tendency_kernel(const __grid_constant__ TendParams p) {
       double a2 = 0, a4 = 0;
       if (p.useA2) {
         const double A = p.A2;
-        a2 = ((A * AT(hq, i + 1, j) * AT(DS, i + 1, j) - A * AT(hq, i, j) * AT(DS, i, j)) / dx
-              - (A * AT(sh, i, j) * AT(DT, i, j) - A * AT(sh, i, j - 1) * AT(DT, i, j - 1)) / dy);
+        a2 = (div_rn(A * AT(hq, i + 1, j) * AT(DS, i + 1, j) - A * AT(hq, i, j) * AT(DS, i, j), dx, rdx)
+              - div_rn(A * AT(sh, i, j) * AT(DT, i, j) - A * AT(sh, i, j - 1) * AT(DT, i, j - 1), dy, rdy));
       }
       if (p.useA4) {
         const double A = p.A4sqrt;
-        double d4s1 = (AT(U4, i + 1, j) - AT(U4, i + 1, j - 1)) / dy + (AT(V4, i + 1, j) - AT(V4, i, j)) / dx;
-        double d4s0 = (AT(U4, i, j) - AT(U4, i, j - 1)) / dy + (AT(V4, i, j) - AT(V4, i - 1, j)) / dx;
-        double d4t0 = (AT(U4, i + 1, j) - AT(U4, i, j)) / dx - (AT(V4, i, j + 1) - AT(V4, i, j)) / dy;
-        double d4tm = (AT(U4, i + 1, j - 1) - AT(U4, i, j - 1)) / dx - (AT(V4, i, j) - AT(V4, i, j - 1)) / dy;
-        a4 = -((A * AT(hq, i + 1, j) * d4s1 - A * AT(hq, i, j) * d4s0) / dx
-               - (A * AT(sh, i, j) * d4t0 - A * AT(sh, i, j - 1) * d4tm) / dy);
+        double d4s1 = div_rn(AT(U4, i + 1, j) - AT(U4, i + 1, j - 1), dy, rdy) + div_rn(AT(V4, i + 1, j) - AT(V4, i, j), dx, rdx);
+        double d4s0 = div_rn(AT(U4, i, j) - AT(U4, i, j - 1), dy, rdy) + div_rn(AT(V4, i, j) - AT(V4, i - 1, j), dx, rdx);
+        double d4t0 = div_rn(AT(U4, i + 1, j) - AT(U4, i, j), dx, rdx) - div_rn(AT(V4, i, j + 1) - AT(V4, i, j), dy, rdy);
+        double d4tm = div_rn(AT(U4, i + 1, j - 1) - AT(U4, i, j - 1), dx, rdx) - div_rn(AT(V4, i, j) - AT(V4, i, j - 1), dy, rdy);
+        a4 = -(div_rn(A * AT(hq, i + 1, j) * d4s1 - A * AT(hq, i, j) * d4s0, dx, rdx)
+               - div_rn(A * AT(sh, i, j) * d4t0 - A * AT(sh, i, j - 1) * d4tm, dy, rdy));
       }
-      rv = gM + gK + rq + ((hsouth != 0) ? (a2 + a4 + 0.0) / hsouth : 0);
+      rv = gM + gK + rq + ((hsouth != 0) ? div_rn(a2 + a4 + 0.0, hsouth, rhs) : 0);
     }
     // ---- diapycnal advection and viscosity (diapycnal.c:203-291) ----
     if (p.use_wdia || p.use_diavisc) {
@@ -415,8 +439,8 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         double dum = (wu1 > 0) ? uc - um : 0;
         double dvp = (wv0 > 0) ? 0 : vp - vc;
         double dvm = (wv1 > 0) ? vc - vm : 0;
-        if (hwest != 0) ru += (-(wu0 * dup + wu1 * dum)) / hwest;
-        if (hsouth != 0) rv += (-(wv0 * dvp + wv1 * dvm)) / hsouth;
+        if (hwest != 0) ru += div_rn(-(wu0 * dup + wu1 * dum), hwest, rhw);
+        if (hsouth != 0) rv += div_rn(-(wv0 * dvp + wv1 * dvm), hsouth, rhs);
       }
       if (p.use_diavisc && L >= 2) {
         double Fu[2] = {0, 0}, Fv[2] = {0, 0};
@@ -438,8 +462,8 @@ tendency_kernel(const __grid_constant__ TendParams p) {
           if (dzu != 0) Fu[s] = nuu * (ua - ub) / dzu;
           if (dzv != 0) Fv[s] = nuv * (va - vb) / dzv;
         }
-        if (hwest != 0) ru += (Fu[0] - Fu[1]) / hwest;
-        if (hsouth != 0) rv += (Fv[0] - Fv[1]) / hsouth;
+        if (hwest != 0) ru += div_rn(Fu[0] - Fu[1], hwest, rhw);
+        if (hsouth != 0) rv += div_rn(Fv[0] - Fv[1], hsouth, rhs);
       }
     }
     // ---- forcing and drag (forcing.c:245-393); hsml = hbbl = 0 fractions ----
@@ -454,30 +478,30 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         double tx_ = p.tw0 * p.taux0[cell] + p.tw1 * p.taux1[cell];
         double ty_ = p.tw0 * p.tauy0[cell] + p.tw1 * p.tauy1[cell];
         double r = tx_ * fsw;
-        if (hwest != 0) ru += r / hwest;
+        if (hwest != 0) ru += div_rn(r, hwest, rhw);
         r = ty_ * fss;
-        if (hsouth != 0) rv += r / hsouth;
+        if (hsouth != 0) rv += div_rn(r, hsouth, rhs);
       }
       if (p.use_fbaro) {
         ru += gload(p.fbx, p, gi, gj, MAP_N, MAP_S);
         rv += gload(p.fby, p, gi, gj, MAP_S, MAP_N);
       }
       if (p.lin_drag > 0) {
-        if (hwest != 0) ru += (-p.lin_drag * uc * fbw) / hwest;
-        if (hsouth != 0) rv += (-p.lin_drag * vc * fbs) / hsouth;
+        if (hwest != 0) ru += div_rn(-p.lin_drag * uc * fbw, hwest, rhw);
+        if (hsouth != 0) rv += div_rn(-p.lin_drag * vc * fbs, hsouth, rhs);
       }
       if (p.lin_drag_surf > 0) {
         if (hwest != 0) {
           double r = -p.lin_drag_surf * (uc - gload(p.uLid, p, gi, gj, MAP_N, MAP_S)) * fsw;
           double hsw = 0.5 * (gload(p.hhs, p, gi, gj, MAP_S, MAP_S) + gload(p.hhs, p, gi - 1, gj, MAP_S, MAP_S));
           if (!p.ocean_surf_drag && p.use_rl && hsw >= 0) r = 0;
-          ru += r / hwest;
+          ru += div_rn(r, hwest, rhw);
         }
         if (hsouth != 0) {
           double r = -p.lin_drag_surf * (vc - gload(p.vLid, p, gi, gj, MAP_S, MAP_N)) * fss;
           double hss = 0.5 * (gload(p.hhs, p, gi, gj, MAP_S, MAP_S) + gload(p.hhs, p, gi, gj - 1, MAP_S, MAP_S));
           if (!p.ocean_surf_drag && p.use_rl && hss >= 0) r = 0;
-          rv += r / hsouth;
+          rv += div_rn(r, hsouth, rhs);
         }
       }
     }
@@ -494,7 +518,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
     // ---- thickness tendency (work.c:1875-1885) ----
     double rh;
     {
-      double adv = (AT(huu, i, j) - AT(huu, i + 1, j)) / dx + (AT(hvv, i, j) - AT(hvv, i, j + 1)) / dy;
+      double adv = div_rn(AT(huu, i, j) - AT(huu, i + 1, j), dx, rdx) + div_rn(AT(hvv, i, j) - AT(hvv, i, j + 1), dy, rdy);
       double rel = 0;
       if (p.use_wdia) {
         const double* W0 = WDall + k * RN;

@@ -13,6 +13,7 @@ struct TendParams {
   int wall_ew, wall_ns;
   int use_rl;
   double dx, dy;
+  double rdx, rdy, r24;           // 1/dx, 1/dy, 1/24 rounded to nearest (for div_rn)
   // Adams-Bashforth epilogue. mode 0 writes the tendency itself to f_out.
   int ab_mode;                    // 0: tendency only, 1: AB1, 2: AB2, 3: AB3
   double c0, c1, c2;              // AB coefficients, computed on the host as the reference does

@@ -3,7 +3,8 @@
 SOR cases: the tendency after the preliminaries equals the reference's init_* dumps, and
 U/V/H/P after each of 3 steps plus every iteration count are bit-identical. Multigrid cases:
 the same quantities within the solver tolerance (the GPU smoother is red-black, the
-reference's lexicographic), iteration counts within a few V-cycles.
+reference's lexicographic; at the fixtures' tol of 1e-10 the states agree to better than 1e-6
+relative L2), iteration counts within a few V-cycles.
 """
 import numpy as np
 import pytest
@@ -29,7 +30,7 @@ def test_gpu_matches_reference_outputs(tmp_path, name):
             if sor:
                 assert value_equal(tend[v][k], ref), (tag, k)
             else:
-                assert rel_l2(tend[v][k], ref) < 1e-8, (tag, k)
+                assert rel_l2(tend[v][k], ref) < 1e-6, (tag, k)
     for n in range(1, 4):
         st = m.step(n)
         s = m.state()
@@ -43,7 +44,8 @@ def test_gpu_matches_reference_outputs(tmp_path, name):
                 if sor:
                     assert value_equal(s[v][k], ref), (n, v, k)
                 else:
-                    assert rel_l2(s[v][k], ref) < 1e-8, (n, v, k, rel_l2(s[v][k], ref))
+                    # both solves stop at max|pi - Jacobi(pi)| <= 1e-10 with different smoothers
+                    assert rel_l2(s[v][k], ref) < 1e-6, (n, v, k, rel_l2(s[v][k], ref))
         if sor:
             assert value_equal(m.get("pi"), z[f"P_{n}"]), n
         # the solve reaches at least the reference's residual quality

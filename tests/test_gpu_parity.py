@@ -75,3 +75,29 @@ def test_mg_steps_tolerance(tmp_path, oracle_mod, lib):
     s_o, s_g = o.state(), m.state()
     for var in ("u", "v", "h"):
         assert rel_l2(s_g[var], s_o[var]) < 1e-9, var
+
+
+@pytest.mark.parametrize("fp32", [0, 1], ids=["fp64", "fp32-defect"])
+@pytest.mark.parametrize("kind,kw", [
+    ("gyre", dict(N=128, solver=1, tol=1e-13, dt=900.0)),
+    ("channel", dict(Nx=128, Ny=64, solver=1, tol=1e-13, dt=150.0)),
+    ("jets", dict(N=64, solver=1, tol=1e-13, dt=100.0)),
+], ids=["gyre128", "channel128x64", "jets64"])
+def test_mg_tiled_levels_tolerance(tmp_path, oracle_mod, lib, fp32, kind, kw):
+    """Grids large enough for the tiled multigrid levels (above the one-CTA coarse block),
+    in FP64 and in FP32 V-cycles inside FP64 defect correction: 6 steps against the oracle's
+    serial multigrid at tol 1e-13."""
+    _, cfg, f = make_setup(tmp_path, kind, **kw)
+    o = oracle_mod.Oracle(cfg, f)
+    m = lib.Model(cfg, f, mg_fp32=fp32)
+    o.prelim()
+    m.prelim()
+    for n in range(1, 7):
+        o.integrator_step(n)
+        o.pressure(True)
+        st = m.step(n)
+        assert 1 <= st["iters"] < 80, st
+        assert st["stop_measure"] <= 1e-13
+    s_o, s_g = o.state(), m.state()
+    for var in ("u", "v", "h"):
+        assert rel_l2(s_g[var], s_o[var]) < 1e-9, (var, rel_l2(s_g[var], s_o[var]))
