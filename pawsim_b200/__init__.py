@@ -45,7 +45,7 @@ class GpuConfig(ctypes.Structure):
         "quad_drag_surf", "tau_period", "wdia_period", "conv_diff", "pi_tol", "sor_rp",
         "omega_mg")] + [("mg_fp32", ctypes.c_int), ("mg_pre", ctypes.c_int),
                         ("mg_post", ctypes.c_int), ("mg_omega", ctypes.c_double),
-                        ("serial_sums", ctypes.c_int)]
+                        ("serial_sums", ctypes.c_int), ("mg_tile", ctypes.c_int)]
 
 
 class GpuStats(ctypes.Structure):
@@ -138,6 +138,7 @@ def gpu_config(cfg: inputs.Config, **over) -> GpuConfig:
         setattr(g, a, float(v[b]))
     g.mg_fp32, g.mg_pre, g.mg_post, g.mg_omega = 0, 1, 1, 1.0
     g.serial_sums = -1
+    g.mg_tile = 0
     for k, val in over.items():
         setattr(g, k, val)
     return g

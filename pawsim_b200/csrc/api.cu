@@ -328,6 +328,7 @@ static int init(Model* m) {
     o.post = m->c.mg_post > 0 ? m->c.mg_post : 1;
     o.omega_rb = m->c.mg_omega > 0 ? m->c.mg_omega : 1.0;
     o.full_mg = m->c.use_full_mg;
+    o.tile_shape = m->c.mg_tile - 1;
     m->mg = new Multigrid(m->Nx, m->Ny, m->c.Lx, m->c.Ly, m->c.wall_ew, m->c.wall_ns, Hc.data(), o, m->s);
     if (!m->mg->ok()) return fail(PAWSIM_GPU_ECUDA, "multigrid allocation failed");
   }

@@ -28,17 +28,18 @@ struct LV {
   int Nx, Ny, pitch;
   const T *Ow, *Os, *Osum, *rOsum;
   T *e, *rhs, *res;
+  T* tmp;   // output of the fused down kernel, input of the fused up kernel
 };
 
 template <typename T>
 LV<T> view(const Multigrid::Level& l);
 template <>
 LV<double> view<double>(const Multigrid::Level& l) {
-  return LV<double>{l.Nx, l.Ny, l.pitch, l.Ow, l.Os, l.Osum, l.rOsum, l.e, l.rhs, l.res};
+  return LV<double>{l.Nx, l.Ny, l.pitch, l.Ow, l.Os, l.Osum, l.rOsum, l.e, l.rhs, l.res, l.tmp};
 }
 template <>
 LV<float> view<float>(const Multigrid::Level& l) {
-  return LV<float>{l.Nx, l.Ny, l.pitch, l.Ow32, l.Os32, l.Osum32, l.rOsum32, l.e32, l.rhs32, l.res32};
+  return LV<float>{l.Nx, l.Ny, l.pitch, l.Ow32, l.Os32, l.Osum32, l.rOsum32, l.e32, l.rhs32, l.res32, l.tmp32};
 }
 
 #define IX(l, i, j) ((size_t)(j) * (l).pitch + (i))
@@ -168,137 +169,330 @@ __global__ void prolong_correct_kernel(LV<T> f, LV<T> c, int power2, int wew, in
 
 // ---------------------------------------------------------------- fused tile kernels
 
-constexpr int BX = 32, BY = 8, BT = BX * BY;
-const dim3 TB(BX, BY);
+// max over the block (warp shuffles, then the warps' maxima), one atomic per block
+__device__ inline void block_max_to(double m, unsigned long long* bits) {
+  __shared__ double wm[32];
+  const int t = threadIdx.x + threadIdx.y * blockDim.x;
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((t & 31) == 0) wm[t >> 5] = m;
+  __syncthreads();
+  if (t == 0) {
+    const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+    double b = 0;
+    for (int w = 0; w < nw; ++w) b = fmax(b, wm[w]);
+    if (b > 0) atomicMax(bits, (unsigned long long)__double_as_longlong(b));
+  }
+}
 
-// smem tile of a level: raw coordinates [X0-H, X0+BX+H) x [Y0-H, Y0+BY+H), plus one more
-// column of Ow and one more row of Os (the east/north faces)
-template <int H>
-struct TileGeom {
-  static constexpr int W = BX + 2 * H, Hh = BY + 2 * H, N = W * Hh;
-  static constexpr int WO = W + 1, NO = WO * (Hh + 1);   // operator arrays
+// A CTA owns OX x OY cells at (X0, Y0) and keeps a shared-memory tile of e, rhs, 1/Osum,
+// Ow and Os over [X0-H, X0+OX+H) x [Y0-H, Y0+OY+H). In shared memory each array is split
+// into two planes by the parity of the tile column, so the cells of one colour along a
+// row are contiguous: a red-black half sweep gives each thread one cell of a (red, black)
+// pair and every shared access of a warp is stride 1. A half sweep at reach R updates the
+// cells of one colour within R of the owned block; R shrinks by one per half sweep, so
+// after the sweeps the owned cells (and, with one spare halo row, their neighbours) hold
+// what a global sweep would give. Tiles read their halo from the kernel's input array and
+// write their owned cells to a different output array, so no tile can see a neighbour's
+// result. The tile arrives by cp.async, straight from global to shared memory.
+__host__ __device__ constexpr int plane_pad(int n, int bytes) {
+  // the second plane starts half a 128-byte bank row after the first, so a half warp
+  // touching 8 cells of each plane (FP64) or a warp touching 16 of each (FP32) hits
+  // disjoint banks
+  while ((n * bytes) % 128 != 64) ++n;
+  return n;
+}
+
+template <typename T, int OX, int OY, int H>
+struct PT {
+  static constexpr int W = OX + 2 * H, Hh = OY + 2 * H, N = W * Hh;
+  static constexpr int PW = (W + 1) / 2, PL = plane_pad(PW * Hh, (int)sizeof(T)), ARR = 2 * PL;
+  // coarse cells read by the bilinear prolongation of the tile (fine H <= 3)
+  static constexpr int CW = OX / 2 + 4, CH = OY / 2 + 4, NC = CW * CH;
+  static constexpr int BUF = 5 * ARR + NC;   // elements of one tile buffer
+  __device__ static int at(int lx, int ly) { return (lx & 1) * PL + ly * PW + (lx >> 1); }
+  // east and west neighbours of the cell at index q in column parity s
+  __device__ static int east(int q, int s) { return q + (s ? 1 - PL : PL); }
+  __device__ static int west(int q, int s) { return q + (s ? -PL : PL - 1); }
 };
 
-template <typename T, int H>
-__device__ inline void load_tile(const LV<T>& l, int X0, int Y0, T* e, T* rhs, T* Ow, T* Os, T* rO,
-                                 bool zero_e) {
-  using G = TileGeom<H>;
-  // tiles whose halo (and the extra east/north face) lies inside the level load directly
-  const bool inner = X0 - H >= 0 && X0 + BX + H + 1 <= l.Nx && Y0 - H >= 0 && Y0 + BY + H + 1 <= l.Ny;
-  for (int ly = threadIdx.y; ly < G::Hh + 1; ly += BY)
-    for (int lx = threadIdx.x; lx < G::WO; lx += BX) {
-      int gi = X0 - H + lx, gj = Y0 - H + ly;
-      if (!inner) {
-        gi = wrapi(gi, l.Nx);
-        gj = wrapi(gj, l.Ny);
-      }
-      size_t g = IX(l, gi, gj);
-      int q = ly * G::WO + lx;
-      Ow[q] = l.Ow[g];
-      Os[q] = l.Os[g];
-      if (lx < G::W && ly < G::Hh) {
-        int p = ly * G::W + lx;
-        e[p] = zero_e ? T(0) : l.e[g];
-        rhs[p] = l.rhs[g];
-        rO[p] = l.rOsum[g];
-      }
-    }
+template <typename T, int OX, int OY, int H>
+constexpr size_t tile_bytes() {
+  return (size_t)PT<T, OX, OY, H>::BUF * sizeof(T);
 }
 
-// one red-black half sweep over tile cells within `reach` of the owned tile
-template <typename T, int H>
-__device__ inline void tile_half_sweep(int X0, int Y0, int color, int reach, T omega, T* e, const T* rhs,
-                                       const T* Ow, const T* Os, const T* rO) {
-  using G = TileGeom<H>;
-  const int par = (X0 + Y0 + color) & 1;   // (X0-H+lx + Y0-H+ly) & 1 == color, H*2 even
-  for (int ly = H - reach + threadIdx.y; ly < H + BY + reach; ly += BY)
-    for (int lx = H - reach + threadIdx.x; lx < H + BX + reach; lx += BX) {
-      if (((lx + ly) & 1) != par) continue;
-      int q = ly * G::W + lx, o = ly * G::WO + lx;
-      T s = Os[o + G::WO] * e[q + G::W] + Os[o] * e[q - G::W] + Ow[o + 1] * e[q + 1] + Ow[o] * e[q - 1];
-      e[q] = omega * rO[q] * (s - rhs[q]) + (T(1) - omega) * e[q];
-    }
+// interior tiles: halo, the prolongation's coarse cells and the wall-special cells all lie
+// inside the level, so loads need no wrap and the prolongation weights no wall cases
+template <int OX, int OY, int H>
+__device__ inline bool tile_inner(int X0, int Y0, int Nx, int Ny) {
+  constexpr int M = H + 1 > 4 ? H + 1 : 4;
+  return X0 >= M && X0 + OX + M <= Nx && Y0 >= M && Y0 + OY + M <= Ny;
 }
 
-// pre-smoothing, residual and 2x2 restriction into the coarse rhs (the coarse correction
-// starts from zero: the coarse kernels treat it as zero instead of reading it)
-template <typename T, int NU>
-__global__ void __launch_bounds__(BT) down_kernel(LV<T> f, LV<T> c, T omega, int zero_e) {
+template <typename T>
+__device__ inline void cp_async(T* dst, const T* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ inline void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <typename T, int OX, int OY, int H>
+struct TileBuf {
+  T *e, *rhs, *rO, *Ow, *Os, *ce;
+  __device__ explicit TileBuf(T* base) {
+    using G = PT<T, OX, OY, H>;
+    e = base;
+    rhs = e + G::ARR;
+    rO = rhs + G::ARR;
+    Ow = rO + G::ARR;
+    Os = Ow + G::ARR;
+    ce = Os + G::ARR;
+  }
+};
+
+// issue the asynchronous loads of one tile (and, for the up kernel, of its coarse cells)
+template <typename T, int OX, int OY, int H, int NT>
+__device__ inline void issue_tile(const LV<T>& l, const LV<T>& c, int X0, int Y0, bool zero_e, bool coarse,
+                                  const TileBuf<T, OX, OY, H>& b) {
+  using G = PT<T, OX, OY, H>;
+  const bool inner = tile_inner<OX, OY, H>(X0, Y0, l.Nx, l.Ny);
+  if (inner) {
+    const int base = (Y0 - H) * l.pitch + (X0 - H);
+    const T *pe = l.e + base, *pr = l.rhs + base, *po = l.rOsum + base, *pw = l.Ow + base, *ps = l.Os + base;
+    for (int k = threadIdx.x; k < G::N; k += NT) {
+      const int ly = k / G::W, lx = k - ly * G::W;
+      const int g = ly * l.pitch + lx, s = G::at(lx, ly);
+      if (zero_e) b.e[s] = T(0);
+      else cp_async(b.e + s, pe + g);
+      cp_async(b.rhs + s, pr + g);
+      cp_async(b.rO + s, po + g);
+      cp_async(b.Ow + s, pw + g);
+      cp_async(b.Os + s, ps + g);
+    }
+    if (coarse) {
+      const T* pc = c.e + ((Y0 / 2 - 2) * c.pitch + (X0 / 2 - 2));
+      for (int k = threadIdx.x; k < G::NC; k += NT) {
+        const int cy = k / G::CW, cx = k - cy * G::CW;
+        cp_async(b.ce + k, pc + cy * c.pitch + cx);
+      }
+    }
+  } else {
+    for (int k = threadIdx.x; k < G::N; k += NT) {
+      const int ly = k / G::W, lx = k - ly * G::W;
+      const size_t g = IX(l, wrapi(X0 - H + lx, l.Nx), wrapi(Y0 - H + ly, l.Ny));
+      const int s = G::at(lx, ly);
+      if (zero_e) b.e[s] = T(0);
+      else cp_async(b.e + s, l.e + g);
+      cp_async(b.rhs + s, l.rhs + g);
+      cp_async(b.rO + s, l.rOsum + g);
+      cp_async(b.Ow + s, l.Ow + g);
+      cp_async(b.Os + s, l.Os + g);
+    }
+  }
+  cp_async_commit();
+}
+
+// one red-black half sweep at reach R; par0 = colour + X0 + Y0
+template <typename T, int OX, int OY, int H, int NT, int R>
+__device__ inline void half_sweep(int par0, T omega, const TileBuf<T, OX, OY, H>& b) {
+  using G = PT<T, OX, OY, H>;
+  constexpr int hw = (OX + 2 * R) / 2, U = hw * (OY + 2 * R);
+#pragma unroll 2
+  for (int k = threadIdx.x; k < U; k += NT) {
+    const int row = k / hw, p = k - row * hw;
+    const int a = H - R + ((par0 + row) & 1);   // tile column = a + 2p
+    const int sp = a & 1;
+    const int q = sp * G::PL + (H - R + row) * G::PW + p + (a >> 1);
+    const int qe = G::east(q, sp), qw = G::west(q, sp);
+    T s = b.Os[q + G::PW] * b.e[q + G::PW] + b.Os[q] * b.e[q - G::PW] + b.Ow[qe] * b.e[qe] + b.Ow[q] * b.e[qw];
+    b.e[q] = omega * b.rO[q] * (s - b.rhs[q]) + (T(1) - omega) * b.e[q];
+  }
+}
+
+// NU red-black sweeps (red first), reach H-1 down to H-2NU
+template <typename T, int OX, int OY, int H, int NT, int NU, int S = 0>
+__device__ inline void tile_sweeps(int xy, T omega, const TileBuf<T, OX, OY, H>& b) {
+  if constexpr (S < NU) {
+    half_sweep<T, OX, OY, H, NT, H - (2 * S + 1)>(xy, omega, b);
+    __syncthreads();
+    half_sweep<T, OX, OY, H, NT, H - (2 * S + 2)>(xy + 1, omega, b);
+    __syncthreads();
+    tile_sweeps<T, OX, OY, H, NT, NU, S + 1>(xy, omega, b);
+  }
+}
+
+// pre-smoothing of f.e (or of zero) into `out`, residual and 2x2 restriction into the
+// coarse rhs (the coarse correction starts from zero: the coarse kernels never read it)
+template <typename T, int OX, int OY, int NT, int NU>
+__global__ void __launch_bounds__(NT) down_tile(LV<T> f, LV<T> c, T omega, int zero_e, T* __restrict__ out) {
   constexpr int H = 2 * NU + 1;
-  using G = TileGeom<H>;
-  extern __shared__ unsigned char sm_raw[];
-  T* e = reinterpret_cast<T*>(sm_raw);
-  T* rhs = e + G::N;
-  T* rO = rhs + G::N;
-  T* Ow = rO + G::N;
-  T* Os = Ow + G::NO;
-  const int X0 = blockIdx.x * BX, Y0 = blockIdx.y * BY;
-  load_tile<T, H>(f, X0, Y0, e, rhs, Ow, Os, rO, zero_e);
+  using G = PT<T, OX, OY, H>;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  const TileBuf<T, OX, OY, H> b(reinterpret_cast<T*>(sm_raw));
+  const int X0 = blockIdx.x * OX, Y0 = blockIdx.y * OY;
+  const bool inner = tile_inner<OX, OY, H>(X0, Y0, f.Nx, f.Ny);
+  issue_tile<T, OX, OY, H, NT>(f, c, X0, Y0, zero_e != 0, false, b);
+  cp_async_wait<0>();
   __syncthreads();
-  for (int s = 0; s < NU; ++s) {
-    tile_half_sweep<T, H>(X0, Y0, 0, H - (2 * s + 1), omega, e, rhs, Ow, Os, rO);
-    __syncthreads();
-    tile_half_sweep<T, H>(X0, Y0, 1, H - (2 * s + 2), omega, e, rhs, Ow, Os, rO);
-    __syncthreads();
+  tile_sweeps<T, OX, OY, H, NT, NU>(X0 + Y0, omega, b);
+  // write the smoothed owned cells and form their residuals (multigrid.c:604-623); the
+  // residuals go, split by column parity, where 1/Osum was (the residual does not read it)
+  T* res = b.rO;
+  constexpr int RP = plane_pad((OX / 2) * OY, (int)sizeof(T));
+  for (int k = threadIdx.x; k < OX * OY; k += NT) {
+    const int ly = k / OX, lx = k - ly * OX;
+    const int gi = X0 + lx, gj = Y0 + ly;
+    const int sp = (lx + H) & 1;
+    const int q = G::at(lx + H, ly + H), qe = G::east(q, sp), qw = G::west(q, sp);
+    T r = 0;
+    if (inner || (gi < f.Nx && gj < f.Ny)) {
+      const T ec = b.e[q];
+      out[IX(f, gi, gj)] = ec;
+      const T osum = b.Ow[q] + b.Ow[qe] + b.Os[q] + b.Os[q + G::PW];
+      const T s = b.Os[q + G::PW] * b.e[q + G::PW] + b.Os[q] * b.e[q - G::PW] + b.Ow[qe] * b.e[qe]
+                + b.Ow[q] * b.e[qw];
+      r = s - osum * ec - b.rhs[q];
+    }
+    res[(lx & 1) * RP + ly * (OX / 2) + (lx >> 1)] = r;
   }
-  // write the smoothed owned cells and form their residuals (multigrid.c:604-623)
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int lx = tx + H, ly = ty + H;
-  const int q = ly * G::W + lx, o = ly * G::WO + lx;
-  const int gi = X0 + tx, gj = Y0 + ty;
-  T r = 0;
-  if (gi < f.Nx && gj < f.Ny) {
-    T ec = e[q];
-    f.e[IX(f, gi, gj)] = ec;
-    T osum = Ow[o] + Ow[o + 1] + Os[o] + Os[o + G::WO];
-    T s = Os[o + G::WO] * e[q + G::W] + Os[o] * e[q - G::W] + Ow[o + 1] * e[q + 1] + Ow[o] * e[q - 1];
-    r = s - osum * ec - rhs[q];
-  }
-  __syncthreads();
-  T* res = rO;   // rOsum is no longer needed
-  res[ty * BX + tx] = r;
   __syncthreads();
   // restriction, order of restrict_power2_MG: (2i,2j) + (2i+1,2j) + (2i,2j+1) + (2i+1,2j+1)
-  const int t = ty * BX + tx;
-  if (t < (BX / 2) * (BY / 2)) {
-    int cx = t % (BX / 2), cy = t / (BX / 2);
-    int ic = X0 / 2 + cx, jc = Y0 / 2 + cy;
-    if (ic < c.Nx && jc < c.Ny) {
-      const T* rr = res + (2 * cy) * BX + 2 * cx;
-      c.rhs[IX(c, ic, jc)] = T(0.25) * (rr[0] + rr[1] + rr[BX] + rr[BX + 1]);
+  for (int k = threadIdx.x; k < (OX / 2) * (OY / 2); k += NT) {
+    const int cy = k / (OX / 2), cx = k - cy * (OX / 2);
+    const int ic = X0 / 2 + cx, jc = Y0 / 2 + cy;
+    if (inner || (ic < c.Nx && jc < c.Ny)) {
+      const T* r0 = res + (2 * cy) * (OX / 2) + cx;
+      c.rhs[IX(c, ic, jc)] = T(0.25) * (r0[0] + r0[RP] + r0[OX / 2] + r0[RP + OX / 2]);
     }
   }
 }
 
-// prolongation + correction over the tile and halo, then post-smoothing
-template <typename T, int NU>
-__global__ void __launch_bounds__(BT) up_kernel(LV<T> f, LV<T> c, T omega, int wew, int wns, int zero_e) {
-  constexpr int H = 2 * NU;
-  using G = TileGeom<H>;
-  extern __shared__ unsigned char sm_raw[];
-  T* e = reinterpret_cast<T*>(sm_raw);
-  T* rhs = e + G::N;
-  T* rO = rhs + G::N;
-  T* Ow = rO + G::N;
-  T* Os = Ow + G::NO;
-  const int X0 = blockIdx.x * BX, Y0 = blockIdx.y * BY;
-  load_tile<T, H>(f, X0, Y0, e, rhs, Ow, Os, rO, zero_e);
+// prolongation of the coarse correction c.e, correction of f.e and post-smoothing, into
+// `out`. With MEASURE the tile carries one more halo row and the kernel also folds
+// max |e - Jacobi(e)| over its owned cells into *bits: the stopping measure of the
+// finished V-cycle (multigrid.c:1123-1156).
+template <typename T, int OX, int OY, int NT, int NU, bool MEASURE>
+__global__ void __launch_bounds__(NT) up_tile(LV<T> f, LV<T> c, T omega, int wew, int wns,
+                                              unsigned long long* bits, T* __restrict__ out) {
+  constexpr int H = 2 * NU + (MEASURE ? 1 : 0);
+  using G = PT<T, OX, OY, H>;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  const TileBuf<T, OX, OY, H> b(reinterpret_cast<T*>(sm_raw));
+  const int X0 = blockIdx.x * OX, Y0 = blockIdx.y * OY;
+  const bool inner = tile_inner<OX, OY, H>(X0, Y0, f.Nx, f.Ny);
+  issue_tile<T, OX, OY, H, NT>(f, c, X0, Y0, false, true, b);
+  cp_async_wait<0>();
   __syncthreads();
-  auto ec = [&](int a, int b) { return c.e[IX(c, a, b)]; };
-  for (int ly = threadIdx.y; ly < G::Hh; ly += BY)
-    for (int lx = threadIdx.x; lx < G::W; lx += BX) {
-      int gi = wrapi(X0 - H + lx, f.Nx), gj = wrapi(Y0 - H + ly, f.Ny);
-      e[ly * G::W + lx] -= prolong_at<T>(gi, gj, f.Nx, f.Ny, c.Nx, c.Ny, true, wew, wns, ec);
+  if (inner) {
+    // interior cells: plain bilinear weights (multigrid.c:376-400) from the staged coarse cells
+#pragma unroll 2
+    for (int k = threadIdx.x; k < G::N; k += NT) {
+      const int ly = k / G::W, lx = k - ly * G::W;
+      const int cip = (lx + 5 - H) >> 1, cjp = (ly + 5 - H) >> 1;
+      const bool io = ((lx + H) & 1) != 0, jo = ((ly + H) & 1) != 0;
+      const T ai = io ? T(0.75) : T(0.25), bi = io ? T(0.25) : T(0.75);
+      const T aj = jo ? T(0.75) : T(0.25), bj = jo ? T(0.25) : T(0.75);
+      const T wmm = ai * aj, wmp = ai * bj, wpm = bi * aj, wpp = bi * bj;
+      const T* cc = b.ce + cjp * G::CW + cip;
+      b.e[G::at(lx, ly)] -= wmm * cc[-G::CW - 1] + wpm * cc[-G::CW] + wmp * cc[-1] + wpp * cc[0];
     }
-  __syncthreads();
-  for (int s = 0; s < NU; ++s) {
-    tile_half_sweep<T, H>(X0, Y0, 0, H - (2 * s + 1), omega, e, rhs, Ow, Os, rO);
-    __syncthreads();
-    tile_half_sweep<T, H>(X0, Y0, 1, H - (2 * s + 2), omega, e, rhs, Ow, Os, rO);
-    __syncthreads();
+  } else {
+    auto ec = [&](int a, int bb) { return c.e[IX(c, a, bb)]; };
+    for (int k = threadIdx.x; k < G::N; k += NT) {
+      const int ly = k / G::W, lx = k - ly * G::W;
+      const int gi = wrapi(X0 - H + lx, f.Nx), gj = wrapi(Y0 - H + ly, f.Ny);
+      b.e[G::at(lx, ly)] -= prolong_at<T>(gi, gj, f.Nx, f.Ny, c.Nx, c.Ny, true, wew, wns, ec);
+    }
   }
-  const int gi = X0 + threadIdx.x, gj = Y0 + threadIdx.y;
-  if (gi < f.Nx && gj < f.Ny) f.e[IX(f, gi, gj)] = e[(threadIdx.y + H) * G::W + threadIdx.x + H];
+  __syncthreads();
+  tile_sweeps<T, OX, OY, H, NT, NU>(X0 + Y0, omega, b);
+  double m = 0;
+  for (int k = threadIdx.x; k < OX * OY; k += NT) {
+    const int ly = k / OX, lx = k - ly * OX;
+    const int gi = X0 + lx, gj = Y0 + ly;
+    if (inner || (gi < f.Nx && gj < f.Ny)) {
+      const int q = G::at(lx + H, ly + H);
+      out[IX(f, gi, gj)] = b.e[q];
+      if constexpr (MEASURE) {
+        const int sp = (lx + H) & 1;
+        const int qe = G::east(q, sp), qw = G::west(q, sp);
+        const T s = b.Os[q + G::PW] * b.e[q + G::PW] + b.Os[q] * b.e[q - G::PW] + b.Ow[qe] * b.e[qe]
+                  + b.Ow[q] * b.e[qw];
+        const T r = b.e[q] - b.rO[q] * (s - b.rhs[q]);
+        m = fmax(m, fabs((double)r));
+      }
+    }
+  }
+  if constexpr (MEASURE) block_max_to(m, bits);
+}
+
+// tile shapes the autotuner chooses from (owned OX x OY cells, NT threads):
+// 0: 32x8/256, 1: 32x16/256, 2: 64x8/256, 3: 64x16/512
+constexpr int kNumTileShapes = 4;
+
+template <typename T, int OX, int OY, int NT>
+void set_tile_attrs() {
+  cudaFuncSetAttribute(down_tile<T, OX, OY, NT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)tile_bytes<T, OX, OY, 3>());
+  cudaFuncSetAttribute(up_tile<T, OX, OY, NT, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)tile_bytes<T, OX, OY, 2>());
+  cudaFuncSetAttribute(up_tile<T, OX, OY, NT, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)tile_bytes<T, OX, OY, 3>());
+}
+
+template <typename T, int OX, int OY, int NT>
+void launch_down_shape(const LV<T>& f, const LV<T>& c, T omega, int zero_e, T* out, cudaStream_t s) {
+  const dim3 grid((f.Nx + OX - 1) / OX, (f.Ny + OY - 1) / OY);
+  down_tile<T, OX, OY, NT, 1><<<grid, NT, tile_bytes<T, OX, OY, 3>(), s>>>(f, c, omega, zero_e, out);
+}
+
+template <typename T, int OX, int OY, int NT>
+void launch_up_shape(const LV<T>& f, const LV<T>& c, T omega, int wew, int wns, unsigned long long* bits,
+                     T* out, cudaStream_t s) {
+  const dim3 grid((f.Nx + OX - 1) / OX, (f.Ny + OY - 1) / OY);
+  if (bits)
+    up_tile<T, OX, OY, NT, 1, true><<<grid, NT, tile_bytes<T, OX, OY, 3>(), s>>>(f, c, omega, wew, wns, bits, out);
+  else
+    up_tile<T, OX, OY, NT, 1, false><<<grid, NT, tile_bytes<T, OX, OY, 2>(), s>>>(f, c, omega, wew, wns, bits, out);
+}
+
+template <typename T>
+void set_all_tile_attrs() {
+  set_tile_attrs<T, 32, 8, 256>();
+  set_tile_attrs<T, 32, 16, 256>();
+  set_tile_attrs<T, 64, 8, 256>();
+  set_tile_attrs<T, 64, 16, 512>();
+}
+
+template <typename T>
+void launch_down(int shape, const LV<T>& f, const LV<T>& c, T omega, int zero_e, T* out, cudaStream_t s) {
+  switch (shape) {
+    case 0: launch_down_shape<T, 32, 8, 256>(f, c, omega, zero_e, out, s); break;
+    case 1: launch_down_shape<T, 32, 16, 256>(f, c, omega, zero_e, out, s); break;
+    case 2: launch_down_shape<T, 64, 8, 256>(f, c, omega, zero_e, out, s); break;
+    default: launch_down_shape<T, 64, 16, 512>(f, c, omega, zero_e, out, s); break;
+  }
+}
+
+template <typename T>
+void launch_up(int shape, const LV<T>& f, const LV<T>& c, T omega, int wew, int wns, unsigned long long* bits,
+               T* out, cudaStream_t s) {
+  switch (shape) {
+    case 0: launch_up_shape<T, 32, 8, 256>(f, c, omega, wew, wns, bits, out, s); break;
+    case 1: launch_up_shape<T, 32, 16, 256>(f, c, omega, wew, wns, bits, out, s); break;
+    case 2: launch_up_shape<T, 64, 8, 256>(f, c, omega, wew, wns, bits, out, s); break;
+    default: launch_up_shape<T, 64, 16, 512>(f, c, omega, wew, wns, bits, out, s); break;
+  }
+}
+
+// a level runs the tile kernels when its transfer is exactly 2:1 (so every coloured
+// neighbour across a periodic wrap keeps its parity) and it holds the tile's halo
+inline bool tile_ok(int Nx, int Ny, bool power2, int pre, int post) {
+  return power2 && pre == 1 && post == 1 && Nx >= 8 && Ny >= 8;
 }
 
 // ---------------------------------------------------------------- coarse levels in one CTA
@@ -418,21 +612,6 @@ __global__ void __launch_bounds__(CT) coarse_kernel(const __grid_constant__ Coar
 
 // ---------------------------------------------------------------- stopping test and loop control
 
-// max over the block (warp shuffles, then the warps' maxima), one atomic per block
-__device__ inline void block_max_to(double m, unsigned long long* bits) {
-  __shared__ double wm[32];
-  const int t = threadIdx.x + threadIdx.y * blockDim.x;
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
-  if ((t & 31) == 0) wm[t >> 5] = m;
-  __syncthreads();
-  if (t == 0) {
-    const int nw = (blockDim.x * blockDim.y + 31) >> 5;
-    double b = 0;
-    for (int w = 0; w < nw; ++w) b = fmax(b, wm[w]);
-    if (b > 0) atomicMax(bits, (unsigned long long)__double_as_longlong(b));
-  }
-}
-
 struct LoopState {
   unsigned long long bits;   // max |pi - Jacobi(pi)| as an integer bit pattern
   int iters;
@@ -548,11 +727,6 @@ void host_restrict(int fnx, int fny, const std::vector<double>& f, int cnx, int 
   }
 }
 
-template <typename T, int H>
-size_t tile_smem() {
-  using G = TileGeom<H>;
-  return (size_t)(3 * G::N + 2 * G::NO) * sizeof(T);
-}
 
 }  // namespace
 
@@ -648,6 +822,8 @@ Multigrid::Multigrid(int Nx, int Ny, double Lx, double Ly, bool wew, bool wns, c
       cudaMemcpy(*dst32[a], buf32.data(), np * sizeof(float), cudaMemcpyHostToDevice);
     }
     L.e = dalloc<double>(np); L.rhs = dalloc<double>(np); L.res = dalloc<double>(np);
+    L.tmp = dalloc<double>(np); L.tmp32 = dalloc<float>(np);
+    good = good && L.tmp && L.tmp32;
     L.e32 = dalloc<float>(np); L.rhs32 = dalloc<float>(np); L.res32 = dalloc<float>(np);
     good = good && L.e && L.rhs && L.res && L.e32 && L.rhs32 && L.res32;
   }
@@ -665,6 +841,8 @@ Multigrid::Multigrid(int Nx, int Ny, double Lx, double Ly, bool wew, bool wns, c
   ok_ = good;
   cudaFuncSetAttribute(coarse_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(coarse_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  set_all_tile_attrs<double>();
+  set_all_tile_attrs<float>();
 }
 
 Multigrid::~Multigrid() {
@@ -681,27 +859,26 @@ Multigrid::~Multigrid() {
   for (auto& L : lv_) {
     cudaFree(L.Ow); cudaFree(L.Os); cudaFree(L.Osum); cudaFree(L.rOsum);
     cudaFree(L.Ow32); cudaFree(L.Os32); cudaFree(L.Osum32); cudaFree(L.rOsum32);
-    cudaFree(L.e); cudaFree(L.rhs); cudaFree(L.res);
+    cudaFree(L.e); cudaFree(L.rhs); cudaFree(L.res); cudaFree(L.tmp); cudaFree(L.tmp32);
     cudaFree(L.e32); cudaFree(L.rhs32); cudaFree(L.res32);
   }
   cudaFree(dstate_);
 }
 
 template <typename T>
-void Multigrid::enqueue_vcycle(cudaStream_t s) {
+void Multigrid::enqueue_vcycle(cudaStream_t s, unsigned long long* measure_bits) {
   const int top = (int)lv_.size() - 1;
   const T omega = (T)opt_.omega_rb;
   const int pre = opt_.pre, post = opt_.post;
+  bool measured = false;
   // down through the tiled levels
   for (int n = top; n > ctop_; --n) {
     Level& F = lv_[n];
     LV<T> f = view<T>(F), c = view<T>(lv_[n - 1]);
     // coarse corrections, and the FP32 correction of the defect loop, start from zero
     bool zero_e = (n != top) || (sizeof(T) == 4);
-    bool fused = F.power2 && F.Nx >= BX && F.Ny >= BY && pre == 1;
-    if (fused) {
-      down_kernel<T, 1><<<dim3((F.Nx + BX - 1) / BX, (F.Ny + BY - 1) / BY), TB, tile_smem<T, 3>(), s>>>(
-          f, c, omega, zero_e ? 1 : 0);
+    if (tile_ok(F.Nx, F.Ny, F.power2, pre, post)) {
+      launch_down<T>(sizeof(T) == 8 ? F.shape64 : F.shape32, f, c, omega, zero_e ? 1 : 0, f.tmp, s);
       ++g_launches;
     } else {
       if (zero_e) cudaMemsetAsync(f.e, 0, (size_t)F.pitch * F.Ny * sizeof(T), s);
@@ -739,15 +916,17 @@ void Multigrid::enqueue_vcycle(cudaStream_t s) {
     coarse_kernel<T><<<1, CT, shm, s>>>(d, omega);
     ++g_launches;
   }
-  // up through the tiled levels
+  // up through the tiled levels; the finest FP64 up kernel also forms the stopping measure
   for (int n = ctop_ + 1; n <= top; ++n) {
     Level& F = lv_[n];
     LV<T> f = view<T>(F), c = view<T>(lv_[n - 1]);
-    bool fused = F.power2 && F.Nx >= BX && F.Ny >= BY && post == 1;
-    if (fused) {
-      up_kernel<T, 1><<<dim3((F.Nx + BX - 1) / BX, (F.Ny + BY - 1) / BY), TB, tile_smem<T, 2>(), s>>>(
-          f, c, omega, wew_, wns_, 0);
+    if (tile_ok(F.Nx, F.Ny, F.power2, pre, post)) {
+      unsigned long long* mb = (n == top) ? measure_bits : nullptr;
+      LV<T> fin = f;
+      fin.e = f.tmp;   // the pre-smoothed correction written by the down kernel
+      launch_up<T>(sizeof(T) == 8 ? F.shape64 : F.shape32, fin, c, omega, wew_, wns_, mb, f.e, s);
       ++g_launches;
+      if (mb) measured = true;
     } else {
       prolong_correct_kernel<T><<<g2(f.Nx, f.Ny), B2, 0, s>>>(f, c, F.power2 ? 1 : 0, wew_, wns_);
       for (int q = 0; q < post; ++q) {
@@ -757,6 +936,61 @@ void Multigrid::enqueue_vcycle(cudaStream_t s) {
       g_launches += 1 + 2 * post;
     }
   }
+  if (measure_bits && !measured) {
+    LV<double> f = view<double>(lv_.back());
+    max_residual_kernel<<<g2(f.Nx, f.Ny), B2, 0, s>>>(f, measure_bits);
+    ++g_launches;
+  }
+}
+
+// Choose the tile shape of every tiled level by timing each shape's down and up kernels
+// on that level. The runs read and write the level's scratch arrays only (the finest
+// level's output goes to its `res` array), never the caller's pi. The choice only
+// affects speed: every shape gives the same values.
+template <typename T>
+void Multigrid::tune(cudaStream_t s) {
+  const int top = (int)lv_.size() - 1;
+  LoopState* st = reinterpret_cast<LoopState*>(dstate_);
+  cudaEvent_t ev[2];
+  cudaEventCreate(&ev[0]);
+  cudaEventCreate(&ev[1]);
+  const long long counted = g_launches;
+  for (int n = ctop_ + 1; n <= top; ++n) {
+    Level& F = lv_[n];
+    bool& tuned = sizeof(T) == 8 ? F.tuned64 : F.tuned32;
+    int& shape = sizeof(T) == 8 ? F.shape64 : F.shape32;
+    if (tuned) continue;
+    tuned = true;
+    if (opt_.tile_shape >= 0) {
+      shape = opt_.tile_shape < kNumTileShapes ? opt_.tile_shape : kNumTileShapes - 1;
+      continue;
+    }
+    if (!tile_ok(F.Nx, F.Ny, F.power2, opt_.pre, opt_.post)) continue;
+    LV<T> f = view<T>(F), c = view<T>(lv_[n - 1]);
+    LV<T> fin = f;
+    fin.e = f.tmp;
+    T* out = f.res;
+    unsigned long long* mb = (n == top && sizeof(T) == 8) ? &st->bits : nullptr;
+    float best = 1e30f;
+    for (int k = 0; k < kNumTileShapes; ++k) {
+      float ms = 0;
+      for (int rep = 0; rep < 4; ++rep) {
+        if (rep == 1) cudaEventRecord(ev[0], s);
+        launch_down<T>(k, f, c, (T)opt_.omega_rb, 1, f.tmp, s);
+        launch_up<T>(k, fin, c, (T)opt_.omega_rb, wew_, wns_, mb, out, s);
+      }
+      cudaEventRecord(ev[1], s);
+      if (cudaEventSynchronize(ev[1]) != cudaSuccess) break;
+      cudaEventElapsedTime(&ms, ev[0], ev[1]);
+      if (ms < best) {
+        best = ms;
+        shape = k;
+      }
+    }
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  g_launches = counted;   // tuning runs are not steps of the solve
 }
 
 void Multigrid::set_fine(double* pi, const double* rhs) {
@@ -784,16 +1018,15 @@ int Multigrid::build_graph(int prec) {
     return -1;
   Level& F = lv_.back();
   if (prec == 0) {
-    enqueue_vcycle<double>(cap_);
-    LV<double> f = view<double>(F);
-    max_residual_kernel<<<g2(f.Nx, f.Ny), B2, 0, cap_>>>(f, &st->bits);
+    enqueue_vcycle<double>(cap_, &st->bits);
   } else {
-    enqueue_vcycle<float>(cap_);
+    enqueue_vcycle<float>(cap_, nullptr);
     LV<double> f = view<double>(F);
     defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, cap_>>>(f, F.e32, F.pitch, F.rhs32, F.res, 1, &st->bits);
     commit_kernel<<<g2(f.Nx, f.Ny), B2, 0, cap_>>>(F.e, F.res, F.Nx, F.Ny, F.pitch);
   }
   loop_finalize_kernel<<<1, 1, 0, cap_>>>(st, g_->handle[prec]);
+  body_launches_[prec] = (int)(g_launches - counted) + (prec ? 3 : 1);   // + defect, commit, finalize
   g_launches = counted;
   if (cudaStreamEndCapture(cap_, &body) != cudaSuccess) return -1;
   if (cudaGraphInstantiate(&g_->exec[prec], G, 0) != cudaSuccess) return -1;
@@ -836,6 +1069,8 @@ int Multigrid::solve(double* pi, int pitch, const double* rhs, int rhs_pitch, do
   }
   set_fine(pi, rhs);
   LoopState* st = reinterpret_cast<LoopState*>(dstate_);
+  if (prec == 0) tune<double>(s_);
+  else tune<float>(s_);
   if (getenv("PAWSIM_MG_HOST_LOOP")) {
     // host-driven loop with the same kernels (for profilers that do not see inside the
     // conditional graph node)
@@ -850,10 +1085,9 @@ int Multigrid::solve(double* pi, int pitch, const double* rhs, int rhs_pitch, do
     while (mres > tol && it < maxiters) {
       cudaMemsetAsync(&st->bits, 0, sizeof(unsigned long long), s_);
       if (prec == 0) {
-        enqueue_vcycle<double>(s_);
-        max_residual_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f, &st->bits);
+        enqueue_vcycle<double>(s_, &st->bits);
       } else {
-        enqueue_vcycle<float>(s_);
+        enqueue_vcycle<float>(s_, nullptr);
         defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f, F.e32, F.pitch, F.rhs32, F.res, 1, &st->bits);
         commit_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(F.e, F.res, F.Nx, F.Ny, F.pitch);
       }
@@ -881,23 +1115,12 @@ int Multigrid::solve(double* pi, int pitch, const double* rhs, int rhs_pitch, do
   cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s_);
   if (cudaStreamSynchronize(s_) != cudaSuccess) return -1;
   // kernels of the graph body, counted once per executed V-cycle
-  g_launches += (long long)h.iters * body_launches(prec);
+  g_launches += (long long)h.iters * body_launches_[prec];
   if (maxres_out) *maxres_out = h.maxres;
   return h.iters;
 }
 
-int Multigrid::body_launches(int prec) const {
-  const int top = (int)lv_.size() - 1;
-  int k = 0;
-  for (int n = top; n > ctop_; --n) {
-    const Level& F = lv_[n];
-    bool fused = F.power2 && F.Nx >= BX && F.Ny >= BY;
-    k += fused ? 2 : (2 * opt_.pre + 2) + (1 + 2 * opt_.post);
-  }
-  return k + 1 + (prec ? 3 : 2);
-}
-
-template void Multigrid::enqueue_vcycle<double>(cudaStream_t);
-template void Multigrid::enqueue_vcycle<float>(cudaStream_t);
+template void Multigrid::enqueue_vcycle<double>(cudaStream_t, unsigned long long*);
+template void Multigrid::enqueue_vcycle<float>(cudaStream_t, unsigned long long*);
 
 }  // namespace pawsim

@@ -22,6 +22,7 @@ struct MGOptions {
   int pre = 1, post = 1;   // red-black sweeps before and after the coarse correction
   double omega_rb = 1.0;   // smoother weight
   int full_mg = 0;         // use_fullMG: nested iteration from the coarsest level
+  int tile_shape = -1;     // fused level kernels: -1 autotune per level, 0..3 force a shape
 };
 
 class Multigrid {
@@ -50,13 +51,18 @@ class Multigrid {
     float *Ow32, *Os32, *Osum32, *rOsum32;
     double *e, *rhs, *res;              // FP64 work
     float *e32, *rhs32, *res32;         // FP32 work
+    double* tmp = nullptr;              // fused down kernel output / up kernel input
+    float* tmp32 = nullptr;
+    int shape64 = 0, shape32 = 0;       // tile shape of the fused kernels per precision
+    bool tuned64 = false, tuned32 = false;
   };
 
  private:
-  template <typename T> void enqueue_vcycle(cudaStream_t s);
+  template <typename T> void enqueue_vcycle(cudaStream_t s, unsigned long long* measure_bits);
+  template <typename T> void tune(cudaStream_t s);
   void set_fine(double* pi, const double* rhs);
   int build_graph(int prec);
-  int body_launches(int prec) const;
+  int body_launches_[2] = {0, 0};   // kernels per executed V-cycle of each graph body
   struct Graphs;
   bool ok_ = false;
   int Nx_, Ny_;

@@ -20,7 +20,7 @@ __device__ inline double ld_s(const double* f, const Grid2& g, int i, int j) {
 // Gathered face thickness with wrapped indices (work.c:865-1030), at an owned cell.
 __device__ inline double hw_gathered(const Grid2& g, const double* h, int i, int j) {
   int Nx = g.Nx, Ny = g.Ny;
-  int im1 = i == 0 ? Nx - 1 : i - 1, ip1 = i + 1 == Nx ? 0 : i + 1;
+  int im1 = i == 0 ? Nx - 1 : i - 1;
   int jm1 = j == 0 ? Ny - 1 : j - 1, jp1 = j + 1 == Ny ? 0 : j + 1;
   const int P = g.pitch;
 #define H(ii, jj) h[(size_t)(jj) * P + (ii)]
@@ -31,7 +31,6 @@ __device__ inline double hw_gathered(const Grid2& g, const double* h, int i, int
       return (1.0 / 3) * (1.25 * (H(i, j) + H(im1, j)) + 0.25 * (H(i, jm1) + H(im1, jm1)));
     return (1.0 / 3) * (H(i, j) + H(im1, j) + 0.25 * (H(i, jp1) + H(im1, jp1) + H(i, jm1) + H(im1, jm1)));
   }
-  (void)ip1;
   return 0.5 * (H(i, j) + H(im1, j));
 }
 

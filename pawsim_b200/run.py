@@ -1,7 +1,8 @@
 """Run a seeded synthetic set-up through the library (quick runs, profiling, timing).
 
     python -m pawsim_b200.run --setup gyre --N 1024 --steps 4 [--integrator-only]
-                              [--solver 0|1] [--mg-fp32] [--dt 60] [--param FILE]
+                              [--solver 0|1] [--mg-fp32] [--mg-tile K] [--mg-omega W]
+                              [--mg-pre P] [--mg-post Q] [--dt 60] [--param FILE]
 
 ``--integrator-only`` advances with ``pawsim_gpu_integrator_step`` alone (one fused tendency
 kernel per step, no pressure correction), which isolates the tendency kernel for a profiler.
@@ -29,6 +30,10 @@ def main(argv=None):
     ap.add_argument("--dt", type=float, default=None)
     ap.add_argument("--solver", type=int, default=1)
     ap.add_argument("--mg-fp32", action="store_true")
+    ap.add_argument("--mg-tile", type=int, default=0, help="0 autotune, 1..4 force a tile shape")
+    ap.add_argument("--mg-omega", type=float, default=1.0)
+    ap.add_argument("--mg-pre", type=int, default=1)
+    ap.add_argument("--mg-post", type=int, default=1)
     ap.add_argument("--integrator-only", action="store_true")
     a = ap.parse_args(argv)
     with tempfile.TemporaryDirectory() as d:
@@ -45,7 +50,8 @@ def main(argv=None):
             elif a.setup == "gyre":
                 kw["dt"] = 60.0 * 2048 / a.N if a.N <= 2048 else 60.0
             cfg = inputs.read_config(SETUPS[a.setup](d, **kw))
-        m = Model(cfg, mg_fp32=int(a.mg_fp32))
+        m = Model(cfg, mg_fp32=int(a.mg_fp32), mg_tile=a.mg_tile, mg_omega=a.mg_omega, mg_pre=a.mg_pre,
+                  mg_post=a.mg_post)
         t0 = time.perf_counter()
         if a.integrator_only:
             for n in range(1, a.steps + 1):
@@ -55,8 +61,11 @@ def main(argv=None):
         else:
             m.prelim()
             rep = {}
+            iters = []
             for n in range(1, a.steps + 1):
                 rep = m.step(n)
+                iters.append(rep["iters"])
+            rep["iters_per_step"] = iters
         m.synchronize()
         dt = time.perf_counter() - t0
         print(json.dumps({"setup": a.param or a.setup, "N": [cfg.Nx, cfg.Ny, cfg.Nlay], "steps": a.steps,

@@ -101,3 +101,28 @@ def test_mg_tiled_levels_tolerance(tmp_path, oracle_mod, lib, fp32, kind, kw):
     s_o, s_g = o.state(), m.state()
     for var in ("u", "v", "h"):
         assert rel_l2(s_g[var], s_o[var]) < 1e-9, (var, rel_l2(s_g[var], s_o[var]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fp32", [0, 1], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("kind,kw", [
+    ("gyre", dict(N=256, solver=1, tol=1e-12, dt=450.0)),
+    ("channel", dict(Nx=256, Ny=128, solver=1, tol=1e-12, dt=150.0)),
+    ("gyre", dict(N=1024, solver=1, tol=1e-11, dt=120.0)),
+], ids=["gyre256", "channel256x128", "gyre1024"])
+def test_mg_tile_shapes_identical(tmp_path, lib, fp32, kind, kw):
+    """Every tile shape of the fused multigrid level kernels, and the autotuned choice,
+    gives bit-identical states and iteration counts: the shape changes only the speed.
+    At 1024^2 every CTA of the persistent kernels walks several tiles."""
+    _, cfg, f = make_setup(tmp_path, kind, **kw)
+    runs = []
+    for tile in (0, 1, 2, 3, 4):
+        m = lib.Model(cfg, f, mg_fp32=fp32, mg_tile=tile)
+        m.prelim()
+        iters = [m.step(n)["iters"] for n in range(1, 5)]
+        runs.append((tile, iters, m.state()))
+    _, iters0, s0 = runs[1]
+    for tile, iters, s in runs:
+        assert iters == iters0, (tile, iters, iters0)
+        for var in ("u", "v", "h"):
+            assert np.array_equal(s[var], s0[var]), (tile, var)
