@@ -135,6 +135,20 @@ PAWSIM_API const char * pawsim_gpu_last_error (void);
  * n host values x / d; *bad receives the number of results that differ in any bit. */
 PAWSIM_API int pawsim_gpu_check_division (const double * x, size_t n, double d, long long * bad);
 
+/* ---- Learned pressure warm start: network building blocks (no reference counterpart).
+ * Device pointers; activations NHWC bf16 with C in {16, 32, 48, 64}; weights [Cout][3][3][Cin]
+ * bf16; dev_err (nullable) is a device int set to 1 when a bounded wait inside a kernel
+ * gave up. Convolutions run on the tcgen05 tensor cores with FP32 accumulation. */
+PAWSIM_API int pawsim_nn_conv3x3 (const void * in_bf16, int B, int H, int W, int Cin, const void * w_bf16,
+                                  const float * bias, int Cout, int relu, void * out_bf16, float * out_f32,
+                                  int * dev_err, void * stream);
+/* dw[co][ky][kx][ci] += sum_p dout[p][co] in[p shifted][ci]; db[co] += sum_p dout[p][co] (FP32) */
+PAWSIM_API int pawsim_nn_conv3x3_wgrad (const void * in_bf16, const void * dout_bf16, int B, int H, int W,
+                                        int Cin, int Cout, float * dw, float * db, int * dev_err,
+                                        void * stream);
+/* w_t[ci][ky][kx][co] = w[co][2-ky][2-kx][ci]: input-gradient weights of a convolution */
+PAWSIM_API int pawsim_nn_flip_weights (const void * w_bf16, int Cout, int Cin, void * w_t_bf16, void * stream);
+
 /* No counterpart in the reference. For callers that cannot allocate device memory (code
  * running under an allocator or memory pool it does not own, hosts that forbid device
  * allocation after start-up): builds the rigid-lid right-hand side, sum_k div(h_k u_k)/dt

@@ -64,6 +64,7 @@ EXPORTS = (
     "pawsim_gpu_pressure_correct", "pawsim_gpu_prelim", "pawsim_gpu_step", "pawsim_gpu_run",
     "pawsim_gpu_solve_mg", "pawsim_gpu_set_stream", "pawsim_gpu_synchronize",
     "pawsim_gpu_time", "pawsim_gpu_launch_count", "pawsim_gpu_last_error",
+    "pawsim_nn_conv3x3", "pawsim_nn_conv3x3_wgrad", "pawsim_nn_flip_weights",
 )
 
 _LIB = None
@@ -98,6 +99,10 @@ def load_library(path: str = LIB_PATH):
     lib.pawsim_gpu_time.restype = ctypes.c_double
     lib.pawsim_gpu_launch_count.argtypes = [P]
     lib.pawsim_gpu_launch_count.restype = ctypes.c_longlong
+    I, F = ctypes.c_int, ctypes.POINTER(ctypes.c_float)
+    lib.pawsim_nn_conv3x3.argtypes = [P, I, I, I, I, P, P, I, I, P, P, P, P]
+    lib.pawsim_nn_conv3x3_wgrad.argtypes = [P, P, I, I, I, I, I, P, P, P, P]
+    lib.pawsim_nn_flip_weights.argtypes = [P, I, I, P, P]
     lib.pawsim_gpu_last_error.argtypes = []
     lib.pawsim_gpu_last_error.restype = ctypes.c_char_p
     _LIB = lib
