@@ -90,7 +90,9 @@ typedef struct pawsim_gpu_stats
   double residual_max, residual_rms;   /* rhs - L(pi), pressure.c:652-690 (pressure_timing) */
   double div_max, div_rms;             /* sum_k div(h u) after projection, pressure.c:693-737 */
   double stop_measure;       /* value of the solver's own stopping test at exit */
-  double solve_ms;           /* device time of the solve alone */
+  double solve_ms;           /* device time of the solve alone (with the warm start's guess) */
+  int warm_start;            /* learned warm start: 0 none, 1 guess used, 2 guess rejected
+                                (the solve started from the previous pressure) */
 } pawsim_gpu_stats;
 
 typedef struct pawsim_gpu pawsim_gpu;
@@ -148,6 +150,38 @@ PAWSIM_API int pawsim_nn_conv3x3_wgrad (const void * in_bf16, const void * dout_
                                         void * stream);
 /* w_t[ci][ky][kx][co] = w[co][2-ky][2-kx][ci]: input-gradient weights of a convolution */
 PAWSIM_API int pawsim_nn_flip_weights (const void * w_bf16, int Cout, int Cin, void * w_t_bf16, void * stream);
+
+/* ---- Learned warm start of a model's multigrid solve (no reference counterpart).
+ * mode bit 0: after every solve, store a training pair (network inputs and the solved
+ * correction) in a device ring of max_pairs pairs; bit 1: start each solve from the trained
+ * network's guess when its stopping measure is below that of the previous pressure.
+ * batch: training batch size. Needs the multigrid solver and a grid whose side, coarsened
+ * to at most 512 cells, is a multiple of 8. The first call allocates; later calls change
+ * the mode only. */
+PAWSIM_API int pawsim_gpu_nn_setup (pawsim_gpu * m, int mode, int max_pairs, int batch,
+                                    unsigned long long seed);
+/* Adam (learning rate lr) over the collected pairs for `epochs` passes; *loss receives the
+ * last epoch's mean squared error of the normalised correction. */
+PAWSIM_API int pawsim_gpu_nn_train (pawsim_gpu * m, int epochs, float lr, double * loss);
+PAWSIM_API int pawsim_gpu_nn_pairs (pawsim_gpu * m);
+/* the model's network (owned by the model: do not destroy), for pawsim_nn_net_* below */
+PAWSIM_API void * pawsim_gpu_nn_net (pawsim_gpu * m);
+
+/* A standalone warm-start network on an H x W grid (multiples of 8) for batches of at most
+ * Bmax: parameters flattened per layer as w[Cout][3][3][Cin] then b[Cout] (FP32 master
+ * copy; the kernels use its bf16 rounding). forward/backward take device inputs
+ * (B, H, W, 16) bf16; forward copies output channel 0 (B, H, W) to the host; backward
+ * recomputes the loss mean((out0 - target)^2) and all parameter gradients. */
+PAWSIM_API int pawsim_nn_net_create (int H, int W, int Bmax, unsigned long long seed, void ** net);
+PAWSIM_API void pawsim_nn_net_destroy (void * net);
+PAWSIM_API long long pawsim_nn_net_param_count (void * net);
+PAWSIM_API int pawsim_nn_net_get_params (void * net, float * host, size_t n);
+PAWSIM_API int pawsim_nn_net_set_params (void * net, const float * host, size_t n);
+PAWSIM_API int pawsim_nn_net_get_grads (void * net, float * host, size_t n);
+PAWSIM_API int pawsim_nn_net_forward (void * net, const void * in_bf16, int B, float * out_host);
+PAWSIM_API int pawsim_nn_net_backward (void * net, const void * in_bf16, const float * target, int B,
+                                       double * loss);
+PAWSIM_API int pawsim_nn_net_adam (void * net, float lr);
 
 /* No counterpart in the reference. For callers that cannot allocate device memory (code
  * running under an allocator or memory pool it does not own, hosts that forbid device

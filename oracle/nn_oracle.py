@@ -73,3 +73,116 @@ def flip(w):
 def conv3x3_dgrad(dout, w):
     """Gradient with respect to the input of conv3x3(x, w)."""
     return conv3x3(dout, flip(w))
+
+
+# ---------------------------------------------------------------- the warm-start network
+
+LAYERS = [(16, 32, 0, True), (32, 32, 0, True), (32, 64, 1, True), (64, 64, 1, True), (64, 64, 2, True),
+          (64, 64, 3, True), (64, 64, 2, True), (64, 32, 1, True), (32, 32, 0, True), (32, 16, 0, False)]
+
+
+def param_count():
+    return sum(co * 9 * ci + co for ci, co, _, _ in LAYERS)
+
+
+def unflatten(p):
+    """Flat parameters (per layer w[Cout][3][3][Cin] then b[Cout]) -> [(w, b), ...]."""
+    out, o = [], 0
+    p = np.asarray(p, dtype=np.float64)
+    for ci, co, _, _ in LAYERS:
+        w = p[o:o + co * 9 * ci].reshape(co, 3, 3, ci)
+        o += co * 9 * ci
+        out.append((w, p[o:o + co]))
+        o += co
+    return out
+
+
+def flatten(pairs):
+    return np.concatenate([np.concatenate([w.ravel(), b.ravel()]) for w, b in pairs])
+
+
+def _pool(x):
+    return 0.25 * (((x[:, 0::2, 0::2] + x[:, 0::2, 1::2]) + x[:, 1::2, 0::2]) + x[:, 1::2, 1::2])
+
+
+def _up(x):
+    return np.repeat(np.repeat(x, 2, axis=1), 2, axis=2)
+
+
+def _pool_sum(x):
+    return ((x[:, 0::2, 0::2] + x[:, 0::2, 1::2]) + x[:, 1::2, 0::2]) + x[:, 1::2, 1::2]
+
+
+def _f32(x):
+    return np.asarray(x, dtype=np.float32).astype(np.float64)
+
+
+def net_forward(params, x, quant=True):
+    """Forward pass of the warm-start network on x (B, H, W, 16). Returns (out0, cache).
+
+    With quant the weights, every stored activation and the pooled/upsampled sums are
+    rounded to bf16 and the output to FP32, as on the GPU."""
+    q = bf16 if quant else (lambda a: np.asarray(a, dtype=np.float64))
+    f = _f32 if quant else (lambda a: np.asarray(a, dtype=np.float64))
+    ws = [(q(w), f(b)) for w, b in unflatten(params)]
+
+    def conv(l, inp):
+        w, b = ws[l]
+        y = conv3x3(inp, w, b, relu=LAYERS[l][3])
+        return q(y) if l < 9 else f(y)
+
+    A = [None] * 10
+    x = q(x)
+    A[0] = conv(0, x)
+    A[1] = conv(1, A[0])
+    P1 = q(_pool(A[1]))
+    A[2] = conv(2, P1)
+    A[3] = conv(3, A[2])
+    P2 = q(_pool(A[3]))
+    A[4] = conv(4, P2)
+    P3 = q(_pool(A[4]))
+    A[5] = conv(5, P3)
+    U3 = q(_up(A[5]) + A[4])
+    A[6] = conv(6, U3)
+    U2 = q(_up(A[6]) + A[3])
+    A[7] = conv(7, U2)
+    U1 = q(_up(A[7]) + A[1])
+    A[8] = conv(8, U1)
+    out = conv(9, A[8])
+    ins = [x, A[0], P1, A[2], P2, P3, U3, U2, U1, A[8]]
+    return out[..., 0], (ws, A, ins, out)
+
+
+def net_loss_grad(params, x, target, quant=True):
+    """Loss mean((out0 - target)^2) and the flat gradient of all parameters."""
+    q = bf16 if quant else (lambda a: np.asarray(a, dtype=np.float64))
+    f = _f32 if quant else (lambda a: np.asarray(a, dtype=np.float64))
+    out0, (ws, A, ins, out) = net_forward(params, x, quant)
+    n = out0.size
+    d = f(f(out0) - f(target))
+    loss = float(np.mean(d * d))
+    dout = np.zeros_like(out)
+    dout[..., 0] = q(f(2.0 * d / n))
+    grads = [None] * 10
+    G = [None] * 10
+
+    def back(l, Gl):
+        g = dout if l == 9 else q(np.where(A[l] > 0, Gl, 0.0))
+        dw, db = conv3x3_wgrad(ins[l], g)
+        grads[l] = (dw, db)
+        return conv3x3(g, flip(ws[l][0]))
+
+    G[8] = back(9, None)
+    G[1] = back(8, G[8])
+    G[7] = _pool_sum(G[1])
+    G[3] = back(7, G[7])
+    G[6] = _pool_sum(G[3])
+    G[4] = back(6, G[6])
+    G[5] = _pool_sum(G[4])
+    G[4] = G[4] + 0.25 * _up(back(5, G[5]))
+    G[3] = G[3] + 0.25 * _up(back(4, G[4]))
+    G[2] = back(3, G[3])
+    G[1] = G[1] + 0.25 * _up(back(2, G[2]))
+    G[0] = back(1, G[1])
+    back(0, G[0])
+    return loss, flatten(grads)

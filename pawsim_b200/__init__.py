@@ -52,7 +52,7 @@ class GpuStats(ctypes.Structure):
     _fields_ = [("iters", ctypes.c_int), ("residual_max", ctypes.c_double),
                 ("residual_rms", ctypes.c_double), ("div_max", ctypes.c_double),
                 ("div_rms", ctypes.c_double), ("stop_measure", ctypes.c_double),
-                ("solve_ms", ctypes.c_double)]
+                ("solve_ms", ctypes.c_double), ("warm_start", ctypes.c_int)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -65,6 +65,10 @@ EXPORTS = (
     "pawsim_gpu_solve_mg", "pawsim_gpu_set_stream", "pawsim_gpu_synchronize",
     "pawsim_gpu_time", "pawsim_gpu_launch_count", "pawsim_gpu_last_error",
     "pawsim_nn_conv3x3", "pawsim_nn_conv3x3_wgrad", "pawsim_nn_flip_weights",
+    "pawsim_gpu_nn_setup", "pawsim_gpu_nn_train", "pawsim_gpu_nn_pairs", "pawsim_gpu_nn_net",
+    "pawsim_nn_net_create", "pawsim_nn_net_destroy", "pawsim_nn_net_param_count",
+    "pawsim_nn_net_get_params", "pawsim_nn_net_set_params", "pawsim_nn_net_get_grads",
+    "pawsim_nn_net_forward", "pawsim_nn_net_backward", "pawsim_nn_net_adam",
 )
 
 _LIB = None
@@ -103,6 +107,22 @@ def load_library(path: str = LIB_PATH):
     lib.pawsim_nn_conv3x3.argtypes = [P, I, I, I, I, P, P, I, I, P, P, P, P]
     lib.pawsim_nn_conv3x3_wgrad.argtypes = [P, P, I, I, I, I, I, P, P, P, P]
     lib.pawsim_nn_flip_weights.argtypes = [P, I, I, P, P]
+    U64, SZ = ctypes.c_ulonglong, ctypes.c_size_t
+    lib.pawsim_gpu_nn_setup.argtypes = [P, I, I, I, U64]
+    lib.pawsim_gpu_nn_train.argtypes = [P, I, ctypes.c_float, ctypes.POINTER(ctypes.c_double)]
+    lib.pawsim_gpu_nn_pairs.argtypes = [P]
+    lib.pawsim_gpu_nn_net.argtypes = [P]
+    lib.pawsim_gpu_nn_net.restype = P
+    lib.pawsim_nn_net_create.argtypes = [I, I, I, U64, ctypes.POINTER(P)]
+    lib.pawsim_nn_net_destroy.argtypes = [P]
+    lib.pawsim_nn_net_destroy.restype = None
+    lib.pawsim_nn_net_param_count.argtypes = [P]
+    lib.pawsim_nn_net_param_count.restype = ctypes.c_longlong
+    for fn in ("pawsim_nn_net_get_params", "pawsim_nn_net_set_params", "pawsim_nn_net_get_grads"):
+        getattr(lib, fn).argtypes = [P, F, SZ]
+    lib.pawsim_nn_net_forward.argtypes = [P, P, I, F]
+    lib.pawsim_nn_net_backward.argtypes = [P, P, P, I, ctypes.POINTER(ctypes.c_double)]
+    lib.pawsim_nn_net_adam.argtypes = [P, ctypes.c_float]
     lib.pawsim_gpu_last_error.argtypes = []
     lib.pawsim_gpu_last_error.restype = ctypes.c_char_p
     _LIB = lib
@@ -257,6 +277,27 @@ class Model:
     def synchronize(self) -> None:
         _check(self.lib.pawsim_gpu_synchronize(self._h))
 
+    # ---- learned warm start (no counterpart in the reference) ----
+    def nn_setup(self, collect: bool = True, use: bool = False, max_pairs: int = 256, batch: int = 8,
+                 seed: int = 1) -> None:
+        """Collect training pairs after each solve and/or start solves from the network's guess."""
+        mode = (1 if collect else 0) | (2 if use else 0)
+        _check(self.lib.pawsim_gpu_nn_setup(self._h, mode, max_pairs, batch, seed))
+
+    def nn_train(self, epochs: int, lr: float = 1e-3) -> float:
+        loss = ctypes.c_double()
+        _check(self.lib.pawsim_gpu_nn_train(self._h, epochs, lr, ctypes.byref(loss)))
+        return loss.value
+
+    def nn_pairs(self) -> int:
+        return self.lib.pawsim_gpu_nn_pairs(self._h)
+
+    def nn_net(self) -> "Net":
+        h = self.lib.pawsim_gpu_nn_net(self._h)
+        if not h:
+            raise PawsimError(-1, "warm start not configured")
+        return Net(handle=h, owner=self)
+
     def set_stream(self, stream_ptr: int) -> None:
         _check(self.lib.pawsim_gpu_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
 
@@ -266,3 +307,64 @@ class Model:
 
     def launch_count(self) -> int:
         return self.lib.pawsim_gpu_launch_count(self._h)
+
+
+class Net:
+    """A warm-start network on the GPU (standalone, or the one a Model owns)."""
+
+    def __init__(self, H: int = 0, W: int = 0, Bmax: int = 1, seed: int = 1, handle=None, owner=None):
+        self.lib = load_library()
+        self._owner = owner
+        if handle is not None:
+            self._h, self._own = ctypes.c_void_p(handle), False
+        else:
+            h = ctypes.c_void_p()
+            _check(self.lib.pawsim_nn_net_create(H, W, Bmax, seed, ctypes.byref(h)))
+            self._h, self._own = h, True
+
+    def close(self):
+        if getattr(self, "_own", False) and self._h:
+            self.lib.pawsim_nn_net_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def param_count(self) -> int:
+        return int(self.lib.pawsim_nn_net_param_count(self._h))
+
+    def _vec(self, fn, a=None):
+        n = self.param_count
+        if a is None:
+            a = np.zeros(n, dtype=np.float32)
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        _check(fn(self._h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n))
+        return a
+
+    def get_params(self) -> np.ndarray:
+        return self._vec(self.lib.pawsim_nn_net_get_params)
+
+    def set_params(self, p) -> None:
+        self._vec(self.lib.pawsim_nn_net_set_params, p)
+
+    def get_grads(self) -> np.ndarray:
+        return self._vec(self.lib.pawsim_nn_net_get_grads)
+
+    def forward(self, in_ptr: int, B: int, H: int, W: int) -> np.ndarray:
+        out = np.zeros((B, H, W), dtype=np.float32)
+        _check(self.lib.pawsim_nn_net_forward(self._h, ctypes.c_void_p(in_ptr), B,
+                                              out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
+
+    def backward(self, in_ptr: int, target_ptr: int, B: int) -> float:
+        loss = ctypes.c_double()
+        _check(self.lib.pawsim_nn_net_backward(self._h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(target_ptr), B,
+                                               ctypes.byref(loss)))
+        return loss.value
+
+    def adam(self, lr: float) -> None:
+        _check(self.lib.pawsim_nn_net_adam(self._h, lr))

@@ -14,6 +14,7 @@
 #include "common.cuh"
 #include "mg.cuh"
 #include "pressure.cuh"
+#include "warmstart.cuh"
 #include "tendency.cuh"
 
 namespace pawsim {
@@ -83,6 +84,8 @@ struct Model {
   double gg[LMAX], geff[LMAX];
   std::vector<double> hhs_host, hhb_host;
   Multigrid* mg = nullptr;
+  WarmStart* ws = nullptr;   // learned warm start (nullptr until configured)
+  int nn_mode = 0;
   bool thickness_fixed = false;
   bool ready = false;
   cudaEvent_t ev0, ev1;
@@ -95,6 +98,7 @@ struct Model {
     return (T*)p;
   }
   ~Model() {
+    delete ws;
     delete mg;
     for (void* p : allocs) cudaFree(p);
     cudaEventDestroy(ev0);
@@ -479,10 +483,17 @@ static int pressure_correct(Model* m, int update_diags, pawsim_gpu_stats* st) {
     PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
   } else if (m->c.solver == PAWSIM_GPU_SOLVER_MG) {
     double mres = 0;
+    if (m->ws && m->ws->before_solve(m->pi, m->rhs, m->mg, (m->nn_mode & 2) != 0, m->s) < 0)
+      return fail(PAWSIM_GPU_ECUDA, "warm-start guess failed");
     iters = m->mg->solve(m->pi, m->pitch, m->rhs, m->pitch, m->c.pi_tol, m->c.maxiters, &mres);
     local.stop_measure = mres;
     PAWSIM_CUDA_OK(cudaEventRecord(m->ev1, m->s));
     PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
+    if (m->ws) {
+      local.warm_start = m->ws->last_decision(m->s);
+      if (m->ws->after_solve(m->pi, m->rhs, (m->nn_mode & 1) != 0, m->s) < 0)
+        return fail(PAWSIM_GPU_ECUDA, "warm-start pair collection failed");
+    }
   } else {
     return fail(PAWSIM_GPU_EUNSUPPORTED, "pressureSolver 2 is not built yet");
   }
@@ -640,6 +651,108 @@ long long pawsim_gpu_launch_count(const pawsim_gpu* h) {
 }
 
 const char* pawsim_gpu_last_error(void) { return g_err; }
+
+int pawsim_gpu_nn_setup(pawsim_gpu* h, int mode, int max_pairs, int batch, unsigned long long seed) {
+  if (!h) return PAWSIM_GPU_EBADCONFIG;
+  Model* m = h->m;
+  if (mode && (m->c.solver != PAWSIM_GPU_SOLVER_MG || !m->mg))
+    return fail(PAWSIM_GPU_EUNSUPPORTED, "the learned warm start needs the multigrid solver (after init)");
+  if (mode && !m->ws) {
+    if (!WarmStart::factor(m->Nx, m->Ny))
+      return fail(PAWSIM_GPU_EUNSUPPORTED, "grid not supported by the warm-start network");
+    if (max_pairs < 1 || batch < 1) return fail(PAWSIM_GPU_EBADCONFIG, "max_pairs and batch must be positive");
+    m->ws = new WarmStart(m->Nx, m->Ny, m->pitch, max_pairs, batch, seed, m->s);
+    if (!m->ws->ok()) {
+      delete m->ws;
+      m->ws = nullptr;
+      return fail(PAWSIM_GPU_ECUDA, "warm-start allocation failed");
+    }
+  }
+  m->nn_mode = mode;
+  return 0;
+}
+
+int pawsim_gpu_nn_train(pawsim_gpu* h, int epochs, float lr, double* loss) {
+  if (!h || !h->m->ws) return fail(PAWSIM_GPU_EBADCONFIG, "warm start not configured");
+  int r = h->m->ws->train(epochs, lr, 1234567ull, loss, h->m->s);
+  if (r == -3) return fail(PAWSIM_GPU_ECUDA, "a tensor-core kernel gave up waiting");
+  if (r) return fail(PAWSIM_GPU_ECUDA, "warm-start training failed (no pairs, or a CUDA error)");
+  return 0;
+}
+
+int pawsim_gpu_nn_pairs(pawsim_gpu* h) { return (h && h->m->ws) ? h->m->ws->pairs() : 0; }
+
+void* pawsim_gpu_nn_net(pawsim_gpu* h) { return (h && h->m->ws) ? (void*)h->m->ws->net() : nullptr; }
+
+int pawsim_nn_net_create(int H, int W, int Bmax, unsigned long long seed, void** net) {
+  if (!net) return PAWSIM_GPU_EBADCONFIG;
+  WarmNet* n = new WarmNet(H, W, Bmax, seed);
+  if (!n->ok()) {
+    delete n;
+    return fail(PAWSIM_GPU_EBADCONFIG, "network sizes must be multiples of 8 (or allocation failed)");
+  }
+  *net = n;
+  return 0;
+}
+
+void pawsim_nn_net_destroy(void* net) { delete static_cast<WarmNet*>(net); }
+
+long long pawsim_nn_net_param_count(void* net) {
+  return net ? (long long)static_cast<WarmNet*>(net)->param_count() : 0;
+}
+
+int pawsim_nn_net_get_params(void* net, float* host, size_t n) {
+  WarmNet* w = static_cast<WarmNet*>(net);
+  if (!w || !host || n != w->param_count()) return PAWSIM_GPU_EBADCONFIG;
+  return w->get_params(host) ? fail(PAWSIM_GPU_ECUDA, "copy failed") : 0;
+}
+
+int pawsim_nn_net_set_params(void* net, const float* host, size_t n) {
+  WarmNet* w = static_cast<WarmNet*>(net);
+  if (!w || !host || n != w->param_count()) return PAWSIM_GPU_EBADCONFIG;
+  return w->set_params(host) ? fail(PAWSIM_GPU_ECUDA, "copy failed") : 0;
+}
+
+int pawsim_nn_net_get_grads(void* net, float* host, size_t n) {
+  WarmNet* w = static_cast<WarmNet*>(net);
+  if (!w || !host || n != w->param_count()) return PAWSIM_GPU_EBADCONFIG;
+  return w->get_grads(host) ? fail(PAWSIM_GPU_ECUDA, "copy failed") : 0;
+}
+
+int pawsim_nn_net_forward(void* net, const void* in, int B, float* out_host) {
+  WarmNet* w = static_cast<WarmNet*>(net);
+  if (!w || !in || !out_host || B < 1 || B > w->Bmax()) return PAWSIM_GPU_EBADCONFIG;
+  if (w->forward(static_cast<const __nv_bfloat16*>(in), B, 0)) return fail(PAWSIM_GPU_ECUDA, "forward failed");
+  PAWSIM_CUDA_OK(cudaMemcpy2D(out_host, sizeof(float), w->out(), 16 * sizeof(float), sizeof(float),
+                              (size_t)B * w->H() * w->W(), cudaMemcpyDeviceToHost));
+  int e = 0;
+  PAWSIM_CUDA_OK(cudaMemcpy(&e, w->err(), sizeof(int), cudaMemcpyDeviceToHost));
+  return e ? fail(PAWSIM_GPU_ECUDA, "a tensor-core kernel gave up waiting") : 0;
+}
+
+int pawsim_nn_net_backward(void* net, const void* in, const float* target, int B, double* loss) {
+  WarmNet* w = static_cast<WarmNet*>(net);
+  if (!w || !in || !target || B < 1 || B > w->Bmax()) return PAWSIM_GPU_EBADCONFIG;
+  double* dl = nullptr;
+  PAWSIM_CUDA_OK(cudaMalloc(&dl, sizeof(double)));
+  int r = w->backward(static_cast<const __nv_bfloat16*>(in), target, B, dl, 0);
+  double hl = 0;
+  cudaMemcpy(&hl, dl, sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(dl);
+  if (r) return fail(PAWSIM_GPU_ECUDA, "backward failed");
+  if (loss) *loss = hl;
+  int e = 0;
+  PAWSIM_CUDA_OK(cudaMemcpy(&e, w->err(), sizeof(int), cudaMemcpyDeviceToHost));
+  return e ? fail(PAWSIM_GPU_ECUDA, "a tensor-core kernel gave up waiting") : 0;
+}
+
+int pawsim_nn_net_adam(void* net, float lr) {
+  WarmNet* w = static_cast<WarmNet*>(net);
+  if (!w) return PAWSIM_GPU_EBADCONFIG;
+  if (w->adam_step(lr, 0)) return fail(PAWSIM_GPU_ECUDA, "adam step failed");
+  PAWSIM_CUDA_OK(cudaDeviceSynchronize());
+  return 0;
+}
 
 int pawsim_gpu_check_division(const double* x_host, size_t n, double d, long long* bad) {
   if (!x_host || !bad || n == 0) return fail(PAWSIM_GPU_EBADCONFIG, "null argument");

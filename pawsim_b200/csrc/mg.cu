@@ -1033,6 +1033,15 @@ int Multigrid::build_graph(int prec) {
   return 0;
 }
 
+void Multigrid::measure_async(const double* pi, const double* rhs, unsigned long long* bits, cudaStream_t s) {
+  LV<double> f = view<double>(lv_.back());
+  f.e = const_cast<double*>(pi);
+  f.rhs = const_cast<double*>(rhs);
+  cudaMemsetAsync(bits, 0, sizeof(unsigned long long), s);
+  max_residual_kernel<<<g2(f.Nx, f.Ny), B2, 0, s>>>(f, bits);
+  ++g_launches;
+}
+
 double Multigrid::max_residual(const double* pi, int pitch, const double* rhs, int rhs_pitch) {
   Level& F = lv_.back();
   LV<double> f = view<double>(F);

@@ -38,6 +38,9 @@ class Multigrid {
             double* maxres_out);
   // one evaluation of the stopping measure (for diagnostics and warm-start decisions)
   double max_residual(const double* pi, int pi_pitch, const double* rhs, int rhs_pitch);
+  // the same measure, left on the device: *bits = max |pi - Jacobi(pi)| as an integer bit
+  // pattern (zeroed first), enqueued on `s` without a host synchronisation
+  void measure_async(const double* pi, const double* rhs, unsigned long long* bits, cudaStream_t s);
   void set_options(const MGOptions& o) { opt_ = o; }
   const MGOptions& options() const { return opt_; }
   int levels() const { return (int)lv_.size(); }
