@@ -139,6 +139,57 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def pressure_comparison(cfg, fields, stream, spin, steps, epochs, pairs):
+    """Pressure ms/step and V-cycles/step of the plain FP64 multigrid (started from the
+    previous pressure, as the reference's solver is) against FP32 V-cycles in FP64 defect
+    correction started from the learned guess. Both models run the same `spin` untimed
+    steps (the learned one collecting its training pairs), the network is trained on the GPU
+    (untimed), then `steps` steps of each are timed with CUDA events."""
+    import torch
+    import pawsim_b200
+    res = {}
+    for name, fp32, learn in (("plain_fp64", 0, False), ("learned_fp32", 1, True)):
+        m = pawsim_b200.Model(cfg, fields, mg_fp32=fp32)
+        m.set_stream(stream.cuda_stream)
+        with torch.cuda.stream(stream):
+            if learn:
+                m.nn_setup(collect=True, use=False, max_pairs=pairs, batch=8, seed=7)
+            m.prelim()
+            n = 1
+            for _ in range(spin):
+                m.step(n)
+                n += 1
+            extra = {}
+            if learn:
+                t0 = time.perf_counter()
+                loss = m.nn_train(epochs=epochs, lr=1e-3)
+                torch.cuda.synchronize()
+                extra = {"train_pairs": m.nn_pairs(), "train_epochs": epochs, "train_s": time.perf_counter() - t0,
+                         "train_loss": loss, "params": m.nn_net().param_count}
+                m.nn_setup(collect=False, use=True)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            iters, solve, used = [], [], 0
+            e0.record(stream)
+            for _ in range(steps):
+                st = m.step(n)
+                iters.append(st["iters"])
+                solve.append(st["solve_ms"])
+                used += st["warm_start"] == 1
+                n += 1
+            e1.record(stream)
+            torch.cuda.synchronize()
+            step_ms = e0.elapsed_time(e1) / steps
+        res[name] = {"pressure_ms_per_step": float(np.mean(solve)), "vcycles_per_step": float(np.mean(iters)),
+                     "ms_per_step": step_ms, "sim_days_per_s": DT / 86400.0 / (step_ms / 1e3), **extra}
+        if learn:
+            res[name]["guess_used_steps"] = int(used)
+        m.close()
+    res["window"] = f"steps {spin + 1}..{spin + steps} after prelim"
+    res["pressure_speedup"] = res["plain_fp64"]["pressure_ms_per_step"] / res["learned_fp32"]["pressure_ms_per_step"]
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -147,6 +198,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mg-fp32", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-warm-start", action="store_true", help="skip the learned+FP32 pressure comparison")
+    ap.add_argument("--ws-spin", type=int, default=160, help="spin-up steps that collect training pairs")
+    ap.add_argument("--ws-epochs", type=int, default=30)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -250,6 +304,10 @@ def main():
         dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
     e2e_value = world * args.steps * DT / 86400.0 / float(t_e2e[0])
 
+    ws = None
+    if not args.no_warm_start:
+        ws = pressure_comparison(cfg, fields, stream, args.ws_spin, args.steps, args.ws_epochs, args.ws_spin)
+
     peak, peak_kind = peaks()
     ncell = cfg.Nx * cfg.Ny
     alg_bytes = ncell * (120 * L + 24)
@@ -275,6 +333,8 @@ def main():
                      "algorithmic_bytes": alg_bytes, "peak_kind": peak_kind},
         "clocks": clk.summary(),
     }
+    if ws is not None:
+        line["pressure_learned_fp32_vs_plain_fp64"] = ws
     if rank == 0 and not args.no_cpu_baseline:
         secs, sample = cpu_reference(param, 2, "reference")
         if secs is not None:

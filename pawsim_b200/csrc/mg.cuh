@@ -41,6 +41,9 @@ class Multigrid {
   // the same measure, left on the device: *bits = max |pi - Jacobi(pi)| as an integer bit
   // pattern (zeroed first), enqueued on `s` without a host synchronisation
   void measure_async(const double* pi, const double* rhs, unsigned long long* bits, cudaStream_t s);
+  // the measures of two candidate fields in one pass: bits[0] for pa, bits[1] for pb
+  void measure2_async(const double* pa, const double* pb, const double* rhs, unsigned long long* bits,
+                      cudaStream_t s);
   void set_options(const MGOptions& o) { opt_ = o; }
   const MGOptions& options() const { return opt_; }
   int levels() const { return (int)lv_.size(); }

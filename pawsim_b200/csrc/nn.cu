@@ -19,6 +19,8 @@
 // returns.
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "../../include/pawsim_b200.h"
 #include "common.cuh"
 #include "nn.cuh"
@@ -179,62 +181,81 @@ __global__ void __launch_bounds__(NTH) conv_fwd_kernel(const bf16* __restrict__ 
 
   const int tid = threadIdx.x;
   const long long npix = (long long)B * H * W;
-  const long long p = (long long)blockIdx.x * MT + tid;   // this thread's output pixel (A row)
-  int pb = 0, py = 0, px = 0;
-  const bool pvalid = p < npix;
-  if (pvalid) {
-    px = (int)(p % W);
-    long long t = p / W;
-    py = (int)(t % H);
-    pb = (int)(t / H);
-  }
-  // weights, K-major: 16-byte chunk (n, k8) at ((k8 * COUT/8) + n/8) * 128 + (n%8) * 16
+  const long long ntiles = (npix + MT - 1) / MT;
+  // weights, K-major: 16-byte chunk (n, k8) at ((k8 * COUT/8) + n/8) * 128 + (n%8) * 16;
+  // loaded once and kept for every tile this (persistent) CTA computes
   for (int q = tid; q < COUT * (K / 8); q += NTH) {
     const int n = q / (K / 8), k8 = q - n * (K / 8);
     const uint4 v = *reinterpret_cast<const uint4*>(w + (size_t)n * K + k8 * 8);
     *reinterpret_cast<uint4*>(sB + (k8 * (COUT / 8) + n / 8) * 128 + (n % 8) * 16) = v;
   }
   const uint32_t tmem = umma_setup<NCOLS>(mbar, &tmem_sh);
-  int issued = 0;
-  for (int r = 0; r < ROUNDS; ++r) {
-    const int buf = r & 1;
-    unsigned char* a = sA + buf * A_STAGE;
-    const bool fail = r >= 2 && !mbar_wait(&mbar[buf], (uint32_t)(((r - 2) >> 1) & 1));
-    if (__syncthreads_or(fail)) break;
-    // stage this thread's row of A for the round's K steps
-#pragma unroll
-    for (int sl = 0; sl < RSTEPS; ++sl) {
-      const int s = r * RSTEPS + sl;
-      if (s >= S) break;
-      const int tap = (s * KS) / CIN, ci0 = (s * KS) % CIN;
-      const int yy = py + tap / 3 - 1, xx = px + tap % 3 - 1;
-      uint4 v0 = make_uint4(0, 0, 0, 0), v1 = v0;
-      if (pvalid && yy >= 0 && yy < H && xx >= 0 && xx < W) {
-        const bf16* src = in + (((size_t)pb * H + yy) * W + xx) * CIN + ci0;
-        v0 = *reinterpret_cast<const uint4*>(src);
-        v1 = *reinterpret_cast<const uint4*>(src + 8);
-      }
-      unsigned char* dst = a + (2 * sl * (MT / 8) + tid / 8) * 128 + (tid % 8) * 16;
-      *reinterpret_cast<uint4*>(dst) = v0;
-      *reinterpret_cast<uint4*>(dst + LBO_A) = v1;
+  int rg = 0;   // rounds issued by this CTA over all its tiles (mbarrier phases)
+  bool ok = true;
+  for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const long long p = tile * MT + tid;   // this thread's output pixel (A row)
+    int pb = 0, py = 0, px = 0;
+    const bool pvalid = p < npix;
+    if (pvalid) {
+      px = (int)(p % W);
+      const long long t = p / W;
+      py = (int)(t % H);
+      pb = (int)(t / H);
     }
-    fence_async_smem();
-    __syncthreads();
-    if (tid == 0) {
-      tc_fence_after();
-      const uint32_t abase = smem_u32(a), bbase = smem_u32(sB);
+    int issued = 0;
+    for (int r = 0; r < ROUNDS; ++r) {
+      const int buf = rg & 1;
+      unsigned char* a = sA + buf * A_STAGE;
+      const bool fail = rg >= 2 && !mbar_wait(&mbar[buf], (uint32_t)(((rg - 2) >> 1) & 1));
+      if (__syncthreads_or(fail)) break;
+      // stage this thread's row of A for the round's K steps
+#pragma unroll
       for (int sl = 0; sl < RSTEPS; ++sl) {
         const int s = r * RSTEPS + sl;
         if (s >= S) break;
-        umma_bf16(tmem, make_desc(abase + 2 * sl * LBO_A, LBO_A, 128), make_desc(bbase + 2 * s * LBO_B, LBO_B, 128),
-                  IDESC, s > 0 ? 1u : 0u);
+        const int tap = (s * KS) / CIN, ci0 = (s * KS) % CIN;
+        const int yy = py + tap / 3 - 1, xx = px + tap % 3 - 1;
+        uint4 v0 = make_uint4(0, 0, 0, 0), v1 = v0;
+        if (pvalid && yy >= 0 && yy < H && xx >= 0 && xx < W) {
+          const bf16* src = in + (((size_t)pb * H + yy) * W + xx) * CIN + ci0;
+          v0 = *reinterpret_cast<const uint4*>(src);
+          v1 = *reinterpret_cast<const uint4*>(src + 8);
+        }
+        unsigned char* dst = a + (2 * sl * (MT / 8) + tid / 8) * 128 + (tid % 8) * 16;
+        *reinterpret_cast<uint4*>(dst) = v0;
+        *reinterpret_cast<uint4*>(dst + LBO_A) = v1;
       }
-      umma_commit(&mbar[buf]);
+      fence_async_smem();
+      __syncthreads();
+      if (tid == 0) {
+        tc_fence_after();
+        const uint32_t abase = smem_u32(a), bbase = smem_u32(sB);
+        for (int sl = 0; sl < RSTEPS; ++sl) {
+          const int s = r * RSTEPS + sl;
+          if (s >= S) break;
+          umma_bf16(tmem, make_desc(abase + 2 * sl * LBO_A, LBO_A, 128),
+                    make_desc(bbase + 2 * s * LBO_B, LBO_B, 128), IDESC, s > 0 ? 1u : 0u);
+        }
+        umma_commit(&mbar[buf]);
+      }
+      ++issued;
+      ++rg;
     }
-    ++issued;
-  }
-  const bool ok = umma_drain(mbar, issued, ROUNDS, err);
-  if (ok) {
+    // wait for this tile's last commit (it covers every earlier MMA of the CTA)
+    bool done = issued == ROUNDS;
+    if (issued > 0) {
+      const uint32_t par = (uint32_t)(((rg - 1) >> 1) & 1);
+      if (!mbar_wait(&mbar[(rg - 1) & 1], par)) {
+        done = false;
+        mbar_wait(&mbar[(rg - 1) & 1], par);
+      }
+    }
+    ok = !__syncthreads_or(!done);
+    tc_fence_after();
+    if (!ok) {
+      if (tid == 0 && err) atomicExch(err, 1);
+      break;
+    }
     // row `tid` of the accumulator sits in TMEM lane tid (warp w reads lanes 32w..32w+31);
     // every lane takes part in the warp-wide loads, lanes without a pixel store nothing
     const uint32_t trow = tmem + ((uint32_t)((tid / 32) * 32) << 16);
@@ -260,6 +281,8 @@ __global__ void __launch_bounds__(NTH) conv_fwd_kernel(const bf16* __restrict__ 
         *reinterpret_cast<uint4*>(out_bf + p * COUT + c0) = *reinterpret_cast<const uint4*>(hv);
       }
     }
+    // the next tile's MMAs overwrite the accumulator only after every lane has read it
+    tc_fence_before();
   }
   tc_fence_before();
   __syncthreads();
@@ -396,8 +419,17 @@ int launch_fwd(const bf16* in, int B, int H, int W, const bf16* w, const float* 
       return -1;
     attr = true;
   }
-  const long long npix = (long long)B * H * W;
-  const unsigned grid = (unsigned)((npix + MT - 1) / MT);
+  static int per_sm = 0, nsm = 0;
+  if (!per_sm) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv_fwd_kernel<CIN, COUT>, NTH, smem) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+  }
+  const long long ntiles = ((long long)B * H * W + MT - 1) / MT;
+  const unsigned grid = (unsigned)std::min<long long>(ntiles, (long long)nsm * per_sm);
   conv_fwd_kernel<CIN, COUT><<<grid, NTH, smem, s>>>(in, B, H, W, w, bias, relu ? 1 : 0, ob, of, err);
   ++g_launches;
   return cudaGetLastError() == cudaSuccess ? 0 : -1;

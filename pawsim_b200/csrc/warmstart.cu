@@ -484,7 +484,7 @@ int WarmNet::adam_step(float lr, cudaStream_t s) {
 
 int WarmStart::factor(int Nx, int Ny) {
   int F = 1;
-  while (Nx / F > 512 || Ny / F > 512) F *= 2;
+  while (Nx / F > 256 || Ny / F > 256) F *= 2;
   if (Nx % (8 * F) || Ny % (8 * F) || Nx / F < 8 || Ny / F < 8) return 0;
   return F;
 }
@@ -555,8 +555,7 @@ int WarmStart::before_solve(double* pi, const double* rhs, Multigrid* mg, bool u
   dim3 b(32, 8), g((Nx_ + 31) / 32, (Ny_ + 7) / 8);
   guess_kernel<<<g, b, 0, s>>>(net_->out(), F_, Hc_, Wc_, pi1_, pi2_, scal_, Nx_, Ny_, pitch_, pi);
   ++g_launches;
-  mg->measure_async(pi, rhs, &bits_[0], s);
-  mg->measure_async(pi1_, rhs, &bits_[1], s);
+  mg->measure2_async(pi, pi1_, rhs, bits_, s);
   select_kernel<<<g, b, 0, s>>>(bits_, pi1_, Nx_, Ny_, pitch_, pi, decision_);
   ++g_launches;
   guessed_ = true;

@@ -11,7 +11,7 @@
 // to the encoder activation of the same level.
 //
 // WarmStart: the network's inputs and use inside a time step. On a grid coarsened by a
-// power of two F (the largest level of at most 512 x 512), it sees
+// power of two F (the largest level of at most 256 x 256), it sees
 //   c0 = R(rhs) / s_d,  c1 = R(pi1 - pi2) / s_p,  c2 = (R(pi1) - mean) / s_pp
 // (R = F x F mean, pi1 = pi(t-1), pi2 = pi(t-2), s_* the RMS of each field) and predicts
 // d = R(pi(t) - (2 pi1 - pi2)) / s_p. The guess is 2 pi1 - pi2 + s_p P(d) with P the
