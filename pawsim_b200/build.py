@@ -4,6 +4,8 @@
 ``csrc/*.cu`` into ``pawsim_b200/libpawsim_b200.so`` with nvcc for sm_100a. The tendency
 and pressure kernels are compiled with ``-fmad=false`` so that no multiply-add is fused,
 as in the reference's x86-64 build; this is what makes the FP64 path bit-identical.
+It then links the C host driver ``host/pawsim_main.c`` against the library into
+``pawsim_b200/bin/PAWSIM_B200.exe`` (the drop-in for the reference's ``PAWSIM.exe``).
 """
 from __future__ import annotations
 
@@ -19,6 +21,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC,-O3",
          "-Xcompiler", "-fvisibility=hidden"]
 SOURCES = ["api.cu", "tendency.cu", "pressure.cu", "mg.cu", "noalloc.cu", "nn.cu", "warmstart.cu"]
+DRIVER_SRC = os.path.join(HERE, "host", "pawsim_main.c")
+DRIVER = os.path.join(HERE, "bin", "PAWSIM_B200.exe")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 
 def _stale(target, deps):
@@ -28,7 +33,27 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def build_driver(force: bool = False, verbose: bool = False) -> str:
+    """gcc the host driver against the library (rpath to the library's directory)."""
+    deps = [DRIVER_SRC, LIB, os.path.join(INCLUDE, "pawsim_b200.h")]
+    if not force and not _stale(DRIVER, deps):
+        return DRIVER
+    os.makedirs(os.path.dirname(DRIVER), exist_ok=True)
+    cmd = ["gcc", "-O2", "-std=c11", "-Wall", "-Wextra", "-I", INCLUDE, DRIVER_SRC, "-o", DRIVER,
+           "-L", HERE, "-lpawsim_b200", "-Wl,-rpath,$ORIGIN/..", "-lm"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return DRIVER
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    lib = build_lib(force, verbose)
+    build_driver(force, verbose)
+    return lib
+
+
+def build_lib(force: bool = False, verbose: bool = False) -> str:
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     deps.append(os.path.join(os.path.dirname(HERE), "include", "pawsim_b200.h"))
