@@ -93,6 +93,8 @@ typedef struct pawsim_gpu_stats
   double solve_ms;           /* device time of the solve alone (with the warm start's guess) */
   int warm_start;            /* learned warm start: 0 none, 1 guess used, 2 guess rejected
                                 (the solve started from the previous pressure) */
+  int fallback;              /* 1 when pressureSolver 2 fell back to the gathered multigrid
+                                (grid without a first clean 2:1 coarsening) */
 } pawsim_gpu_stats;
 
 typedef struct pawsim_gpu pawsim_gpu;

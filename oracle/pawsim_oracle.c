@@ -1925,6 +1925,264 @@ static void apply_correction (orc_model * m)
   state_halos(m,m->u,m->v,m->h);
 }
 
+/* ------------------------------------- distributed multigrid, serial build (DMG) */
+
+/* pressure.c:916-2176 with one rank: every level is one tile, transfers are the local
+ * 2:1 ones, and the last level (a side <= 8 or odd) is solved by the serial red-black SOR
+ * of the gathered tail. */
+#define DMG_PRE 3
+#define DMG_POST 3
+#define DMG_MIN 8
+#define DMG_MAXL 32
+
+typedef struct
+{
+  int Nx, Ny;
+  double dx, dy;
+  F2 x, rhs, res, Hc, Hw, Hs;
+} dmg_level;
+
+static double dmg_ow (orc_model * m, const dmg_level * l, int i, int j)
+{
+  int gi = i - G;
+  if (m->c.wall_ew && ((gi == 0) || (gi == l->Nx))) return 0;
+  return A(&l->Hw,i,j) / SQ(l->dx);
+}
+
+static double dmg_os (orc_model * m, const dmg_level * l, int i, int j)
+{
+  int gj = j - G;
+  if (m->c.wall_ns && ((gj == 0) || (gj == l->Ny))) return 0;
+  return A(&l->Hs,i,j) / SQ(l->dy);
+}
+
+/* pressure.c:1387-1438: in-place weighted sweeps (x outer, y inner) whose halo comes from
+ * the previous sweep; returns the largest update of the last sweep */
+static double dmg_smooth (orc_model * m, dmg_level * l, int nsweeps)
+{
+  int sweep,i,j;
+  double gmax = 0;
+  for (sweep = 0; sweep < nsweeps; sweep ++)
+  {
+    double lmax = 0;
+    xch(m,&l->x,K_SCALAR);
+    for (i = G; i < G+l->Nx; i ++)
+      for (j = G; j < G+l->Ny; j ++)
+      {
+        double Ow = dmg_ow(m,l,i,j), Oe = dmg_ow(m,l,i+1,j), Os = dmg_os(m,l,i,j), On = dmg_os(m,l,i,j+1);
+        double Osum = Ow + Oe + Os + On, xo, xj, xn;
+        if (Osum == 0) continue;
+        xo = A(&l->x,i,j);
+        xj = (Oe*A(&l->x,i+1,j) + Ow*A(&l->x,i-1,j) + On*A(&l->x,i,j+1) + Os*A(&l->x,i,j-1)
+            - A(&l->rhs,i,j)) / Osum;
+        xn = xo + m->c.omega_mg*(xj-xo);
+        A(&l->x,i,j) = xn;
+        lmax = fmax(lmax,fabs(xn-xo));
+      }
+    gmax = lmax;
+  }
+  xch(m,&l->x,K_SCALAR);
+  return gmax;
+}
+
+/* pressure.c:1441-1466: res = rhs - L(x) */
+static void dmg_residual (orc_model * m, dmg_level * l)
+{
+  int i,j;
+  xch(m,&l->x,K_SCALAR);
+  for (i = G; i < G+l->Nx; i ++)
+    for (j = G; j < G+l->Ny; j ++)
+    {
+      double Ow = dmg_ow(m,l,i,j), Oe = dmg_ow(m,l,i+1,j), Os = dmg_os(m,l,i,j), On = dmg_os(m,l,i,j+1);
+      double xc = A(&l->x,i,j);
+      A(&l->res,i,j) = A(&l->rhs,i,j)
+                     - (Oe*(A(&l->x,i+1,j)-xc) + Ow*(A(&l->x,i-1,j)-xc)
+                      + On*(A(&l->x,i,j+1)-xc) + Os*(A(&l->x,i,j-1)-xc));
+    }
+  xch(m,&l->res,K_SCALAR);
+}
+
+/* pressure.c:1469-1544: kind 0 = 2x2 mean, 1 = west faces (y pair), 2 = south faces (x pair) */
+static void dmg_restrict (orc_model * m, F2 * c, const F2 * f, int cNx, int cNy, int kind)
+{
+  int i,j;
+  f2_zero(c);
+  for (i = 0; i < cNx; i ++)
+    for (j = 0; j < cNy; j ++)
+    {
+      int a = 2*i + G, b = 2*j + G;
+      if (kind == 0)
+        A(c,i+G,j+G) = 0.25*(A(f,a,b) + A(f,a+1,b) + A(f,a,b+1) + A(f,a+1,b+1));
+      else if (kind == 1)
+        A(c,i+G,j+G) = 0.5*(A(f,a,b) + A(f,a,b+1));
+      else
+        A(c,i+G,j+G) = 0.5*(A(f,a,b) + A(f,a+1,b));
+    }
+  xch(m,c,K_SCALAR);
+}
+
+/* pressure.c:1547-1600: fine x += bilinear(coarse x); returns max |correction| */
+static double dmg_prolong (orc_model * m, dmg_level * f, dmg_level * c)
+{
+  int i,j;
+  double mx = 0;
+  xch(m,&c->x,K_SCALAR);
+  for (i = 0; i < c->Nx; i ++)
+    for (j = 0; j < c->Ny; j ++)
+    {
+      int ic = i+G, jc = j+G, a = 2*i+G, b = 2*j+G;
+      F2 * X = &c->x;
+      double e_sw = 0.5625*A(X,ic,jc) + 0.1875*A(X,ic-1,jc) + 0.1875*A(X,ic,jc-1) + 0.0625*A(X,ic-1,jc-1);
+      double e_se = 0.5625*A(X,ic,jc) + 0.1875*A(X,ic+1,jc) + 0.1875*A(X,ic,jc-1) + 0.0625*A(X,ic+1,jc-1);
+      double e_nw = 0.5625*A(X,ic,jc) + 0.1875*A(X,ic-1,jc) + 0.1875*A(X,ic,jc+1) + 0.0625*A(X,ic-1,jc+1);
+      double e_ne = 0.5625*A(X,ic,jc) + 0.1875*A(X,ic+1,jc) + 0.1875*A(X,ic,jc+1) + 0.0625*A(X,ic+1,jc+1);
+      A(&f->x,a,b) += e_sw;
+      A(&f->x,a+1,b) += e_se;
+      A(&f->x,a,b+1) += e_nw;
+      A(&f->x,a+1,b+1) += e_ne;
+      mx = fmax(mx,fabs(e_sw));
+      mx = fmax(mx,fabs(e_se));
+      mx = fmax(mx,fabs(e_nw));
+      mx = fmax(mx,fabs(e_ne));
+    }
+  xch(m,&f->x,K_SCALAR);
+  return mx;
+}
+
+/* pressure.c:360-437 and 1713-1780: serial red-black SOR of the last level from its Hc
+ * (faces averaged with modular indices, wall faces zeroed); the mean is removed at the
+ * end. Its own updates do not enter the V-cycle's measure. */
+static void dmg_tail (orc_model * m, dmg_level * l)
+{
+  int Nx = l->Nx, Ny = l->Ny, i, j, color, iters = 0;
+  double * Hw = (double *) calloc((size_t) Nx*Ny,sizeof(double));
+  double * Hs = (double *) calloc((size_t) Nx*Ny,sizeof(double));
+  double mu = m->c.pi_tol + 1, mean = 0, om = m->c.sor_rp;
+#define HC(a,b) A(&l->Hc,G+(a),G+(b))
+#define PX(a,b) A(&l->x,G+(a),G+(b))
+  for (i = 0; i < Nx; i ++)
+    for (j = 0; j < Ny; j ++)
+    {
+      int im1 = (i+Nx-1) % Nx, jm1 = (j+Ny-1) % Ny;
+      Hw[(size_t) i*Ny+j] = 0.5*(HC(i,j) + HC(im1,j));
+      Hs[(size_t) i*Ny+j] = 0.5*(HC(i,j) + HC(i,jm1));
+    }
+  if (m->c.wall_ew) for (j = 0; j < Ny; j ++) Hw[j] = 0;
+  if (m->c.wall_ns) for (i = 0; i < Nx; i ++) Hs[(size_t) i*Ny] = 0;
+  while ((mu > m->c.pi_tol) && (iters < m->c.maxiters))
+  {
+    mu = 0;
+    for (color = 0; color < 2; color ++)
+      for (i = 0; i < Nx; i ++)
+      {
+        int im1 = (i+Nx-1) % Nx, ip1 = (i+1) % Nx;
+        for (j = 0; j < Ny; j ++)
+        {
+          int jm1 = (j+Ny-1) % Ny, jp1 = (j+1) % Ny;
+          double Ow = (m->c.wall_ew && i == 0) ? 0 : Hw[(size_t) i*Ny+j] / SQ(l->dx);
+          double Oe = (m->c.wall_ew && i+1 == Nx) ? 0 : Hw[(size_t) ((i+1) % Nx)*Ny+j] / SQ(l->dx);
+          double Os = (m->c.wall_ns && j == 0) ? 0 : Hs[(size_t) i*Ny+j] / SQ(l->dy);
+          double On = (m->c.wall_ns && j+1 == Ny) ? 0 : Hs[(size_t) i*Ny+(j+1) % Ny] / SQ(l->dy);
+          double Osum = Ow + Oe + Os + On, old, nv;
+          if (((i+j) & 1) != color) continue;
+          if (Osum == 0) continue;
+          old = PX(i,j);
+          nv = (1-om)*old + om*(Oe*PX(ip1,j) + Ow*PX(im1,j) + On*PX(i,jp1) + Os*PX(i,jm1) - A(&l->rhs,G+i,G+j)) / Osum;
+          PX(i,j) = nv;
+          mu = fmax(mu,fabs(nv-old));
+        }
+      }
+    iters ++;
+  }
+  for (i = 0; i < Nx; i ++)
+    for (j = 0; j < Ny; j ++) mean += PX(i,j);
+  mean /= ((double) Nx * (double) Ny);
+  for (i = 0; i < Nx; i ++)
+    for (j = 0; j < Ny; j ++) PX(i,j) -= mean;
+#undef HC
+#undef PX
+  free(Hw);
+  free(Hs);
+  xch(m,&l->x,K_SCALAR);
+}
+
+/* pressure.c:2063-2123 */
+static double dmg_vcycle (orc_model * m, dmg_level * lv, int n, int l)
+{
+  double mu;
+  dmg_level * c;
+  if (l == n-1)
+  {
+    dmg_tail(m,&lv[l]);
+    return 0;
+  }
+  c = &lv[l+1];
+  mu = dmg_smooth(m,&lv[l],DMG_PRE);
+  dmg_residual(m,&lv[l]);
+  dmg_restrict(m,&c->rhs,&lv[l].res,c->Nx,c->Ny,0);
+  dmg_restrict(m,&c->Hc,&lv[l].Hc,c->Nx,c->Ny,0);
+  dmg_restrict(m,&c->Hw,&lv[l].Hw,c->Nx,c->Ny,1);
+  dmg_restrict(m,&c->Hs,&lv[l].Hs,c->Nx,c->Ny,2);
+  f2_zero(&c->x);
+  mu = fmax(mu,dmg_vcycle(m,lv,n,l+1));
+  mu = fmax(mu,dmg_prolong(m,&lv[l],c));
+  mu = fmax(mu,dmg_smooth(m,&lv[l],DMG_POST));
+  return mu;
+}
+
+/* pressure.c:2126-2176; grids that cannot start with a clean 2:1 coarsening fall back to
+ * the gathered multigrid, as the reference does */
+static int solve_dmg (orc_model * m)
+{
+  dmg_level lv[DMG_MAXL];
+  int n = 0, Nx = m->Nx, Ny = m->Ny, cycles = 0, l, i, j;
+  double mu = m->c.pi_tol + 1;
+  if ((Nx <= DMG_MIN) || (Ny <= DMG_MIN) || (Nx % 2) || (Ny % 2)) return solve_mg(m);
+  while (n < DMG_MAXL)
+  {
+    dmg_level * L = &lv[n];
+    L->Nx = Nx; L->Ny = Ny;
+    L->dx = m->c.Lx / Nx; L->dy = m->c.Ly / Ny;
+    if (!f2_alloc(&L->x,Nx,Ny) || !f2_alloc(&L->rhs,Nx,Ny) || !f2_alloc(&L->res,Nx,Ny)
+     || !f2_alloc(&L->Hc,Nx,Ny) || !f2_alloc(&L->Hw,Nx,Ny) || !f2_alloc(&L->Hs,Nx,Ny))
+      return -1;
+    n ++;
+    if ((Nx <= DMG_MIN) || (Ny <= DMG_MIN) || (Nx % 2) || (Ny % 2)) break;
+    Nx = (Nx+1)/2;
+    Ny = (Ny+1)/2;
+  }
+  for (i = G; i < G+m->Nx; i ++)
+    for (j = G; j < G+m->Ny; j ++)
+    {
+      A(&lv[0].x,i,j) = A(&m->pi,i,j);
+      A(&lv[0].rhs,i,j) = A(&m->rhs,i,j);
+      A(&lv[0].Hc,i,j) = A(&m->Hc,i,j);
+      A(&lv[0].Hw,i,j) = A(&m->Hw,i,j);
+      A(&lv[0].Hs,i,j) = A(&m->Hs,i,j);
+    }
+  xch(m,&lv[0].x,K_SCALAR);
+  xch(m,&lv[0].rhs,K_SCALAR);
+  xch(m,&lv[0].Hc,K_SCALAR);
+  xch(m,&lv[0].Hw,K_SCALAR);
+  xch(m,&lv[0].Hs,K_SCALAR);
+  while ((mu > m->c.pi_tol) && (cycles < m->c.maxiters))
+  {
+    mu = dmg_vcycle(m,lv,n,0);
+    subtract_mean(m,&lv[0].x);
+    cycles ++;
+  }
+  for (i = G; i < G+m->Nx; i ++)
+    for (j = G; j < G+m->Ny; j ++) A(&m->pi,i,j) = A(&lv[0].x,i,j);
+  for (l = 0; l < n; l ++)
+  {
+    free(lv[l].x.d); free(lv[l].rhs.d); free(lv[l].res.d);
+    free(lv[l].Hc.d); free(lv[l].Hw.d); free(lv[l].Hs.d);
+  }
+  subtract_mean(m,&m->pi);
+  xch(m,&m->pi,K_SCALAR);
+  return cycles;
+}
+
 int orc_pressure (orc_model * m, int update_diags, orc_pstats * st)
 {
   int iters;
@@ -1934,7 +2192,7 @@ int orc_pressure (orc_model * m, int update_diags, orc_pstats * st)
   correct_thickness(m);
   build_rhs(m);
   if (m->c.solver == 1) iters = solve_mg(m);
-  else if (m->c.solver == 2) return -2;
+  else if (m->c.solver == 2) iters = solve_dmg(m);
   else iters = solve_sor(m);
   if (m->c.pressure_timing) residual_norms(m);
   apply_correction(m);

@@ -52,7 +52,7 @@ class GpuStats(ctypes.Structure):
     _fields_ = [("iters", ctypes.c_int), ("residual_max", ctypes.c_double),
                 ("residual_rms", ctypes.c_double), ("div_max", ctypes.c_double),
                 ("div_rms", ctypes.c_double), ("stop_measure", ctypes.c_double),
-                ("solve_ms", ctypes.c_double), ("warm_start", ctypes.c_int)]
+                ("solve_ms", ctypes.c_double), ("warm_start", ctypes.c_int), ("fallback", ctypes.c_int)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

@@ -20,7 +20,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC,-O3",
          "-Xcompiler", "-fvisibility=hidden"]
-SOURCES = ["api.cu", "tendency.cu", "pressure.cu", "mg.cu", "noalloc.cu", "nn.cu", "warmstart.cu"]
+SOURCES = ["api.cu", "tendency.cu", "pressure.cu", "mg.cu", "noalloc.cu", "nn.cu", "warmstart.cu", "dmg.cu"]
 DRIVER_SRC = os.path.join(HERE, "host", "pawsim_main.c")
 DRIVER = os.path.join(HERE, "bin", "PAWSIM_B200.exe")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")

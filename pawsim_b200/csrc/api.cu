@@ -12,6 +12,7 @@
 
 #include "../../include/pawsim_b200.h"
 #include "common.cuh"
+#include "dmg.cuh"
 #include "mg.cuh"
 #include "pressure.cuh"
 #include "warmstart.cuh"
@@ -84,6 +85,7 @@ struct Model {
   double gg[LMAX], geff[LMAX];
   std::vector<double> hhs_host, hhb_host;
   Multigrid* mg = nullptr;
+  DMG* dmg = nullptr;        // pressureSolver 2 (nullptr: grid falls back to the gathered MG)
   WarmStart* ws = nullptr;   // learned warm start (nullptr until configured)
   int nn_mode = 0;
   bool thickness_fixed = false;
@@ -99,6 +101,7 @@ struct Model {
   }
   ~Model() {
     delete ws;
+    delete dmg;
     delete mg;
     for (void* p : allocs) cudaFree(p);
     cudaEventDestroy(ev0);
@@ -335,6 +338,13 @@ static int init(Model* m) {
     o.tile_shape = m->c.mg_tile - 1;
     m->mg = new Multigrid(m->Nx, m->Ny, m->c.Lx, m->c.Ly, m->c.wall_ew, m->c.wall_ns, Hc.data(), o, m->s);
     if (!m->mg->ok()) return fail(PAWSIM_GPU_ECUDA, "multigrid allocation failed");
+    delete m->dmg;
+    m->dmg = nullptr;
+    if (m->c.solver == PAWSIM_GPU_SOLVER_MG_DISTRIBUTED && DMG::can_start(m->Nx, m->Ny)) {
+      m->dmg = new DMG(m->Nx, m->Ny, m->c.Lx, m->c.Ly, m->c.wall_ew, m->c.wall_ns, Hc.data(), m->c.omega_mg,
+                       m->c.sor_rp, m->s);
+      if (!m->dmg->ok()) return fail(PAWSIM_GPU_ECUDA, "distributed multigrid allocation failed");
+    }
   }
   PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
   m->ready = true;
@@ -494,8 +504,25 @@ static int pressure_correct(Model* m, int update_diags, pawsim_gpu_stats* st) {
       if (m->ws->after_solve(m->pi, m->rhs, (m->nn_mode & 1) != 0, m->s) < 0)
         return fail(PAWSIM_GPU_ECUDA, "warm-start pair collection failed");
     }
+  } else if (m->dmg) {
+    double mu = 0;
+    iters = m->dmg->solve(m->pi, m->pitch, m->rhs, m->pitch, m->c.pi_tol, m->c.maxiters, &mu);
+    if (iters < 0) return fail(PAWSIM_GPU_ECUDA, "distributed multigrid solve failed");
+    // the reference removes the mean of pi once more after copying it back (pressure.c:2169)
+    launch_sum(m->pi, m->Nx, m->Ny, m->pitch, m->serial(), m->scratch, m->dsum, m->s);
+    launch_subtract_mean(m->pi, m->Nx, m->Ny, m->pitch, m->dsum, m->s);
+    g_launches += m->serial() ? 2 : 3;
+    local.stop_measure = mu;
+    PAWSIM_CUDA_OK(cudaEventRecord(m->ev1, m->s));
+    PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
   } else {
-    return fail(PAWSIM_GPU_EUNSUPPORTED, "pressureSolver 2 is not built yet");
+    // grids without a first clean 2:1 coarsening use the gathered multigrid (pressure.c:2136-2148)
+    double mres = 0;
+    iters = m->mg->solve(m->pi, m->pitch, m->rhs, m->pitch, m->c.pi_tol, m->c.maxiters, &mres);
+    local.stop_measure = mres;
+    local.fallback = 1;
+    PAWSIM_CUDA_OK(cudaEventRecord(m->ev1, m->s));
+    PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
   }
   float ms = 0;
   cudaEventElapsedTime(&ms, m->ev0, m->ev1);
@@ -634,6 +661,7 @@ int pawsim_gpu_set_stream(pawsim_gpu* h, void* stream) {
   if (!h) return PAWSIM_GPU_EBADCONFIG;
   h->m->s = (cudaStream_t)stream;
   if (h->m->mg) h->m->mg->set_stream(h->m->s);
+  if (h->m->dmg) h->m->dmg->set_stream(h->m->s);
   return 0;
 }
 

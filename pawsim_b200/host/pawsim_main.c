@@ -531,7 +531,7 @@ int main (int argc, char ** argv)
   pawsim_gpu_stats st;
   const char * outdir;
   double * plane = NULL;
-  unsigned n, n_saves, solves = 0;
+  unsigned n, n_saves, solves = 0, fallbacks = 0;
   double wall_total = 0, iters_total = 0;
   const char * slash;
   int rc = 1;
@@ -610,11 +610,14 @@ int main (int argc, char ** argv)
     solves ++;
     wall_total += st.solve_ms / 1e3;
     iters_total += st.iters;
+    fallbacks += st.fallback != 0;
     if (c.pressureTiming)
-      printf("PAWSIM pressure solve: phase=prelim n=0 solver=%s iters=%u walltime=%0.6f s residual_max=%0.6e "
-             "residual_rms=%0.6e div_max=%0.6e div_rms=%0.6e\n",
-             solver_name(c.pressureSolver),(unsigned) st.iters,st.solve_ms / 1e3,st.residual_max,st.residual_rms,
-             st.div_max,st.div_rms);
+    {
+      printf("PAWSIM pressure solve: phase=prelim n=0 solver=%s",st.fallback ? "MG_GATHERED" : solver_name(c.pressureSolver));
+      if (st.fallback) printf(" requested=%s fallback=1",solver_name(c.pressureSolver));
+      printf(" iters=%u walltime=%0.6f s residual_max=%0.6e residual_rms=%0.6e div_max=%0.6e div_rms=%0.6e\n",
+             (unsigned) st.iters,st.solve_ms / 1e3,st.residual_max,st.residual_rms,st.div_max,st.div_rms);
+    }
     printf("PAWSIM pressure iterations: %u\n",(unsigned) st.iters);
     fflush(stdout);
   }
@@ -635,12 +638,14 @@ int main (int argc, char ** argv)
       solves ++;
       wall_total += st.solve_ms / 1e3;
       iters_total += st.iters;
+      fallbacks += st.fallback != 0;
       if (c.pressureTiming)
       {
-        printf("PAWSIM pressure solve: phase=step n=%u solver=%s iters=%u walltime=%0.6f s residual_max=%0.6e "
-               "residual_rms=%0.6e div_max=%0.6e div_rms=%0.6e\n",
-               n,solver_name(c.pressureSolver),(unsigned) st.iters,st.solve_ms / 1e3,st.residual_max,
-               st.residual_rms,st.div_max,st.div_rms);
+        printf("PAWSIM pressure solve: phase=step n=%u solver=%s",n,
+               st.fallback ? "MG_GATHERED" : solver_name(c.pressureSolver));
+        if (st.fallback) printf(" requested=%s fallback=1",solver_name(c.pressureSolver));
+        printf(" iters=%u walltime=%0.6f s residual_max=%0.6e residual_rms=%0.6e div_max=%0.6e div_rms=%0.6e\n",
+               (unsigned) st.iters,st.solve_ms / 1e3,st.residual_max,st.residual_rms,st.div_max,st.div_rms);
         fflush(stdout);
       }
       if ((unsigned) st.iters == c.maxiters)
@@ -660,9 +665,9 @@ int main (int argc, char ** argv)
   }
   if (c.pressureTiming && solves > 0)
   {
-    printf("PAWSIM pressure summary: requested=%s solves=%u fallback_solves=0 total_walltime=%0.6f s "
+    printf("PAWSIM pressure summary: requested=%s solves=%u fallback_solves=%u total_walltime=%0.6f s "
            "mean_walltime=%0.6f s mean_iters=%0.2f\n",
-           solver_name(c.pressureSolver),solves,wall_total,wall_total / solves,iters_total / solves);
+           solver_name(c.pressureSolver),solves,fallbacks,wall_total,wall_total / solves,iters_total / solves);
     fflush(stdout);
   }
   rc = 0;

@@ -35,6 +35,8 @@ CASES = {
     "jets": (inputs.jets, dict(N=16, dt=100.0, solver=1)),
     "full": (inputs.full_physics, dict(N=16, dt=50.0, solver=1, Ly=320e3, bathy_len=20e3,
                                        sponge=40e3)),
+    "gyre_dmg": (inputs.gyre, dict(N=32, Ny=24, dt=900.0, solver=2, tol=1e-10)),
+    "jets_dmg": (inputs.jets, dict(N=32, dt=100.0, solver=2)),
 }
 LINE = re.compile(r"iters=(\d+) walltime=\S+ s residual_max=(\S+) residual_rms=(\S+) "
                   r"div_max=(\S+) div_rms=(\S+)")
@@ -69,7 +71,10 @@ def make(name, fn, kw, outdir):
 
 
 if __name__ == "__main__":
+    # python tests/golden/make_golden.py [case ...]   (all cases when none are named)
     oracle.build(ref=True)
     for name, (fn, kw) in CASES.items():
+        if len(sys.argv) > 1 and name not in sys.argv[1:]:
+            continue
         make(name, fn, kw, HERE)
         print("wrote", name)

@@ -5,7 +5,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden")
-CASES = ["gyre_sor", "gyre_mg", "gyre_hk83_a4", "channel", "jets", "full"]
+CASES = ["gyre_sor", "gyre_mg", "gyre_hk83_a4", "channel", "jets", "full", "gyre_dmg", "jets_dmg"]
 
 
 def load_case(name, tmp):
