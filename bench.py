@@ -48,6 +48,17 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def tendency_traffic():
+    """DRAM bytes per launch of the tendency kernel from the committed ncu summary of the same
+    workload (one ncu capture; ncu cannot run inside the timed benchmark)."""
+    p = os.path.join(ROOT, "profiles", f"tendency_kernel_gyre{N_GRID}x{N_GRID}x2.txt")
+    if os.path.exists(p):
+        for line in open(p):
+            if line.startswith("dram_bytes_per_launch:"):
+                return int(line.split()[1])
+    return None
+
+
 def make_inputs(d):
     from pawsim_b200 import inputs
     return inputs.gyre(d, N=N_GRID, dt=DT, Nt=1000, solver=1, tol=TOL, seed=0)
@@ -328,7 +339,7 @@ def main():
         "e2e": {"value": e2e_value, "unit": "sim-days/s", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": tendency_traffic(),
                      "kernel": "tendency_kernel (fused tendency + AB3)", "kernel_ms": k_ms,
                      "algorithmic_bytes": alg_bytes, "peak_kind": peak_kind},
         "clocks": clk.summary(),

@@ -291,17 +291,18 @@ __global__ void __launch_bounds__(NTH) conv_fwd_kernel(const bf16* __restrict__ 
 
 // ------------------------------------------------------------------ weight gradient
 
-constexpr int WG_PIX = 2048;   // pixels reduced by one CTA
+constexpr int WG_PIX_MAX = 2048;   // most pixels reduced by one CTA
 
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(NTH) conv_wgrad_kernel(const bf16* __restrict__ in, const bf16* __restrict__ dout,
-                                                         int B, int H, int W, float* __restrict__ dw, int* err) {
+                                                         int B, int H, int W, int pix_per_cta, float* __restrict__ dw,
+                                                         int* err) {
   constexpr int MROWS = 9 * CIN;          // rows (tap, ci) of the gradient
   constexpr int NCOLS = tmem_cols<COUT>();
   constexpr uint32_t LBO_B = (COUT / 8) * 128;
   constexpr int B_STAGE = RSTEPS * 2 * (COUT / 8) * 128;
   constexpr uint32_t IDESC = make_idesc(COUT);
-  constexpr int ROUNDS = WG_PIX / (RSTEPS * KS);   // 64 pixels per round
+  const int ROUNDS = pix_per_cta / (RSTEPS * KS);   // 64 pixels per round
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned char* sA = smem;                         // 2 x A_STAGE
   unsigned char* sB = smem + 2 * A_STAGE;           // 2 x B_STAGE
@@ -311,7 +312,7 @@ __global__ void __launch_bounds__(NTH) conv_wgrad_kernel(const bf16* __restrict_
   const int tid = threadIdx.x;
   const int row0 = blockIdx.x * MT;                 // first (tap, ci) row of this tile
   const long long npix = (long long)B * H * W;
-  const long long pix0 = (long long)blockIdx.y * WG_PIX;
+  const long long pix0 = (long long)blockIdx.y * pix_per_cta;
   const uint32_t tmem = umma_setup<NCOLS>(mbar, &tmem_sh);
   int issued = 0;
   for (int r = 0; r < ROUNDS; ++r) {
@@ -424,9 +425,12 @@ int launch_fwd(const bf16* in, int B, int H, int W, const bf16* w, const float* 
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv_fwd_kernel<CIN, COUT>, NTH, smem) != cudaSuccess ||
-        per_sm < 1)
-      per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv_fwd_kernel<CIN, COUT>, NTH, smem) != cudaSuccess)
+      per_sm = 0;
+    // shared memory is the binding limit (each CTA holds the weights and two A stages; the
+    // tensor memory of 4 CTAs x 64 columns fits the SM's 512)
+    const int by_smem = (int)((227u * 1024u) / (smem + 1024));
+    per_sm = std::max(per_sm, std::min(4, std::max(1, by_smem)));
   }
   const long long ntiles = ((long long)B * H * W + MT - 1) / MT;
   const unsigned grid = (unsigned)std::min<long long>(ntiles, (long long)nsm * per_sm);
@@ -446,8 +450,12 @@ int launch_wgrad(const bf16* in, const bf16* dout, int B, int H, int W, float* d
     attr = true;
   }
   const long long npix = (long long)B * H * W;
-  dim3 grid((9 * CIN + MT - 1) / MT, (unsigned)((npix + WG_PIX - 1) / WG_PIX));
-  conv_wgrad_kernel<CIN, COUT><<<grid, NTH, smem, s>>>(in, dout, B, H, W, dw, err);
+  // pixels per CTA: a multiple of 64, small enough that the grid covers about 4 CTAs per SM
+  const int mtiles = (9 * CIN + MT - 1) / MT;
+  long long per = (npix * mtiles + 4 * 148 - 1) / (4 * 148);
+  per = std::min<long long>(WG_PIX_MAX, std::max<long long>(64, (per + 63) / 64 * 64));
+  dim3 grid(mtiles, (unsigned)((npix + per - 1) / per));
+  conv_wgrad_kernel<CIN, COUT><<<grid, NTH, smem, s>>>(in, dout, B, H, W, (int)per, dw, err);
   ++g_launches;
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -3,10 +3,14 @@
     python -m pawsim_b200.run --setup gyre --N 1024 --steps 4 [--integrator-only]
                               [--solver 0|1] [--mg-fp32] [--mg-tile K] [--mg-omega W]
                               [--mg-pre P] [--mg-post Q] [--dt 60] [--param FILE]
+                              [--ws-collect S --ws-epochs E]
 
 ``--integrator-only`` advances with ``pawsim_gpu_integrator_step`` alone (one fused tendency
 kernel per step, no pressure correction), which isolates the tendency kernel for a profiler.
 ``--param`` runs an existing AWSIM parameter file instead of a synthetic set-up.
+``--ws-collect S`` first runs S steps that collect warm-start training pairs, trains the
+network for ``--ws-epochs`` epochs on the GPU, then runs ``--steps`` steps whose solves start
+from the network's guess (this exercises the tcgen05 convolution kernels).
 """
 from __future__ import annotations
 
@@ -35,6 +39,8 @@ def main(argv=None):
     ap.add_argument("--mg-pre", type=int, default=1)
     ap.add_argument("--mg-post", type=int, default=1)
     ap.add_argument("--integrator-only", action="store_true")
+    ap.add_argument("--ws-collect", type=int, default=0)
+    ap.add_argument("--ws-epochs", type=int, default=2)
     a = ap.parse_args(argv)
     with tempfile.TemporaryDirectory() as d:
         if a.param:
@@ -59,13 +65,28 @@ def main(argv=None):
             m.synchronize()
             rep = {}
         else:
+            n0 = 1
+            ws = {}
+            if a.ws_collect:
+                m.nn_setup(collect=True, use=False, max_pairs=a.ws_collect, batch=8)
             m.prelim()
+            if a.ws_collect:
+                for n0 in range(1, a.ws_collect + 1):
+                    m.step(n0)
+                n0 += 1
+                ws["loss"] = m.nn_train(epochs=a.ws_epochs)
+                ws["pairs"] = m.nn_pairs()
+                m.nn_setup(collect=False, use=True)
             rep = {}
-            iters = []
-            for n in range(1, a.steps + 1):
+            iters, used = [], 0
+            for n in range(n0, n0 + a.steps):
                 rep = m.step(n)
                 iters.append(rep["iters"])
+                used += rep["warm_start"] == 1
             rep["iters_per_step"] = iters
+            if ws:
+                rep["warm_start_used"] = used
+                rep["warm_start_training"] = ws
         m.synchronize()
         dt = time.perf_counter() - t0
         print(json.dumps({"setup": a.param or a.setup, "N": [cfg.Nx, cfg.Ny, cfg.Nlay], "steps": a.steps,
