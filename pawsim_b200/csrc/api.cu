@@ -117,6 +117,7 @@ struct Model {
     g.Nx = Nx; g.Ny = Ny; g.pitch = pitch; g.L = L; g.lstride = lstride;
     g.wall_ew = c.wall_ew; g.wall_ns = c.wall_ns; g.dx = dx; g.dy = dy; g.dt = c.dt;
     g.thick_scheme = c.thick_scheme;
+    g.kt00_sigma = c.KT00_sigma;
     g.rdx = 1.0 / dx; g.rdy = 1.0 / dy;
     g.rdxdt = 1.0 / (dx * c.dt); g.rdydt = 1.0 / (dy * c.dt);
     return g;
@@ -137,10 +138,13 @@ static int create(const pawsim_gpu_config* cfg, Model** out) {
     return fail(PAWSIM_GPU_EBADCONFIG, "PAWSIM only supports AB1, AB2 and AB3 time stepping so far");
   if (c.mom_scheme < 0 || c.mom_scheme > 3 || c.thick_scheme < 0 || c.thick_scheme > 3)
     return fail(PAWSIM_GPU_EBADCONFIG, "Unknown or unsupported numerical scheme identifier");
-  if (c.thick_scheme > 1) return fail(PAWSIM_GPU_EUNSUPPORTED, "UP3/KT00 thickness schemes are not built yet");
-  if (c.A2smag > 0 || c.A4smag > 0) return fail(PAWSIM_GPU_EUNSUPPORTED, "Smagorinsky viscosity is not built yet");
-  if (c.quad_drag > 0 || c.quad_drag_surf > 0) return fail(PAWSIM_GPU_EUNSUPPORTED, "quadratic drag is not built yet");
-  if (c.hsml > 0 || c.hbbl > 0) return fail(PAWSIM_GPU_EUNSUPPORTED, "hsml/hbbl layer fractions are not built yet");
+  // quadratic drag reads the velocity of the whole boundary layer at neighbouring faces; the
+  // fused kernel builds it from the top or bottom layer's tile, so a drag whose layer is
+  // spread by a fraction depth is not built
+  if (c.quad_drag > 0 && c.hbbl > 0)
+    return fail(PAWSIM_GPU_EUNSUPPORTED, "quadratic bottom drag with hbbl > 0 is not built");
+  if (c.quad_drag_surf > 0 && c.hsml > 0)
+    return fail(PAWSIM_GPU_EUNSUPPORTED, "quadratic surface drag with hsml > 0 is not built");
   if (c.tau_nrecs < 1 || c.wdia_nrecs < 1) return fail(PAWSIM_GPU_EBADCONFIG, "record counts must be positive");
   if (c.solver < 0 || c.solver > 2) return fail(PAWSIM_GPU_EBADCONFIG, "Unknown pressureSolver identifier");
   Model* m = new Model();
@@ -381,6 +385,20 @@ static TendParams base_params(Model* m) {
   p.useA4 = (c.A4 > 0) || (c.A4smag > 0);
   p.A2 = c.A2;
   p.A4sqrt = sqrt(c.A4);
+  p.A4 = c.A4;
+  // Smagorinsky factors, as work.c:1587-1592 forms them
+  p.use_smag = (c.A2smag > 0 ? 1 : 0) | (c.A4smag > 0 ? 2 : 0);
+  {
+    const double mdx = fmax(m->dx, m->dy);
+    p.A2f = (c.A2smag * fmax(m->dx, m->dy) / 3.14159265358979323846) * (c.A2smag * fmax(m->dx, m->dy) / 3.14159265358979323846);
+    p.A4f = (c.A4smag / 3.14159265358979323846) * (c.A4smag / 3.14159265358979323846) * (mdx * mdx * mdx * mdx) / 8;
+  }
+  p.kt00_sigma = c.KT00_sigma;
+  p.quad_drag = c.quad_drag;
+  p.quad_drag_surf = c.quad_drag_surf;
+  p.wfb = c.wind_feedback ? 0.3 : 0.0;
+  p.use_fractions = (c.hsml > 0 || c.hbbl > 0) ? 1 : 0;
+  p.hsml = c.hsml; p.hmin_surf = c.hmin_surf; p.hbbl = c.hbbl; p.hmin_bot = c.hmin_bot;
   p.use_wind = c.use_wind; p.use_fbaro = c.use_fbaro;
   int n0, n1;
   record_weights(c.tau_nrecs, c.tau_period, m->t, &n0, &n1, &p.tw0, &p.tw1);

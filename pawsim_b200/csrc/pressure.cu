@@ -17,8 +17,16 @@ __device__ inline double ld_s(const double* f, const Grid2& g, int i, int j) {
   return load_mapped(f, g.pitch, i, j, g.Nx, g.Ny, g.wall_ew, g.wall_ns, MAP_S, MAP_S);
 }
 
-// Gathered face thickness with wrapped indices (work.c:865-1030), at an owned cell.
-__device__ inline double hw_gathered(const Grid2& g, const double* h, int i, int j) {
+// minmod of three slopes (defs.c:1000-1014): zero unless all share a sign, else the smallest
+__device__ inline double minmod3(double a, double b, double c) {
+  if ((a > 0) && (b > 0) && (c > 0)) return fmin(a, fmin(b, c));
+  if ((a < 0) && (b < 0) && (c < 0)) return fmax(a, fmax(b, c));
+  return 0;
+}
+
+// Gathered face thickness with wrapped indices (work.c:865-1030), at an owned cell; u, v are
+// the layer's velocities (the upwind schemes read their sign at the face).
+__device__ inline double hw_gathered(const Grid2& g, const double* h, const double* u, int i, int j) {
   int Nx = g.Nx, Ny = g.Ny;
   int im1 = i == 0 ? Nx - 1 : i - 1;
   int jm1 = j == 0 ? Ny - 1 : j - 1, jp1 = j + 1 == Ny ? 0 : j + 1;
@@ -31,11 +39,28 @@ __device__ inline double hw_gathered(const Grid2& g, const double* h, int i, int
       return (1.0 / 3) * (1.25 * (H(i, j) + H(im1, j)) + 0.25 * (H(i, jm1) + H(im1, jm1)));
     return (1.0 / 3) * (H(i, j) + H(im1, j) + 0.25 * (H(i, jp1) + H(im1, jp1) + H(i, jm1) + H(im1, jm1)));
   }
+  if (g.thick_scheme >= 2) {
+    const int im2 = im1 == 0 ? Nx - 1 : im1 - 1, ip1 = i + 1 == Nx ? 0 : i + 1;
+    const double uc = u[(size_t)j * P + i];
+    if (g.thick_scheme == 2) {
+      // UP3 (work.c:600-629): centred mean minus a sixth of the upwind second difference
+      const double d2m = H(i, j) - 2 * H(im1, j) + H(im2, j);
+      const double d2c = H(ip1, j) - 2 * H(i, j) + H(im1, j);
+      return 0.5 * (H(i, j) + H(im1, j)) - (1 / 6.0) * ((uc > 0) ? d2m : d2c);
+    }
+    // KT00 (work.c:630-684): limited linear reconstruction from the upwind side
+    const double s = g.kt00_sigma;
+    const double dm = minmod3(s * (H(i, j) - H(im1, j)), 0.5 * (H(i, j) - H(im2, j)), s * (H(im1, j) - H(im2, j)));
+    const double dc = minmod3(s * (H(ip1, j) - H(i, j)), 0.5 * (H(ip1, j) - H(im1, j)), s * (H(i, j) - H(im1, j)));
+    const double xm = H(im1, j) + 0.5 * dm;
+    const double xp = H(i, j) - 0.5 * dc;
+    return (uc > 0) ? xm : xp;
+  }
   return 0.5 * (H(i, j) + H(im1, j));
 }
 
-__device__ inline double hs_gathered(const Grid2& g, const double* h, int i, int j) {
-  int Nx = g.Nx;
+__device__ inline double hs_gathered(const Grid2& g, const double* h, const double* v, int i, int j) {
+  int Nx = g.Nx, Ny = g.Ny;
   int im1 = i == 0 ? Nx - 1 : i - 1, ip1 = i + 1 == Nx ? 0 : i + 1;
   int jm1 = j == 0 ? g.Ny - 1 : j - 1;
   const int P = g.pitch;
@@ -46,19 +71,34 @@ __device__ inline double hs_gathered(const Grid2& g, const double* h, int i, int
       return (1.0 / 3) * (1.25 * (H(i, j) + H(i, jm1)) + 0.25 * (H(im1, j) + H(im1, jm1)));
     return (1.0 / 3) * (H(i, j) + H(i, jm1) + 0.25 * (H(ip1, j) + H(im1, j) + H(ip1, jm1) + H(im1, jm1)));
   }
+  if (g.thick_scheme >= 2) {
+    const int jm2 = jm1 == 0 ? Ny - 1 : jm1 - 1, jp1 = j + 1 == Ny ? 0 : j + 1;
+    const double vc = v[(size_t)j * P + i];
+    if (g.thick_scheme == 2) {
+      const double d2m = H(i, j) - 2 * H(i, jm1) + H(i, jm2);
+      const double d2c = H(i, jp1) - 2 * H(i, j) + H(i, jm1);
+      return 0.5 * (H(i, j) + H(i, jm1)) - (1 / 6.0) * ((vc > 0) ? d2m : d2c);
+    }
+    const double s = g.kt00_sigma;
+    const double dm = minmod3(s * (H(i, j) - H(i, jm1)), 0.5 * (H(i, j) - H(i, jm2)), s * (H(i, jm1) - H(i, jm2)));
+    const double dc = minmod3(s * (H(i, jp1) - H(i, j)), 0.5 * (H(i, jp1) - H(i, jm1)), s * (H(i, j) - H(i, jm1)));
+    const double ym = H(i, jm1) + 0.5 * dm;
+    const double yp = H(i, j) + 0.5 * dc;   // the reference adds the half slope on this side too
+    return (vc > 0) ? ym : yp;
+  }
   return 0.5 * (H(i, j) + H(i, jm1));
 #undef H
 }
 
 // the gathered face arrays are scalar-filled afterwards: a face one past the last cell
 // copies the last face on a wall and the first face when periodic (field.c:121-241)
-__device__ inline double hw_face(const Grid2& g, const double* h, int i, int j) {
+__device__ inline double hw_face(const Grid2& g, const double* h, const double* u, int i, int j) {
   if (i >= g.Nx) i = g.wall_ew ? 2 * g.Nx - i - 1 : i - g.Nx;
-  return hw_gathered(g, h, i, j);
+  return hw_gathered(g, h, u, i, j);
 }
-__device__ inline double hs_face(const Grid2& g, const double* h, int i, int j) {
+__device__ inline double hs_face(const Grid2& g, const double* h, const double* v, int i, int j) {
   if (j >= g.Ny) j = g.wall_ns ? 2 * g.Ny - j - 1 : j - g.Ny;
-  return hs_gathered(g, h, i, j);
+  return hs_gathered(g, h, v, i, j);
 }
 
 __device__ inline double ld_u(const Grid2& g, const double* u, int i, int j) {
@@ -91,10 +131,10 @@ __global__ void rhs_kernel(const Grid2 g, const double* __restrict__ u, const do
       hv_s = vk[c] * (0.5 * (hc + hk[c - P]));
       hv_n = vk[c + P] * (0.5 * (hk[c + P] + hc));
     } else {
-      hu_w = ld_u(g, uk, i, j) * hw_face(g, hk, i, j);
-      hu_e = ld_u(g, uk, i + 1, j) * hw_face(g, hk, i + 1, j);
-      hv_s = ld_v(g, vk, i, j) * hs_face(g, hk, i, j);
-      hv_n = ld_v(g, vk, i, j + 1) * hs_face(g, hk, i, j + 1);
+      hu_w = ld_u(g, uk, i, j) * hw_face(g, hk, uk, i, j);
+      hu_e = ld_u(g, uk, i + 1, j) * hw_face(g, hk, uk, i + 1, j);
+      hv_s = ld_v(g, vk, i, j) * hs_face(g, hk, vk, i, j);
+      hv_n = ld_v(g, vk, i, j + 1) * hs_face(g, hk, vk, i, j + 1);
     }
     if (with_dt)
       acc += div_rn(hu_e - hu_w, dxdt, g.rdxdt) + div_rn(hv_n - hv_s, dydt, g.rdydt);

@@ -14,6 +14,7 @@ struct Grid2 {
   double dx, dy, dt;
   int thick_scheme;
   double rdx, rdy, rdxdt, rdydt;   // reciprocals rounded to nearest, for div_rn
+  double kt00_sigma;               // KT00 slope-limiter factor (thick_scheme 3)
 };
 
 // rhs = sum_k div(h_k u_k) / dt with the gathered face thickness (pressure.c:570-606)

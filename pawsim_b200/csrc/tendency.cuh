@@ -31,13 +31,22 @@ struct TendParams {
   double h0;
   double A2, A4sqrt;
   int useA2, useA4;
+  // Smagorinsky coefficients (work.c:1587-1610): A2f * |D|, A4f * |D| with floors A2, A4
+  int use_smag;
+  double A2f, A4f, A4;
+  double kt00_sigma;              // KT00 slope limiter (thickness scheme 3)
   // forcing (model_code/forcing.c)
   int use_wind, use_fbaro;
   const double *taux0, *taux1, *tauy0, *tauy1;
   double tw0, tw1;
   const double *fbx, *fby;
   double lin_drag, lin_drag_surf;
+  double quad_drag, quad_drag_surf;   // quadratic bottom / surface drag coefficients
+  double wfb;                         // wind feedback: 0.3 when windFeedback, else 0
   int ocean_surf_drag;
+  // surface / bottom layer fractions (work.c:2151-2340); off when both depths are <= 0
+  int use_fractions;
+  double hsml, hmin_surf, hbbl, hmin_bot;
   const double *uLid, *vLid;
   // restoring and diapycnal (model_code/restoring.c, diapycnal.c)
   int use_relax, use_wdia, use_wdia_file, use_diavisc;
