@@ -668,28 +668,39 @@ __global__ void loop_finalize_kernel(LoopState* st, cudaGraphConditionalHandle h
 
 // FP64 defect step of the mixed-precision solve: pi_new = pi - e32 (when `correct`), the
 // residual L(pi_new) - rhs stored as FP32 on the fine FP32 level, and the stopping measure
-// of pi_new. pi_new goes to `out` and is copied back by commit_kernel.
-__global__ void defect_kernel(LV<double> l, const float* __restrict__ e32, int p32, float* r32, double* out,
-                              int correct, unsigned long long* bits) {
+// of pi_new. pi ping-pongs between two arrays: cycle i reads `a` and writes `b` when i is
+// even, the other way round when odd (i = *iter_dev, the device cycle count, or iter_host),
+// so no copy-back pass is needed. Osum and 1/Osum are formed from the face coefficients
+// already loaded (same sums and the same IEEE division as the stored arrays).
+__global__ void defect_kernel(LV<double> l, double* a, double* b, const int* iter_dev, int iter_host,
+                              const float* __restrict__ e32, int p32, float* r32, int correct,
+                              unsigned long long* bits) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int it = iter_dev ? *iter_dev : iter_host;
+  const double* pin = (it & 1) ? b : a;
+  double* pout = (it & 1) ? a : b;
   double m = 0;
   if (i < l.Nx && j < l.Ny) {
     int ip1 = i + 1 == l.Nx ? 0 : i + 1, im1 = i == 0 ? l.Nx - 1 : i - 1;
     int jp1 = j + 1 == l.Ny ? 0 : j + 1, jm1 = j == 0 ? l.Ny - 1 : j - 1;
-    auto P = [&](int a, int b) {
-      double v = l.e[IX(l, a, b)];
-      if (correct) v -= (double)e32[(size_t)b * p32 + a];
+    auto P = [&](int x, int y) {
+      double v = pin[IX(l, x, y)];
+      if (correct) v -= (double)e32[(size_t)y * p32 + x];
       return v;
     };
+    const size_t c = IX(l, i, j);
+    const double ow = l.Ow[c], oe = l.Ow[IX(l, ip1, j)], os = l.Os[c], on = l.Os[IX(l, i, jp1)];
+    const double osum = ow + oe + os + on;
+    double ro = 1 / osum;
+    if (!isfinite(ro)) ro = 0;
     double pc = P(i, j);
-    double s = l.Os[IX(l, i, jp1)] * P(i, jp1) + l.Os[IX(l, i, j)] * P(i, jm1)
-             + l.Ow[IX(l, ip1, j)] * P(ip1, j) + l.Ow[IX(l, i, j)] * P(im1, j);
-    size_t c = IX(l, i, j);
-    m = fabs(pc - l.rOsum[c] * (s - l.rhs[c]));
+    double s = on * P(i, jp1) + os * P(i, jm1) + oe * P(ip1, j) + ow * P(im1, j);
+    const double rh = l.rhs[c];
+    m = fabs(pc - ro * (s - rh));
     if (m != m) m = 0;
-    r32[(size_t)j * p32 + i] = (float)(s - l.Osum[c] * pc - l.rhs[c]);
-    if (correct) out[c] = pc;
+    r32[(size_t)j * p32 + i] = (float)(s - osum * pc - rh);
+    if (correct) pout[c] = pc;
   }
   block_max_to(m, bits);
 }
@@ -1037,11 +1048,11 @@ int Multigrid::build_graph(int prec) {
   } else {
     enqueue_vcycle<float>(cap_, nullptr);
     LV<double> f = view<double>(F);
-    defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, cap_>>>(f, F.e32, F.pitch, F.rhs32, F.res, 1, &st->bits);
-    commit_kernel<<<g2(f.Nx, f.Ny), B2, 0, cap_>>>(F.e, F.res, F.Nx, F.Ny, F.pitch);
+    defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, cap_>>>(f, F.e, F.res, &st->iters, 0, F.e32, F.pitch, F.rhs32, 1,
+                                                   &st->bits);
   }
   loop_finalize_kernel<<<1, 1, 0, cap_>>>(st, g_->handle[prec]);
-  body_launches_[prec] = (int)(g_launches - counted) + (prec ? 3 : 1);   // + defect, commit, finalize
+  body_launches_[prec] = (int)(g_launches - counted) + (prec ? 2 : 1);   // + defect, finalize
   g_launches = counted;
   if (cudaStreamEndCapture(cap_, &body) != cudaSuccess) return -1;
   if (cudaGraphInstantiate(&g_->exec[prec], G, 0) != cudaSuccess) return -1;
@@ -1113,7 +1124,7 @@ int Multigrid::solve(double* pi, int pitch, const double* rhs, int rhs_pitch, do
     double mres = tol + 1;
     if (prec == 1) {
       cudaMemsetAsync(&st->bits, 0, sizeof(unsigned long long), s_);
-      defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f, F.e32, F.pitch, F.rhs32, F.res, 0, &st->bits);
+      defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f, F.e, F.res, nullptr, 0, F.e32, F.pitch, F.rhs32, 0, &st->bits);
     }
     while (mres > tol && it < maxiters) {
       cudaMemsetAsync(&st->bits, 0, sizeof(unsigned long long), s_);
@@ -1121,8 +1132,8 @@ int Multigrid::solve(double* pi, int pitch, const double* rhs, int rhs_pitch, do
         enqueue_vcycle<double>(s_, &st->bits);
       } else {
         enqueue_vcycle<float>(s_, nullptr);
-        defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f, F.e32, F.pitch, F.rhs32, F.res, 1, &st->bits);
-        commit_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(F.e, F.res, F.Nx, F.Ny, F.pitch);
+        defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f, F.e, F.res, nullptr, it, F.e32, F.pitch, F.rhs32, 1,
+                                                     &st->bits);
       }
       unsigned long long b = 0;
       cudaMemcpyAsync(&b, &st->bits, sizeof(b), cudaMemcpyDeviceToHost, s_);
@@ -1130,6 +1141,9 @@ int Multigrid::solve(double* pi, int pitch, const double* rhs, int rhs_pitch, do
       memcpy(&mres, &b, sizeof(mres));
       ++it;
     }
+    // the last cycle wrote pi to the scratch array when its index was even
+    if (prec == 1 && it > 0 && ((it - 1) & 1) == 0)
+      commit_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(F.e, F.res, F.Nx, F.Ny, F.pitch);
     if (maxres_out) *maxres_out = mres;
     return it;
   }
@@ -1139,7 +1153,7 @@ int Multigrid::solve(double* pi, int pitch, const double* rhs, int rhs_pitch, do
   if (prec == 1) {
     Level& F = lv_.back();
     LV<double> f = view<double>(F);
-    defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f, F.e32, F.pitch, F.rhs32, F.res, 0, &st->bits);
+    defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f, F.e, F.res, nullptr, 0, F.e32, F.pitch, F.rhs32, 0, &st->bits);
     cudaMemsetAsync(&st->bits, 0, sizeof(unsigned long long), s_);
     ++g_launches;
   }
@@ -1147,6 +1161,13 @@ int Multigrid::solve(double* pi, int pitch, const double* rhs, int rhs_pitch, do
   LoopState h;
   cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s_);
   if (cudaStreamSynchronize(s_) != cudaSuccess) return -1;
+  if (prec == 1 && h.iters > 0 && ((h.iters - 1) & 1) == 0) {
+    // the last cycle wrote pi to the scratch array
+    Level& F = lv_.back();
+    commit_kernel<<<g2(F.Nx, F.Ny), B2, 0, s_>>>(F.e, F.res, F.Nx, F.Ny, F.pitch);
+    ++g_launches;
+    if (cudaStreamSynchronize(s_) != cudaSuccess) return -1;
+  }
   // kernels of the graph body, counted once per executed V-cycle
   g_launches += (long long)h.iters * body_launches_[prec];
   if (maxres_out) *maxres_out = h.maxres;
