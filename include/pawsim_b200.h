@@ -77,9 +77,10 @@ typedef struct pawsim_gpu_config
   /* 1: sums in the reference's serial order (bitwise parity), 0: fixed pairwise tree,
    * -1: serial order for grids of at most 65536 cells. */
   int serial_sums;
-  /* Tile shape of the multigrid's fused level kernels: 0 times every shape on each level
-   * when the solver is first used and keeps the fastest; 1..4 forces one shape. The
-   * shape changes only the speed, never the result. */
+  /* Shape of the multigrid's fused level kernels: 0 times every shape on each level
+   * when the solver is first used and keeps the fastest; 1..4 forces one tile shape
+   * (32x8, 32x16, 64x8, 64x16 cells), 5 the streamed strips (levels of at least 64 x 48
+   * cells). The shape changes only the speed, never the result. */
   int mg_tile;
 } pawsim_gpu_config;
 

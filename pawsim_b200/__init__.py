@@ -210,13 +210,19 @@ class Model:
                                              a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                              a.size))
 
-    def get(self, name: str, k: int = 0) -> np.ndarray:
+    def get(self, name: str, k: int = 0, out: np.ndarray | None = None) -> np.ndarray:
+        """Copy field `name` (layer or record k) to the host; `out` (C-contiguous float64 of
+        the field's shape, e.g. a view of pinned memory) receives it when given."""
         if name == "omegaz":
-            out = np.empty((self.Ny + 1, self.Nx + 1))
+            shape = (self.Ny + 1, self.Nx + 1)
         elif name == "gg":
-            out = np.empty(self.L)
+            shape = (self.L,)
         else:
-            out = np.empty((self.Ny, self.Nx))
+            shape = (self.Ny, self.Nx)
+        if out is None:
+            out = np.empty(shape)
+        elif out.shape != shape or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError(f"out must be C-contiguous float64 of shape {shape}")
         _check(self.lib.pawsim_gpu_get_field(self._h, name.encode(), k,
                                              out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                              out.size))

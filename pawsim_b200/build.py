@@ -21,6 +21,11 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC,-O3",
          "-Xcompiler", "-fvisibility=hidden"]
 SOURCES = ["api.cu", "tendency.cu", "pressure.cu", "mg.cu", "noalloc.cu", "nn.cu", "warmstart.cu", "dmg.cu"]
+# (object name, source, extra flags): the fused tendency kernel is built for two tile heights
+UNITS = [(s.replace(".cu", ""), s, []) for s in SOURCES] + [
+    ("tendency_ty8", "tendency_tile.cu", ["-DPAWSIM_TEND_TY=8"]),
+    ("tendency_ty16", "tendency_tile.cu", ["-DPAWSIM_TEND_TY=16"]),
+]
 DRIVER_SRC = os.path.join(HERE, "host", "pawsim_main.c")
 DRIVER = os.path.join(HERE, "bin", "PAWSIM_B200.exe")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
@@ -54,19 +59,25 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
 
 def build_lib(force: bool = False, verbose: bool = False) -> str:
-    srcs = [os.path.join(CSRC, s) for s in SOURCES]
+    srcs = sorted({os.path.join(CSRC, u[1]) for u in UNITS})
     deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     deps.append(os.path.join(os.path.dirname(HERE), "include", "pawsim_b200.h"))
     if not force and not _stale(LIB, deps):
         return LIB
-    objs = []
-    for s in srcs:
-        o = os.path.join(CSRC, os.path.basename(s).replace(".cu", ".o"))
-        cmd = [NVCC, *ARCH, *FLAGS, "-c", s, "-o", o]
+    cmds, objs = [], []
+    for name, src, extra in UNITS:
+        o = os.path.join(CSRC, name + ".o")
+        cmds.append([NVCC, *ARCH, *FLAGS, *extra, "-c", os.path.join(CSRC, src), "-o", o])
+        objs.append(o)
+    # translation units compile in parallel (the tendency kernels dominate the build time)
+    procs = []
+    for cmd in cmds:
         if verbose:
             print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
-        objs.append(o)
+        procs.append(subprocess.Popen(cmd))
+    failed = [c for c, p in zip(cmds, procs) if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
     cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
     if verbose:
         print(" ".join(cmd))

@@ -83,12 +83,14 @@ inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 // is within one ulp of x/d and r is the correctly rounded reciprocal, the remainder
 // x - q*d is exact and q + (x - q*d)*r rounds to x/d. The first correction makes q = x*r
 // faithful, the second rounds it. Zeros keep their sign; tiny, huge and non-finite
-// operands take the IEEE division. Checked against the hardware division bit for bit by
+// operands take the IEEE division. The range test reads the biased exponent of x from its
+// high word (integer instructions): 2^-899 <= |x| < 2^900, exponents 124..1922, take the
+// corrections. Checked against the hardware division bit for bit by
 // pawsim_gpu_check_division (tests/test_gpu_division.py).
 __device__ __forceinline__ double div_rn(double x, double d, double r) {
   double q = x * r;
-  double ax = fabs(x);
-  if (!(ax > 0x1p-900 && ax < 0x1p900)) return (x == 0) ? q : x / d;
+  const unsigned be = ((unsigned)__double2hiint(x) >> 20) & 0x7ffu;
+  if (be - 124u > 1922u - 124u) return (x == 0) ? q : x / d;
   double e = fma(-q, d, x);
   q = fma(e, r, q);
   e = fma(-q, d, x);

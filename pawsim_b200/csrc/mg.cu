@@ -107,6 +107,35 @@ __global__ void restrict_general_kernel(LV<T> f, LV<T> c) {
   c.e[IX(c, ic, jc)] = T(0);
 }
 
+// bilinear prolongation weights of fine cell (i, j) of an exact 2:1 transfer, including
+// the wall and corner overrides (multigrid.c:376-442): m/p = coarse point west/east (first
+// letter) and south/north (second letter) of the cell
+template <typename T>
+__device__ inline void prolong_weights(int i, int j, int fNx, int fNy, bool wew, bool wns, T& wmm, T& wpm, T& wmp,
+                                       T& wpp) {
+  const bool io = (i & 1) != 0, jo = (j & 1) != 0;
+  T ai = io ? T(0.75) : T(0.25), bi = io ? T(0.25) : T(0.75);
+  T aj = jo ? T(0.75) : T(0.25), bj = jo ? T(0.25) : T(0.75);
+  wmm = ai * aj;
+  wmp = ai * bj;
+  wpm = bi * aj;
+  wpp = bi * bj;
+  if (wns) {
+    if (j == 0) { wmm = 0; wpm = 0; wmp = ai; wpp = bi; }
+    if (j == fNy - 1) { wmp = 0; wpp = 0; wmm = ai; wpm = bi; }
+  }
+  if (wew) {
+    if (i == 0) { wmm = 0; wmp = 0; wpm = aj; wpp = bj; }
+    if (i == fNx - 1) { wpm = 0; wpp = 0; wmm = aj; wmp = bj; }
+  }
+  if (wns && wew) {
+    if (i == 0 && j == 0) { wmm = 0; wmp = 0; wpm = 0; wpp = 1; }
+    if (i == 0 && j == fNy - 1) { wmm = 0; wmp = 0; wpm = 1; wpp = 0; }
+    if (i == fNx - 1 && j == 0) { wmm = 0; wmp = 1; wpm = 0; wpp = 0; }
+    if (i == fNx - 1 && j == fNy - 1) { wmm = 1; wmp = 0; wpm = 0; wpp = 0; }
+  }
+}
+
 // bilinear prolongation weights and coarse indices of one fine cell (multigrid.c:376-442,
 // 827-932); returns the interpolated coarse correction
 template <typename T, typename Get>
@@ -119,24 +148,8 @@ __device__ inline T prolong_at(int i, int j, int fNx, int fNy, int cNx, int cNy,
     if (ip >= hx) ip -= hx;
     if (jp >= hy) jp -= hy;
     int im = ip == 0 ? hx - 1 : ip - 1, jm = jp == 0 ? hy - 1 : jp - 1;
-    const bool io = (i & 1) != 0, jo = (j & 1) != 0;
-    T ai = io ? T(0.75) : T(0.25), bi = io ? T(0.25) : T(0.75);
-    T aj = jo ? T(0.75) : T(0.25), bj = jo ? T(0.25) : T(0.75);
-    T wmm = ai * aj, wmp = ai * bj, wpm = bi * aj, wpp = bi * bj;
-    if (wns) {
-      if (j == 0) { wmm = 0; wpm = 0; wmp = ai; wpp = bi; }
-      if (j == fNy - 1) { wmp = 0; wpp = 0; wmm = ai; wpm = bi; }
-    }
-    if (wew) {
-      if (i == 0) { wmm = 0; wmp = 0; wpm = aj; wpp = bj; }
-      if (i == fNx - 1) { wpm = 0; wpp = 0; wmm = aj; wmp = bj; }
-    }
-    if (wns && wew) {
-      if (i == 0 && j == 0) { wmm = 0; wmp = 0; wpm = 0; wpp = 1; }
-      if (i == 0 && j == fNy - 1) { wmm = 0; wmp = 0; wpm = 1; wpp = 0; }
-      if (i == fNx - 1 && j == 0) { wmm = 0; wmp = 1; wpm = 0; wpp = 0; }
-      if (i == fNx - 1 && j == fNy - 1) { wmm = 1; wmp = 0; wpm = 0; wpp = 0; }
-    }
+    T wmm, wpm, wmp, wpp;
+    prolong_weights<T>(i, j, fNx, fNy, wew, wns, wmm, wpm, wmp, wpp);
     return wmm * ec(im, jm) + wpm * ec(ip, jm) + wmp * ec(im, jp) + wpp * ec(ip, jp);
   }
   double x = ((double)i + 0.5) * cNx / fNx - 0.5, y = ((double)j + 0.5) * cNy / fNy - 0.5, tx, ty;
@@ -430,9 +443,38 @@ __global__ void __launch_bounds__(NT) up_tile(LV<T> f, LV<T> c, T omega, int wew
   if constexpr (MEASURE) block_max_to(m, bits);
 }
 
-// tile shapes the autotuner chooses from (owned OX x OY cells, NT threads):
-// 0: 32x8/256, 1: 32x16/256, 2: 64x8/256, 3: 64x16/512
-constexpr int kNumTileShapes = 4;
+#include "mg_strip.cuh"
+
+// shapes the autotuner chooses from (tiles of owned OX x OY cells with NT threads, or
+// streamed strips): 0: 32x8/256, 1: 32x16/256, 2: 64x8/256, 3: 64x16/512, 4: strips
+constexpr int kNumTileShapes = 5;
+constexpr int kStripShape = 4;
+
+// strips need a few segments' worth of rows and at least one full strip of columns
+inline bool strip_ok(int Nx, int Ny) { return Nx >= 64 && Ny >= 48; }
+
+inline int num_sms() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+  }
+  return n;
+}
+
+struct StripGrid {
+  int S, nstrips, nsegs;
+  unsigned blocks;
+};
+inline StripGrid strip_grid(int Nx, int Ny) {
+  StripGrid g;
+  g.S = strip_rows(Nx, Ny, num_sms());
+  g.nstrips = (Nx + SP_OWN - 1) / SP_OWN;
+  g.nsegs = (Ny + g.S - 1) / g.S;
+  g.blocks = (unsigned)((g.nstrips * g.nsegs + SP_WARPS - 1) / SP_WARPS);
+  return g;
+}
 
 template <typename T, int OX, int OY, int NT>
 void set_tile_attrs() {
@@ -462,6 +504,9 @@ void launch_up_shape(const LV<T>& f, const LV<T>& c, T omega, int wew, int wns, 
 
 template <typename T>
 void set_all_tile_attrs() {
+  cudaFuncSetAttribute(down_strip<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)strip_smem_bytes<T>(false));
+  cudaFuncSetAttribute(up_strip<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)strip_smem_bytes<T>(true));
+  cudaFuncSetAttribute(up_strip<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)strip_smem_bytes<T>(true));
   set_tile_attrs<T, 32, 8, 256>();
   set_tile_attrs<T, 32, 16, 256>();
   set_tile_attrs<T, 64, 8, 256>();
@@ -470,22 +515,39 @@ void set_all_tile_attrs() {
 
 template <typename T>
 void launch_down(int shape, const LV<T>& f, const LV<T>& c, T omega, int zero_e, T* out, cudaStream_t s) {
+  if (shape == kStripShape && !strip_ok(f.Nx, f.Ny)) shape = 3;
   switch (shape) {
     case 0: launch_down_shape<T, 32, 8, 256>(f, c, omega, zero_e, out, s); break;
     case 1: launch_down_shape<T, 32, 16, 256>(f, c, omega, zero_e, out, s); break;
     case 2: launch_down_shape<T, 64, 8, 256>(f, c, omega, zero_e, out, s); break;
-    default: launch_down_shape<T, 64, 16, 512>(f, c, omega, zero_e, out, s); break;
+    case 3: launch_down_shape<T, 64, 16, 512>(f, c, omega, zero_e, out, s); break;
+    default: {
+      const StripGrid g = strip_grid(f.Nx, f.Ny);
+      down_strip<T><<<g.blocks, SP_WARPS * 32, strip_smem_bytes<T>(false), s>>>(f, c, omega, zero_e, out, g.S,
+                                                                                 g.nstrips, g.nsegs);
+    }
   }
 }
 
 template <typename T>
 void launch_up(int shape, const LV<T>& f, const LV<T>& c, T omega, int wew, int wns, unsigned long long* bits,
                T* out, cudaStream_t s) {
+  if (shape == kStripShape && !strip_ok(f.Nx, f.Ny)) shape = 3;
   switch (shape) {
     case 0: launch_up_shape<T, 32, 8, 256>(f, c, omega, wew, wns, bits, out, s); break;
     case 1: launch_up_shape<T, 32, 16, 256>(f, c, omega, wew, wns, bits, out, s); break;
     case 2: launch_up_shape<T, 64, 8, 256>(f, c, omega, wew, wns, bits, out, s); break;
-    default: launch_up_shape<T, 64, 16, 512>(f, c, omega, wew, wns, bits, out, s); break;
+    case 3: launch_up_shape<T, 64, 16, 512>(f, c, omega, wew, wns, bits, out, s); break;
+    default: {
+      const StripGrid g = strip_grid(f.Nx, f.Ny);
+      const size_t shm = strip_smem_bytes<T>(true);
+      if (bits)
+        up_strip<T, true><<<g.blocks, SP_WARPS * 32, shm, s>>>(f, c, omega, wew, wns, bits, out, g.S, g.nstrips,
+                                                               g.nsegs);
+      else
+        up_strip<T, false><<<g.blocks, SP_WARPS * 32, shm, s>>>(f, c, omega, wew, wns, bits, out, g.S, g.nstrips,
+                                                                g.nsegs);
+    }
   }
 }
 
@@ -999,6 +1061,7 @@ void Multigrid::tune(cudaStream_t s) {
     unsigned long long* mb = (n == top && sizeof(T) == 8) ? &st->bits : nullptr;
     float best = 1e30f;
     for (int k = 0; k < kNumTileShapes; ++k) {
+      if (k == kStripShape && !strip_ok(F.Nx, F.Ny)) continue;
       float ms = 0;
       for (int rep = 0; rep < 4; ++rep) {
         if (rep == 1) cudaEventRecord(ev[0], s);

@@ -22,7 +22,7 @@ struct MGOptions {
   int pre = 1, post = 1;   // red-black sweeps before and after the coarse correction
   double omega_rb = 1.0;   // smoother weight
   int full_mg = 0;         // use_fullMG: nested iteration from the coarsest level
-  int tile_shape = -1;     // fused level kernels: -1 autotune per level, 0..3 force a shape
+  int tile_shape = -1;     // fused level kernels: -1 autotune per level, 0..3 force a tile shape, 4 strips
 };
 
 class Multigrid {

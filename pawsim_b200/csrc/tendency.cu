@@ -1,847 +1,24 @@
-// tendency.cu -- fused layer tendency + Adams-Bashforth step (the K-tend kernel).
+// tendency.cu -- chooses the tile height of the fused tendency kernel (tendency_tile.cu).
 //
-// One CTA owns a TX x TY tile of cells for every layer. It replaces, for that tile, the
-// reference's whole derivative evaluation and state update:
-//   model_code/tendency.c:81-115 (pawsim_tendency_eval) with the stages of work.c
-//   (face thickness :566-684, eta :1173-1203, PV :1231-1288, PV coefficients :1294-1404,
-//   Bernoulli :1410-1512, momentum :1520-1857, thickness :1864-1941), restoring.c:29-220,
-//   diapycnal.c:72-291, forcing.c:30-395, and the AB1/AB2/AB3 update of
-//   integrator.c:15-198, plus the rigid-lid column correction of pressure.c:525-561.
-// Every intermediate lives in shared memory over exactly the region later stages read.
-// The halo exchanges of field.c become index maps at load time (common.cuh), and each
-// derived field is evaluated either directly at a ghost position (fields the reference
-// computes over its ghost ring) or at the mirrored owned position (fields the reference
-// re-fills after computing them), so results equal the reference's bit for bit. This
-// file is compiled with -fmad=false: no multiply-add is contracted, as in the reference's
-// x86-64 build.
-#include "common.cuh"
+// Both heights compute the same values; 32 x 16 tiles (512 threads) spend fewer halo
+// evaluations per owned cell than 32 x 8 tiles (256 threads) but hold twice the shared
+// memory. The taller tile is used while two of its CTAs still fit in one SM's shared memory.
+#include <cuda_runtime.h>
+
 #include "tendency.cuh"
 
 namespace pawsim {
 
-namespace {
-
-constexpr int TX = 32;
-constexpr int TY = 8;
-constexpr int NT = TX * TY;
-// tile halo: 2 cells cover TW81 + A2 + A4; the upwind thickness schemes (UP3, KT00) and the
-// Smagorinsky biharmonic coefficient reach one cell further
-template <int H>
-struct Geo {
-  static constexpr int RW = TX + 2 * H, RH = TY + 2 * H, RN = RW * RH;
-};
-enum { F_U, F_V, F_H, F_HW, F_HS, F_QQ, F_HQ, F_KE, F_HUU, F_HVV, F_DT, F_DS, F_U4, F_V4, F_NUM };
-// Smagorinsky coefficients (allocated only when used): A2 and sqrt(A4) at cells and q points
-enum { S_A2H, S_A2Q, S_A4H, S_A4Q, S_NUM };
-
-template <int HALO>
-struct Tile {
-  int X0, Y0;
-  int Nx, Ny;
-  bool wx, wy;
-  // raw coordinate of local index
-  __device__ int gx(int lx) const { return X0 - HALO + lx; }
-  __device__ int gy(int ly) const { return Y0 - HALO + ly; }
-  // raw position within the band that owned cells can reach (mirrors stay in the tile)
-  __device__ bool near(int lx, int ly) const {
-    int x = gx(lx), y = gy(ly);
-    return x >= -HALO && x < Nx + HALO && y >= -HALO && y < Ny + HALO;
-  }
-  // local index of the owned cell that a filled (mirror-symmetric) field copies at raw x
-  __device__ int mlx(int lx) const {
-    if (!wx) return lx;
-    int g = gx(lx);
-    if (g < 0) g = -g - 1;
-    else if (g >= Nx) g = 2 * Nx - g - 1;
-    return g - X0 + HALO;
-  }
-  __device__ int mly(int ly) const {
-    if (!wy) return ly;
-    int g = gy(ly);
-    if (g < 0) g = -g - 1;
-    else if (g >= Ny) g = 2 * Ny - g - 1;
-    return g - Y0 + HALO;
-  }
-};
-
-// tile accessor; RW is the row length of the instantiation in scope
-#define AT(arr, lx, ly) (arr)[(ly) * RW + (lx)]
-
-__device__ inline double sq(double x) { return x * x; }
-
-// PV interpolation coefficients (work.c:1294-1404) evaluated from qq in shared memory
-template <int MS, int RW> struct Coef {
-  const double* q;
-  double r24;
-  __device__ double D(double x) const { return div_rn(x, 24.0, r24); }
-  __device__ double Q(int x, int y) const { return AT(q, x, y); }
-  __device__ double alpha(int i, int j) const {
-    if (MS == 3)
-      return D(2 * Q(i + 1, j + 1) + 3 * Q(i, j + 1) + 2 * Q(i, j) + Q(i + 1, j) - Q(i, j + 2) - Q(i - 1, j + 1));
-    return D(2 * Q(i + 1, j + 1) + Q(i, j + 1) + 2 * Q(i, j) + Q(i + 1, j));
-  }
-  __device__ double beta(int i, int j) const {
-    if (MS == 3)
-      return D(3 * Q(i, j + 1) + 2 * Q(i - 1, j + 1) + Q(i - 1, j) + 2 * Q(i, j) - Q(i + 1, j + 1) - Q(i, j + 2));
-    return D(Q(i, j + 1) + 2 * Q(i - 1, j + 1) + Q(i - 1, j) + 2 * Q(i, j));
-  }
-  __device__ double gamma(int i, int j) const {
-    if (MS == 3)
-      return D(2 * Q(i, j + 1) + Q(i - 1, j + 1) + 2 * Q(i - 1, j) + 3 * Q(i, j) - Q(i, j - 1) - Q(i + 1, j));
-    return D(2 * Q(i, j + 1) + Q(i - 1, j + 1) + 2 * Q(i - 1, j) + Q(i, j));
-  }
-  __device__ double delta(int i, int j) const {
-    if (MS == 3)
-      return D(Q(i + 1, j + 1) + 2 * Q(i, j + 1) + 3 * Q(i, j) + 2 * Q(i + 1, j) - Q(i - 1, j) - Q(i, j - 1));
-    return D(Q(i + 1, j + 1) + 2 * Q(i, j + 1) + Q(i, j) + 2 * Q(i + 1, j));
-  }
-  __device__ double epsilon(int i, int j) const {
-    return D(Q(i + 1, j + 1) + Q(i, j + 1) - Q(i, j) - Q(i + 1, j));
-  }
-  __device__ double phi(int i, int j) const {
-    return D(-Q(i + 1, j + 1) + Q(i, j + 1) + Q(i, j) - Q(i + 1, j));
-  }
-  __device__ double lambda(int i, int j) const { return D(Q(i + 1, j) - Q(i - 1, j)); }
-  __device__ double mu(int i, int j) const { return D(Q(i, j - 1) - Q(i, j + 1)); }
-};
-
-__device__ inline double minmod3(double a, double b, double c) {
-  // defs.c:1000-1014: zero unless all three share a sign, else the smallest magnitude
-  if ((a > 0) && (b > 0) && (c > 0)) return fmin(a, fmin(b, c));
-  if ((a < 0) && (b < 0) && (c < 0)) return fmax(a, fmax(b, c));
-  return 0;
-}
-
-// face thickness of one layer at a local position (work.c:566-684): AL81 centred mean, HK83
-// weighted mean, UP3 mean minus a sixth of the upwind second difference, KT00 limited
-// reconstruction from the upwind side (the velocity's sign is read at the face)
-template <int TS, int RW>
-__device__ inline double face_west(const double* h, const double* u, double sig, int i, int j) {
-  if (TS == 1)
-    return (1.0 / 3) * (AT(h, i, j) + AT(h, i - 1, j)
-                        + 0.25 * (AT(h, i, j + 1) + AT(h, i - 1, j + 1) + AT(h, i, j - 1) + AT(h, i - 1, j - 1)));
-  if (TS == 2) {
-    const double d2m = AT(h, i, j) - 2 * AT(h, i - 1, j) + AT(h, i - 2, j);
-    const double d2c = AT(h, i + 1, j) - 2 * AT(h, i, j) + AT(h, i - 1, j);
-    return 0.5 * (AT(h, i, j) + AT(h, i - 1, j)) - (1 / 6.0) * ((AT(u, i, j) > 0) ? d2m : d2c);
-  }
-  if (TS == 3) {
-    const double dm = minmod3(sig * (AT(h, i, j) - AT(h, i - 1, j)), 0.5 * (AT(h, i, j) - AT(h, i - 2, j)),
-                              sig * (AT(h, i - 1, j) - AT(h, i - 2, j)));
-    const double dc = minmod3(sig * (AT(h, i + 1, j) - AT(h, i, j)), 0.5 * (AT(h, i + 1, j) - AT(h, i - 1, j)),
-                              sig * (AT(h, i, j) - AT(h, i - 1, j)));
-    const double xm = AT(h, i - 1, j) + 0.5 * dm;
-    const double xp = AT(h, i, j) - 0.5 * dc;
-    return (AT(u, i, j) > 0) ? xm : xp;
-  }
-  return 0.5 * (AT(h, i, j) + AT(h, i - 1, j));
-}
-template <int TS, int RW>
-__device__ inline double face_south(const double* h, const double* v, double sig, int i, int j) {
-  if (TS == 1)
-    return (1.0 / 3) * (AT(h, i, j) + AT(h, i, j - 1)
-                        + 0.25 * (AT(h, i + 1, j) + AT(h, i - 1, j) + AT(h, i + 1, j - 1) + AT(h, i - 1, j - 1)));
-  if (TS == 2) {
-    const double d2m = AT(h, i, j) - 2 * AT(h, i, j - 1) + AT(h, i, j - 2);
-    const double d2c = AT(h, i, j + 1) - 2 * AT(h, i, j) + AT(h, i, j - 1);
-    return 0.5 * (AT(h, i, j) + AT(h, i, j - 1)) - (1 / 6.0) * ((AT(v, i, j) > 0) ? d2m : d2c);
-  }
-  if (TS == 3) {
-    const double dm = minmod3(sig * (AT(h, i, j) - AT(h, i, j - 1)), 0.5 * (AT(h, i, j) - AT(h, i, j - 2)),
-                              sig * (AT(h, i, j - 1) - AT(h, i, j - 2)));
-    const double dc = minmod3(sig * (AT(h, i, j + 1) - AT(h, i, j)), 0.5 * (AT(h, i, j + 1) - AT(h, i, j - 1)),
-                              sig * (AT(h, i, j) - AT(h, i, j - 1)));
-    const double ym = AT(h, i, j - 1) + 0.5 * dm;
-    const double yp = AT(h, i, j) + 0.5 * dc;   // the reference adds the half slope on this side too
-    return (AT(v, i, j) > 0) ? ym : yp;
-  }
-  return 0.5 * (AT(h, i, j) + AT(h, i, j - 1));
-}
-
-// kinetic energy of the Bernoulli function (work.c:1437-1499)
-template <int MS, int RW>
-__device__ inline double kinetic(const double* u, const double* v, int i, int j) {
-  if (MS == 1) {
-    return (sq(AT(u, i + 1, j)) + sq(AT(u, i, j))
-            + 0.25 * (sq(AT(u, i + 1, j + 1)) + sq(AT(u, i, j + 1)) + sq(AT(u, i + 1, j - 1)) + sq(AT(u, i, j - 1)))
-            + sq(AT(v, i, j + 1)) + sq(AT(v, i, j))
-            + 0.25 * (sq(AT(v, i + 1, j + 1)) + sq(AT(v, i + 1, j)) + sq(AT(v, i - 1, j + 1)) + sq(AT(v, i - 1, j)))) / 6;
-  }
-  if (MS == 3) {
-    return 0.25 * ((2.0 / 3.0) * sq(AT(u, i, j))
-                   + (1.0 / 3.0) * sq(0.5 * (AT(u, i - 1, j) + AT(u, i + 1, j)))
-                   + (2.0 / 3.0) * sq(AT(u, i + 1, j))
-                   + (1.0 / 3.0) * sq(0.5 * (AT(u, i, j) + AT(u, i + 2, j)))
-                   + (2.0 / 3.0) * sq(AT(v, i, j))
-                   + (1.0 / 3.0) * sq(0.5 * (AT(v, i, j - 1) + AT(v, i, j + 1)))
-                   + (2.0 / 3.0) * sq(AT(v, i, j + 1))
-                   + (1.0 / 3.0) * sq(0.5 * (AT(v, i, j) + AT(v, i, j + 2))));
-  }
-  return (sq(AT(u, i + 1, j)) + sq(AT(u, i, j))) / 4 + (sq(AT(v, i, j + 1)) + sq(AT(v, i, j))) / 4;
-}
-
-__device__ inline double gload(const double* f, const TendParams& p, int gi, int gj, int kx, int ky) {
-  return load_mapped(f, p.pitch, gi, gj, p.Nx, p.Ny, p.wall_ew, p.wall_ns, kx, ky);
-}
-
-// face thickness of a layer at an owned cell, read from global memory (h, u, v of that layer;
-// ghost positions through the scalar / velocity maps)
-template <int TS>
-__device__ inline double gface_west(const TendParams& p, const double* h, const double* u, int i, int j) {
-  auto H = [&](int a, int b) { return gload(h, p, a, b, MAP_S, MAP_S); };
-  if (TS == 1)
-    return (1.0 / 3) * (H(i, j) + H(i - 1, j) + 0.25 * (H(i, j + 1) + H(i - 1, j + 1) + H(i, j - 1) + H(i - 1, j - 1)));
-  if (TS == 2 || TS == 3) {
-    const double uc = gload(u, p, i, j, MAP_N, MAP_S);
-    if (TS == 2) {
-      const double d2m = H(i, j) - 2 * H(i - 1, j) + H(i - 2, j);
-      const double d2c = H(i + 1, j) - 2 * H(i, j) + H(i - 1, j);
-      return 0.5 * (H(i, j) + H(i - 1, j)) - (1 / 6.0) * ((uc > 0) ? d2m : d2c);
-    }
-    const double sg = p.kt00_sigma;
-    const double dm = minmod3(sg * (H(i, j) - H(i - 1, j)), 0.5 * (H(i, j) - H(i - 2, j)), sg * (H(i - 1, j) - H(i - 2, j)));
-    const double dc = minmod3(sg * (H(i + 1, j) - H(i, j)), 0.5 * (H(i + 1, j) - H(i - 1, j)), sg * (H(i, j) - H(i - 1, j)));
-    return (uc > 0) ? H(i - 1, j) + 0.5 * dm : H(i, j) - 0.5 * dc;
-  }
-  return 0.5 * (H(i, j) + H(i - 1, j));
-}
-template <int TS>
-__device__ inline double gface_south(const TendParams& p, const double* h, const double* v, int i, int j) {
-  auto H = [&](int a, int b) { return gload(h, p, a, b, MAP_S, MAP_S); };
-  if (TS == 1)
-    return (1.0 / 3) * (H(i, j) + H(i, j - 1) + 0.25 * (H(i + 1, j) + H(i - 1, j) + H(i + 1, j - 1) + H(i - 1, j - 1)));
-  if (TS == 2 || TS == 3) {
-    const double vc = gload(v, p, i, j, MAP_S, MAP_N);
-    if (TS == 2) {
-      const double d2m = H(i, j) - 2 * H(i, j - 1) + H(i, j - 2);
-      const double d2c = H(i, j + 1) - 2 * H(i, j) + H(i, j - 1);
-      return 0.5 * (H(i, j) + H(i, j - 1)) - (1 / 6.0) * ((vc > 0) ? d2m : d2c);
-    }
-    const double sg = p.kt00_sigma;
-    const double dm = minmod3(sg * (H(i, j) - H(i, j - 1)), 0.5 * (H(i, j) - H(i, j - 2)), sg * (H(i, j - 1) - H(i, j - 2)));
-    const double dc = minmod3(sg * (H(i, j + 1) - H(i, j)), 0.5 * (H(i, j + 1) - H(i, j - 1)), sg * (H(i, j) - H(i, j - 1)));
-    return (vc > 0) ? H(i, j - 1) + 0.5 * dm : H(i, j) + 0.5 * dc;
-  }
-  return 0.5 * (H(i, j) + H(i, j - 1));
-}
-
-#ifndef PAWSIM_TEND_MINB
-#define PAWSIM_TEND_MINB 4
-#endif
-
-template <int MS, int TS, int H>
-__global__ void __launch_bounds__(NT, PAWSIM_TEND_MINB)
-tendency_kernel(const __grid_constant__ TendParams p) {
-  constexpr int RW = Geo<H>::RW, RH = Geo<H>::RH, RN = Geo<H>::RN;
-  extern __shared__ double smem[];
-  double* F[F_NUM];
-#pragma unroll
-  for (int f = 0; f < F_NUM; ++f) F[f] = smem + f * RN;
-  double* MMall = smem + F_NUM * RN;            // [L][RN]
-  double* WDall = MMall + p.L * RN;             // [L+1][RN] when use_wdia
-  double* SM = WDall + (p.use_wdia ? (p.L + 1) * RN : 0);   // [S_NUM][RN] when use_smag
-  double* FR = SM + (p.use_smag ? S_NUM * RN : 0);          // [4][L][NT] when use_fractions
-
-  const int tid = threadIdx.x;
-  Tile<H> t;
-  t.X0 = blockIdx.x * TX;
-  t.Y0 = blockIdx.y * TY;
-  t.Nx = p.Nx;
-  t.Ny = p.Ny;
-  t.wx = p.wall_ew;
-  t.wy = p.wall_ns;
-  const int L = p.L;
-  const double dx = p.dx, dy = p.dy, rdx = p.rdx, rdy = p.rdy, r24 = p.r24;
-  // tiles whose halo lies inside the domain read global memory without boundary maps
-  const bool inner = t.X0 - H >= 0 && t.X0 + TX + H <= p.Nx && t.Y0 - H >= 0 && t.Y0 + TY + H <= p.Ny;
-
-  // ---- column prologue over the Bernoulli region: eta, pp, Montgomery MM, wdia ----
-  for (int q = tid; q < RN; q += NT) {
-    int lx = q % RW, ly = q / RW;
-    if (lx < H - 1 || lx > TX + H - 1 || ly < H - 1 || ly > TY + H - 1) continue;
-    if (!t.near(lx, ly)) {
-      for (int k = 0; k < L; ++k) MMall[k * RN + q] = 0;
-      if (p.use_wdia)
-        for (int k = 0; k <= L; ++k) WDall[k * RN + q] = 0;
-      continue;
-    }
-    int gi = t.gx(lx), gj = t.gy(ly);
-    double hk[LMAX], eta[LMAX + 1];
-    const size_t gc = (size_t)gj * p.pitch + gi;
-    double hb = inner ? p.hhb[gc] : gload(p.hhb, p, gi, gj, MAP_S, MAP_S);
-    eta[L] = hb;
-    for (int k = L - 1; k >= 0; --k) {
-      hk[k] = inner ? p.h[k * p.lstride + gc] : gload(p.h + k * p.lstride, p, gi, gj, MAP_S, MAP_S);
-      eta[k] = eta[k + 1] + hk[k];
-    }
-    double pp = 0;
-    for (int k = 0; k < L; ++k) {
-      if (k == 0) pp = p.use_rl ? 0 : p.gg[0] * eta[0];
-      else pp = pp + p.gg[k] * eta[k];
-      double mm = pp;
-      if (p.h0 != 0) {
-        double h0 = p.h0, hc = hk[k];
-        mm -= p.geff[k] * (h0 * h0 * h0 * h0) / (hc * hc * hc) / 3;
-      }
-      MMall[k * RN + q] = mm;
-    }
-    if (p.use_wdia) {
-      double wd[LMAX + 1];
-      for (int k = 0; k <= L; ++k) {
-        if (p.use_wdia_file) {
-          wd[k] = p.ww0 * gload(p.wd0 + k * p.lstride, p, gi, gj, MAP_S, MAP_S)
-                + p.ww1 * gload(p.wd1 + k * p.lstride, p, gi, gj, MAP_S, MAP_S);
-        } else {
-          wd[k] = 0;
-        }
-      }
-      if (p.use_relax) {
-        double acc = 0;
-        double ht = gload(p.hTime, p, gi, gj, MAP_S, MAP_S);
-        for (int k = L - 1; k >= 0; --k) {
-          if (ht > 0) {
-            acc += (hk[k] - gload(p.hRelax + k * p.lstride, p, gi, gj, MAP_S, MAP_S)) / ht;
-            wd[k] += acc;
-          }
-          double et = gload(p.eTime + k * p.lstride, p, gi, gj, MAP_S, MAP_S);
-          if (et > 0) wd[k] += (eta[k] - gload(p.eRelax + k * p.lstride, p, gi, gj, MAP_S, MAP_S)) / et;
-        }
-      }
-      for (int k = 0; k <= L; ++k) WDall[k * RN + q] = wd[k];
-      if (p.wdia_out && lx >= H && lx < H + TX && ly >= H && ly < H + TY && gi < p.Nx && gj < p.Ny) {
-        for (int k = 0; k <= L; ++k) p.wdia_out[k * p.lstride + (size_t)gj * p.pitch + gi] = wd[k];
-      }
-    }
-  }
-
-  // per-thread output cell
-  const int tx = tid % TX, ty = tid / TX;
-  const int ox = tx + H, oy = ty + H;
-  const int gi = t.X0 + tx, gj = t.Y0 + ty;
-  const bool valid = gi < p.Nx && gj < p.Ny;
-  const size_t cell = (size_t)gj * p.pitch + gi;
-  double hnew[LMAX];
-
-  // ---- surface and bottom layer fractions at the owned cell (work.c:2151-2340) ----
-  // FR[(f * L + k) * NT + tid], f = 0 hFsw, 1 hFss, 2 hFbw, 3 hFbs
-  if (p.use_fractions && valid) {
-    double hwk[LMAX], hsk[LMAX];
-    for (int k = 0; k < L; ++k) {
-      hwk[k] = gface_west<TS>(p, p.h + k * p.lstride, p.u + k * p.lstride, gi, gj);
-      hsk[k] = gface_south<TS>(p, p.h + k * p.lstride, p.v + k * p.lstride, gi, gj);
-    }
-    for (int f = 0; f < 4; ++f)
-      for (int k = 0; k < L; ++k) FR[(f * L + k) * NT + tid] = 0;
-    if (p.hsml <= 0) {
-      FR[(0 * L + 0) * NT + tid] = 1;
-      FR[(1 * L + 0) * NT + tid] = 1;
-    } else {
-      const double hsw = 0.5 * (gload(p.hhs, p, gi, gj, MAP_S, MAP_S) + gload(p.hhs, p, gi - 1, gj, MAP_S, MAP_S));
-      const double hss = 0.5 * (gload(p.hhs, p, gi, gj, MAP_S, MAP_S) + gload(p.hhs, p, gi, gj - 1, MAP_S, MAP_S));
-      double zw = hsw - p.hsml, zs = hss - p.hsml, ew = hsw, es = hss, sw = 0, ss = 0;
-      for (int k = 0; k < L; ++k) {
-        const double ewl = ew - hwk[k], esl = es - hsk[k];
-        if (sw < 1.0) {
-          zw -= fmin(p.hmin_surf, hwk[k]);
-          double he = fmax(ew, zw) - fmax(ewl, zw);
-          he = fmax(he - p.hmin_surf, 0.0);
-          const double fr = he / p.hsml;
-          FR[(0 * L + k) * NT + tid] = fr;
-          sw += fr;
-        }
-        if (ss < 1.0) {
-          zs -= fmin(p.hmin_surf, hsk[k]);
-          double he = fmax(es, zs) - fmax(esl, zs);
-          he = fmax(he - p.hmin_surf, 0.0);
-          const double fr = he / p.hsml;
-          FR[(1 * L + k) * NT + tid] = fr;
-          ss += fr;
-        }
-        ew = ewl;
-        es = esl;
-      }
-    }
-    if (p.hbbl <= 0) {
-      FR[(2 * L + L - 1) * NT + tid] = 1;
-      FR[(3 * L + L - 1) * NT + tid] = 1;
-    } else {
-      const double hbw = 0.5 * (gload(p.hhb, p, gi, gj, MAP_S, MAP_S) + gload(p.hhb, p, gi - 1, gj, MAP_S, MAP_S));
-      const double hbs = 0.5 * (gload(p.hhb, p, gi, gj, MAP_S, MAP_S) + gload(p.hhb, p, gi, gj - 1, MAP_S, MAP_S));
-      double zw = hbw + p.hbbl, zs = hbs + p.hbbl, ewl = hbw, esl = hbs, sw = 0, ss = 0;
-      for (int k = L; k > 0; --k) {
-        const int kk = k - 1;
-        const double ewu = ewl + hwk[kk], esu = esl + hsk[kk];
-        if (sw < 1.0) {
-          zw += fmin(p.hmin_bot, hwk[kk]);
-          double he = fmin(ewu, zw) - fmin(ewl, zw);
-          he = fmax(he - p.hmin_bot, 0.0);
-          const double fr = he / p.hbbl;
-          FR[(2 * L + kk) * NT + tid] = fr;
-          sw += fr;
-        }
-        if (ss < 1.0) {
-          zs += fmin(p.hmin_bot, hsk[kk]);
-          double he = fmin(esu, zs) - fmin(esl, zs);
-          he = fmax(he - p.hmin_bot, 0.0);
-          const double fr = he / p.hbbl;
-          FR[(3 * L + kk) * NT + tid] = fr;
-          ss += fr;
-        }
-        ewl = ewu;
-        esl = esu;
-      }
-    }
-  }
-
-  for (int k = 0; k < L; ++k) {
-    const double* uk = p.u + k * p.lstride;
-    const double* vk = p.v + k * p.lstride;
-    const double* hkp = p.h + k * p.lstride;
-    __syncthreads();
-    // ---- load the layer's u, v, h with the reference's ghost semantics ----
-    if (inner) {
-      for (int q = tid; q < RN; q += NT) {
-        int lx = q % RW, ly = q / RW;
-        size_t g = (size_t)t.gy(ly) * p.pitch + t.gx(lx);
-        F[F_U][q] = uk[g];
-        F[F_V][q] = vk[g];
-        F[F_H][q] = hkp[g];
-      }
-    } else {
-      for (int q = tid; q < RN; q += NT) {
-        int lx = q % RW, ly = q / RW;
-        int gx = t.gx(lx), gy = t.gy(ly);
-        bool in = gx >= -H && gx < p.Nx + H && gy >= -H && gy < p.Ny + H;
-        F[F_U][q] = in ? gload(uk, p, gx, gy, MAP_N, MAP_S) : 0.0;
-        F[F_V][q] = in ? gload(vk, p, gx, gy, MAP_S, MAP_N) : 0.0;
-        F[F_H][q] = in ? gload(hkp, p, gx, gy, MAP_S, MAP_S) : 0.0;
-      }
-    }
-    __syncthreads();
-    const double* su = F[F_U];
-    const double* sv = F[F_V];
-    const double* sh = F[F_H];
-    // ---- face thickness, PV, kinetic energy, deformation rates ----
-    for (int q = tid; q < RN; q += NT) {
-      int lx = q % RW, ly = q / RW;
-      const bool nr = t.near(lx, ly);
-      if (lx >= H - 1 && lx <= TX + H && ly >= H - 1 && ly <= TY + H && nr) {
-        int mx = t.mlx(lx), my = t.mly(ly);
-        F[F_HW][q] = face_west<TS, RW>(sh, su, p.kt00_sigma, mx, my);
-        F[F_HS][q] = face_south<TS, RW>(sh, sv, p.kt00_sigma, mx, my);
-      }
-      if (lx >= H - 1 && ly >= H - 1 && lx <= TX + H + 1 && ly <= TY + H + 1) {
-        // zeta, h on the q grid and q itself (work.c:1261-1270)
-        double z = div_rn(AT(su, lx, ly - 1) - AT(su, lx, ly), dy, rdy)
-                 + div_rn(AT(sv, lx, ly) - AT(sv, lx - 1, ly), dx, rdx);
-        double hq = 0.25 * (AT(sh, lx, ly) + AT(sh, lx - 1, ly - 1) + AT(sh, lx - 1, ly) + AT(sh, lx, ly - 1));
-        double om = inner ? p.omz[(size_t)t.gy(ly) * p.qpitch + t.gx(lx)]
-                          : load_mapped(p.omz, p.qpitch, t.gx(lx), t.gy(ly), p.Nx, p.Ny, p.wall_ew, p.wall_ns, MAP_Q, MAP_Q);
-        F[F_QQ][q] = (2 * om + z) / hq;
-        F[F_HQ][q] = hq;
-      }
-      if (lx >= H - 1 && lx <= TX + H - 1 && ly >= H - 1 && ly <= TY + H - 1) {
-        F[F_KE][q] = nr ? kinetic<MS, RW>(su, sv, t.mlx(lx), t.mly(ly)) : 0.0;
-      }
-      if (p.useA2 || p.useA4) {
-        if (lx >= H - 2 && lx <= RW - 2 && ly >= H - 2 && ly <= RH - 2)
-          F[F_DT][q] = div_rn(AT(su, lx + 1, ly) - AT(su, lx, ly), dx, rdx)
-                     - div_rn(AT(sv, lx, ly + 1) - AT(sv, lx, ly), dy, rdy);
-        if (lx >= 1 && ly >= 1 && lx >= H - 2 && ly >= H - 2)
-          F[F_DS][q] = div_rn(AT(su, lx, ly) - AT(su, lx, ly - 1), dy, rdy)
-                     + div_rn(AT(sv, lx, ly) - AT(sv, lx - 1, ly), dx, rdx);
-      }
-    }
-    __syncthreads();
-    const double* hw = F[F_HW];
-    const double* hs = F[F_HS];
-    const double* hq = F[F_HQ];
-    const double* DT = F[F_DT];
-    const double* DS = F[F_DS];
-    // ---- Smagorinsky coefficients from the deformation rates (work.c:1587-1610) ----
-    const double* A2h = SM + S_A2H * RN;
-    const double* A2q = SM + S_A2Q * RN;
-    const double* A4h = SM + S_A4H * RN;
-    const double* A4q = SM + S_A4Q * RN;
-    if (p.use_smag) {
-      for (int q = tid; q < RN; q += NT) {
-        int lx = q % RW, ly = q / RW;
-        // cells: A2 and sqrt(A4) from |D| at the cell centre
-        if (lx >= H - 2 && lx <= TX + H && ly >= H - 2 && ly <= TY + H && lx >= 1 && ly >= 1) {
-          const double DDh = sqrt(sq(AT(DT, lx, ly))
-                                  + sq(0.25 * (AT(DS, lx, ly) + AT(DS, lx + 1, ly) + AT(DS, lx, ly + 1) + AT(DS, lx + 1, ly + 1))));
-          SM[S_A2H * RN + q] = fmax(p.A2, p.A2f * DDh);
-          SM[S_A4H * RN + q] = sqrt(fmax(p.A4, p.A4f * DDh));
-        }
-        // q points
-        if (lx >= H - 1 && lx <= TX + H + 1 && ly >= H - 1 && ly <= TY + H + 1 && lx <= RW - 2 && ly <= RH - 2) {
-          const double DDq = sqrt(sq(0.25 * (AT(DT, lx, ly) + AT(DT, lx - 1, ly) + AT(DT, lx, ly - 1) + AT(DT, lx - 1, ly - 1)))
-                                  + sq(AT(DS, lx, ly)));
-          SM[S_A2Q * RN + q] = fmax(p.A2, p.A2f * DDq);
-          SM[S_A4Q * RN + q] = sqrt(fmax(p.A4, p.A4f * DDq));
-        }
-      }
-      __syncthreads();
-    }
-    // without its Smagorinsky term a coefficient is the constant itself (fmax(A, 0) = A and
-    // sqrt(fmax(A4, 0)) = sqrt(A4) in the reference)
-    const bool smag2 = (p.use_smag & 1) != 0, smag4 = (p.use_smag & 2) != 0;
-    auto A2H = [&](int x, int y) { return smag2 ? AT(A2h, x, y) : p.A2; };
-    auto A2Q = [&](int x, int y) { return smag2 ? AT(A2q, x, y) : p.A2; };
-    auto A4H = [&](int x, int y) { return smag4 ? AT(A4h, x, y) : p.A4sqrt; };
-    auto A4Q = [&](int x, int y) { return smag4 ? AT(A4q, x, y) : p.A4sqrt; };
-    // ---- mass fluxes and the biharmonic intermediate velocities ----
-    for (int q = tid; q < RN; q += NT) {
-      int lx = q % RW, ly = q / RW;
-      if (lx >= H - 1 && lx <= TX + H && ly >= H - 1 && ly <= TY + H - 1) F[F_HUU][q] = su[q] * hw[q];
-      if (lx >= H - 1 && lx <= TX + H - 1 && ly >= H - 1 && ly <= TY + H) F[F_HVV][q] = sv[q] * hs[q];
-      if (p.useA4 && lx >= H - 1 && lx <= TX + H && ly >= H - 1 && ly <= TY + H) {
-        F[F_U4][q] = (div_rn(A4H(lx, ly) * AT(sh, lx, ly) * AT(DT, lx, ly) - A4H(lx - 1, ly) * AT(sh, lx - 1, ly) * AT(DT, lx - 1, ly), dx, rdx)
-                      + div_rn(A4Q(lx, ly + 1) * AT(hq, lx, ly + 1) * AT(DS, lx, ly + 1) - A4Q(lx, ly) * AT(hq, lx, ly) * AT(DS, lx, ly), dy, rdy))
-                     / AT(hw, lx, ly);
-        F[F_V4][q] = (div_rn(A4Q(lx + 1, ly) * AT(hq, lx + 1, ly) * AT(DS, lx + 1, ly) - A4Q(lx, ly) * AT(hq, lx, ly) * AT(DS, lx, ly), dx, rdx)
-                      - div_rn(A4H(lx, ly) * AT(sh, lx, ly) * AT(DT, lx, ly) - A4H(lx, ly - 1) * AT(sh, lx, ly - 1) * AT(DT, lx, ly - 1), dy, rdy))
-                     / AT(hs, lx, ly);
-      }
-    }
-    __syncthreads();
-    if (!valid) continue;
-
-    const double* huu = F[F_HUU];
-    const double* hvv = F[F_HVV];
-    const double* KE = F[F_KE];
-    const double* MM = MMall + k * RN;
-    const double* U4 = F[F_U4];
-    const double* V4 = F[F_V4];
-    Coef<MS, RW> c{F[F_QQ], r24};
-    const double* qq = F[F_QQ];
-    const int i = ox, j = oy;
-    const double hwest = AT(hw, i, j), hsouth = AT(hs, i, j);
-    const double rhw = 1.0 / hwest, rhs = 1.0 / hsouth;   // reciprocals for div_rn
-    const double uc = AT(su, i, j), vc = AT(sv, i, j);
-
-    // ---- u momentum (work.c:1667-1752) ----
-    double ru;
-    {
-      double gM = div_rn(-(AT(MM, i, j) - AT(MM, i - 1, j)), dx, rdx);
-      double gK = div_rn(-(AT(KE, i, j) - AT(KE, i - 1, j)), dx, rdx);
-      double rq = 0;
-      if (MS == 0 || MS == 1) {
-        rq += c.alpha(i, j) * AT(hvv, i, j + 1) + c.beta(i, j) * AT(hvv, i - 1, j + 1)
-            + c.gamma(i, j) * AT(hvv, i - 1, j) + c.delta(i, j) * AT(hvv, i, j)
-            - c.epsilon(i, j) * AT(huu, i + 1, j) + c.epsilon(i - 1, j) * AT(huu, i - 1, j);
-      } else if (MS == 3) {
-        rq += c.alpha(i, j) * AT(hvv, i, j + 1) + c.beta(i, j) * AT(hvv, i - 1, j + 1)
-            + c.gamma(i, j) * AT(hvv, i - 1, j) + c.delta(i, j) * AT(hvv, i, j)
-            - c.epsilon(i, j) * AT(huu, i + 1, j) + c.epsilon(i - 1, j) * AT(huu, i - 1, j)
-            - c.lambda(i, j + 1) * AT(huu, i, j) + c.lambda(i, j) * AT(huu, i, j - 1);
-      } else {
-        rq += 0.25 * AT(qq, i, j) * (AT(hvv, i, j) + AT(hvv, i - 1, j))
-            + 0.25 * AT(qq, i, j + 1) * (AT(hvv, i, j + 1) + AT(hvv, i - 1, j + 1));
-      }
-      double a2 = 0, a4 = 0;
-      if (p.useA2) {
-        a2 = (div_rn(A2H(i, j) * AT(sh, i, j) * AT(DT, i, j) - A2H(i - 1, j) * AT(sh, i - 1, j) * AT(DT, i - 1, j), dx, rdx)
-              + div_rn(A2Q(i, j + 1) * AT(hq, i, j + 1) * AT(DS, i, j + 1) - A2Q(i, j) * AT(hq, i, j) * AT(DS, i, j), dy, rdy));
-      }
-      if (p.useA4) {
-        double d4t0 = div_rn(AT(U4, i + 1, j) - AT(U4, i, j), dx, rdx) - div_rn(AT(V4, i, j + 1) - AT(V4, i, j), dy, rdy);
-        double d4tm = div_rn(AT(U4, i, j) - AT(U4, i - 1, j), dx, rdx) - div_rn(AT(V4, i - 1, j + 1) - AT(V4, i - 1, j), dy, rdy);
-        double d4s1 = div_rn(AT(U4, i, j + 1) - AT(U4, i, j), dy, rdy) + div_rn(AT(V4, i, j + 1) - AT(V4, i - 1, j + 1), dx, rdx);
-        double d4s0 = div_rn(AT(U4, i, j) - AT(U4, i, j - 1), dy, rdy) + div_rn(AT(V4, i, j) - AT(V4, i - 1, j), dx, rdx);
-        a4 = -(div_rn(A4H(i, j) * AT(sh, i, j) * d4t0 - A4H(i - 1, j) * AT(sh, i - 1, j) * d4tm, dx, rdx)
-               + div_rn(A4Q(i, j + 1) * AT(hq, i, j + 1) * d4s1 - A4Q(i, j) * AT(hq, i, j) * d4s0, dy, rdy));
-      }
-      ru = gM + gK + rq + ((hwest != 0) ? div_rn(a2 + a4 + 0.0, hwest, rhw) : 0);
-    }
-    // ---- v momentum (work.c:1759-1852) ----
-    double rv;
-    {
-      double gM = div_rn(-(AT(MM, i, j) - AT(MM, i, j - 1)), dy, rdy);
-      double gK = div_rn(-(AT(KE, i, j) - AT(KE, i, j - 1)), dy, rdy);
-      double rq = 0;
-      if (MS == 0 || MS == 1) {
-        rq += c.phi(i, j - 1) * AT(hvv, i, j - 1) - c.phi(i, j) * AT(hvv, i, j + 1)
-            - c.gamma(i + 1, j) * AT(huu, i + 1, j) - c.delta(i, j) * AT(huu, i, j)
-            - c.alpha(i, j - 1) * AT(huu, i, j - 1) - c.beta(i + 1, j - 1) * AT(huu, i + 1, j - 1);
-      } else if (MS == 3) {
-        rq += c.phi(i, j - 1) * AT(hvv, i, j - 1) - c.phi(i, j) * AT(hvv, i, j + 1)
-            - c.gamma(i + 1, j) * AT(huu, i + 1, j) - c.delta(i, j) * AT(huu, i, j)
-            - c.alpha(i, j - 1) * AT(huu, i, j - 1) - c.beta(i + 1, j - 1) * AT(huu, i + 1, j - 1)
-            - c.mu(i + 1, j) * AT(hvv, i, j) + c.mu(i, j) * AT(hvv, i - 1, j);
-      } else {
-        rq -= 0.25 * AT(qq, i, j) * (AT(huu, i, j) + AT(huu, i, j - 1))
-            + 0.25 * AT(qq, i + 1, j) * (AT(huu, i + 1, j) + AT(huu, i + 1, j - 1));
-      }
-      double a2 = 0, a4 = 0;
-      if (p.useA2) {
-        a2 = (div_rn(A2Q(i + 1, j) * AT(hq, i + 1, j) * AT(DS, i + 1, j) - A2Q(i, j) * AT(hq, i, j) * AT(DS, i, j), dx, rdx)
-              - div_rn(A2H(i, j) * AT(sh, i, j) * AT(DT, i, j) - A2H(i, j - 1) * AT(sh, i, j - 1) * AT(DT, i, j - 1), dy, rdy));
-      }
-      if (p.useA4) {
-        double d4s1 = div_rn(AT(U4, i + 1, j) - AT(U4, i + 1, j - 1), dy, rdy) + div_rn(AT(V4, i + 1, j) - AT(V4, i, j), dx, rdx);
-        double d4s0 = div_rn(AT(U4, i, j) - AT(U4, i, j - 1), dy, rdy) + div_rn(AT(V4, i, j) - AT(V4, i - 1, j), dx, rdx);
-        double d4t0 = div_rn(AT(U4, i + 1, j) - AT(U4, i, j), dx, rdx) - div_rn(AT(V4, i, j + 1) - AT(V4, i, j), dy, rdy);
-        double d4tm = div_rn(AT(U4, i + 1, j - 1) - AT(U4, i, j - 1), dx, rdx) - div_rn(AT(V4, i, j) - AT(V4, i, j - 1), dy, rdy);
-        a4 = -(div_rn(A4Q(i + 1, j) * AT(hq, i + 1, j) * d4s1 - A4Q(i, j) * AT(hq, i, j) * d4s0, dx, rdx)
-               - div_rn(A4H(i, j) * AT(sh, i, j) * d4t0 - A4H(i, j - 1) * AT(sh, i, j - 1) * d4tm, dy, rdy));
-      }
-      rv = gM + gK + rq + ((hsouth != 0) ? div_rn(a2 + a4 + 0.0, hsouth, rhs) : 0);
-    }
-    // ---- diapycnal advection and viscosity (diapycnal.c:203-291) ----
-    if (p.use_wdia || p.use_diavisc) {
-      if (p.use_wdia) {
-        const double* W0 = WDall + k * RN;
-        const double* W1 = WDall + (k + 1) * RN;
-        double wu0 = 0.5 * (AT(W0, i, j) + AT(W0, i - 1, j));
-        double wu1 = 0.5 * (AT(W1, i, j) + AT(W1, i - 1, j));
-        double wv0 = 0.5 * (AT(W0, i, j) + AT(W0, i, j - 1));
-        double wv1 = 0.5 * (AT(W1, i, j) + AT(W1, i, j - 1));
-        double up = (k == 0) ? 0 : p.u[(k - 1) * p.lstride + cell];
-        double um = (k == L - 1) ? 0 : p.u[(k + 1) * p.lstride + cell];
-        double vp = (k == 0) ? 0 : p.v[(k - 1) * p.lstride + cell];
-        double vm = (k == L - 1) ? 0 : p.v[(k + 1) * p.lstride + cell];
-        // the wall face carries a zero tendency at the end, whatever is accumulated here
-        double dup = (wu0 > 0) ? 0 : up - uc;
-        double dum = (wu1 > 0) ? uc - um : 0;
-        double dvp = (wv0 > 0) ? 0 : vp - vc;
-        double dvm = (wv1 > 0) ? vc - vm : 0;
-        if (hwest != 0) ru += div_rn(-(wu0 * dup + wu1 * dum), hwest, rhw);
-        if (hsouth != 0) rv += div_rn(-(wv0 * dvp + wv1 * dvm), hsouth, rhs);
-      }
-      if (p.use_diavisc && L >= 2) {
-        double Fu[2] = {0, 0}, Fv[2] = {0, 0};
-        for (int s = 0; s < 2; ++s) {
-          int kk = k + s;                    // interface kk between layers kk-1 and kk
-          if (kk < 1 || kk > L - 1) continue;
-          double hwa = gface_west<TS>(p, p.h + (kk - 1) * p.lstride, p.u + (kk - 1) * p.lstride, gi, gj);
-          double hwb = gface_west<TS>(p, p.h + kk * p.lstride, p.u + kk * p.lstride, gi, gj);
-          double hsa = gface_south<TS>(p, p.h + (kk - 1) * p.lstride, p.v + (kk - 1) * p.lstride, gi, gj);
-          double hsb = gface_south<TS>(p, p.h + kk * p.lstride, p.v + kk * p.lstride, gi, gj);
-          double dzu = 0.5 * (hwb + hwa);
-          double dzv = 0.5 * (hsb + hsa);
-          double nuu = gload(p.nu_u + kk * p.lstride, p, gi, gj, MAP_N, MAP_S);
-          double nuv = gload(p.nu_v + kk * p.lstride, p, gi, gj, MAP_S, MAP_N);
-          double ua = gload(p.u + (kk - 1) * p.lstride, p, gi, gj, MAP_N, MAP_S);
-          double ub = gload(p.u + kk * p.lstride, p, gi, gj, MAP_N, MAP_S);
-          double va = gload(p.v + (kk - 1) * p.lstride, p, gi, gj, MAP_S, MAP_N);
-          double vb = gload(p.v + kk * p.lstride, p, gi, gj, MAP_S, MAP_N);
-          if (dzu != 0) Fu[s] = nuu * (ua - ub) / dzu;
-          if (dzv != 0) Fv[s] = nuv * (va - vb) / dzv;
-        }
-        if (hwest != 0) ru += div_rn(Fu[0] - Fu[1], hwest, rhw);
-        if (hsouth != 0) rv += div_rn(Fv[0] - Fv[1], hsouth, rhs);
-      }
-    }
-    // ---- forcing and drag (forcing.c:149-395) ----
-    {
-      const bool wface_u = p.wall_ew && gi == 0;
-      const bool wface_v = p.wall_ns && gj == 0;
-      // layer fractions: computed ones, or all to the top / bottom layer; zero on a wall face
-      double fsw, fss, fbw, fbs;
-      if (p.use_fractions) {
-        fsw = FR[(0 * L + k) * NT + tid];
-        fss = FR[(1 * L + k) * NT + tid];
-        fbw = FR[(2 * L + k) * NT + tid];
-        fbs = FR[(3 * L + k) * NT + tid];
-      } else {
-        fsw = fss = (k == 0) ? 1.0 : 0.0;
-        fbw = fbs = (k == L - 1) ? 1.0 : 0.0;
-      }
-      if (wface_u) fsw = fbw = 0.0;
-      if (wface_v) fss = fbs = 0.0;
-      if (p.use_wind) {
-        double tx_ = p.tw0 * p.taux0[cell] + p.tw1 * p.taux1[cell];
-        double ty_ = p.tw0 * p.tauy0[cell] + p.tw1 * p.tauy1[cell];
-        double r = tx_ * fsw;
-        if (hwest != 0) ru += div_rn(r, hwest, rhw);
-        r = ty_ * fss;
-        if (hsouth != 0) rv += div_rn(r, hsouth, rhs);
-      }
-      if (p.use_fbaro) {
-        ru += gload(p.fbx, p, gi, gj, MAP_N, MAP_S);
-        rv += gload(p.fby, p, gi, gj, MAP_S, MAP_N);
-      }
-      if (p.lin_drag > 0) {
-        if (hwest != 0) ru += div_rn(-p.lin_drag * uc * fbw, hwest, rhw);
-        if (hsouth != 0) rv += div_rn(-p.lin_drag * vc * fbs, hsouth, rhs);
-      }
-      // the surface drag is off under a rigid lid over land unless oceanSurfDrag
-      auto surf_mask_u = [&]() {
-        double hsw = 0.5 * (gload(p.hhs, p, gi, gj, MAP_S, MAP_S) + gload(p.hhs, p, gi - 1, gj, MAP_S, MAP_S));
-        return !p.ocean_surf_drag && p.use_rl && hsw >= 0;
-      };
-      auto surf_mask_v = [&]() {
-        double hss = 0.5 * (gload(p.hhs, p, gi, gj, MAP_S, MAP_S) + gload(p.hhs, p, gi, gj - 1, MAP_S, MAP_S));
-        return !p.ocean_surf_drag && p.use_rl && hss >= 0;
-      };
-      if (p.lin_drag_surf > 0) {
-        if (hwest != 0) {
-          double r = -p.lin_drag_surf * (uc - gload(p.uLid, p, gi, gj, MAP_N, MAP_S)) * fsw;
-          if (surf_mask_u()) r = 0;
-          ru += div_rn(r, hwest, rhw);
-        }
-        if (hsouth != 0) {
-          double r = -p.lin_drag_surf * (vc - gload(p.vLid, p, gi, gj, MAP_S, MAP_N)) * fss;
-          if (surf_mask_v()) r = 0;
-          rv += div_rn(r, hsouth, rhs);
-        }
-      }
-      // quadratic drag (forcing.c:95-143, 330-393): the speed at the cell centre from the
-      // squared bottom (surface) velocities of the neighbouring faces. Without layer
-      // fractions it acts on the bottom (top) layer alone, whose tile is in shared memory.
-      if (p.quad_drag > 0 && k == L - 1) {
-        auto uab = [&](int a, int b) {
-          return sqrt(0.5 * (sq(AT(su, a, b)) + sq(AT(su, a + 1, b))) + 0.5 * (sq(AT(sv, a, b)) + sq(AT(sv, a, b + 1))));
-        };
-        if (hwest != 0) {
-          const double ua = 0.5 * (uab(i, j) + uab(i - 1, j));
-          ru -= div_rn(p.quad_drag * ua * uc * fbw, hwest, rhw);
-        }
-        if (hsouth != 0) {
-          const double ua = 0.5 * (uab(i, j) + uab(i, j - 1));
-          rv -= div_rn(p.quad_drag * ua * vc * fbs, hsouth, rhs);
-        }
-      }
-      if (p.quad_drag_surf > 0 && k == 0) {
-        const double wf = 1.0 - p.wfb;
-        auto lidu = [&](int a, int b) { return gload(p.uLid, p, t.gx(a), t.gy(b), MAP_N, MAP_S); };
-        auto lidv = [&](int a, int b) { return gload(p.vLid, p, t.gx(a), t.gy(b), MAP_S, MAP_N); };
-        auto usq = [&](int a, int b) { const double r = wf * AT(su, a, b) - lidu(a, b); return r * r; };
-        auto vsq = [&](int a, int b) { const double r = wf * AT(sv, a, b) - lidv(a, b); return r * r; };
-        auto uab = [&](int a, int b) { return sqrt(0.5 * (usq(a, b) + usq(a + 1, b)) + 0.5 * (vsq(a, b) + vsq(a, b + 1))); };
-        if (hwest != 0) {
-          const double ua = 0.5 * (uab(i, j) + uab(i - 1, j));
-          double r = -p.quad_drag_surf * ua * (wf * uc - gload(p.uLid, p, gi, gj, MAP_N, MAP_S)) * fsw;
-          if (surf_mask_u()) r = 0;
-          ru += div_rn(r, hwest, rhw);
-        }
-        if (hsouth != 0) {
-          const double ua = 0.5 * (uab(i, j) + uab(i, j - 1));
-          double r = -p.quad_drag_surf * ua * (wf * vc - gload(p.vLid, p, gi, gj, MAP_S, MAP_N)) * fss;
-          if (surf_mask_v()) r = 0;
-          rv += div_rn(r, hsouth, rhs);
-        }
-      }
-    }
-    // ---- Newtonian velocity restoring (restoring.c:172-220) ----
-    if (p.use_relax) {
-      double ut = gload(p.uTime + k * p.lstride, p, gi, gj, MAP_N, MAP_S);
-      if (ut > 0) ru += (-(uc - gload(p.uRelax + k * p.lstride, p, gi, gj, MAP_N, MAP_S))) / ut;
-      double vt = gload(p.vTime + k * p.lstride, p, gi, gj, MAP_S, MAP_N);
-      if (vt > 0) rv += (-(vc - gload(p.vRelax + k * p.lstride, p, gi, gj, MAP_S, MAP_N))) / vt;
-    }
-    // the wall-normal tendency is zero on the wall face (field.c:173-176, 216-220)
-    if (p.wall_ew && gi == 0) ru = 0.0;
-    if (p.wall_ns && gj == 0) rv = 0.0;
-    // ---- thickness tendency (work.c:1875-1885) ----
-    double rh;
-    {
-      double adv = div_rn(AT(huu, i, j) - AT(huu, i + 1, j), dx, rdx) + div_rn(AT(hvv, i, j) - AT(hvv, i, j + 1), dy, rdy);
-      double rel = 0;
-      if (p.use_wdia) {
-        const double* W0 = WDall + k * RN;
-        const double* W1 = WDall + (k + 1) * RN;
-        rel = -(AT(W0, i, j) - AT(W1, i, j));
-      } else {
-        rel = -(0.0 - 0.0);
-      }
-      rh = adv + rel;
-    }
-    // ---- Adams-Bashforth epilogue (integrator.c:15-69) ----
-    const size_t o = k * p.lstride + cell;
-    if (p.ab_mode == 0) {
-      p.fu_out[o] = ru;
-      p.fv_out[o] = rv;
-      p.fh_out[o] = rh;
-      continue;
-    }
-    double un, vn, hn;
-    const double hc = sh[j * RW + i];
-    if (p.ab_mode == 1) {
-      un = uc + p.c0 * ru;
-      vn = vc + p.c0 * rv;
-      hn = hc + p.c0 * rh;
-    } else if (p.ab_mode == 2) {
-      un = uc + (p.c0 * ru - p.c1 * p.f1u[o]);
-      vn = vc + (p.c0 * rv - p.c1 * p.f1v[o]);
-      hn = hc + (p.c0 * rh - p.c1 * p.f1h[o]);
-    } else {
-      un = uc + (p.c0 * ru - p.c1 * p.f1u[o] + p.c2 * p.f2u[o]);
-      vn = vc + (p.c0 * rv - p.c1 * p.f1v[o] + p.c2 * p.f2v[o]);
-      hn = hc + (p.c0 * rh - p.c1 * p.f1h[o] + p.c2 * p.f2h[o]);
-    }
-    // after the update the reference re-imposes the wall face (field.c:173-176, 216-220)
-    if (p.wall_ew && gi == 0) un = 0.0;
-    if (p.wall_ns && gj == 0) vn = 0.0;
-    if (p.write_hist) {
-      p.fu_out[o] = ru;
-      p.fv_out[o] = rv;
-      p.fh_out[o] = rh;
-    }
-    p.u_out[o] = un;
-    p.v_out[o] = vn;
-    hnew[k] = hn;
-    if (!p.fuse_thickness_fix) p.h_out[o] = hn;
-  }
-
-  // ---- rigid-lid column thickness constraint (pressure.c:525-561) ----
-  if (p.ab_mode != 0 && p.fuse_thickness_fix && valid) {
-    double tot = 0;
-    for (int k = 0; k < L; ++k) tot += hnew[k];
-    if (tot != 0) {
-      double err = tot - p.Hc[cell];
-      for (int k = 0; k < L; ++k) hnew[k] *= (1 - err / tot);
-    }
-    for (int k = 0; k < L; ++k) p.h_out[k * p.lstride + cell] = hnew[k];
-  }
-}
-
-template <int MS, int TS, int H>
-int launch_t(const TendParams& p, cudaStream_t s) {
-  constexpr int RN = Geo<H>::RN;
-  size_t shm = (size_t)(F_NUM + p.L + (p.use_wdia ? p.L + 1 : 0) + (p.use_smag ? S_NUM : 0)) * RN * sizeof(double)
-             + (p.use_fractions ? (size_t)4 * p.L * NT * sizeof(double) : 0);
-  static bool attr_done = false;
-  if (!attr_done) {
-    cudaFuncSetAttribute(tendency_kernel<MS, TS, H>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_done = true;
-  }
-  if (shm > 200 * 1024) return -1;
-  dim3 grid((p.Nx + TX - 1) / TX, (p.Ny + TY - 1) / TY);
-  tendency_kernel<MS, TS, H><<<grid, NT, shm, s>>>(p);
-  return 0;
-}
-
-template <int TS, int H>
-int launch_ms(const TendParams& p, int ms, cudaStream_t s) {
-  switch (ms) {
-    case 0: return launch_t<0, TS, H>(p, s);
-    case 1: return launch_t<1, TS, H>(p, s);
-    case 2: return launch_t<2, TS, H>(p, s);
-    case 3: return launch_t<3, TS, H>(p, s);
-  }
-  return -1;
-}
-
-}  // namespace
+size_t tendency_smem_ty8(const TendParams& p, int ts);
+size_t tendency_smem_ty16(const TendParams& p, int ts);
+int launch_tendency_ty8(const TendParams& p, int ms, int ts, cudaStream_t s);
+int launch_tendency_ty16(const TendParams& p, int ms, int ts, cudaStream_t s);
 
 int launch_tendency(const TendParams& p, int ms, int ts, cudaStream_t s) {
-  if (p.L < 1 || p.L > LMAX) return -1;
-  // the upwind thickness schemes and the Smagorinsky biharmonic reach a third halo cell
-  const bool wide = ts >= 2 || (p.use_smag & 2);
-  if (!wide) {
-    if (ts == 0) return launch_ms<0, 2>(p, ms, s);
-    if (ts == 1) return launch_ms<1, 2>(p, ms, s);
-    return -1;
-  }
-  switch (ts) {
-    case 0: return launch_ms<0, 3>(p, ms, s);
-    case 1: return launch_ms<1, 3>(p, ms, s);
-    case 2: return launch_ms<2, 3>(p, ms, s);
-    case 3: return launch_ms<3, 3>(p, ms, s);
-  }
-  return -1;
+  // two CTAs per SM: 228 KB of shared memory, 1 KB reserved per CTA
+  constexpr size_t kTwoPerSM = 113 * 1024;
+  if (tendency_smem_ty16(p, ts) <= kTwoPerSM) return launch_tendency_ty16(p, ms, ts, s);
+  return launch_tendency_ty8(p, ms, ts, s);
 }
 
 }  // namespace pawsim

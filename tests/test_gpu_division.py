@@ -21,6 +21,10 @@ def test_division_matches_ieee():
     mant = rng.uniform(1.0, 2.0, n)
     expo = rng.integers(-200, 200, n)
     x = np.ldexp(mant, expo) * rng.choice([-1.0, 1.0], n)
+    # both ends of the range that takes the corrections (binary exponents -899 .. 899)
+    edge = np.ldexp(rng.uniform(1.0, 2.0, 4096), rng.integers(-903, -895, 4096))
+    edge = np.concatenate([edge, np.ldexp(rng.uniform(1.0, 2.0, 4096), rng.integers(895, 903, 4096))])
+    x = np.concatenate([x, edge, -edge, np.ldexp(1.0, np.arange(-905, 905))])
     divisors = [24.0, 3.0, 1953.125, 2000e3 / 128, 4000e3 / 1024, 977.0, 7812.5 * 900.0,
                 1000.0 + 1e-3, 3000.0 - 0.7, 0.1, 1.0 / 3.0, 123456.789]
     for d in divisors:

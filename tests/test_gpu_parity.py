@@ -108,15 +108,16 @@ def test_mg_tiled_levels_tolerance(tmp_path, oracle_mod, lib, fp32, kind, kw):
 @pytest.mark.parametrize("kind,kw", [
     ("gyre", dict(N=256, solver=1, tol=1e-12, dt=450.0)),
     ("channel", dict(Nx=256, Ny=128, solver=1, tol=1e-12, dt=150.0)),
+    ("jets", dict(N=256, solver=1, tol=1e-12, dt=100.0)),
     ("gyre", dict(N=1024, solver=1, tol=1e-11, dt=120.0)),
-], ids=["gyre256", "channel256x128", "gyre1024"])
+], ids=["gyre256", "channel256x128", "jets256", "gyre1024"])
 def test_mg_tile_shapes_identical(tmp_path, lib, fp32, kind, kw):
-    """Every tile shape of the fused multigrid level kernels, and the autotuned choice,
-    gives bit-identical states and iteration counts: the shape changes only the speed.
-    At 1024^2 every CTA of the persistent kernels walks several tiles."""
+    """Every shape of the fused multigrid level kernels (four tile shapes, the streamed
+    strips) and the autotuned choice give bit-identical states and iteration counts: the
+    shape changes only the speed. At 1024^2 the strips cover several segments per column."""
     _, cfg, f = make_setup(tmp_path, kind, **kw)
     runs = []
-    for tile in (0, 1, 2, 3, 4):
+    for tile in (0, 1, 2, 3, 4, 5):
         m = lib.Model(cfg, f, mg_fp32=fp32, mg_tile=tile)
         m.prelim()
         iters = [m.step(n)["iters"] for n in range(1, 5)]
