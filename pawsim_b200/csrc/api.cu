@@ -492,10 +492,10 @@ static int pressure_correct(Model* m, int update_diags, pawsim_gpu_stats* st) {
     ++g_launches;
   }
   m->thickness_fixed = false;
-  launch_pressure_rhs(g, m->u[cur], m->v[cur], m->h[cur], m->rhs, m->s);
+  g_launches += launch_pressure_rhs(g, m->u[cur], m->v[cur], m->h[cur], m->rhs, m->s);
   launch_sum(m->rhs, m->Nx, m->Ny, m->pitch, m->serial(), m->scratch, m->dsum, m->s);
   launch_subtract_mean(m->rhs, m->Nx, m->Ny, m->pitch, m->dsum, m->s);
-  g_launches += m->serial() ? 3 : 4;
+  g_launches += m->serial() ? 2 : 3;
   PAWSIM_CUDA_OK(cudaGetLastError());
   PAWSIM_CUDA_OK(cudaEventRecord(m->ev0, m->s));
   int iters = 0;
@@ -556,8 +556,7 @@ static int pressure_correct(Model* m, int update_diags, pawsim_gpu_stats* st) {
   launch_projection(g, m->pi, m->u[cur], m->v[cur], m->s);
   ++g_launches;
   if (m->c.pressure_timing) {
-    launch_divergence_field(g, m->u[cur], m->v[cur], m->h[cur], m->work, m->s);
-    ++g_launches;
+    g_launches += launch_divergence_field(g, m->u[cur], m->v[cur], m->h[cur], m->work, m->s);
     int r = finish_norms(m, m->work, &local.div_max, &local.div_rms);
     if (r) return r;
   }

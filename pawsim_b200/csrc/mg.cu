@@ -559,12 +559,14 @@ inline bool tile_ok(int Nx, int Ny, bool power2, int pre, int post) {
 
 // ---------------------------------------------------------------- coarse levels in one CTA
 
+}  // namespace
+
 constexpr int CMAX_LEVELS = 12;
-constexpr int CT = 1024;
 
 struct CoarseDesc {
   int n;                        // levels 0..n-1, index n-1 is the top of the block
   int Nx[CMAX_LEVELS], Ny[CMAX_LEVELS], pitch[CMAX_LEVELS], power2[CMAX_LEVELS];
+  int lgx[CMAX_LEVELS];         // log2(Nx) when Nx is a power of two, else -1
   int off[CMAX_LEVELS];         // offset of each level inside every smem array
   int total;                    // cells of all levels
   const void *Ow[CMAX_LEVELS], *Os[CMAX_LEVELS], *rO[CMAX_LEVELS];
@@ -572,8 +574,24 @@ struct CoarseDesc {
   void* top_e;                  // output correction of the top level
   int top_from_e;               // start the top level from top_e instead of zero
   int wew, wns, pre, post;
+  // tabulation mode: CTA b solves for the unit rhs at top cell b and writes the top
+  // correction as column b of the row-major unit_n x unit_n matrix unit_out
+  void* unit_out;
+  int unit_n;
 };
 
+namespace {
+
+constexpr int CT = 1024;
+
+// levels of at most this many cells run on one warp, with warp barriers between phases
+constexpr int CWARP_CELLS = 64;
+
+// The coarse levels of the V-cycle in one CTA, all in shared memory. Levels above
+// CWARP_CELLS cells run each phase (colour of a sweep, residual, restriction,
+// prolongation) on the whole block with a block barrier after it; the small levels at the
+// bottom of the cycle (down, coarsest, up) run on warp 0 alone with warp barriers, while
+// the other warps wait at one block barrier.
 template <typename T>
 __global__ void __launch_bounds__(CT) coarse_kernel(const __grid_constant__ CoarseDesc d, T omega) {
   extern __shared__ unsigned char sm_raw[];
@@ -596,10 +614,21 @@ __global__ void __launch_bounds__(CT) coarse_kernel(const __grid_constant__ Coar
       S[d.off[l] + q] = os[g];
       Q[d.off[l] + q] = ro[g];
       E[d.off[l] + q] = (l == d.n - 1 && d.top_from_e) ? ((const T*)d.top_e)[g] : T(0);
-      if (l == d.n - 1) R[d.off[l] + q] = ((const T*)d.top_rhs)[g];
+      if (l == d.n - 1)
+        R[d.off[l] + q] = d.unit_out ? T(q == (int)blockIdx.x ? 1 : 0) : ((const T*)d.top_rhs)[g];
     }
   }
   __syncthreads();
+  auto cell = [&](int l, int q, int& i, int& j) {
+    const int lg = d.lgx[l];
+    if (lg >= 0) {
+      i = q & ((1 << lg) - 1);
+      j = q >> lg;
+    } else {
+      i = q % d.Nx[l];
+      j = q / d.Nx[l];
+    }
+  };
   auto nsum = [&](int l, int i, int j) {
     int nx = d.Nx[l], ny = d.Ny[l], b = d.off[l];
     int ip1 = i + 1 == nx ? 0 : i + 1, im1 = i == 0 ? nx - 1 : i - 1;
@@ -607,33 +636,36 @@ __global__ void __launch_bounds__(CT) coarse_kernel(const __grid_constant__ Coar
     return S[b + jp1 * nx + i] * E[b + jp1 * nx + i] + S[b + j * nx + i] * E[b + jm1 * nx + i]
          + W[b + j * nx + ip1] * E[b + j * nx + ip1] + W[b + j * nx + i] * E[b + j * nx + im1];
   };
-  auto smooth = [&](int l, int sweeps) {
+  // the phases of one level, executed by threads q0, q0 + dq, ... with sync() after each
+  auto smooth = [&](int l, int sweeps, int q0, int dq, auto sync) {
     int nx = d.Nx[l], b = d.off[l], cnt = nx * d.Ny[l];
     for (int s = 0; s < sweeps; ++s)
       for (int color = 0; color < 2; ++color) {
-        for (int q = tid; q < cnt; q += CT) {
-          int i = q % nx, j = q / nx;
+        for (int q = q0; q < cnt; q += dq) {
+          int i, j;
+          cell(l, q, i, j);
           if (((i + j) & 1) != color) continue;
           T sm = nsum(l, i, j);
           E[b + q] = omega * Q[b + q] * (sm - R[b + q]) + (T(1) - omega) * E[b + q];
         }
-        __syncthreads();
+        sync();
       }
   };
-  // down
-  for (int l = d.n - 1; l >= 1; --l) {
-    smooth(l, d.pre);
+  auto down = [&](int l, int q0, int dq, auto sync) {
+    smooth(l, d.pre, q0, dq, sync);
     int nx = d.Nx[l], ny = d.Ny[l], b = d.off[l], cnt = nx * ny;
-    for (int q = tid; q < cnt; q += CT) {
-      int i = q % nx, j = q / nx;
+    for (int q = q0; q < cnt; q += dq) {
+      int i, j;
+      cell(l, q, i, j);
       int ip1 = i + 1 == nx ? 0 : i + 1, jp1 = j + 1 == ny ? 0 : j + 1;
       T osum = W[b + q] + W[b + j * nx + ip1] + S[b + q] + S[b + jp1 * nx + i];
       RES[q] = nsum(l, i, j) - osum * E[b + q] - R[b + q];
     }
-    __syncthreads();
+    sync();
     int cnx = d.Nx[l - 1], cny = d.Ny[l - 1], cb = d.off[l - 1];
-    for (int q = tid; q < cnx * cny; q += CT) {
-      int ic = q % cnx, jc = q / cnx;
+    for (int q = q0; q < cnx * cny; q += dq) {
+      int ic, jc;
+      cell(l - 1, q, ic, jc);
       T v;
       if (d.power2[l]) {
         const T* rr = RES + (2 * jc) * nx + 2 * ic;
@@ -644,32 +676,80 @@ __global__ void __launch_bounds__(CT) coarse_kernel(const __grid_constant__ Coar
       R[cb + q] = v;
       E[cb + q] = 0;
     }
-    __syncthreads();
-  }
-  // coarsest: a single cell carries no information (multigrid.c:472-476)
-  if (d.Nx[0] * d.Ny[0] == 1) {
-    if (tid == 0) E[d.off[0]] = 0;
-    __syncthreads();
-  } else {
-    smooth(0, d.pre + d.post);
-  }
-  // up
-  for (int l = 1; l < d.n; ++l) {
+    sync();
+  };
+  auto up = [&](int l, int q0, int dq, auto sync) {
     int nx = d.Nx[l], ny = d.Ny[l], b = d.off[l];
     int cnx = d.Nx[l - 1], cny = d.Ny[l - 1], cb = d.off[l - 1];
     auto ec = [&](int a, int bb) { return E[cb + bb * cnx + a]; };
-    for (int q = tid; q < nx * ny; q += CT) {
-      int i = q % nx, j = q / nx;
+    for (int q = q0; q < nx * ny; q += dq) {
+      int i, j;
+      cell(l, q, i, j);
       E[b + q] -= prolong_at<T>(i, j, nx, ny, cnx, cny, d.power2[l] != 0, d.wew, d.wns, ec);
     }
-    __syncthreads();
-    smooth(l, d.post);
+    sync();
+    smooth(l, d.post, q0, dq, sync);
+  };
+  auto block_sync = [] { __syncthreads(); };
+  auto warp_sync = [] { __syncwarp(); };
+  // levels 0..ls are small (level sizes grow with the index)
+  int ls = -1;
+  while (ls + 1 < d.n && d.Nx[ls + 1] * d.Ny[ls + 1] <= CWARP_CELLS) ++ls;
+  for (int l = d.n - 1; l > ls && l >= 1; --l) down(l, tid, CT, block_sync);
+  if (tid < 32) {
+    if (ls >= 0) {
+      for (int l = ls; l >= 1; --l) down(l, tid, 32, warp_sync);
+      // coarsest: a single cell carries no information (multigrid.c:472-476)
+      if (d.Nx[0] * d.Ny[0] == 1) {
+        if (tid == 0) E[d.off[0]] = 0;
+        __syncwarp();
+      } else {
+        smooth(0, d.pre + d.post, tid, 32, warp_sync);
+      }
+      for (int l = 1; l <= ls; ++l) up(l, tid, 32, warp_sync);
+    }
   }
+  __syncthreads();
+  if (ls < 0) smooth(0, d.pre + d.post, tid, CT, block_sync);   // a coarsest level above CWARP_CELLS
+  for (int l = (ls < 0 ? 1 : ls + 1); l < d.n; ++l) up(l, tid, CT, block_sync);
   int l = d.n - 1;
   for (int q = tid; q < d.Nx[l] * d.Ny[l]; q += CT) {
     int i = q % d.Nx[l], j = q / d.Nx[l];
-    ((T*)d.top_e)[(size_t)j * d.pitch[l] + i] = E[d.off[l] + q];
+    if (d.unit_out) ((T*)d.unit_out)[(size_t)q * d.unit_n + blockIdx.x] = E[d.off[l] + q];
+    else ((T*)d.top_e)[(size_t)j * d.pitch[l] + i] = E[d.off[l] + q];
   }
+}
+
+// The coarse block started from a zero correction is a linear map of the top level's rhs
+// (smoothing from zero, restriction and prolongation are linear): e_top = C rhs_top. C is
+// tabulated once by running coarse_kernel on every unit rhs, then each V-cycle applies it
+// as a matrix-vector product spread over the GPU (one warp per row, the rhs in shared
+// memory), instead of one CTA walking the coarse levels phase by phase.
+constexpr int CA_WARPS = 4;
+template <typename T>
+__global__ void __launch_bounds__(CA_WARPS * 32) coarse_apply_kernel(const T* __restrict__ C, int n, int Nx, int pitch,
+                                                                    const T* __restrict__ rhs, T* __restrict__ e) {
+  __shared__ T x[1024];
+  for (int q = threadIdx.x; q < n; q += CA_WARPS * 32) x[q] = rhs[(size_t)(q / Nx) * pitch + q % Nx];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int row = blockIdx.x * CA_WARPS + (threadIdx.x >> 5);
+  if (row >= n) return;
+  const T* c = C + (size_t)row * n;
+  // four independent partial sums so that the loads of a row are all in flight at once
+  T a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+  int k = lane;
+#pragma unroll 4
+  for (; k + 96 < n; k += 128) {
+    a0 += __ldg(c + k) * x[k];
+    a1 += __ldg(c + k + 32) * x[k + 32];
+    a2 += __ldg(c + k + 64) * x[k + 64];
+    a3 += __ldg(c + k + 96) * x[k + 96];
+  }
+  for (; k < n; k += 32) a0 += __ldg(c + k) * x[k];
+  T acc = (a0 + a1) + (a2 + a3);
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) e[(size_t)(row / Nx) * pitch + row % Nx] = acc;
 }
 
 // ---------------------------------------------------------------- stopping test and loop control
@@ -951,6 +1031,68 @@ Multigrid::~Multigrid() {
     cudaFree(L.e32); cudaFree(L.rhs32); cudaFree(L.res32);
   }
   cudaFree(dstate_);
+  cudaFree(cmat_[0]);
+  cudaFree(cmat_[1]);
+}
+
+template <typename T>
+CoarseDesc Multigrid::coarse_desc(void* unit_out) const {
+  CoarseDesc dd;
+  memset(&dd, 0, sizeof(dd));
+  CoarseDesc* d = &dd;
+  const int top = (int)lv_.size() - 1;
+  d->n = ctop_ + 1;
+  int total = 0;
+  for (int m = 0; m <= ctop_; ++m) {
+    const Level& L = lv_[m];
+    d->Nx[m] = L.Nx; d->Ny[m] = L.Ny; d->pitch[m] = L.pitch; d->power2[m] = L.power2 ? 1 : 0;
+    d->lgx[m] = -1;
+    for (int b = 0; b < 30; ++b)
+      if (L.Nx == (1 << b)) d->lgx[m] = b;
+    d->off[m] = total;
+    total += L.Nx * L.Ny;
+    if (sizeof(T) == 8) { d->Ow[m] = L.Ow; d->Os[m] = L.Os; d->rO[m] = L.rOsum; }
+    else { d->Ow[m] = L.Ow32; d->Os[m] = L.Os32; d->rO[m] = L.rOsum32; }
+  }
+  d->total = total;
+  const Level& Ltop = lv_[ctop_];
+  d->top_rhs = sizeof(T) == 8 ? (const void*)Ltop.rhs : (const void*)Ltop.rhs32;
+  d->top_e = sizeof(T) == 8 ? (void*)Ltop.e : (void*)Ltop.e32;
+  // when the coarse block is the whole problem, the FP64 solve iterates on pi itself
+  d->top_from_e = (ctop_ == top && sizeof(T) == 8) ? 1 : 0;
+  d->wew = wew_; d->wns = wns_; d->pre = opt_.pre; d->post = opt_.post;
+  d->unit_out = unit_out;
+  d->unit_n = Ltop.Nx * Ltop.Ny;
+  return dd;
+}
+
+template <typename T>
+size_t Multigrid::coarse_smem() const {
+  int total = 0;
+  for (int m = 0; m <= ctop_; ++m) total += lv_[m].Nx * lv_[m].Ny;
+  return (size_t)(5 * total + lv_[ctop_].Nx * lv_[ctop_].Ny) * sizeof(T);
+}
+
+// tabulate the coarse block's linear map for the current smoother options (once per
+// precision and option set; the tabulation runs the coarse kernel on every unit rhs)
+template <typename T>
+void Multigrid::tabulate_coarse(cudaStream_t s) {
+  const int p = sizeof(T) == 8 ? 0 : 1;
+  const int top = (int)lv_.size() - 1;
+  if (ctop_ == top) return;   // the coarse block is the whole problem: iterate on pi itself
+  if (cmat_[p] && cmat_pre_[p] == opt_.pre && cmat_post_[p] == opt_.post && cmat_omega_[p] == opt_.omega_rb)
+    return;
+  const int n = lv_[ctop_].Nx * lv_[ctop_].Ny;
+  if (!cmat_[p] && cudaMalloc(&cmat_[p], (size_t)n * n * sizeof(T)) != cudaSuccess) {
+    cmat_[p] = nullptr;
+    return;
+  }
+  // a set-up launch, like the autotuner's, not counted as a step of the solve
+  const CoarseDesc d = coarse_desc<T>(cmat_[p]);
+  coarse_kernel<T><<<n, CT, coarse_smem<T>(), s>>>(d, (T)opt_.omega_rb);
+  cmat_pre_[p] = opt_.pre;
+  cmat_post_[p] = opt_.post;
+  cmat_omega_[p] = opt_.omega_rb;
 }
 
 template <typename T>
@@ -979,29 +1121,18 @@ void Multigrid::enqueue_vcycle(cudaStream_t s, unsigned long long* measure_bits)
       g_launches += 2 * pre + 2;
     }
   }
-  // coarse block
+  // coarse block: the tabulated linear map when available, else the one-CTA kernel
   {
-    CoarseDesc d;
-    memset(&d, 0, sizeof(d));
-    d.n = ctop_ + 1;
-    int total = 0;
-    for (int m = 0; m <= ctop_; ++m) {
-      const Level& L = lv_[m];
-      d.Nx[m] = L.Nx; d.Ny[m] = L.Ny; d.pitch[m] = L.pitch; d.power2[m] = L.power2 ? 1 : 0;
-      d.off[m] = total;
-      total += L.Nx * L.Ny;
-      if (sizeof(T) == 8) { d.Ow[m] = L.Ow; d.Os[m] = L.Os; d.rO[m] = L.rOsum; }
-      else { d.Ow[m] = L.Ow32; d.Os[m] = L.Os32; d.rO[m] = L.rOsum32; }
-    }
-    d.total = total;
     const Level& Ltop = lv_[ctop_];
-    d.top_rhs = sizeof(T) == 8 ? (const void*)Ltop.rhs : (const void*)Ltop.rhs32;
-    d.top_e = sizeof(T) == 8 ? (void*)Ltop.e : (void*)Ltop.e32;
-    // when the coarse block is the whole problem, the FP64 solve iterates on pi itself
-    d.top_from_e = (ctop_ == top && sizeof(T) == 8) ? 1 : 0;
-    d.wew = wew_; d.wns = wns_; d.pre = pre; d.post = post;
-    size_t shm = (size_t)(5 * total + Ltop.Nx * Ltop.Ny) * sizeof(T);
-    coarse_kernel<T><<<1, CT, shm, s>>>(d, omega);
+    const CoarseDesc d = coarse_desc<T>(nullptr);
+    const T* C = static_cast<const T*>(cmat_[sizeof(T) == 8 ? 0 : 1]);
+    if (C && !d.top_from_e) {
+      const int n = Ltop.Nx * Ltop.Ny;
+      coarse_apply_kernel<T><<<(n + CA_WARPS - 1) / CA_WARPS, CA_WARPS * 32, 0, s>>>(
+          C, n, Ltop.Nx, Ltop.pitch, static_cast<const T*>(d.top_rhs), static_cast<T*>(d.top_e));
+    } else {
+      coarse_kernel<T><<<1, CT, coarse_smem<T>(), s>>>(d, omega);
+    }
     ++g_launches;
   }
   // up through the tiled levels; the finest FP64 up kernel also forms the stopping measure
@@ -1176,8 +1307,13 @@ int Multigrid::solve(double* pi, int pitch, const double* rhs, int rhs_pitch, do
   }
   set_fine(pi, rhs);
   LoopState* st = reinterpret_cast<LoopState*>(dstate_);
-  if (prec == 0) tune<double>(s_);
-  else tune<float>(s_);
+  if (prec == 0) {
+    tune<double>(s_);
+    tabulate_coarse<double>(s_);
+  } else {
+    tune<float>(s_);
+    tabulate_coarse<float>(s_);
+  }
   if (getenv("PAWSIM_MG_HOST_LOOP")) {
     // host-driven loop with the same kernels (for profilers that do not see inside the
     // conditional graph node)

@@ -17,6 +17,8 @@
 
 namespace pawsim {
 
+struct CoarseDesc;   // the coarse block's launch descriptor (mg.cu)
+
 struct MGOptions {
   int fp32_cycles = 0;     // 0: FP64 V-cycles, 1: FP32 V-cycles in FP64 defect correction
   int pre = 1, post = 1;   // red-black sweeps before and after the coarse correction
@@ -65,6 +67,13 @@ class Multigrid {
 
  private:
   template <typename T> void enqueue_vcycle(cudaStream_t s, unsigned long long* measure_bits);
+  template <typename T> CoarseDesc coarse_desc(void* unit_out) const;
+  template <typename T> size_t coarse_smem() const;
+  template <typename T> void tabulate_coarse(cudaStream_t s);
+  // the coarse block's linear map per precision (FP64, FP32) and the options it was made for
+  void* cmat_[2] = {nullptr, nullptr};
+  int cmat_pre_[2] = {-1, -1}, cmat_post_[2] = {-1, -1};
+  double cmat_omega_[2] = {-1, -1};
   template <typename T> void tune(cudaStream_t s);
   void set_fine(double* pi, const double* rhs);
   int build_graph(int prec);

@@ -68,10 +68,10 @@ extern "C" int pawsim_pressure_rhs_noalloc(const double* u, const double* v, con
   g.wall_ew = wall_ew; g.wall_ns = wall_ns; g.dx = dx; g.dy = dy; g.dt = dt; g.thick_scheme = thick_scheme;
   g.rdx = 1.0 / dx; g.rdy = 1.0 / dy; g.rdxdt = 1.0 / (dx * dt); g.rdydt = 1.0 / (dy * dt);
   bool serial = serial_sum == 1 || (serial_sum < 0 && (long long)Nx * Ny <= 65536);
-  launch_pressure_rhs(g, u, v, h, rhs, s);
+  g_launches += launch_pressure_rhs(g, u, v, h, rhs, s);
   launch_sum(rhs, Nx, Ny, pitch, serial, scratch + 1, scratch, s);
   launch_subtract_mean(rhs, Nx, Ny, pitch, scratch, s);
-  g_launches += serial ? 3 : 4;
+  g_launches += serial ? 2 : 3;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_cuda_error(e, "pawsim_pressure_rhs_noalloc", __FILE__, __LINE__);
   return 0;

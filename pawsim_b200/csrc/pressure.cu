@@ -108,40 +108,81 @@ __device__ inline double ld_v(const Grid2& g, const double* v, int i, int j) {
   return load_mapped(v, g.pitch, i, j, g.Nx, g.Ny, g.wall_ew, g.wall_ns, MAP_S, MAP_N);
 }
 
-__global__ void rhs_kernel(const Grid2 g, const double* __restrict__ u, const double* __restrict__ v,
-                           const double* __restrict__ h, double* __restrict__ rhs, int with_dt) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= g.Nx || j >= g.Ny) return;
+// divergence terms of one cell (all layers): the gathered face thickness of the thickness
+// scheme at every face, with the boundary maps
+__device__ double rhs_cell(const Grid2& g, const double* __restrict__ u, const double* __restrict__ v,
+                           const double* __restrict__ h, int i, int j, int with_dt) {
   double acc = 0;
-  double dxdt = g.dx * g.dt, dydt = g.dy * g.dt;
-  const bool inner = i > 0 && j > 0 && i + 1 < g.Nx && j + 1 < g.Ny && g.thick_scheme == 0;
-  const size_t c = (size_t)j * g.pitch + i;
+  const double dxdt = g.dx * g.dt, dydt = g.dy * g.dt;
   for (int k = 0; k < g.L; ++k) {
     const double* uk = u + k * g.lstride;
     const double* vk = v + k * g.lstride;
     const double* hk = h + k * g.lstride;
-    double hu_w, hu_e, hv_s, hv_n;
-    if (inner) {
-      // owned neighbours only: plain loads, AL81 face averages (work.c:889-901)
-      const size_t P = g.pitch;
-      double hc = hk[c];
-      hu_w = uk[c] * (0.5 * (hc + hk[c - 1]));
-      hu_e = uk[c + 1] * (0.5 * (hk[c + 1] + hc));
-      hv_s = vk[c] * (0.5 * (hc + hk[c - P]));
-      hv_n = vk[c + P] * (0.5 * (hk[c + P] + hc));
-    } else {
-      hu_w = ld_u(g, uk, i, j) * hw_face(g, hk, uk, i, j);
-      hu_e = ld_u(g, uk, i + 1, j) * hw_face(g, hk, uk, i + 1, j);
-      hv_s = ld_v(g, vk, i, j) * hs_face(g, hk, vk, i, j);
-      hv_n = ld_v(g, vk, i, j + 1) * hs_face(g, hk, vk, i, j + 1);
-    }
+    const double hu_w = ld_u(g, uk, i, j) * hw_face(g, hk, uk, i, j);
+    const double hu_e = ld_u(g, uk, i + 1, j) * hw_face(g, hk, uk, i + 1, j);
+    const double hv_s = ld_v(g, vk, i, j) * hs_face(g, hk, vk, i, j);
+    const double hv_n = ld_v(g, vk, i, j + 1) * hs_face(g, hk, vk, i, j + 1);
     if (with_dt)
       acc += div_rn(hu_e - hu_w, dxdt, g.rdxdt) + div_rn(hv_n - hv_s, dydt, g.rdydt);
     else
       acc += div_rn(hu_e - hu_w, g.dx, g.rdx) + div_rn(hv_n - hv_s, g.dy, g.rdy);
   }
-  rhs[(size_t)j * g.pitch + i] = acc;
+  return acc;
+}
+
+// cells whose four faces lie between owned cells, with the AL81 face average
+// (work.c:889-901): plain loads, no boundary maps; the border ring and the other thickness
+// schemes go through rhs_cell
+__global__ void rhs_inner_kernel(const Grid2 g, const double* __restrict__ u, const double* __restrict__ v,
+                                 const double* __restrict__ h, double* __restrict__ rhs, int with_dt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i < 1 || j < 1 || i + 1 >= g.Nx || j + 1 >= g.Ny) return;
+  const double dxdt = g.dx * g.dt, dydt = g.dy * g.dt;
+  const size_t c = (size_t)j * g.pitch + i;
+  const size_t P = g.pitch;
+  double acc = 0;
+#pragma unroll 2
+  for (int k = 0; k < g.L; ++k) {
+    const double* uk = u + k * g.lstride;
+    const double* vk = v + k * g.lstride;
+    const double* hk = h + k * g.lstride;
+    const double hc = hk[c];
+    const double hu_w = uk[c] * (0.5 * (hc + hk[c - 1]));
+    const double hu_e = uk[c + 1] * (0.5 * (hk[c + 1] + hc));
+    const double hv_s = vk[c] * (0.5 * (hc + hk[c - P]));
+    const double hv_n = vk[c + P] * (0.5 * (hk[c + P] + hc));
+    if (with_dt)
+      acc += div_rn(hu_e - hu_w, dxdt, g.rdxdt) + div_rn(hv_n - hv_s, dydt, g.rdydt);
+    else
+      acc += div_rn(hu_e - hu_w, g.dx, g.rdx) + div_rn(hv_n - hv_s, g.dy, g.rdy);
+  }
+  rhs[c] = acc;
+}
+
+// every cell (all thickness schemes), or with `border` only the outermost ring of cells,
+// enumerated as rows 0 and Ny-1, then columns 0 and Nx-1 of the rows between
+__global__ void rhs_kernel(const Grid2 g, const double* __restrict__ u, const double* __restrict__ v,
+                           const double* __restrict__ h, double* __restrict__ rhs, int with_dt, int border) {
+  int i, j;
+  if (border) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int rows = g.Ny > 1 ? 2 * g.Nx : g.Nx;
+    if (p < rows) {
+      i = p % g.Nx;
+      j = p < g.Nx ? 0 : g.Ny - 1;
+    } else {
+      const int q = p - rows;
+      if (g.Ny <= 2 || q >= 2 * (g.Ny - 2)) return;
+      j = 1 + (q >> 1);
+      i = (q & 1) ? g.Nx - 1 : 0;
+    }
+  } else {
+    i = blockIdx.x * blockDim.x + threadIdx.x;
+    j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.Nx || j >= g.Ny) return;
+  }
+  rhs[(size_t)j * g.pitch + i] = rhs_cell(g, u, v, h, i, j, with_dt);
 }
 
 // ---------------------------------------------------------------- reductions
@@ -334,7 +375,8 @@ __global__ void __launch_bounds__(512) sor_kernel(const Grid2 g, double* pi, con
 
 // ---------------------------------------------------------------- projection
 
-__global__ void projection_kernel(const Grid2 g, const double* __restrict__ pi, double* u, double* v) {
+__global__ void projection_kernel(const Grid2 g, const double* __restrict__ pi, double* __restrict__ u,
+                                  double* __restrict__ v) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= g.Nx || j >= g.Ny) return;
@@ -344,10 +386,13 @@ __global__ void projection_kernel(const Grid2 g, const double* __restrict__ pi, 
   double ps = j > 0 ? pi[c - g.pitch] : ld_s(pi, g, i, j - 1);
   bool skip_u = g.wall_ew && i == 0;
   bool skip_v = g.wall_ns && j == 0;
+  const double du = div_rn(-g.dt * (pc - pw), g.dx, g.rdx);
+  const double dv = div_rn(-g.dt * (pc - ps), g.dy, g.rdy);
+#pragma unroll 4
   for (int k = 0; k < g.L; ++k) {
     size_t o = k * g.lstride + c;
-    if (!skip_u) u[o] += div_rn(-g.dt * (pc - pw), g.dx, g.rdx);
-    if (!skip_v) v[o] += div_rn(-g.dt * (pc - ps), g.dy, g.rdy);
+    if (!skip_u) u[o] += du;
+    if (!skip_v) v[o] += dv;
   }
 }
 
@@ -369,16 +414,29 @@ inline dim3 grid2(int Nx, int Ny, dim3 b) { return dim3((Nx + b.x - 1) / b.x, (N
 
 }  // namespace
 
-void launch_pressure_rhs(const Grid2& g, const double* u, const double* v, const double* h, double* rhs,
-                         cudaStream_t s) {
+// interior cells with plain loads when the face thickness is the AL81 average, then the
+// border ring through the boundary maps; otherwise every cell through the maps
+static int launch_rhs(const Grid2& g, const double* u, const double* v, const double* h, double* out,
+                      int with_dt, cudaStream_t s) {
   dim3 b(32, 8);
-  rhs_kernel<<<grid2(g.Nx, g.Ny, b), b, 0, s>>>(g, u, v, h, rhs, 1);
+  if (g.thick_scheme == 0 && g.Nx >= 3 && g.Ny >= 3) {
+    rhs_inner_kernel<<<grid2(g.Nx, g.Ny, b), b, 0, s>>>(g, u, v, h, out, with_dt);
+    const int ring = 2 * g.Nx + 2 * (g.Ny - 2);
+    rhs_kernel<<<(ring + 127) / 128, 128, 0, s>>>(g, u, v, h, out, with_dt, 1);
+    return 2;
+  }
+  rhs_kernel<<<grid2(g.Nx, g.Ny, b), b, 0, s>>>(g, u, v, h, out, with_dt, 0);
+  return 1;
 }
 
-void launch_divergence_field(const Grid2& g, const double* u, const double* v, const double* h, double* out,
-                             cudaStream_t s) {
-  dim3 b(32, 8);
-  rhs_kernel<<<grid2(g.Nx, g.Ny, b), b, 0, s>>>(g, u, v, h, out, 0);
+int launch_pressure_rhs(const Grid2& g, const double* u, const double* v, const double* h, double* rhs,
+                        cudaStream_t s) {
+  return launch_rhs(g, u, v, h, rhs, 1, s);
+}
+
+int launch_divergence_field(const Grid2& g, const double* u, const double* v, const double* h, double* out,
+                            cudaStream_t s) {
+  return launch_rhs(g, u, v, h, out, 0, s);
 }
 
 size_t reduce_scratch_elems(int Nx, int Ny) { (void)Nx; return (size_t)(Ny + RED_ROWS - 1) / RED_ROWS + 4; }

@@ -18,7 +18,7 @@ struct Grid2 {
 };
 
 // rhs = sum_k div(h_k u_k) / dt with the gathered face thickness (pressure.c:570-606)
-void launch_pressure_rhs(const Grid2& g, const double* u, const double* v, const double* h,
+int launch_pressure_rhs(const Grid2& g, const double* u, const double* v, const double* h,
                          double* rhs, cudaStream_t s);
 
 // sum of the owned cells in the reference's serial order (x outer, y inner) or in a fixed
@@ -51,7 +51,7 @@ void launch_projection(const Grid2& g, const double* pi, double* u, double* v, c
 // per-cell residual rhs - L(pi) and barotropic divergence (pressure.c:652-737)
 void launch_residual_field(const Grid2& g, const double* pi, const double* rhs,
                            const Operator& op, double* out, cudaStream_t s);
-void launch_divergence_field(const Grid2& g, const double* u, const double* v, const double* h,
+int launch_divergence_field(const Grid2& g, const double* u, const double* v, const double* h,
                              double* out, cudaStream_t s);
 // max |f| and sum f^2 (serial order or tree) into out[0], out[1]
 void launch_norms(const double* f, int Nx, int Ny, int pitch, bool serial_order,
