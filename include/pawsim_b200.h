@@ -71,7 +71,9 @@ typedef struct pawsim_gpu_config
   double pi_tol, sor_rp, omega_mg;
   /* GPU multigrid controls: 0 FP64 V-cycles, 1 FP32 V-cycles inside FP64 defect
    * correction; red-black sweeps before/after the coarse correction and their weight
-   * (0 selects the defaults 1, 1, 1.0). */
+   * (0 selects the defaults 1, 1, 1.0). A negative mg_omega lets the solver choose the
+   * weight on its first time-step solve: each of 1.0, 1.05, 1.1, 1.15, 1.2, 1.3 solves from
+   * the same pi and the one with the fewest V-cycles is kept. */
   int mg_fp32, mg_pre, mg_post;
   double mg_omega;
   /* 1: sums in the reference's serial order (bitwise parity), 0: fixed pairwise tree,
@@ -96,6 +98,7 @@ typedef struct pawsim_gpu_stats
                                 (the solve started from the previous pressure) */
   int fallback;              /* 1 when pressureSolver 2 fell back to the gathered multigrid
                                 (grid without a first clean 2:1 coarsening) */
+  double mg_omega;           /* red-black weight the gathered multigrid used (0 for SOR, DMG) */
 } pawsim_gpu_stats;
 
 typedef struct pawsim_gpu pawsim_gpu;

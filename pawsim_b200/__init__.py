@@ -52,7 +52,8 @@ class GpuStats(ctypes.Structure):
     _fields_ = [("iters", ctypes.c_int), ("residual_max", ctypes.c_double),
                 ("residual_rms", ctypes.c_double), ("div_max", ctypes.c_double),
                 ("div_rms", ctypes.c_double), ("stop_measure", ctypes.c_double),
-                ("solve_ms", ctypes.c_double), ("warm_start", ctypes.c_int), ("fallback", ctypes.c_int)]
+                ("solve_ms", ctypes.c_double), ("warm_start", ctypes.c_int), ("fallback", ctypes.c_int),
+                ("mg_omega", ctypes.c_double)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -161,7 +162,7 @@ def gpu_config(cfg: inputs.Config, **over) -> GpuConfig:
                  ("conv_diff", "convDiff"), ("pi_tol", "tol"), ("sor_rp", "SOR_rp"),
                  ("omega_mg", "omega_MG")):
         setattr(g, a, float(v[b]))
-    g.mg_fp32, g.mg_pre, g.mg_post, g.mg_omega = 0, 1, 1, 1.0
+    g.mg_fp32, g.mg_pre, g.mg_post, g.mg_omega = 0, 1, 1, -1.0   # weight chosen by the solver
     g.serial_sums = -1
     g.mg_tile = 0
     for k, val in over.items():

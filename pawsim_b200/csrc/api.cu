@@ -338,6 +338,7 @@ static int init(Model* m) {
     o.pre = m->c.mg_pre > 0 ? m->c.mg_pre : 1;
     o.post = m->c.mg_post > 0 ? m->c.mg_post : 1;
     o.omega_rb = m->c.mg_omega > 0 ? m->c.mg_omega : 1.0;
+    o.omega_auto = m->c.mg_omega < 0 ? 1 : 0;
     o.full_mg = m->c.use_full_mg;
     o.tile_shape = m->c.mg_tile - 1;
     m->mg = new Multigrid(m->Nx, m->Ny, m->c.Lx, m->c.Ly, m->c.wall_ew, m->c.wall_ns, Hc.data(), o, m->s);
@@ -515,6 +516,7 @@ static int pressure_correct(Model* m, int update_diags, pawsim_gpu_stats* st) {
       return fail(PAWSIM_GPU_ECUDA, "warm-start guess failed");
     iters = m->mg->solve(m->pi, m->pitch, m->rhs, m->pitch, m->c.pi_tol, m->c.maxiters, &mres);
     local.stop_measure = mres;
+    local.mg_omega = m->mg->omega();
     PAWSIM_CUDA_OK(cudaEventRecord(m->ev1, m->s));
     PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
     if (m->ws) {
@@ -538,6 +540,7 @@ static int pressure_correct(Model* m, int update_diags, pawsim_gpu_stats* st) {
     double mres = 0;
     iters = m->mg->solve(m->pi, m->pitch, m->rhs, m->pitch, m->c.pi_tol, m->c.maxiters, &mres);
     local.stop_measure = mres;
+    local.mg_omega = m->mg->omega();
     local.fallback = 1;
     PAWSIM_CUDA_OK(cudaEventRecord(m->ev1, m->s));
     PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
@@ -667,6 +670,7 @@ int pawsim_gpu_solve_mg(pawsim_gpu* h, pawsim_gpu_stats* st) {
     memset(st, 0, sizeof(*st));
     st->iters = it;
     st->stop_measure = mres;
+    st->mg_omega = m->mg->omega();
     float ms = 0;
     cudaEventElapsedTime(&ms, m->ev0, m->ev1);
     st->solve_ms = ms;

@@ -1292,6 +1292,35 @@ double Multigrid::max_residual(const double* pi, int pitch, const double* rhs, i
 int Multigrid::solve(double* pi, int pitch, const double* rhs, int rhs_pitch, double tol, int maxiters,
                      double* maxres_out) {
   (void)pitch; (void)rhs_pitch;
+  if (opt_.omega_auto && !omega_tuned_ && nsolves_ >= 1) {
+    omega_tuned_ = true;
+    const Level& F = lv_.back();
+    const size_t bytes = (size_t)F.pitch * F.Ny * sizeof(double);
+    double* backup = nullptr;
+    if (cudaMalloc(&backup, bytes) == cudaSuccess) {
+      cudaMemcpyAsync(backup, pi, bytes, cudaMemcpyDeviceToDevice, s_);
+      double best = 1.0;
+      int best_it = -1;
+      for (double w : kOmegaCandidates) {
+        opt_.omega_rb = w;
+        cudaMemcpyAsync(pi, backup, bytes, cudaMemcpyDeviceToDevice, s_);
+        const int it = solve_once(pi, rhs, tol, maxiters, nullptr);
+        if (it >= 0 && (best_it < 0 || it < best_it)) {
+          best_it = it;
+          best = w;
+        }
+      }
+      opt_.omega_rb = best;
+      cudaMemcpyAsync(pi, backup, bytes, cudaMemcpyDeviceToDevice, s_);
+      cudaStreamSynchronize(s_);
+      cudaFree(backup);
+    }
+  }
+  ++nsolves_;
+  return solve_once(pi, rhs, tol, maxiters, maxres_out);
+}
+
+int Multigrid::solve_once(double* pi, const double* rhs, double tol, int maxiters, double* maxres_out) {
   const int prec = opt_.fp32_cycles ? 1 : 0;
   if (fine_pi_ != pi || fine_rhs_ != rhs || g_->pre != opt_.pre || g_->post != opt_.post ||
       g_->omega != opt_.omega_rb) {

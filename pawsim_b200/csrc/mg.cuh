@@ -25,7 +25,14 @@ struct MGOptions {
   double omega_rb = 1.0;   // smoother weight
   int full_mg = 0;         // use_fullMG: nested iteration from the coarsest level
   int tile_shape = -1;     // fused level kernels: -1 autotune per level, 0..3 force a tile shape, 4 strips
+  // choose omega_rb on the second solve (the first of a time step; the first is the
+  // start-up solve from rest): each candidate solves from the same pi and the weight with
+  // the fewest V-cycles is kept (the smallest among ties), so the choice is deterministic
+  int omega_auto = 0;
 };
+
+// candidate weights of the automatic choice
+constexpr double kOmegaCandidates[] = {1.0, 1.05, 1.1, 1.15, 1.2, 1.3};
 
 class Multigrid {
  public:
@@ -38,6 +45,8 @@ class Multigrid {
   // maxres_out receives max |pi - Jacobi(pi)| of the last check.
   int solve(double* pi, int pi_pitch, const double* rhs, int rhs_pitch, double tol, int maxiters,
             double* maxres_out);
+  // the weight in use (after the automatic choice, the chosen one)
+  double omega() const { return opt_.omega_rb; }
   // one evaluation of the stopping measure (for diagnostics and warm-start decisions)
   double max_residual(const double* pi, int pi_pitch, const double* rhs, int rhs_pitch);
   // the same measure, left on the device: *bits = max |pi - Jacobi(pi)| as an integer bit
@@ -67,6 +76,9 @@ class Multigrid {
 
  private:
   template <typename T> void enqueue_vcycle(cudaStream_t s, unsigned long long* measure_bits);
+  int solve_once(double* pi, const double* rhs, double tol, int maxiters, double* maxres_out);
+  int nsolves_ = 0;
+  bool omega_tuned_ = false;
   template <typename T> CoarseDesc coarse_desc(void* unit_out) const;
   template <typename T> size_t coarse_smem() const;
   template <typename T> void tabulate_coarse(cudaStream_t s);

@@ -586,7 +586,7 @@ int main (int argc, char ** argv)
   g.tau_period = c.tauPeriod; g.wdia_period = c.wDiaPeriod; g.conv_diff = c.convDiff;
   g.pi_tol = c.tol; g.sor_rp = c.SOR_rp; g.omega_mg = c.omega_MG;
   g.mg_fp32 = getenv("PAWSIM_GPU_MG_FP32") ? atoi(getenv("PAWSIM_GPU_MG_FP32")) : 0;
-  g.mg_pre = 1; g.mg_post = 1; g.mg_omega = 1.0;
+  g.mg_pre = 1; g.mg_post = 1; g.mg_omega = -1.0;   /* weight chosen by the solver */
   g.serial_sums = -1;
   g.mg_tile = 0;
   if (c.useTracer)

@@ -35,7 +35,7 @@ def main(argv=None):
     ap.add_argument("--solver", type=int, default=1)
     ap.add_argument("--mg-fp32", action="store_true")
     ap.add_argument("--mg-tile", type=int, default=0, help="0 autotune, 1..4 force a tile shape, 5 strips")
-    ap.add_argument("--mg-omega", type=float, default=1.0)
+    ap.add_argument("--mg-omega", type=float, default=-1.0, help="red-black weight; negative: chosen by the solver")
     ap.add_argument("--mg-pre", type=int, default=1)
     ap.add_argument("--mg-post", type=int, default=1)
     ap.add_argument("--integrator-only", action="store_true")

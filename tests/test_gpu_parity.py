@@ -174,3 +174,40 @@ def test_dmg_falls_back_to_gathered_mg(tmp_path, oracle_mod, lib):
     s_o, s_g = o.state(), m.state()
     for var in ("u", "v", "h"):
         assert rel_l2(s_g[var], s_o[var]) < 1e-8, var
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind,kw", [
+    ("gyre", dict(N=256, solver=1, tol=1e-12, dt=450.0)),
+    ("jets", dict(N=128, solver=1, tol=1e-12, dt=100.0)),
+], ids=["gyre256", "jets128"])
+def test_mg_omega_choice(tmp_path, oracle_mod, lib, kind, kw):
+    """The automatic red-black weight: the start-up solve uses 1.0, the first time-step
+    solve tries every candidate from the same pressure and keeps the one with the fewest
+    V-cycles (so two models choose the same); the choice never needs more V-cycles than
+    1.0 on that solve, and the state still agrees with the oracle to the solver tolerance."""
+    _, cfg, f = make_setup(tmp_path, kind, **kw)
+    runs = {}
+    for omega in (1.0, -1.0, -1.0):
+        m = lib.Model(cfg, f, mg_omega=omega)
+        m.prelim()
+        reps = [m.step(n) for n in range(1, 5)]
+        runs.setdefault(omega, []).append((reps, m.state()))
+    fixed = runs[1.0][0][0]
+    (auto_a, sa), (auto_b, sb) = runs[-1.0]
+    assert fixed[0]["mg_omega"] == 1.0
+    chosen = auto_a[0]["mg_omega"]
+    assert chosen in (1.0, 1.05, 1.1, 1.15, 1.2, 1.3)
+    assert all(r["mg_omega"] == chosen for r in auto_a + auto_b)
+    assert [r["iters"] for r in auto_a] == [r["iters"] for r in auto_b]
+    for var in ("u", "v", "h"):
+        assert np.array_equal(sa[var], sb[var])
+    assert auto_a[0]["iters"] <= fixed[0]["iters"]
+    o = oracle_mod.Oracle(cfg, f)
+    o.prelim()
+    for n in range(1, 5):
+        o.integrator_step(n)
+        o.pressure(True)
+    so = o.state()
+    for var in ("u", "v", "h"):
+        assert rel_l2(sa[var], so[var]) < 1e-9, (var, rel_l2(sa[var], so[var]))
