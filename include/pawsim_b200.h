@@ -128,6 +128,18 @@ PAWSIM_API int pawsim_gpu_step (pawsim_gpu * m, unsigned n, pawsim_gpu_stats * s
 /* nsteps passes starting at step n0; st receives the last step's report */
 PAWSIM_API int pawsim_gpu_run (pawsim_gpu * m, unsigned n0, unsigned nsteps, pawsim_gpu_stats * st);
 
+/* Online time averages (diagnostics.c:307-470, the savefreqAvg outputs). accumulate adds
+ * avg_fac * dt times the current state to the running sums (call it after each step, with
+ * avg_fac = 1, or 1 - (t - t_next_avg) / dt on the step that crosses the window's end, as
+ * pawsim_diagnostics_accumulate_averages does); scale multiplies every sum by factor
+ * (1 / savefreqAvg when a window is written); zero resets them. The sums are read with
+ * pawsim_gpu_get_field under the output names U_avg, V_avg, H_avg, M_avg, HU_avg, HV_avg,
+ * HUU_avg, HVV_avg, HUV_avg (k < Nlay), W_avg (k <= Nlay) and P_avg. They live in device
+ * memory allocated by the first call of accumulate. */
+PAWSIM_API int pawsim_gpu_accumulate_averages (pawsim_gpu * m, double avg_fac);
+PAWSIM_API int pawsim_gpu_scale_averages (pawsim_gpu * m, double factor);
+PAWSIM_API int pawsim_gpu_zero_averages (pawsim_gpu * m);
+
 /* Solve L(pi) = rhs on the resident pi/pi_rhs with the GPU multigrid (no projection). */
 PAWSIM_API int pawsim_gpu_solve_mg (pawsim_gpu * m, pawsim_gpu_stats * st);
 

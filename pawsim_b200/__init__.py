@@ -70,6 +70,7 @@ EXPORTS = (
     "pawsim_nn_net_create", "pawsim_nn_net_destroy", "pawsim_nn_net_param_count",
     "pawsim_nn_net_get_params", "pawsim_nn_net_set_params", "pawsim_nn_net_get_grads",
     "pawsim_nn_net_forward", "pawsim_nn_net_backward", "pawsim_nn_net_adam",
+    "pawsim_gpu_accumulate_averages", "pawsim_gpu_scale_averages", "pawsim_gpu_zero_averages",
 )
 
 _LIB = None
@@ -98,6 +99,9 @@ def load_library(path: str = LIB_PATH):
     lib.pawsim_gpu_step.argtypes = [P, ctypes.c_uint, ctypes.POINTER(GpuStats)]
     lib.pawsim_gpu_run.argtypes = [P, ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(GpuStats)]
     lib.pawsim_gpu_solve_mg.argtypes = [P, ctypes.POINTER(GpuStats)]
+    lib.pawsim_gpu_accumulate_averages.argtypes = [P, ctypes.c_double]
+    lib.pawsim_gpu_scale_averages.argtypes = [P, ctypes.c_double]
+    lib.pawsim_gpu_zero_averages.argtypes = [P]
     lib.pawsim_gpu_set_stream.argtypes = [P, P]
     lib.pawsim_gpu_synchronize.argtypes = [P]
     lib.pawsim_gpu_time.argtypes = [P]
@@ -280,6 +284,17 @@ class Model:
         st = GpuStats()
         _check(self.lib.pawsim_gpu_solve_mg(self._h, ctypes.byref(st)))
         return st.as_dict()
+
+    # ----------------------------------------------------------------- online averages
+    def accumulate_averages(self, avg_fac: float = 1.0) -> None:
+        """Add avg_fac * dt times the current state to the running averages."""
+        _check(self.lib.pawsim_gpu_accumulate_averages(self._h, float(avg_fac)))
+
+    def scale_averages(self, factor: float) -> None:
+        _check(self.lib.pawsim_gpu_scale_averages(self._h, float(factor)))
+
+    def zero_averages(self) -> None:
+        _check(self.lib.pawsim_gpu_zero_averages(self._h))
 
     def synchronize(self) -> None:
         _check(self.lib.pawsim_gpu_synchronize(self._h))

@@ -76,6 +76,9 @@ struct Model {
   double *fu[2], *fv[2], *fh[2];
   int h1 = 0;   // history buffer holding the newest stored tendency
   double *dtu, *dtv, *dth, *wdia;
+  // running averages (allocated by the first accumulation): 9 per-layer sums (u, v, h, M,
+  // hu, hv, huu, hvv, huv), then w_dia on L+1 interfaces, then pi
+  double* avg = nullptr;
   double *hhs, *hhb, *Hc, *omz, *taux, *tauy, *fbx, *fby, *uLid, *vLid;
   double *uRelax, *vRelax, *hRelax, *eRelax, *uTime, *vTime, *eTime, *hTime, *wdff, *nu_u, *nu_v;
   double *pi, *rhs, *work, *scratch, *dsum;
@@ -220,6 +223,17 @@ struct FieldRef {
   bool writable;
 };
 
+static_assert(AVG_LMAX == LMAX, "the averages kernel holds one column of LMAX layers");
+
+// index of a per-layer running-average sum inside Model::avg (-1 for other names)
+static int avg_slot(const std::string& n) {
+  static const char* names[9] = {"U_avg", "V_avg", "H_avg", "M_avg", "HU_avg", "HV_avg", "HUU_avg", "HVV_avg",
+                                 "HUV_avg"};
+  for (int q = 0; q < 9; ++q)
+    if (n == names[q]) return q;
+  return -1;
+}
+
 static bool lookup(Model* m, const std::string& n, FieldRef& f) {
   int L = m->L;
   f = FieldRef{nullptr, m->Ny, m->Nx, m->pitch, m->lstride, 1, true};
@@ -259,6 +273,9 @@ static bool lookup(Model* m, const std::string& n, FieldRef& f) {
     else if (n == "tend_u") { f.base = m->fu[m->h1]; f.nk = L; }
     else if (n == "tend_v") { f.base = m->fv[m->h1]; f.nk = L; }
     else if (n == "tend_h") { f.base = m->fh[m->h1]; f.nk = L; }
+    else if (m->avg && avg_slot(n) >= 0) { f.base = m->avg + (size_t)avg_slot(n) * L * m->lstride; f.nk = L; }
+    else if (m->avg && n == "W_avg") { f.base = m->avg + (size_t)9 * L * m->lstride; f.nk = L + 1; }
+    else if (m->avg && n == "P_avg") f.base = m->avg + (size_t)(10 * L + 1) * m->lstride;
     else return false;
   }
   return true;
@@ -654,6 +671,50 @@ int pawsim_gpu_run(pawsim_gpu* h, unsigned n0, unsigned nsteps, pawsim_gpu_stats
     int r = pawsim_gpu_step(h, n, st);
     if (r) return r;
   }
+  return 0;
+}
+
+int pawsim_gpu_accumulate_averages(pawsim_gpu* h, double avg_fac) {
+  if (!h) return PAWSIM_GPU_EBADCONFIG;
+  Model* m = h->m;
+  if (!m->ready) return fail(PAWSIM_GPU_EBADCONFIG, "pawsim_gpu_init must follow the uploads");
+  if (!m->avg) {
+    m->avg = m->alloc<double>((size_t)(10 * m->L + 2) * m->lstride);
+    if (!m->avg) return fail(PAWSIM_GPU_ECUDA, "average storage allocation failed");
+  }
+  const size_t ls = m->lstride;
+  double* b = m->avg;
+  AvgParams a;
+  a.dtfac = avg_fac * m->c.dt;   // dtfac of diagnostics.c:337
+  a.use_rl = m->c.use_rl;
+  a.h0 = m->c.h0;
+  for (int k = 0; k < m->L; ++k) { a.gg[k] = m->gg[k]; a.geff[k] = m->geff[k]; }
+  a.u = m->u[m->cur]; a.v = m->v[m->cur]; a.h = m->h[m->cur];
+  a.pi = m->pi; a.hhb = m->hhb; a.wdia = m->wdia;
+  const size_t Ls = (size_t)m->L * ls;
+  a.au = b; a.av = b + Ls; a.ah = b + 2 * Ls; a.aM = b + 3 * Ls; a.ahu = b + 4 * Ls; a.ahv = b + 5 * Ls;
+  a.ahuu = b + 6 * Ls; a.ahvv = b + 7 * Ls; a.ahuv = b + 8 * Ls; a.aW = b + 9 * Ls; a.api = a.aW + Ls + ls;
+  launch_accumulate_averages(m->grid2(), a, m->s);
+  ++g_launches;
+  PAWSIM_CUDA_OK(cudaGetLastError());
+  return 0;
+}
+
+int pawsim_gpu_scale_averages(pawsim_gpu* h, double factor) {
+  if (!h) return PAWSIM_GPU_EBADCONFIG;
+  Model* m = h->m;
+  if (!m->avg) return fail(PAWSIM_GPU_EBADCONFIG, "no averages accumulated");
+  launch_scale(m->avg, (size_t)(10 * m->L + 2) * m->lstride, factor, m->s);
+  ++g_launches;
+  PAWSIM_CUDA_OK(cudaGetLastError());
+  return 0;
+}
+
+int pawsim_gpu_zero_averages(pawsim_gpu* h) {
+  if (!h) return PAWSIM_GPU_EBADCONFIG;
+  Model* m = h->m;
+  if (m->avg)
+    PAWSIM_CUDA_OK(cudaMemsetAsync(m->avg, 0, (size_t)(10 * m->L + 2) * m->lstride * sizeof(double), m->s));
   return 0;
 }
 

@@ -410,9 +410,80 @@ __global__ void residual_field_kernel(const Grid2 g, const double* __restrict__ 
   out[c] = rhs[c] - Lp;
 }
 
+// running averages (diagnostics.c:307-375), one thread per owned cell and all layers; the
+// column's eta and Montgomery potential as work.c:1173-1203 and 1410-1512 form them
+__global__ void accumulate_averages_kernel(const Grid2 g, const AvgParams a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.Nx || j >= g.Ny) return;
+  const size_t c = (size_t)j * g.pitch + i;
+  const int L = g.L;
+  double hk[AVG_LMAX], eta[AVG_LMAX];
+  double e_acc = a.hhb[c];
+#pragma unroll
+  for (int k = AVG_LMAX - 1; k >= 0; --k) {
+    if (k < L) {
+      hk[k] = a.h[k * g.lstride + c];
+      e_acc = e_acc + hk[k];
+      eta[k] = e_acc;
+    }
+  }
+  const double d = a.dtfac;
+  const double pic = a.pi[c];
+  double pp = 0;
+#pragma unroll
+  for (int k = 0; k < AVG_LMAX; ++k) {
+    if (k < L) {
+      if (k == 0) pp = a.use_rl ? 0 : a.gg[0] * eta[0];
+      else pp = pp + a.gg[k] * eta[k];
+      double mm = pp;
+      if (a.h0 != 0) {
+        const double h0 = a.h0, hc = hk[k];
+        mm -= a.geff[k] * (h0 * h0 * h0 * h0) / (hc * hc * hc) / 3;
+      }
+      const size_t o = k * g.lstride + c;
+      const double* uk = a.u + k * g.lstride;
+      const double* vk = a.v + k * g.lstride;
+      const double* hkp = a.h + k * g.lstride;
+      const double uc = uk[c], vc = vk[c], hc = hk[k];
+      const double hw = hw_face(g, hkp, uk, i, j), hs = hs_face(g, hkp, vk, i, j);
+      const double hq = 0.25 * (hc + ld_s(hkp, g, i - 1, j) + ld_s(hkp, g, i, j - 1) + ld_s(hkp, g, i - 1, j - 1));
+      const double uq = 0.5 * (uc + ld_u(g, uk, i, j - 1));
+      const double vq = 0.5 * (vc + ld_v(g, vk, i - 1, j));
+      a.au[o] += d * uc;
+      a.av[o] += d * vc;
+      a.ah[o] += d * hc;
+      a.aM[o] += d * (mm + (a.use_rl ? pic : 0));
+      a.aW[o] += d * a.wdia[o];
+      a.ahu[o] += d * hw * uc;
+      a.ahv[o] += d * hs * vc;
+      a.ahuu[o] += d * hw * uc * uc;
+      a.ahvv[o] += d * hs * vc * vc;
+      a.ahuv[o] += d * hq * uq * vq;
+    }
+  }
+  const size_t oL = (size_t)L * g.lstride + c;
+  a.aW[oL] += d * a.wdia[oL];
+  a.api[c] += d * pic;
+}
+
+__global__ void scale_kernel(double* f, size_t n, double factor) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+    f[q] *= factor;
+}
+
 inline dim3 grid2(int Nx, int Ny, dim3 b) { return dim3((Nx + b.x - 1) / b.x, (Ny + b.y - 1) / b.y); }
 
 }  // namespace
+
+void launch_accumulate_averages(const Grid2& g, const AvgParams& a, cudaStream_t s) {
+  dim3 b(32, 8);
+  accumulate_averages_kernel<<<grid2(g.Nx, g.Ny, b), b, 0, s>>>(g, a);
+}
+
+void launch_scale(double* f, size_t n, double factor, cudaStream_t s) {
+  scale_kernel<<<1184, 256, 0, s>>>(f, n, factor);
+}
 
 // interior cells with plain loads when the face thickness is the AL81 average, then the
 // border ring through the boundary maps; otherwise every cell through the maps

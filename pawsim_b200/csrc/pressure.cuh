@@ -53,6 +53,24 @@ void launch_residual_field(const Grid2& g, const double* pi, const double* rhs,
                            const Operator& op, double* out, cudaStream_t s);
 int launch_divergence_field(const Grid2& g, const double* u, const double* v, const double* h,
                              double* out, cudaStream_t s);
+// Running time averages of the state (diagnostics.c:307-375): at every cell each field
+// is incremented by dtfac * value. u, v, h, M (Montgomery potential plus pi under the
+// rigid lid), h_west u, h_south v, h_west u^2, h_south v^2 and hq uq vq (q-point means) per
+// layer, w_dia per interface, pi; face thickness gathered as in the pressure RHS. Per-layer
+// arrays are lstride apart.
+constexpr int AVG_LMAX = 8;
+struct AvgParams {
+  double dtfac;
+  int use_rl;
+  double h0;
+  double gg[AVG_LMAX], geff[AVG_LMAX];
+  const double *u, *v, *h, *pi, *hhb, *wdia;
+  double *au, *av, *ah, *aM, *aW, *ahu, *ahv, *ahuu, *ahvv, *ahuv, *api;
+};
+void launch_accumulate_averages(const Grid2& g, const AvgParams& a, cudaStream_t s);
+// f[i] *= factor for n contiguous doubles
+void launch_scale(double* f, size_t n, double factor, cudaStream_t s);
+
 // max |f| and sum f^2 (serial order or tree) into out[0], out[1]
 void launch_norms(const double* f, int Nx, int Ny, int pitch, bool serial_order,
                   double* partials, double* out, cudaStream_t s);

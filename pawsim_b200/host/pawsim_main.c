@@ -42,7 +42,7 @@ typedef struct
   int useTrad, use_MG, use_fullMG, pressureTiming, writeInitDiagnostics, restart, useWallEW,
       useWallNS, useRL, oceanSurfDrag, windFeedback, useTracer, useBuoyancy, useRandomForcing;
   /* reals (strtod) */
-  double Lx, Ly, dt, tmin, tmax, savefrequency, KT00_sigma, h0, hsml, hmin_surf, hbbl, hmin_bot,
+  double Lx, Ly, dt, tmin, tmax, savefrequency, savefreqAvg, KT00_sigma, h0, hsml, hmin_surf, hbbl, hmin_bot,
       A2, A4, A2smag, A4smag, K2, K4, linDragCoeff, quadDragCoeff, linDragSurf, quadDragSurf,
       tauPeriod, wDiaPeriod, convDiff, omega_MG, tol, SOR_rp;
   /* derived */
@@ -103,7 +103,7 @@ static const keydef KEYS[] = {
     U(thicknessScheme), U(tracerScheme), U(tauNrecs), U(wDiaNrecs), U(maxiters), S(mpiNx), S(mpiNy),
     B(useTrad), B(use_MG), B(use_fullMG), B(pressureTiming), B(writeInitDiagnostics), B(restart),
     B(useWallEW), B(useWallNS), B(useRL), B(oceanSurfDrag), B(windFeedback), B(useTracer),
-    B(useBuoyancy), B(useRandomForcing), R(Lx), R(Ly), R(dt), R(tmin), R(tmax), R(savefrequency),
+    B(useBuoyancy), B(useRandomForcing), R(Lx), R(Ly), R(dt), R(tmin), R(tmax), R(savefrequency), R(savefreqAvg),
     R(KT00_sigma), R(h0), R(hsml), R(hmin_surf), R(hbbl), R(hmin_bot), R(A2), R(A4), R(A2smag),
     R(A4smag), R(K2), R(K4), R(linDragCoeff), R(quadDragCoeff), R(linDragSurf), R(quadDragSurf),
     R(tauPeriod), R(wDiaPeriod), R(convDiff), R(omega_MG), R(tol), {NULL, K_REAL, 0}};
@@ -518,6 +518,31 @@ static int write_state (pawsim_gpu * m, const config * c, const char * outdir, u
   return 1;
 }
 
+/* one completed online-average window under AWSIM's names (diagnostics.c:378-420) */
+static int write_averages (pawsim_gpu * m, const config * c, const char * outdir, unsigned n, double * plane)
+{
+  const size_t N = (size_t) c->Nx * c->Ny;
+  const char * nm[10] = {"U_avg","V_avg","H_avg","M_avg","W_avg","HU_avg","HV_avg","HUU_avg","HVV_avg","HUV_avg"};
+  char name[NAMELEN];
+  unsigned k;
+  int a;
+  for (k = 0; k < c->Nlay; k ++)
+    for (a = 0; a < 10; a ++)
+    {
+      snprintf(name,sizeof(name),"%s%u_n=%u.dat",nm[a],k,n);
+      if (!gpu_ok(pawsim_gpu_get_field(m,nm[a],(int) k,plane,N),nm[a]) || !write_f64(outdir,name,plane,N)) return 0;
+    }
+  snprintf(name,sizeof(name),"W_avg%u_n=%u.dat",c->Nlay,n);
+  if (!gpu_ok(pawsim_gpu_get_field(m,"W_avg",(int) c->Nlay,plane,N),"W_avg") || !write_f64(outdir,name,plane,N))
+    return 0;
+  if (c->useRL)
+  {
+    snprintf(name,sizeof(name),"P_avg_n=%u.dat",n);
+    if (!gpu_ok(pawsim_gpu_get_field(m,"P_avg",0,plane,N),"P_avg") || !write_f64(outdir,name,plane,N)) return 0;
+  }
+  return 1;
+}
+
 static const char * solver_name (unsigned s)
 {
   return s == 0 ? "SOR" : (s == 1 ? "MG_GATHERED" : (s == 2 ? "MG_DISTRIBUTED" : "UNKNOWN"));
@@ -531,7 +556,8 @@ int main (int argc, char ** argv)
   pawsim_gpu_stats st;
   const char * outdir;
   double * plane = NULL;
-  unsigned n, n_saves, solves = 0, fallbacks = 0;
+  unsigned n, n_saves, solves = 0, fallbacks = 0, n_avg = 0;
+  double t_next_avg = 0;
   double wall_total = 0, iters_total = 0;
   const char * slash;
   int rc = 1;
@@ -602,6 +628,12 @@ int main (int argc, char ** argv)
   fflush(stdout);
 
   n_saves = c.restart ? c.startIdx : 0;
+  if (c.savefreqAvg > 0)
+  {
+    /* restarted runs continue AWSIM's diagnostic numbering (pawsim.c:428-433) */
+    n_avg = (unsigned) round(c.tmin / c.savefreqAvg) + 1;
+    t_next_avg = c.tmin + c.savefreqAvg;
+  }
   /* preliminary rigid-lid correction, then the n = 0 (or pickup) state (pawsim.c:278-312) */
   memset(&st,0,sizeof(st));
   if (!gpu_ok(pawsim_gpu_prelim(m,&st),"preliminary pressure correction")) goto done;
@@ -661,6 +693,25 @@ int main (int argc, char ** argv)
         goto done;
       }
       n_saves ++;
+    }
+    /* online averages (diagnostics.c:307-470): the step that crosses the window's end adds
+     * only its share, then the window is normalised, written and reset */
+    if (c.savefreqAvg > 0)
+    {
+      double avg_fac = (t < t_next_avg) ? 1 : 1 - (t - t_next_avg) / c.dt;
+      if (!gpu_ok(pawsim_gpu_accumulate_averages(m,avg_fac),"averages")) goto done;
+      if (!(t < t_next_avg))
+      {
+        if (!gpu_ok(pawsim_gpu_scale_averages(m,1 / c.savefreqAvg),"averages")
+         || !write_averages(m,&c,outdir,n_avg,plane)
+         || !gpu_ok(pawsim_gpu_zero_averages(m),"averages"))
+        {
+          fprintf(stderr,"ERROR: PAWSIM diagnostic averaging failed at n=%u\n",n);
+          goto done;
+        }
+        n_avg ++;
+        t_next_avg = n_avg * c.savefreqAvg;
+      }
     }
   }
   if (c.pressureTiming && solves > 0)

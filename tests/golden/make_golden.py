@@ -8,7 +8,8 @@ themselves (parameter text and raw data files, so the fixture does not depend on
 generator), and what the reference printed and wrote: the init_* tendency dumps of
 ``writeInitDiagnostics 1`` (model_code/diagnostics.c:914-972), U/V/H/P after each step
 (diagnostics.c:874-908) and the ``PAWSIM pressure solve`` lines of ``pressureTiming 1``
-(model_code/pawsim.c:100-108).
+(model_code/pawsim.c:100-108). The ``*_avg`` cases hold the online-average files of
+``savefreqAvg`` (diagnostics.c:378-470) instead.
 """
 import os
 import re
@@ -38,6 +39,16 @@ CASES = {
     "gyre_dmg": (inputs.gyre, dict(N=32, Ny=24, dt=900.0, solver=2, tol=1e-10)),
     "jets_dmg": (inputs.jets, dict(N=32, dt=100.0, solver=2)),
 }
+# online-average cases (savefreqAvg, diagnostics.c:307-470): windows of 2.5 steps, so the
+# step that crosses a window's end adds only part of itself; SOR keeps them bit-exact
+AVG_NSTEPS = 8
+AVG_CASES = {
+    "gyre_sor_avg": (inputs.gyre, dict(N=16, Ny=12, dt=900.0, solver=0, tol=1e-10)),
+    "full_sor_avg": (inputs.full_physics, dict(N=16, dt=50.0, solver=0, Ly=320e3, bathy_len=20e3,
+                                               sponge=40e3)),
+}
+AVG_FIELDS = ["U_avg", "V_avg", "H_avg", "M_avg", "W_avg", "HU_avg", "HV_avg", "HUU_avg", "HVV_avg",
+              "HUV_avg"]
 LINE = re.compile(r"iters=(\d+) walltime=\S+ s residual_max=(\S+) residual_rms=(\S+) "
                   r"div_max=(\S+) div_rms=(\S+)")
 
@@ -70,6 +81,34 @@ def make(name, fn, kw, outdir):
         np.savez_compressed(os.path.join(outdir, name + ".npz"), **rec)
 
 
+def make_avg(name, fn, kw, outdir):
+    """Inputs and the reference's online-average files of every completed window."""
+    with tempfile.TemporaryDirectory() as d:
+        kw = dict(kw)
+        extra = dict(kw.pop("extra", {}) or {})
+        dt = kw["dt"]
+        extra.update(savefreqAvg=2.5 * dt)
+        p = fn(os.path.join(d, "in"), Nt=AVG_NSTEPS, savefrequency=4 * dt, extra=extra, **kw)
+        cfg = inputs.read_config(p)
+        out = os.path.join(d, "out")
+        os.makedirs(out)
+        subprocess.run([oracle.reference_exe(), p, out], capture_output=True, text=True, check=True)
+        L, Nx, Ny = cfg.Nlay, cfg.Nx, cfg.Ny
+        rec = {"param_text": np.array(open(p).read())}
+        for f in sorted(os.listdir(os.path.dirname(p))):
+            if f.endswith(".dat") and f != "params.dat":
+                rec["in_" + f] = np.fromfile(os.path.join(os.path.dirname(p), f), dtype="<f8")
+        windows = sorted({int(f.split("_n=")[1][:-4]) for f in os.listdir(out) if f.startswith("U_avg0_n=")})
+        rec["windows"] = np.array(windows)
+        for n in windows:
+            for k in range(L):
+                for fld in AVG_FIELDS:
+                    rec[f"{fld}{k}_{n}"] = inputs.read_data(os.path.join(out, f"{fld}{k}_n={n}.dat"), (Ny, Nx))
+            rec[f"W_avg{L}_{n}"] = inputs.read_data(os.path.join(out, f"W_avg{L}_n={n}.dat"), (Ny, Nx))
+            rec[f"P_avg_{n}"] = inputs.read_data(os.path.join(out, f"P_avg_n={n}.dat"), (Ny, Nx))
+        np.savez_compressed(os.path.join(outdir, name + ".npz"), **rec)
+
+
 if __name__ == "__main__":
     # python tests/golden/make_golden.py [case ...]   (all cases when none are named)
     oracle.build(ref=True)
@@ -77,4 +116,9 @@ if __name__ == "__main__":
         if len(sys.argv) > 1 and name not in sys.argv[1:]:
             continue
         make(name, fn, kw, HERE)
+        print("wrote", name)
+    for name, (fn, kw) in AVG_CASES.items():
+        if len(sys.argv) > 1 and name not in sys.argv[1:]:
+            continue
+        make_avg(name, fn, kw, HERE)
         print("wrote", name)
