@@ -411,13 +411,26 @@ __global__ void residual_field_kernel(const Grid2 g, const double* __restrict__ 
 }
 
 // running averages (diagnostics.c:307-375), one thread per owned cell and all layers; the
-// column's eta and Montgomery potential as work.c:1173-1203 and 1410-1512 form them
+// column's eta and Montgomery potential as work.c:1173-1203 and 1410-1512 form them. The
+// sums of a layer are all read before any is written (restrict-qualified, so the loads of
+// the ten sums are in flight together).
 __global__ void accumulate_averages_kernel(const Grid2 g, const AvgParams a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= g.Nx || j >= g.Ny) return;
   const size_t c = (size_t)j * g.pitch + i;
   const int L = g.L;
+  double* __restrict__ au = a.au;
+  double* __restrict__ av = a.av;
+  double* __restrict__ ah = a.ah;
+  double* __restrict__ aM = a.aM;
+  double* __restrict__ aW = a.aW;
+  double* __restrict__ ahu = a.ahu;
+  double* __restrict__ ahv = a.ahv;
+  double* __restrict__ ahuu = a.ahuu;
+  double* __restrict__ ahvv = a.ahvv;
+  double* __restrict__ ahuv = a.ahuv;
+  const double* __restrict__ wdia = a.wdia;
   double hk[AVG_LMAX], eta[AVG_LMAX];
   double e_acc = a.hhb[c];
 #pragma unroll
@@ -434,6 +447,9 @@ __global__ void accumulate_averages_kernel(const Grid2 g, const AvgParams a) {
 #pragma unroll
   for (int k = 0; k < AVG_LMAX; ++k) {
     if (k < L) {
+      const size_t o = k * g.lstride + c;
+      const double su = au[o], sv = av[o], sh = ah[o], sM = aM[o], sW = aW[o], shu = ahu[o], shv = ahv[o],
+                   shuu = ahuu[o], shvv = ahvv[o], shuv = ahuv[o], wd = wdia[o];
       if (k == 0) pp = a.use_rl ? 0 : a.gg[0] * eta[0];
       else pp = pp + a.gg[k] * eta[k];
       double mm = pp;
@@ -441,7 +457,6 @@ __global__ void accumulate_averages_kernel(const Grid2 g, const AvgParams a) {
         const double h0 = a.h0, hc = hk[k];
         mm -= a.geff[k] * (h0 * h0 * h0 * h0) / (hc * hc * hc) / 3;
       }
-      const size_t o = k * g.lstride + c;
       const double* uk = a.u + k * g.lstride;
       const double* vk = a.v + k * g.lstride;
       const double* hkp = a.h + k * g.lstride;
@@ -450,20 +465,20 @@ __global__ void accumulate_averages_kernel(const Grid2 g, const AvgParams a) {
       const double hq = 0.25 * (hc + ld_s(hkp, g, i - 1, j) + ld_s(hkp, g, i, j - 1) + ld_s(hkp, g, i - 1, j - 1));
       const double uq = 0.5 * (uc + ld_u(g, uk, i, j - 1));
       const double vq = 0.5 * (vc + ld_v(g, vk, i - 1, j));
-      a.au[o] += d * uc;
-      a.av[o] += d * vc;
-      a.ah[o] += d * hc;
-      a.aM[o] += d * (mm + (a.use_rl ? pic : 0));
-      a.aW[o] += d * a.wdia[o];
-      a.ahu[o] += d * hw * uc;
-      a.ahv[o] += d * hs * vc;
-      a.ahuu[o] += d * hw * uc * uc;
-      a.ahvv[o] += d * hs * vc * vc;
-      a.ahuv[o] += d * hq * uq * vq;
+      au[o] = su + d * uc;
+      av[o] = sv + d * vc;
+      ah[o] = sh + d * hc;
+      aM[o] = sM + d * (mm + (a.use_rl ? pic : 0));
+      aW[o] = sW + d * wd;
+      ahu[o] = shu + d * hw * uc;
+      ahv[o] = shv + d * hs * vc;
+      ahuu[o] = shuu + d * hw * uc * uc;
+      ahvv[o] = shvv + d * hs * vc * vc;
+      ahuv[o] = shuv + d * hq * uq * vq;
     }
   }
   const size_t oL = (size_t)L * g.lstride + c;
-  a.aW[oL] += d * a.wdia[oL];
+  aW[oL] += d * wdia[oL];
   a.api[c] += d * pic;
 }
 
