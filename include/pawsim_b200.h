@@ -84,6 +84,11 @@ typedef struct pawsim_gpu_config
    * (32x8, 32x16, 64x8, 64x16 cells), 5 the streamed strips (levels of at least 64 x 48
    * cells). The shape changes only the speed, never the result. */
   int mg_tile;
+  /* passive tracer b (work.c:1947-2144): useTracer, tracerScheme (0 AL81, 1 UP3, 2 KT00) and
+   * the Laplacian / biharmonic diffusivities K2, K4. The buoyancy coupling (useBuoyancy) and
+   * diapycnal diffusion (diaDiffFile, bFluxFile) are not built. */
+  int use_tracer, tracer_scheme;
+  double K2, K4;
 } pawsim_gpu_config;
 
 /* Per-solve report, the numbers of the "PAWSIM pressure solve" line (pawsim.c:100-108). */
@@ -134,7 +139,7 @@ PAWSIM_API int pawsim_gpu_run (pawsim_gpu * m, unsigned n0, unsigned nsteps, paw
  * pawsim_diagnostics_accumulate_averages does); scale multiplies every sum by factor
  * (1 / savefreqAvg when a window is written); zero resets them. The sums are read with
  * pawsim_gpu_get_field under the output names U_avg, V_avg, H_avg, M_avg, HU_avg, HV_avg,
- * HUU_avg, HVV_avg, HUV_avg (k < Nlay), W_avg (k <= Nlay) and P_avg. They live in device
+ * HUU_avg, HVV_avg, HUV_avg, B_avg (tracer; k < Nlay), W_avg (k <= Nlay) and P_avg. They live in device
  * memory allocated by the first call of accumulate. */
 PAWSIM_API int pawsim_gpu_accumulate_averages (pawsim_gpu * m, double avg_fac);
 PAWSIM_API int pawsim_gpu_scale_averages (pawsim_gpu * m, double factor);

@@ -45,7 +45,9 @@ class GpuConfig(ctypes.Structure):
         "quad_drag_surf", "tau_period", "wdia_period", "conv_diff", "pi_tol", "sor_rp",
         "omega_mg")] + [("mg_fp32", ctypes.c_int), ("mg_pre", ctypes.c_int),
                         ("mg_post", ctypes.c_int), ("mg_omega", ctypes.c_double),
-                        ("serial_sums", ctypes.c_int), ("mg_tile", ctypes.c_int)]
+                        ("serial_sums", ctypes.c_int), ("mg_tile", ctypes.c_int),
+                        ("use_tracer", ctypes.c_int), ("tracer_scheme", ctypes.c_int),
+                        ("K2", ctypes.c_double), ("K4", ctypes.c_double)]
 
 
 class GpuStats(ctypes.Structure):
@@ -169,6 +171,8 @@ def gpu_config(cfg: inputs.Config, **over) -> GpuConfig:
     g.mg_fp32, g.mg_pre, g.mg_post, g.mg_omega = 0, 1, 1, -1.0   # weight chosen by the solver
     g.serial_sums = -1
     g.mg_tile = 0
+    g.use_tracer, g.tracer_scheme = int(v["useTracer"]), int(v["tracerScheme"])
+    g.K2, g.K4 = float(v["K2"]), float(v["K4"])
     for k, val in over.items():
         setattr(g, k, val)
     return g
@@ -178,8 +182,9 @@ class Model:
     """One model resident on the GPU (the drop-in for the reference's hot path)."""
 
     def __init__(self, cfg: inputs.Config, fields: dict | None = None, **options):
-        if cfg.values["useTracer"]:
-            raise PawsimError(-5, "the tracer equation is not part of this path yet")
+        if cfg.values["useTracer"] and (cfg.values["useBuoyancy"] or cfg.files.get("diaDiffFile")
+                                        or cfg.files.get("bFluxFile")):
+            raise PawsimError(-5, "the tracer's buoyancy coupling and diapycnal diffusion are not built")
         self.lib = load_library()
         self.cfg = cfg
         self.L, self.Nx, self.Ny = cfg.values["Nlay"], cfg.values["Nx"], cfg.values["Ny"]
@@ -248,9 +253,14 @@ class Model:
             for k in range(L + 1):
                 self.set("wdia_ff", r * (L + 1) + k, f["wdia_ff"][r, k])
         self.set("gg", 0, f["gg"])
+        if self._gc.use_tracer:
+            for name in ("b", "bRelax", "bTime"):
+                for k in range(L):
+                    self.set(name, k, f[name][k])
 
     def state(self) -> dict:
-        return {n: np.stack([self.get(n, k) for k in range(self.L)]) for n in ("u", "v", "h")}
+        names = ("u", "v", "h", "b") if self._gc.use_tracer else ("u", "v", "h")
+        return {n: np.stack([self.get(n, k) for k in range(self.L)]) for n in names}
 
     # ----------------------------------------------------------------- hot path
     def tendency_eval(self) -> dict:

@@ -20,7 +20,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC,-O3",
          "-Xcompiler", "-fvisibility=hidden"]
-SOURCES = ["api.cu", "tendency.cu", "pressure.cu", "mg.cu", "noalloc.cu", "nn.cu", "warmstart.cu", "dmg.cu"]
+SOURCES = ["api.cu", "tendency.cu", "pressure.cu", "mg.cu", "noalloc.cu", "nn.cu", "warmstart.cu", "dmg.cu",
+           "tracer.cu"]
 # (object name, source, extra flags): the fused tendency kernel is built for two tile heights
 UNITS = [(s.replace(".cu", ""), s, []) for s in SOURCES] + [
     ("tendency_ty8", "tendency_tile.cu", ["-DPAWSIM_TEND_TY=8"]),

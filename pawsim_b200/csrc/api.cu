@@ -17,6 +17,7 @@
 #include "pressure.cuh"
 #include "warmstart.cuh"
 #include "tendency.cuh"
+#include "tracer.cuh"
 
 namespace pawsim {
 
@@ -79,6 +80,8 @@ struct Model {
   // running averages (allocated by the first accumulation): 9 per-layer sums (u, v, h, M,
   // hu, hv, huu, hvv, huv), then w_dia on L+1 interfaces, then pi
   double* avg = nullptr;
+  // tracer (when use_tracer): state b[2] beside u/v/h, tendency history fb[2], restoring
+  double *b[2] = {nullptr, nullptr}, *fb[2] = {nullptr, nullptr}, *bRelax = nullptr, *bTime = nullptr;
   double *hhs, *hhb, *Hc, *omz, *taux, *tauy, *fbx, *fby, *uLid, *vLid;
   double *uRelax, *vRelax, *hRelax, *eRelax, *uTime, *vTime, *eTime, *hTime, *wdff, *nu_u, *nu_v;
   double *pi, *rhs, *work, *scratch, *dsum;
@@ -149,6 +152,9 @@ static int create(const pawsim_gpu_config* cfg, Model** out) {
   if (c.quad_drag_surf > 0 && c.hsml > 0)
     return fail(PAWSIM_GPU_EUNSUPPORTED, "quadratic surface drag with hsml > 0 is not built");
   if (c.tau_nrecs < 1 || c.wdia_nrecs < 1) return fail(PAWSIM_GPU_EBADCONFIG, "record counts must be positive");
+  if (c.use_tracer && (c.tracer_scheme < 0 || c.tracer_scheme > 2))
+    return fail(PAWSIM_GPU_EBADCONFIG, "Unknown or unsupported numerical scheme identifier");
+  if (c.use_tracer && (c.K2 < 0 || c.K4 < 0)) return fail(PAWSIM_GPU_EBADCONFIG, "K2 and K4 must be non-negative");
   if (c.solver < 0 || c.solver > 2) return fail(PAWSIM_GPU_EBADCONFIG, "Unknown pressureSolver identifier");
   Model* m = new Model();
   m->c = c;
@@ -169,6 +175,10 @@ static int create(const pawsim_gpu_config* cfg, Model** out) {
     ok &= (m->fu[b] = m->alloc<double>(Ls)) && (m->fv[b] = m->alloc<double>(Ls)) && (m->fh[b] = m->alloc<double>(Ls));
   }
   ok &= (m->dtu = m->alloc<double>(Ls)) && (m->dtv = m->alloc<double>(Ls)) && (m->dth = m->alloc<double>(Ls));
+  if (c.use_tracer) {
+    for (int b = 0; b < 2; ++b) ok &= (m->b[b] = m->alloc<double>(Ls)) && (m->fb[b] = m->alloc<double>(Ls));
+    ok &= (m->bRelax = m->alloc<double>(Ls)) && (m->bTime = m->alloc<double>(Ls));
+  }
   ok &= (m->wdia = m->alloc<double>((m->L + 1) * m->lstride)) != nullptr;
   ok &= (m->hhs = m->alloc<double>(m->plane)) && (m->hhb = m->alloc<double>(m->plane)) && (m->Hc = m->alloc<double>(m->plane));
   ok &= (m->omz = m->alloc<double>((size_t)(c.Ny + 1) * m->qpitch)) != nullptr;
@@ -198,6 +208,7 @@ static int create(const pawsim_gpu_config* cfg, Model** out) {
     fill_d(m->hRelax + k * m->lstride, m->lstride, 1000.0 / m->L);
     fill_d(m->eRelax + k * m->lstride, m->lstride, 1000.0 * k / m->L);
     fill_d(m->uTime + k * m->lstride, m->lstride, -1);
+    if (m->bTime) fill_d(m->bTime + k * m->lstride, m->lstride, -1);
     fill_d(m->vTime + k * m->lstride, m->lstride, -1);
     fill_d(m->eTime + k * m->lstride, m->lstride, -1);
     m->gg[k] = 9.81;
@@ -225,6 +236,11 @@ struct FieldRef {
 
 static_assert(AVG_LMAX == LMAX, "the averages kernel holds one column of LMAX layers");
 
+// running-average storage: 10 L + 2 fields, and L more for the tracer
+static size_t avg_elems(const Model* m) {
+  return (size_t)(10 * m->L + 2 + (m->b[0] ? m->L : 0)) * m->lstride;
+}
+
 // index of a per-layer running-average sum inside Model::avg (-1 for other names)
 static int avg_slot(const std::string& n) {
   static const char* names[9] = {"U_avg", "V_avg", "H_avg", "M_avg", "HU_avg", "HV_avg", "HUU_avg", "HVV_avg",
@@ -240,6 +256,9 @@ static bool lookup(Model* m, const std::string& n, FieldRef& f) {
   if (n == "u") { f.base = m->u[m->cur]; f.nk = L; }
   else if (n == "v") { f.base = m->v[m->cur]; f.nk = L; }
   else if (n == "h") { f.base = m->h[m->cur]; f.nk = L; }
+  else if (n == "b" && m->b[0]) { f.base = m->b[m->cur]; f.nk = L; }
+  else if (n == "bRelax" && m->bRelax) { f.base = m->bRelax; f.nk = L; }
+  else if (n == "bTime" && m->bTime) { f.base = m->bTime; f.nk = L; }
   else if (n == "uRelax") { f.base = m->uRelax; f.nk = L; }
   else if (n == "vRelax") { f.base = m->vRelax; f.nk = L; }
   else if (n == "hRelax") { f.base = m->hRelax; f.nk = L; }
@@ -276,6 +295,7 @@ static bool lookup(Model* m, const std::string& n, FieldRef& f) {
     else if (m->avg && avg_slot(n) >= 0) { f.base = m->avg + (size_t)avg_slot(n) * L * m->lstride; f.nk = L; }
     else if (m->avg && n == "W_avg") { f.base = m->avg + (size_t)9 * L * m->lstride; f.nk = L + 1; }
     else if (m->avg && n == "P_avg") f.base = m->avg + (size_t)(10 * L + 1) * m->lstride;
+    else if (m->avg && m->b[0] && n == "B_avg") { f.base = m->avg + (size_t)(10 * L + 2) * m->lstride; f.nk = L; }
     else return false;
   }
   return true;
@@ -474,6 +494,22 @@ static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
   if (launch_tendency(p, c.mom_scheme, c.thick_scheme, m->s) != 0)
     return fail(PAWSIM_GPU_EUNSUPPORTED, "scheme combination not available");
   ++g_launches;
+  if (c.use_tracer) {
+    // the tracer reads the state of the start of the step and the w_dia the tendency
+    // kernel just wrote; same AB coefficients and history slots
+    TracerParams tp;
+    tp.Nx = m->Nx; tp.Ny = m->Ny; tp.L = m->L; tp.pitch = m->pitch; tp.lstride = m->lstride;
+    tp.wall_ew = c.wall_ew; tp.wall_ns = c.wall_ns;
+    tp.scheme = c.tracer_scheme; tp.thick_scheme = c.thick_scheme; tp.kt00_sigma = c.KT00_sigma;
+    tp.dx = m->dx; tp.dy = m->dy; tp.K2 = c.K2; tp.K4 = c.K4;
+    tp.use_wdia = c.use_wdia;
+    tp.u = m->u[m->cur]; tp.v = m->v[m->cur]; tp.h = m->h[m->cur]; tp.b = m->b[m->cur];
+    tp.bRelax = m->bRelax; tp.bTime = m->bTime; tp.wdia = m->wdia;
+    tp.ab_mode = p.ab_mode; tp.c0 = p.c0; tp.c1 = p.c1; tp.c2 = p.c2; tp.write_hist = p.write_hist;
+    tp.f1b = m->fb[m->h1]; tp.f2b = m->fb[h2]; tp.fb_out = m->fb[h2]; tp.b_out = m->b[nb];
+    launch_tracer(tp, m->s);
+    ++g_launches;
+  }
   PAWSIM_CUDA_OK(cudaGetLastError());
   if (shift) m->h1 = h2;
   m->cur = nb;
@@ -679,7 +715,7 @@ int pawsim_gpu_accumulate_averages(pawsim_gpu* h, double avg_fac) {
   Model* m = h->m;
   if (!m->ready) return fail(PAWSIM_GPU_EBADCONFIG, "pawsim_gpu_init must follow the uploads");
   if (!m->avg) {
-    m->avg = m->alloc<double>((size_t)(10 * m->L + 2) * m->lstride);
+    m->avg = m->alloc<double>(avg_elems(m));
     if (!m->avg) return fail(PAWSIM_GPU_ECUDA, "average storage allocation failed");
   }
   const size_t ls = m->lstride;
@@ -694,6 +730,8 @@ int pawsim_gpu_accumulate_averages(pawsim_gpu* h, double avg_fac) {
   const size_t Ls = (size_t)m->L * ls;
   a.au = b; a.av = b + Ls; a.ah = b + 2 * Ls; a.aM = b + 3 * Ls; a.ahu = b + 4 * Ls; a.ahv = b + 5 * Ls;
   a.ahuu = b + 6 * Ls; a.ahvv = b + 7 * Ls; a.ahuv = b + 8 * Ls; a.aW = b + 9 * Ls; a.api = a.aW + Ls + ls;
+  a.b = m->b[0] ? m->b[m->cur] : nullptr;
+  a.ab = m->b[0] ? a.api + ls : nullptr;
   launch_accumulate_averages(m->grid2(), a, m->s);
   ++g_launches;
   PAWSIM_CUDA_OK(cudaGetLastError());
@@ -704,7 +742,7 @@ int pawsim_gpu_scale_averages(pawsim_gpu* h, double factor) {
   if (!h) return PAWSIM_GPU_EBADCONFIG;
   Model* m = h->m;
   if (!m->avg) return fail(PAWSIM_GPU_EBADCONFIG, "no averages accumulated");
-  launch_scale(m->avg, (size_t)(10 * m->L + 2) * m->lstride, factor, m->s);
+  launch_scale(m->avg, avg_elems(m), factor, m->s);
   ++g_launches;
   PAWSIM_CUDA_OK(cudaGetLastError());
   return 0;
@@ -714,7 +752,7 @@ int pawsim_gpu_zero_averages(pawsim_gpu* h) {
   if (!h) return PAWSIM_GPU_EBADCONFIG;
   Model* m = h->m;
   if (m->avg)
-    PAWSIM_CUDA_OK(cudaMemsetAsync(m->avg, 0, (size_t)(10 * m->L + 2) * m->lstride * sizeof(double), m->s));
+    PAWSIM_CUDA_OK(cudaMemsetAsync(m->avg, 0, avg_elems(m) * sizeof(double), m->s));
   return 0;
 }
 

@@ -475,6 +475,7 @@ __global__ void accumulate_averages_kernel(const Grid2 g, const AvgParams a) {
       ahuu[o] = shuu + d * hw * uc * uc;
       ahvv[o] = shvv + d * hs * vc * vc;
       ahuv[o] = shuv + d * hq * uq * vq;
+      if (a.ab) a.ab[o] += d * a.b[o];
     }
   }
   const size_t oL = (size_t)L * g.lstride + c;

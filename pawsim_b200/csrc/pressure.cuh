@@ -66,6 +66,8 @@ struct AvgParams {
   double gg[AVG_LMAX], geff[AVG_LMAX];
   const double *u, *v, *h, *pi, *hhb, *wdia;
   double *au, *av, *ah, *aM, *aW, *ahu, *ahv, *ahuu, *ahvv, *ahuv, *api;
+  const double* b;   // tracer (nullable) and its sums
+  double* ab;
 };
 void launch_accumulate_averages(const Grid2& g, const AvgParams& a, cudaStream_t s);
 // f[i] *= factor for n contiguous doubles

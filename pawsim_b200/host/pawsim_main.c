@@ -387,6 +387,9 @@ static int upload_inputs (pawsim_gpu * m, const config * c, const char * outdir)
           && put_layers(m,c,"eTimeFile","eTime",-1,0,plane,buf)
           && put_layers(m,c,"diaViscUFile","nu_u_dia",0,0,plane,buf)
           && put_layers(m,c,"diaViscVFile","nu_v_dia",0,0,plane,buf);
+  if (c->useTracer)   /* tracer state and restoring (state.c:968-1006: b 0, bRelax 0, bTime -1) */
+    ok = ok && put_layers(m,c,"bInitFile","b",0,0,plane,buf) && put_layers(m,c,"bRelaxFile","bRelax",0,0,plane,buf)
+            && put_layers(m,c,"bTimeFile","bTime",-1,0,plane,buf);
   ok = ok && put_plane(m,c,"hsFile","hhs",0,plane) && put_plane(m,c,"hbFile","hhb",0,plane)
           && put_plane(m,c,"uLidFile","uLid",0,plane) && put_plane(m,c,"vLidFile","vLid",0,plane)
           && put_plane(m,c,"FbaroXFile","Fbaro_x",0,plane) && put_plane(m,c,"FbaroYFile","Fbaro_y",0,plane)
@@ -471,11 +474,11 @@ static int upload_inputs (pawsim_gpu * m, const config * c, const char * outdir)
   /* restart: the U/V/H pickup files of the output directory (state.c:1106-1151) */
   if (ok && c->restart)
   {
-    const char * pre[3] = {"U","V","H"};
-    const char * nm[3] = {"u","v","h"};
+    const char * pre[4] = {"U","V","H","B"};
+    const char * nm[4] = {"u","v","h","b"};
     int a;
     for (k = 0; ok && k < L; k ++)
-      for (a = 0; ok && a < 3; a ++)
+      for (a = 0; ok && a < (c->useTracer ? 4 : 3); a ++)
       {
         snprintf(path,sizeof(path),"%s/%s%u_n=%u.dat",outdir,pre[a],k,c->startIdx);
         ok = read_f64(path,plane,N) && put(m,nm[a],(int) k,plane,N);
@@ -492,12 +495,12 @@ static int write_state (pawsim_gpu * m, const config * c, const char * outdir, u
   const size_t N = (size_t) c->Nx * c->Ny;
   char name[NAMELEN];
   unsigned k;
-  const char * pre[3] = {"U","V","H"};
-  const char * nm[3] = {"u","v","h"};
+  const char * pre[4] = {"U","V","H","B"};
+  const char * nm[4] = {"u","v","h","b"};
   int a;
   for (k = 0; k < c->Nlay; k ++)
   {
-    for (a = 0; a < 3; a ++)
+    for (a = 0; a < (c->useTracer ? 4 : 3); a ++)
     {
       snprintf(name,sizeof(name),"%s%u_n=%u.dat",pre[a],k,n);
       if (!gpu_ok(pawsim_gpu_get_field(m,nm[a],(int) k,plane,N),nm[a]) || !write_f64(outdir,name,plane,N))
@@ -527,11 +530,18 @@ static int write_averages (pawsim_gpu * m, const config * c, const char * outdir
   unsigned k;
   int a;
   for (k = 0; k < c->Nlay; k ++)
+  {
     for (a = 0; a < 10; a ++)
     {
       snprintf(name,sizeof(name),"%s%u_n=%u.dat",nm[a],k,n);
       if (!gpu_ok(pawsim_gpu_get_field(m,nm[a],(int) k,plane,N),nm[a]) || !write_f64(outdir,name,plane,N)) return 0;
     }
+    if (c->useTracer)
+    {
+      snprintf(name,sizeof(name),"B_avg%u_n=%u.dat",k,n);
+      if (!gpu_ok(pawsim_gpu_get_field(m,"B_avg",(int) k,plane,N),"B_avg") || !write_f64(outdir,name,plane,N)) return 0;
+    }
+  }
   snprintf(name,sizeof(name),"W_avg%u_n=%u.dat",c->Nlay,n);
   if (!gpu_ok(pawsim_gpu_get_field(m,"W_avg",(int) c->Nlay,plane,N),"W_avg") || !write_f64(outdir,name,plane,N))
     return 0;
@@ -615,9 +625,12 @@ int main (int argc, char ** argv)
   g.mg_pre = 1; g.mg_post = 1; g.mg_omega = -1.0;   /* weight chosen by the solver */
   g.serial_sums = -1;
   g.mg_tile = 0;
-  if (c.useTracer)
+  g.use_tracer = c.useTracer;
+  g.tracer_scheme = (int) c.tracerScheme;
+  g.K2 = c.K2; g.K4 = c.K4;
+  if (c.useTracer && (c.useBuoyancy || file_of(&c,"diaDiffFile")[0] || file_of(&c,"bFluxFile")[0]))
   {
-    fprintf(stderr,"ERROR: the tracer equation is not built on the GPU\n");
+    fprintf(stderr,"ERROR: the tracer's buoyancy coupling and diapycnal diffusion are not built on the GPU\n");
     return 1;
   }
 

@@ -300,6 +300,7 @@ def load_fields(cfg: Config) -> dict:
         "Fbaro_y": np.zeros((Ny, Nx)), "hTime": np.full((Ny, Nx), -1.0),
         "taux": np.zeros((nt, Ny, Nx)), "tauy": np.zeros((nt, Ny, Nx)),
         "wdia_ff": np.zeros((nw, L + 1, Ny, Nx)),
+        "b": np.zeros((L, Ny, Nx)), "bRelax": np.zeros((L, Ny, Nx)), "bTime": np.full((L, Ny, Nx), -1.0),
     }
 
     def rd2(key, name):
@@ -326,6 +327,9 @@ def load_fields(cfg: Config) -> dict:
                       ("uTimeFile", "uTime"), ("vTimeFile", "vTime"), ("eTimeFile", "eTime"),
                       ("diaViscUFile", "nu_u_dia"), ("diaViscVFile", "nu_v_dia")):
         rd3(key, name)
+    if v["useTracer"]:
+        for key, name in (("bInitFile", "b"), ("bRelaxFile", "bRelax"), ("bTimeFile", "bTime")):
+            rd3(key, name)
     for key, name in (("tauxFile", "taux"), ("tauyFile", "tauy")):
         p = _resolve(cfg, key)
         if p:
@@ -345,6 +349,34 @@ def load_fields(cfg: Config) -> dict:
 # ------------------------------------------------------------- synthetic set-ups
 
 RHO0 = 1000.0
+
+
+def add_tracer(param_path, scheme=2, relax_days=100.0, K2=0.0, K4=0.0, amp=1.0, seed=7):
+    """Add a passive tracer to an existing set-up: b = amp * (sin(2 pi y / Ly) + noise) per
+    layer (bInitFile), relaxation to it on relax_days (bRelaxFile, bTimeFile; <= 0 turns
+    relaxation off), tracerScheme and the K2 / K4 diffusivities. Returns the parameter path."""
+    cfg = read_config(param_path)
+    v = cfg.values
+    L, Nx, Ny = v["Nlay"], v["Nx"], v["Ny"]
+    rng = np.random.default_rng(seed)
+    y = (np.arange(Ny) + 0.5) / Ny
+    b = np.stack([amp * (np.sin(2 * np.pi * (y + 0.1 * k))[:, None] * np.ones((1, Nx))
+                         + 0.1 * _smoothed_noise(rng, Ny, Nx, 1.0, 3, True, True)) for k in range(L)])
+    d = os.path.dirname(param_path)
+    write_data(os.path.join(d, "bInit.dat"), _layer_stack(b))
+    write_data(os.path.join(d, "bRelax.dat"), _layer_stack(b))
+    t = relax_days * 86400.0 if relax_days > 0 else -1.0
+    write_data(os.path.join(d, "bTime.dat"), _layer_stack(np.full((L, Ny, Nx), t)))
+    params = {}
+    with open(param_path) as fh:
+        for line in fh:
+            parts = line.split()
+            if len(parts) >= 2:
+                params[parts[0]] = parts[1]
+    params.update(useTracer=1, tracerScheme=scheme, K2=K2, K4=K4, bInitFile="bInit.dat",
+                  bRelaxFile="bRelax.dat", bTimeFile="bTime.dat")
+    write_param_file(param_path, params)
+    return param_path
 
 
 def _smoothed_noise(rng, ny, nx, sigma, width, periodic_x, periodic_y):

@@ -49,6 +49,21 @@ AVG_CASES = {
 }
 AVG_FIELDS = ["U_avg", "V_avg", "H_avg", "M_avg", "W_avg", "HU_avg", "HV_avg", "HUU_avg", "HVV_avg",
               "HUV_avg"]
+# passive tracer cases (work.c:1947-2144): the three tracer schemes with K2, K4, w_dia and
+# relaxation; SOR pressure keeps them bit-exact. (set-up, its arguments, add_tracer arguments)
+TRC_NSTEPS = 4
+TRC_CASES = {
+    "jets_tracer_kt00": (inputs.jets, dict(N=16, dt=100.0, solver=0, tol=1e-10),
+                         dict(scheme=2, relax_days=100.0)),
+    "gyre_tracer_up3": (inputs.gyre, dict(N=16, Ny=12, dt=900.0, solver=0, tol=1e-10),
+                        dict(scheme=1, relax_days=-1.0, K2=200.0, K4=1e9)),
+    "gyre_tracer_al81_hk83": (inputs.gyre, dict(N=20, Ny=12, dt=600.0, solver=0, tol=1e-10,
+                                                extra=dict(thicknessScheme=1)),
+                              dict(scheme=0, relax_days=30.0, K2=500.0)),
+    "full_tracer_kt00": (inputs.full_physics, dict(N=16, dt=50.0, solver=0, Ly=320e3, bathy_len=20e3,
+                                                   sponge=40e3, extra=dict(savefreqAvg=125.0)),
+                         dict(scheme=2, relax_days=30.0, K4=1e8)),
+}
 LINE = re.compile(r"iters=(\d+) walltime=\S+ s residual_max=(\S+) residual_rms=(\S+) "
                   r"div_max=(\S+) div_rms=(\S+)")
 
@@ -109,6 +124,38 @@ def make_avg(name, fn, kw, outdir):
         np.savez_compressed(os.path.join(outdir, name + ".npz"), **rec)
 
 
+def make_tracer(name, fn, kw, tkw, outdir):
+    """Inputs (with the tracer files) and the reference's U/V/H/B/P after each step, plus the
+    online-average files when the set-up asks for them."""
+    with tempfile.TemporaryDirectory() as d:
+        kw = dict(kw)
+        extra = dict(kw.pop("extra", {}) or {})
+        dt = kw["dt"]
+        p = fn(os.path.join(d, "in"), Nt=TRC_NSTEPS, savefrequency=dt, extra=extra, **kw)
+        inputs.add_tracer(p, **tkw)
+        cfg = inputs.read_config(p)
+        out = os.path.join(d, "out")
+        os.makedirs(out)
+        subprocess.run([oracle.reference_exe(), p, out], capture_output=True, text=True, check=True)
+        L, Nx, Ny = cfg.Nlay, cfg.Nx, cfg.Ny
+        rec = {"param_text": np.array(open(p).read())}
+        for f in sorted(os.listdir(os.path.dirname(p))):
+            if f.endswith(".dat") and f != "params.dat":
+                rec["in_" + f] = np.fromfile(os.path.join(os.path.dirname(p), f), dtype="<f8")
+        for n in range(0, TRC_NSTEPS + 1):
+            for k in range(L):
+                for v in ("U", "V", "H", "B"):
+                    rec[f"{v}{k}_{n}"] = inputs.read_data(os.path.join(out, f"{v}{k}_n={n}.dat"), (Ny, Nx))
+            rec[f"P_{n}"] = inputs.read_data(os.path.join(out, f"P_n={n}.dat"), (Ny, Nx))
+        windows = sorted({int(f.split("_n=")[1][:-4]) for f in os.listdir(out) if f.startswith("B_avg0_n=")})
+        rec["windows"] = np.array(windows, dtype=int)
+        for n in windows:
+            for k in range(L):
+                rec[f"B_avg{k}_{n}"] = inputs.read_data(os.path.join(out, f"B_avg{k}_n={n}.dat"), (Ny, Nx))
+                rec[f"U_avg{k}_{n}"] = inputs.read_data(os.path.join(out, f"U_avg{k}_n={n}.dat"), (Ny, Nx))
+        np.savez_compressed(os.path.join(outdir, name + ".npz"), **rec)
+
+
 if __name__ == "__main__":
     # python tests/golden/make_golden.py [case ...]   (all cases when none are named)
     oracle.build(ref=True)
@@ -121,4 +168,9 @@ if __name__ == "__main__":
         if len(sys.argv) > 1 and name not in sys.argv[1:]:
             continue
         make_avg(name, fn, kw, HERE)
+        print("wrote", name)
+    for name, (fn, kw, tkw) in TRC_CASES.items():
+        if len(sys.argv) > 1 and name not in sys.argv[1:]:
+            continue
+        make_tracer(name, fn, kw, tkw, HERE)
         print("wrote", name)
