@@ -150,6 +150,36 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def tracer_timing(cfg, stream, reps):
+    """Device time of the tracer kernel per step: integrator steps of the same set-up with and
+    without a passive tracer (CUDA events on the model's stream), the difference."""
+    import tempfile as _tf
+    import pawsim_b200
+    out = []
+    with _tf.TemporaryDirectory() as d:
+        for tracer in (False, True):
+            p = pawsim_b200.inputs.gyre(d + f"/t{int(tracer)}", N=N_GRID, solver=1, dt=DT)
+            if tracer:
+                pawsim_b200.inputs.add_tracer(p, scheme=2, relax_days=100.0, K2=100.0)
+            c = pawsim_b200.inputs.read_config(p)
+            m = pawsim_b200.Model(c)
+            m.set_stream(stream.cuda_stream)
+            with torch.cuda.stream(stream):
+                m.prelim()
+                for n in range(1, 4):
+                    m.integrator_step(n)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record(stream)
+                for n in range(4, 4 + reps):
+                    m.integrator_step(n)
+                e1.record(stream)
+                torch.cuda.synchronize()
+            out.append(e0.elapsed_time(e1) / reps)
+            m.close()
+    return out[1] - out[0]
+
+
 def pressure_comparison(cfg, fields, stream, spin, steps, epochs, pairs):
     """Pressure ms/step and V-cycles/step of the plain FP64 multigrid (started from the
     previous pressure, as the reference's solver is) against FP32 V-cycles in FP64 defect
@@ -365,12 +395,20 @@ def main():
                      "algorithmic_bytes": alg_bytes, "peak_kind": peak_kind},
         "clocks": clk.summary(),
     }
+    # the passive tracer (a set-up with useTracer: KT00 advection, K2, relaxation) on the same
+    # grid, not part of the headline step
+    tr = tracer_timing(cfg, stream, args.steps)
     # bytes per cell: read u, v, h and pi, hhb, w_dia; read and write the 10 L + 2 sums
     avg_bytes = ncell * (24 * L + 8 * (L + 3) + 16 * (10 * L + 2))
     line["averages"] = {"kernel": "accumulate_averages_kernel", "ms_per_step": avg_ms,
                         "algorithmic_bytes": avg_bytes,
                         "achieved_gbs": avg_bytes / (avg_ms / 1e3) / 1e9,
                         "frac": avg_bytes / (avg_ms / 1e3) / 1e9 / peak}
+    if tr is not None:
+        tr_bytes = ncell * L * 88   # read u, v, h, b, bRelax, bTime, f1, f2, w_dia; write b, f
+        line["tracer"] = {"kernel": "tracer_tile_kernel (KT00, K2, relaxation)", "ms_per_step": tr,
+                          "algorithmic_bytes": tr_bytes, "achieved_gbs": tr_bytes / (tr / 1e3) / 1e9,
+                          "frac": tr_bytes / (tr / 1e3) / 1e9 / peak}
     if ws is not None:
         line["pressure_learned_fp32_vs_plain_fp64"] = ws
     if rank == 0 and not args.no_cpu_baseline:

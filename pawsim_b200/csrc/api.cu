@@ -502,6 +502,8 @@ static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
     tp.wall_ew = c.wall_ew; tp.wall_ns = c.wall_ns;
     tp.scheme = c.tracer_scheme; tp.thick_scheme = c.thick_scheme; tp.kt00_sigma = c.KT00_sigma;
     tp.dx = m->dx; tp.dy = m->dy; tp.K2 = c.K2; tp.K4 = c.K4;
+    tp.rdx = 1.0 / m->dx; tp.rdy = 1.0 / m->dy;
+    tp.rdxsq = 1.0 / (m->dx * m->dx); tp.rdysq = 1.0 / (m->dy * m->dy);
     tp.use_wdia = c.use_wdia;
     tp.u = m->u[m->cur]; tp.v = m->v[m->cur]; tp.h = m->h[m->cur]; tp.b = m->b[m->cur];
     tp.bRelax = m->bRelax; tp.bTime = m->bTime; tp.wdia = m->wdia;

@@ -1,12 +1,10 @@
 // tracer.cu -- passive tracer tendency and Adams-Bashforth update (see tracer.cuh).
 //
-// One thread per owned cell and layer, reading its stencil through the boundary maps of
-// common.cuh (cached loads; the tracer is a small share of a step). The ghost semantics are
-// those of the fused tendency kernel: b is a scalar mirrored at walls; the face thickness
-// h_west / h_south, which the reference re-fills after computing it, is evaluated at the
-// mirrored owned position; the fields the reference computes over its ghost ring and never
-// re-fills (h u, h v, the tracer gradients and fluxes, BB4) are evaluated directly at the
-// ghost position. Expression order follows work.c:1947-2144 so that the results are those
+// The ghost semantics are those of the fused tendency kernel: b is a scalar mirrored at
+// walls; the face thickness h_west / h_south, which the reference re-fills after computing
+// it, is evaluated at the mirrored owned position; the fields the reference computes over
+// its ghost ring and never re-fills (h u, h v, the tracer gradients and fluxes, BB4) are
+// evaluated directly at the ghost position. Expression order follows work.c:1947-2144 so that the results are those
 // of the reference bit for bit (this file is compiled with -fmad=false).
 #include "common.cuh"
 #include "tracer.cuh"
@@ -15,138 +13,200 @@ namespace pawsim {
 
 namespace {
 
-struct TView {
-  const TracerParams& p;
-  const double *u, *v, *h, *b;
-  __device__ double B(int a, int c) const {
-    return load_mapped(b, p.pitch, a, c, p.Nx, p.Ny, p.wall_ew, p.wall_ns, MAP_S, MAP_S);
-  }
-  __device__ double Hc(int a, int c) const {
-    return load_mapped(h, p.pitch, a, c, p.Nx, p.Ny, p.wall_ew, p.wall_ns, MAP_S, MAP_S);
-  }
-  __device__ double U(int a, int c) const {
-    return load_mapped(u, p.pitch, a, c, p.Nx, p.Ny, p.wall_ew, p.wall_ns, MAP_N, MAP_S);
-  }
-  __device__ double V(int a, int c) const {
-    return load_mapped(v, p.pitch, a, c, p.Nx, p.Ny, p.wall_ew, p.wall_ns, MAP_S, MAP_N);
-  }
-  __device__ int mx(int a) const { return map_axis(a, p.Nx, p.wall_ew, MAP_S).idx; }
-  __device__ int my(int c) const { return map_axis(c, p.Ny, p.wall_ns, MAP_S).idx; }
+// minmod of three slopes (defs.c:1000-1014)
+__device__ inline double mm3(double x, double y, double z) {
+  if ((x > 0) && (y > 0) && (z > 0)) return fmin(x, fmin(y, z));
+  if ((x < 0) && (y < 0) && (z < 0)) return fmax(x, fmax(y, z));
+  return 0;
+}
 
-  // face thickness of work.c:566-684 at an owned cell (i, j)
-  __device__ double face_w_owned(int i, int j) const {
-    auto H = [&](int a, int c) { return Hc(a, c); };
-    const int TS = p.thick_scheme;
-    if (TS == 1)
-      return (1.0 / 3) * (H(i, j) + H(i - 1, j) + 0.25 * (H(i, j + 1) + H(i - 1, j + 1) + H(i, j - 1) + H(i - 1, j - 1)));
-    if (TS == 2 || TS == 3) {
-      const double uc = U(i, j);
-      if (TS == 2) {
-        const double d2m = H(i, j) - 2 * H(i - 1, j) + H(i - 2, j);
-        const double d2c = H(i + 1, j) - 2 * H(i, j) + H(i - 1, j);
-        return 0.5 * (H(i, j) + H(i - 1, j)) - (1 / 6.0) * ((uc > 0) ? d2m : d2c);
-      }
-      const double sg = p.kt00_sigma;
-      const double dm = mm3(sg * (H(i, j) - H(i - 1, j)), 0.5 * (H(i, j) - H(i - 2, j)), sg * (H(i - 1, j) - H(i - 2, j)));
-      const double dc = mm3(sg * (H(i + 1, j) - H(i, j)), 0.5 * (H(i + 1, j) - H(i - 1, j)), sg * (H(i, j) - H(i - 1, j)));
-      return (uc > 0) ? H(i - 1, j) + 0.5 * dm : H(i, j) - 0.5 * dc;
-    }
-    return 0.5 * (H(i, j) + H(i - 1, j));
-  }
-  __device__ double face_s_owned(int i, int j) const {
-    auto H = [&](int a, int c) { return Hc(a, c); };
-    const int TS = p.thick_scheme;
-    if (TS == 1)
-      return (1.0 / 3) * (H(i, j) + H(i, j - 1) + 0.25 * (H(i + 1, j) + H(i - 1, j) + H(i + 1, j - 1) + H(i - 1, j - 1)));
-    if (TS == 2 || TS == 3) {
-      const double vc = V(i, j);
-      if (TS == 2) {
-        const double d2m = H(i, j) - 2 * H(i, j - 1) + H(i, j - 2);
-        const double d2c = H(i, j + 1) - 2 * H(i, j) + H(i, j - 1);
-        return 0.5 * (H(i, j) + H(i, j - 1)) - (1 / 6.0) * ((vc > 0) ? d2m : d2c);
-      }
-      const double sg = p.kt00_sigma;
-      const double dm = mm3(sg * (H(i, j) - H(i, j - 1)), 0.5 * (H(i, j) - H(i, j - 2)), sg * (H(i, j - 1) - H(i, j - 2)));
-      const double dc = mm3(sg * (H(i, j + 1) - H(i, j)), 0.5 * (H(i, j + 1) - H(i, j - 1)), sg * (H(i, j) - H(i, j - 1)));
-      return (vc > 0) ? H(i, j - 1) + 0.5 * dm : H(i, j) + 0.5 * dc;
-    }
-    return 0.5 * (H(i, j) + H(i, j - 1));
-  }
-  // re-filled fields: the value of the mirrored owned position
-  __device__ double Hw(int a, int c) const { return face_w_owned(mx(a), my(c)); }
-  __device__ double Hs(int a, int c) const { return face_s_owned(mx(a), my(c)); }
-  // layer mass fluxes (work.c:162-186), at the raw position
-  __device__ double huu(int a, int c) const { return U(a, c) * Hw(a, c); }
-  __device__ double hvv(int a, int c) const { return V(a, c) * Hs(a, c); }
+// ---------------------------------------------------------------- tile kernel
+// One CTA owns a TTX x TTY tile and walks its layers. u, v, h, b are staged in shared memory over a
+// TH-cell halo with the boundary maps; then, in stages separated by barriers, the face
+// thickness (at the mirrored owned position), the mass fluxes, the scheme's
+// gradients or second differences, the tracer fluxes and BB4 are formed over the part of
+// the halo the owned cells read; finally each thread forms its cell's tendency and AB update.
+constexpr int TTX = 32, TTY = 16, TNT = TTX * TTY, TH = 3;
+constexpr int TRW = TTX + 2 * TH, TRH = TTY + 2 * TH, TRN = TRW * TRH;
+enum { T_U, T_V, T_H, T_B, T_HW, T_HS, T_HUU, T_HVV, T_X1, T_X2, T_HUB, T_HVB, T_BB4, T_NUM };
 
-  // minmod of three slopes (defs.c:1000-1014)
-  __device__ static double mm3(double x, double y, double z) {
-    if ((x > 0) && (y > 0) && (z > 0)) return fmin(x, fmin(y, z));
-    if ((x < 0) && (y < 0) && (z < 0)) return fmax(x, fmax(y, z));
-    return 0;
-  }
-
-  // tracer gradients and fluxes (work.c:1967-2053), at the raw position
-  __device__ double db_dx(int a, int c) const { return (B(a, c) - B(a - 1, c)) / p.dx; }
-  __device__ double db_dy(int a, int c) const { return (B(a, c) - B(a, c - 1)) / p.dy; }
-  __device__ double d2bx(int a, int c) const { return B(a + 1, c) - 2 * B(a, c) + B(a - 1, c); }
-  __device__ double d2by(int a, int c) const { return B(a, c + 1) - 2 * B(a, c) + B(a, c - 1); }
-  __device__ double kt_dx(int a, int c) const {
-    const double s = p.kt00_sigma;
-    return mm3(s * (B(a + 1, c) - B(a, c)), 0.5 * (B(a + 1, c) - B(a - 1, c)), s * (B(a, c) - B(a - 1, c))) / p.dx;
-  }
-  __device__ double kt_dy(int a, int c) const {
-    const double s = p.kt00_sigma;
-    return mm3(s * (B(a, c + 1) - B(a, c)), 0.5 * (B(a, c + 1) - B(a, c - 1)), s * (B(a, c) - B(a, c - 1))) / p.dy;
-  }
-  __device__ double hub(int a, int c) const {
-    if (p.scheme == 1) {
-      double r = 0.5 * (B(a, c) + B(a - 1, c)) - (1 / 6.0) * ((U(a, c) > 0) ? d2bx(a - 1, c) : d2bx(a, c));
-      return r * huu(a, c);
-    }
-    const double b_xm = B(a - 1, c) + 0.5 * kt_dx(a - 1, c) * p.dx;
-    const double b_xp = B(a, c) - 0.5 * kt_dx(a, c) * p.dx;
-    return ((U(a, c) > 0) ? b_xm : b_xp) * huu(a, c);
-  }
-  __device__ double hvb(int a, int c) const {
-    if (p.scheme == 1) {
-      double r = 0.5 * (B(a, c) + B(a, c - 1)) - (1 / 6.0) * ((V(a, c) > 0) ? d2by(a, c - 1) : d2by(a, c));
-      return r * hvv(a, c);
-    }
-    const double b_ym = B(a, c - 1) + 0.5 * kt_dy(a, c - 1) * p.dy;
-    const double b_yp = B(a, c) + 0.5 * kt_dy(a, c) * p.dy;
-    return ((V(a, c) > 0) ? b_ym : b_yp) * hvv(a, c);
-  }
-  // thickness-weighted Laplacian of f over the face thickness (the K2 bracket and BB4's)
-  template <typename F>
-  __device__ double lap(F f, int a, int c) const {
-    const double dxsq = p.dx * p.dx, dysq = p.dy * p.dy;
-    return (Hw(a + 1, c) * (f(a + 1, c) - f(a, c)) - Hw(a, c) * (f(a, c) - f(a - 1, c))) / dxsq
-         + (Hs(a, c + 1) * (f(a, c + 1) - f(a, c)) - Hs(a, c) * (f(a, c) - f(a, c - 1))) / dysq;
-  }
-  __device__ double BB4(int a, int c) const {
-    return lap([&](int x, int y) { return B(x, y); }, a, c) / Hc(a, c);
-  }
-};
-
-__global__ void tracer_kernel(const TracerParams p) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
-  if (i >= p.Nx || j >= p.Ny) return;
+__global__ void __launch_bounds__(TNT) tracer_tile_kernel(const TracerParams p) {
+  extern __shared__ double tsm[];
+  double (*S)[TRN] = reinterpret_cast<double (*)[TRN]>(tsm);
+  const int tid = threadIdx.x;
+  const int X0 = blockIdx.x * TTX, Y0 = blockIdx.y * TTY;
+  // tiles whose halo lies inside the domain load without boundary maps
+  const bool inner = X0 - TH >= 0 && X0 + TTX + TH <= p.Nx && Y0 - TH >= 0 && Y0 + TTY + TH <= p.Ny;
+  const double dx = p.dx, dy = p.dy;
+  auto at = [](int x, int y) { return y * TRW + x; };
+  // local index of the owned cell a filled field copies at local x (y): the MAP_S mirror
+  auto mlx = [&](int lx) {
+    if (!p.wall_ew) return lx;
+    int g = X0 - TH + lx;
+    if (g < 0) g = -g - 1;
+    else if (g >= p.Nx) g = 2 * p.Nx - g - 1;
+    return g - X0 + TH;
+  };
+  auto mly = [&](int ly) {
+    if (!p.wall_ns) return ly;
+    int g = Y0 - TH + ly;
+    if (g < 0) g = -g - 1;
+    else if (g >= p.Ny) g = 2 * p.Ny - g - 1;
+    return g - Y0 + TH;
+  };
+  for (int k = 0; k < p.L; ++k) {
   const size_t lk = (size_t)k * p.lstride;
-  const TView t{p, p.u + lk, p.v + lk, p.h + lk, p.b + lk};
+  const double *uk = p.u + lk, *vk = p.v + lk, *hk = p.h + lk, *bk = p.b + lk;
+  __syncthreads();   // the previous layer's stages are done with the tile
+  // stage 0: the layer's u, v, h, b with the reference's ghost values
+  if (inner) {
+    for (int q = tid; q < TRN; q += TNT) {
+      const int lx = q % TRW, ly = q / TRW;
+      const size_t g = (size_t)(Y0 - TH + ly) * p.pitch + (X0 - TH + lx);
+      S[T_U][q] = uk[g];
+      S[T_V][q] = vk[g];
+      S[T_H][q] = hk[g];
+      S[T_B][q] = bk[g];
+    }
+  } else {
+    for (int q = tid; q < TRN; q += TNT) {
+      const int lx = q % TRW, ly = q / TRW;
+      const int gx = X0 - TH + lx, gy = Y0 - TH + ly;
+      const bool in = gx >= -TH && gx < p.Nx + TH && gy >= -TH && gy < p.Ny + TH;
+      S[T_U][q] = in ? load_mapped(uk, p.pitch, gx, gy, p.Nx, p.Ny, p.wall_ew, p.wall_ns, MAP_N, MAP_S) : 0.0;
+      S[T_V][q] = in ? load_mapped(vk, p.pitch, gx, gy, p.Nx, p.Ny, p.wall_ew, p.wall_ns, MAP_S, MAP_N) : 0.0;
+      S[T_H][q] = in ? load_mapped(hk, p.pitch, gx, gy, p.Nx, p.Ny, p.wall_ew, p.wall_ns, MAP_S, MAP_S) : 0.0;
+      S[T_B][q] = in ? load_mapped(bk, p.pitch, gx, gy, p.Nx, p.Ny, p.wall_ew, p.wall_ns, MAP_S, MAP_S) : 0.0;
+    }
+  }
+  __syncthreads();
+  const double* SU = S[T_U];
+  const double* SV = S[T_V];
+  const double* SH = S[T_H];
+  const double* SB = S[T_B];
+  // face thickness of work.c:566-684 at local (i, j) of an owned cell
+  auto face_w = [&](int i, int j) {
+    auto Hh = [&](int a, int c) { return SH[at(a, c)]; };
+    const int TS = p.thick_scheme;
+    if (TS == 1)
+      return (1.0 / 3) * (Hh(i, j) + Hh(i - 1, j) + 0.25 * (Hh(i, j + 1) + Hh(i - 1, j + 1) + Hh(i, j - 1) + Hh(i - 1, j - 1)));
+    if (TS == 2 || TS == 3) {
+      const double uc = SU[at(i, j)];
+      if (TS == 2) {
+        const double d2m = Hh(i, j) - 2 * Hh(i - 1, j) + Hh(i - 2, j);
+        const double d2c = Hh(i + 1, j) - 2 * Hh(i, j) + Hh(i - 1, j);
+        return 0.5 * (Hh(i, j) + Hh(i - 1, j)) - (1 / 6.0) * ((uc > 0) ? d2m : d2c);
+      }
+      const double sg = p.kt00_sigma;
+      const double dm = mm3(sg * (Hh(i, j) - Hh(i - 1, j)), 0.5 * (Hh(i, j) - Hh(i - 2, j)), sg * (Hh(i - 1, j) - Hh(i - 2, j)));
+      const double dc = mm3(sg * (Hh(i + 1, j) - Hh(i, j)), 0.5 * (Hh(i + 1, j) - Hh(i - 1, j)), sg * (Hh(i, j) - Hh(i - 1, j)));
+      return (uc > 0) ? Hh(i - 1, j) + 0.5 * dm : Hh(i, j) - 0.5 * dc;
+    }
+    return 0.5 * (Hh(i, j) + Hh(i - 1, j));
+  };
+  auto face_s = [&](int i, int j) {
+    auto Hh = [&](int a, int c) { return SH[at(a, c)]; };
+    const int TS = p.thick_scheme;
+    if (TS == 1)
+      return (1.0 / 3) * (Hh(i, j) + Hh(i, j - 1) + 0.25 * (Hh(i + 1, j) + Hh(i - 1, j) + Hh(i + 1, j - 1) + Hh(i - 1, j - 1)));
+    if (TS == 2 || TS == 3) {
+      const double vc = SV[at(i, j)];
+      if (TS == 2) {
+        const double d2m = Hh(i, j) - 2 * Hh(i, j - 1) + Hh(i, j - 2);
+        const double d2c = Hh(i, j + 1) - 2 * Hh(i, j) + Hh(i, j - 1);
+        return 0.5 * (Hh(i, j) + Hh(i, j - 1)) - (1 / 6.0) * ((vc > 0) ? d2m : d2c);
+      }
+      const double sg = p.kt00_sigma;
+      const double dm = mm3(sg * (Hh(i, j) - Hh(i, j - 1)), 0.5 * (Hh(i, j) - Hh(i, j - 2)), sg * (Hh(i, j - 1) - Hh(i, j - 2)));
+      const double dc = mm3(sg * (Hh(i, j + 1) - Hh(i, j)), 0.5 * (Hh(i, j + 1) - Hh(i, j - 1)), sg * (Hh(i, j) - Hh(i, j - 1)));
+      return (vc > 0) ? Hh(i, j - 1) + 0.5 * dm : Hh(i, j) + 0.5 * dc;
+    }
+    return 0.5 * (Hh(i, j) + Hh(i, j - 1));
+  };
+  // stage 1: face thickness (local 2 .. RW-2 / RH-2) and the scheme's gradients
+  for (int q = tid; q < TRN; q += TNT) {
+    const int lx = q % TRW, ly = q / TRW;
+    if (lx >= 2 && lx <= TRW - 2 && ly >= 2 && ly <= TRH - 2) {
+      // owned cells read the face thickness at most two cells beyond the domain; there the
+      // mirrored owned position's stencil is inside the tile
+      const int gx = X0 - TH + lx, gy = Y0 - TH + ly;
+      const bool nr = gx >= -2 && gx < p.Nx + 2 && gy >= -2 && gy < p.Ny + 2;
+      const int mx = mlx(lx), my = mly(ly);
+      S[T_HW][q] = nr ? face_w(mx, my) : 0.0;
+      S[T_HS][q] = nr ? face_s(mx, my) : 0.0;
+    }
+    if (lx >= 1 && lx <= TRW - 2 && ly >= 1 && ly <= TRH - 2) {
+      if (p.scheme == 0) {
+        S[T_X1][q] = SU[q] * div_rn(SB[q] - SB[q - 1], dx, p.rdx);
+        S[T_X2][q] = SV[q] * div_rn(SB[q] - SB[q - TRW], dy, p.rdy);
+      } else if (p.scheme == 1) {
+        S[T_X1][q] = SB[q + 1] - 2 * SB[q] + SB[q - 1];
+        S[T_X2][q] = SB[q + TRW] - 2 * SB[q] + SB[q - TRW];
+      } else {
+        const double sg = p.kt00_sigma;
+        S[T_X1][q] = div_rn(mm3(sg * (SB[q + 1] - SB[q]), 0.5 * (SB[q + 1] - SB[q - 1]), sg * (SB[q] - SB[q - 1])), dx,
+                            p.rdx);
+        S[T_X2][q] = div_rn(mm3(sg * (SB[q + TRW] - SB[q]), 0.5 * (SB[q + TRW] - SB[q - TRW]), sg * (SB[q] - SB[q - TRW])),
+                            dy, p.rdy);
+      }
+    }
+  }
+  __syncthreads();
+  const double* HW = S[T_HW];
+  const double* HS = S[T_HS];
+  const double* X1 = S[T_X1];
+  const double* X2 = S[T_X2];
+  const double dxsq = dx * dx, dysq = dy * dy;
+  // thickness-weighted Laplacian over the face thickness (the K2 bracket and BB4's)
+  auto lap = [&](const double* F, int q) {
+    return div_rn(HW[q + 1] * (F[q + 1] - F[q]) - HW[q] * (F[q] - F[q - 1]), dxsq, p.rdxsq)
+         + div_rn(HS[q + TRW] * (F[q + TRW] - F[q]) - HS[q] * (F[q] - F[q - TRW]), dysq, p.rdysq);
+  };
+  // stage 2: mass fluxes, tracer fluxes (local 2 .. RW-2) and BB4 (owned +- 1)
+  for (int q = tid; q < TRN; q += TNT) {
+    const int lx = q % TRW, ly = q / TRW;
+    if (lx >= 2 && lx <= TRW - 2 && ly >= 2 && ly <= TRH - 2) {
+      const double huu = SU[q] * HW[q], hvv = SV[q] * HS[q];
+      S[T_HUU][q] = huu;
+      S[T_HVV][q] = hvv;
+      if (p.scheme == 1) {
+        double r = 0.5 * (SB[q] + SB[q - 1]) - (1 / 6.0) * ((SU[q] > 0) ? X1[q - 1] : X1[q]);
+        S[T_HUB][q] = r * huu;
+        r = 0.5 * (SB[q] + SB[q - TRW]) - (1 / 6.0) * ((SV[q] > 0) ? X2[q - TRW] : X2[q]);
+        S[T_HVB][q] = r * hvv;
+      } else if (p.scheme == 2) {
+        const double b_xm = SB[q - 1] + 0.5 * X1[q - 1] * dx;
+        const double b_xp = SB[q] - 0.5 * X1[q] * dx;
+        const double b_ym = SB[q - TRW] + 0.5 * X2[q - TRW] * dy;
+        const double b_yp = SB[q] + 0.5 * X2[q] * dy;
+        S[T_HUB][q] = ((SU[q] > 0) ? b_xm : b_xp) * huu;
+        S[T_HVB][q] = ((SV[q] > 0) ? b_ym : b_yp) * hvv;
+      }
+    }
+    if (p.K4 > 0 && lx >= TH - 1 && lx <= TH + TTX && ly >= TH - 1 && ly <= TH + TTY)
+      S[T_BB4][q] = lap(SB, q) / SH[q];
+  }
+  __syncthreads();
+  // stage 3: the owned cell's tendency (work.c:2055-2140) and AB update
+  const int tx = tid % TTX, ty = tid / TTX;
+  const int i = X0 + tx, j = Y0 + ty;
+  if (i < p.Nx && j < p.Ny) {
+  const int q = at(tx + TH, ty + TH);
+  const double* HUU = S[T_HUU];
+  const double* HVV = S[T_HVV];
+  const double* HUB = S[T_HUB];
+  const double* HVB = S[T_HVB];
   const size_t cell = (size_t)j * p.pitch + i;
-  const double h = t.h[cell];
-  const double bc = t.b[cell];
+  const double h = SH[q];
+  const double bc = SB[q];
+  const double rh = 1.0 / h;   // reciprocal for div_rn by h
   double rhs_b = 0;
   double rhs_adv = 0;
   if (p.scheme == 0) {
-    rhs_adv = -0.5 * (t.U(i + 1, j) * t.db_dx(i + 1, j) + t.U(i, j) * t.db_dx(i, j)
-                      + t.V(i, j + 1) * t.db_dy(i, j + 1) + t.V(i, j) * t.db_dy(i, j));
+    rhs_adv = -0.5 * (X1[q + 1] + X1[q] + X2[q + TRW] + X2[q]);
   } else if (h != 0) {
-    rhs_adv = -((t.hub(i + 1, j) - t.hub(i, j)) / p.dx + (t.hvb(i, j + 1) - t.hvb(i, j)) / p.dy) / h
-            + bc * ((t.huu(i + 1, j) - t.huu(i, j)) / p.dx + (t.hvv(i, j + 1) - t.hvv(i, j)) / p.dy) / h;
+    rhs_adv = div_rn(-(div_rn(HUB[q + 1] - HUB[q], dx, p.rdx) + div_rn(HVB[q + TRW] - HVB[q], dy, p.rdy)), h, rh)
+            + div_rn(bc * (div_rn(HUU[q + 1] - HUU[q], dx, p.rdx) + div_rn(HVV[q + TRW] - HVV[q], dy, p.rdy)), h, rh);
   }
   rhs_b += rhs_adv;
   if (p.use_wdia && h != 0) {
@@ -156,15 +216,15 @@ __global__ void tracer_kernel(const TracerParams p) {
     const double db_p = (w0 > 0) ? 0 : b_p - bc;
     const double db_m = (w1 > 0) ? bc - b_m : 0;
     const double rhs_wdia = -(w0 * db_p + w1 * db_m);
-    rhs_b += rhs_wdia / h;
+    rhs_b += div_rn(rhs_wdia, h, rh);
   }
   if (p.K2 > 0 && h != 0) {
-    const double rhs_K2 = p.K2 * t.lap([&](int x, int y) { return t.B(x, y); }, i, j);
-    rhs_b += rhs_K2 / h;
+    const double rhs_K2 = p.K2 * lap(SB, q);
+    rhs_b += div_rn(rhs_K2, h, rh);
   }
   if (p.K4 > 0 && h != 0) {
-    const double rhs_K4 = -p.K4 * t.lap([&](int x, int y) { return t.BB4(x, y); }, i, j);
-    rhs_b += rhs_K4 / h;
+    const double rhs_K4 = -p.K4 * lap(S[T_BB4], q);
+    rhs_b += div_rn(rhs_K4, h, rh);
   }
   const double bt = p.bTime[lk + cell];
   if (bt > 0) {
@@ -174,21 +234,29 @@ __global__ void tracer_kernel(const TracerParams p) {
   const size_t o = lk + cell;
   if (p.ab_mode == 0) {
     p.fb_out[o] = rhs_b;
-    return;
+  } else {
+    double bn;
+    if (p.ab_mode == 1) bn = bc + p.c0 * rhs_b;
+    else if (p.ab_mode == 2) bn = bc + (p.c0 * rhs_b - p.c1 * p.f1b[o]);
+    else bn = bc + (p.c0 * rhs_b - p.c1 * p.f1b[o] + p.c2 * p.f2b[o]);
+    if (p.write_hist) p.fb_out[o] = rhs_b;
+    p.b_out[o] = bn;
   }
-  double bn;
-  if (p.ab_mode == 1) bn = bc + p.c0 * rhs_b;
-  else if (p.ab_mode == 2) bn = bc + (p.c0 * rhs_b - p.c1 * p.f1b[o]);
-  else bn = bc + (p.c0 * rhs_b - p.c1 * p.f1b[o] + p.c2 * p.f2b[o]);
-  if (p.write_hist) p.fb_out[o] = rhs_b;
-  p.b_out[o] = bn;
+  }   // owned cell
+  }   // layer
 }
 
 }  // namespace
 
 void launch_tracer(const TracerParams& p, cudaStream_t s) {
-  dim3 b(32, 8), g((p.Nx + 31) / 32, (p.Ny + 7) / 8, p.L);
-  tracer_kernel<<<g, b, 0, s>>>(p);
+  constexpr size_t shm = (size_t)T_NUM * TRN * sizeof(double);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(tracer_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    attr = true;
+  }
+  dim3 g((p.Nx + TTX - 1) / TTX, (p.Ny + TTY - 1) / TTY);
+  tracer_tile_kernel<<<g, TNT, shm, s>>>(p);
 }
 
 }  // namespace pawsim

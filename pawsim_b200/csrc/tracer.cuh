@@ -19,6 +19,7 @@ struct TracerParams {
   int thick_scheme;    // thicknessScheme of the face thickness (0 AL81, 1 HK83, 2 UP3, 3 KT00)
   double kt00_sigma;   // KT00_sigma (both KT00 limiters)
   double dx, dy, K2, K4;
+  double rdx, rdy, rdxsq, rdysq;    // 1/dx, 1/dy, 1/(dx dx), 1/(dy dy) rounded to nearest (div_rn)
   int use_wdia;
   const double *u, *v, *h, *b;      // state at the start of the step
   const double *bRelax, *bTime;
