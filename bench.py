@@ -155,6 +155,7 @@ def tracer_timing(cfg, stream, reps):
     without a passive tracer (CUDA events on the model's stream), the difference."""
     import tempfile as _tf
     import pawsim_b200
+    import torch
     out = []
     with _tf.TemporaryDirectory() as d:
         for tracer in (False, True):
