@@ -76,13 +76,25 @@ class Clocks:
         self.p = None
         self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
 
+    def _lines(self):
+        with open(self.out.name) as fh:
+            return fh.read().count("\n")
+
     def __enter__(self):
+        # the sampler is running (its first line written) before the timed region starts;
+        # rows from the last one before the region onwards are kept
+        self.first = 0
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=self.out, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+            return self
+        t0 = time.time()
+        while time.time() - t0 < 10 and self.p.poll() is None and self._lines() == 0:
+            time.sleep(0.01)
+        self.first = max(self._lines() - 1, 0)
         return self
 
     def __exit__(self, *a):
@@ -97,7 +109,7 @@ class Clocks:
         self.out.flush()
         rows = []
         with open(self.out.name) as fh:
-            for line in fh:
+            for line in fh.readlines()[self.first:]:
                 parts = [x.strip() for x in line.split(",")]
                 if len(parts) >= 6:
                     rows.append(parts)
@@ -235,7 +247,7 @@ def pressure_comparison(cfg, fields, stream, spin, steps, epochs, pairs):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mg-fp32", type=int, default=0)
@@ -321,6 +333,19 @@ def main():
         torch.cuda.synchronize()
         avg_ms = a0.elapsed_time(a1) / reps
 
+        # the energy and enstrophy sums of one EZdiags.dat line (savefreqEZ): the terms kernel
+        # with per-block partials, the final tree and the read of KE, PE, Z_k; per call
+        model.energy()
+        ez_ms = 0.0
+        for _ in range(reps):
+            z0, z1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            z0.record(stream)
+            model.energy()
+            z1.record(stream)
+            torch.cuda.synchronize()
+            ez_ms += z0.elapsed_time(z1)
+        ez_ms /= reps
+
     t_all = torch.tensor([ms], dtype=torch.float64)
     if dist is not None:
         dist.all_reduce(t_all, op=dist.ReduceOp.MAX)
@@ -405,6 +430,12 @@ def main():
                         "algorithmic_bytes": avg_bytes,
                         "achieved_gbs": avg_bytes / (avg_ms / 1e3) / 1e9,
                         "frac": avg_bytes / (avg_ms / 1e3) / 1e9 / peak}
+    # bytes per cell: read u, v, h per layer (the thickness for eta is h under the rigid
+    # lid), hhb and Coriolis
+    ez_bytes = ncell * (24 * L + 16)
+    line["energy"] = {"kernel": "ez_partial_kernel + ez_final_kernel", "ms_per_call": ez_ms,
+                      "algorithmic_bytes": ez_bytes, "achieved_gbs": ez_bytes / (ez_ms / 1e3) / 1e9,
+                      "frac": ez_bytes / (ez_ms / 1e3) / 1e9 / peak}
     if tr is not None:
         tr_bytes = ncell * L * 88   # read u, v, h, b, bRelax, bTime, f1, f2, w_dia; write b, f
         line["tracer"] = {"kernel": "tracer_tile_kernel (KT00, K2, relaxation)", "ms_per_step": tr,

@@ -76,8 +76,9 @@ typedef struct pawsim_gpu_config
    * the same pi and the one with the fewest V-cycles is kept. */
   int mg_fp32, mg_pre, mg_post;
   double mg_omega;
-  /* 1: sums in the reference's serial order (bitwise parity), 0: fixed pairwise tree,
-   * -1: serial order for grids of at most 65536 cells. */
+  /* Global sums (the pressure RHS mean, the solve norms and the energy diagnostics):
+   * 1 in the reference's serial order (bitwise parity), 0 in a fixed pairwise tree,
+   * -1 serial order for grids of at most 65536 cells. */
   int serial_sums;
   /* Shape of the multigrid's fused level kernels: 0 times every shape on each level
    * when the solver is first used and keeps the fastest; 1..4 forces one tile shape
@@ -144,6 +145,18 @@ PAWSIM_API int pawsim_gpu_run (pawsim_gpu * m, unsigned n0, unsigned nsteps, paw
 PAWSIM_API int pawsim_gpu_accumulate_averages (pawsim_gpu * m, double avg_fac);
 PAWSIM_API int pawsim_gpu_scale_averages (pawsim_gpu * m, double factor);
 PAWSIM_API int pawsim_gpu_zero_averages (pawsim_gpu * m);
+
+/* Energy and enstrophy diagnostics (replaces the sums of pawsim_diagnostics_write_EZ_if_due,
+ * model_code/diagnostics.c:478-700, whose line of EZdiags.dat the caller writes): the
+ * domain's kinetic energy *KE, potential energy *PE and the potential enstrophy Z[k] of each
+ * of the Nlay layers, for the current state. The interface heights are built upward from the
+ * bottom topography with the layer thickness the reference last copied into its work arrays:
+ * the current one (eta_from_step_start = 0; rigid lid, or online averages on, which reload the
+ * state every step) or the thickness at the start of the last step (1; free surface without
+ * averages), which needs a step since the last upload of h. The sums follow
+ * serial_sums: the reference's serial order (layer, x, y), or a fixed tree. Synchronous. */
+PAWSIM_API int pawsim_gpu_energy (pawsim_gpu * m, int eta_from_step_start, double * KE, double * PE,
+                                  double * Z);
 
 /* Solve L(pi) = rhs on the resident pi/pi_rhs with the GPU multigrid (no projection). */
 PAWSIM_API int pawsim_gpu_solve_mg (pawsim_gpu * m, pawsim_gpu_stats * st);

@@ -65,6 +65,9 @@ def _lib():
                                   ctypes.POINTER(OrcPstats)]
     lib.orc_time.argtypes = [ctypes.c_void_p]
     lib.orc_time.restype = ctypes.c_double
+    lib.orc_energy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                               ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    lib.orc_energy.restype = ctypes.c_int
     return lib
 
 
@@ -196,6 +199,13 @@ class Oracle:
     @property
     def t(self):
         return lib().orc_time(self._m)
+
+    def energy(self, reload=False):
+        """(KE, PE, Z[Nlay]) of the current state, diagnostics.c:478-700."""
+        ke, pe = ctypes.c_double(), ctypes.c_double()
+        z = (ctypes.c_double * self.L)()
+        lib().orc_energy(self._m, int(reload), ctypes.byref(ke), ctypes.byref(pe), z)
+        return ke.value, pe.value, list(z)
 
 
 def reference_exe():

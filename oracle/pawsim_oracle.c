@@ -2241,6 +2241,94 @@ double orc_time (const orc_model * m)
   return m->t;
 }
 
+/* diagnostics.c:478-700: kinetic and potential energy of the whole domain and the potential
+ * enstrophy of each layer, summed in the reference's serial order (layer, then x, then y).
+ * h, u, v are the state (halos current); eta is built from the thickness last copied into
+ * the work arrays, which `reload` refreshes first, as the online averages do every step. */
+int orc_energy (orc_model * m, int reload, double * ke, double * pe, double * z)
+{
+  int i,j,k;
+  const double dx = m->dx, dy = m->dy;
+  double KE = 0, PE = 0;
+  if (reload) load_state(m);
+  calc_eta(m);
+  for (k = 0; k < m->L; k ++)
+  {
+    const F2 * h = &m->h[k], * u = &m->u[k], * v = &m->v[k];
+    double Z = 0;
+    for (i = G; i < G+m->Nx; i ++)
+    {
+      const int gi = i - G;
+      for (j = G; j < G+m->Ny; j ++)
+      {
+        const int gj = j - G;
+        double hq, zeta, pv, ked = 0, gtot;
+        if (m->c.wall_ns && gj == 0)
+        {
+          hq = 0.5*(A(h,i-1,j) + A(h,i,j));
+          zeta = 0;
+        }
+        else if (m->c.wall_ew && gi == 0)
+        {
+          hq = 0.5*(A(h,i,j-1) + A(h,i,j));
+          zeta = 0;
+        }
+        else
+        {
+          hq = 0.25*(A(h,i,j) + A(h,i-1,j-1) + A(h,i-1,j) + A(h,i,j-1));
+          zeta = (A(u,i,j-1) - A(u,i,j)) / dy + (A(v,i,j) - A(v,i-1,j)) / dx;
+        }
+        if (hq != 0)
+        {
+          pv = (2*A(&m->omz,i,j) + zeta) / hq;
+          Z += dx*dy * 0.5 * hq * SQ(pv);
+        }
+        if (m->c.thick_scheme == 1)
+        {
+          /* HK83 (diagnostics.c:577-642) */
+          ked = 0;
+          if (m->c.wall_ns && gj == 0)
+            ked += (A(h,i,j)+A(h,i+1,j)) * (1.25*SQ(A(u,i+1,j)) + 0.25*SQ(A(u,i+1,j+1)))
+                 + (A(h,i-1,j)+A(h,i,j)) * (1.25*SQ(A(u,i,j)) + 0.25*SQ(A(u,i,j+1)));
+          else if (m->c.wall_ns && gj == m->Ny-1)
+            ked += (A(h,i,j)+A(h,i+1,j)) * (1.25*SQ(A(u,i+1,j)) + 0.25*SQ(A(u,i+1,j-1)))
+                 + (A(h,i-1,j)+A(h,i,j)) * (1.25*SQ(A(u,i,j)) + 0.25*SQ(A(u,i,j-1)));
+          else
+            ked += (A(h,i,j)+A(h,i+1,j)) * (SQ(A(u,i+1,j)) + 0.25*SQ(A(u,i+1,j+1)) + 0.25*SQ(A(u,i+1,j-1)))
+                 + (A(h,i-1,j)+A(h,i,j)) * (SQ(A(u,i,j)) + 0.25*SQ(A(u,i,j+1)) + 0.25*SQ(A(u,i,j-1)));
+          if (m->c.wall_ew && gi == 0)
+            ked += (A(h,i,j)+A(h,i,j+1)) * (1.25*SQ(A(v,i,j+1)) + 0.25*SQ(A(v,i+1,j+1)))
+                 + (A(h,i,j-1)+A(h,i,j)) * (1.25*SQ(A(v,i,j)) + 0.25*SQ(A(v,i+1,j)));
+          else if (m->c.wall_ew && gi == m->Nx-1)
+            ked += (A(h,i,j)+A(h,i,j+1)) * (1.25*SQ(A(v,i,j+1)) + 0.25*SQ(A(v,i-1,j+1)))
+                 + (A(h,i,j-1)+A(h,i,j)) * (1.25*SQ(A(v,i,j)) + 0.25*SQ(A(v,i-1,j)));
+          else
+            ked += (A(h,i,j)+A(h,i,j+1)) * (SQ(A(v,i,j+1)) + 0.25*SQ(A(v,i+1,j+1)) + 0.25*SQ(A(v,i-1,j+1)))
+                 + (A(h,i,j-1)+A(h,i,j)) * (SQ(A(v,i,j)) + 0.25*SQ(A(v,i+1,j)) + 0.25*SQ(A(v,i-1,j)));
+          ked *= dx*dy/12.0;
+        }
+        else
+        {
+          /* AL81, UP3, KT00 (diagnostics.c:562-575) */
+          ked = 0.125 * dx*dy
+              * ((A(h,i,j)+A(h,i+1,j)) * SQ(A(u,i+1,j))
+               + (A(h,i-1,j)+A(h,i,j)) * SQ(A(u,i,j))
+               + (A(h,i,j)+A(h,i,j+1)) * SQ(A(v,i,j+1))
+               + (A(h,i,j-1)+A(h,i,j)) * SQ(A(v,i,j)));
+        }
+        gtot = m->geff[k];
+        KE += ked;
+        PE += dx*dy * gtot * A(h,i,j) * (A(&m->eta[k],i,j) - 0.5*A(h,i,j));
+        PE += dx*dy * gtot * (m->c.h0*m->c.h0*m->c.h0*m->c.h0) / SQ(A(h,i,j)) / 6;
+      }
+    }
+    z[k] = Z;
+  }
+  *ke = KE;
+  *pe = PE;
+  return 0;
+}
+
 /* ------------------------------------------------------------ lifecycle */
 
 orc_model * orc_create (const orc_cfg * cfg)

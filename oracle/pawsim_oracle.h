@@ -96,6 +96,10 @@ int orc_run_steps (orc_model * m, int n0, int nsteps, orc_pstats * last);
 
 double orc_time (const orc_model * m);
 
+/* Kinetic and potential energy and per-layer potential enstrophy of the current state
+ * (diagnostics.c:478-700); reload = copy the state into the work arrays first. */
+int orc_energy (orc_model * m, int reload, double * ke, double * pe, double * z);
+
 #ifdef __cplusplus
 }
 #endif

@@ -73,6 +73,7 @@ EXPORTS = (
     "pawsim_nn_net_get_params", "pawsim_nn_net_set_params", "pawsim_nn_net_get_grads",
     "pawsim_nn_net_forward", "pawsim_nn_net_backward", "pawsim_nn_net_adam",
     "pawsim_gpu_accumulate_averages", "pawsim_gpu_scale_averages", "pawsim_gpu_zero_averages",
+    "pawsim_gpu_energy",
 )
 
 _LIB = None
@@ -104,6 +105,8 @@ def load_library(path: str = LIB_PATH):
     lib.pawsim_gpu_accumulate_averages.argtypes = [P, ctypes.c_double]
     lib.pawsim_gpu_scale_averages.argtypes = [P, ctypes.c_double]
     lib.pawsim_gpu_zero_averages.argtypes = [P]
+    D = ctypes.POINTER(ctypes.c_double)
+    lib.pawsim_gpu_energy.argtypes = [P, ctypes.c_int, D, D, D]
     lib.pawsim_gpu_set_stream.argtypes = [P, P]
     lib.pawsim_gpu_synchronize.argtypes = [P]
     lib.pawsim_gpu_time.argtypes = [P]
@@ -305,6 +308,17 @@ class Model:
 
     def zero_averages(self) -> None:
         _check(self.lib.pawsim_gpu_zero_averages(self._h))
+
+    def energy(self, eta_from_step_start: bool = False):
+        """(KE, PE, [Z_k]) of the current state: the sums of one EZdiags.dat line
+        (model_code/diagnostics.c:478-700). eta_from_step_start builds the interface heights
+        from the thickness at the start of the last step, as the reference does with a free
+        surface and no online averages."""
+        ke, pe = ctypes.c_double(), ctypes.c_double()
+        z = (ctypes.c_double * self.L)()
+        _check(self.lib.pawsim_gpu_energy(self._h, int(eta_from_step_start), ctypes.byref(ke),
+                                          ctypes.byref(pe), z))
+        return ke.value, pe.value, list(z)
 
     def synchronize(self) -> None:
         _check(self.lib.pawsim_gpu_synchronize(self._h))

@@ -96,6 +96,10 @@ struct Model {
   int nn_mode = 0;
   bool thickness_fixed = false;
   bool ready = false;
+  bool prev_h = false;       // h[1 - cur] holds the thickness at the start of the last step
+  double* ez = nullptr;      // energy-diagnostic scratch (terms or partials) and its size
+  size_t ez_elems = 0;
+  double* ez_out = nullptr;  // KE, PE, Z[L]
   cudaEvent_t ev0, ev1;
 
   template <typename T> T* alloc(size_t n) {
@@ -317,6 +321,7 @@ static int set_field(Model* m, const char* name, int k, const double* host, size
   if (n != (size_t)f.rows * f.cols) return fail(PAWSIM_GPU_EBADNAME, "wrong element count for field");
   PAWSIM_CUDA_OK(cudaMemcpy2DAsync(f.base + k * f.kstride, f.pitch * sizeof(double), host, f.cols * sizeof(double),
                                    f.cols * sizeof(double), f.rows, cudaMemcpyHostToDevice, m->s));
+  if (nm == "h") m->prev_h = false;
   // the state halo fill (state.c:1052-1057) puts +0 on wall faces of the normal velocity
   if (nm == "u" && m->c.wall_ew)
     PAWSIM_CUDA_OK(cudaMemset2DAsync(f.base + k * f.kstride, f.pitch * sizeof(double), 0, sizeof(double), f.rows, m->s));
@@ -515,6 +520,7 @@ static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
   PAWSIM_CUDA_OK(cudaGetLastError());
   if (shift) m->h1 = h2;
   m->cur = nb;
+  m->prev_h = true;
   m->t += dt;
   m->thickness_fixed = p.fuse_thickness_fix != 0;
   return 0;
@@ -755,6 +761,42 @@ int pawsim_gpu_zero_averages(pawsim_gpu* h) {
   Model* m = h->m;
   if (m->avg)
     PAWSIM_CUDA_OK(cudaMemsetAsync(m->avg, 0, avg_elems(m) * sizeof(double), m->s));
+  return 0;
+}
+
+int pawsim_gpu_energy(pawsim_gpu* h, int eta_from_step_start, double* KE, double* PE, double* Z) {
+  if (!h || !KE || !PE || !Z) return fail(PAWSIM_GPU_EBADCONFIG, "null argument");
+  Model* m = h->m;
+  if (!m->ready) return fail(PAWSIM_GPU_EBADCONFIG, "pawsim_gpu_init must follow the uploads");
+  if (eta_from_step_start && !m->prev_h)
+    return fail(PAWSIM_GPU_EBADCONFIG, "no step since the thickness was loaded");
+  const Grid2 g = m->grid2();
+  const bool serial = m->serial();
+  const size_t need = ez_scratch_elems(g, serial);
+  if (m->ez_elems < need) {
+    double* p = m->alloc<double>(need);
+    if (!p) return fail(PAWSIM_GPU_ECUDA, "energy scratch allocation failed");
+    m->ez = p;   // an earlier, smaller buffer stays in the model's list until it is destroyed
+    m->ez_elems = need;
+  }
+  if (!m->ez_out) {
+    m->ez_out = m->alloc<double>(AVG_LMAX + 2);
+    if (!m->ez_out) return fail(PAWSIM_GPU_ECUDA, "energy scratch allocation failed");
+  }
+  EzParams e;
+  e.h0 = m->c.h0;
+  for (int k = 0; k < m->L; ++k) e.geff[k] = m->geff[k];
+  e.u = m->u[m->cur]; e.v = m->v[m->cur]; e.h = m->h[m->cur];
+  e.hw = eta_from_step_start ? m->h[1 - m->cur] : m->h[m->cur];
+  e.hhb = m->hhb; e.omz = m->omz; e.qpitch = m->qpitch;
+  g_launches += launch_energy(g, e, serial, m->ez, m->ez_out, m->s);
+  PAWSIM_CUDA_OK(cudaGetLastError());
+  double out[AVG_LMAX + 2];
+  PAWSIM_CUDA_OK(cudaMemcpyAsync(out, m->ez_out, (m->L + 2) * sizeof(double), cudaMemcpyDeviceToHost, m->s));
+  PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
+  *KE = out[0];
+  *PE = out[1];
+  for (int k = 0; k < m->L; ++k) Z[k] = out[2 + k];
   return 0;
 }
 

@@ -488,6 +488,212 @@ __global__ void scale_kernel(double* f, size_t n, double factor) {
     f[q] *= factor;
 }
 
+// ------------------------------------------------ energy and enstrophy diagnostics
+
+constexpr int EZ_BX = 32, EZ_BY = 8;
+constexpr int EZ_MAX_ROW_BLOCKS = 64;   // row blocks of the tree grid; each thread strides over rows
+
+// The energy terms of one cell of layer k (diagnostics.c:514-646): the kinetic energy KE, the
+// two potential-energy increments PE1, PE2 and the enstrophy increment Z (-0.0, the identity
+// of addition, where h_q is zero and the reference adds nothing).
+struct EzCell {
+  double ke, pe1, pe2, z;
+};
+
+__device__ inline EzCell ez_cell(const Grid2& g, const EzParams& e, int k, int i, int j, double eta) {
+  const double* __restrict__ h = e.h + k * g.lstride;
+  const double* __restrict__ u = e.u + k * g.lstride;
+  const double* __restrict__ v = e.v + k * g.lstride;
+  const bool inner = i >= 1 && i + 1 < g.Nx && j >= 1 && j + 1 < g.Ny;
+  const size_t c = (size_t)j * g.pitch + i;
+  auto H = [&](int di, int dj) {
+    return inner ? h[c + (ptrdiff_t)dj * g.pitch + di] : ld_s(h, g, i + di, j + dj);
+  };
+  auto U = [&](int di, int dj) {
+    return inner ? u[c + (ptrdiff_t)dj * g.pitch + di] : ld_u(g, u, i + di, j + dj);
+  };
+  auto V = [&](int di, int dj) {
+    return inner ? v[c + (ptrdiff_t)dj * g.pitch + di] : ld_v(g, v, i + di, j + dj);
+  };
+  const double dx = g.dx, dy = g.dy;
+  const double hc = h[c];
+  EzCell r;
+  double hq, zeta;
+  if (g.wall_ns && j == 0) {
+    hq = 0.5 * (H(-1, 0) + hc);
+    zeta = 0;
+  } else if (g.wall_ew && i == 0) {
+    hq = 0.5 * (H(0, -1) + hc);
+    zeta = 0;
+  } else {
+    hq = 0.25 * (hc + H(-1, -1) + H(-1, 0) + H(0, -1));
+    zeta = (U(0, -1) - U(0, 0)) / dy + (V(0, 0) - V(-1, 0)) / dx;
+  }
+  r.z = -0.0;
+  if (hq != 0) {
+    const double pv = (2 * e.omz[(size_t)j * e.qpitch + i] + zeta) / hq;
+    r.z = dx * dy * 0.5 * hq * (pv * pv);
+  }
+  double ked;
+  if (g.thick_scheme == 1) {
+    // HK83 (diagnostics.c:577-642)
+    const double he = hc + H(1, 0), hwst = H(-1, 0) + hc, hn = hc + H(0, 1), hs = H(0, -1) + hc;
+    const double ue = U(1, 0), uw = U(0, 0), vn = V(0, 1), vs = V(0, 0);
+    ked = 0;
+    if (g.wall_ns && j == 0) {
+      ked += he * (1.25 * (ue * ue) + 0.25 * (U(1, 1) * U(1, 1))) + hwst * (1.25 * (uw * uw) + 0.25 * (U(0, 1) * U(0, 1)));
+    } else if (g.wall_ns && j == g.Ny - 1) {
+      ked += he * (1.25 * (ue * ue) + 0.25 * (U(1, -1) * U(1, -1))) + hwst * (1.25 * (uw * uw) + 0.25 * (U(0, -1) * U(0, -1)));
+    } else {
+      const double a = U(1, 1), b = U(1, -1), cc = U(0, 1), d = U(0, -1);
+      ked += he * (ue * ue + 0.25 * (a * a) + 0.25 * (b * b)) + hwst * (uw * uw + 0.25 * (cc * cc) + 0.25 * (d * d));
+    }
+    if (g.wall_ew && i == 0) {
+      ked += hn * (1.25 * (vn * vn) + 0.25 * (V(1, 1) * V(1, 1))) + hs * (1.25 * (vs * vs) + 0.25 * (V(1, 0) * V(1, 0)));
+    } else if (g.wall_ew && i == g.Nx - 1) {
+      ked += hn * (1.25 * (vn * vn) + 0.25 * (V(-1, 1) * V(-1, 1))) + hs * (1.25 * (vs * vs) + 0.25 * (V(-1, 0) * V(-1, 0)));
+    } else {
+      const double a = V(1, 1), b = V(-1, 1), cc = V(1, 0), d = V(-1, 0);
+      ked += hn * (vn * vn + 0.25 * (a * a) + 0.25 * (b * b)) + hs * (vs * vs + 0.25 * (cc * cc) + 0.25 * (d * d));
+    }
+    ked *= dx * dy / 12.0;
+  } else {
+    // AL81, UP3, KT00 (diagnostics.c:562-575)
+    const double ue = U(1, 0), uw = U(0, 0), vn = V(0, 1), vs = V(0, 0);
+    ked = 0.125 * dx * dy
+        * ((hc + H(1, 0)) * (ue * ue) + (H(-1, 0) + hc) * (uw * uw) + (hc + H(0, 1)) * (vn * vn)
+           + (H(0, -1) + hc) * (vs * vs));
+  }
+  r.ke = ked;
+  const double gtot = e.geff[k];
+  r.pe1 = dx * dy * gtot * hc * (eta - 0.5 * hc);
+  const double h0 = e.h0;
+  r.pe2 = dx * dy * gtot * (h0 * h0 * h0 * h0) / (hc * hc) / 6;
+  return r;
+}
+
+// per-cell terms in four planes of L*lstride: KE, PE1, PE2, Z
+__global__ void ez_terms_kernel(const Grid2 g, const EzParams e, double* __restrict__ terms) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.Nx || j >= g.Ny) return;
+  const size_t c = (size_t)j * g.pitch + i;
+  const size_t P = (size_t)g.L * g.lstride;
+  double eta = e.hhb[c];
+  for (int k = g.L - 1; k >= 0; --k) {
+    eta = eta + e.hw[k * g.lstride + c];
+    const EzCell r = ez_cell(g, e, k, i, j, eta);
+    const size_t o = k * g.lstride + c;
+    terms[o] = r.ke;
+    terms[P + o] = r.pe1;
+    terms[2 * P + o] = r.pe2;
+    terms[3 * P + o] = r.z;
+  }
+}
+
+// the reference's order: layer outer, then x, then y; KE, PE (two increments per cell) and
+// Z_k are independent chains. One thread; loads are batched ahead of the additions.
+__global__ void ez_serial_kernel(const Grid2 g, const double* __restrict__ terms, double* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const size_t P = (size_t)g.L * g.lstride;
+  double ke = 0, pe = 0;
+  for (int k = 0; k < g.L; ++k) {
+    double z = 0;
+    for (int i = 0; i < g.Nx; ++i) {
+      const double* t = terms + k * g.lstride + i;
+      int j = 0;
+      for (; j + 4 <= g.Ny; j += 4) {
+        double a[4][4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int p = 0; p < 4; ++p) a[p][q] = t[p * P + (size_t)(j + q) * g.pitch];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          ke += a[0][q];
+          pe += a[1][q];
+          pe += a[2][q];
+          z += a[3][q];
+        }
+      }
+      for (; j < g.Ny; ++j) {
+        const size_t o = (size_t)j * g.pitch;
+        ke += t[o];
+        pe += t[P + o];
+        pe += t[2 * P + o];
+        z += t[3 * P + o];
+      }
+    }
+    out[2 + k] = z;
+  }
+  out[0] = ke;
+  out[1] = pe;
+}
+
+// fixed tree: every thread sums its column over a fixed set of rows, then the block sums its
+// threads in a fixed shuffle order; partials[(L+2) * block + q]
+__global__ void __launch_bounds__(EZ_BX * EZ_BY) ez_partial_kernel(const Grid2 g, const EzParams e,
+                                                                   double* __restrict__ partials) {
+  const int i = blockIdx.x * EZ_BX + threadIdx.x;
+  const int L = g.L;
+  double ke = 0, pe = 0, z[AVG_LMAX];
+#pragma unroll
+  for (int k = 0; k < AVG_LMAX; ++k) z[k] = 0;
+  if (i < g.Nx) {
+    for (int j = blockIdx.y * EZ_BY + threadIdx.y; j < g.Ny; j += gridDim.y * EZ_BY) {
+      const size_t c = (size_t)j * g.pitch + i;
+      double eta = e.hhb[c];
+#pragma unroll
+      for (int k = AVG_LMAX - 1; k >= 0; --k) {
+        if (k < L) {
+          eta = eta + e.hw[k * g.lstride + c];
+          const EzCell r = ez_cell(g, e, k, i, j, eta);
+          ke += r.ke;
+          pe += r.pe1;
+          pe += r.pe2;
+          z[k] += r.z;
+        }
+      }
+    }
+  }
+  __shared__ double ws[AVG_LMAX + 2][EZ_BX * EZ_BY / 32];
+  const int lane = threadIdx.x & 31, warp = (threadIdx.y * EZ_BX + threadIdx.x) >> 5;
+  double vals[AVG_LMAX + 2];
+  vals[0] = ke;
+  vals[1] = pe;
+#pragma unroll
+  for (int k = 0; k < AVG_LMAX; ++k) vals[2 + k] = z[k];
+#pragma unroll
+  for (int q = 0; q < AVG_LMAX + 2; ++q) {
+    double x = vals[q];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) ws[q][warp] = x;
+  }
+  __syncthreads();
+  const int t = threadIdx.y * EZ_BX + threadIdx.x;
+  if (t < L + 2) {
+    double x = 0;
+    for (int w = 0; w < EZ_BX * EZ_BY / 32; ++w) x += ws[t][w];
+    partials[(size_t)(L + 2) * (blockIdx.y * gridDim.x + blockIdx.x) + t] = x;
+  }
+}
+
+// one block per quantity q: the partials of all blocks in a fixed order
+__global__ void ez_final_kernel(const double* __restrict__ partials, int nblocks, int nq, double* out) {
+  __shared__ double ws[RED_BLOCK / 32];
+  const int q = blockIdx.x;
+  double s = 0;
+  for (int b = threadIdx.x; b < nblocks; b += RED_BLOCK) s += partials[(size_t)nq * b + q];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < RED_BLOCK / 32; ++w) t += ws[w];
+    out[q] = t;
+  }
+}
+
 inline dim3 grid2(int Nx, int Ny, dim3 b) { return dim3((Nx + b.x - 1) / b.x, (Ny + b.y - 1) / b.y); }
 
 }  // namespace
@@ -499,6 +705,30 @@ void launch_accumulate_averages(const Grid2& g, const AvgParams& a, cudaStream_t
 
 void launch_scale(double* f, size_t n, double factor, cudaStream_t s) {
   scale_kernel<<<1184, 256, 0, s>>>(f, n, factor);
+}
+
+static dim3 ez_tree_grid(const Grid2& g) {
+  const int rows = (g.Ny + EZ_BY - 1) / EZ_BY;
+  return dim3((g.Nx + EZ_BX - 1) / EZ_BX, rows < EZ_MAX_ROW_BLOCKS ? rows : EZ_MAX_ROW_BLOCKS);
+}
+
+size_t ez_scratch_elems(const Grid2& g, bool serial) {
+  if (serial) return 4 * (size_t)g.L * g.lstride;
+  const dim3 gr = ez_tree_grid(g);
+  return (size_t)(g.L + 2) * gr.x * gr.y;
+}
+
+int launch_energy(const Grid2& g, const EzParams& e, bool serial, double* terms, double* out, cudaStream_t s) {
+  if (serial) {
+    dim3 b(32, 8);
+    ez_terms_kernel<<<grid2(g.Nx, g.Ny, b), b, 0, s>>>(g, e, terms);
+    ez_serial_kernel<<<1, 32, 0, s>>>(g, terms, out);
+    return 2;
+  }
+  const dim3 gr = ez_tree_grid(g);
+  ez_partial_kernel<<<gr, dim3(EZ_BX, EZ_BY), 0, s>>>(g, e, terms);
+  ez_final_kernel<<<g.L + 2, RED_BLOCK, 0, s>>>(terms, gr.x * gr.y, g.L + 2, out);
+  return 2;
 }
 
 // interior cells with plain loads when the face thickness is the AL81 average, then the

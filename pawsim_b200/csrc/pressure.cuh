@@ -73,6 +73,22 @@ void launch_accumulate_averages(const Grid2& g, const AvgParams& a, cudaStream_t
 // f[i] *= factor for n contiguous doubles
 void launch_scale(double* f, size_t n, double factor, cudaStream_t s);
 
+// Kinetic and potential energy of the domain and the potential enstrophy of each layer
+// (diagnostics.c:478-700). h, u, v are the current state; eta is built upward from hhb with
+// the thickness `hw` (the state the reference last copied into its work arrays). Results go
+// to out[0] = KE, out[1] = PE, out[2 + k] = Z_k (device). serial_order sums every cell in the
+// reference's order (layer, then x, then y) from per-cell terms in `terms`
+// (ez_scratch_elems doubles); otherwise a fixed tree sums per-block partials held in `terms`.
+struct EzParams {
+  double h0;
+  double geff[AVG_LMAX];
+  const double *u, *v, *h, *hw, *hhb, *omz;
+  int qpitch;
+};
+size_t ez_scratch_elems(const Grid2& g, bool serial_order);
+int launch_energy(const Grid2& g, const EzParams& e, bool serial_order, double* terms, double* out,
+                  cudaStream_t s);
+
 // max |f| and sum f^2 (serial order or tree) into out[0], out[1]
 void launch_norms(const double* f, int Nx, int Ny, int pitch, bool serial_order,
                   double* partials, double* out, cudaStream_t s);

@@ -14,6 +14,8 @@
  *   - runs the preliminary pressure correction, writes the n = 0 state, steps Nt times and
  *     writes U{k}, V{k}, H{k}, W{k} and P on the model-time save schedule
  *     (pawsim.c:318-350; diagnostics.c:84-93, 874-908);
+ *   - accumulates the online averages of savefreqAvg and writes each window, and appends
+ *     the energy and enstrophy line of savefreqEZ to EZdiags.dat (diagnostics.c:307-700);
  *   - prints "PAWSIM pressure solve" lines and the closing summary when pressureTiming is
  *     set (pawsim.c:100-108, 515-522).
  * Exit status 0 on success, 1 on any failure, with the message on stderr.
@@ -42,7 +44,7 @@ typedef struct
   int useTrad, use_MG, use_fullMG, pressureTiming, writeInitDiagnostics, restart, useWallEW,
       useWallNS, useRL, oceanSurfDrag, windFeedback, useTracer, useBuoyancy, useRandomForcing;
   /* reals (strtod) */
-  double Lx, Ly, dt, tmin, tmax, savefrequency, savefreqAvg, KT00_sigma, h0, hsml, hmin_surf, hbbl, hmin_bot,
+  double Lx, Ly, dt, tmin, tmax, savefrequency, savefreqAvg, savefreqEZ, KT00_sigma, h0, hsml, hmin_surf, hbbl, hmin_bot,
       A2, A4, A2smag, A4smag, K2, K4, linDragCoeff, quadDragCoeff, linDragSurf, quadDragSurf,
       tauPeriod, wDiaPeriod, convDiff, omega_MG, tol, SOR_rp;
   /* derived */
@@ -104,7 +106,7 @@ static const keydef KEYS[] = {
     B(useTrad), B(use_MG), B(use_fullMG), B(pressureTiming), B(writeInitDiagnostics), B(restart),
     B(useWallEW), B(useWallNS), B(useRL), B(oceanSurfDrag), B(windFeedback), B(useTracer),
     B(useBuoyancy), B(useRandomForcing), R(Lx), R(Ly), R(dt), R(tmin), R(tmax), R(savefrequency), R(savefreqAvg),
-    R(KT00_sigma), R(h0), R(hsml), R(hmin_surf), R(hbbl), R(hmin_bot), R(A2), R(A4), R(A2smag),
+    R(savefreqEZ), R(KT00_sigma), R(h0), R(hsml), R(hmin_surf), R(hbbl), R(hmin_bot), R(A2), R(A4), R(A2smag),
     R(A4smag), R(K2), R(K4), R(linDragCoeff), R(quadDragCoeff), R(linDragSurf), R(quadDragSurf),
     R(tauPeriod), R(wDiaPeriod), R(convDiff), R(omega_MG), R(tol), {NULL, K_REAL, 0}};
 #undef U
@@ -553,6 +555,40 @@ static int write_averages (pawsim_gpu * m, const config * c, const char * outdir
   return 1;
 }
 
+/* every EZdiags.dat line now due (diagnostics.c:478-700): the time of the line, KE, PE,
+ * KE+PE and the enstrophy of each layer, all from the current state */
+static int write_ez (pawsim_gpu * m, const config * c, const char * outdir, double t, unsigned * n_EZ,
+                     double * t_next_EZ)
+{
+  char path[8192];
+  double KE, PE, Z[8];
+  size_t len = strlen(outdir);
+  unsigned k;
+  /* the reference builds eta from the thickness last copied into its work arrays: the
+   * pressure RHS (rigid lid) and the online averages copy the current state; otherwise the
+   * last tendency evaluation copied the state of the start of the step */
+  int eta_prev = !c->useRL && !(c->savefreqAvg > 0);
+  if (!gpu_ok(pawsim_gpu_energy(m,eta_prev,&KE,&PE,Z),"energy diagnostics")) return 0;
+  snprintf(path,sizeof(path),"%s%sEZdiags.dat",outdir,(len > 0 && outdir[len - 1] != '/') ? "/" : "");
+  while (t >= *t_next_EZ)
+  {
+    FILE * fh = fopen(path,(c->restart || *n_EZ > 1) ? "a" : "w");
+    if (!fh)
+    {
+      fprintf(stderr,"Could not open %s for writing\n",path);
+      return 0;
+    }
+    fprintf(fh,"%le",*t_next_EZ);
+    fprintf(fh," %.50e %.50e %.50e ",KE,PE,KE + PE);
+    for (k = 0; k < c->Nlay; k ++) fprintf(fh,"%.50e ",Z[k]);
+    fprintf(fh,"\n");
+    fclose(fh);
+    (*n_EZ) ++;
+    *t_next_EZ = *n_EZ * c->savefreqEZ;
+  }
+  return 1;
+}
+
 static const char * solver_name (unsigned s)
 {
   return s == 0 ? "SOR" : (s == 1 ? "MG_GATHERED" : (s == 2 ? "MG_DISTRIBUTED" : "UNKNOWN"));
@@ -566,8 +602,8 @@ int main (int argc, char ** argv)
   pawsim_gpu_stats st;
   const char * outdir;
   double * plane = NULL;
-  unsigned n, n_saves, solves = 0, fallbacks = 0, n_avg = 0;
-  double t_next_avg = 0;
+  unsigned n, n_saves, solves = 0, fallbacks = 0, n_avg = 0, n_EZ = 0;
+  double t_next_avg = 0, t_next_EZ = 0;
   double wall_total = 0, iters_total = 0;
   const char * slash;
   int rc = 1;
@@ -647,6 +683,11 @@ int main (int argc, char ** argv)
     n_avg = (unsigned) round(c.tmin / c.savefreqAvg) + 1;
     t_next_avg = c.tmin + c.savefreqAvg;
   }
+  if (c.savefreqEZ > 0)
+  {
+    n_EZ = (unsigned) round(c.tmin / c.savefreqEZ) + 1;
+    t_next_EZ = c.tmin + c.savefreqEZ;
+  }
   /* preliminary rigid-lid correction, then the n = 0 (or pickup) state (pawsim.c:278-312) */
   memset(&st,0,sizeof(st));
   if (!gpu_ok(pawsim_gpu_prelim(m,&st),"preliminary pressure correction")) goto done;
@@ -725,6 +766,11 @@ int main (int argc, char ** argv)
         n_avg ++;
         t_next_avg = n_avg * c.savefreqAvg;
       }
+    }
+    if (c.savefreqEZ > 0 && t >= t_next_EZ && !write_ez(m,&c,outdir,t,&n_EZ,&t_next_EZ))
+    {
+      fprintf(stderr,"ERROR: PAWSIM diagnostic averaging failed at n=%u\n",n);
+      goto done;
     }
   }
   if (c.pressureTiming && solves > 0)

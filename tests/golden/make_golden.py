@@ -9,7 +9,8 @@ generator), and what the reference printed and wrote: the init_* tendency dumps 
 ``writeInitDiagnostics 1`` (model_code/diagnostics.c:914-972), U/V/H/P after each step
 (diagnostics.c:874-908) and the ``PAWSIM pressure solve`` lines of ``pressureTiming 1``
 (model_code/pawsim.c:100-108). The ``*_avg`` cases hold the online-average files of
-``savefreqAvg`` (diagnostics.c:378-470) instead.
+``savefreqAvg`` (diagnostics.c:378-470) instead; the ``*_ez`` cases the text of
+``EZdiags.dat`` (``savefreqEZ``, diagnostics.c:478-700).
 """
 import os
 import re
@@ -63,6 +64,17 @@ TRC_CASES = {
     "full_tracer_kt00": (inputs.full_physics, dict(N=16, dt=50.0, solver=0, Ly=320e3, bathy_len=20e3,
                                                    sponge=40e3, extra=dict(savefreqAvg=125.0)),
                          dict(scheme=2, relax_days=30.0, K4=1e8)),
+}
+# energy/enstrophy cases (savefreqEZ, diagnostics.c:478-700): a rigid-lid gyre with two lines
+# per step, a free-surface periodic jet (eta from the thickness of the start of the step) and a
+# free-surface HK83 gyre whose online averages reload the state every step
+EZ_NSTEPS = 6
+EZ_CASES = {
+    "gyre_sor_ez": (inputs.gyre, dict(N=16, Ny=12, dt=900.0, solver=0, tol=1e-10), 0.5),
+    "jets_free_ez": (inputs.jets, dict(N=16, dt=30.0, solver=0, extra=dict(useRL=0)), 1.5),
+    "gyre_hk83_free_avg_ez": (inputs.gyre, dict(N=20, Ny=12, dt=300.0, solver=0,
+                                                extra=dict(useRL=0, thicknessScheme=1,
+                                                           savefreqAvg=750.0)), 1.0),
 }
 LINE = re.compile(r"iters=(\d+) walltime=\S+ s residual_max=(\S+) residual_rms=(\S+) "
                   r"div_max=(\S+) div_rms=(\S+)")
@@ -156,6 +168,25 @@ def make_tracer(name, fn, kw, tkw, outdir):
         np.savez_compressed(os.path.join(outdir, name + ".npz"), **rec)
 
 
+def make_ez(name, fn, kw, every, outdir):
+    """Inputs and the reference's EZdiags.dat text (savefreqEZ = every * dt)."""
+    with tempfile.TemporaryDirectory() as d:
+        kw = dict(kw)
+        extra = dict(kw.pop("extra", {}) or {})
+        dt = kw["dt"]
+        extra.update(savefreqEZ=every * dt)
+        p = fn(os.path.join(d, "in"), Nt=EZ_NSTEPS, savefrequency=EZ_NSTEPS * dt, extra=extra, **kw)
+        out = os.path.join(d, "out")
+        os.makedirs(out)
+        subprocess.run([oracle.reference_exe(), p, out], capture_output=True, text=True, check=True)
+        rec = {"param_text": np.array(open(p).read())}
+        for f in sorted(os.listdir(os.path.dirname(p))):
+            if f.endswith(".dat") and f != "params.dat":
+                rec["in_" + f] = np.fromfile(os.path.join(os.path.dirname(p), f), dtype="<f8")
+        rec["ez_text"] = np.array(open(os.path.join(out, "EZdiags.dat")).read())
+        np.savez_compressed(os.path.join(outdir, name + ".npz"), **rec)
+
+
 if __name__ == "__main__":
     # python tests/golden/make_golden.py [case ...]   (all cases when none are named)
     oracle.build(ref=True)
@@ -173,4 +204,9 @@ if __name__ == "__main__":
         if len(sys.argv) > 1 and name not in sys.argv[1:]:
             continue
         make_tracer(name, fn, kw, tkw, HERE)
+        print("wrote", name)
+    for name, (fn, kw, every) in EZ_CASES.items():
+        if len(sys.argv) > 1 and name not in sys.argv[1:]:
+            continue
+        make_ez(name, fn, kw, every, HERE)
         print("wrote", name)
