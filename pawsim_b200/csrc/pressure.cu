@@ -491,7 +491,6 @@ __global__ void scale_kernel(double* f, size_t n, double factor) {
 // ------------------------------------------------ energy and enstrophy diagnostics
 
 constexpr int EZ_BX = 32, EZ_BY = 8;
-constexpr int EZ_MAX_ROW_BLOCKS = 64;   // row blocks of the tree grid; each thread strides over rows
 
 // The energy terms of one cell of layer k (diagnostics.c:514-646): the kinetic energy KE, the
 // two potential-energy increments PE1, PE2 and the enstrophy increment Z (-0.0, the identity
@@ -500,11 +499,15 @@ struct EzCell {
   double ke, pe1, pe2, z;
 };
 
-__device__ inline EzCell ez_cell(const Grid2& g, const EzParams& e, int k, int i, int j, double eta) {
+// HK: the HK83 kinetic energy; PLAIN: the whole block is at least one cell inside the grid,
+// so every neighbour is an owned cell and loads need no boundary map
+template <bool HK, bool PLAIN>
+__device__ inline EzCell ez_cell(const Grid2& g, const EzParams& e, int k, int i, int j, double eta,
+                                 double gtot) {
   const double* __restrict__ h = e.h + k * g.lstride;
   const double* __restrict__ u = e.u + k * g.lstride;
   const double* __restrict__ v = e.v + k * g.lstride;
-  const bool inner = i >= 1 && i + 1 < g.Nx && j >= 1 && j + 1 < g.Ny;
+  const bool inner = PLAIN || (i >= 1 && i + 1 < g.Nx && j >= 1 && j + 1 < g.Ny);
   const size_t c = (size_t)j * g.pitch + i;
   auto H = [&](int di, int dj) {
     return inner ? h[c + (ptrdiff_t)dj * g.pitch + di] : ld_s(h, g, i + di, j + dj);
@@ -519,15 +522,15 @@ __device__ inline EzCell ez_cell(const Grid2& g, const EzParams& e, int k, int i
   const double hc = h[c];
   EzCell r;
   double hq, zeta;
-  if (g.wall_ns && j == 0) {
+  if (!PLAIN && g.wall_ns && j == 0) {
     hq = 0.5 * (H(-1, 0) + hc);
     zeta = 0;
-  } else if (g.wall_ew && i == 0) {
+  } else if (!PLAIN && g.wall_ew && i == 0) {
     hq = 0.5 * (H(0, -1) + hc);
     zeta = 0;
   } else {
     hq = 0.25 * (hc + H(-1, -1) + H(-1, 0) + H(0, -1));
-    zeta = (U(0, -1) - U(0, 0)) / dy + (V(0, 0) - V(-1, 0)) / dx;
+    zeta = div_rn(U(0, -1) - U(0, 0), dy, g.rdy) + div_rn(V(0, 0) - V(-1, 0), dx, g.rdx);
   }
   r.z = -0.0;
   if (hq != 0) {
@@ -535,22 +538,22 @@ __device__ inline EzCell ez_cell(const Grid2& g, const EzParams& e, int k, int i
     r.z = dx * dy * 0.5 * hq * (pv * pv);
   }
   double ked;
-  if (g.thick_scheme == 1) {
+  if (HK) {
     // HK83 (diagnostics.c:577-642)
     const double he = hc + H(1, 0), hwst = H(-1, 0) + hc, hn = hc + H(0, 1), hs = H(0, -1) + hc;
     const double ue = U(1, 0), uw = U(0, 0), vn = V(0, 1), vs = V(0, 0);
     ked = 0;
-    if (g.wall_ns && j == 0) {
+    if (!PLAIN && g.wall_ns && j == 0) {
       ked += he * (1.25 * (ue * ue) + 0.25 * (U(1, 1) * U(1, 1))) + hwst * (1.25 * (uw * uw) + 0.25 * (U(0, 1) * U(0, 1)));
-    } else if (g.wall_ns && j == g.Ny - 1) {
+    } else if (!PLAIN && g.wall_ns && j == g.Ny - 1) {
       ked += he * (1.25 * (ue * ue) + 0.25 * (U(1, -1) * U(1, -1))) + hwst * (1.25 * (uw * uw) + 0.25 * (U(0, -1) * U(0, -1)));
     } else {
       const double a = U(1, 1), b = U(1, -1), cc = U(0, 1), d = U(0, -1);
       ked += he * (ue * ue + 0.25 * (a * a) + 0.25 * (b * b)) + hwst * (uw * uw + 0.25 * (cc * cc) + 0.25 * (d * d));
     }
-    if (g.wall_ew && i == 0) {
+    if (!PLAIN && g.wall_ew && i == 0) {
       ked += hn * (1.25 * (vn * vn) + 0.25 * (V(1, 1) * V(1, 1))) + hs * (1.25 * (vs * vs) + 0.25 * (V(1, 0) * V(1, 0)));
-    } else if (g.wall_ew && i == g.Nx - 1) {
+    } else if (!PLAIN && g.wall_ew && i == g.Nx - 1) {
       ked += hn * (1.25 * (vn * vn) + 0.25 * (V(-1, 1) * V(-1, 1))) + hs * (1.25 * (vs * vs) + 0.25 * (V(-1, 0) * V(-1, 0)));
     } else {
       const double a = V(1, 1), b = V(-1, 1), cc = V(1, 0), d = V(-1, 0);
@@ -565,11 +568,26 @@ __device__ inline EzCell ez_cell(const Grid2& g, const EzParams& e, int k, int i
            + (H(0, -1) + hc) * (vs * vs));
   }
   r.ke = ked;
-  const double gtot = e.geff[k];
   r.pe1 = dx * dy * gtot * hc * (eta - 0.5 * hc);
   const double h0 = e.h0;
-  r.pe2 = dx * dy * gtot * (h0 * h0 * h0 * h0) / (hc * hc) / 6;
+  constexpr double kSixth = 1.0 / 6.0;   // rounded to nearest at compile time
+  r.pe2 = div_rn(dx * dy * gtot * (h0 * h0 * h0 * h0) / (hc * hc), 6.0, kSixth);
   return r;
+}
+
+// geff[k] for a runtime k without a local copy of the parameter array
+__device__ inline double ez_geff(const EzParams& e, int k) {
+  double x = 0;
+#pragma unroll
+  for (int q = 0; q < AVG_LMAX; ++q)
+    if (q == k) x = e.geff[q];
+  return x;
+}
+
+__device__ inline EzCell ez_cell_any(const Grid2& g, const EzParams& e, int k, int i, int j, double eta) {
+  const double gt = ez_geff(e, k);
+  return g.thick_scheme == 1 ? ez_cell<true, false>(g, e, k, i, j, eta, gt)
+                             : ez_cell<false, false>(g, e, k, i, j, eta, gt);
 }
 
 // per-cell terms in four planes of L*lstride: KE, PE1, PE2, Z
@@ -582,7 +600,7 @@ __global__ void ez_terms_kernel(const Grid2 g, const EzParams e, double* __restr
   double eta = e.hhb[c];
   for (int k = g.L - 1; k >= 0; --k) {
     eta = eta + e.hw[k * g.lstride + c];
-    const EzCell r = ez_cell(g, e, k, i, j, eta);
+    const EzCell r = ez_cell_any(g, e, k, i, j, eta);
     const size_t o = k * g.lstride + c;
     terms[o] = r.ke;
     terms[P + o] = r.pe1;
@@ -630,60 +648,65 @@ __global__ void ez_serial_kernel(const Grid2 g, const double* __restrict__ terms
   out[1] = pe;
 }
 
-// fixed tree: every thread sums its column over a fixed set of rows, then the block sums its
-// threads in a fixed shuffle order; partials[(L+2) * block + q]
-__global__ void __launch_bounds__(EZ_BX * EZ_BY) ez_partial_kernel(const Grid2 g, const EzParams e,
-                                                                   double* __restrict__ partials) {
-  const int i = blockIdx.x * EZ_BX + threadIdx.x;
-  const int L = g.L;
-  double ke = 0, pe = 0, z[AVG_LMAX];
-#pragma unroll
-  for (int k = 0; k < AVG_LMAX; ++k) z[k] = 0;
-  if (i < g.Nx) {
-    for (int j = blockIdx.y * EZ_BY + threadIdx.y; j < g.Ny; j += gridDim.y * EZ_BY) {
-      const size_t c = (size_t)j * g.pitch + i;
-      double eta = e.hhb[c];
-#pragma unroll
-      for (int k = AVG_LMAX - 1; k >= 0; --k) {
-        if (k < L) {
-          eta = eta + e.hw[k * g.lstride + c];
-          const EzCell r = ez_cell(g, e, k, i, j, eta);
-          ke += r.ke;
-          pe += r.pe1;
-          pe += r.pe2;
-          z[k] += r.z;
-        }
-      }
-    }
-  }
-  __shared__ double ws[AVG_LMAX + 2][EZ_BX * EZ_BY / 32];
-  const int lane = threadIdx.x & 31, warp = (threadIdx.y * EZ_BX + threadIdx.x) >> 5;
-  double vals[AVG_LMAX + 2];
-  vals[0] = ke;
-  vals[1] = pe;
-#pragma unroll
-  for (int k = 0; k < AVG_LMAX; ++k) vals[2 + k] = z[k];
-#pragma unroll
-  for (int q = 0; q < AVG_LMAX + 2; ++q) {
-    double x = vals[q];
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-    if (lane == 0) ws[q][warp] = x;
-  }
-  __syncthreads();
+// sum of one value over the block (32x8 threads) in a fixed order, valid in thread 0
+__device__ inline double ez_block_sum(double x, double* ws) {
   const int t = threadIdx.y * EZ_BX + threadIdx.x;
-  if (t < L + 2) {
-    double x = 0;
-    for (int w = 0; w < EZ_BX * EZ_BY / 32; ++w) x += ws[t][w];
-    partials[(size_t)(L + 2) * (blockIdx.y * gridDim.x + blockIdx.x) + t] = x;
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+  if ((t & 31) == 0) ws[t >> 5] = x;
+  __syncthreads();
+  double s = 0;
+  if (t == 0)
+    for (int w = 0; w < EZ_BX * EZ_BY / 32; ++w) s += ws[w];
+  __syncthreads();
+  return s;
+}
+
+// fixed tree: one thread per column of one 32x8 tile walks the layers bottom-up; the block
+// sums each layer's enstrophy, then KE and PE, into partials[q * blocks + block]
+template <bool HK>
+__global__ void __launch_bounds__(EZ_BX * EZ_BY, HK ? 2 : 4) ez_partial_kernel(const Grid2 g, const EzParams e,
+                                                                   double* __restrict__ partials) {
+  __shared__ double ws[EZ_BX * EZ_BY / 32];
+  const int i = blockIdx.x * EZ_BX + threadIdx.x;
+  const int j = blockIdx.y * EZ_BY + threadIdx.y;
+  const bool in = i < g.Nx && j < g.Ny;
+  const bool plain = blockIdx.x * EZ_BX >= 1 && (blockIdx.x + 1) * EZ_BX + 1 <= g.Nx &&
+                     blockIdx.y * EZ_BY >= 1 && (blockIdx.y + 1) * EZ_BY + 1 <= g.Ny;
+  const int L = g.L;
+  const size_t c = in ? (size_t)j * g.pitch + i : 0;
+  const size_t nb = (size_t)gridDim.x * gridDim.y;
+  double* out = partials + (blockIdx.y * gridDim.x + blockIdx.x);
+  double ke = 0, pe = 0;
+  double eta = in ? e.hhb[c] : 0;
+#pragma unroll 1
+  for (int k = L - 1; k >= 0; --k) {
+    double z = 0;
+    if (in) {
+      eta = eta + e.hw[k * g.lstride + c];
+      const double gt = ez_geff(e, k);
+      const EzCell r = plain ? ez_cell<HK, true>(g, e, k, i, j, eta, gt) : ez_cell<HK, false>(g, e, k, i, j, eta, gt);
+      ke += r.ke;
+      pe += r.pe1;
+      pe += r.pe2;
+      z = r.z;
+    }
+    z = ez_block_sum(z, ws);
+    if (threadIdx.x == 0 && threadIdx.y == 0) out[(2 + k) * nb] = z;
+  }
+  ke = ez_block_sum(ke, ws);
+  pe = ez_block_sum(pe, ws);
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    out[0] = ke;
+    out[nb] = pe;
   }
 }
 
 // one block per quantity q: the partials of all blocks in a fixed order
-__global__ void ez_final_kernel(const double* __restrict__ partials, int nblocks, int nq, double* out) {
+__global__ void ez_final_kernel(const double* __restrict__ partials, int nblocks, double* out) {
   __shared__ double ws[RED_BLOCK / 32];
   const int q = blockIdx.x;
   double s = 0;
-  for (int b = threadIdx.x; b < nblocks; b += RED_BLOCK) s += partials[(size_t)nq * b + q];
+  for (int b = threadIdx.x; b < nblocks; b += RED_BLOCK) s += partials[(size_t)q * nblocks + b];
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
   __syncthreads();
@@ -708,8 +731,7 @@ void launch_scale(double* f, size_t n, double factor, cudaStream_t s) {
 }
 
 static dim3 ez_tree_grid(const Grid2& g) {
-  const int rows = (g.Ny + EZ_BY - 1) / EZ_BY;
-  return dim3((g.Nx + EZ_BX - 1) / EZ_BX, rows < EZ_MAX_ROW_BLOCKS ? rows : EZ_MAX_ROW_BLOCKS);
+  return dim3((g.Nx + EZ_BX - 1) / EZ_BX, (g.Ny + EZ_BY - 1) / EZ_BY);
 }
 
 size_t ez_scratch_elems(const Grid2& g, bool serial) {
@@ -726,8 +748,11 @@ int launch_energy(const Grid2& g, const EzParams& e, bool serial, double* terms,
     return 2;
   }
   const dim3 gr = ez_tree_grid(g);
-  ez_partial_kernel<<<gr, dim3(EZ_BX, EZ_BY), 0, s>>>(g, e, terms);
-  ez_final_kernel<<<g.L + 2, RED_BLOCK, 0, s>>>(terms, gr.x * gr.y, g.L + 2, out);
+  if (g.thick_scheme == 1)
+    ez_partial_kernel<true><<<gr, dim3(EZ_BX, EZ_BY), 0, s>>>(g, e, terms);
+  else
+    ez_partial_kernel<false><<<gr, dim3(EZ_BX, EZ_BY), 0, s>>>(g, e, terms);
+  ez_final_kernel<<<g.L + 2, RED_BLOCK, 0, s>>>(terms, gr.x * gr.y, out);
   return 2;
 }
 

@@ -3,7 +3,8 @@
     python -m pawsim_b200.run --setup gyre --N 1024 --steps 4 [--integrator-only]
                               [--solver 0|1] [--mg-fp32] [--mg-tile K] [--mg-omega W]
                               [--mg-pre P] [--mg-post Q] [--dt 60] [--param FILE]
-                              [--ws-collect S --ws-epochs E]
+                              [--ws-collect S --ws-epochs E] [--tracer SCHEME]
+                              [--averages] [--energy]
 
 ``--integrator-only`` advances with ``pawsim_gpu_integrator_step`` alone (one fused tendency
 kernel per step, no pressure correction), which isolates the tendency kernel for a profiler.
@@ -11,6 +12,9 @@ kernel per step, no pressure correction), which isolates the tendency kernel for
 ``--ws-collect S`` first runs S steps that collect warm-start training pairs, trains the
 network for ``--ws-epochs`` epochs on the GPU, then runs ``--steps`` steps whose solves start
 from the network's guess (this exercises the tcgen05 convolution kernels).
+``--tracer SCHEME`` adds a passive tracer (0 AL81, 1 UP3, 2 KT00; K2 = 100, relaxation over
+100 days). ``--averages`` accumulates the online averages after every step; ``--energy``
+computes the energy and enstrophy sums after every step.
 """
 from __future__ import annotations
 
@@ -41,6 +45,9 @@ def main(argv=None):
     ap.add_argument("--integrator-only", action="store_true")
     ap.add_argument("--ws-collect", type=int, default=0)
     ap.add_argument("--ws-epochs", type=int, default=2)
+    ap.add_argument("--tracer", type=int, default=-1, help="tracer scheme 0..2; negative: no tracer")
+    ap.add_argument("--averages", action="store_true")
+    ap.add_argument("--energy", action="store_true")
     a = ap.parse_args(argv)
     with tempfile.TemporaryDirectory() as d:
         if a.param:
@@ -55,13 +62,23 @@ def main(argv=None):
                 kw["dt"] = a.dt
             elif a.setup == "gyre":
                 kw["dt"] = 60.0 * 2048 / a.N if a.N <= 2048 else 60.0
-            cfg = inputs.read_config(SETUPS[a.setup](d, **kw))
+            p = SETUPS[a.setup](d, **kw)
+            if a.tracer >= 0:
+                inputs.add_tracer(p, scheme=a.tracer, relax_days=100.0, K2=100.0)
+            cfg = inputs.read_config(p)
         m = Model(cfg, mg_fp32=int(a.mg_fp32), mg_tile=a.mg_tile, mg_omega=a.mg_omega, mg_pre=a.mg_pre,
                   mg_post=a.mg_post)
         t0 = time.perf_counter()
+        def diagnostics():
+            if a.averages:
+                m.accumulate_averages(1.0)
+            if a.energy:
+                m.energy()
+
         if a.integrator_only:
             for n in range(1, a.steps + 1):
                 m.integrator_step(n)
+                diagnostics()
             m.synchronize()
             rep = {}
         else:
@@ -81,6 +98,7 @@ def main(argv=None):
             iters, used = [], 0
             for n in range(n0, n0 + a.steps):
                 rep = m.step(n)
+                diagnostics()
                 iters.append(rep["iters"])
                 used += rep["warm_start"] == 1
             rep["iters_per_step"] = iters
