@@ -158,6 +158,21 @@ PAWSIM_API int pawsim_gpu_zero_averages (pawsim_gpu * m);
 PAWSIM_API int pawsim_gpu_energy (pawsim_gpu * m, int eta_from_step_start, double * KE, double * PE,
                                   double * Z);
 
+/* Asynchronous state output (replaces the synchronous reads and writes of
+ * pawsim_diagnostics_write_model_state, model_code/diagnostics.c:874-908; no reference
+ * counterpart for the overlap). save_begin copies, on the device and in stream order with the
+ * steps, the planes of one save into one of two staging slots: u, v, h (and b with a tracer)
+ * of each layer in turn, w_dia on the Nlay+1 interfaces, and pi under the rigid lid
+ * (pawsim_gpu_save_planes planes of Nx*Ny doubles, x fastest). Their device-to-host copy into
+ * page-locked memory held by the library runs on a second stream, and the call returns at once
+ * with the slot index: the model steps on while the copy and the caller's file writes proceed.
+ * save_wait (any thread) blocks until the slot's host copy is complete and returns it;
+ * save_release hands the slot back. save_begin blocks (up to 600 s) while its slot is held. */
+PAWSIM_API int pawsim_gpu_save_begin (pawsim_gpu * m, int * slot);
+PAWSIM_API int pawsim_gpu_save_wait (pawsim_gpu * m, int slot, const double ** host);
+PAWSIM_API int pawsim_gpu_save_release (pawsim_gpu * m, int slot);
+PAWSIM_API size_t pawsim_gpu_save_planes (const pawsim_gpu * m);
+
 /* Solve L(pi) = rhs on the resident pi/pi_rhs with the GPU multigrid (no projection). */
 PAWSIM_API int pawsim_gpu_solve_mg (pawsim_gpu * m, pawsim_gpu_stats * st);
 

@@ -73,7 +73,8 @@ EXPORTS = (
     "pawsim_nn_net_get_params", "pawsim_nn_net_set_params", "pawsim_nn_net_get_grads",
     "pawsim_nn_net_forward", "pawsim_nn_net_backward", "pawsim_nn_net_adam",
     "pawsim_gpu_accumulate_averages", "pawsim_gpu_scale_averages", "pawsim_gpu_zero_averages",
-    "pawsim_gpu_energy",
+    "pawsim_gpu_energy", "pawsim_gpu_save_begin", "pawsim_gpu_save_wait", "pawsim_gpu_save_release",
+    "pawsim_gpu_save_planes",
 )
 
 _LIB = None
@@ -107,6 +108,11 @@ def load_library(path: str = LIB_PATH):
     lib.pawsim_gpu_zero_averages.argtypes = [P]
     D = ctypes.POINTER(ctypes.c_double)
     lib.pawsim_gpu_energy.argtypes = [P, ctypes.c_int, D, D, D]
+    lib.pawsim_gpu_save_begin.argtypes = [P, ctypes.POINTER(ctypes.c_int)]
+    lib.pawsim_gpu_save_wait.argtypes = [P, ctypes.c_int, ctypes.POINTER(D)]
+    lib.pawsim_gpu_save_release.argtypes = [P, ctypes.c_int]
+    lib.pawsim_gpu_save_planes.argtypes = [P]
+    lib.pawsim_gpu_save_planes.restype = ctypes.c_size_t
     lib.pawsim_gpu_set_stream.argtypes = [P, P]
     lib.pawsim_gpu_synchronize.argtypes = [P]
     lib.pawsim_gpu_time.argtypes = [P]
@@ -308,6 +314,24 @@ class Model:
 
     def zero_averages(self) -> None:
         _check(self.lib.pawsim_gpu_zero_averages(self._h))
+
+    def save_begin(self) -> int:
+        """Snapshot the state of one save on the device and start its copy to host memory;
+        returns the slot (the model can step on at once)."""
+        slot = ctypes.c_int()
+        _check(self.lib.pawsim_gpu_save_begin(self._h, ctypes.byref(slot)))
+        return slot.value
+
+    def save_wait(self, slot: int) -> np.ndarray:
+        """The planes of a save (u, v, h[, b] per layer, w_dia per interface, pi), shape
+        (planes, Ny, Nx), copied out of the slot."""
+        ptr = ctypes.POINTER(ctypes.c_double)()
+        _check(self.lib.pawsim_gpu_save_wait(self._h, slot, ctypes.byref(ptr)))
+        n = self.lib.pawsim_gpu_save_planes(self._h)
+        return np.ctypeslib.as_array(ptr, shape=(n, self.Ny, self.Nx)).copy()
+
+    def save_release(self, slot: int) -> None:
+        _check(self.lib.pawsim_gpu_save_release(self._h, slot))
 
     def energy(self, eta_from_step_start: bool = False):
         """(KE, PE, [Z_k]) of the current state: the sums of one EZdiags.dat line

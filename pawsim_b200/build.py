@@ -45,8 +45,8 @@ def build_driver(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale(DRIVER, deps):
         return DRIVER
     os.makedirs(os.path.dirname(DRIVER), exist_ok=True)
-    cmd = ["gcc", "-O2", "-std=c11", "-Wall", "-Wextra", "-I", INCLUDE, DRIVER_SRC, "-o", DRIVER,
-           "-L", HERE, "-lpawsim_b200", "-Wl,-rpath,$ORIGIN/..", "-lm"]
+    cmd = ["gcc", "-O2", "-std=gnu11", "-Wall", "-Wextra", "-I", INCLUDE, DRIVER_SRC, "-o", DRIVER,
+           "-L", HERE, "-lpawsim_b200", "-Wl,-rpath,$ORIGIN/..", "-lm", "-pthread"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

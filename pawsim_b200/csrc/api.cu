@@ -7,6 +7,9 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <chrono>
+#include <condition_variable>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -100,6 +103,20 @@ struct Model {
   double* ez = nullptr;      // energy-diagnostic scratch (terms or partials) and its size
   size_t ez_elems = 0;
   double* ez_out = nullptr;  // KE, PE, Z[L]
+  // asynchronous saves: two staging slots (device, packed planes) with page-locked host
+  // copies, filled by a copy stream; busy until the caller releases the slot
+  struct SaveSlot {
+    double* dev = nullptr;
+    double* host = nullptr;
+    cudaEvent_t staged = nullptr, done = nullptr;
+    bool busy = false;
+  };
+  SaveSlot save[2];
+  int save_next = 0, device = 0;
+  size_t save_planes = 0;
+  cudaStream_t copy_s = nullptr;
+  std::mutex save_mu;
+  std::condition_variable save_cv;
   cudaEvent_t ev0, ev1;
 
   template <typename T> T* alloc(size_t n) {
@@ -110,6 +127,13 @@ struct Model {
     return (T*)p;
   }
   ~Model() {
+    if (copy_s) cudaStreamSynchronize(copy_s);
+    for (SaveSlot& q : save) {
+      if (q.host) cudaFreeHost(q.host);
+      if (q.staged) cudaEventDestroy(q.staged);
+      if (q.done) cudaEventDestroy(q.done);
+    }
+    if (copy_s) cudaStreamDestroy(copy_s);
     delete ws;
     delete dmg;
     delete mg;
@@ -799,6 +823,89 @@ int pawsim_gpu_energy(pawsim_gpu* h, int eta_from_step_start, double* KE, double
   for (int k = 0; k < m->L; ++k) Z[k] = out[2 + k];
   return 0;
 }
+
+// planes of one save, in file order: u, v, h (and b) per layer, w_dia per interface, pi
+static size_t save_plane_count(const Model* m) {
+  return (size_t)m->L * (m->c.use_tracer ? 4 : 3) + (m->L + 1) + (m->c.use_rl ? 1 : 0);
+}
+
+int pawsim_gpu_save_begin(pawsim_gpu* h, int* slot_out) {
+  if (!h || !slot_out) return fail(PAWSIM_GPU_EBADCONFIG, "null argument");
+  Model* m = h->m;
+  if (!m->ready) return fail(PAWSIM_GPU_EBADCONFIG, "pawsim_gpu_init must follow the uploads");
+  const size_t N = (size_t)m->Nx * m->Ny;
+  if (!m->copy_s) {
+    PAWSIM_CUDA_OK(cudaGetDevice(&m->device));
+    PAWSIM_CUDA_OK(cudaStreamCreateWithFlags(&m->copy_s, cudaStreamNonBlocking));
+    m->save_planes = save_plane_count(m);
+    for (Model::SaveSlot& q : m->save) {
+      q.dev = m->alloc<double>(m->save_planes * N);
+      if (!q.dev) return fail(PAWSIM_GPU_ECUDA, "save staging allocation failed");
+      PAWSIM_CUDA_OK(cudaMallocHost(&q.host, m->save_planes * N * sizeof(double)));
+      PAWSIM_CUDA_OK(cudaEventCreateWithFlags(&q.staged, cudaEventDisableTiming));
+      PAWSIM_CUDA_OK(cudaEventCreateWithFlags(&q.done, cudaEventDisableTiming));
+    }
+  }
+  const int sl = m->save_next;
+  Model::SaveSlot& q = m->save[sl];
+  {
+    // a slot is reused only after its previous contents were handed back
+    std::unique_lock<std::mutex> lk(m->save_mu);
+    if (!m->save_cv.wait_for(lk, std::chrono::seconds(600), [&] { return !q.busy; }))
+      return fail(PAWSIM_GPU_EBADCONFIG, "no save slot was released within 600 s");
+    q.busy = true;
+  }
+  m->save_next ^= 1;
+  std::vector<const double*> src;
+  const int cur = m->cur;
+  for (int k = 0; k < m->L; ++k) {
+    src.push_back(m->u[cur] + k * m->lstride);
+    src.push_back(m->v[cur] + k * m->lstride);
+    src.push_back(m->h[cur] + k * m->lstride);
+    if (m->c.use_tracer) src.push_back(m->b[cur] + k * m->lstride);
+  }
+  for (int k = 0; k <= m->L; ++k) src.push_back(m->wdia + k * m->lstride);
+  if (m->c.use_rl) src.push_back(m->pi);
+  // the slot's previous copy-out (if any) must be finished before the slot is refilled;
+  // pack on the model's stream (ordered with the steps), then copy out on the copy stream
+  PAWSIM_CUDA_OK(cudaStreamWaitEvent(m->s, q.done, 0));
+  for (size_t p = 0; p < src.size(); ++p)
+    PAWSIM_CUDA_OK(cudaMemcpy2DAsync(q.dev + p * N, m->Nx * sizeof(double), src[p], m->pitch * sizeof(double),
+                                     m->Nx * sizeof(double), m->Ny, cudaMemcpyDeviceToDevice, m->s));
+  PAWSIM_CUDA_OK(cudaEventRecord(q.staged, m->s));
+  PAWSIM_CUDA_OK(cudaStreamWaitEvent(m->copy_s, q.staged, 0));
+  PAWSIM_CUDA_OK(cudaMemcpyAsync(q.host, q.dev, src.size() * N * sizeof(double), cudaMemcpyDeviceToHost, m->copy_s));
+  PAWSIM_CUDA_OK(cudaEventRecord(q.done, m->copy_s));
+  *slot_out = sl;
+  return 0;
+}
+
+int pawsim_gpu_save_wait(pawsim_gpu* h, int slot, const double** host) {
+  if (!h || !host || slot < 0 || slot > 1) return fail(PAWSIM_GPU_EBADCONFIG, "bad argument");
+  Model* m = h->m;
+  Model::SaveSlot& q = m->save[slot];
+  {
+    std::lock_guard<std::mutex> lk(m->save_mu);
+    if (!q.busy) return fail(PAWSIM_GPU_EBADCONFIG, "slot holds no save");
+  }
+  PAWSIM_CUDA_OK(cudaSetDevice(m->device));
+  PAWSIM_CUDA_OK(cudaEventSynchronize(q.done));
+  *host = q.host;
+  return 0;
+}
+
+int pawsim_gpu_save_release(pawsim_gpu* h, int slot) {
+  if (!h || slot < 0 || slot > 1) return fail(PAWSIM_GPU_EBADCONFIG, "bad argument");
+  Model* m = h->m;
+  {
+    std::lock_guard<std::mutex> lk(m->save_mu);
+    m->save[slot].busy = false;
+  }
+  m->save_cv.notify_all();
+  return 0;
+}
+
+size_t pawsim_gpu_save_planes(const pawsim_gpu* h) { return h ? save_plane_count(h->m) : 0; }
 
 int pawsim_gpu_solve_mg(pawsim_gpu* h, pawsim_gpu_stats* st) {
   if (!h) return PAWSIM_GPU_EBADCONFIG;

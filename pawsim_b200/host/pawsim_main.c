@@ -20,9 +20,12 @@
  *     set (pawsim.c:100-108, 515-522).
  * Exit status 0 on success, 1 on any failure, with the message on stderr.
  * GPU-only controls come from the environment: PAWSIM_GPU_MG_FP32=1 runs FP32 V-cycles
- * inside FP64 defect correction.
+ * inside FP64 defect correction; PAWSIM_GPU_SYNC_OUTPUT=1 writes each save before the next
+ * step instead of from the background writer (the default: the state is snapshotted on the
+ * device and a second thread writes the files while the model steps on).
  */
 #include <math.h>
+#include <pthread.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -523,6 +526,134 @@ static int write_state (pawsim_gpu * m, const config * c, const char * outdir, u
   return 1;
 }
 
+/* the files of one save from the planes of pawsim_gpu_save_begin (u, v, h, b per layer,
+ * w_dia per interface, pi), under the names of write_state */
+static int write_save_planes (const config * c, const char * outdir, unsigned n, const double * host)
+{
+  const size_t N = (size_t) c->Nx * c->Ny;
+  const char * pre[4] = {"U","V","H","B"};
+  char name[NAMELEN];
+  unsigned k;
+  int a;
+  for (k = 0; k < c->Nlay; k ++)
+  {
+    for (a = 0; a < (c->useTracer ? 4 : 3); a ++)
+    {
+      snprintf(name,sizeof(name),"%s%u_n=%u.dat",pre[a],k,n);
+      if (!write_f64(outdir,name,host,N)) return 0;
+      host += N;
+    }
+  }
+  for (k = 0; k <= c->Nlay; k ++)
+  {
+    snprintf(name,sizeof(name),"W%u_n=%u.dat",k,n);
+    if (!write_f64(outdir,name,host,N)) return 0;
+    host += N;
+  }
+  if (c->useRL)
+  {
+    snprintf(name,sizeof(name),"P_n=%u.dat",n);
+    if (!write_f64(outdir,name,host,N)) return 0;
+  }
+  return 1;
+}
+
+/* Background writer of the asynchronous saves: the main loop snapshots the state with
+ * pawsim_gpu_save_begin and queues (slot, n); this thread waits for the slot's host copy,
+ * writes that save's files and releases the slot, while the model steps on. */
+typedef struct
+{
+  pawsim_gpu * m;
+  const config * c;
+  const char * outdir;
+  pthread_t th;
+  pthread_mutex_t mu;
+  pthread_cond_t cv;
+  int slot[2];
+  unsigned n[2];
+  int head, count, stop, failed;
+} writer;
+
+static void * writer_main (void * arg)
+{
+  writer * w = (writer *) arg;
+  for (;;)
+  {
+    int slot, ok;
+    unsigned n;
+    const double * host = NULL;
+    pthread_mutex_lock(&w->mu);
+    while (w->count == 0 && !w->stop) pthread_cond_wait(&w->cv,&w->mu);
+    if (w->count == 0)
+    {
+      pthread_mutex_unlock(&w->mu);
+      break;
+    }
+    slot = w->slot[w->head];
+    n = w->n[w->head];
+    pthread_mutex_unlock(&w->mu);
+    ok = gpu_ok(pawsim_gpu_save_wait(w->m,slot,&host),"save") && write_save_planes(w->c,w->outdir,n,host);
+    if (!ok) fprintf(stderr,"Unable to write model state n=%u\n",n);
+    pawsim_gpu_save_release(w->m,slot);
+    pthread_mutex_lock(&w->mu);
+    w->head = (w->head + 1) % 2;
+    w->count --;
+    if (!ok) w->failed = 1;
+    pthread_cond_broadcast(&w->cv);
+    pthread_mutex_unlock(&w->mu);
+  }
+  return NULL;
+}
+
+static int writer_start (writer * w, pawsim_gpu * m, const config * c, const char * outdir)
+{
+  memset(w,0,sizeof(*w));
+  w->m = m;
+  w->c = c;
+  w->outdir = outdir;
+  pthread_mutex_init(&w->mu,NULL);
+  pthread_cond_init(&w->cv,NULL);
+  if (pthread_create(&w->th,NULL,writer_main,w) != 0)
+  {
+    fprintf(stderr,"ERROR: could not start the output thread\n");
+    return 0;
+  }
+  return 1;
+}
+
+/* snapshot the current state as save n and queue its files */
+static int writer_push (writer * w, unsigned n)
+{
+  int slot, failed;
+  pthread_mutex_lock(&w->mu);
+  failed = w->failed;
+  pthread_mutex_unlock(&w->mu);
+  if (failed || !gpu_ok(pawsim_gpu_save_begin(w->m,&slot),"save")) return 0;
+  pthread_mutex_lock(&w->mu);
+  while (w->count == 2) pthread_cond_wait(&w->cv,&w->mu);
+  w->slot[(w->head + w->count) % 2] = slot;
+  w->n[(w->head + w->count) % 2] = n;
+  w->count ++;
+  pthread_cond_broadcast(&w->cv);
+  pthread_mutex_unlock(&w->mu);
+  return 1;
+}
+
+/* write what is queued, stop the thread; 0 if any save failed */
+static int writer_finish (writer * w)
+{
+  int failed;
+  pthread_mutex_lock(&w->mu);
+  w->stop = 1;
+  pthread_cond_broadcast(&w->cv);
+  pthread_mutex_unlock(&w->mu);
+  pthread_join(w->th,NULL);
+  failed = w->failed;
+  pthread_mutex_destroy(&w->mu);
+  pthread_cond_destroy(&w->cv);
+  return !failed;
+}
+
 /* one completed online-average window under AWSIM's names (diagnostics.c:378-420) */
 static int write_averages (pawsim_gpu * m, const config * c, const char * outdir, unsigned n, double * plane)
 {
@@ -607,6 +738,9 @@ int main (int argc, char ** argv)
   double wall_total = 0, iters_total = 0;
   const char * slash;
   int rc = 1;
+  writer wr;
+  int async_out = !(getenv("PAWSIM_GPU_SYNC_OUTPUT") && atoi(getenv("PAWSIM_GPU_SYNC_OUTPUT")));
+  int writer_on = 0;
 
   if (argc < 3)
   {
@@ -707,7 +841,12 @@ int main (int argc, char ** argv)
     printf("PAWSIM pressure iterations: %u\n",(unsigned) st.iters);
     fflush(stdout);
   }
-  if (!write_state(m,&c,outdir,n_saves,plane)) goto done;
+  if (async_out)
+  {
+    if (!writer_start(&wr,m,&c,outdir)) goto done;
+    writer_on = 1;
+  }
+  if (!(async_out ? writer_push(&wr,n_saves) : write_state(m,&c,outdir,n_saves,plane))) goto done;
   n_saves ++;
 
   for (n = 1; n <= c.Nt; n ++)
@@ -741,7 +880,7 @@ int main (int argc, char ** argv)
     t = pawsim_gpu_time(m);
     while (c.savefrequency > 0 && !(t + eps < n_saves * c.savefrequency))
     {
-      if (!write_state(m,&c,outdir,n_saves,plane))
+      if (!(async_out ? writer_push(&wr,n_saves) : write_state(m,&c,outdir,n_saves,plane)))
       {
         fprintf(stderr,"Unable to write model state n=%u\n",n_saves);
         goto done;
@@ -782,6 +921,7 @@ int main (int argc, char ** argv)
   }
   rc = 0;
 done:
+  if (writer_on && !writer_finish(&wr)) rc = 1;
   free(plane);
   pawsim_gpu_destroy(m);
   return rc;
