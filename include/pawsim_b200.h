@@ -90,7 +90,27 @@ typedef struct pawsim_gpu_config
    * diapycnal diffusion (diaDiffFile, bFluxFile) are not built. */
   int use_tracer, tracer_scheme;
   double K2, K4;
+  /* First guess of the multigrid solves (pressureSolver 1 and 2): 0 the previous pressure,
+   * as the reference; 1 the linear extrapolation 2 pi(n-1) - pi(n-2) of the last two
+   * solutions (from the third solve on). The stopping test is unchanged, so the solution
+   * meets the same tolerance; only the number of V-cycles changes. SOR ignores it. */
+  int pi_guess;
+  /* Tendency budgets kept on the device (work.c:1753-1937 and the terms of forcing.c,
+   * restoring.c, diapycnal.c and the pressure correction): a bit mask of the families,
+   * PAWSIM_GPU_BUDGET_UMOM (savefreqUMom), _VMOM, _THIC, _ENERGY, _TRAC. Each step then adds
+   * every term times dt to its running sum; the sums are read with pawsim_gpu_get_field under
+   * the reference's output names (UMom_PVadvection, ..., Tracer_relaxation; k = layer). */
+  int budgets;
 } pawsim_gpu_config;
+
+enum
+{
+  PAWSIM_GPU_BUDGET_UMOM = 1,
+  PAWSIM_GPU_BUDGET_VMOM = 2,
+  PAWSIM_GPU_BUDGET_THIC = 4,
+  PAWSIM_GPU_BUDGET_ENERGY = 8,
+  PAWSIM_GPU_BUDGET_TRAC = 16
+};
 
 /* Per-solve report, the numbers of the "PAWSIM pressure solve" line (pawsim.c:100-108). */
 typedef struct pawsim_gpu_stats
@@ -145,6 +165,14 @@ PAWSIM_API int pawsim_gpu_run (pawsim_gpu * m, unsigned n0, unsigned nsteps, paw
 PAWSIM_API int pawsim_gpu_accumulate_averages (pawsim_gpu * m, double avg_fac);
 PAWSIM_API int pawsim_gpu_scale_averages (pawsim_gpu * m, double factor);
 PAWSIM_API int pawsim_gpu_zero_averages (pawsim_gpu * m);
+
+/* Budget windows (pawsim_diagnostics_write_budgets_if_due, diagnostics.c:756-866): scale
+ * multiplies every sum of the families in `mask` by factor (1 / ((n - n_prev) dt) when a
+ * family's window is written); zero resets them. The sums accumulate in
+ * pawsim_gpu_integrator_step / pawsim_gpu_step (the tendency, forcing, restoring, diapycnal
+ * and tracer terms) and in the step's pressure correction (the Montgomery terms). */
+PAWSIM_API int pawsim_gpu_scale_budgets (pawsim_gpu * m, int mask, double factor);
+PAWSIM_API int pawsim_gpu_zero_budgets (pawsim_gpu * m, int mask);
 
 /* Energy and enstrophy diagnostics (replaces the sums of pawsim_diagnostics_write_EZ_if_due,
  * model_code/diagnostics.c:478-700, whose line of EZdiags.dat the caller writes): the

@@ -47,7 +47,8 @@ class GpuConfig(ctypes.Structure):
                         ("mg_post", ctypes.c_int), ("mg_omega", ctypes.c_double),
                         ("serial_sums", ctypes.c_int), ("mg_tile", ctypes.c_int),
                         ("use_tracer", ctypes.c_int), ("tracer_scheme", ctypes.c_int),
-                        ("K2", ctypes.c_double), ("K4", ctypes.c_double)]
+                        ("K2", ctypes.c_double), ("K4", ctypes.c_double),
+                        ("pi_guess", ctypes.c_int), ("budgets", ctypes.c_int)]
 
 
 class GpuStats(ctypes.Structure):
@@ -74,7 +75,7 @@ EXPORTS = (
     "pawsim_nn_net_forward", "pawsim_nn_net_backward", "pawsim_nn_net_adam",
     "pawsim_gpu_accumulate_averages", "pawsim_gpu_scale_averages", "pawsim_gpu_zero_averages",
     "pawsim_gpu_energy", "pawsim_gpu_save_begin", "pawsim_gpu_save_wait", "pawsim_gpu_save_release",
-    "pawsim_gpu_save_planes",
+    "pawsim_gpu_save_planes", "pawsim_gpu_scale_budgets", "pawsim_gpu_zero_budgets",
 )
 
 _LIB = None
@@ -113,6 +114,8 @@ def load_library(path: str = LIB_PATH):
     lib.pawsim_gpu_save_release.argtypes = [P, ctypes.c_int]
     lib.pawsim_gpu_save_planes.argtypes = [P]
     lib.pawsim_gpu_save_planes.restype = ctypes.c_size_t
+    lib.pawsim_gpu_scale_budgets.argtypes = [P, ctypes.c_int, ctypes.c_double]
+    lib.pawsim_gpu_zero_budgets.argtypes = [P, ctypes.c_int]
     lib.pawsim_gpu_set_stream.argtypes = [P, P]
     lib.pawsim_gpu_synchronize.argtypes = [P]
     lib.pawsim_gpu_time.argtypes = [P]
@@ -182,6 +185,9 @@ def gpu_config(cfg: inputs.Config, **over) -> GpuConfig:
     g.mg_tile = 0
     g.use_tracer, g.tracer_scheme = int(v["useTracer"]), int(v["tracerScheme"])
     g.K2, g.K4 = float(v["K2"]), float(v["K4"])
+    # budget families of the savefreq keys (work.c:310-319)
+    g.budgets = sum(bit for bit, key in ((1, "savefreqUMom"), (2, "savefreqVMom"), (4, "savefreqThic"),
+                                         (8, "savefreqEnergy"), (16, "savefreqTracer")) if v[key] > 0)
     for k, val in over.items():
         setattr(g, k, val)
     return g
@@ -314,6 +320,12 @@ class Model:
 
     def zero_averages(self) -> None:
         _check(self.lib.pawsim_gpu_zero_averages(self._h))
+
+    def scale_budgets(self, mask: int, factor: float) -> None:
+        _check(self.lib.pawsim_gpu_scale_budgets(self._h, mask, factor))
+
+    def zero_budgets(self, mask: int = 31) -> None:
+        _check(self.lib.pawsim_gpu_zero_budgets(self._h, mask))
 
     def save_begin(self) -> int:
         """Snapshot the state of one save on the device and start its copy to host memory;

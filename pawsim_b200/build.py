@@ -26,6 +26,7 @@ SOURCES = ["api.cu", "tendency.cu", "pressure.cu", "mg.cu", "noalloc.cu", "nn.cu
 UNITS = [(s.replace(".cu", ""), s, []) for s in SOURCES] + [
     ("tendency_ty8", "tendency_tile.cu", ["-DPAWSIM_TEND_TY=8"]),
     ("tendency_ty16", "tendency_tile.cu", ["-DPAWSIM_TEND_TY=16"]),
+    ("tendency_budget", "tendency_tile.cu", ["-DPAWSIM_TEND_TY=8", "-DPAWSIM_TEND_BUD=1", "-DPAWSIM_TEND_MINB=2"]),
 ]
 DRIVER_SRC = os.path.join(HERE, "host", "pawsim_main.c")
 DRIVER = os.path.join(HERE, "bin", "PAWSIM_B200.exe")

@@ -38,6 +38,17 @@ static int fail(int code, const char* msg) {
   return code;
 }
 
+// first guess 2 pi - prev (linear extrapolation of the last two solutions); prev <- pi
+__global__ void extrapolate_kernel(double* pi, double* prev, int Nx, int Ny, int pitch) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= Nx || j >= Ny) return;
+  size_t c = (size_t)j * pitch + i;
+  const double a = pi[c], b = prev[c];
+  pi[c] = 2 * a - b;
+  prev[c] = a;
+}
+
 // rigid-lid column constraint (pressure.c:525-561) when it is not fused into K-tend
 __global__ void thickness_fix_kernel(double* h, const double* Hc, int Nx, int Ny, int pitch, size_t ls, int L) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -103,6 +114,10 @@ struct Model {
   double* ez = nullptr;      // energy-diagnostic scratch (terms or partials) and its size
   size_t ez_elems = 0;
   double* ez_out = nullptr;  // KE, PE, Z[L]
+  // budget families (config bit q): [term][layer] planes lstride apart, nullptr when off
+  double* bud[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  double* pi_prev = nullptr;   // solution before the last one (pi_guess = 1)
+  int pi_solves = 0;           // multigrid solves completed, for the extrapolated guess
   // asynchronous saves: two staging slots (device, packed planes) with page-locked host
   // copies, filled by a copy stream; busy until the caller releases the slot
   struct SaveSlot {
@@ -166,6 +181,8 @@ static void fill_d(double* d, size_t n, double v) {
 static int create(const pawsim_gpu_config* cfg, Model** out) {
   const pawsim_gpu_config& c = *cfg;
   if (c.Nlay < 1 || c.Nlay > LMAX) return fail(PAWSIM_GPU_EBADCONFIG, "Nlay must be in 1..8");
+  if (c.pi_guess < 0 || c.pi_guess > 1) return fail(PAWSIM_GPU_EBADCONFIG, "pi_guess must be 0 or 1");
+  if (c.budgets < 0 || c.budgets > 31) return fail(PAWSIM_GPU_EBADCONFIG, "budgets is a mask of five families");
   if (c.Nx < 4 || c.Ny < 4) return fail(PAWSIM_GPU_EBADCONFIG, "Nx and Ny must be at least 4");
   if (c.Ly <= 0 || c.Lx <= 0 || c.dt <= 0) return fail(PAWSIM_GPU_EBADCONFIG, "Lx, Ly and dt must be positive");
   if (c.ts_scheme < 3 || c.ts_scheme > 5)
@@ -278,6 +295,29 @@ static int avg_slot(const std::string& n) {
   return -1;
 }
 
+// the budget families in config-bit order and their output names (defs.h:217-288)
+static const int kBudgetTerms[5] = {BU_NTERMS, BU_NTERMS, BH_NTERMS, BE_NTERMS, BB_NTERMS};
+static const char* const kBudgetNames[5][BU_NTERMS] = {
+    {"UMom_PVadvection", "UMom_Montgomery", "UMom_KEgradient", "UMom_dhdt", "UMom_viscosity", "UMom_hypervisc",
+     "UMom_linBotDrag", "UMom_linSurfDrag", "UMom_quadBotDrag", "UMom_quadSurfDrag", "UMom_windStress",
+     "UMom_buoyForce", "UMom_relaxation", "UMom_diapycnal", "UMom_baroForcing", "UMom_diaVisc"},
+    {"VMom_PVadvection", "VMom_Montgomery", "VMom_KEgradient", "VMom_dhdt", "VMom_viscosity", "VMom_hypervisc",
+     "VMom_linBotDrag", "VMom_linSurfDrag", "VMom_quadBotDrag", "VMom_quadSurfDrag", "VMom_windStress",
+     "VMom_buoyForce", "VMom_relaxation", "VMom_diapycnal", "VMom_baroForcing", "VMom_diaVisc"},
+    {"Thic_advection", "Thic_relaxation"},
+    {"Energy_advection", "Energy_Montgomery", "Energy_windStress", "Energy_linBotDrag", "Energy_linSurfDrag",
+     "Energy_quadBotDrag", "Energy_quadSurfDrag", "Energy_viscosity", "Energy_hypervisc", "Energy_diaProd",
+     "Energy_diaAdv", "Energy_baroForcing", "Energy_buoyForce", "Energy_relaxation", "Energy_diaVisc"},
+    {"Tracer_advection", "Tracer_diaAdv", "Tracer_isoDiff", "Tracer_hyperdiff", "Tracer_diaDiff",
+     "Tracer_relaxation"}};
+
+static double* budget_plane(Model* m, const std::string& n) {
+  for (int f = 0; f < 5; ++f)
+    for (int t = 0; m->bud[f] && t < kBudgetTerms[f]; ++t)
+      if (n == kBudgetNames[f][t]) return m->bud[f] + (size_t)t * m->L * m->lstride;
+  return nullptr;
+}
+
 static bool lookup(Model* m, const std::string& n, FieldRef& f) {
   int L = m->L;
   f = FieldRef{nullptr, m->Ny, m->Nx, m->pitch, m->lstride, 1, true};
@@ -324,6 +364,7 @@ static bool lookup(Model* m, const std::string& n, FieldRef& f) {
     else if (m->avg && n == "W_avg") { f.base = m->avg + (size_t)9 * L * m->lstride; f.nk = L + 1; }
     else if (m->avg && n == "P_avg") f.base = m->avg + (size_t)(10 * L + 1) * m->lstride;
     else if (m->avg && m->b[0] && n == "B_avg") { f.base = m->avg + (size_t)(10 * L + 2) * m->lstride; f.nk = L; }
+    else if (double* bp = budget_plane(m, n)) { f.base = bp; f.nk = L; }
     else return false;
   }
   return true;
@@ -346,6 +387,7 @@ static int set_field(Model* m, const char* name, int k, const double* host, size
   PAWSIM_CUDA_OK(cudaMemcpy2DAsync(f.base + k * f.kstride, f.pitch * sizeof(double), host, f.cols * sizeof(double),
                                    f.cols * sizeof(double), f.rows, cudaMemcpyHostToDevice, m->s));
   if (nm == "h") m->prev_h = false;
+  if (nm == "pi") m->pi_solves = 0;
   // the state halo fill (state.c:1052-1057) puts +0 on wall faces of the normal velocity
   if (nm == "u" && m->c.wall_ew)
     PAWSIM_CUDA_OK(cudaMemset2DAsync(f.base + k * f.kstride, f.pitch * sizeof(double), 0, sizeof(double), f.rows, m->s));
@@ -378,6 +420,12 @@ static int get_field(Model* m, const char* name, int k, double* host, size_t n) 
 }
 
 static int init(Model* m) {
+  for (int f = 0; f < 5; ++f) {
+    if (!(m->c.budgets & (1 << f)) || m->bud[f]) continue;
+    if (f == 4 && !m->c.use_tracer) continue;   // the tracer family needs a tracer
+    m->bud[f] = m->alloc<double>((size_t)kBudgetTerms[f] * m->L * m->lstride);
+    if (!m->bud[f]) return fail(PAWSIM_GPU_ECUDA, "budget storage allocation failed");
+  }
   // state halo fill of state.c:1052-1057: wall-normal velocity is zero on the wall face
   for (int k = 0; k < m->L; ++k) {
     if (m->c.wall_ew)
@@ -520,7 +568,14 @@ static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
   int nb = 1 - m->cur;
   p.u_out = m->u[nb]; p.v_out = m->v[nb]; p.h_out = m->h[nb];
   p.fuse_thickness_fix = (fuse_fix && c.use_rl) ? 1 : 0;
-  if (launch_tendency(p, c.mom_scheme, c.thick_scheme, m->s) != 0)
+  const bool budgets = m->bud[0] || m->bud[1] || m->bud[2] || m->bud[3] || m->bud[4];
+  if (budgets) {
+    p.dt = dt;
+    p.bud_u = m->bud[0]; p.bud_v = m->bud[1]; p.bud_h = m->bud[2]; p.bud_e = m->bud[3]; p.bud_b = m->bud[4];
+    p.b = c.use_tracer ? m->b[m->cur] : nullptr;
+  }
+  if ((budgets ? launch_tendency_budget(p, c.mom_scheme, c.thick_scheme, m->s)
+               : launch_tendency(p, c.mom_scheme, c.thick_scheme, m->s)) != 0)
     return fail(PAWSIM_GPU_EUNSUPPORTED, "scheme combination not available");
   ++g_launches;
   if (c.use_tracer) {
@@ -538,6 +593,7 @@ static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
     tp.bRelax = m->bRelax; tp.bTime = m->bTime; tp.wdia = m->wdia;
     tp.ab_mode = p.ab_mode; tp.c0 = p.c0; tp.c1 = p.c1; tp.c2 = p.c2; tp.write_hist = p.write_hist;
     tp.f1b = m->fb[m->h1]; tp.f2b = m->fb[h2]; tp.fb_out = m->fb[h2]; tp.b_out = m->b[nb];
+    tp.bud_b = m->bud[4]; tp.dt = dt;
     launch_tracer(tp, m->s);
     ++g_launches;
   }
@@ -562,7 +618,6 @@ static int finish_norms(Model* m, const double* field, double* mx, double* rms) 
 }
 
 static int pressure_correct(Model* m, int update_diags, pawsim_gpu_stats* st) {
-  (void)update_diags;
   pawsim_gpu_stats local;
   memset(&local, 0, sizeof(local));
   if (!m->ready) return fail(PAWSIM_GPU_EBADCONFIG, "pawsim_gpu_init must follow the uploads");
@@ -584,6 +639,21 @@ static int pressure_correct(Model* m, int update_diags, pawsim_gpu_stats* st) {
   g_launches += m->serial() ? 2 : 3;
   PAWSIM_CUDA_OK(cudaGetLastError());
   PAWSIM_CUDA_OK(cudaEventRecord(m->ev0, m->s));
+  if (m->c.pi_guess == 1 && m->c.solver != PAWSIM_GPU_SOLVER_SOR) {
+    // pi holds the last solution; from the third solve on start from the extrapolation
+    if (!m->pi_prev) {
+      m->pi_prev = m->alloc<double>((size_t)m->Ny * m->pitch);
+      if (!m->pi_prev) return fail(PAWSIM_GPU_ECUDA, "pressure history allocation failed");
+    }
+    if (m->pi_solves >= 2) {
+      extrapolate_kernel<<<gr, b, 0, m->s>>>(m->pi, m->pi_prev, m->Nx, m->Ny, m->pitch);
+      ++g_launches;
+    } else if (m->pi_solves == 1) {
+      PAWSIM_CUDA_OK(cudaMemcpyAsync(m->pi_prev, m->pi, (size_t)m->Ny * m->pitch * sizeof(double),
+                                     cudaMemcpyDeviceToDevice, m->s));
+    }
+    ++m->pi_solves;
+  }
   int iters = 0;
   if (m->c.solver == PAWSIM_GPU_SOLVER_SOR) {
     if (launch_sor(g, m->pi, m->rhs, m->op, m->c.sor_rp, m->c.pi_tol, m->c.maxiters, m->slots, m->diters, m->s) != 0)
@@ -641,7 +711,10 @@ static int pressure_correct(Model* m, int update_diags, pawsim_gpu_stats* st) {
     int r = finish_norms(m, m->work, &local.residual_max, &local.residual_rms);
     if (r) return r;
   }
-  launch_projection(g, m->pi, m->u[cur], m->v[cur], m->s);
+  if (update_diags && (m->bud[0] || m->bud[1] || m->bud[3]))
+    launch_projection_budget(g, m->pi, m->u[cur], m->v[cur], m->h[cur], m->bud[0], m->bud[1], m->bud[3], m->s);
+  else
+    launch_projection(g, m->pi, m->u[cur], m->v[cur], m->s);
   ++g_launches;
   if (m->c.pressure_timing) {
     g_launches += launch_divergence_field(g, m->u[cur], m->v[cur], m->h[cur], m->work, m->s);
@@ -785,6 +858,27 @@ int pawsim_gpu_zero_averages(pawsim_gpu* h) {
   Model* m = h->m;
   if (m->avg)
     PAWSIM_CUDA_OK(cudaMemsetAsync(m->avg, 0, avg_elems(m) * sizeof(double), m->s));
+  return 0;
+}
+
+int pawsim_gpu_scale_budgets(pawsim_gpu* h, int mask, double factor) {
+  if (!h) return PAWSIM_GPU_EBADCONFIG;
+  Model* m = h->m;
+  for (int f = 0; f < 5; ++f)
+    if ((mask & (1 << f)) && m->bud[f]) {
+      launch_scale(m->bud[f], (size_t)kBudgetTerms[f] * m->L * m->lstride, factor, m->s);
+      ++g_launches;
+    }
+  PAWSIM_CUDA_OK(cudaGetLastError());
+  return 0;
+}
+
+int pawsim_gpu_zero_budgets(pawsim_gpu* h, int mask) {
+  if (!h) return PAWSIM_GPU_EBADCONFIG;
+  Model* m = h->m;
+  for (int f = 0; f < 5; ++f)
+    if ((mask & (1 << f)) && m->bud[f])
+      PAWSIM_CUDA_OK(cudaMemsetAsync(m->bud[f], 0, (size_t)kBudgetTerms[f] * m->L * m->lstride * sizeof(double), m->s));
   return 0;
 }
 

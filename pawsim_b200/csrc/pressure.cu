@@ -6,6 +6,7 @@
 
 #include "common.cuh"
 #include "pressure.cuh"
+#include "tendency.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -393,6 +394,43 @@ __global__ void projection_kernel(const Grid2 g, const double* __restrict__ pi, 
     size_t o = k * g.lstride + c;
     if (!skip_u) u[o] += du;
     if (!skip_v) v[o] += dv;
+  }
+}
+
+// the projection with its budget terms (pressure.c:2182-2245): the face thickness of the
+// state being corrected (as in the RHS, with the velocity before the update) times the
+// increment, and that times the updated velocity
+__global__ void projection_budget_kernel(const Grid2 g, const double* __restrict__ pi, double* __restrict__ u,
+                                         double* __restrict__ v, const double* __restrict__ h, double* bu,
+                                         double* bv, double* be) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.Nx || j >= g.Ny) return;
+  size_t c = (size_t)j * g.pitch + i;
+  double pc = pi[c];
+  double pw = i > 0 ? pi[c - 1] : ld_s(pi, g, i - 1, j);
+  double ps = j > 0 ? pi[c - g.pitch] : ld_s(pi, g, i, j - 1);
+  bool skip_u = g.wall_ew && i == 0;
+  bool skip_v = g.wall_ns && j == 0;
+  const double du = div_rn(-g.dt * (pc - pw), g.dx, g.rdx);
+  const double dv = div_rn(-g.dt * (pc - ps), g.dy, g.rdy);
+  for (int k = 0; k < g.L; ++k) {
+    const size_t o = k * g.lstride + c;
+    const double* hk = h + k * g.lstride;
+    if (!skip_u) {
+      const double hw = hw_face(g, hk, u + k * g.lstride, i, j);
+      const double un = u[o] + du;
+      u[o] = un;
+      budget_add(bu, BU_GRADM, k, g.L, g.lstride, c, hw * du);
+      budget_add(be, BE_GRADM, k, g.L, g.lstride, c, hw * du * un);
+    }
+    if (!skip_v) {
+      const double hs = hs_face(g, hk, v + k * g.lstride, i, j);
+      const double vn = v[o] + dv;
+      v[o] = vn;
+      budget_add(bv, BU_GRADM, k, g.L, g.lstride, c, hs * dv);
+      budget_add(be, BE_GRADM, k, g.L, g.lstride, c, hs * dv * vn);
+    }
   }
 }
 
@@ -844,6 +882,12 @@ int launch_sor(const Grid2& g, double* pi, const double* rhs, const Operator& op
 void launch_projection(const Grid2& g, const double* pi, double* u, double* v, cudaStream_t s) {
   dim3 b(32, 8);
   projection_kernel<<<grid2(g.Nx, g.Ny, b), b, 0, s>>>(g, pi, u, v);
+}
+
+void launch_projection_budget(const Grid2& g, const double* pi, double* u, double* v, const double* h, double* bu,
+                              double* bv, double* be, cudaStream_t s) {
+  dim3 b(32, 8);
+  projection_budget_kernel<<<grid2(g.Nx, g.Ny, b), b, 0, s>>>(g, pi, u, v, h, bu, bv, be);
 }
 
 void launch_residual_field(const Grid2& g, const double* pi, const double* rhs, const Operator& op, double* out,

@@ -47,6 +47,9 @@ int launch_sor(const Grid2& g, double* pi, const double* rhs, const Operator& op
 
 // u -= dt dpi/dx, v -= dt dpi/dy on every layer, skipping wall faces (pressure.c:2182-2248)
 void launch_projection(const Grid2& g, const double* pi, double* u, double* v, cudaStream_t s);
+// the same, adding the Montgomery terms of the u, v and energy budgets (nullable families)
+void launch_projection_budget(const Grid2& g, const double* pi, double* u, double* v, const double* h, double* bu,
+                              double* bv, double* be, cudaStream_t s);
 
 // per-cell residual rhs - L(pi) and barotropic divergence (pressure.c:652-737)
 void launch_residual_field(const Grid2& g, const double* pi, const double* rhs,

@@ -13,12 +13,17 @@ size_t tendency_smem_ty8(const TendParams& p, int ts);
 size_t tendency_smem_ty16(const TendParams& p, int ts);
 int launch_tendency_ty8(const TendParams& p, int ms, int ts, cudaStream_t s);
 int launch_tendency_ty16(const TendParams& p, int ms, int ts, cudaStream_t s);
+int launch_tendency_budget_tile(const TendParams& p, int ms, int ts, cudaStream_t s);
 
 int launch_tendency(const TendParams& p, int ms, int ts, cudaStream_t s) {
   // two CTAs per SM: 228 KB of shared memory, 1 KB reserved per CTA
   constexpr size_t kTwoPerSM = 113 * 1024;
   if (tendency_smem_ty16(p, ts) <= kTwoPerSM) return launch_tendency_ty16(p, ms, ts, s);
   return launch_tendency_ty8(p, ms, ts, s);
+}
+
+int launch_tendency_budget(const TendParams& p, int ms, int ts, cudaStream_t s) {
+  return launch_tendency_budget_tile(p, ms, ts, s);
 }
 
 }  // namespace pawsim

@@ -1,6 +1,7 @@
 // tendency.cuh -- parameters of the fused tendency + Adams-Bashforth kernel.
 #pragma once
 
+#include <cuda_runtime.h>
 #include <stddef.h>
 
 namespace pawsim {
@@ -57,9 +58,35 @@ struct TendParams {
   const double *nu_u, *nu_v;
   // outputs for diagnostics
   double *wdia_out;               // interface velocities [L+1] (nullable)
+  // tendency budgets (work.c:1753-1937, forcing.c:243-389, restoring.c:190-214,
+  // diapycnal.c:243-284): running sums of each term times dt, one family per array of
+  // [term][layer] planes lstride apart, nullptr when the family is off. Used only by the
+  // budget build of the kernel (launch_tendency_budget).
+  double dt;
+  double *bud_u, *bud_v, *bud_h, *bud_e, *bud_b;
+  const double* b;                // tracer at the start of the step (Tracer_advection/diaAdv)
 };
+
+// budget term indices (work.h:18-91)
+enum { BU_Q, BU_GRADM, BU_GRADKE, BU_DHDT, BU_A2, BU_A4, BU_RDRAG, BU_RSURF, BU_CDBOT, BU_CDSURF,
+       BU_WIND, BU_BUOY, BU_RELAX, BU_WDIA, BU_FBARO, BU_DIAVISC, BU_NTERMS };
+enum { BH_ADV, BH_RELAX, BH_NTERMS };
+enum { BE_ADV, BE_GRADM, BE_WIND, BE_RDRAG, BE_RSURF, BE_CDBOT, BE_CDSURF, BE_A2, BE_A4, BE_WDIAPE,
+       BE_WDIAKE, BE_FBARO, BE_BUOY, BE_RELAX, BE_DIAVISC, BE_NTERMS };
+enum { BB_ADV, BB_WDIA, BB_K2, BB_K4, BB_DIADIFF, BB_RELAX, BB_NTERMS };
+
+// family[term][k] += v at one cell (a no-op for a family that is off)
+__device__ inline void budget_add(double* fam, int term, int k, int L, size_t lstride, size_t cell, double v) {
+  if (fam) {
+    double* q = fam + ((size_t)term * L + k) * lstride + cell;
+    *q = *q + v;
+  }
+}
 
 int launch_tendency(const TendParams& p, int momentum_scheme, int thickness_scheme,
                     cudaStream_t stream);
+// the same step with every enabled budget family accumulated (32 x 8 tiles)
+int launch_tendency_budget(const TendParams& p, int momentum_scheme, int thickness_scheme,
+                           cudaStream_t stream);
 
 }  // namespace pawsim

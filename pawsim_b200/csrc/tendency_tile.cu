@@ -28,6 +28,11 @@ namespace {
 #ifndef PAWSIM_TEND_TY
 #define PAWSIM_TEND_TY 8
 #endif
+// PAWSIM_TEND_BUD = 1 builds the budget variant (every enabled budget family accumulated)
+#ifndef PAWSIM_TEND_BUD
+#define PAWSIM_TEND_BUD 0
+#endif
+constexpr bool BUD = PAWSIM_TEND_BUD != 0;
 constexpr int TX = 32;
 constexpr int TY = PAWSIM_TEND_TY;
 constexpr int NT = TX * TY;
@@ -572,6 +577,19 @@ tendency_kernel(const __grid_constant__ TendParams p) {
                + div_rn(A4Q(i, j + 1) * AT(hq, i, j + 1) * d4s1 - A4Q(i, j) * AT(hq, i, j) * d4s0, dy, rdy));
       }
       ru = gM + gK + rq + ((hwest != 0) ? div_rn(a2 + a4 + 0.0, hwest, rhw) : 0);
+      if constexpr (BUD) {
+        // work.c:1753-1763 (the buoyancy terms are zero: buoyancy is not built)
+        const bool active = !(p.wall_ew && gi == 0);
+        budget_add(p.bud_u, BU_GRADM, k, L, p.lstride, cell, hwest * gM * p.dt);
+        budget_add(p.bud_u, BU_GRADKE, k, L, p.lstride, cell, hwest * gK * p.dt);
+        budget_add(p.bud_u, BU_Q, k, L, p.lstride, cell, hwest * rq * p.dt);
+        budget_add(p.bud_u, BU_A2, k, L, p.lstride, cell, active ? a2 * p.dt : 0);
+        budget_add(p.bud_u, BU_A4, k, L, p.lstride, cell, active ? a4 * p.dt : 0);
+        budget_add(p.bud_e, BE_GRADM, k, L, p.lstride, cell, hwest * gM * uc * p.dt);
+        budget_add(p.bud_e, BE_ADV, k, L, p.lstride, cell, hwest * (gK + rq) * uc * p.dt);
+        budget_add(p.bud_e, BE_A2, k, L, p.lstride, cell, a2 * uc * p.dt);
+        budget_add(p.bud_e, BE_A4, k, L, p.lstride, cell, a4 * uc * p.dt);
+      }
     }
     // ---- v momentum (work.c:1759-1852) ----
     double rv;
@@ -606,6 +624,19 @@ tendency_kernel(const __grid_constant__ TendParams p) {
                - div_rn(A4H(i, j) * AT(sh, i, j) * d4t0 - A4H(i, j - 1) * AT(sh, i, j - 1) * d4tm, dy, rdy));
       }
       rv = gM + gK + rq + ((hsouth != 0) ? div_rn(a2 + a4 + 0.0, hsouth, rhs) : 0);
+      if constexpr (BUD) {
+        // work.c:1837-1847
+        const bool active = !(p.wall_ns && gj == 0);
+        budget_add(p.bud_v, BU_GRADM, k, L, p.lstride, cell, hsouth * gM * p.dt);
+        budget_add(p.bud_v, BU_GRADKE, k, L, p.lstride, cell, hsouth * gK * p.dt);
+        budget_add(p.bud_v, BU_Q, k, L, p.lstride, cell, hsouth * rq * p.dt);
+        budget_add(p.bud_v, BU_A2, k, L, p.lstride, cell, active ? a2 * p.dt : 0);
+        budget_add(p.bud_v, BU_A4, k, L, p.lstride, cell, active ? a4 * p.dt : 0);
+        budget_add(p.bud_e, BE_GRADM, k, L, p.lstride, cell, hsouth * gM * vc * p.dt);
+        budget_add(p.bud_e, BE_ADV, k, L, p.lstride, cell, hsouth * (gK + rq) * vc * p.dt);
+        budget_add(p.bud_e, BE_A2, k, L, p.lstride, cell, a2 * vc * p.dt);
+        budget_add(p.bud_e, BE_A4, k, L, p.lstride, cell, a4 * vc * p.dt);
+      }
     }
     // ---- diapycnal advection and viscosity (diapycnal.c:203-291) ----
     if (p.use_wdia || p.use_diavisc) {
@@ -625,8 +656,22 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         double dum = (wu1 > 0) ? uc - um : 0;
         double dvp = (wv0 > 0) ? 0 : vp - vc;
         double dvm = (wv1 > 0) ? vc - vm : 0;
-        if (hwest != 0) ru += div_rn(-(wu0 * dup + wu1 * dum), hwest, rhw);
-        if (hsouth != 0) rv += div_rn(-(wv0 * dvp + wv1 * dvm), hsouth, rhs);
+        if (hwest != 0) {
+          const double r = -(wu0 * dup + wu1 * dum);
+          ru += div_rn(r, hwest, rhw);
+          if constexpr (BUD) {
+            budget_add(p.bud_u, BU_WDIA, k, L, p.lstride, cell, r * p.dt);
+            budget_add(p.bud_e, BE_WDIAKE, k, L, p.lstride, cell, r * uc * p.dt);
+          }
+        }
+        if (hsouth != 0) {
+          const double r = -(wv0 * dvp + wv1 * dvm);
+          rv += div_rn(r, hsouth, rhs);
+          if constexpr (BUD) {
+            budget_add(p.bud_v, BU_WDIA, k, L, p.lstride, cell, r * p.dt);
+            budget_add(p.bud_e, BE_WDIAKE, k, L, p.lstride, cell, r * vc * p.dt);
+          }
+        }
       }
       if (p.use_diavisc && L >= 2) {
         double Fu[2] = {0, 0}, Fv[2] = {0, 0};
@@ -648,8 +693,22 @@ tendency_kernel(const __grid_constant__ TendParams p) {
           if (dzu != 0) Fu[s] = nuu * (ua - ub) / dzu;
           if (dzv != 0) Fv[s] = nuv * (va - vb) / dzv;
         }
-        if (hwest != 0) ru += div_rn(Fu[0] - Fu[1], hwest, rhw);
-        if (hsouth != 0) rv += div_rn(Fv[0] - Fv[1], hsouth, rhs);
+        if (hwest != 0) {
+          const double r = Fu[0] - Fu[1];
+          ru += div_rn(r, hwest, rhw);
+          if constexpr (BUD) {
+            budget_add(p.bud_u, BU_DIAVISC, k, L, p.lstride, cell, r * p.dt);
+            budget_add(p.bud_e, BE_DIAVISC, k, L, p.lstride, cell, r * uc * p.dt);
+          }
+        }
+        if (hsouth != 0) {
+          const double r = Fv[0] - Fv[1];
+          rv += div_rn(r, hsouth, rhs);
+          if constexpr (BUD) {
+            budget_add(p.bud_v, BU_DIAVISC, k, L, p.lstride, cell, r * p.dt);
+            budget_add(p.bud_e, BE_DIAVISC, k, L, p.lstride, cell, r * vc * p.dt);
+          }
+        }
       }
     }
     // ---- forcing and drag (forcing.c:149-395) ----
@@ -674,16 +733,44 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         double ty_ = p.tw0 * p.tauy0[cell] + p.tw1 * p.tauy1[cell];
         double r = tx_ * fsw;
         if (hwest != 0) ru += div_rn(r, hwest, rhw);
+        if constexpr (BUD) {
+          budget_add(p.bud_u, BU_WIND, k, L, p.lstride, cell, r * p.dt);
+          budget_add(p.bud_e, BE_WIND, k, L, p.lstride, cell, r * uc * p.dt);
+        }
         r = ty_ * fss;
         if (hsouth != 0) rv += div_rn(r, hsouth, rhs);
+        if constexpr (BUD) {
+          budget_add(p.bud_v, BU_WIND, k, L, p.lstride, cell, r * p.dt);
+          budget_add(p.bud_e, BE_WIND, k, L, p.lstride, cell, r * vc * p.dt);
+        }
       }
       if (p.use_fbaro) {
-        ru += gload(p.fbx, p, gi, gj, MAP_N, MAP_S);
-        rv += gload(p.fby, p, gi, gj, MAP_S, MAP_N);
+        const double fx = gload(p.fbx, p, gi, gj, MAP_N, MAP_S), fy = gload(p.fby, p, gi, gj, MAP_S, MAP_N);
+        ru += fx;
+        rv += fy;
+        if constexpr (BUD) {
+          budget_add(p.bud_u, BU_FBARO, k, L, p.lstride, cell, hwest * fx * p.dt);
+          budget_add(p.bud_v, BU_FBARO, k, L, p.lstride, cell, hsouth * fy * p.dt);
+          budget_add(p.bud_e, BE_FBARO, k, L, p.lstride, cell, (hwest * fx * uc + hsouth * fy * vc) * p.dt);
+        }
       }
       if (p.lin_drag > 0) {
-        if (hwest != 0) ru += div_rn(-p.lin_drag * uc * fbw, hwest, rhw);
-        if (hsouth != 0) rv += div_rn(-p.lin_drag * vc * fbs, hsouth, rhs);
+        if (hwest != 0) {
+          const double r = -p.lin_drag * uc * fbw;
+          ru += div_rn(r, hwest, rhw);
+          if constexpr (BUD) {
+            budget_add(p.bud_u, BU_RDRAG, k, L, p.lstride, cell, r * p.dt);
+            budget_add(p.bud_e, BE_RDRAG, k, L, p.lstride, cell, r * uc * p.dt);
+          }
+        }
+        if (hsouth != 0) {
+          const double r = -p.lin_drag * vc * fbs;
+          rv += div_rn(r, hsouth, rhs);
+          if constexpr (BUD) {
+            budget_add(p.bud_v, BU_RDRAG, k, L, p.lstride, cell, r * p.dt);
+            budget_add(p.bud_e, BE_RDRAG, k, L, p.lstride, cell, r * vc * p.dt);
+          }
+        }
       }
       // the surface drag is off under a rigid lid over land unless oceanSurfDrag
       auto surf_mask_u = [&]() {
@@ -699,11 +786,19 @@ tendency_kernel(const __grid_constant__ TendParams p) {
           double r = -p.lin_drag_surf * (uc - gload(p.uLid, p, gi, gj, MAP_N, MAP_S)) * fsw;
           if (surf_mask_u()) r = 0;
           ru += div_rn(r, hwest, rhw);
+          if constexpr (BUD) {
+            budget_add(p.bud_u, BU_RSURF, k, L, p.lstride, cell, r * p.dt);
+            budget_add(p.bud_e, BE_RSURF, k, L, p.lstride, cell, r * uc * p.dt);
+          }
         }
         if (hsouth != 0) {
           double r = -p.lin_drag_surf * (vc - gload(p.vLid, p, gi, gj, MAP_S, MAP_N)) * fss;
           if (surf_mask_v()) r = 0;
           rv += div_rn(r, hsouth, rhs);
+          if constexpr (BUD) {
+            budget_add(p.bud_v, BU_RSURF, k, L, p.lstride, cell, r * p.dt);
+            budget_add(p.bud_e, BE_RSURF, k, L, p.lstride, cell, r * vc * p.dt);
+          }
         }
       }
       // quadratic drag (forcing.c:95-143, 330-393): the speed at the cell centre from the
@@ -716,10 +811,18 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         if (hwest != 0) {
           const double ua = 0.5 * (uab(i, j) + uab(i - 1, j));
           ru -= div_rn(p.quad_drag * ua * uc * fbw, hwest, rhw);
+          if constexpr (BUD) {
+            budget_add(p.bud_u, BU_CDBOT, k, L, p.lstride, cell, -p.quad_drag * ua * uc * fbw * p.dt);
+            budget_add(p.bud_e, BE_CDBOT, k, L, p.lstride, cell, -p.quad_drag * ua * sq(uc) * fbw * p.dt);
+          }
         }
         if (hsouth != 0) {
           const double ua = 0.5 * (uab(i, j) + uab(i, j - 1));
           rv -= div_rn(p.quad_drag * ua * vc * fbs, hsouth, rhs);
+          if constexpr (BUD) {
+            budget_add(p.bud_v, BU_CDBOT, k, L, p.lstride, cell, -p.quad_drag * ua * vc * fbs * p.dt);
+            budget_add(p.bud_e, BE_CDBOT, k, L, p.lstride, cell, -p.quad_drag * ua * sq(vc) * fbs * p.dt);
+          }
         }
       }
       if (p.quad_drag_surf > 0 && k == 0) {
@@ -734,21 +837,43 @@ tendency_kernel(const __grid_constant__ TendParams p) {
           double r = -p.quad_drag_surf * ua * (wf * uc - gload(p.uLid, p, gi, gj, MAP_N, MAP_S)) * fsw;
           if (surf_mask_u()) r = 0;
           ru += div_rn(r, hwest, rhw);
+          if constexpr (BUD) {
+            budget_add(p.bud_u, BU_CDSURF, k, L, p.lstride, cell, r * p.dt);
+            budget_add(p.bud_e, BE_CDSURF, k, L, p.lstride, cell, r * uc * p.dt);
+          }
         }
         if (hsouth != 0) {
           const double ua = 0.5 * (uab(i, j) + uab(i, j - 1));
           double r = -p.quad_drag_surf * ua * (wf * vc - gload(p.vLid, p, gi, gj, MAP_S, MAP_N)) * fss;
           if (surf_mask_v()) r = 0;
           rv += div_rn(r, hsouth, rhs);
+          if constexpr (BUD) {
+            budget_add(p.bud_v, BU_CDSURF, k, L, p.lstride, cell, r * p.dt);
+            budget_add(p.bud_e, BE_CDSURF, k, L, p.lstride, cell, r * vc * p.dt);
+          }
         }
       }
     }
     // ---- Newtonian velocity restoring (restoring.c:172-220) ----
     if (p.use_relax) {
       double ut = gload(p.uTime + k * p.lstride, p, gi, gj, MAP_N, MAP_S);
-      if (ut > 0) ru += (-(uc - gload(p.uRelax + k * p.lstride, p, gi, gj, MAP_N, MAP_S))) / ut;
+      if (ut > 0) {
+        const double r = (-(uc - gload(p.uRelax + k * p.lstride, p, gi, gj, MAP_N, MAP_S))) / ut;
+        ru += r;
+        if constexpr (BUD) {
+          budget_add(p.bud_u, BU_RELAX, k, L, p.lstride, cell, hwest * r * p.dt);
+          budget_add(p.bud_e, BE_RELAX, k, L, p.lstride, cell, hwest * r * uc * p.dt);
+        }
+      }
       double vt = gload(p.vTime + k * p.lstride, p, gi, gj, MAP_S, MAP_N);
-      if (vt > 0) rv += (-(vc - gload(p.vRelax + k * p.lstride, p, gi, gj, MAP_S, MAP_N))) / vt;
+      if (vt > 0) {
+        const double r = (-(vc - gload(p.vRelax + k * p.lstride, p, gi, gj, MAP_S, MAP_N))) / vt;
+        rv += r;
+        if constexpr (BUD) {
+          budget_add(p.bud_v, BU_RELAX, k, L, p.lstride, cell, hsouth * r * p.dt);
+          budget_add(p.bud_e, BE_RELAX, k, L, p.lstride, cell, hsouth * r * vc * p.dt);
+        }
+      }
     }
     // the wall-normal tendency is zero on the wall face (field.c:173-176, 216-220)
     if (p.wall_ew && gi == 0) ru = 0.0;
@@ -766,6 +891,44 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         rel = -(0.0 - 0.0);
       }
       rh = adv + rel;
+      if constexpr (BUD) {
+        // work.c:1891-1906 and the second loop of work.c:1913-1937
+        const double hc0 = AT(sh, i, j);
+        const double ke2 = 0.5 * (sq(uc) + sq(vc));
+        const double w0 = p.use_wdia ? AT(WDall + k * RN, i, j) : 0.0;
+        const double w1 = p.use_wdia ? AT(WDall + (k + 1) * RN, i, j) : 0.0;
+        double eta1 = p.hhb[cell];   // eta_w[k+1] and eta_w[k], built upward as in work.c:1184-1199
+        for (int m = L - 1; m > k; --m) eta1 = eta1 + p.h[m * p.lstride + cell];
+        const double eta0 = eta1 + hc0;
+        const double g = p.geff[k], h0 = p.h0;
+        budget_add(p.bud_h, BH_ADV, k, L, p.lstride, cell, adv * p.dt);
+        budget_add(p.bud_h, BH_RELAX, k, L, p.lstride, cell, rel * p.dt);
+        budget_add(p.bud_e, BE_ADV, k, L, p.lstride, cell, ke2 * adv * p.dt);
+        budget_add(p.bud_e, BE_WDIAKE, k, L, p.lstride, cell, ke2 * rel * p.dt);
+        budget_add(p.bud_e, BE_WDIAPE, k, L, p.lstride, cell,
+                   -g * (eta0 * w0 - eta1 * w1) * p.dt
+                   - (-g * (h0 * h0 * h0 * h0) / (hc0 * hc0 * hc0) / 3) * (-rel) * p.dt);
+        if (p.b) {
+          const double bc = p.b[k * p.lstride + cell];
+          budget_add(p.bud_b, BB_ADV, k, L, p.lstride, cell, bc * adv * p.dt);
+          budget_add(p.bud_b, BB_WDIA, k, L, p.lstride, cell, bc * rel * p.dt);
+        }
+        if (p.bud_u || p.bud_v) {
+          const double adv_w = div_rn(AT(huu, i - 1, j) - AT(huu, i, j), dx, rdx)
+                             + div_rn(AT(hvv, i - 1, j) - AT(hvv, i - 1, j + 1), dy, rdy);
+          const double adv_s = div_rn(AT(huu, i, j - 1) - AT(huu, i + 1, j - 1), dx, rdx)
+                             + div_rn(AT(hvv, i, j - 1) - AT(hvv, i, j), dy, rdy);
+          double rel_w = -(0.0 - 0.0), rel_s = -(0.0 - 0.0);
+          if (p.use_wdia) {
+            rel_w = -(AT(WDall + k * RN, i - 1, j) - AT(WDall + (k + 1) * RN, i - 1, j));
+            rel_s = -(AT(WDall + k * RN, i, j - 1) - AT(WDall + (k + 1) * RN, i, j - 1));
+          }
+          budget_add(p.bud_u, BU_DHDT, k, L, p.lstride, cell, 0.5 * uc * (adv + adv_w) * p.dt);
+          budget_add(p.bud_u, BU_WDIA, k, L, p.lstride, cell, 0.5 * uc * (rel + rel_w) * p.dt);
+          budget_add(p.bud_v, BU_DHDT, k, L, p.lstride, cell, 0.5 * vc * (adv + adv_s) * p.dt);
+          budget_add(p.bud_v, BU_WDIA, k, L, p.lstride, cell, 0.5 * vc * (rel + rel_s) * p.dt);
+        }
+      }
     }
     // ---- Adams-Bashforth epilogue (integrator.c:15-69) ----
     const size_t o = k * p.lstride + cell;
@@ -855,11 +1018,19 @@ inline bool wide_halo(const TendParams& p, int ts) { return ts >= 2 || (p.use_sm
 #define PAWSIM_TEND_CAT2(a, b) a##b
 #define PAWSIM_TEND_CAT(a, b) PAWSIM_TEND_CAT2(a, b)
 
-size_t PAWSIM_TEND_CAT(tendency_smem_ty, PAWSIM_TEND_TY)(const TendParams& p, int ts) {
+#if PAWSIM_TEND_BUD
+#define PAWSIM_TEND_SMEM_FN tendency_smem_budget
+#define PAWSIM_TEND_LAUNCH_FN launch_tendency_budget_tile
+#else
+#define PAWSIM_TEND_SMEM_FN PAWSIM_TEND_CAT(tendency_smem_ty, PAWSIM_TEND_TY)
+#define PAWSIM_TEND_LAUNCH_FN PAWSIM_TEND_CAT(launch_tendency_ty, PAWSIM_TEND_TY)
+#endif
+
+size_t PAWSIM_TEND_SMEM_FN(const TendParams& p, int ts) {
   return wide_halo(p, ts) ? smem_bytes<3>(p) : smem_bytes<2>(p);
 }
 
-int PAWSIM_TEND_CAT(launch_tendency_ty, PAWSIM_TEND_TY)(const TendParams& p, int ms, int ts, cudaStream_t s) {
+int PAWSIM_TEND_LAUNCH_FN(const TendParams& p, int ms, int ts, cudaStream_t s) {
   if (p.L < 1 || p.L > LMAX) return -1;
   if (!wide_halo(p, ts)) {
     if (ts == 0) return launch_ms<0, 2>(p, ms, s);

@@ -209,27 +209,38 @@ __global__ void __launch_bounds__(TNT) tracer_tile_kernel(const TracerParams p) 
             + div_rn(bc * (div_rn(HUU[q + 1] - HUU[q], dx, p.rdx) + div_rn(HVV[q + TRW] - HVV[q], dy, p.rdy)), h, rh);
   }
   rhs_b += rhs_adv;
+  double rhs_wdia = 0, rhs_K2 = 0, rhs_K4 = 0, rhs_relax = 0;
   if (p.use_wdia && h != 0) {
     const double w0 = p.wdia[lk + cell], w1 = p.wdia[lk + p.lstride + cell];
     const double b_p = (k == 0) ? 0 : p.b[lk - p.lstride + cell];
     const double b_m = (k == p.L - 1) ? 0 : p.b[lk + p.lstride + cell];
     const double db_p = (w0 > 0) ? 0 : b_p - bc;
     const double db_m = (w1 > 0) ? bc - b_m : 0;
-    const double rhs_wdia = -(w0 * db_p + w1 * db_m);
+    rhs_wdia = -(w0 * db_p + w1 * db_m);
     rhs_b += div_rn(rhs_wdia, h, rh);
   }
   if (p.K2 > 0 && h != 0) {
-    const double rhs_K2 = p.K2 * lap(SB, q);
+    rhs_K2 = p.K2 * lap(SB, q);
     rhs_b += div_rn(rhs_K2, h, rh);
   }
   if (p.K4 > 0 && h != 0) {
-    const double rhs_K4 = -p.K4 * lap(S[T_BB4], q);
+    rhs_K4 = -p.K4 * lap(S[T_BB4], q);
     rhs_b += div_rn(rhs_K4, h, rh);
   }
   const double bt = p.bTime[lk + cell];
   if (bt > 0) {
-    const double rhs_relax = -(bc - p.bRelax[lk + cell]) / bt;
+    rhs_relax = -(bc - p.bRelax[lk + cell]) / bt;
     rhs_b += rhs_relax;
+  }
+  if (p.bud_b) {
+    // work.c:2131-2136 (the diapycnal diffusion term is zero: it is not built)
+    double* f = p.bud_b + lk + cell;
+    const size_t P = (size_t)p.L * p.lstride;   // one term's planes
+    f[0] = f[0] + h * rhs_adv * p.dt;
+    f[P] = f[P] + rhs_wdia * p.dt;
+    f[2 * P] = f[2 * P] + rhs_K2 * p.dt;
+    f[3 * P] = f[3 * P] + rhs_K4 * p.dt;
+    f[5 * P] = f[5 * P] + h * rhs_relax * p.dt;
   }
   const size_t o = lk + cell;
   if (p.ab_mode == 0) {

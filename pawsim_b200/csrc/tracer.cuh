@@ -29,6 +29,9 @@ struct TracerParams {
   int write_hist;
   const double *f1b, *f2b;
   double *fb_out, *b_out;
+  // Tracer_* budget (work.c:2131-2136): [term][layer] planes lstride apart, or nullptr
+  double* bud_b;
+  double dt;
 };
 
 void launch_tracer(const TracerParams& p, cudaStream_t s);

@@ -47,7 +47,8 @@ typedef struct
   int useTrad, use_MG, use_fullMG, pressureTiming, writeInitDiagnostics, restart, useWallEW,
       useWallNS, useRL, oceanSurfDrag, windFeedback, useTracer, useBuoyancy, useRandomForcing;
   /* reals (strtod) */
-  double Lx, Ly, dt, tmin, tmax, savefrequency, savefreqAvg, savefreqEZ, KT00_sigma, h0, hsml, hmin_surf, hbbl, hmin_bot,
+  double Lx, Ly, dt, tmin, tmax, savefrequency, savefreqAvg, savefreqEZ, savefreqUMom, savefreqVMom,
+      savefreqThic, savefreqEnergy, savefreqTracer, KT00_sigma, h0, hsml, hmin_surf, hbbl, hmin_bot,
       A2, A4, A2smag, A4smag, K2, K4, linDragCoeff, quadDragCoeff, linDragSurf, quadDragSurf,
       tauPeriod, wDiaPeriod, convDiff, omega_MG, tol, SOR_rp;
   /* derived */
@@ -109,7 +110,8 @@ static const keydef KEYS[] = {
     B(useTrad), B(use_MG), B(use_fullMG), B(pressureTiming), B(writeInitDiagnostics), B(restart),
     B(useWallEW), B(useWallNS), B(useRL), B(oceanSurfDrag), B(windFeedback), B(useTracer),
     B(useBuoyancy), B(useRandomForcing), R(Lx), R(Ly), R(dt), R(tmin), R(tmax), R(savefrequency), R(savefreqAvg),
-    R(savefreqEZ), R(KT00_sigma), R(h0), R(hsml), R(hmin_surf), R(hbbl), R(hmin_bot), R(A2), R(A4), R(A2smag),
+    R(savefreqEZ), R(savefreqUMom), R(savefreqVMom), R(savefreqThic), R(savefreqEnergy), R(savefreqTracer),
+    R(KT00_sigma), R(h0), R(hsml), R(hmin_surf), R(hbbl), R(hmin_bot), R(A2), R(A4), R(A2smag),
     R(A4smag), R(K2), R(K4), R(linDragCoeff), R(quadDragCoeff), R(linDragSurf), R(quadDragSurf),
     R(tauPeriod), R(wDiaPeriod), R(convDiff), R(omega_MG), R(tol), {NULL, K_REAL, 0}};
 #undef U
@@ -720,6 +722,42 @@ static int write_ez (pawsim_gpu * m, const config * c, const char * outdir, doub
   return 1;
 }
 
+/* budget families (config bit f) and their output names (diagnostics.c:758-796) */
+static const char * const BUDGET_NAMES[5][16] = {
+  {"UMom_PVadvection","UMom_Montgomery","UMom_KEgradient","UMom_dhdt","UMom_viscosity","UMom_hypervisc",
+   "UMom_linBotDrag","UMom_linSurfDrag","UMom_quadBotDrag","UMom_quadSurfDrag","UMom_windStress",
+   "UMom_buoyForce","UMom_relaxation","UMom_diapycnal","UMom_baroForcing","UMom_diaVisc"},
+  {"VMom_PVadvection","VMom_Montgomery","VMom_KEgradient","VMom_dhdt","VMom_viscosity","VMom_hypervisc",
+   "VMom_linBotDrag","VMom_linSurfDrag","VMom_quadBotDrag","VMom_quadSurfDrag","VMom_windStress",
+   "VMom_buoyForce","VMom_relaxation","VMom_diapycnal","VMom_baroForcing","VMom_diaVisc"},
+  {"Thic_advection","Thic_relaxation"},
+  {"Energy_advection","Energy_Montgomery","Energy_windStress","Energy_linBotDrag","Energy_linSurfDrag",
+   "Energy_quadBotDrag","Energy_quadSurfDrag","Energy_viscosity","Energy_hypervisc","Energy_diaProd",
+   "Energy_diaAdv","Energy_baroForcing","Energy_buoyForce","Energy_relaxation","Energy_diaVisc"},
+  {"Tracer_advection","Tracer_diaAdv","Tracer_isoDiff","Tracer_hyperdiff","Tracer_diaDiff","Tracer_relaxation"}};
+static const unsigned BUDGET_TERMS[5] = {16,16,2,15,6};
+
+/* one family's window (diagnostics.c:798-864): sums / ((n - n_prev) dt), written, reset */
+static int write_budget (pawsim_gpu * m, const config * c, const char * outdir, int f, unsigned n,
+                         unsigned n_prev, unsigned n_out, double * plane)
+{
+  const size_t N = (size_t) c->Nx * c->Ny;
+  char name[NAMELEN];
+  unsigned t, k;
+  double len = (n - n_prev) * c->dt;
+  if (!gpu_ok(pawsim_gpu_scale_budgets(m,1 << f,1 / len),"budgets")) return 0;
+  for (t = 0; t < BUDGET_TERMS[f]; t ++)
+  {
+    for (k = 0; k < c->Nlay; k ++)
+    {
+      snprintf(name,sizeof(name),"%s%u_n=%u.dat",BUDGET_NAMES[f][t],k,n_out);
+      if (!gpu_ok(pawsim_gpu_get_field(m,BUDGET_NAMES[f][t],(int) k,plane,N),"budgets")
+       || !write_f64(outdir,name,plane,N)) return 0;
+    }
+  }
+  return gpu_ok(pawsim_gpu_zero_budgets(m,1 << f),"budgets");
+}
+
 static const char * solver_name (unsigned s)
 {
   return s == 0 ? "SOR" : (s == 1 ? "MG_GATHERED" : (s == 2 ? "MG_DISTRIBUTED" : "UNKNOWN"));
@@ -735,6 +773,10 @@ int main (int argc, char ** argv)
   double * plane = NULL;
   unsigned n, n_saves, solves = 0, fallbacks = 0, n_avg = 0, n_EZ = 0;
   double t_next_avg = 0, t_next_EZ = 0;
+  double bfreq[5];
+  unsigned b_out[5] = {0,0,0,0,0}, b_prev[5] = {0,0,0,0,0};
+  double b_next[5] = {0,0,0,0,0};
+  int f;
   double wall_total = 0, iters_total = 0;
   const char * slash;
   int rc = 1;
@@ -798,6 +840,8 @@ int main (int argc, char ** argv)
   g.use_tracer = c.useTracer;
   g.tracer_scheme = (int) c.tracerScheme;
   g.K2 = c.K2; g.K4 = c.K4;
+  g.budgets = (c.savefreqUMom > 0 ? 1 : 0) | (c.savefreqVMom > 0 ? 2 : 0) | (c.savefreqThic > 0 ? 4 : 0)
+            | (c.savefreqEnergy > 0 ? 8 : 0) | (c.savefreqTracer > 0 ? 16 : 0);
   if (c.useTracer && (c.useBuoyancy || file_of(&c,"diaDiffFile")[0] || file_of(&c,"bFluxFile")[0]))
   {
     fprintf(stderr,"ERROR: the tracer's buoyancy coupling and diapycnal diffusion are not built on the GPU\n");
@@ -821,6 +865,16 @@ int main (int argc, char ** argv)
   {
     n_EZ = (unsigned) round(c.tmin / c.savefreqEZ) + 1;
     t_next_EZ = c.tmin + c.savefreqEZ;
+  }
+  bfreq[0] = c.savefreqUMom; bfreq[1] = c.savefreqVMom; bfreq[2] = c.savefreqThic;
+  bfreq[3] = c.savefreqEnergy; bfreq[4] = c.useTracer ? c.savefreqTracer : 0;
+  for (f = 0; f < 5; f ++)
+  {
+    if (bfreq[f] > 0)
+    {
+      b_out[f] = (unsigned) round(c.tmin / bfreq[f]) + 1;
+      b_next[f] = c.tmin + bfreq[f];
+    }
   }
   /* preliminary rigid-lid correction, then the n = 0 (or pickup) state (pawsim.c:278-312) */
   memset(&st,0,sizeof(st));
@@ -910,6 +964,21 @@ int main (int argc, char ** argv)
     {
       fprintf(stderr,"ERROR: PAWSIM diagnostic averaging failed at n=%u\n",n);
       goto done;
+    }
+    /* budget windows, each family on its own clock (diagnostics.c:756-866) */
+    for (f = 0; f < 5; f ++)
+    {
+      if (bfreq[f] > 0 && t >= b_next[f])
+      {
+        if (!write_budget(m,&c,outdir,f,n,b_prev[f],b_out[f],plane))
+        {
+          fprintf(stderr,"ERROR: PAWSIM diagnostic averaging failed at n=%u\n",n);
+          goto done;
+        }
+        b_prev[f] = n;
+        b_out[f] ++;
+        b_next[f] = b_out[f] * bfreq[f];
+      }
     }
   }
   if (c.pressureTiming && solves > 0)

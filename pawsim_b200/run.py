@@ -2,7 +2,7 @@
 
     python -m pawsim_b200.run --setup gyre --N 1024 --steps 4 [--integrator-only]
                               [--solver 0|1] [--mg-fp32] [--mg-tile K] [--mg-omega W]
-                              [--mg-pre P] [--mg-post Q] [--dt 60] [--param FILE]
+                              [--mg-pre P] [--mg-post Q] [--pi-guess G] [--dt 60] [--param FILE]
                               [--ws-collect S --ws-epochs E] [--tracer SCHEME]
                               [--averages] [--energy]
 
@@ -38,6 +38,7 @@ def main(argv=None):
     ap.add_argument("--dt", type=float, default=None)
     ap.add_argument("--solver", type=int, default=1)
     ap.add_argument("--mg-fp32", action="store_true")
+    ap.add_argument("--pi-guess", type=int, default=0, help="1: extrapolated first guess of the solves")
     ap.add_argument("--mg-tile", type=int, default=0, help="0 autotune, 1..4 force a tile shape, 5 strips")
     ap.add_argument("--mg-omega", type=float, default=-1.0, help="red-black weight; negative: chosen by the solver")
     ap.add_argument("--mg-pre", type=int, default=1)
@@ -67,7 +68,7 @@ def main(argv=None):
                 inputs.add_tracer(p, scheme=a.tracer, relax_days=100.0, K2=100.0)
             cfg = inputs.read_config(p)
         m = Model(cfg, mg_fp32=int(a.mg_fp32), mg_tile=a.mg_tile, mg_omega=a.mg_omega, mg_pre=a.mg_pre,
-                  mg_post=a.mg_post)
+                  mg_post=a.mg_post, pi_guess=a.pi_guess)
         t0 = time.perf_counter()
         def diagnostics():
             if a.averages:

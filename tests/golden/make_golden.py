@@ -76,6 +76,20 @@ EZ_CASES = {
                                                 extra=dict(useRL=0, thicknessScheme=1,
                                                            savefreqAvg=750.0)), 1.0),
 }
+# tendency-budget cases (savefreqUMom/VMom/Thic/Energy/Tracer, work.c:1753-1937 and the
+# forcing, restoring, diapycnal and pressure terms; diagnostics.c:756-866): windows of 2 steps
+# (Tracer: 3), SOR pressure so the states are bit-identical
+BUD_NSTEPS = 6
+BUD_PREFIXES = ["UMom_", "VMom_", "Thic_", "Energy_", "Tracer_"]
+BUD_CASES = {
+    "gyre_sor_budget": (inputs.gyre, dict(N=16, Ny=12, dt=900.0, solver=0, tol=1e-10), None),
+    "full_sor_budget": (inputs.full_physics, dict(N=16, dt=50.0, solver=0, Ly=320e3, bathy_len=20e3,
+                                                  sponge=40e3), None),
+    "gyre_hk83_a4_budget": (inputs.gyre, dict(N=20, Ny=12, dt=600.0, solver=0, A2=0.0, A4=1e9,
+                                              extra=dict(momentumScheme=1, thicknessScheme=1)), None),
+    "jets_tracer_budget": (inputs.jets, dict(N=16, dt=100.0, solver=0, tol=1e-10),
+                           dict(scheme=2, relax_days=100.0, K2=100.0)),
+}
 LINE = re.compile(r"iters=(\d+) walltime=\S+ s residual_max=(\S+) residual_rms=(\S+) "
                   r"div_max=(\S+) div_rms=(\S+)")
 
@@ -187,6 +201,33 @@ def make_ez(name, fn, kw, every, outdir):
         np.savez_compressed(os.path.join(outdir, name + ".npz"), **rec)
 
 
+def make_budget(name, fn, kw, tkw, outdir):
+    """Inputs and the reference's budget files of every completed window."""
+    with tempfile.TemporaryDirectory() as d:
+        kw = dict(kw)
+        extra = dict(kw.pop("extra", {}) or {})
+        dt = kw["dt"]
+        extra.update(savefreqUMom=2 * dt, savefreqVMom=2 * dt, savefreqThic=2 * dt, savefreqEnergy=2 * dt)
+        if tkw is not None:
+            extra.update(savefreqTracer=3 * dt)
+        p = fn(os.path.join(d, "in"), Nt=BUD_NSTEPS, savefrequency=BUD_NSTEPS * dt, extra=extra, **kw)
+        if tkw is not None:
+            inputs.add_tracer(p, **tkw)
+        cfg = inputs.read_config(p)
+        out = os.path.join(d, "out")
+        os.makedirs(out)
+        subprocess.run([oracle.reference_exe(), p, out], capture_output=True, text=True, check=True)
+        rec = {"param_text": np.array(open(p).read())}
+        for f in sorted(os.listdir(os.path.dirname(p))):
+            if f.endswith(".dat") and f != "params.dat":
+                rec["in_" + f] = np.fromfile(os.path.join(os.path.dirname(p), f), dtype="<f8")
+        names = sorted(f for f in os.listdir(out) if any(f.startswith(x) for x in BUD_PREFIXES))
+        rec["budget_files"] = np.array(names)
+        for f in names:
+            rec["b_" + f[:-4]] = inputs.read_data(os.path.join(out, f), (cfg.Ny, cfg.Nx))
+        np.savez_compressed(os.path.join(outdir, name + ".npz"), **rec)
+
+
 if __name__ == "__main__":
     # python tests/golden/make_golden.py [case ...]   (all cases when none are named)
     oracle.build(ref=True)
@@ -209,4 +250,9 @@ if __name__ == "__main__":
         if len(sys.argv) > 1 and name not in sys.argv[1:]:
             continue
         make_ez(name, fn, kw, every, HERE)
+        print("wrote", name)
+    for name, (fn, kw, tkw) in BUD_CASES.items():
+        if len(sys.argv) > 1 and name not in sys.argv[1:]:
+            continue
+        make_budget(name, fn, kw, tkw, HERE)
         print("wrote", name)
