@@ -193,6 +193,37 @@ def tracer_timing(cfg, stream, reps):
     return out[1] - out[0]
 
 
+def budget_timing(stream, reps):
+    """Device time per step of the budget build of the tendency kernel with the u, v,
+    thickness and energy budgets on (savefreqUMom/VMom/Thic/Energy), against the plain
+    kernel: integrator steps of the same set-up with and without budgets, the difference."""
+    import tempfile as _tf
+    import pawsim_b200
+    import torch
+    out = []
+    with _tf.TemporaryDirectory() as d:
+        for bud in (False, True):
+            extra = dict(savefreqUMom=3600.0, savefreqVMom=3600.0, savefreqThic=3600.0,
+                         savefreqEnergy=3600.0) if bud else None
+            p = pawsim_b200.inputs.gyre(d + f"/b{int(bud)}", N=N_GRID, solver=1, dt=DT, extra=extra)
+            m = pawsim_b200.Model(pawsim_b200.inputs.read_config(p))
+            m.set_stream(stream.cuda_stream)
+            with torch.cuda.stream(stream):
+                m.prelim()
+                for n in range(1, 4):
+                    m.integrator_step(n)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record(stream)
+                for n in range(4, 4 + reps):
+                    m.integrator_step(n)
+                e1.record(stream)
+                torch.cuda.synchronize()
+            out.append(e0.elapsed_time(e1) / reps)
+            m.close()
+    return out
+
+
 def pressure_comparison(cfg, fields, stream, spin, steps, epochs, pairs):
     """Pressure ms/step and V-cycles/step of the plain FP64 multigrid (started from the
     previous pressure, as the reference's solver is) against FP32 V-cycles in FP64 defect
@@ -436,6 +467,14 @@ def main():
     line["energy"] = {"kernel": "ez_partial_kernel + ez_final_kernel", "ms_per_call": ez_ms,
                       "algorithmic_bytes": ez_bytes, "achieved_gbs": ez_bytes / (ez_ms / 1e3) / 1e9,
                       "frac": ez_bytes / (ez_ms / 1e3) / 1e9 / peak}
+    bt = budget_timing(stream, min(args.steps, 20))
+    # budget sums read and written once per step: 16 + 16 + 2 + 15 terms per layer; the kernel
+    # itself as in the roofline line
+    bud_bytes = ncell * L * 16 * (16 + 16 + 2 + 15)
+    line["budgets"] = {"kernel": "tendency_kernel budget build (32 x 8 tiles)", "families": "UMom VMom Thic Energy",
+                       "ms_per_step": bt[1], "plain_ms_per_step": bt[0], "extra_ms": bt[1] - bt[0],
+                       "budget_bytes": bud_bytes,
+                       "budget_gbs": bud_bytes / ((bt[1] - bt[0]) / 1e3) / 1e9 if bt[1] > bt[0] else None}
     if tr is not None:
         tr_bytes = ncell * L * 88   # read u, v, h, b, bRelax, bTime, f1, f2, w_dia; write b, f
         line["tracer"] = {"kernel": "tracer_tile_kernel (KT00, K2, relaxation)", "ms_per_step": tr,

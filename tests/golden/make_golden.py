@@ -89,6 +89,12 @@ BUD_CASES = {
                                               extra=dict(momentumScheme=1, thicknessScheme=1)), None),
     "jets_tracer_budget": (inputs.jets, dict(N=16, dt=100.0, solver=0, tol=1e-10),
                            dict(scheme=2, relax_days=100.0, K2=100.0)),
+    "gyre_quad_budget": (inputs.gyre, dict(N=20, Ny=12, dt=600.0, solver=0,
+                                           extra=dict(quadDragCoeff=2e-3, quadDragSurf=1e-3, windFeedback=1,
+                                                      oceanSurfDrag=0)), None),
+    "gyre_fractions_budget": (inputs.gyre, dict(N=20, Ny=12, dt=600.0, solver=0,
+                                                extra=dict(hsml=1500.0, hmin_surf=5.0, hbbl=500.0, hmin_bot=10.0,
+                                                           linDragSurf=1e-4, thicknessScheme=3)), None),
 }
 LINE = re.compile(r"iters=(\d+) walltime=\S+ s residual_max=(\S+) residual_rms=(\S+) "
                   r"div_max=(\S+) div_rms=(\S+)")

@@ -9,7 +9,8 @@ writes each window under the reference's names. On the committed fixtures (windo
 steps, three for the tracer; SOR pressure, so the states are bit-identical) every budget
 file must equal the reference binary's bit for bit: walled gyre with wind and drag, the
 four-layer full-physics set-up (bathymetry, sponge restoring, w_dia, A4), HK83 momentum and
-thickness with A4, and a periodic jet with a KT00 tracer."""
+thickness with A4, a periodic jet with a KT00 tracer, quadratic bottom and surface drag with
+wind feedback, and surface/bottom layer fractions with linear surface drag and KT00 thickness."""
 import os
 import subprocess
 
@@ -22,7 +23,8 @@ from golden_util import load_case
 pytestmark = pytest.mark.gpu
 
 DRIVER = os.path.join(ROOT, "pawsim_b200", "bin", "PAWSIM_B200.exe")
-CASES = ["gyre_sor_budget", "full_sor_budget", "gyre_hk83_a4_budget", "jets_tracer_budget"]
+CASES = ["gyre_sor_budget", "full_sor_budget", "gyre_hk83_a4_budget", "jets_tracer_budget", "gyre_quad_budget",
+         "gyre_fractions_budget"]
 
 
 @pytest.mark.parametrize("name", CASES)
