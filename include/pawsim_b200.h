@@ -85,9 +85,9 @@ typedef struct pawsim_gpu_config
    * (32x8, 32x16, 64x8, 64x16 cells), 5 the streamed strips (levels of at least 64 x 48
    * cells). The shape changes only the speed, never the result. */
   int mg_tile;
-  /* passive tracer b (work.c:1947-2144): useTracer, tracerScheme (0 AL81, 1 UP3, 2 KT00) and
-   * the Laplacian / biharmonic diffusivities K2, K4. The buoyancy coupling (useBuoyancy) and
-   * diapycnal diffusion (diaDiffFile, bFluxFile) are not built. */
+  /* tracer b (work.c:1947-2144): useTracer, tracerScheme (0 AL81, 1 UP3, 2 KT00) and the
+   * Laplacian / biharmonic diffusivities K2, K4 (the buoyancy coupling is use_buoyancy
+   * below). Diapycnal diffusion (diaDiffFile, bFluxFile) is not built. */
   int use_tracer, tracer_scheme;
   double K2, K4;
   /* First guess of the multigrid solves (pressureSolver 1 and 2): 0 the previous pressure,
@@ -101,6 +101,10 @@ typedef struct pawsim_gpu_config
    * every term times dt to its running sum; the sums are read with pawsim_gpu_get_field under
    * the reference's output names (UMom_PVadvection, ..., Tracer_relaxation; k = layer). */
   int budgets;
+  /* useBuoyancy: the tracer acts as a buoyancy anomaly in the Bernoulli pressure, the
+   * momentum (-hz db/dx), the tracer's diapycnal advection and the local reduced gravity of
+   * the convective viscosity (convDiff); needs use_tracer. */
+  int use_buoyancy;
 } pawsim_gpu_config;
 
 enum

@@ -48,7 +48,8 @@ class GpuConfig(ctypes.Structure):
                         ("serial_sums", ctypes.c_int), ("mg_tile", ctypes.c_int),
                         ("use_tracer", ctypes.c_int), ("tracer_scheme", ctypes.c_int),
                         ("K2", ctypes.c_double), ("K4", ctypes.c_double),
-                        ("pi_guess", ctypes.c_int), ("budgets", ctypes.c_int)]
+                        ("pi_guess", ctypes.c_int), ("budgets", ctypes.c_int),
+                        ("use_buoyancy", ctypes.c_int)]
 
 
 class GpuStats(ctypes.Structure):
@@ -185,6 +186,7 @@ def gpu_config(cfg: inputs.Config, **over) -> GpuConfig:
     g.mg_tile = 0
     g.use_tracer, g.tracer_scheme = int(v["useTracer"]), int(v["tracerScheme"])
     g.K2, g.K4 = float(v["K2"]), float(v["K4"])
+    g.use_buoyancy = int(bool(v["useBuoyancy"]) and bool(v["useTracer"]))
     # budget families of the savefreq keys (work.c:310-319)
     g.budgets = sum(bit for bit, key in ((1, "savefreqUMom"), (2, "savefreqVMom"), (4, "savefreqThic"),
                                          (8, "savefreqEnergy"), (16, "savefreqTracer")) if v[key] > 0)
@@ -197,9 +199,8 @@ class Model:
     """One model resident on the GPU (the drop-in for the reference's hot path)."""
 
     def __init__(self, cfg: inputs.Config, fields: dict | None = None, **options):
-        if cfg.values["useTracer"] and (cfg.values["useBuoyancy"] or cfg.files.get("diaDiffFile")
-                                        or cfg.files.get("bFluxFile")):
-            raise PawsimError(-5, "the tracer's buoyancy coupling and diapycnal diffusion are not built")
+        if cfg.values["useTracer"] and (cfg.files.get("diaDiffFile") or cfg.files.get("bFluxFile")):
+            raise PawsimError(-5, "the tracer's diapycnal diffusion is not built")
         self.lib = load_library()
         self.cfg = cfg
         self.L, self.Nx, self.Ny = cfg.values["Nlay"], cfg.values["Nx"], cfg.values["Ny"]

@@ -183,6 +183,7 @@ static int create(const pawsim_gpu_config* cfg, Model** out) {
   if (c.Nlay < 1 || c.Nlay > LMAX) return fail(PAWSIM_GPU_EBADCONFIG, "Nlay must be in 1..8");
   if (c.pi_guess < 0 || c.pi_guess > 1) return fail(PAWSIM_GPU_EBADCONFIG, "pi_guess must be 0 or 1");
   if (c.budgets < 0 || c.budgets > 31) return fail(PAWSIM_GPU_EBADCONFIG, "budgets is a mask of five families");
+  if (c.use_buoyancy && !c.use_tracer) return fail(PAWSIM_GPU_EBADCONFIG, "useBuoyancy requires useTracer");
   if (c.Nx < 4 || c.Ny < 4) return fail(PAWSIM_GPU_EBADCONFIG, "Nx and Ny must be at least 4");
   if (c.Ly <= 0 || c.Lx <= 0 || c.dt <= 0) return fail(PAWSIM_GPU_EBADCONFIG, "Lx, Ly and dt must be positive");
   if (c.ts_scheme < 3 || c.ts_scheme > 5)
@@ -531,7 +532,17 @@ static TendParams base_params(Model* m) {
   p.uRelax = m->uRelax; p.vRelax = m->vRelax; p.uTime = m->uTime; p.vTime = m->vTime;
   p.nu_u = m->nu_u; p.nu_v = m->nu_v;
   p.wdia_out = m->wdia;
+  p.use_buoy = c.use_buoyancy;
+  p.b = c.use_tracer ? m->b[m->cur] : nullptr;
+  p.conv_diff = c.conv_diff;
   return p;
+}
+
+// the plain fused kernel, or its budget build when budgets accumulate or buoyancy couples
+static int launch_step_kernel(const Model* m, const TendParams& p) {
+  const bool ext = p.use_buoy || p.bud_u || p.bud_v || p.bud_h || p.bud_e || p.bud_b;
+  return ext ? launch_tendency_budget(p, m->c.mom_scheme, m->c.thick_scheme, m->s)
+             : launch_tendency(p, m->c.mom_scheme, m->c.thick_scheme, m->s);
 }
 
 static int tendency_eval(Model* m) {
@@ -539,7 +550,7 @@ static int tendency_eval(Model* m) {
   TendParams p = base_params(m);
   p.ab_mode = 0;
   p.fu_out = m->dtu; p.fv_out = m->dtv; p.fh_out = m->dth;
-  if (launch_tendency(p, m->c.mom_scheme, m->c.thick_scheme, m->s) != 0)
+  if (launch_step_kernel(m, p) != 0)
     return fail(PAWSIM_GPU_EUNSUPPORTED, "scheme combination not available");
   ++g_launches;
   PAWSIM_CUDA_OK(cudaGetLastError());
@@ -572,10 +583,8 @@ static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
   if (budgets) {
     p.dt = dt;
     p.bud_u = m->bud[0]; p.bud_v = m->bud[1]; p.bud_h = m->bud[2]; p.bud_e = m->bud[3]; p.bud_b = m->bud[4];
-    p.b = c.use_tracer ? m->b[m->cur] : nullptr;
   }
-  if ((budgets ? launch_tendency_budget(p, c.mom_scheme, c.thick_scheme, m->s)
-               : launch_tendency(p, c.mom_scheme, c.thick_scheme, m->s)) != 0)
+  if (launch_step_kernel(m, p) != 0)
     return fail(PAWSIM_GPU_EUNSUPPORTED, "scheme combination not available");
   ++g_launches;
   if (c.use_tracer) {
@@ -594,6 +603,8 @@ static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
     tp.ab_mode = p.ab_mode; tp.c0 = p.c0; tp.c1 = p.c1; tp.c2 = p.c2; tp.write_hist = p.write_hist;
     tp.f1b = m->fb[m->h1]; tp.f2b = m->fb[h2]; tp.fb_out = m->fb[h2]; tp.b_out = m->b[nb];
     tp.bud_b = m->bud[4]; tp.dt = dt;
+    tp.use_buoy = c.use_buoyancy;
+    for (int k = 0; k < m->L; ++k) tp.gg[k] = m->gg[k];
     launch_tracer(tp, m->s);
     ++g_launches;
   }
@@ -836,6 +847,7 @@ int pawsim_gpu_accumulate_averages(pawsim_gpu* h, double avg_fac) {
   a.au = b; a.av = b + Ls; a.ah = b + 2 * Ls; a.aM = b + 3 * Ls; a.ahu = b + 4 * Ls; a.ahv = b + 5 * Ls;
   a.ahuu = b + 6 * Ls; a.ahvv = b + 7 * Ls; a.ahuv = b + 8 * Ls; a.aW = b + 9 * Ls; a.api = a.aW + Ls + ls;
   a.b = m->b[0] ? m->b[m->cur] : nullptr;
+  a.use_buoy = m->c.use_buoyancy;
   a.ab = m->b[0] ? a.api + ls : nullptr;
   launch_accumulate_averages(m->grid2(), a, m->s);
   ++g_launches;
@@ -907,6 +919,7 @@ int pawsim_gpu_energy(pawsim_gpu* h, int eta_from_step_start, double* KE, double
   e.u = m->u[m->cur]; e.v = m->v[m->cur]; e.h = m->h[m->cur];
   e.hw = eta_from_step_start ? m->h[1 - m->cur] : m->h[m->cur];
   e.hhb = m->hhb; e.omz = m->omz; e.qpitch = m->qpitch;
+  e.b = m->c.use_buoyancy ? m->b[m->cur] : nullptr;
   g_launches += launch_energy(g, e, serial, m->ez, m->ez_out, m->s);
   PAWSIM_CUDA_OK(cudaGetLastError());
   double out[AVG_LMAX + 2];

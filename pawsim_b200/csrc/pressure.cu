@@ -490,6 +490,13 @@ __global__ void accumulate_averages_kernel(const Grid2 g, const AvgParams a) {
                    shuu = ahuu[o], shvv = ahvv[o], shuv = ahuv[o], wd = wdia[o];
       if (k == 0) pp = a.use_rl ? 0 : a.gg[0] * eta[0];
       else pp = pp + a.gg[k] * eta[k];
+      if (a.use_buoy) {
+        if (k == 0) {
+          if (!a.use_rl) pp -= a.b[c] * eta[0];
+        } else {
+          pp += eta[k] * (a.b[(k - 1) * g.lstride + c] - a.b[k * g.lstride + c]);
+        }
+      }
       double mm = pp;
       if (a.h0 != 0) {
         const double h0 = a.h0, hc = hk[k];
@@ -622,8 +629,14 @@ __device__ inline double ez_geff(const EzParams& e, int k) {
   return x;
 }
 
-__device__ inline EzCell ez_cell_any(const Grid2& g, const EzParams& e, int k, int i, int j, double eta) {
+// g_tot of layer k at one cell
+__device__ inline double ez_gtot(const Grid2& g, const EzParams& e, int k, size_t c) {
   const double gt = ez_geff(e, k);
+  return e.b ? gt - e.b[k * g.lstride + c] : gt;
+}
+
+__device__ inline EzCell ez_cell_any(const Grid2& g, const EzParams& e, int k, int i, int j, double eta) {
+  const double gt = ez_gtot(g, e, k, (size_t)j * g.pitch + i);
   return g.thick_scheme == 1 ? ez_cell<true, false>(g, e, k, i, j, eta, gt)
                              : ez_cell<false, false>(g, e, k, i, j, eta, gt);
 }
@@ -721,7 +734,7 @@ __global__ void __launch_bounds__(EZ_BX * EZ_BY, HK ? 2 : 4) ez_partial_kernel(c
     double z = 0;
     if (in) {
       eta = eta + e.hw[k * g.lstride + c];
-      const double gt = ez_geff(e, k);
+      const double gt = ez_gtot(g, e, k, c);
       const EzCell r = plain ? ez_cell<HK, true>(g, e, k, i, j, eta, gt) : ez_cell<HK, false>(g, e, k, i, j, eta, gt);
       ke += r.ke;
       pe += r.pe1;

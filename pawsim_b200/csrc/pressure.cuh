@@ -71,6 +71,7 @@ struct AvgParams {
   double *au, *av, *ah, *aM, *aW, *ahu, *ahv, *ahuu, *ahvv, *ahuv, *api;
   const double* b;   // tracer (nullable) and its sums
   double* ab;
+  int use_buoy;      // the tracer as buoyancy in the Montgomery potential (work.c:1438-1452)
 };
 void launch_accumulate_averages(const Grid2& g, const AvgParams& a, cudaStream_t s);
 // f[i] *= factor for n contiguous doubles
@@ -87,6 +88,7 @@ struct EzParams {
   double geff[AVG_LMAX];
   const double *u, *v, *h, *hw, *hhb, *omz;
   int qpitch;
+  const double* b;   // useBuoyancy: g_tot = geff - b (diagnostics.c:653-655), else nullptr
 };
 size_t ez_scratch_elems(const Grid2& g, bool serial_order);
 int launch_energy(const Grid2& g, const EzParams& e, bool serial_order, double* terms, double* out,

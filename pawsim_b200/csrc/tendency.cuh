@@ -64,7 +64,11 @@ struct TendParams {
   // budget build of the kernel (launch_tendency_budget).
   double dt;
   double *bud_u, *bud_v, *bud_h, *bud_e, *bud_b;
-  const double* b;                // tracer at the start of the step (Tracer_advection/diaAdv)
+  const double* b;                // tracer at the start of the step (budgets, buoyancy)
+  // the tracer as a buoyancy anomaly (useBuoyancy; work.c:190-212, 1438-1452, 1745-1748,
+  // 1829-1832; diapycnal.c:40-66, 104-114): also only in the budget build
+  int use_buoy;
+  double conv_diff;               // convDiff: added viscosity where the local g' < 0
 };
 
 // budget term indices (work.h:18-91)
@@ -85,7 +89,8 @@ __device__ inline void budget_add(double* fam, int term, int k, int L, size_t ls
 
 int launch_tendency(const TendParams& p, int momentum_scheme, int thickness_scheme,
                     cudaStream_t stream);
-// the same step with every enabled budget family accumulated (32 x 8 tiles)
+// the same step with every enabled budget family accumulated and the buoyancy coupling
+// (32 x 8 tiles)
 int launch_tendency_budget(const TendParams& p, int momentum_scheme, int thickness_scheme,
                            cudaStream_t stream);
 

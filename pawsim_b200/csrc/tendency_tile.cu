@@ -196,6 +196,16 @@ __device__ inline double gload(const double* f, const TendParams& p, int gi, int
   return load_mapped(f, p.pitch, gi, gj, p.Nx, p.Ny, p.wall_ew, p.wall_ns, kx, ky);
 }
 
+// hz = h (eta_k + eta_k+1) / 2 of layer k at raw (x, y) (work.c:205-208), interface heights
+// built upward from the bottom as work.c:1184-1199 does; ghost positions through the maps
+__device__ inline double buoy_hz(const TendParams& p, int k, int x, int y) {
+  double e1 = gload(p.hhb, p, x, y, MAP_S, MAP_S);
+  for (int m = p.L - 1; m > k; --m) e1 = e1 + gload(p.h + m * p.lstride, p, x, y, MAP_S, MAP_S);
+  const double hk = gload(p.h + k * p.lstride, p, x, y, MAP_S, MAP_S);
+  const double e0 = e1 + hk;
+  return hk * 0.5 * (e0 + e1);
+}
+
 // face thickness of a layer at an owned cell, read from global memory (h, u, v of that layer;
 // ghost positions through the scalar / velocity maps)
 template <int TS>
@@ -294,11 +304,24 @@ tendency_kernel(const __grid_constant__ TendParams p) {
       }
     }
     double pp = 0;
+    double bprev = 0;   // tracer of the layer above (buoyancy build)
 #pragma unroll
     for (int k = 0; k < LMAX; ++k) {
       if (k < L) {
         if (k == 0) pp = p.use_rl ? 0 : p.gg[0] * eta[0];
         else pp = pp + p.gg[k] * eta[k];
+        if constexpr (BUD) {
+          // the buoyancy anomaly in the Bernoulli pressure (work.c:1438-1452)
+          if (p.use_buoy) {
+            const double bk = inner ? p.b[k * p.lstride + gc] : gload(p.b + k * p.lstride, p, gi, gj, MAP_S, MAP_S);
+            if (k == 0) {
+              if (!p.use_rl) pp -= bk * eta[0];
+            } else {
+              pp += eta[k] * (bprev - bk);
+            }
+            bprev = bk;
+          }
+        }
         double mm = pp;
         if (p.h0 != 0) {
           double h0 = p.h0, hc = hk[k];
@@ -576,9 +599,17 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         a4 = -(div_rn(A4H(i, j) * AT(sh, i, j) * d4t0 - A4H(i - 1, j) * AT(sh, i - 1, j) * d4tm, dx, rdx)
                + div_rn(A4Q(i, j + 1) * AT(hq, i, j + 1) * d4s1 - A4Q(i, j) * AT(hq, i, j) * d4s0, dy, rdy));
       }
-      ru = gM + gK + rq + ((hwest != 0) ? div_rn(a2 + a4 + 0.0, hwest, rhw) : 0);
+      double buoy = 0;
       if constexpr (BUD) {
-        // work.c:1753-1763 (the buoyancy terms are zero: buoyancy is not built)
+        // -0.5 (hz(i) + hz(i-1)) db/dx (work.c:1745-1748)
+        if (p.use_buoy && hwest != 0)
+          buoy = -0.5 * (buoy_hz(p, k, gi, gj) + buoy_hz(p, k, gi - 1, gj))
+               * div_rn(gload(p.b + k * p.lstride, p, gi, gj, MAP_S, MAP_S)
+                        - gload(p.b + k * p.lstride, p, gi - 1, gj, MAP_S, MAP_S), dx, rdx);
+      }
+      ru = gM + gK + rq + ((hwest != 0) ? div_rn(a2 + a4 + buoy, hwest, rhw) : 0);
+      if constexpr (BUD) {
+        // work.c:1753-1763
         const bool active = !(p.wall_ew && gi == 0);
         budget_add(p.bud_u, BU_GRADM, k, L, p.lstride, cell, hwest * gM * p.dt);
         budget_add(p.bud_u, BU_GRADKE, k, L, p.lstride, cell, hwest * gK * p.dt);
@@ -589,6 +620,8 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         budget_add(p.bud_e, BE_ADV, k, L, p.lstride, cell, hwest * (gK + rq) * uc * p.dt);
         budget_add(p.bud_e, BE_A2, k, L, p.lstride, cell, a2 * uc * p.dt);
         budget_add(p.bud_e, BE_A4, k, L, p.lstride, cell, a4 * uc * p.dt);
+        budget_add(p.bud_u, BU_BUOY, k, L, p.lstride, cell, buoy * p.dt);
+        budget_add(p.bud_e, BE_BUOY, k, L, p.lstride, cell, buoy * uc * p.dt);
       }
     }
     // ---- v momentum (work.c:1759-1852) ----
@@ -623,7 +656,15 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         a4 = -(div_rn(A4Q(i + 1, j) * AT(hq, i + 1, j) * d4s1 - A4Q(i, j) * AT(hq, i, j) * d4s0, dx, rdx)
                - div_rn(A4H(i, j) * AT(sh, i, j) * d4t0 - A4H(i, j - 1) * AT(sh, i, j - 1) * d4tm, dy, rdy));
       }
-      rv = gM + gK + rq + ((hsouth != 0) ? div_rn(a2 + a4 + 0.0, hsouth, rhs) : 0);
+      double buoy = 0;
+      if constexpr (BUD) {
+        // work.c:1829-1832
+        if (p.use_buoy && hsouth != 0)
+          buoy = -0.5 * (buoy_hz(p, k, gi, gj) + buoy_hz(p, k, gi, gj - 1))
+               * div_rn(gload(p.b + k * p.lstride, p, gi, gj, MAP_S, MAP_S)
+                        - gload(p.b + k * p.lstride, p, gi, gj - 1, MAP_S, MAP_S), dy, rdy);
+      }
+      rv = gM + gK + rq + ((hsouth != 0) ? div_rn(a2 + a4 + buoy, hsouth, rhs) : 0);
       if constexpr (BUD) {
         // work.c:1837-1847
         const bool active = !(p.wall_ns && gj == 0);
@@ -636,6 +677,8 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         budget_add(p.bud_e, BE_ADV, k, L, p.lstride, cell, hsouth * (gK + rq) * vc * p.dt);
         budget_add(p.bud_e, BE_A2, k, L, p.lstride, cell, a2 * vc * p.dt);
         budget_add(p.bud_e, BE_A4, k, L, p.lstride, cell, a4 * vc * p.dt);
+        budget_add(p.bud_v, BU_BUOY, k, L, p.lstride, cell, buoy * p.dt);
+        budget_add(p.bud_e, BE_BUOY, k, L, p.lstride, cell, buoy * vc * p.dt);
       }
     }
     // ---- diapycnal advection and viscosity (diapycnal.c:203-291) ----
@@ -686,6 +729,19 @@ tendency_kernel(const __grid_constant__ TendParams p) {
           double dzv = 0.5 * (hsb + hsa);
           double nuu = gload(p.nu_u + kk * p.lstride, p, gi, gj, MAP_N, MAP_S);
           double nuv = gload(p.nu_v + kk * p.lstride, p, gi, gj, MAP_S, MAP_N);
+          if constexpr (BUD) {
+            // convective viscosity where the local reduced gravity g' = gg + b(k-1) - b(k) is
+            // negative (diapycnal.c:40-66, 104-114); without buoyancy g' = gg >= 0
+            if (p.use_buoy && p.conv_diff != 0) {
+              auto gp = [&](int x, int y) {
+                return p.gg[kk] + (gload(p.b + (kk - 1) * p.lstride, p, x, y, MAP_S, MAP_S)
+                                   - gload(p.b + kk * p.lstride, p, x, y, MAP_S, MAP_S));
+              };
+              const double g0 = gp(gi, gj);
+              if (g0 < 0 || gp(gi - 1, gj) < 0) nuu += p.conv_diff;
+              if (g0 < 0 || gp(gi, gj - 1) < 0) nuv += p.conv_diff;
+            }
+          }
           double ua = gload(p.u + (kk - 1) * p.lstride, p, gi, gj, MAP_N, MAP_S);
           double ub = gload(p.u + kk * p.lstride, p, gi, gj, MAP_N, MAP_S);
           double va = gload(p.v + (kk - 1) * p.lstride, p, gi, gj, MAP_S, MAP_N);

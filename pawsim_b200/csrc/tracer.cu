@@ -214,8 +214,12 @@ __global__ void __launch_bounds__(TNT) tracer_tile_kernel(const TracerParams p) 
     const double w0 = p.wdia[lk + cell], w1 = p.wdia[lk + p.lstride + cell];
     const double b_p = (k == 0) ? 0 : p.b[lk - p.lstride + cell];
     const double b_m = (k == p.L - 1) ? 0 : p.b[lk + p.lstride + cell];
-    const double db_p = (w0 > 0) ? 0 : b_p - bc;
-    const double db_m = (w1 > 0) ? bc - b_m : 0;
+    double db_p = (w0 > 0) ? 0 : b_p - bc;
+    double db_m = (w1 > 0) ? bc - b_m : 0;
+    if (p.use_buoy) {
+      db_p += (w0 > 0) ? 0 : p.gg[k];
+      db_m += ((k + 1 < p.L) && (w1 > 0)) ? p.gg[k + 1] : 0;
+    }
     rhs_wdia = -(w0 * db_p + w1 * db_m);
     rhs_b += div_rn(rhs_wdia, h, rh);
   }

@@ -32,6 +32,9 @@ struct TracerParams {
   // Tracer_* budget (work.c:2131-2136): [term][layer] planes lstride apart, or nullptr
   double* bud_b;
   double dt;
+  // useBuoyancy: the diapycnal jumps include the layers' reduced gravities (work.c:2088-2093)
+  int use_buoy;
+  double gg[8];
 };
 
 void launch_tracer(const TracerParams& p, cudaStream_t s);

@@ -842,9 +842,10 @@ int main (int argc, char ** argv)
   g.K2 = c.K2; g.K4 = c.K4;
   g.budgets = (c.savefreqUMom > 0 ? 1 : 0) | (c.savefreqVMom > 0 ? 2 : 0) | (c.savefreqThic > 0 ? 4 : 0)
             | (c.savefreqEnergy > 0 ? 8 : 0) | (c.savefreqTracer > 0 ? 16 : 0);
-  if (c.useTracer && (c.useBuoyancy || file_of(&c,"diaDiffFile")[0] || file_of(&c,"bFluxFile")[0]))
+  g.use_buoyancy = c.useTracer && c.useBuoyancy;
+  if (c.useTracer && (file_of(&c,"diaDiffFile")[0] || file_of(&c,"bFluxFile")[0]))
   {
-    fprintf(stderr,"ERROR: the tracer's buoyancy coupling and diapycnal diffusion are not built on the GPU\n");
+    fprintf(stderr,"ERROR: the tracer's diapycnal diffusion is not built on the GPU\n");
     return 1;
   }
 

@@ -351,10 +351,11 @@ def load_fields(cfg: Config) -> dict:
 RHO0 = 1000.0
 
 
-def add_tracer(param_path, scheme=2, relax_days=100.0, K2=0.0, K4=0.0, amp=1.0, seed=7):
-    """Add a passive tracer to an existing set-up: b = amp * (sin(2 pi y / Ly) + noise) per
-    layer (bInitFile), relaxation to it on relax_days (bRelaxFile, bTimeFile; <= 0 turns
-    relaxation off), tracerScheme and the K2 / K4 diffusivities. Returns the parameter path."""
+def add_tracer(param_path, scheme=2, relax_days=100.0, K2=0.0, K4=0.0, amp=1.0, seed=7, buoyancy=False):
+    """Add a tracer to an existing set-up: b = amp * (sin(2 pi y / Ly) + noise) per layer
+    (bInitFile), relaxation to it on relax_days (bRelaxFile, bTimeFile; <= 0 turns relaxation
+    off), tracerScheme and the K2 / K4 diffusivities; ``buoyancy`` makes it an active buoyancy
+    anomaly (useBuoyancy). Returns the parameter path."""
     cfg = read_config(param_path)
     v = cfg.values
     L, Nx, Ny = v["Nlay"], v["Nx"], v["Ny"]
@@ -375,6 +376,8 @@ def add_tracer(param_path, scheme=2, relax_days=100.0, K2=0.0, K4=0.0, amp=1.0, 
                 params[parts[0]] = parts[1]
     params.update(useTracer=1, tracerScheme=scheme, K2=K2, K4=K4, bInitFile="bInit.dat",
                   bRelaxFile="bRelax.dat", bTimeFile="bTime.dat")
+    if buoyancy:
+        params.update(useBuoyancy=1)
     write_param_file(param_path, params)
     return param_path
 

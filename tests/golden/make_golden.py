@@ -64,6 +64,15 @@ TRC_CASES = {
     "full_tracer_kt00": (inputs.full_physics, dict(N=16, dt=50.0, solver=0, Ly=320e3, bathy_len=20e3,
                                                    sponge=40e3, extra=dict(savefreqAvg=125.0)),
                          dict(scheme=2, relax_days=30.0, K4=1e8)),
+    # the tracer as buoyancy (useBuoyancy): rigid lid, free surface, and four layers with w_dia,
+    # online averages (M_avg) and the energy diagnostics (g_tot = geff - b)
+    "jets_buoy_kt00": (inputs.jets, dict(N=16, dt=100.0, solver=0, tol=1e-10),
+                       dict(scheme=2, relax_days=100.0, K2=100.0, amp=0.002, buoyancy=True)),
+    "jets_buoy_free": (inputs.jets, dict(N=16, dt=30.0, solver=0, extra=dict(useRL=0)),
+                       dict(scheme=1, relax_days=-1.0, amp=0.002, buoyancy=True)),
+    "full_buoy_avg": (inputs.full_physics, dict(N=16, dt=50.0, solver=0, Ly=320e3, bathy_len=20e3, sponge=40e3,
+                                                extra=dict(savefreqAvg=125.0, savefreqEZ=50.0)),
+                      dict(scheme=2, relax_days=30.0, amp=0.001, buoyancy=True)),
 }
 # energy/enstrophy cases (savefreqEZ, diagnostics.c:478-700): a rigid-lid gyre with two lines
 # per step, a free-surface periodic jet (eta from the thickness of the start of the step) and a
@@ -178,13 +187,17 @@ def make_tracer(name, fn, kw, tkw, outdir):
             for k in range(L):
                 for v in ("U", "V", "H", "B"):
                     rec[f"{v}{k}_{n}"] = inputs.read_data(os.path.join(out, f"{v}{k}_n={n}.dat"), (Ny, Nx))
-            rec[f"P_{n}"] = inputs.read_data(os.path.join(out, f"P_n={n}.dat"), (Ny, Nx))
+            if cfg.values["useRL"]:
+                rec[f"P_{n}"] = inputs.read_data(os.path.join(out, f"P_n={n}.dat"), (Ny, Nx))
         windows = sorted({int(f.split("_n=")[1][:-4]) for f in os.listdir(out) if f.startswith("B_avg0_n=")})
         rec["windows"] = np.array(windows, dtype=int)
         for n in windows:
             for k in range(L):
                 rec[f"B_avg{k}_{n}"] = inputs.read_data(os.path.join(out, f"B_avg{k}_n={n}.dat"), (Ny, Nx))
                 rec[f"U_avg{k}_{n}"] = inputs.read_data(os.path.join(out, f"U_avg{k}_n={n}.dat"), (Ny, Nx))
+                rec[f"M_avg{k}_{n}"] = inputs.read_data(os.path.join(out, f"M_avg{k}_n={n}.dat"), (Ny, Nx))
+        if os.path.exists(os.path.join(out, "EZdiags.dat")):
+            rec["ez_text"] = np.array(open(os.path.join(out, "EZdiags.dat")).read())
         np.savez_compressed(os.path.join(outdir, name + ".npz"), **rec)
 
 

@@ -4,7 +4,10 @@ three tracer schemes (AL81, UP3, KT00) with Laplacian and biharmonic diffusion, 
 advection by w_dia, relaxation to bRelax, walled and doubly periodic grids, AL81 and HK83
 face thickness. SOR pressure keeps the runs bit-exact, so every B file (and U, V, H, P)
 must equal the reference's bit for bit, through the drop-in executable and through the
-Python API; B_avg (savefreqAvg) likewise."""
+Python API; B_avg (savefreqAvg) likewise. With useBuoyancy the tracer is a buoyancy anomaly
+(Bernoulli pressure, -hz db/dx in the momentum, g' in the tracer's diapycnal jumps): rigid
+lid, free surface, and four layers with w_dia whose M_avg and EZdiags.dat (g_tot = geff - b)
+must also match."""
 import os
 import subprocess
 
@@ -17,7 +20,8 @@ from golden_util import load_case
 pytestmark = pytest.mark.gpu
 
 DRIVER = os.path.join(ROOT, "pawsim_b200", "bin", "PAWSIM_B200.exe")
-CASES = ["jets_tracer_kt00", "gyre_tracer_up3", "gyre_tracer_al81_hk83", "full_tracer_kt00"]
+CASES = ["jets_tracer_kt00", "gyre_tracer_up3", "gyre_tracer_al81_hk83", "full_tracer_kt00",
+         "jets_buoy_kt00", "jets_buoy_free", "full_buoy_avg"]
 NSTEPS = 4
 
 
@@ -37,12 +41,17 @@ def test_driver_tracer_matches_reference(tmp_path, name):
                 got = inputs.read_data(str(out / f"{v}{k}_n={n}.dat"), shape)
                 ref = z[f"{v}{k}_{n}"]
                 assert value_equal(got, ref), (n, v, k, np.abs(got - ref).max())
-        assert value_equal(inputs.read_data(str(out / f"P_n={n}.dat"), shape), z[f"P_{n}"]), n
+        if cfg.values["useRL"]:
+            assert value_equal(inputs.read_data(str(out / f"P_n={n}.dat"), shape), z[f"P_{n}"]), n
     for n in [int(w) for w in z["windows"]]:
         for k in range(cfg.Nlay):
-            for v in ("B_avg", "U_avg"):
+            for v in ("B_avg", "U_avg", "M_avg"):
+                if f"{v}{k}_{n}" not in z.files:
+                    continue
                 got = inputs.read_data(str(out / f"{v}{k}_n={n}.dat"), shape)
                 assert value_equal(got, z[f"{v}{k}_{n}"]), (n, v, k)
+    if "ez_text" in z.files:
+        assert (out / "EZdiags.dat").read_text() == str(z["ez_text"])
 
 
 @pytest.mark.parametrize("name", ["jets_tracer_kt00", "gyre_tracer_up3"])
