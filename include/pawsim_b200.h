@@ -87,7 +87,7 @@ typedef struct pawsim_gpu_config
   int mg_tile;
   /* tracer b (work.c:1947-2144): useTracer, tracerScheme (0 AL81, 1 UP3, 2 KT00) and the
    * Laplacian / biharmonic diffusivities K2, K4 (the buoyancy coupling is use_buoyancy
-   * below). Diapycnal diffusion (diaDiffFile, bFluxFile) is not built. */
+   * below, its diapycnal diffusion use_diadiff). */
   int use_tracer, tracer_scheme;
   double K2, K4;
   /* First guess of the multigrid solves (pressureSolver 1 and 2): 0 the previous pressure,
@@ -105,6 +105,10 @@ typedef struct pawsim_gpu_config
    * momentum (-hz db/dx), the tracer's diapycnal advection and the local reduced gravity of
    * the convective viscosity (convDiff); needs use_tracer. */
   int use_buoyancy;
+  /* useDiaDiff (diaDiffFile, bFluxFile or convDiff != 0) with a tracer: diapycnal diffusion of
+   * b through the interfaces (diapycnal.c:140-197) with the diffusivity kappa_dia per
+   * interface and the surface flux Fsurf_b (fields of those names). */
+  int use_diadiff;
 } pawsim_gpu_config;
 
 enum

@@ -49,7 +49,7 @@ class GpuConfig(ctypes.Structure):
                         ("use_tracer", ctypes.c_int), ("tracer_scheme", ctypes.c_int),
                         ("K2", ctypes.c_double), ("K4", ctypes.c_double),
                         ("pi_guess", ctypes.c_int), ("budgets", ctypes.c_int),
-                        ("use_buoyancy", ctypes.c_int)]
+                        ("use_buoyancy", ctypes.c_int), ("use_diadiff", ctypes.c_int)]
 
 
 class GpuStats(ctypes.Structure):
@@ -187,6 +187,7 @@ def gpu_config(cfg: inputs.Config, **over) -> GpuConfig:
     g.use_tracer, g.tracer_scheme = int(v["useTracer"]), int(v["tracerScheme"])
     g.K2, g.K4 = float(v["K2"]), float(v["K4"])
     g.use_buoyancy = int(bool(v["useBuoyancy"]) and bool(v["useTracer"]))
+    g.use_diadiff = int(bool(v["useDiaDiff"]) and bool(v["useTracer"]))
     # budget families of the savefreq keys (work.c:310-319)
     g.budgets = sum(bit for bit, key in ((1, "savefreqUMom"), (2, "savefreqVMom"), (4, "savefreqThic"),
                                          (8, "savefreqEnergy"), (16, "savefreqTracer")) if v[key] > 0)
@@ -199,8 +200,6 @@ class Model:
     """One model resident on the GPU (the drop-in for the reference's hot path)."""
 
     def __init__(self, cfg: inputs.Config, fields: dict | None = None, **options):
-        if cfg.values["useTracer"] and (cfg.files.get("diaDiffFile") or cfg.files.get("bFluxFile")):
-            raise PawsimError(-5, "the tracer's diapycnal diffusion is not built")
         self.lib = load_library()
         self.cfg = cfg
         self.L, self.Nx, self.Ny = cfg.values["Nlay"], cfg.values["Nx"], cfg.values["Ny"]
@@ -270,9 +269,10 @@ class Model:
                 self.set("wdia_ff", r * (L + 1) + k, f["wdia_ff"][r, k])
         self.set("gg", 0, f["gg"])
         if self._gc.use_tracer:
-            for name in ("b", "bRelax", "bTime"):
+            for name in ("b", "bRelax", "bTime", "kappa_dia"):
                 for k in range(L):
                     self.set(name, k, f[name][k])
+            self.set("Fsurf_b", 0, f["Fsurf_b"])
 
     def state(self) -> dict:
         names = ("u", "v", "h", "b") if self._gc.use_tracer else ("u", "v", "h")

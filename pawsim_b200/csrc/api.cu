@@ -96,6 +96,7 @@ struct Model {
   double* avg = nullptr;
   // tracer (when use_tracer): state b[2] beside u/v/h, tendency history fb[2], restoring
   double *b[2] = {nullptr, nullptr}, *fb[2] = {nullptr, nullptr}, *bRelax = nullptr, *bTime = nullptr;
+  double *kappa = nullptr, *fsurf = nullptr;   // diapycnal diffusivity (per layer) and surface flux
   double *hhs, *hhb, *Hc, *omz, *taux, *tauy, *fbx, *fby, *uLid, *vLid;
   double *uRelax, *vRelax, *hRelax, *eRelax, *uTime, *vTime, *eTime, *hTime, *wdff, *nu_u, *nu_v;
   double *pi, *rhs, *work, *scratch, *dsum;
@@ -224,6 +225,7 @@ static int create(const pawsim_gpu_config* cfg, Model** out) {
   if (c.use_tracer) {
     for (int b = 0; b < 2; ++b) ok &= (m->b[b] = m->alloc<double>(Ls)) && (m->fb[b] = m->alloc<double>(Ls));
     ok &= (m->bRelax = m->alloc<double>(Ls)) && (m->bTime = m->alloc<double>(Ls));
+    ok &= (m->kappa = m->alloc<double>(Ls)) && (m->fsurf = m->alloc<double>(m->plane));
   }
   ok &= (m->wdia = m->alloc<double>((m->L + 1) * m->lstride)) != nullptr;
   ok &= (m->hhs = m->alloc<double>(m->plane)) && (m->hhb = m->alloc<double>(m->plane)) && (m->Hc = m->alloc<double>(m->plane));
@@ -328,6 +330,8 @@ static bool lookup(Model* m, const std::string& n, FieldRef& f) {
   else if (n == "b" && m->b[0]) { f.base = m->b[m->cur]; f.nk = L; }
   else if (n == "bRelax" && m->bRelax) { f.base = m->bRelax; f.nk = L; }
   else if (n == "bTime" && m->bTime) { f.base = m->bTime; f.nk = L; }
+  else if (n == "kappa_dia" && m->kappa) { f.base = m->kappa; f.nk = L; }
+  else if (n == "Fsurf_b" && m->fsurf) f.base = m->fsurf;
   else if (n == "uRelax") { f.base = m->uRelax; f.nk = L; }
   else if (n == "vRelax") { f.base = m->vRelax; f.nk = L; }
   else if (n == "hRelax") { f.base = m->hRelax; f.nk = L; }
@@ -605,6 +609,7 @@ static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
     tp.bud_b = m->bud[4]; tp.dt = dt;
     tp.use_buoy = c.use_buoyancy;
     for (int k = 0; k < m->L; ++k) tp.gg[k] = m->gg[k];
+    tp.use_diadiff = c.use_diadiff; tp.kappa = m->kappa; tp.fsurf = m->fsurf; tp.conv_diff = c.conv_diff;
     launch_tracer(tp, m->s);
     ++g_launches;
   }

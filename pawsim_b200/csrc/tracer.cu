@@ -223,6 +223,27 @@ __global__ void __launch_bounds__(TNT) tracer_tile_kernel(const TracerParams p) 
     rhs_wdia = -(w0 * db_p + w1 * db_m);
     rhs_b += div_rn(rhs_wdia, h, rh);
   }
+  double rhs_diadiff = 0;
+  if (p.use_diadiff && h != 0) {
+    // Fdia_b at interfaces k and k+1 of this column: the surface flux on top, zero at the
+    // bottom, kappa (db + gg with buoyancy) / dz between layers, plus convDiff where the
+    // local reduced gravity is negative (diapycnal.c:165-190)
+    auto fdia = [&](int kk) -> double {
+      if (kk == 0) return p.fsurf[cell];
+      if (kk == p.L) return 0.0;
+      const double ba = p.b[(kk - 1) * p.lstride + cell], bb = p.b[kk * p.lstride + cell];
+      double db = ba - bb;
+      const double dz = 0.5 * (p.h[kk * p.lstride + cell] + p.h[(kk - 1) * p.lstride + cell]);
+      double kappa = p.kappa[kk * p.lstride + cell];
+      if (p.use_buoy) db += p.gg[kk];
+      double gprime = p.gg[kk];
+      if (p.use_buoy) gprime += ba - bb;
+      if (p.conv_diff != 0 && gprime < 0) kappa += p.conv_diff;
+      return dz != 0 ? kappa * db / dz : 0.0;
+    };
+    rhs_diadiff = fdia(k) - fdia(k + 1);
+    rhs_b += div_rn(rhs_diadiff, h, rh);
+  }
   if (p.K2 > 0 && h != 0) {
     rhs_K2 = p.K2 * lap(SB, q);
     rhs_b += div_rn(rhs_K2, h, rh);
@@ -237,13 +258,14 @@ __global__ void __launch_bounds__(TNT) tracer_tile_kernel(const TracerParams p) 
     rhs_b += rhs_relax;
   }
   if (p.bud_b) {
-    // work.c:2131-2136 (the diapycnal diffusion term is zero: it is not built)
+    // work.c:2131-2136
     double* f = p.bud_b + lk + cell;
     const size_t P = (size_t)p.L * p.lstride;   // one term's planes
     f[0] = f[0] + h * rhs_adv * p.dt;
     f[P] = f[P] + rhs_wdia * p.dt;
     f[2 * P] = f[2 * P] + rhs_K2 * p.dt;
     f[3 * P] = f[3 * P] + rhs_K4 * p.dt;
+    f[4 * P] = f[4 * P] + rhs_diadiff * p.dt;
     f[5 * P] = f[5 * P] + h * rhs_relax * p.dt;
   }
   const size_t o = lk + cell;

@@ -35,6 +35,11 @@ struct TracerParams {
   // useBuoyancy: the diapycnal jumps include the layers' reduced gravities (work.c:2088-2093)
   int use_buoy;
   double gg[8];
+  // diapycnal diffusion (diapycnal.c:140-197, work.c:2098-2102): interface diffusivity
+  // kappa_dia (layer planes; interface k between layers k-1 and k), surface flux Fsurf_b
+  int use_diadiff;
+  const double *kappa, *fsurf;
+  double conv_diff;
 };
 
 void launch_tracer(const TracerParams& p, cudaStream_t s);

@@ -396,7 +396,9 @@ static int upload_inputs (pawsim_gpu * m, const config * c, const char * outdir)
           && put_layers(m,c,"diaViscVFile","nu_v_dia",0,0,plane,buf);
   if (c->useTracer)   /* tracer state and restoring (state.c:968-1006: b 0, bRelax 0, bTime -1) */
     ok = ok && put_layers(m,c,"bInitFile","b",0,0,plane,buf) && put_layers(m,c,"bRelaxFile","bRelax",0,0,plane,buf)
-            && put_layers(m,c,"bTimeFile","bTime",-1,0,plane,buf);
+            && put_layers(m,c,"bTimeFile","bTime",-1,0,plane,buf)
+            && put_layers(m,c,"diaDiffFile","kappa_dia",0,0,plane,buf)
+            && put_plane(m,c,"bFluxFile","Fsurf_b",0,plane);
   ok = ok && put_plane(m,c,"hsFile","hhs",0,plane) && put_plane(m,c,"hbFile","hhb",0,plane)
           && put_plane(m,c,"uLidFile","uLid",0,plane) && put_plane(m,c,"vLidFile","vLid",0,plane)
           && put_plane(m,c,"FbaroXFile","Fbaro_x",0,plane) && put_plane(m,c,"FbaroYFile","Fbaro_y",0,plane)
@@ -843,11 +845,8 @@ int main (int argc, char ** argv)
   g.budgets = (c.savefreqUMom > 0 ? 1 : 0) | (c.savefreqVMom > 0 ? 2 : 0) | (c.savefreqThic > 0 ? 4 : 0)
             | (c.savefreqEnergy > 0 ? 8 : 0) | (c.savefreqTracer > 0 ? 16 : 0);
   g.use_buoyancy = c.useTracer && c.useBuoyancy;
-  if (c.useTracer && (file_of(&c,"diaDiffFile")[0] || file_of(&c,"bFluxFile")[0]))
-  {
-    fprintf(stderr,"ERROR: the tracer's diapycnal diffusion is not built on the GPU\n");
-    return 1;
-  }
+  /* useDiaDiff (config.c:309-310) */
+  g.use_diadiff = c.useTracer && (file_of(&c,"diaDiffFile")[0] || file_of(&c,"bFluxFile")[0] || c.convDiff != 0);
 
   if (!gpu_ok(pawsim_gpu_create(&g,&m),"pawsim_gpu_create")) return 1;
   plane = malloc(((size_t) (c.Nx + 1) * (c.Ny + 1) + c.Nlay + 1) * sizeof(double));

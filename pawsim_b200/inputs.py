@@ -301,6 +301,7 @@ def load_fields(cfg: Config) -> dict:
         "taux": np.zeros((nt, Ny, Nx)), "tauy": np.zeros((nt, Ny, Nx)),
         "wdia_ff": np.zeros((nw, L + 1, Ny, Nx)),
         "b": np.zeros((L, Ny, Nx)), "bRelax": np.zeros((L, Ny, Nx)), "bTime": np.full((L, Ny, Nx), -1.0),
+        "kappa_dia": np.zeros((L, Ny, Nx)), "Fsurf_b": np.zeros((Ny, Nx)),
     }
 
     def rd2(key, name):
@@ -328,8 +329,10 @@ def load_fields(cfg: Config) -> dict:
                       ("diaViscUFile", "nu_u_dia"), ("diaViscVFile", "nu_v_dia")):
         rd3(key, name)
     if v["useTracer"]:
-        for key, name in (("bInitFile", "b"), ("bRelaxFile", "bRelax"), ("bTimeFile", "bTime")):
+        for key, name in (("bInitFile", "b"), ("bRelaxFile", "bRelax"), ("bTimeFile", "bTime"),
+                          ("diaDiffFile", "kappa_dia")):
             rd3(key, name)
+        rd2("bFluxFile", "Fsurf_b")
     for key, name in (("tauxFile", "taux"), ("tauyFile", "tauy")):
         p = _resolve(cfg, key)
         if p:
@@ -378,6 +381,32 @@ def add_tracer(param_path, scheme=2, relax_days=100.0, K2=0.0, K4=0.0, amp=1.0, 
                   bRelaxFile="bRelax.dat", bTimeFile="bTime.dat")
     if buoyancy:
         params.update(useBuoyancy=1)
+    write_param_file(param_path, params)
+    return param_path
+
+
+def add_diapycnal_diffusion(param_path, kappa=1e-4, flux=1e-9, conv_diff=0.0, seed=11):
+    """Give an existing tracer set-up diapycnal diffusion: a diffusivity kappa (times 1 + noise/2)
+    at every interface (diaDiffFile), a surface flux flux * (1 + noise) (bFluxFile) and, when
+    conv_diff is not zero, convective mixing where the local reduced gravity is negative."""
+    cfg = read_config(param_path)
+    v = cfg.values
+    L, Nx, Ny = v["Nlay"], v["Nx"], v["Ny"]
+    rng = np.random.default_rng(seed)
+    kap = kappa * (1 + 0.5 * np.stack([_smoothed_noise(rng, Ny, Nx, 1.0, 3, True, True) for _ in range(L)]))
+    fl = flux * (1 + _smoothed_noise(rng, Ny, Nx, 1.0, 3, True, True))
+    d = os.path.dirname(param_path)
+    write_data(os.path.join(d, "diaDiff.dat"), _layer_stack(kap))
+    write_data(os.path.join(d, "bFlux.dat"), fl)
+    params = {}
+    with open(param_path) as fh:
+        for line in fh:
+            parts = line.split()
+            if len(parts) >= 2:
+                params[parts[0]] = parts[1]
+    params.update(diaDiffFile="diaDiff.dat", bFluxFile="bFlux.dat")
+    if conv_diff:
+        params.update(convDiff=conv_diff)
     write_param_file(param_path, params)
     return param_path
 

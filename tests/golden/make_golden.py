@@ -73,6 +73,14 @@ TRC_CASES = {
     "full_buoy_avg": (inputs.full_physics, dict(N=16, dt=50.0, solver=0, Ly=320e3, bathy_len=20e3, sponge=40e3,
                                                 extra=dict(savefreqAvg=125.0, savefreqEZ=50.0)),
                       dict(scheme=2, relax_days=30.0, amp=0.001, buoyancy=True)),
+    # diapycnal diffusion of the tracer (diaDiffFile, bFluxFile): passive on a walled gyre; as
+    # buoyancy with convective mixing (convDiff) where the local reduced gravity is negative,
+    # which also turns on the convective viscosity of the momentum
+    "gyre_diadiff": (inputs.gyre, dict(N=16, Ny=12, dt=900.0, solver=0, tol=1e-10),
+                     dict(scheme=1, relax_days=30.0, diadiff=dict(kappa=1e-4, flux=1e-8))),
+    "jets_diadiff_conv": (inputs.jets, dict(N=16, dt=100.0, solver=0, tol=1e-10),
+                          dict(scheme=2, relax_days=100.0, amp=0.05, buoyancy=True,
+                               diadiff=dict(kappa=1e-4, flux=1e-9, conv_diff=1e-2))),
 }
 # energy/enstrophy cases (savefreqEZ, diagnostics.c:478-700): a rigid-lid gyre with two lines
 # per step, a free-surface periodic jet (eta from the thickness of the start of the step) and a
@@ -101,12 +109,25 @@ BUD_CASES = {
     "gyre_quad_budget": (inputs.gyre, dict(N=20, Ny=12, dt=600.0, solver=0,
                                            extra=dict(quadDragCoeff=2e-3, quadDragSurf=1e-3, windFeedback=1,
                                                       oceanSurfDrag=0)), None),
+    "jets_diadiff_budget": (inputs.jets, dict(N=16, dt=100.0, solver=0, tol=1e-10),
+                            dict(scheme=2, relax_days=100.0, amp=0.05, buoyancy=True,
+                                 diadiff=dict(kappa=1e-4, flux=1e-9, conv_diff=1e-2))),
     "gyre_fractions_budget": (inputs.gyre, dict(N=20, Ny=12, dt=600.0, solver=0,
                                                 extra=dict(hsml=1500.0, hmin_surf=5.0, hbbl=500.0, hmin_bot=10.0,
                                                            linDragSurf=1e-4, thicknessScheme=3)), None),
 }
 LINE = re.compile(r"iters=(\d+) walltime=\S+ s residual_max=(\S+) residual_rms=(\S+) "
                   r"div_max=(\S+) div_rms=(\S+)")
+
+
+def add_tracer_and_mixing(p, tkw):
+    """add_tracer with the arguments of tkw; its "diadiff" entry, if any, goes to
+    add_diapycnal_diffusion."""
+    tkw = dict(tkw)
+    dd = tkw.pop("diadiff", None)
+    inputs.add_tracer(p, **tkw)
+    if dd:
+        inputs.add_diapycnal_diffusion(p, **dd)
 
 
 def make(name, fn, kw, outdir):
@@ -173,7 +194,7 @@ def make_tracer(name, fn, kw, tkw, outdir):
         extra = dict(kw.pop("extra", {}) or {})
         dt = kw["dt"]
         p = fn(os.path.join(d, "in"), Nt=TRC_NSTEPS, savefrequency=dt, extra=extra, **kw)
-        inputs.add_tracer(p, **tkw)
+        add_tracer_and_mixing(p, tkw)
         cfg = inputs.read_config(p)
         out = os.path.join(d, "out")
         os.makedirs(out)
@@ -231,7 +252,7 @@ def make_budget(name, fn, kw, tkw, outdir):
             extra.update(savefreqTracer=3 * dt)
         p = fn(os.path.join(d, "in"), Nt=BUD_NSTEPS, savefrequency=BUD_NSTEPS * dt, extra=extra, **kw)
         if tkw is not None:
-            inputs.add_tracer(p, **tkw)
+            add_tracer_and_mixing(p, tkw)
         cfg = inputs.read_config(p)
         out = os.path.join(d, "out")
         os.makedirs(out)

@@ -7,7 +7,9 @@ must equal the reference's bit for bit, through the drop-in executable and throu
 Python API; B_avg (savefreqAvg) likewise. With useBuoyancy the tracer is a buoyancy anomaly
 (Bernoulli pressure, -hz db/dx in the momentum, g' in the tracer's diapycnal jumps): rigid
 lid, free surface, and four layers with w_dia whose M_avg and EZdiags.dat (g_tot = geff - b)
-must also match."""
+must also match. Diapycnal diffusion (diaDiffFile, bFluxFile): passive on a walled gyre, and
+as buoyancy with convective mixing (convDiff) where the local reduced gravity is negative,
+which also drives the convective viscosity of the momentum."""
 import os
 import subprocess
 
@@ -21,7 +23,7 @@ pytestmark = pytest.mark.gpu
 
 DRIVER = os.path.join(ROOT, "pawsim_b200", "bin", "PAWSIM_B200.exe")
 CASES = ["jets_tracer_kt00", "gyre_tracer_up3", "gyre_tracer_al81_hk83", "full_tracer_kt00",
-         "jets_buoy_kt00", "jets_buoy_free", "full_buoy_avg"]
+         "jets_buoy_kt00", "jets_buoy_free", "full_buoy_avg", "gyre_diadiff", "jets_diadiff_conv"]
 NSTEPS = 4
 
 
