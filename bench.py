@@ -39,6 +39,21 @@ DT = 60.0
 TOL = 1e-10
 
 
+def max_over_ranks(x, dist=None):
+    """The largest of each rank's x (a CPU all-reduce over the replica group; x itself
+    without one)."""
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t[0])
+
+
+def job_throughput(world, steps, seconds):
+    """Whole-job sim-days/s: every replica advances `steps` steps of DT in `seconds`."""
+    return world * steps * DT / 86400.0 / seconds
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -377,12 +392,9 @@ def main():
             ez_ms += z0.elapsed_time(z1)
         ez_ms /= reps
 
-    t_all = torch.tensor([ms], dtype=torch.float64)
-    if dist is not None:
-        dist.all_reduce(t_all, op=dist.ReduceOp.MAX)
-    ms_max = float(t_all[0])
+    ms_max = max_over_ranks(ms, dist)
     sec = ms_max / 1e3
-    value = world * args.steps * DT / 86400.0 / sec
+    value = job_throughput(world, args.steps, sec)
 
     # e2e through the public API: upload the state from pinned host memory, step, read the
     # per-step report, download the final state -- all inside the timed region
@@ -418,10 +430,7 @@ def main():
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
     d2h = sum(t.numel() * 8 for t in pinned_out.values()) + args.steps * 7 * 8
-    t_e2e = torch.tensor([e2e_s], dtype=torch.float64)
-    if dist is not None:
-        dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.steps * DT / 86400.0 / float(t_e2e[0])
+    e2e_value = job_throughput(world, args.steps, max_over_ranks(e2e_s, dist))
 
     ws = None
     if not args.no_warm_start:
