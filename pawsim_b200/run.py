@@ -4,7 +4,7 @@
                               [--solver 0|1] [--mg-fp32] [--mg-tile K] [--mg-omega W]
                               [--mg-pre P] [--mg-post Q] [--pi-guess G] [--dt 60] [--param FILE]
                               [--ws-collect S --ws-epochs E] [--tracer SCHEME]
-                              [--averages] [--energy]
+                              [--averages] [--energy] [--budgets]
 
 ``--integrator-only`` advances with ``pawsim_gpu_integrator_step`` alone (one fused tendency
 kernel per step, no pressure correction), which isolates the tendency kernel for a profiler.
@@ -14,7 +14,8 @@ network for ``--ws-epochs`` epochs on the GPU, then runs ``--steps`` steps whose
 from the network's guess (this exercises the tcgen05 convolution kernels).
 ``--tracer SCHEME`` adds a passive tracer (0 AL81, 1 UP3, 2 KT00; K2 = 100, relaxation over
 100 days). ``--averages`` accumulates the online averages after every step; ``--energy``
-computes the energy and enstrophy sums after every step.
+computes the energy and enstrophy sums after every step; ``--budgets`` turns on the u, v,
+thickness and energy budgets (the budget build of the fused kernel).
 """
 from __future__ import annotations
 
@@ -49,6 +50,7 @@ def main(argv=None):
     ap.add_argument("--tracer", type=int, default=-1, help="tracer scheme 0..2; negative: no tracer")
     ap.add_argument("--averages", action="store_true")
     ap.add_argument("--energy", action="store_true")
+    ap.add_argument("--budgets", action="store_true")
     a = ap.parse_args(argv)
     with tempfile.TemporaryDirectory() as d:
         if a.param:
@@ -59,6 +61,9 @@ def main(argv=None):
                 kw.update(Nx=a.N, Ny=max(a.N // 2, 4))
             else:
                 kw["N"] = a.N
+            if a.budgets:
+                kw["extra"] = dict(savefreqUMom=86400.0, savefreqVMom=86400.0, savefreqThic=86400.0,
+                                   savefreqEnergy=86400.0)
             if a.dt:
                 kw["dt"] = a.dt
             elif a.setup == "gyre":
