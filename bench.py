@@ -37,6 +37,7 @@ METRIC = "sim-days/s at 2048^2 2-layer (double gyre, rigid lid, AB3, MG pressure
 N_GRID = int(os.environ.get("PAWSIM_BENCH_N", "2048"))
 DT = 60.0
 TOL = 1e-10
+FP32_INNER = 4   # FP32 V-cycles per FP64 defect-correction step in the mixed-precision solves
 
 
 def max_over_ranks(x, dist=None):
@@ -242,14 +243,15 @@ def budget_timing(stream, reps):
 def pressure_comparison(cfg, fields, stream, spin, steps, epochs, pairs):
     """Pressure ms/step and V-cycles/step of the plain FP64 multigrid (started from the
     previous pressure, as the reference's solver is) against FP32 V-cycles in FP64 defect
-    correction started from the learned guess. Both models run the same `spin` untimed
-    steps (the learned one collecting its training pairs), the network is trained on the GPU
-    (untimed), then `steps` steps of each are timed with CUDA events."""
+    correction (FP32_INNER cycles per FP64 defect step), without and with the learned guess.
+    All models run the same `spin` untimed steps (the learned one collecting its training
+    pairs), the network is trained on the GPU (untimed), then `steps` steps of each are timed
+    with CUDA events. vcycles_per_step counts every V-cycle (defect steps x FP32_INNER)."""
     import torch
     import pawsim_b200
     res = {}
-    for name, fp32, learn in (("plain_fp64", 0, False), ("learned_fp32", 1, True)):
-        m = pawsim_b200.Model(cfg, fields, mg_fp32=fp32)
+    for name, fp32, learn in (("plain_fp64", 0, False), ("fp32", 1, False), ("learned_fp32", 1, True)):
+        m = pawsim_b200.Model(cfg, fields, mg_fp32=fp32, mg_fp32_inner=FP32_INNER if fp32 else 1)
         m.set_stream(stream.cuda_stream)
         with torch.cuda.stream(stream):
             if learn:
@@ -280,13 +282,17 @@ def pressure_comparison(cfg, fields, stream, spin, steps, epochs, pairs):
             e1.record(stream)
             torch.cuda.synchronize()
             step_ms = e0.elapsed_time(e1) / steps
-        res[name] = {"pressure_ms_per_step": float(np.mean(solve)), "vcycles_per_step": float(np.mean(iters)),
+        inner = FP32_INNER if fp32 else 1
+        res[name] = {"pressure_ms_per_step": float(np.mean(solve)),
+                     "vcycles_per_step": float(np.mean(iters)) * inner,
+                     "defect_steps_per_step": float(np.mean(iters)) if fp32 else None,
                      "ms_per_step": step_ms, "sim_days_per_s": DT / 86400.0 / (step_ms / 1e3), **extra}
         if learn:
             res[name]["guess_used_steps"] = int(used)
         m.close()
     res["window"] = f"steps {spin + 1}..{spin + steps} after prelim"
     res["pressure_speedup"] = res["plain_fp64"]["pressure_ms_per_step"] / res["learned_fp32"]["pressure_ms_per_step"]
+    res["fp32_inner"] = FP32_INNER
     return res
 
 

@@ -109,6 +109,10 @@ typedef struct pawsim_gpu_config
    * b through the interfaces (diapycnal.c:140-197) with the diffusivity kappa_dia per
    * interface and the surface flux Fsurf_b (fields of those names). */
   int use_diadiff;
+  /* With mg_fp32 = 1: FP32 V-cycles per FP64 defect-correction step (0 or 1: one; at most 8).
+   * Each after the first continues from the correction the previous one left, so a step
+   * reduces the defect further before the FP64 residual pass; stats.iters counts steps. */
+  int mg_fp32_inner;
 } pawsim_gpu_config;
 
 enum

@@ -49,7 +49,8 @@ class GpuConfig(ctypes.Structure):
                         ("use_tracer", ctypes.c_int), ("tracer_scheme", ctypes.c_int),
                         ("K2", ctypes.c_double), ("K4", ctypes.c_double),
                         ("pi_guess", ctypes.c_int), ("budgets", ctypes.c_int),
-                        ("use_buoyancy", ctypes.c_int), ("use_diadiff", ctypes.c_int)]
+                        ("use_buoyancy", ctypes.c_int), ("use_diadiff", ctypes.c_int),
+                        ("mg_fp32_inner", ctypes.c_int)]
 
 
 class GpuStats(ctypes.Structure):

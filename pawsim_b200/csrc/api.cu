@@ -185,6 +185,7 @@ static int create(const pawsim_gpu_config* cfg, Model** out) {
   if (c.pi_guess < 0 || c.pi_guess > 1) return fail(PAWSIM_GPU_EBADCONFIG, "pi_guess must be 0 or 1");
   if (c.budgets < 0 || c.budgets > 31) return fail(PAWSIM_GPU_EBADCONFIG, "budgets is a mask of five families");
   if (c.use_buoyancy && !c.use_tracer) return fail(PAWSIM_GPU_EBADCONFIG, "useBuoyancy requires useTracer");
+  if (c.mg_fp32_inner < 0 || c.mg_fp32_inner > 8) return fail(PAWSIM_GPU_EBADCONFIG, "mg_fp32_inner must be in 0..8");
   if (c.Nx < 4 || c.Ny < 4) return fail(PAWSIM_GPU_EBADCONFIG, "Nx and Ny must be at least 4");
   if (c.Ly <= 0 || c.Lx <= 0 || c.dt <= 0) return fail(PAWSIM_GPU_EBADCONFIG, "Lx, Ly and dt must be positive");
   if (c.ts_scheme < 3 || c.ts_scheme > 5)
@@ -454,6 +455,7 @@ static int init(Model* m) {
     for (size_t q = 0; q < Hc.size(); ++q) Hc[q] = m->hhs_host[q] - m->hhb_host[q];
     MGOptions o;
     o.fp32_cycles = m->c.mg_fp32;
+    o.fp32_inner = m->c.mg_fp32_inner > 0 ? m->c.mg_fp32_inner : 1;
     o.pre = m->c.mg_pre > 0 ? m->c.mg_pre : 1;
     o.post = m->c.mg_post > 0 ? m->c.mg_post : 1;
     o.omega_rb = m->c.mg_omega > 0 ? m->c.mg_omega : 1.0;

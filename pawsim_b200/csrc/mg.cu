@@ -1096,7 +1096,7 @@ void Multigrid::tabulate_coarse(cudaStream_t s) {
 }
 
 template <typename T>
-void Multigrid::enqueue_vcycle(cudaStream_t s, unsigned long long* measure_bits) {
+void Multigrid::enqueue_vcycle(cudaStream_t s, unsigned long long* measure_bits, bool cont) {
   const int top = (int)lv_.size() - 1;
   const T omega = (T)opt_.omega_rb;
   const int pre = opt_.pre, post = opt_.post;
@@ -1105,8 +1105,9 @@ void Multigrid::enqueue_vcycle(cudaStream_t s, unsigned long long* measure_bits)
   for (int n = top; n > ctop_; --n) {
     Level& F = lv_[n];
     LV<T> f = view<T>(F), c = view<T>(lv_[n - 1]);
-    // coarse corrections, and the FP32 correction of the defect loop, start from zero
-    bool zero_e = (n != top) || (sizeof(T) == 4);
+    // coarse corrections, and the FP32 correction of the defect loop, start from zero (a
+    // continuing FP32 cycle starts from the correction of the previous one)
+    bool zero_e = (n != top) || (sizeof(T) == 4 && !cont);
     if (tile_ok(F.Nx, F.Ny, F.power2, pre, post)) {
       launch_down<T>(sizeof(T) == 8 ? F.shape64 : F.shape32, f, c, omega, zero_e ? 1 : 0, f.tmp, s);
       ++g_launches;
@@ -1124,7 +1125,8 @@ void Multigrid::enqueue_vcycle(cudaStream_t s, unsigned long long* measure_bits)
   // coarse block: the tabulated linear map when available, else the one-CTA kernel
   {
     const Level& Ltop = lv_[ctop_];
-    const CoarseDesc d = coarse_desc<T>(nullptr);
+    CoarseDesc d = coarse_desc<T>(nullptr);
+    if (cont && ctop_ == top) d.top_from_e = 1;
     const T* C = static_cast<const T*>(cmat_[sizeof(T) == 8 ? 0 : 1]);
     if (C && !d.top_from_e) {
       const int n = Ltop.Nx * Ltop.Ny;
@@ -1241,6 +1243,7 @@ int Multigrid::build_graph(int prec) {
     enqueue_vcycle<double>(cap_, &st->bits);
   } else {
     enqueue_vcycle<float>(cap_, nullptr);
+    for (int q = 1; q < opt_.fp32_inner; ++q) enqueue_vcycle<float>(cap_, nullptr, true);
     LV<double> f = view<double>(F);
     defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, cap_>>>(f, F.e, F.res, &st->iters, 0, F.e32, F.pitch, F.rhs32, 1,
                                                    &st->bits);
@@ -1360,6 +1363,7 @@ int Multigrid::solve_once(double* pi, const double* rhs, double tol, int maxiter
         enqueue_vcycle<double>(s_, &st->bits);
       } else {
         enqueue_vcycle<float>(s_, nullptr);
+        for (int q = 1; q < opt_.fp32_inner; ++q) enqueue_vcycle<float>(s_, nullptr, true);
         defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f, F.e, F.res, nullptr, it, F.e32, F.pitch, F.rhs32, 1,
                                                      &st->bits);
       }
@@ -1402,7 +1406,7 @@ int Multigrid::solve_once(double* pi, const double* rhs, double tol, int maxiter
   return h.iters;
 }
 
-template void Multigrid::enqueue_vcycle<double>(cudaStream_t, unsigned long long*);
-template void Multigrid::enqueue_vcycle<float>(cudaStream_t, unsigned long long*);
+template void Multigrid::enqueue_vcycle<double>(cudaStream_t, unsigned long long*, bool);
+template void Multigrid::enqueue_vcycle<float>(cudaStream_t, unsigned long long*, bool);
 
 }  // namespace pawsim

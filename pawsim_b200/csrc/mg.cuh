@@ -21,6 +21,8 @@ struct CoarseDesc;   // the coarse block's launch descriptor (mg.cu)
 
 struct MGOptions {
   int fp32_cycles = 0;     // 0: FP64 V-cycles, 1: FP32 V-cycles in FP64 defect correction
+  int fp32_inner = 1;      // FP32 V-cycles per defect-correction step (each after the first
+                           // continues from the correction the previous one left)
   int pre = 1, post = 1;   // red-black sweeps before and after the coarse correction
   double omega_rb = 1.0;   // smoother weight
   int full_mg = 0;         // use_fullMG: nested iteration from the coarsest level
@@ -75,7 +77,8 @@ class Multigrid {
   };
 
  private:
-  template <typename T> void enqueue_vcycle(cudaStream_t s, unsigned long long* measure_bits);
+  // cont: an FP32 cycle that continues from the current correction instead of zero
+  template <typename T> void enqueue_vcycle(cudaStream_t s, unsigned long long* measure_bits, bool cont = false);
   int solve_once(double* pi, const double* rhs, double tol, int maxiters, double* maxres_out);
   int nsolves_ = 0;
   bool omega_tuned_ = false;

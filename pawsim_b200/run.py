@@ -40,6 +40,7 @@ def main(argv=None):
     ap.add_argument("--solver", type=int, default=1)
     ap.add_argument("--mg-fp32", action="store_true")
     ap.add_argument("--pi-guess", type=int, default=0, help="1: extrapolated first guess of the solves")
+    ap.add_argument("--fp32-inner", type=int, default=1, help="FP32 V-cycles per defect-correction step")
     ap.add_argument("--mg-tile", type=int, default=0, help="0 autotune, 1..4 force a tile shape, 5 strips")
     ap.add_argument("--mg-omega", type=float, default=-1.0, help="red-black weight; negative: chosen by the solver")
     ap.add_argument("--mg-pre", type=int, default=1)
@@ -73,7 +74,7 @@ def main(argv=None):
                 inputs.add_tracer(p, scheme=a.tracer, relax_days=100.0, K2=100.0)
             cfg = inputs.read_config(p)
         m = Model(cfg, mg_fp32=int(a.mg_fp32), mg_tile=a.mg_tile, mg_omega=a.mg_omega, mg_pre=a.mg_pre,
-                  mg_post=a.mg_post, pi_guess=a.pi_guess)
+                  mg_post=a.mg_post, pi_guess=a.pi_guess, mg_fp32_inner=a.fp32_inner)
         t0 = time.perf_counter()
         def diagnostics():
             if a.averages:

@@ -104,6 +104,34 @@ def test_mg_tiled_levels_tolerance(tmp_path, oracle_mod, lib, fp32, kind, kw):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("inner", [2, 4])
+@pytest.mark.parametrize("kind,kw", [
+    ("gyre", dict(N=16, solver=1, tol=1e-13, dt=900.0)),
+    ("gyre", dict(N=128, solver=1, tol=1e-13, dt=900.0)),
+    ("jets", dict(N=64, solver=1, tol=1e-13, dt=100.0)),
+], ids=["gyre16", "gyre128", "jets64"])
+def test_mg_fp32_inner_cycles_tolerance(tmp_path, oracle_mod, lib, inner, kind, kw):
+    """Several FP32 V-cycles per FP64 defect-correction step (each continuing from the
+    correction the previous one left; on the 16 x 16 grid the whole hierarchy is the one-CTA
+    coarse block): the solves still stop on the reference's test and the states stay within
+    1e-9 of the oracle's serial multigrid at tol 1e-13 over 6 steps."""
+    _, cfg, f = make_setup(tmp_path, kind, **kw)
+    o = oracle_mod.Oracle(cfg, f)
+    m = lib.Model(cfg, f, mg_fp32=1, mg_fp32_inner=inner)
+    o.prelim()
+    m.prelim()
+    for n in range(1, 7):
+        o.integrator_step(n)
+        o.pressure(True)
+        st = m.step(n)
+        assert 1 <= st["iters"] < 80, st
+        assert st["stop_measure"] <= 1e-13
+    s_o, s_g = o.state(), m.state()
+    for var in ("u", "v", "h"):
+        assert rel_l2(s_g[var], s_o[var]) < 1e-9, (var, rel_l2(s_g[var], s_o[var]))
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("fp32", [0, 1], ids=["fp64", "fp32"])
 @pytest.mark.parametrize("kind,kw", [
     ("gyre", dict(N=256, solver=1, tol=1e-12, dt=450.0)),
