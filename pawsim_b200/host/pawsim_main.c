@@ -20,7 +20,7 @@
  *     set (pawsim.c:100-108, 515-522).
  * Exit status 0 on success, 1 on any failure, with the message on stderr.
  * GPU-only controls come from the environment: PAWSIM_GPU_MG_FP32=1 runs FP32 V-cycles
- * inside FP64 defect correction; PAWSIM_GPU_SYNC_OUTPUT=1 writes each save before the next
+ * inside FP64 defect correction (PAWSIM_GPU_MG_FP32_INNER of them per defect step); PAWSIM_GPU_SYNC_OUTPUT=1 writes each save before the next
  * step instead of from the background writer (the default: the state is snapshotted on the
  * device and a second thread writes the files while the model steps on).
  */
@@ -836,6 +836,7 @@ int main (int argc, char ** argv)
   g.tau_period = c.tauPeriod; g.wdia_period = c.wDiaPeriod; g.conv_diff = c.convDiff;
   g.pi_tol = c.tol; g.sor_rp = c.SOR_rp; g.omega_mg = c.omega_MG;
   g.mg_fp32 = getenv("PAWSIM_GPU_MG_FP32") ? atoi(getenv("PAWSIM_GPU_MG_FP32")) : 0;
+  g.mg_fp32_inner = getenv("PAWSIM_GPU_MG_FP32_INNER") ? atoi(getenv("PAWSIM_GPU_MG_FP32_INNER")) : 0;
   g.mg_pre = 1; g.mg_post = 1; g.mg_omega = -1.0;   /* weight chosen by the solver */
   g.serial_sums = -1;
   g.mg_tile = 0;
