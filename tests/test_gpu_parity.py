@@ -132,6 +132,27 @@ def test_mg_fp32_inner_cycles_tolerance(tmp_path, oracle_mod, lib, inner, kind, 
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("solver", [1, 2], ids=["mg", "dmg"])
+def test_extrapolated_first_guess_tolerance(tmp_path, oracle_mod, lib, solver):
+    """pi_guess = 1 starts each multigrid solve (from the third on) at 2 pi(n-1) - pi(n-2):
+    the stopping test is the reference's, so the states stay within 1e-9 of the oracle's
+    serial solver at tol 1e-13 over 8 steps."""
+    _, cfg, f = make_setup(tmp_path, "gyre", N=64, solver=solver, tol=1e-13, dt=900.0)
+    o = oracle_mod.Oracle(cfg, f)
+    m = lib.Model(cfg, f, pi_guess=1)
+    o.prelim()
+    m.prelim()
+    for n in range(1, 9):
+        o.integrator_step(n)
+        o.pressure(True)
+        st = m.step(n)
+        assert 1 <= st["iters"] < 200, st
+    s_o, s_g = o.state(), m.state()
+    for var in ("u", "v", "h"):
+        assert rel_l2(s_g[var], s_o[var]) < 1e-9, (var, rel_l2(s_g[var], s_o[var]))
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("fp32", [0, 1], ids=["fp64", "fp32"])
 @pytest.mark.parametrize("kind,kw", [
     ("gyre", dict(N=256, solver=1, tol=1e-12, dt=450.0)),
