@@ -459,6 +459,8 @@ def main():
         "pressure_ms_per_step": float(np.mean(solve_ms)),
         "vcycles_per_step": float(np.mean(iters)),
         "gpu_launches": int(launches),
+        # the secondary throughput of the metric: grid-point-layer updates per second, all ranks
+        "gpl_updates_per_s": world * args.steps * ncell * cfg.Nlay / sec,
         "e2e": {"value": e2e_value, "unit": "sim-days/s", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
