@@ -112,6 +112,7 @@ BUD_CASES = {
     "jets_diadiff_budget": (inputs.jets, dict(N=16, dt=100.0, solver=0, tol=1e-10),
                             dict(scheme=2, relax_days=100.0, amp=0.05, buoyancy=True,
                                  diadiff=dict(kappa=1e-4, flux=1e-9, conv_diff=1e-2))),
+    "gyre_relax_fbaro_budget": (inputs.gyre, dict(N=16, Ny=12, dt=900.0, solver=0, tol=1e-10), "relax"),
     "gyre_fractions_budget": (inputs.gyre, dict(N=20, Ny=12, dt=600.0, solver=0,
                                                 extra=dict(hsml=1500.0, hmin_surf=5.0, hbbl=500.0, hmin_bot=10.0,
                                                            linDragSurf=1e-4, thicknessScheme=3)), None),
@@ -128,6 +129,34 @@ def add_tracer_and_mixing(p, tkw):
     inputs.add_tracer(p, **tkw)
     if dd:
         inputs.add_diapycnal_diffusion(p, **dd)
+
+
+def add_relax_fbaro(p, days=20.0, fbaro=1e-6, seed=5):
+    """Velocity restoring (uRelax/vRelax towards a seeded field on `days`, uTime/vTime) and a
+    barotropic body force (FbaroX/FbaroY) added to an existing set-up."""
+    cfg = inputs.read_config(p)
+    v = cfg.values
+    L, Nx, Ny = v["Nlay"], v["Nx"], v["Ny"]
+    rng = np.random.default_rng(seed)
+    d = os.path.dirname(p)
+    ur = 0.05 * rng.standard_normal((L, Ny, Nx))
+    vr = 0.05 * rng.standard_normal((L, Ny, Nx))
+    t = np.full((L, Ny, Nx), days * 86400.0)
+    inputs.write_data(os.path.join(d, "uRelax.dat"), inputs._layer_stack(ur))
+    inputs.write_data(os.path.join(d, "vRelax.dat"), inputs._layer_stack(vr))
+    inputs.write_data(os.path.join(d, "uTime.dat"), inputs._layer_stack(t))
+    inputs.write_data(os.path.join(d, "vTime.dat"), inputs._layer_stack(t))
+    inputs.write_data(os.path.join(d, "FbaroX.dat"), fbaro * (1 + 0.1 * rng.standard_normal((Ny, Nx))))
+    inputs.write_data(os.path.join(d, "FbaroY.dat"), fbaro * 0.1 * rng.standard_normal((Ny, Nx)))
+    params = {}
+    with open(p) as fh:
+        for line in fh:
+            parts = line.split()
+            if len(parts) >= 2:
+                params[parts[0]] = parts[1]
+    params.update(uRelaxFile="uRelax.dat", vRelaxFile="vRelax.dat", uTimeFile="uTime.dat", vTimeFile="vTime.dat",
+                  FbaroXFile="FbaroX.dat", FbaroYFile="FbaroY.dat")
+    inputs.write_param_file(p, params)
 
 
 def make(name, fn, kw, outdir):
@@ -241,7 +270,7 @@ def make_ez(name, fn, kw, every, outdir):
         np.savez_compressed(os.path.join(outdir, name + ".npz"), **rec)
 
 
-def make_budget(name, fn, kw, tkw, outdir):
+def make_budget(name, fn, kw, tkw, outdir, relax=False):
     """Inputs and the reference's budget files of every completed window."""
     with tempfile.TemporaryDirectory() as d:
         kw = dict(kw)
@@ -253,6 +282,8 @@ def make_budget(name, fn, kw, tkw, outdir):
         p = fn(os.path.join(d, "in"), Nt=BUD_NSTEPS, savefrequency=BUD_NSTEPS * dt, extra=extra, **kw)
         if tkw is not None:
             add_tracer_and_mixing(p, tkw)
+        if relax:
+            add_relax_fbaro(p)
         cfg = inputs.read_config(p)
         out = os.path.join(d, "out")
         os.makedirs(out)
@@ -294,5 +325,8 @@ if __name__ == "__main__":
     for name, (fn, kw, tkw) in BUD_CASES.items():
         if len(sys.argv) > 1 and name not in sys.argv[1:]:
             continue
-        make_budget(name, fn, kw, tkw, HERE)
+        if tkw == "relax":
+            make_budget(name, fn, kw, None, HERE, relax=True)
+        else:
+            make_budget(name, fn, kw, tkw, HERE)
         print("wrote", name)

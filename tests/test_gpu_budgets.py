@@ -11,7 +11,8 @@ file must equal the reference binary's bit for bit: walled gyre with wind and dr
 four-layer full-physics set-up (bathymetry, sponge restoring, w_dia, A4), HK83 momentum and
 thickness with A4, a periodic jet with a KT00 tracer, quadratic bottom and surface drag with
 wind feedback, surface/bottom layer fractions with linear surface drag and KT00 thickness, and
-a buoyant tracer with diapycnal diffusion and convective mixing (diaDiff and diaVisc terms)."""
+a buoyant tracer with diapycnal diffusion and convective mixing (diaDiff and diaVisc terms),
+and velocity restoring with a barotropic body force (relaxation and baroForcing terms)."""
 import os
 import subprocess
 
@@ -25,7 +26,7 @@ pytestmark = pytest.mark.gpu
 
 DRIVER = os.path.join(ROOT, "pawsim_b200", "bin", "PAWSIM_B200.exe")
 CASES = ["gyre_sor_budget", "full_sor_budget", "gyre_hk83_a4_budget", "jets_tracer_budget", "gyre_quad_budget",
-         "gyre_fractions_budget", "jets_diadiff_budget"]
+         "gyre_fractions_budget", "jets_diadiff_budget", "gyre_relax_fbaro_budget"]
 
 
 @pytest.mark.parametrize("name", CASES)
