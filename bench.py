@@ -139,36 +139,60 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_reference(param, steps, label):
-    """Time the reference's serial step with ref_harness; returns (s/step, sample text)."""
+# the reference arm times at most this many steps (about 4 s each at 2048^2 on one core), so
+# that a run with many --steps still ends within a few minutes; the line states the count
+REF_MAX_STEPS = 40
+
+
+def cpu_reference(param, warmup, steps):
+    """Run the reference's serial step with ref_harness for warmup + steps steps after its
+    set-up; returns (seconds of each of the last `steps` steps, sample text)."""
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
     if not os.path.exists(exe):
         return None, "oracle/_ref/ref_harness not built"
-    r = subprocess.run([exe, param, str(steps)], capture_output=True, text=True, timeout=1800)
+    r = subprocess.run([exe, param, str(warmup + steps)], capture_output=True, text=True, timeout=1800)
     if r.returncode != 0:
         return None, "ref_harness failed: " + r.stderr.strip()[-200:]
-    secs = [json.loads(l)["seconds"] for l in r.stdout.splitlines() if '"phase": "step"' in l]
-    if not secs:
-        return None, "no steps timed"
-    return secs, f"{len(secs)} {label} steps of the {N_GRID}x{N_GRID}x2 gyre after set-up, 1 thread"
+    rows = [json.loads(l) for l in r.stdout.splitlines() if '"phase": "step"' in l]
+    timed = [row for row in rows if row["n"] > warmup]
+    if len(timed) != steps:
+        return None, f"ref_harness timed {len(timed)} of {steps} steps"
+    first, last = timed[0]["n"], timed[-1]["n"]
+    return ([row["seconds"] for row in timed],
+            f"steps {first}..{last} of the {N_GRID}x{N_GRID}x2 gyre (after {warmup} untimed steps and the "
+            f"set-up; steps 1-3 are the AB1/AB2 start-up), reference serial build, 1 thread")
+
+
+def bench_config(world, mg_fp32=0):
+    return {"workload": f"double gyre {N_GRID}x{N_GRID}x2, dt={DT} s, MG tol={TOL}",
+            "pressure": "GPU multigrid, " + ("FP32 V-cycles in FP64 defect correction"
+                                             if mg_fp32 else "FP64 V-cycles"),
+            "l2": "inputs larger than L2 (state 201 MB + history 403 MB)",
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"}
 
 
 def run_reference_arm(args, rank, world):
+    """The reference's own serial build of the same step (oracle/_ref/ref_harness, built from
+    the reference sources) on rank 0's host cores: exactly --warmup untimed steps, then
+    --steps timed steps (at most REF_MAX_STEPS; "steps" states the count timed). The reference
+    has no threaded build and no MPI compiler exists on these hosts, so it runs on one core."""
     if rank != 0:
         return
+    steps = min(args.steps, REF_MAX_STEPS)
     with tempfile.TemporaryDirectory() as d:
         param = make_inputs(d)
-        nsteps = args.warmup + min(args.steps, 8)
-        secs, sample = cpu_reference(param, nsteps, "reference")
+        secs, sample = cpu_reference(param, args.warmup, steps)
     line = {"metric": METRIC, "unit": "sim-days/s", "impl": "reference", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": f"double gyre {N_GRID}x{N_GRID}x2, dt={DT} s, MG tol={TOL}"}}
+            "steps": steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded double-gyre inputs of the headline configuration)",
+            "config": bench_config(world, args.mg_fp32)}
+    if steps != args.steps:
+        line["steps_requested"] = args.steps
     if secs is None:
         line.update({"unavailable": sample})
     else:
-        timed = secs[args.warmup:] or secs
-        per = float(np.mean(timed))
+        per = float(np.mean(secs))
         v = DT / 86400.0 / per
         line.update({"value": v, "ms_per_step": per * 1e3,
                      "cpu_baseline": {"value": v, "unit": "sim-days/s", "cores": 1,
@@ -451,11 +475,7 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded double-gyre inputs of the headline configuration)",
-        "config": {"workload": f"double gyre {N_GRID}x{N_GRID}x2, dt={DT} s, MG tol={TOL}",
-                   "pressure": "GPU multigrid, " + ("FP32 V-cycles in FP64 defect correction"
-                                                    if args.mg_fp32 else "FP64 V-cycles"),
-                   "l2": "inputs larger than L2 (state 201 MB + history 403 MB)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "config": bench_config(world, args.mg_fp32),
         "pressure_ms_per_step": float(np.mean(solve_ms)),
         "vcycles_per_step": float(np.mean(iters)),
         "gpu_launches": int(launches),
@@ -500,7 +520,8 @@ def main():
     if ws is not None:
         line["pressure_learned_fp32_vs_plain_fp64"] = ws
     if rank == 0 and not args.no_cpu_baseline:
-        secs, sample = cpu_reference(param, 2, "reference")
+        # a bounded sample in steady state: steps 4 and 5 (after the AB1/AB2 start-up)
+        secs, sample = cpu_reference(param, 3, 2)
         if secs is not None:
             line["cpu_baseline"] = {"value": DT / 86400.0 / float(np.mean(secs)), "unit": "sim-days/s",
                                     "cores": 1, "kind": "reference", "sample": sample}

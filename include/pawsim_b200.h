@@ -113,6 +113,17 @@ typedef struct pawsim_gpu_config
    * Each after the first continues from the correction the previous one left, so a step
    * reduces the defect further before the FP64 residual pass; stats.iters counts steps. */
   int mg_fp32_inner;
+  /* Failure reporting (no counterpart in the reference, which prints "WARNING: PAWSIM pressure
+   * solve reached maxiters" and runs on, to NaN if the state blows up). Both are off (0) by
+   * default, which keeps the reference's behaviour. check_nonfinite = K > 0: the fused step
+   * kernel raises a device flag when a new u, v or h is not finite (NaN or infinite); every K-th
+   * call of pawsim_gpu_step / pawsim_gpu_integrator_step reads and clears it and returns
+   * PAWSIM_GPU_ENONFINITE when it was raised. fail_on_maxiters = 1: a rigid-lid solve that
+   * stopped at maxiters makes pawsim_gpu_step / pawsim_gpu_pressure_correct return
+   * PAWSIM_GPU_ENOTCONVERGED. In both cases the step itself completes as the reference's does
+   * (the state is advanced and the report filled), so the caller may inspect or continue. */
+  int check_nonfinite;
+  int fail_on_maxiters;
 } pawsim_gpu_config;
 
 enum

@@ -36,10 +36,17 @@ class OrcPstats(ctypes.Structure):
                 ("div_rms", ctypes.c_double)]
 
 
+def reference_source() -> str:
+    """The reference's model_code directory: $PAWSIM_REF_SRC, or model_code of a directory
+    named `reference` beside this repository."""
+    return os.environ.get("PAWSIM_REF_SRC") or os.path.join(
+        os.path.dirname(os.path.dirname(HERE)), "reference", "model_code")
+
+
 def build(ref: bool = True) -> None:
     """Compile liboracle.so, and the reference build when its sources are present."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    src = os.environ.get("PAWSIM_REF_SRC", "/root/reference/model_code")
+    src = reference_source()
     if ref and os.path.isdir(src):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={src}"], check=True)
 

@@ -25,7 +25,7 @@
 namespace pawsim {
 
 static thread_local char g_err[512] = "";
-long long g_launches = 0;
+std::atomic<long long> g_launches{0};
 
 int set_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
   snprintf(g_err, sizeof(g_err), "CUDA error %s (%s) in %s at %s:%d", cudaGetErrorName(e),
@@ -102,6 +102,8 @@ struct Model {
   double *pi, *rhs, *work, *scratch, *dsum;
   unsigned long long* slots;
   int* diters;
+  int* nonfinite = nullptr;   // raised by the fused kernel when a new state value is not finite
+  int nf_calls = 0;           // steps since the flag was last read (check_nonfinite)
   Operator op;
   double gg[LMAX], geff[LMAX];
   std::vector<double> hhs_host, hhb_host;
@@ -204,6 +206,8 @@ static int create(const pawsim_gpu_config* cfg, Model** out) {
     return fail(PAWSIM_GPU_EBADCONFIG, "Unknown or unsupported numerical scheme identifier");
   if (c.use_tracer && (c.K2 < 0 || c.K4 < 0)) return fail(PAWSIM_GPU_EBADCONFIG, "K2 and K4 must be non-negative");
   if (c.solver < 0 || c.solver > 2) return fail(PAWSIM_GPU_EBADCONFIG, "Unknown pressureSolver identifier");
+  if (c.check_nonfinite < 0 || c.fail_on_maxiters < 0 || c.fail_on_maxiters > 1)
+    return fail(PAWSIM_GPU_EBADCONFIG, "check_nonfinite must be >= 0 and fail_on_maxiters 0 or 1");
   Model* m = new Model();
   m->c = c;
   m->Nx = c.Nx; m->Ny = c.Ny; m->L = c.Nlay;
@@ -244,6 +248,7 @@ static int create(const pawsim_gpu_config* cfg, Model** out) {
   ok &= (m->dsum = m->alloc<double>(8)) != nullptr;
   ok &= (m->slots = m->alloc<unsigned long long>(2)) != nullptr;
   ok &= (m->diters = m->alloc<int>(1)) != nullptr;
+  if (c.check_nonfinite > 0) ok &= (m->nonfinite = m->alloc<int>(1)) != nullptr;
   m->op.opitch = round_up(c.Nx + 1, 32);
   ok &= (m->op.Ow = m->alloc<double>((size_t)(c.Ny + 1) * m->op.opitch)) != nullptr;
   ok &= (m->op.Os = m->alloc<double>((size_t)(c.Ny + 1) * m->op.opitch)) != nullptr;
@@ -541,7 +546,33 @@ static TendParams base_params(Model* m) {
   p.use_buoy = c.use_buoyancy;
   p.b = c.use_tracer ? m->b[m->cur] : nullptr;
   p.conv_diff = c.conv_diff;
+  p.nonfinite = m->nonfinite;
   return p;
+}
+
+// check_nonfinite: every K-th step reads and clears the flag the fused kernel raises
+static int check_state_finite(Model* m) {
+  if (!m->nonfinite || ++m->nf_calls < m->c.check_nonfinite) return 0;
+  m->nf_calls = 0;
+  int flag = 0;
+  PAWSIM_CUDA_OK(cudaMemcpyAsync(&flag, m->nonfinite, sizeof(int), cudaMemcpyDeviceToHost, m->s));
+  PAWSIM_CUDA_OK(cudaMemsetAsync(m->nonfinite, 0, sizeof(int), m->s));
+  PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
+  if (flag) {
+    char msg[160];
+    snprintf(msg, sizeof(msg), "the state became non-finite (NaN or Inf) at or before model time %.9g s", m->t);
+    return fail(PAWSIM_GPU_ENONFINITE, msg);
+  }
+  return 0;
+}
+
+// fail_on_maxiters: a rigid-lid solve that stopped at maxiters (the reference's warning case,
+// pawsim.c:488-491)
+static int check_converged(const Model* m, int iters) {
+  if (!m->c.fail_on_maxiters || !m->c.use_rl || iters < m->c.maxiters) return 0;
+  char msg[160];
+  snprintf(msg, sizeof(msg), "the pressure solve reached maxiters (%d) at model time %.9g s", m->c.maxiters, m->t);
+  return fail(PAWSIM_GPU_ENOTCONVERGED, msg);
 }
 
 // the plain fused kernel, or its budget build when budgets accumulate or buoyancy couples
@@ -688,6 +719,7 @@ static int pressure_correct(Model* m, int update_diags, pawsim_gpu_stats* st) {
     if (m->ws && m->ws->before_solve(m->pi, m->rhs, m->mg, (m->nn_mode & 2) != 0, m->s) < 0)
       return fail(PAWSIM_GPU_ECUDA, "warm-start guess failed");
     iters = m->mg->solve(m->pi, m->pitch, m->rhs, m->pitch, m->c.pi_tol, m->c.maxiters, &mres);
+    if (iters < 0) return fail(PAWSIM_GPU_ECUDA, "multigrid solve failed (graph build or stream error)");
     local.stop_measure = mres;
     local.mg_omega = m->mg->omega();
     PAWSIM_CUDA_OK(cudaEventRecord(m->ev1, m->s));
@@ -712,6 +744,7 @@ static int pressure_correct(Model* m, int update_diags, pawsim_gpu_stats* st) {
     // grids without a first clean 2:1 coarsening use the gathered multigrid (pressure.c:2136-2148)
     double mres = 0;
     iters = m->mg->solve(m->pi, m->pitch, m->rhs, m->pitch, m->c.pi_tol, m->c.maxiters, &mres);
+    if (iters < 0) return fail(PAWSIM_GPU_ECUDA, "multigrid solve failed (graph build or stream error)");
     local.stop_measure = mres;
     local.mg_omega = m->mg->omega();
     local.fallback = 1;
@@ -791,13 +824,16 @@ int pawsim_gpu_tendency_eval(pawsim_gpu* h) {
 
 int pawsim_gpu_integrator_step(pawsim_gpu* h, unsigned n) {
   if (!h) return PAWSIM_GPU_EBADCONFIG;
-  return integrator_step(h->m, n, false);
+  int r = integrator_step(h->m, n, false);
+  if (r) return r;
+  return check_state_finite(h->m);
 }
 
 int pawsim_gpu_pressure_correct(pawsim_gpu* h, int update_diags, pawsim_gpu_stats* st) {
   if (!h) return PAWSIM_GPU_EBADCONFIG;
   int r = pressure_correct(h->m, update_diags, st);
-  return r < 0 ? r : 0;
+  if (r < 0) return r;
+  return check_converged(h->m, r);
 }
 
 int pawsim_gpu_prelim(pawsim_gpu* h, pawsim_gpu_stats* st) {
@@ -820,8 +856,11 @@ int pawsim_gpu_step(pawsim_gpu* h, unsigned n, pawsim_gpu_stats* st) {
   if (!h) return PAWSIM_GPU_EBADCONFIG;
   int r = integrator_step(h->m, n, true);
   if (r) return r;
-  r = pressure_correct(h->m, 1, st);
-  return r < 0 ? r : 0;
+  const int iters = pressure_correct(h->m, 1, st);
+  if (iters < 0) return iters;
+  r = check_state_finite(h->m);
+  if (r) return r;
+  return check_converged(h->m, iters);
 }
 
 int pawsim_gpu_run(pawsim_gpu* h, unsigned n0, unsigned nsteps, pawsim_gpu_stats* st) {
@@ -1028,6 +1067,7 @@ int pawsim_gpu_solve_mg(pawsim_gpu* h, pawsim_gpu_stats* st) {
   double mres = 0;
   PAWSIM_CUDA_OK(cudaEventRecord(m->ev0, m->s));
   int it = m->mg->solve(m->pi, m->pitch, m->rhs, m->pitch, m->c.pi_tol, m->c.maxiters, &mres);
+  if (it < 0) return fail(PAWSIM_GPU_ECUDA, "multigrid solve failed (graph build or stream error)");
   PAWSIM_CUDA_OK(cudaEventRecord(m->ev1, m->s));
   PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
   if (st) {

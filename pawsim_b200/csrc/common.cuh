@@ -10,6 +10,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 namespace pawsim {
 
 // Boundary behaviour of a field along one axis (model_code/field.c:158-241):
@@ -107,6 +109,7 @@ __device__ __forceinline__ double div_rn(double x, double d, double r) {
 
 namespace pawsim {
 int set_cuda_error(cudaError_t e, const char* what, const char* file, int line);
-// kernels launched by this library since load (reported by pawsim_gpu_launch_count)
-extern long long g_launches;
+// kernels launched by this library since load (reported by pawsim_gpu_launch_count); atomic
+// because entry points without a model handle may be called from several host threads
+extern std::atomic<long long> g_launches;
 }

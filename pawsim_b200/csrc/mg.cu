@@ -180,6 +180,32 @@ __global__ void prolong_correct_kernel(LV<T> f, LV<T> c, int power2, int wew, in
   f.e[IX(f, i, j)] -= prolong_at<T>(i, j, f.Nx, f.Ny, c.Nx, c.Ny, power2, wew, wns, ec);
 }
 
+// use_fullMG: restriction of a level's right-hand side to the next coarser level
+// (restrict_MG of multigrid.c:1248-1254; 2x2 mean or area-weighted)
+__global__ void restrict_rhs_kernel(LV<double> f, LV<double> c, int power2) {
+  int ic = blockIdx.x * blockDim.x + threadIdx.x;
+  int jc = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ic >= c.Nx || jc >= c.Ny) return;
+  double v;
+  if (power2) {
+    const double* r = f.rhs + IX(f, 2 * ic, 2 * jc);
+    v = 0.25 * (r[0] + r[1] + r[f.pitch] + r[f.pitch + 1]);
+  } else {
+    v = restrict_general_at<double>(f.Nx, f.Ny, c.Nx, c.Ny, ic, jc, f.rhs, f.pitch);
+  }
+  c.rhs[IX(c, ic, jc)] = v;
+}
+
+// use_fullMG: the coarser solution interpolated onto this level, replacing its values
+// (interpolate_MG into the level's pi, multigrid.c:1259-1265)
+__global__ void prolong_set_kernel(LV<double> f, LV<double> c, int power2, int wew, int wns) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= f.Nx || j >= f.Ny) return;
+  auto ec = [&](int a, int b) { return c.e[IX(c, a, b)]; };
+  f.e[IX(f, i, j)] = prolong_at<double>(i, j, f.Nx, f.Ny, c.Nx, c.Ny, power2, wew, wns, ec);
+}
+
 // ---------------------------------------------------------------- fused tile kernels
 
 // max over the block (warp shuffles, then the warps' maxima), one atomic per block
@@ -902,7 +928,8 @@ struct Multigrid::Graphs {
   cudaGraph_t graph[2] = {nullptr, nullptr};
   cudaGraphExec_t exec[2] = {nullptr, nullptr};
   cudaGraphConditionalHandle handle[2];
-  int pre = -1, post = -1;
+  // options the graphs were captured with; any change rebuilds them
+  int pre = -1, post = -1, inner = -1;
   double omega = -1;
 };
 
@@ -1036,14 +1063,15 @@ Multigrid::~Multigrid() {
 }
 
 template <typename T>
-CoarseDesc Multigrid::coarse_desc(void* unit_out) const {
+CoarseDesc Multigrid::coarse_desc(void* unit_out, int root) const {
   CoarseDesc dd;
   memset(&dd, 0, sizeof(dd));
   CoarseDesc* d = &dd;
   const int top = (int)lv_.size() - 1;
-  d->n = ctop_ + 1;
+  const int btop = root >= 0 ? root : ctop_;
+  d->n = btop + 1;
   int total = 0;
-  for (int m = 0; m <= ctop_; ++m) {
+  for (int m = 0; m <= btop; ++m) {
     const Level& L = lv_[m];
     d->Nx[m] = L.Nx; d->Ny[m] = L.Ny; d->pitch[m] = L.pitch; d->power2[m] = L.power2 ? 1 : 0;
     d->lgx[m] = -1;
@@ -1055,11 +1083,12 @@ CoarseDesc Multigrid::coarse_desc(void* unit_out) const {
     else { d->Ow[m] = L.Ow32; d->Os[m] = L.Os32; d->rO[m] = L.rOsum32; }
   }
   d->total = total;
-  const Level& Ltop = lv_[ctop_];
+  const Level& Ltop = lv_[btop];
   d->top_rhs = sizeof(T) == 8 ? (const void*)Ltop.rhs : (const void*)Ltop.rhs32;
   d->top_e = sizeof(T) == 8 ? (void*)Ltop.e : (void*)Ltop.e32;
-  // when the coarse block is the whole problem, the FP64 solve iterates on pi itself
-  d->top_from_e = (ctop_ == top && sizeof(T) == 8) ? 1 : 0;
+  // when the coarse block is the whole problem, the FP64 solve iterates on pi itself; a block
+  // rooted at a lower level (the nested iteration) iterates on that level's solution
+  d->top_from_e = ((btop == top || root >= 0) && sizeof(T) == 8) ? 1 : 0;
   d->wew = wew_; d->wns = wns_; d->pre = opt_.pre; d->post = opt_.post;
   d->unit_out = unit_out;
   d->unit_n = Ltop.Nx * Ltop.Ny;
@@ -1067,10 +1096,11 @@ CoarseDesc Multigrid::coarse_desc(void* unit_out) const {
 }
 
 template <typename T>
-size_t Multigrid::coarse_smem() const {
+size_t Multigrid::coarse_smem(int root) const {
+  const int btop = root >= 0 ? root : ctop_;
   int total = 0;
-  for (int m = 0; m <= ctop_; ++m) total += lv_[m].Nx * lv_[m].Ny;
-  return (size_t)(5 * total + lv_[ctop_].Nx * lv_[ctop_].Ny) * sizeof(T);
+  for (int m = 0; m <= btop; ++m) total += lv_[m].Nx * lv_[m].Ny;
+  return (size_t)(5 * total + lv_[btop].Nx * lv_[btop].Ny) * sizeof(T);
 }
 
 // tabulate the coarse block's linear map for the current smoother options (once per
@@ -1096,11 +1126,24 @@ void Multigrid::tabulate_coarse(cudaStream_t s) {
 }
 
 template <typename T>
-void Multigrid::enqueue_vcycle(cudaStream_t s, unsigned long long* measure_bits, bool cont) {
-  const int top = (int)lv_.size() - 1;
+void Multigrid::enqueue_vcycle(cudaStream_t s, unsigned long long* measure_bits, bool cont, int root) {
+  const int finest = (int)lv_.size() - 1;
+  const int top = root >= 0 ? root : finest;
   const T omega = (T)opt_.omega_rb;
   const int pre = opt_.pre, post = opt_.post;
   bool measured = false;
+  if (top <= ctop_ && top < finest) {
+    // a cycle rooted inside the coarse block (nested iteration): one CTA from the level's e
+    CoarseDesc d = coarse_desc<T>(nullptr, top);
+    coarse_kernel<T><<<1, CT, coarse_smem<T>(top), s>>>(d, omega);
+    ++g_launches;
+    if (measure_bits) {
+      LV<double> f = view<double>(lv_[top]);
+      max_residual_kernel<<<g2(f.Nx, f.Ny), B2, 0, s>>>(f, measure_bits);
+      ++g_launches;
+    }
+    return;
+  }
   // down through the tiled levels
   for (int n = top; n > ctop_; --n) {
     Level& F = lv_[n];
@@ -1142,7 +1185,7 @@ void Multigrid::enqueue_vcycle(cudaStream_t s, unsigned long long* measure_bits,
     Level& F = lv_[n];
     LV<T> f = view<T>(F), c = view<T>(lv_[n - 1]);
     if (tile_ok(F.Nx, F.Ny, F.power2, pre, post)) {
-      unsigned long long* mb = (n == top) ? measure_bits : nullptr;
+      unsigned long long* mb = (n == top && top == finest) ? measure_bits : nullptr;
       LV<T> fin = f;
       fin.e = f.tmp;   // the pre-smoothed correction written by the down kernel
       launch_up<T>(sizeof(T) == 8 ? F.shape64 : F.shape32, fin, c, omega, wew_, wns_, mb, f.e, s);
@@ -1158,7 +1201,7 @@ void Multigrid::enqueue_vcycle(cudaStream_t s, unsigned long long* measure_bits,
     }
   }
   if (measure_bits && !measured) {
-    LV<double> f = view<double>(lv_.back());
+    LV<double> f = view<double>(lv_[top]);
     max_residual_kernel<<<g2(f.Nx, f.Ny), B2, 0, s>>>(f, measure_bits);
     ++g_launches;
   }
@@ -1323,10 +1366,42 @@ int Multigrid::solve(double* pi, int pitch, const double* rhs, int rhs_pitch, do
   return solve_once(pi, rhs, tol, maxiters, maxres_out);
 }
 
+// The nested iteration of full_MG (multigrid.c:1236-1270) below the finest level: the rhs is
+// restricted to every level, the 1 x 1 level holds zero (exactSolve_MG), and each finer level
+// starts from the interpolated coarser solution and runs FP64 V-cycles rooted at itself until
+// its own stopping measure is within tol (or maxiters). The finest level's start is left in pi;
+// its iteration is the regular solve. Host-sequenced: one measure read per coarse cycle.
+int Multigrid::full_mg_start(double tol, int maxiters) {
+  const int top = (int)lv_.size() - 1;
+  LoopState* st = reinterpret_cast<LoopState*>(dstate_);
+  for (int n = top; n > 0; --n) {
+    restrict_rhs_kernel<<<g2(lv_[n - 1].Nx, lv_[n - 1].Ny), B2, 0, s_>>>(view<double>(lv_[n]), view<double>(lv_[n - 1]),
+                                                                       lv_[n].power2 ? 1 : 0);
+    ++g_launches;
+  }
+  cudaMemsetAsync(lv_[0].e, 0, (size_t)lv_[0].pitch * lv_[0].Ny * sizeof(double), s_);
+  for (int n = 1; n <= top; ++n) {
+    LV<double> f = view<double>(lv_[n]), c = view<double>(lv_[n - 1]);
+    prolong_set_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f, c, lv_[n].power2 ? 1 : 0, wew_, wns_);
+    ++g_launches;
+    if (n == top) break;
+    double mres = tol + 1;
+    for (int it = 0; mres > tol && it < maxiters; ++it) {
+      cudaMemsetAsync(&st->bits, 0, sizeof(unsigned long long), s_);
+      enqueue_vcycle<double>(s_, &st->bits, false, n);
+      unsigned long long b = 0;
+      cudaMemcpyAsync(&b, &st->bits, sizeof(b), cudaMemcpyDeviceToHost, s_);
+      if (cudaStreamSynchronize(s_) != cudaSuccess) return -1;
+      memcpy(&mres, &b, sizeof(mres));
+    }
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 int Multigrid::solve_once(double* pi, const double* rhs, double tol, int maxiters, double* maxres_out) {
   const int prec = opt_.fp32_cycles ? 1 : 0;
   if (fine_pi_ != pi || fine_rhs_ != rhs || g_->pre != opt_.pre || g_->post != opt_.post ||
-      g_->omega != opt_.omega_rb) {
+      g_->omega != opt_.omega_rb || g_->inner != opt_.fp32_inner) {
     for (int p = 0; p < 2; ++p) {
       if (g_->exec[p]) cudaGraphExecDestroy(g_->exec[p]);
       if (g_->graph[p]) cudaGraphDestroy(g_->graph[p]);
@@ -1335,6 +1410,7 @@ int Multigrid::solve_once(double* pi, const double* rhs, double tol, int maxiter
     }
     g_->pre = opt_.pre;
     g_->post = opt_.post;
+    g_->inner = opt_.fp32_inner;
     g_->omega = opt_.omega_rb;
   }
   set_fine(pi, rhs);
@@ -1345,6 +1421,14 @@ int Multigrid::solve_once(double* pi, const double* rhs, double tol, int maxiter
   } else {
     tune<float>(s_);
     tabulate_coarse<float>(s_);
+  }
+  if (opt_.full_mg) {
+    // the nested cycles below the finest level run in FP64 with its tile shapes and map
+    if (prec == 1) {
+      tune<double>(s_);
+      tabulate_coarse<double>(s_);
+    }
+    if (full_mg_start(tol, maxiters) != 0) return -1;
   }
   if (getenv("PAWSIM_MG_HOST_LOOP")) {
     // host-driven loop with the same kernels (for profilers that do not see inside the
@@ -1406,7 +1490,7 @@ int Multigrid::solve_once(double* pi, const double* rhs, double tol, int maxiter
   return h.iters;
 }
 
-template void Multigrid::enqueue_vcycle<double>(cudaStream_t, unsigned long long*, bool);
-template void Multigrid::enqueue_vcycle<float>(cudaStream_t, unsigned long long*, bool);
+template void Multigrid::enqueue_vcycle<double>(cudaStream_t, unsigned long long*, bool, int);
+template void Multigrid::enqueue_vcycle<float>(cudaStream_t, unsigned long long*, bool, int);
 
 }  // namespace pawsim

@@ -77,13 +77,21 @@ class Multigrid {
   };
 
  private:
-  // cont: an FP32 cycle that continues from the current correction instead of zero
-  template <typename T> void enqueue_vcycle(cudaStream_t s, unsigned long long* measure_bits, bool cont = false);
+  // cont: an FP32 cycle that continues from the current correction instead of zero;
+  // root: the level the cycle starts from (-1: the finest; lower levels for the nested
+  // iteration of use_fullMG, whose solution lives in that level's e)
+  template <typename T> void enqueue_vcycle(cudaStream_t s, unsigned long long* measure_bits, bool cont = false,
+                                            int root = -1);
   int solve_once(double* pi, const double* rhs, double tol, int maxiters, double* maxres_out);
+  // use_fullMG: the nested iteration below the finest level (multigrid.c:1236-1270), leaving
+  // the interpolated coarse solution in the fine pi; returns 0 or -1 on a CUDA error
+  int full_mg_start(double tol, int maxiters);
   int nsolves_ = 0;
   bool omega_tuned_ = false;
-  template <typename T> CoarseDesc coarse_desc(void* unit_out) const;
-  template <typename T> size_t coarse_smem() const;
+  // the coarse block's descriptor; root >= 0 (at most ctop_) makes a block whose top is that
+  // level, iterated from its current e
+  template <typename T> CoarseDesc coarse_desc(void* unit_out, int root = -1) const;
+  template <typename T> size_t coarse_smem(int root = -1) const;
   template <typename T> void tabulate_coarse(cudaStream_t s);
   // the coarse block's linear map per precision (FP64, FP32) and the options it was made for
   void* cmat_[2] = {nullptr, nullptr};

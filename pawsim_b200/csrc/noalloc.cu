@@ -59,6 +59,13 @@ extern "C" int pawsim_pressure_rhs_noalloc(const double* u, const double* v, con
   if (thick_scheme != 0 && thick_scheme != 1) return PAWSIM_GPU_EUNSUPPORTED;
   // one partial per 8 rows plus the sum must fit in the static scratch
   if ((size_t)(Ny + 7) / 8 + 1 > (size_t)kNoallocScratch) return PAWSIM_GPU_EUNSUPPORTED;
+  // an error left pending by the caller's earlier, unrelated work is reported as such (and
+  // cleared) before anything is launched, so that the check after the launches below sees
+  // only this call's own errors
+  cudaError_t pending = cudaGetLastError();
+  if (pending != cudaSuccess)
+    return set_cuda_error(pending, "a CUDA error was pending before pawsim_pressure_rhs_noalloc", __FILE__,
+                          __LINE__);
   double* scratch = nullptr;
   int r = scratch_address(&scratch);
   if (r) return r;

@@ -69,6 +69,8 @@ struct TendParams {
   // 1829-1832; diapycnal.c:40-66, 104-114): also only in the budget build
   int use_buoy;
   double conv_diff;               // convDiff: added viscosity where the local g' < 0
+  // set to 1 when a new u, v or h is not finite (nullable: no check)
+  int* nonfinite;
 };
 
 // budget term indices (work.h:18-91)

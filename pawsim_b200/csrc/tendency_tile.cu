@@ -1012,6 +1012,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
     // after the update the reference re-imposes the wall face (field.c:173-176, 216-220)
     if (p.wall_ew && gi == 0) un = 0.0;
     if (p.wall_ns && gj == 0) vn = 0.0;
+    if (p.nonfinite && !(isfinite(un) && isfinite(vn) && isfinite(hn))) *p.nonfinite = 1;
     if (p.write_hist) {
       p.fu_out[o] = ru;
       p.fv_out[o] = rv;
