@@ -124,6 +124,13 @@ typedef struct pawsim_gpu_config
    * (the state is advanced and the report filled), so the caller may inspect or continue. */
   int check_nonfinite;
   int fail_on_maxiters;
+  /* Corner ghosts on x-periodic, y-walled grids (the only domain where the two builds of the
+   * reference differ): 0 reproduces the serial build (model_code/field.c:353-532 copies whole
+   * columns periodically before filling the wall rows, so the corner ghosts of a work array
+   * keep the values of its previous fill; those feed the PV, viscosity and face-thickness
+   * stencils next to the walls at the periodic seam); 1 uses the current values there, as the
+   * MPI build's y-then-x exchange does. Other domains are unaffected. */
+  int mpi_corners;
 } pawsim_gpu_config;
 
 enum

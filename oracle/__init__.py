@@ -27,7 +27,7 @@ class OrcCfg(ctypes.Structure):
         "Lx", "Ly", "dt", "tmin", "A2", "A4", "A2smag", "A4smag", "h0", "hsml", "hmin_surf",
         "hbbl", "hmin_bot", "KT00_sigma", "lin_drag", "quad_drag", "lin_drag_surf",
         "quad_drag_surf", "tau_period", "wdia_period", "conv_diff", "pi_tol", "sor_rp",
-        "omega_mg")]
+        "omega_mg")] + [("serial_corners", ctypes.c_int)]
 
 
 class OrcPstats(ctypes.Structure):
@@ -88,7 +88,7 @@ def lib():
     return _LIB
 
 
-def cfg_struct(cfg, pressure_timing=None) -> OrcCfg:
+def cfg_struct(cfg, pressure_timing=None, serial_corners=1) -> OrcCfg:
     v = cfg.values
     c = OrcCfg()
     c.Nx, c.Ny, c.Nlay = v["Nx"], v["Ny"], v["Nlay"]
@@ -113,18 +113,19 @@ def cfg_struct(cfg, pressure_timing=None) -> OrcCfg:
                  ("conv_diff", "convDiff"), ("pi_tol", "tol"), ("sor_rp", "SOR_rp"),
                  ("omega_mg", "omega_MG")):
         setattr(c, a, float(v[b]))
+    c.serial_corners = int(serial_corners)
     return c
 
 
 class Oracle:
     """One oracle model instance loaded from a parsed config and its input fields."""
 
-    def __init__(self, cfg, fields, pressure_timing=None):
+    def __init__(self, cfg, fields, pressure_timing=None, serial_corners=1):
         if cfg.values["useTracer"]:
             raise NotImplementedError("the oracle covers the tracer-free path")
         self.cfg = cfg
         self.L, self.Nx, self.Ny = cfg.values["Nlay"], cfg.values["Nx"], cfg.values["Ny"]
-        self._c = cfg_struct(cfg, pressure_timing)
+        self._c = cfg_struct(cfg, pressure_timing, serial_corners)
         self._m = lib().orc_create(ctypes.byref(self._c))
         if not self._m:
             raise ValueError("orc_create rejected the configuration")

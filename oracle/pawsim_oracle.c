@@ -225,6 +225,15 @@ static void xch (orc_model * m, F2 * f, int kind)
     if (m->c.wall_ew) wall_x(f,kind);
     return;
   }
+  if (m->c.serial_corners)
+  {
+    /* serial order: periodic copies of every row or column first, then the wall ghosts */
+    if (!m->c.wall_ns) per_y(f);
+    if (!m->c.wall_ew) per_x(f);
+    if (m->c.wall_ns) wall_y(f,kind);
+    if (m->c.wall_ew) wall_x(f,kind);
+    return;
+  }
   if (m->c.wall_ns) wall_y(f,kind); else per_y(f);
   if (m->c.wall_ew) wall_x(f,kind); else per_x(f);
 }

@@ -47,6 +47,10 @@ typedef struct orc_cfg
   double lin_drag, quad_drag, lin_drag_surf, quad_drag_surf;
   double tau_period, wdia_period, conv_diff;
   double pi_tol, sor_rp, omega_mg;
+  /* 1: halo fills in the serial build's order (model_code/field.c:353-532: periodic copies,
+   * then wall ghosts), whose corner ghosts on x-periodic, y-walled grids keep the values of
+   * the array's previous fill; 0: walls first (the MPI build's order, current corners) */
+  int serial_corners;
 } orc_cfg;
 
 typedef struct orc_model orc_model;

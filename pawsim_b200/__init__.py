@@ -51,7 +51,7 @@ class GpuConfig(ctypes.Structure):
                         ("pi_guess", ctypes.c_int), ("budgets", ctypes.c_int),
                         ("use_buoyancy", ctypes.c_int), ("use_diadiff", ctypes.c_int),
                         ("mg_fp32_inner", ctypes.c_int), ("check_nonfinite", ctypes.c_int),
-                        ("fail_on_maxiters", ctypes.c_int)]
+                        ("fail_on_maxiters", ctypes.c_int), ("mpi_corners", ctypes.c_int)]
 
 
 class GpuStats(ctypes.Structure):

@@ -102,6 +102,10 @@ struct Model {
   double *pi, *rhs, *work, *scratch, *dsum;
   unsigned long long* slots;
   int* diters;
+  // corner shadows of the work arrays' last two fills (x-periodic, y-walled grids with the
+  // serial build's corners; nullptr otherwise); corner[corner_cur] holds the latest
+  double* corner[2] = {nullptr, nullptr};
+  int corner_cur = 0;
   int* nonfinite = nullptr;   // raised by the fused kernel when a new state value is not finite
   int nf_calls = 0;           // steps since the flag was last read (check_nonfinite)
   Operator op;
@@ -249,6 +253,8 @@ static int create(const pawsim_gpu_config* cfg, Model** out) {
   ok &= (m->slots = m->alloc<unsigned long long>(2)) != nullptr;
   ok &= (m->diters = m->alloc<int>(1)) != nullptr;
   if (c.check_nonfinite > 0) ok &= (m->nonfinite = m->alloc<int>(1)) != nullptr;
+  if (!c.wall_ew && c.wall_ns && !c.mpi_corners)
+    for (int q = 0; q < 2; ++q) ok &= (m->corner[q] = m->alloc<double>(corner_elems(c.Nlay))) != nullptr;
   m->op.opitch = round_up(c.Nx + 1, 32);
   ok &= (m->op.Ow = m->alloc<double>((size_t)(c.Ny + 1) * m->op.opitch)) != nullptr;
   ok &= (m->op.Os = m->alloc<double>((size_t)(c.Ny + 1) * m->op.opitch)) != nullptr;
@@ -547,7 +553,20 @@ static TendParams base_params(Model* m) {
   p.b = c.use_tracer ? m->b[m->cur] : nullptr;
   p.conv_diff = c.conv_diff;
   p.nonfinite = m->nonfinite;
+  p.corners = m->corner[0] ? m->corner[m->corner_cur] : nullptr;
   return p;
+}
+
+// A fill of the work arrays in the reference: record its corner shadow (faces 1: the
+// tendency's per-cell face thickness, 2: the gathered one of the pressure path) from state
+// buffer `sb`, and make it the latest.
+static void corner_fill(Model* m, int sb, int faces) {
+  if (!m->corner[0]) return;
+  const int nx = 1 - m->corner_cur;
+  launch_corner_capture(m->grid2(), m->u[sb], m->v[sb], m->h[sb], m->b[0] ? m->b[sb] : nullptr,
+                        m->corner[m->corner_cur], m->corner[nx], faces, m->s);
+  ++g_launches;
+  m->corner_cur = nx;
 }
 
 // check_nonfinite: every K-th step reads and clears the flag the fused kernel raises
@@ -590,6 +609,7 @@ static int tendency_eval(Model* m) {
   if (launch_step_kernel(m, p) != 0)
     return fail(PAWSIM_GPU_EUNSUPPORTED, "scheme combination not available");
   ++g_launches;
+  corner_fill(m, m->cur, 1);   // the tendency's load_state and face thickness
   PAWSIM_CUDA_OK(cudaGetLastError());
   return 0;
 }
@@ -643,9 +663,11 @@ static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
     tp.use_buoy = c.use_buoyancy;
     for (int k = 0; k < m->L; ++k) tp.gg[k] = m->gg[k];
     tp.use_diadiff = c.use_diadiff; tp.kappa = m->kappa; tp.fsurf = m->fsurf; tp.conv_diff = c.conv_diff;
+    tp.corners = p.corners;
     launch_tracer(tp, m->s);
     ++g_launches;
   }
+  corner_fill(m, m->cur, 1);   // the tendency's load_state and face thickness (state of the step start)
   PAWSIM_CUDA_OK(cudaGetLastError());
   if (shift) m->h1 = h2;
   m->cur = nb;
@@ -683,6 +705,7 @@ static int pressure_correct(Model* m, int update_diags, pawsim_gpu_stats* st) {
   }
   m->thickness_fixed = false;
   g_launches += launch_pressure_rhs(g, m->u[cur], m->v[cur], m->h[cur], m->rhs, m->s);
+  corner_fill(m, cur, 2);   // build_rhs reloads the corrected state (pressure.c:570-606)
   launch_sum(m->rhs, m->Nx, m->Ny, m->pitch, m->serial(), m->scratch, m->dsum, m->s);
   launch_subtract_mean(m->rhs, m->Nx, m->Ny, m->pitch, m->dsum, m->s);
   g_launches += m->serial() ? 2 : 3;
@@ -768,6 +791,7 @@ static int pressure_correct(Model* m, int update_diags, pawsim_gpu_stats* st) {
     launch_projection(g, m->pi, m->u[cur], m->v[cur], m->s);
   ++g_launches;
   if (m->c.pressure_timing) {
+    corner_fill(m, cur, 2);   // the divergence norms reload the projected state (pressure.c:693-737)
     g_launches += launch_divergence_field(g, m->u[cur], m->v[cur], m->h[cur], m->work, m->s);
     int r = finish_norms(m, m->work, &local.div_max, &local.div_rms);
     if (r) return r;
@@ -895,6 +919,7 @@ int pawsim_gpu_accumulate_averages(pawsim_gpu* h, double avg_fac) {
   a.b = m->b[0] ? m->b[m->cur] : nullptr;
   a.use_buoy = m->c.use_buoyancy;
   a.ab = m->b[0] ? a.api + ls : nullptr;
+  corner_fill(m, m->cur, 2);   // the averages reload the state (diagnostics.c:320-324)
   launch_accumulate_averages(m->grid2(), a, m->s);
   ++g_launches;
   PAWSIM_CUDA_OK(cudaGetLastError());

@@ -81,6 +81,48 @@ __host__ __device__ inline double load_mapped(const double* __restrict__ f, int 
 
 inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
+// ---- corner ghosts of the reference's serial build on x-periodic, y-walled grids.
+// There a halo fill copies whole columns periodically in x first, ghost rows included, and
+// only then fills the wall ghost rows of the owned columns (model_code/field.c:353-532), so
+// the four corner blocks keep what the wall rows at the periodic image columns held after
+// the previous fill of the same array. The library keeps those values in a small "corner
+// shadow": per field and layer the owned values of the previous fill at the 3 columns next to
+// each side of the periodic seam and the 4 rows next to each wall. A load at a corner position
+// reads the shadow through the wall mirror instead of the current field.
+constexpr int CORNER_F = 6;        // u, v, h and h_west, h_south of the work arrays, tracer b
+constexpr int CORNER_R = 4;        // rows from each wall
+constexpr int CORNER_C = 6;        // columns: x = 0, 1, 2 and Nx-3, Nx-2, Nx-1
+enum { CF_U, CF_V, CF_H, CF_HW, CF_HS, CF_B };
+
+__host__ __device__ inline size_t corner_elems(int L) {
+  return (size_t)CORNER_F * L * 2 * CORNER_R * CORNER_C;
+}
+// slot of field f, layer k, wall side (0 south, 1 north), row r from that wall, column c
+__host__ __device__ inline size_t corner_slot(int f, int k, int L, int side, int r, int c) {
+  return ((((size_t)f * L + k) * 2 + side) * CORNER_R + r) * CORNER_C + c;
+}
+// owned source position of a slot
+__host__ __device__ inline int corner_x(int c, int Nx) { return c < 3 ? c : Nx - CORNER_C + c; }
+__host__ __device__ inline int corner_y(int side, int r, int Ny) { return side == 0 ? r : Ny - 1 - r; }
+// is raw (x, y) a corner ghost (x outside [0, Nx) and y outside [0, Ny))
+__host__ __device__ inline bool is_corner(int x, int y, int Nx, int Ny) {
+  return (x < 0 || x >= Nx) && (y < 0 || y >= Ny);
+}
+// the value of a corner ghost (x within 3 columns, y within 3 rows of the grid) of field f,
+// layer k; kind_y is the field's wall kind along y (MAP_S, or MAP_N for v)
+__host__ __device__ inline double corner_load(const double* buf, int f, int k, int L, int x, int y, int Nx, int Ny,
+                                              int kind_y) {
+  const int xs = wrap_index(x, Nx);
+  const int c = xs < 3 ? xs : xs - Nx + CORNER_C;
+  if (kind_y == MAP_N) {
+    if (y == Ny) return -0.0;                          // the north wall face
+    if (y < 0) return -buf[corner_slot(f, k, L, 0, -y, c)];
+    return -buf[corner_slot(f, k, L, 1, y - Ny - 1, c)];
+  }
+  if (y < 0) return buf[corner_slot(f, k, L, 0, -y - 1, c)];
+  return buf[corner_slot(f, k, L, 1, y - Ny, c)];
+}
+
 // x / d rounded to nearest, given r = 1/d rounded to nearest. Markstein's theorem: when q
 // is within one ulp of x/d and r is the correctly rounded reciprocal, the remainder
 // x - q*d is exact and q + (x - q*d)*r rounds to x/d. The first correction makes q = x*r

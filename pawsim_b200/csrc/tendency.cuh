@@ -71,6 +71,9 @@ struct TendParams {
   double conv_diff;               // convDiff: added viscosity where the local g' < 0
   // set to 1 when a new u, v or h is not finite (nullable: no check)
   int* nonfinite;
+  // corner shadow of the previous fill (common.cuh; nullable: corner ghosts hold the current
+  // values, as in the MPI build)
+  const double* corners;
 };
 
 // budget term indices (work.h:18-91)

@@ -459,6 +459,12 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         int lx = q % RW, ly = q / RW;
         int gx = t.gx(lx), gy = t.gy(ly);
         bool in = gx >= -H && gx < p.Nx + H && gy >= -H && gy < p.Ny + H;
+        if (in && p.corners && is_corner(gx, gy, p.Nx, p.Ny)) {
+          F[F_U][q] = corner_load(p.corners, CF_U, k, L, gx, gy, p.Nx, p.Ny, MAP_S);
+          F[F_V][q] = corner_load(p.corners, CF_V, k, L, gx, gy, p.Nx, p.Ny, MAP_N);
+          F[F_H][q] = corner_load(p.corners, CF_H, k, L, gx, gy, p.Nx, p.Ny, MAP_S);
+          continue;
+        }
         F[F_U][q] = in ? gload(uk, p, gx, gy, MAP_N, MAP_S) : 0.0;
         F[F_V][q] = in ? gload(vk, p, gx, gy, MAP_S, MAP_N) : 0.0;
         F[F_H][q] = in ? gload(hkp, p, gx, gy, MAP_S, MAP_S) : 0.0;
@@ -473,9 +479,14 @@ tendency_kernel(const __grid_constant__ TendParams p) {
       int lx = q % RW, ly = q / RW;
       const bool nr = t.near(lx, ly);
       if (lx >= H - 1 && lx <= TX + H && ly >= H - 1 && ly <= TY + H && nr) {
-        int mx = t.mlx(lx), my = t.mly(ly);
-        F[F_HW][q] = face_west<TS, RW>(sh, su, p.kt00_sigma, mx, my);
-        F[F_HS][q] = face_south<TS, RW>(sh, sv, p.kt00_sigma, mx, my);
+        if (p.corners && !inner && is_corner(t.gx(lx), t.gy(ly), p.Nx, p.Ny)) {
+          F[F_HW][q] = corner_load(p.corners, CF_HW, k, L, t.gx(lx), t.gy(ly), p.Nx, p.Ny, MAP_S);
+          F[F_HS][q] = corner_load(p.corners, CF_HS, k, L, t.gx(lx), t.gy(ly), p.Nx, p.Ny, MAP_S);
+        } else {
+          int mx = t.mlx(lx), my = t.mly(ly);
+          F[F_HW][q] = face_west<TS, RW>(sh, su, p.kt00_sigma, mx, my);
+          F[F_HS][q] = face_south<TS, RW>(sh, sv, p.kt00_sigma, mx, my);
+        }
       }
       if (lx >= H - 1 && ly >= H - 1 && lx <= TX + H + 1 && ly <= TY + H + 1) {
         // zeta, h on the q grid and q itself (work.c:1261-1270)

@@ -73,6 +73,13 @@ __global__ void __launch_bounds__(TNT) tracer_tile_kernel(const TracerParams p) 
       const int lx = q % TRW, ly = q / TRW;
       const int gx = X0 - TH + lx, gy = Y0 - TH + ly;
       const bool in = gx >= -TH && gx < p.Nx + TH && gy >= -TH && gy < p.Ny + TH;
+      if (in && p.corners && is_corner(gx, gy, p.Nx, p.Ny)) {
+        S[T_U][q] = corner_load(p.corners, CF_U, k, p.L, gx, gy, p.Nx, p.Ny, MAP_S);
+        S[T_V][q] = corner_load(p.corners, CF_V, k, p.L, gx, gy, p.Nx, p.Ny, MAP_N);
+        S[T_H][q] = corner_load(p.corners, CF_H, k, p.L, gx, gy, p.Nx, p.Ny, MAP_S);
+        S[T_B][q] = corner_load(p.corners, CF_B, k, p.L, gx, gy, p.Nx, p.Ny, MAP_S);
+        continue;
+      }
       S[T_U][q] = in ? load_mapped(uk, p.pitch, gx, gy, p.Nx, p.Ny, p.wall_ew, p.wall_ns, MAP_N, MAP_S) : 0.0;
       S[T_V][q] = in ? load_mapped(vk, p.pitch, gx, gy, p.Nx, p.Ny, p.wall_ew, p.wall_ns, MAP_S, MAP_N) : 0.0;
       S[T_H][q] = in ? load_mapped(hk, p.pitch, gx, gy, p.Nx, p.Ny, p.wall_ew, p.wall_ns, MAP_S, MAP_S) : 0.0;
@@ -132,8 +139,13 @@ __global__ void __launch_bounds__(TNT) tracer_tile_kernel(const TracerParams p) 
       const int gx = X0 - TH + lx, gy = Y0 - TH + ly;
       const bool nr = gx >= -2 && gx < p.Nx + 2 && gy >= -2 && gy < p.Ny + 2;
       const int mx = mlx(lx), my = mly(ly);
-      S[T_HW][q] = nr ? face_w(mx, my) : 0.0;
-      S[T_HS][q] = nr ? face_s(mx, my) : 0.0;
+      if (nr && p.corners && !inner && is_corner(gx, gy, p.Nx, p.Ny)) {
+        S[T_HW][q] = corner_load(p.corners, CF_HW, k, p.L, gx, gy, p.Nx, p.Ny, MAP_S);
+        S[T_HS][q] = corner_load(p.corners, CF_HS, k, p.L, gx, gy, p.Nx, p.Ny, MAP_S);
+      } else {
+        S[T_HW][q] = nr ? face_w(mx, my) : 0.0;
+        S[T_HS][q] = nr ? face_s(mx, my) : 0.0;
+      }
     }
     if (lx >= 1 && lx <= TRW - 2 && ly >= 1 && ly <= TRH - 2) {
       if (p.scheme == 0) {

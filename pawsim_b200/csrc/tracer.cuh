@@ -40,6 +40,8 @@ struct TracerParams {
   int use_diadiff;
   const double *kappa, *fsurf;
   double conv_diff;
+  // corner shadow of the previous fill (common.cuh; nullable: current corner values)
+  const double* corners;
 };
 
 void launch_tracer(const TracerParams& p, cudaStream_t s);

@@ -117,6 +117,27 @@ BUD_CASES = {
                                                 extra=dict(hsml=1500.0, hmin_surf=5.0, hbbl=500.0, hmin_bot=10.0,
                                                            linDragSurf=1e-4, thicknessScheme=3)), None),
 }
+# the acceptance point of the plain FP64 path: config 0 (128 x 128 x 2 double gyre, red-black
+# SOR with SOR_rp 1.8, tol 1e-10) at its stable dt of 900 s, 100 steps; the fixture keeps every
+# step's pressure line and the state after step 100
+LONG_NSTEPS = 100
+LONG_KEEP = (100,)
+LONG_CASES = {
+    "config0_sor_100": (inputs.gyre, dict(N=128, dt=900.0, solver=0, tol=1e-10, sor_rp=1.8)),
+}
+# x-periodic, y-walled channels without pressureTiming: the serial build's corner ghosts keep
+# the values of each work array's previous fill (model_code/field.c:353-532); U/V/H/P (and B)
+# after each step. SOR keeps the states bit-exact. (set-up, arguments, tracer arguments)
+CORNER_NSTEPS = 6
+CORNER_CASES = {
+    "channel_corners_sor": (inputs.channel, dict(Nx=32, Ny=16, dt=150.0, solver=0), None),
+    "channel_corners_hk83": (inputs.channel, dict(Nx=40, Ny=16, dt=150.0, solver=0, A2=200.0, A4=0.0,
+                                                  extra=dict(momentumScheme=1, thicknessScheme=1)), None),
+    "channel_corners_free": (inputs.channel, dict(Nx=32, Ny=16, dt=20.0, solver=0, A2=200.0, A4=0.0,
+                                                  extra=dict(useRL=0, thicknessScheme=1)), None),
+    "channel_corners_tracer": (inputs.channel, dict(Nx=32, Ny=16, dt=150.0, solver=0),
+                               dict(scheme=2, relax_days=30.0, K2=100.0)),
+}
 LINE = re.compile(r"iters=(\d+) walltime=\S+ s residual_max=(\S+) residual_rms=(\S+) "
                   r"div_max=(\S+) div_rms=(\S+)")
 
@@ -184,6 +205,60 @@ def make(name, fn, kw, outdir):
                     rec[f"{v}{k}_{n}"] = inputs.read_data(os.path.join(out, f"{v}{k}_n={n}.dat"), (Ny, Nx))
         for n in range(1, NSTEPS + 1):
             rec[f"P_{n}"] = inputs.read_data(os.path.join(out, f"P_n={n}.dat"), (Ny, Nx))
+        np.savez_compressed(os.path.join(outdir, name + ".npz"), **rec)
+
+
+def make_long(name, fn, kw, outdir):
+    """Inputs, every step's pressure line (iterations and the four norms) and U/V/H/P after
+    the steps of LONG_KEEP."""
+    with tempfile.TemporaryDirectory() as d:
+        kw = dict(kw)
+        extra = dict(kw.pop("extra", {}) or {})
+        extra.update(pressureTiming=1)
+        dt = kw["dt"]
+        p = fn(os.path.join(d, "in"), Nt=LONG_NSTEPS, savefrequency=dt, extra=extra, **kw)
+        cfg = inputs.read_config(p)
+        out = os.path.join(d, "out")
+        os.makedirs(out)
+        r = subprocess.run([oracle.reference_exe(), p, out], capture_output=True, text=True, check=True)
+        stats = np.array([[float(x) for x in m.groups()] for m in LINE.finditer(r.stdout)])
+        rec = {"stats": stats, "param_text": np.array(open(p).read()), "keep": np.array(LONG_KEEP)}
+        for f in sorted(os.listdir(os.path.dirname(p))):
+            if f.endswith(".dat") and f != "params.dat":
+                rec["in_" + f] = np.fromfile(os.path.join(os.path.dirname(p), f), dtype="<f8")
+        for n in LONG_KEEP:
+            for k in range(cfg.Nlay):
+                for v in ("U", "V", "H"):
+                    rec[f"{v}{k}_{n}"] = inputs.read_data(os.path.join(out, f"{v}{k}_n={n}.dat"), (cfg.Ny, cfg.Nx))
+            rec[f"P_{n}"] = inputs.read_data(os.path.join(out, f"P_n={n}.dat"), (cfg.Ny, cfg.Nx))
+        np.savez_compressed(os.path.join(outdir, name + ".npz"), **rec)
+
+
+def make_corner(name, fn, kw, tkw, outdir):
+    """Inputs and the reference's U/V/H(/B)/P after each step, pressureTiming off."""
+    with tempfile.TemporaryDirectory() as d:
+        kw = dict(kw)
+        extra = dict(kw.pop("extra", {}) or {})
+        extra.update(pressureTiming=0)
+        dt = kw["dt"]
+        p = fn(os.path.join(d, "in"), Nt=CORNER_NSTEPS, savefrequency=dt, extra=extra, **kw)
+        if tkw is not None:
+            add_tracer_and_mixing(p, tkw)
+        cfg = inputs.read_config(p)
+        out = os.path.join(d, "out")
+        os.makedirs(out)
+        subprocess.run([oracle.reference_exe(), p, out], capture_output=True, text=True, check=True)
+        rec = {"param_text": np.array(open(p).read())}
+        for f in sorted(os.listdir(os.path.dirname(p))):
+            if f.endswith(".dat") and f != "params.dat":
+                rec["in_" + f] = np.fromfile(os.path.join(os.path.dirname(p), f), dtype="<f8")
+        names = ("U", "V", "H", "B") if tkw is not None else ("U", "V", "H")
+        for n in range(1, CORNER_NSTEPS + 1):
+            for k in range(cfg.Nlay):
+                for v in names:
+                    rec[f"{v}{k}_{n}"] = inputs.read_data(os.path.join(out, f"{v}{k}_n={n}.dat"), (cfg.Ny, cfg.Nx))
+            if cfg.values["useRL"]:
+                rec[f"P_{n}"] = inputs.read_data(os.path.join(out, f"P_n={n}.dat"), (cfg.Ny, cfg.Nx))
         np.savez_compressed(os.path.join(outdir, name + ".npz"), **rec)
 
 
@@ -306,6 +381,16 @@ if __name__ == "__main__":
         if len(sys.argv) > 1 and name not in sys.argv[1:]:
             continue
         make(name, fn, kw, HERE)
+        print("wrote", name)
+    for name, (fn, kw) in LONG_CASES.items():
+        if len(sys.argv) > 1 and name not in sys.argv[1:]:
+            continue
+        make_long(name, fn, kw, HERE)
+        print("wrote", name)
+    for name, (fn, kw, tkw) in CORNER_CASES.items():
+        if len(sys.argv) > 1 and name not in sys.argv[1:]:
+            continue
+        make_corner(name, fn, kw, tkw, HERE)
         print("wrote", name)
     for name, (fn, kw) in AVG_CASES.items():
         if len(sys.argv) > 1 and name not in sys.argv[1:]:

@@ -23,6 +23,9 @@ def test_gpu_matches_reference_outputs(tmp_path, name):
     st = m.prelim()
     stats = z["stats"]
     sor = cfg.values["pressureSolver"] == 0
+    # the preliminary correction from rest: its line too
+    assert st["iters"] == int(stats[0, 0]) or not sor, (st["iters"], stats[0, 0])
+    check_norms(st, stats[0], sor, 0)
     tend = m.tendency_eval()
     for k in range(cfg.Nlay):
         for tag, v in (("dudt", "u"), ("dvdt", "v"), ("dhdt", "h")):
@@ -48,5 +51,19 @@ def test_gpu_matches_reference_outputs(tmp_path, name):
                     assert rel_l2(s[v][k], ref) < 1e-6, (n, v, k, rel_l2(s[v][k], ref))
         if sor:
             assert value_equal(m.get("pi"), z[f"P_{n}"]), n
-        # the solve reaches at least the reference's residual quality
-        assert st["residual_max"] <= max(4 * stats[n, 1], 1e-13), (n, st["residual_max"], stats[n, 1])
+        check_norms(st, stats[n], sor, n)
+
+
+def check_norms(st, ref, sor, n):
+    """The four norms of the reference's pressureTiming line (model_code/pressure.c:652-737,
+    printed with %0.6e): max and RMS of rhs - L(pi), and of the barotropic divergence after the
+    projection. SOR states are bit-identical, so the norms agree to the printed precision. The
+    multigrid solves stop at the same test with a different smoother, so their norms (the
+    solver's remaining error, 1e-19..1e-13 here) must be of the reference's size: at most 10 times
+    it (they are usually smaller)."""
+    got = np.array([st["residual_max"], st["residual_rms"], st["div_max"], st["div_rms"]])
+    want = np.asarray(ref[1:5], dtype=float)
+    if sor:
+        np.testing.assert_allclose(got, want, rtol=6e-7, atol=0, err_msg=f"step {n}")
+    else:
+        assert np.all(got >= 0) and np.all(got <= 10 * want + 1e-300), (n, got, want)
