@@ -106,6 +106,7 @@ struct Model {
   // serial build's corners; nullptr otherwise); corner[corner_cur] holds the latest
   double* corner[2] = {nullptr, nullptr};
   int corner_cur = 0;
+  double* dragv = nullptr;    // boundary-layer velocities of the quadratic drags over a fraction depth
   int* nonfinite = nullptr;   // raised by the fused kernel when a new state value is not finite
   int nf_calls = 0;           // steps since the flag was last read (check_nonfinite)
   Operator op;
@@ -198,13 +199,6 @@ static int create(const pawsim_gpu_config* cfg, Model** out) {
     return fail(PAWSIM_GPU_EBADCONFIG, "PAWSIM only supports AB1, AB2 and AB3 time stepping so far");
   if (c.mom_scheme < 0 || c.mom_scheme > 3 || c.thick_scheme < 0 || c.thick_scheme > 3)
     return fail(PAWSIM_GPU_EBADCONFIG, "Unknown or unsupported numerical scheme identifier");
-  // quadratic drag reads the velocity of the whole boundary layer at neighbouring faces; the
-  // fused kernel builds it from the top or bottom layer's tile, so a drag whose layer is
-  // spread by a fraction depth is not built
-  if (c.quad_drag > 0 && c.hbbl > 0)
-    return fail(PAWSIM_GPU_EUNSUPPORTED, "quadratic bottom drag with hbbl > 0 is not built");
-  if (c.quad_drag_surf > 0 && c.hsml > 0)
-    return fail(PAWSIM_GPU_EUNSUPPORTED, "quadratic surface drag with hsml > 0 is not built");
   if (c.tau_nrecs < 1 || c.wdia_nrecs < 1) return fail(PAWSIM_GPU_EBADCONFIG, "record counts must be positive");
   if (c.use_tracer && (c.tracer_scheme < 0 || c.tracer_scheme > 2))
     return fail(PAWSIM_GPU_EBADCONFIG, "Unknown or unsupported numerical scheme identifier");
@@ -253,6 +247,8 @@ static int create(const pawsim_gpu_config* cfg, Model** out) {
   ok &= (m->slots = m->alloc<unsigned long long>(2)) != nullptr;
   ok &= (m->diters = m->alloc<int>(1)) != nullptr;
   if (c.check_nonfinite > 0) ok &= (m->nonfinite = m->alloc<int>(1)) != nullptr;
+  if ((c.quad_drag > 0 && c.hbbl > 0) || (c.quad_drag_surf > 0 && c.hsml > 0))
+    ok &= (m->dragv = m->alloc<double>(4 * m->plane)) != nullptr;
   if (!c.wall_ew && c.wall_ns && !c.mpi_corners)
     for (int q = 0; q < 2; ++q) ok &= (m->corner[q] = m->alloc<double>(corner_elems(c.Nlay))) != nullptr;
   m->op.opitch = round_up(c.Nx + 1, 32);
@@ -554,6 +550,9 @@ static TendParams base_params(Model* m) {
   p.conv_diff = c.conv_diff;
   p.nonfinite = m->nonfinite;
   p.corners = m->corner[0] ? m->corner[m->corner_cur] : nullptr;
+  p.dragv = m->dragv;
+  p.drag_bot = (c.quad_drag > 0 && c.hbbl > 0) ? 1 : 0;
+  p.drag_surf = (c.quad_drag_surf > 0 && c.hsml > 0) ? 1 : 0;
   return p;
 }
 
@@ -608,7 +607,7 @@ static int tendency_eval(Model* m) {
   p.fu_out = m->dtu; p.fv_out = m->dtv; p.fh_out = m->dth;
   if (launch_step_kernel(m, p) != 0)
     return fail(PAWSIM_GPU_EUNSUPPORTED, "scheme combination not available");
-  ++g_launches;
+  g_launches += (p.drag_bot || p.drag_surf) ? 2 : 1;   // the drag pre-pass and the fused kernel
   corner_fill(m, m->cur, 1);   // the tendency's load_state and face thickness
   PAWSIM_CUDA_OK(cudaGetLastError());
   return 0;
@@ -643,7 +642,7 @@ static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
   }
   if (launch_step_kernel(m, p) != 0)
     return fail(PAWSIM_GPU_EUNSUPPORTED, "scheme combination not available");
-  ++g_launches;
+  g_launches += (p.drag_bot || p.drag_surf) ? 2 : 1;   // the drag pre-pass and the fused kernel
   if (c.use_tracer) {
     // the tracer reads the state of the start of the step and the w_dia the tendency
     // kernel just wrote; same AB coefficients and history slots

@@ -74,6 +74,12 @@ struct TendParams {
   // corner shadow of the previous fill (common.cuh; nullable: corner ghosts hold the current
   // values, as in the MPI build)
   const double* corners;
+  // quadratic drag over a fraction depth (forcing.c:95-143, 181-223): planes of the
+  // thickness-weighted bottom-boundary-layer velocity u_bot, v_bot (hbbl > 0) and surface
+  // mixed-layer velocity u_surf, v_surf (hsml > 0), written by a pre-pass of the same launch;
+  // nullptr when the drag acts on the bottom (top) layer alone
+  double* dragv;
+  int drag_bot, drag_surf;
 };
 
 // budget term indices (work.h:18-91)

@@ -247,6 +247,122 @@ __device__ inline double gface_south(const TendParams& p, const double* h, const
   return 0.5 * (H(i, j) + H(i, j - 1));
 }
 
+// Surface and bottom layer fractions of every layer at owned cell (gi, gj) (work.c:2151-2340):
+// out(f, k, value) receives f = 0 hFsurf_west, 1 hFsurf_south, 2 hFbot_west, 3 hFbot_south,
+// zeros included. hsml <= 0 puts the whole surface forcing in the top layer, hbbl <= 0 the
+// whole bottom forcing in the bottom layer.
+template <int TS, typename Out>
+__device__ inline void cell_fractions(const TendParams& p, int gi, int gj, Out out) {
+  const int L = p.L;
+  double hwk[LMAX], hsk[LMAX];
+  for (int k = 0; k < L; ++k) {
+    hwk[k] = gface_west<TS>(p, p.h + k * p.lstride, p.u + k * p.lstride, gi, gj);
+    hsk[k] = gface_south<TS>(p, p.h + k * p.lstride, p.v + k * p.lstride, gi, gj);
+  }
+  for (int f = 0; f < 4; ++f)
+    for (int k = 0; k < L; ++k) out(f, k, 0.0);
+  if (p.hsml <= 0) {
+    out(0, 0, 1.0);
+    out(1, 0, 1.0);
+  } else {
+    const double hsw = 0.5 * (gload(p.hhs, p, gi, gj, MAP_S, MAP_S) + gload(p.hhs, p, gi - 1, gj, MAP_S, MAP_S));
+    const double hss = 0.5 * (gload(p.hhs, p, gi, gj, MAP_S, MAP_S) + gload(p.hhs, p, gi, gj - 1, MAP_S, MAP_S));
+    double zw = hsw - p.hsml, zs = hss - p.hsml, ew = hsw, es = hss, sw = 0, ss = 0;
+    for (int k = 0; k < L; ++k) {
+      const double ewl = ew - hwk[k], esl = es - hsk[k];
+      if (sw < 1.0) {
+        zw -= fmin(p.hmin_surf, hwk[k]);
+        double he = fmax(ew, zw) - fmax(ewl, zw);
+        he = fmax(he - p.hmin_surf, 0.0);
+        const double fr = he / p.hsml;
+        out(0, k, fr);
+        sw += fr;
+      }
+      if (ss < 1.0) {
+        zs -= fmin(p.hmin_surf, hsk[k]);
+        double he = fmax(es, zs) - fmax(esl, zs);
+        he = fmax(he - p.hmin_surf, 0.0);
+        const double fr = he / p.hsml;
+        out(1, k, fr);
+        ss += fr;
+      }
+      ew = ewl;
+      es = esl;
+    }
+  }
+  if (p.hbbl <= 0) {
+    out(2, L - 1, 1.0);
+    out(3, L - 1, 1.0);
+  } else {
+    const double hbw = 0.5 * (gload(p.hhb, p, gi, gj, MAP_S, MAP_S) + gload(p.hhb, p, gi - 1, gj, MAP_S, MAP_S));
+    const double hbs = 0.5 * (gload(p.hhb, p, gi, gj, MAP_S, MAP_S) + gload(p.hhb, p, gi, gj - 1, MAP_S, MAP_S));
+    double zw = hbw + p.hbbl, zs = hbs + p.hbbl, ewl = hbw, esl = hbs, sw = 0, ss = 0;
+    for (int k = L; k > 0; --k) {
+      const int kk = k - 1;
+      const double ewu = ewl + hwk[kk], esu = esl + hsk[kk];
+      if (sw < 1.0) {
+        zw += fmin(p.hmin_bot, hwk[kk]);
+        double he = fmin(ewu, zw) - fmin(ewl, zw);
+        he = fmax(he - p.hmin_bot, 0.0);
+        const double fr = he / p.hbbl;
+        out(2, kk, fr);
+        sw += fr;
+      }
+      if (ss < 1.0) {
+        zs += fmin(p.hmin_bot, hsk[kk]);
+        double he = fmin(esu, zs) - fmin(esl, zs);
+        he = fmax(he - p.hmin_bot, 0.0);
+        const double fr = he / p.hbbl;
+        out(3, kk, fr);
+        ss += fr;
+      }
+      ewl = ewu;
+      esl = esu;
+    }
+  }
+}
+
+// Pre-pass of the quadratic drags whose boundary layer spreads over several layers
+// (forcing.c:95-143, 181-223): at every owned cell the fraction-weighted sums of the layer
+// velocities, u_bot = sum_k u_k hFbot_west_k and v_bot (hbbl > 0), u_surf and v_surf (hsml > 0),
+// in layer order from zero as the reference sums them. Planes of p.dragv: 0 u_bot, 1 v_bot,
+// 2 u_surf, 3 v_surf.
+template <int TS>
+__global__ void drag_speed_kernel(const __grid_constant__ TendParams p) {
+  const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gj = blockIdx.y * blockDim.y + threadIdx.y;
+  if (gi >= p.Nx || gj >= p.Ny) return;
+  const size_t c = (size_t)gj * p.pitch + gi;
+  double fr[4][LMAX];
+  cell_fractions<TS>(p, gi, gj, [&](int f, int k, double v) { fr[f][k] = v; });
+  double ub = 0, vb = 0, us = 0, vs = 0;
+  for (int k = 0; k < p.L; ++k) {
+    const size_t o = k * p.lstride + c;
+    us += p.u[o] * fr[0][k];
+    vs += p.v[o] * fr[1][k];
+    ub += p.u[o] * fr[2][k];
+    vb += p.v[o] * fr[3][k];
+  }
+  if (p.drag_bot) {
+    p.dragv[c] = ub;
+    p.dragv[p.lstride + c] = vb;
+  }
+  if (p.drag_surf) {
+    p.dragv[2 * p.lstride + c] = us;
+    p.dragv[3 * p.lstride + c] = vs;
+  }
+}
+
+// a drag velocity plane at raw (x, y): a product of two fields of the same wall parity, so
+// ghosts take the mirrored value without a sign change and the wall face holds +0
+__device__ inline double drag_load(const double* f, const TendParams& p, int x, int y, int kx, int ky) {
+  AxisMap ax = map_axis(x, p.Nx, p.wall_ew, kx);
+  if (ax.zero) return 0.0;
+  AxisMap ay = map_axis(y, p.Ny, p.wall_ns, ky);
+  if (ay.zero) return 0.0;
+  return f[(size_t)ay.idx * p.pitch + ax.idx];
+}
+
 // 64 registers per thread: four 256-thread or two 512-thread CTAs per SM
 #ifndef PAWSIM_TEND_MINB
 #define PAWSIM_TEND_MINB (1024 / NT)
@@ -371,74 +487,8 @@ tendency_kernel(const __grid_constant__ TendParams p) {
 
   // ---- surface and bottom layer fractions at the owned cell (work.c:2151-2340) ----
   // FR[(f * L + k) * NT + tid], f = 0 hFsw, 1 hFss, 2 hFbw, 3 hFbs
-  if (p.use_fractions && valid) {
-    double hwk[LMAX], hsk[LMAX];
-    for (int k = 0; k < L; ++k) {
-      hwk[k] = gface_west<TS>(p, p.h + k * p.lstride, p.u + k * p.lstride, gi, gj);
-      hsk[k] = gface_south<TS>(p, p.h + k * p.lstride, p.v + k * p.lstride, gi, gj);
-    }
-    for (int f = 0; f < 4; ++f)
-      for (int k = 0; k < L; ++k) FR[(f * L + k) * NT + tid] = 0;
-    if (p.hsml <= 0) {
-      FR[(0 * L + 0) * NT + tid] = 1;
-      FR[(1 * L + 0) * NT + tid] = 1;
-    } else {
-      const double hsw = 0.5 * (gload(p.hhs, p, gi, gj, MAP_S, MAP_S) + gload(p.hhs, p, gi - 1, gj, MAP_S, MAP_S));
-      const double hss = 0.5 * (gload(p.hhs, p, gi, gj, MAP_S, MAP_S) + gload(p.hhs, p, gi, gj - 1, MAP_S, MAP_S));
-      double zw = hsw - p.hsml, zs = hss - p.hsml, ew = hsw, es = hss, sw = 0, ss = 0;
-      for (int k = 0; k < L; ++k) {
-        const double ewl = ew - hwk[k], esl = es - hsk[k];
-        if (sw < 1.0) {
-          zw -= fmin(p.hmin_surf, hwk[k]);
-          double he = fmax(ew, zw) - fmax(ewl, zw);
-          he = fmax(he - p.hmin_surf, 0.0);
-          const double fr = he / p.hsml;
-          FR[(0 * L + k) * NT + tid] = fr;
-          sw += fr;
-        }
-        if (ss < 1.0) {
-          zs -= fmin(p.hmin_surf, hsk[k]);
-          double he = fmax(es, zs) - fmax(esl, zs);
-          he = fmax(he - p.hmin_surf, 0.0);
-          const double fr = he / p.hsml;
-          FR[(1 * L + k) * NT + tid] = fr;
-          ss += fr;
-        }
-        ew = ewl;
-        es = esl;
-      }
-    }
-    if (p.hbbl <= 0) {
-      FR[(2 * L + L - 1) * NT + tid] = 1;
-      FR[(3 * L + L - 1) * NT + tid] = 1;
-    } else {
-      const double hbw = 0.5 * (gload(p.hhb, p, gi, gj, MAP_S, MAP_S) + gload(p.hhb, p, gi - 1, gj, MAP_S, MAP_S));
-      const double hbs = 0.5 * (gload(p.hhb, p, gi, gj, MAP_S, MAP_S) + gload(p.hhb, p, gi, gj - 1, MAP_S, MAP_S));
-      double zw = hbw + p.hbbl, zs = hbs + p.hbbl, ewl = hbw, esl = hbs, sw = 0, ss = 0;
-      for (int k = L; k > 0; --k) {
-        const int kk = k - 1;
-        const double ewu = ewl + hwk[kk], esu = esl + hsk[kk];
-        if (sw < 1.0) {
-          zw += fmin(p.hmin_bot, hwk[kk]);
-          double he = fmin(ewu, zw) - fmin(ewl, zw);
-          he = fmax(he - p.hmin_bot, 0.0);
-          const double fr = he / p.hbbl;
-          FR[(2 * L + kk) * NT + tid] = fr;
-          sw += fr;
-        }
-        if (ss < 1.0) {
-          zs += fmin(p.hmin_bot, hsk[kk]);
-          double he = fmin(esu, zs) - fmin(esl, zs);
-          he = fmax(he - p.hmin_bot, 0.0);
-          const double fr = he / p.hbbl;
-          FR[(3 * L + kk) * NT + tid] = fr;
-          ss += fr;
-        }
-        ewl = ewu;
-        esl = esu;
-      }
-    }
-  }
+  if (p.use_fractions && valid)
+    cell_fractions<TS>(p, gi, gj, [&](int f, int k, double v) { FR[(f * L + k) * NT + tid] = v; });
 
   for (int k = 0; k < L; ++k) {
     const double* uk = p.u + k * p.lstride;
@@ -869,10 +919,18 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         }
       }
       // quadratic drag (forcing.c:95-143, 330-393): the speed at the cell centre from the
-      // squared bottom (surface) velocities of the neighbouring faces. Without layer
-      // fractions it acts on the bottom (top) layer alone, whose tile is in shared memory.
-      if (p.quad_drag > 0 && k == L - 1) {
+      // squared bottom (surface) velocities of the neighbouring faces. Without a fraction
+      // depth it acts on the bottom (top) layer alone, whose tile is in shared memory; with one
+      // it acts on every layer the fractions reach, from the pre-pass's weighted velocities.
+      if (p.quad_drag > 0 && (p.drag_bot || k == L - 1)) {
         auto uab = [&](int a, int b) {
+          if (p.drag_bot) {
+            const double* UB = p.dragv;
+            const double* VB = p.dragv + p.lstride;
+            const int x = t.gx(a), y = t.gy(b);
+            return sqrt(0.5 * (sq(drag_load(UB, p, x, y, MAP_N, MAP_S)) + sq(drag_load(UB, p, x + 1, y, MAP_N, MAP_S)))
+                        + 0.5 * (sq(drag_load(VB, p, x, y, MAP_S, MAP_N)) + sq(drag_load(VB, p, x, y + 1, MAP_S, MAP_N))));
+          }
           return sqrt(0.5 * (sq(AT(su, a, b)) + sq(AT(su, a + 1, b))) + 0.5 * (sq(AT(sv, a, b)) + sq(AT(sv, a, b + 1))));
         };
         if (hwest != 0) {
@@ -892,12 +950,19 @@ tendency_kernel(const __grid_constant__ TendParams p) {
           }
         }
       }
-      if (p.quad_drag_surf > 0 && k == 0) {
+      if (p.quad_drag_surf > 0 && (p.drag_surf || k == 0)) {
         const double wf = 1.0 - p.wfb;
         auto lidu = [&](int a, int b) { return gload(p.uLid, p, t.gx(a), t.gy(b), MAP_N, MAP_S); };
         auto lidv = [&](int a, int b) { return gload(p.vLid, p, t.gx(a), t.gy(b), MAP_S, MAP_N); };
-        auto usq = [&](int a, int b) { const double r = wf * AT(su, a, b) - lidu(a, b); return r * r; };
-        auto vsq = [&](int a, int b) { const double r = wf * AT(sv, a, b) - lidv(a, b); return r * r; };
+        // the surface velocity: the top layer's, or the mixed-layer average of the pre-pass
+        auto sfu = [&](int a, int b) {
+          return p.drag_surf ? drag_load(p.dragv + 2 * p.lstride, p, t.gx(a), t.gy(b), MAP_N, MAP_S) : AT(su, a, b);
+        };
+        auto sfv = [&](int a, int b) {
+          return p.drag_surf ? drag_load(p.dragv + 3 * p.lstride, p, t.gx(a), t.gy(b), MAP_S, MAP_N) : AT(sv, a, b);
+        };
+        auto usq = [&](int a, int b) { const double r = wf * sfu(a, b) - lidu(a, b); return r * r; };
+        auto vsq = [&](int a, int b) { const double r = wf * sfv(a, b) - lidv(a, b); return r * r; };
         auto uab = [&](int a, int b) { return sqrt(0.5 * (usq(a, b) + usq(a + 1, b)) + 0.5 * (vsq(a, b) + vsq(a, b + 1))); };
         if (hwest != 0) {
           const double ua = 0.5 * (uab(i, j) + uab(i - 1, j));
@@ -1062,6 +1127,10 @@ int launch_t(const TendParams& p, cudaStream_t s) {
     attr_done = true;
   }
   if (shm > 200 * 1024) return -1;
+  if (p.drag_bot || p.drag_surf) {
+    dim3 b(32, 8), g((p.Nx + 31) / 32, (p.Ny + 7) / 8);
+    drag_speed_kernel<TS><<<g, b, 0, s>>>(p);
+  }
   dim3 grid((p.Nx + TX - 1) / TX, (p.Ny + TY - 1) / TY);
   tendency_kernel<MS, TS, H><<<grid, NT, shm, s>>>(p);
   return 0;

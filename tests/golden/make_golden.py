@@ -116,6 +116,11 @@ BUD_CASES = {
     "gyre_fractions_budget": (inputs.gyre, dict(N=20, Ny=12, dt=600.0, solver=0,
                                                 extra=dict(hsml=1500.0, hmin_surf=5.0, hbbl=500.0, hmin_bot=10.0,
                                                            linDragSurf=1e-4, thicknessScheme=3)), None),
+    # quadratic bottom and surface drag over boundary layers that span both layers
+    "gyre_quad_fractions_budget": (inputs.gyre, dict(N=20, Ny=12, dt=600.0, solver=0,
+                                                     extra=dict(quadDragCoeff=2e-3, hbbl=3500.0, hmin_bot=10.0,
+                                                                quadDragSurf=1e-3, hsml=1200.0, hmin_surf=5.0,
+                                                                windFeedback=1, oceanSurfDrag=1)), None),
 }
 # the acceptance point of the plain FP64 path: config 0 (128 x 128 x 2 double gyre, red-black
 # SOR with SOR_rp 1.8, tol 1e-10) at its stable dt of 900 s, 100 steps; the fixture keeps every

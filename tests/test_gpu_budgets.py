@@ -26,7 +26,8 @@ pytestmark = pytest.mark.gpu
 
 DRIVER = os.path.join(ROOT, "pawsim_b200", "bin", "PAWSIM_B200.exe")
 CASES = ["gyre_sor_budget", "full_sor_budget", "gyre_hk83_a4_budget", "jets_tracer_budget", "gyre_quad_budget",
-         "gyre_fractions_budget", "jets_diadiff_budget", "gyre_relax_fbaro_budget"]
+         "gyre_fractions_budget", "jets_diadiff_budget", "gyre_relax_fbaro_budget",
+         "gyre_quad_fractions_budget"]
 
 
 @pytest.mark.parametrize("name", CASES)

@@ -1,7 +1,7 @@
 """The optional physics of the tendency against the oracle, bit for bit, through the C ABI:
 UP3 and KT00 thickness (3-cell tile halo, also in the pressure right-hand side),
 Smagorinsky A2 and A4, quadratic bottom and surface drag (with wind feedback), and the
-hsml / hbbl layer fractions of wind and linear drag. Each case is checked as a tendency
+hsml / hbbl layer fractions of wind, linear and quadratic drag. Each case is checked as a tendency
 after the preliminary correction and over 5 SOR steps (state, pi and iteration count); the
 oracle itself is bit-identical to the reference binary on these options
 (tests/test_oracle_physics.py)."""
@@ -28,6 +28,15 @@ CASES = {
                                extra=dict(hsml=1500.0, hmin_surf=5.0, hbbl=500.0, hmin_bot=10.0, linDragSurf=1e-4))),
     "fractions_kt00_quad": ("gyre", dict(N=40, Ny=24, dt=600.0, solver=0,
                                          extra=dict(hsml=800.0, thicknessScheme=3, quadDragCoeff=1e-3))),
+    # quadratic drag whose boundary layer spans several layers (forcing.c:95-143, 181-223)
+    "quad_hbbl": ("gyre", dict(N=40, Ny=24, dt=600.0, solver=0,
+                               extra=dict(quadDragCoeff=2e-3, hbbl=3500.0, hmin_bot=10.0))),
+    "quad_surf_hsml": ("gyre", dict(N=40, Ny=24, dt=600.0, solver=0,
+                                    extra=dict(quadDragSurf=1e-3, windFeedback=1, oceanSurfDrag=1, hsml=1200.0,
+                                               hmin_surf=5.0))),
+    "quad_both_fractions_jets": ("jets", dict(N=32, dt=100.0, solver=0,
+                                              extra=dict(quadDragCoeff=2e-3, hbbl=3800.0, quadDragSurf=1e-3,
+                                                         hsml=700.0, thicknessScheme=1))),
 }
 
 
@@ -61,8 +70,3 @@ def test_physics_bitwise(tmp_path, oracle_mod, lib, name):
             assert value_equal(s_g[var], s_o[var]), (n, var, np.abs(s_g[var] - s_o[var]).max())
         assert value_equal(m.get("pi"), o.get("pi")), n
 
-
-def test_quadratic_drag_with_fraction_depth_is_rejected(tmp_path, lib):
-    _, cfg, f = make_setup(tmp_path, "gyre", N=16, dt=600.0, solver=0, extra=dict(quadDragCoeff=1e-3, hbbl=300.0))
-    with pytest.raises(lib.PawsimError):
-        lib.Model(cfg, f)

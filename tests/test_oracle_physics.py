@@ -18,6 +18,14 @@ CASES = {
     "fractions": ("gyre", dict(N=24, Ny=16, dt=600.0, solver=0,
                                extra=dict(hsml=1500.0, hbbl=500.0, linDragSurf=1e-4))),
     "quad_hbbl": ("gyre", dict(N=24, Ny=16, dt=600.0, solver=0, extra=dict(quadDragCoeff=2e-3, hbbl=500.0, hmin_bot=10.0))),
+    "quad_hbbl_deep": ("gyre", dict(N=24, Ny=16, dt=600.0, solver=0,
+                                    extra=dict(quadDragCoeff=2e-3, hbbl=3500.0, hmin_bot=10.0))),
+    "quad_surf_hsml": ("gyre", dict(N=24, Ny=16, dt=600.0, solver=0,
+                                    extra=dict(quadDragSurf=1e-3, windFeedback=1, oceanSurfDrag=1, hsml=1200.0,
+                                               hmin_surf=5.0))),
+    "quad_both_fractions_jets": ("jets", dict(N=24, dt=100.0, solver=0,
+                                              extra=dict(quadDragCoeff=2e-3, hbbl=3800.0, quadDragSurf=1e-3,
+                                                         hsml=700.0, thicknessScheme=1))),
 }
 
 
