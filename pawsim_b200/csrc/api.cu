@@ -556,14 +556,13 @@ static TendParams base_params(Model* m) {
   return p;
 }
 
-// A fill of the work arrays in the reference: record its corner shadow (faces 1: the
-// tendency's per-cell face thickness, 2: the gathered one of the pressure path) from state
-// buffer `sb`, and make it the latest.
-static void corner_fill(Model* m, int sb, int faces) {
+// A fill of the work arrays in the reference (pawsim_work_load_state): record its corner
+// shadow from state buffer `sb` into the other shadow buffer (the kernels of this fill may
+// still read the current one) and make it the latest.
+static void corner_fill(Model* m, int sb) {
   if (!m->corner[0]) return;
   const int nx = 1 - m->corner_cur;
-  launch_corner_capture(m->grid2(), m->u[sb], m->v[sb], m->h[sb], m->b[0] ? m->b[sb] : nullptr,
-                        m->corner[m->corner_cur], m->corner[nx], faces, m->s);
+  launch_corner_capture(m->grid2(), m->u[sb], m->v[sb], m->h[sb], m->b[0] ? m->b[sb] : nullptr, m->corner[nx], m->s);
   ++g_launches;
   m->corner_cur = nx;
 }
@@ -608,7 +607,7 @@ static int tendency_eval(Model* m) {
   if (launch_step_kernel(m, p) != 0)
     return fail(PAWSIM_GPU_EUNSUPPORTED, "scheme combination not available");
   g_launches += (p.drag_bot || p.drag_surf) ? 2 : 1;   // the drag pre-pass and the fused kernel
-  corner_fill(m, m->cur, 1);   // the tendency's load_state and face thickness
+  corner_fill(m, m->cur);   // the tendency's load_state and face thickness
   PAWSIM_CUDA_OK(cudaGetLastError());
   return 0;
 }
@@ -666,7 +665,7 @@ static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
     launch_tracer(tp, m->s);
     ++g_launches;
   }
-  corner_fill(m, m->cur, 1);   // the tendency's load_state and face thickness (state of the step start)
+  corner_fill(m, m->cur);   // the tendency's load_state and face thickness (state of the step start)
   PAWSIM_CUDA_OK(cudaGetLastError());
   if (shift) m->h1 = h2;
   m->cur = nb;
@@ -704,7 +703,7 @@ static int pressure_correct(Model* m, int update_diags, pawsim_gpu_stats* st) {
   }
   m->thickness_fixed = false;
   g_launches += launch_pressure_rhs(g, m->u[cur], m->v[cur], m->h[cur], m->rhs, m->s);
-  corner_fill(m, cur, 2);   // build_rhs reloads the corrected state (pressure.c:570-606)
+  corner_fill(m, cur);   // build_rhs reloads the corrected state (pressure.c:570-606)
   launch_sum(m->rhs, m->Nx, m->Ny, m->pitch, m->serial(), m->scratch, m->dsum, m->s);
   launch_subtract_mean(m->rhs, m->Nx, m->Ny, m->pitch, m->dsum, m->s);
   g_launches += m->serial() ? 2 : 3;
@@ -790,7 +789,7 @@ static int pressure_correct(Model* m, int update_diags, pawsim_gpu_stats* st) {
     launch_projection(g, m->pi, m->u[cur], m->v[cur], m->s);
   ++g_launches;
   if (m->c.pressure_timing) {
-    corner_fill(m, cur, 2);   // the divergence norms reload the projected state (pressure.c:693-737)
+    corner_fill(m, cur);   // the divergence norms reload the projected state (pressure.c:693-737)
     g_launches += launch_divergence_field(g, m->u[cur], m->v[cur], m->h[cur], m->work, m->s);
     int r = finish_norms(m, m->work, &local.div_max, &local.div_rms);
     if (r) return r;
@@ -918,7 +917,7 @@ int pawsim_gpu_accumulate_averages(pawsim_gpu* h, double avg_fac) {
   a.b = m->b[0] ? m->b[m->cur] : nullptr;
   a.use_buoy = m->c.use_buoyancy;
   a.ab = m->b[0] ? a.api + ls : nullptr;
-  corner_fill(m, m->cur, 2);   // the averages reload the state (diagnostics.c:320-324)
+  corner_fill(m, m->cur);   // the averages reload the state (diagnostics.c:320-324)
   launch_accumulate_averages(m->grid2(), a, m->s);
   ++g_launches;
   PAWSIM_CUDA_OK(cudaGetLastError());

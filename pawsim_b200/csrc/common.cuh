@@ -84,15 +84,18 @@ inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 // ---- corner ghosts of the reference's serial build on x-periodic, y-walled grids.
 // There a halo fill copies whole columns periodically in x first, ghost rows included, and
 // only then fills the wall ghost rows of the owned columns (model_code/field.c:353-532), so
-// the four corner blocks keep what the wall rows at the periodic image columns held after
-// the previous fill of the same array. The library keeps those values in a small "corner
-// shadow": per field and layer the owned values of the previous fill at the 3 columns next to
-// each side of the periodic seam and the 4 rows next to each wall. A load at a corner position
-// reads the shadow through the wall mirror instead of the current field.
-constexpr int CORNER_F = 6;        // u, v, h and h_west, h_south of the work arrays, tracer b
+// the four corner blocks receive what the ghost rows of the periodic image columns held
+// before this fill. For the copied work arrays (u, v, h, b: pawsim_work_load_state,
+// work.c:538-559) that is the previous fill's wall mirror. The library keeps those values in a
+// small "corner shadow": per field and layer the owned values of the previous fill at the 3
+// columns next to each side of the periodic seam and the 4 rows next to each wall. A load at a
+// corner position reads the shadow through the wall mirror instead of the current field.
+// (Fields computed over the ghosted array before their fill, such as the face thickness, get
+// at a corner the value computed at the periodic image: corner_face below.)
+constexpr int CORNER_F = 4;        // u, v, h and the tracer b of the work arrays
 constexpr int CORNER_R = 4;        // rows from each wall
 constexpr int CORNER_C = 6;        // columns: x = 0, 1, 2 and Nx-3, Nx-2, Nx-1
-enum { CF_U, CF_V, CF_H, CF_HW, CF_HS, CF_B };
+enum { CF_U, CF_V, CF_H, CF_B };
 
 __host__ __device__ inline size_t corner_elems(int L) {
   return (size_t)CORNER_F * L * 2 * CORNER_R * CORNER_C;
@@ -121,6 +124,67 @@ __host__ __device__ inline double corner_load(const double* buf, int f, int k, i
   }
   if (y < 0) return buf[corner_slot(f, k, L, 0, -y - 1, c)];
   return buf[corner_slot(f, k, L, 1, y - Ny, c)];
+}
+
+// The face thickness h_west (west) or h_south of one layer at a corner ghost (x, y) of an
+// x-periodic, y-walled grid in the serial build: calc_face_thickness_layer (work.c:566-684)
+// evaluates its formula over the ghosted array, then the fill copies into the corner the value
+// at the periodic image (wrap(x), y), computed from the work copy of h whose own corner ghosts
+// hold the previous fill (the shadow `sh`). uv is the layer's u (west) or v, read for the sign
+// of the upwind schemes. ts: 0 AL81, 1 HK83, 2 UP3, 3 KT00 (the same expression order as the
+// tile kernels' face_west / face_south). At an owned (x, y) it is the cell's own face thickness
+// with the corner ghosts of its stencil taken from the shadow.
+__device__ inline double corner_minmod3(double a, double b, double c) {
+  if ((a > 0) && (b > 0) && (c > 0)) return fmin(a, fmin(b, c));
+  if ((a < 0) && (b < 0) && (c < 0)) return fmax(a, fmax(b, c));
+  return 0;
+}
+template <bool WEST>
+__device__ inline double corner_face(const double* h, const double* uv, int pitch, int Nx, int Ny, int ts, double sig,
+                                     const double* sh, int k, int L, int x, int y) {
+  const int i = wrap_index(x, Nx), j = y;
+  auto H = [&](int a, int b) {
+    if (is_corner(a, b, Nx, Ny)) return corner_load(sh, CF_H, k, L, a, b, Nx, Ny, MAP_S);
+    return load_mapped(h, pitch, a, b, Nx, Ny, false, true, MAP_S, MAP_S);
+  };
+  if (WEST) {
+    if (ts == 1)
+      return (1.0 / 3) * (H(i, j) + H(i - 1, j) + 0.25 * (H(i, j + 1) + H(i - 1, j + 1) + H(i, j - 1) + H(i - 1, j - 1)));
+    if (ts == 2 || ts == 3) {
+      const double uc = load_mapped(uv, pitch, i, j, Nx, Ny, false, true, MAP_N, MAP_S);
+      if (ts == 2) {
+        const double d2m = H(i, j) - 2 * H(i - 1, j) + H(i - 2, j);
+        const double d2c = H(i + 1, j) - 2 * H(i, j) + H(i - 1, j);
+        return 0.5 * (H(i, j) + H(i - 1, j)) - (1 / 6.0) * ((uc > 0) ? d2m : d2c);
+      }
+      const double dm = corner_minmod3(sig * (H(i, j) - H(i - 1, j)), 0.5 * (H(i, j) - H(i - 2, j)),
+                                       sig * (H(i - 1, j) - H(i - 2, j)));
+      const double dc = corner_minmod3(sig * (H(i + 1, j) - H(i, j)), 0.5 * (H(i + 1, j) - H(i - 1, j)),
+                                       sig * (H(i, j) - H(i - 1, j)));
+      const double xm = H(i - 1, j) + 0.5 * dm;
+      const double xp = H(i, j) - 0.5 * dc;
+      return (uc > 0) ? xm : xp;
+    }
+    return 0.5 * (H(i, j) + H(i - 1, j));
+  }
+  if (ts == 1)
+    return (1.0 / 3) * (H(i, j) + H(i, j - 1) + 0.25 * (H(i + 1, j) + H(i - 1, j) + H(i + 1, j - 1) + H(i - 1, j - 1)));
+  if (ts == 2 || ts == 3) {
+    const double vc = load_mapped(uv, pitch, i, j, Nx, Ny, false, true, MAP_S, MAP_N);
+    if (ts == 2) {
+      const double d2m = H(i, j) - 2 * H(i, j - 1) + H(i, j - 2);
+      const double d2c = H(i, j + 1) - 2 * H(i, j) + H(i, j - 1);
+      return 0.5 * (H(i, j) + H(i, j - 1)) - (1 / 6.0) * ((vc > 0) ? d2m : d2c);
+    }
+    const double dm = corner_minmod3(sig * (H(i, j) - H(i, j - 1)), 0.5 * (H(i, j) - H(i, j - 2)),
+                                     sig * (H(i, j - 1) - H(i, j - 2)));
+    const double dc = corner_minmod3(sig * (H(i, j + 1) - H(i, j)), 0.5 * (H(i, j + 1) - H(i, j - 1)),
+                                     sig * (H(i, j) - H(i, j - 1)));
+    const double ym = H(i, j - 1) + 0.5 * dm;
+    const double yp = H(i, j) + 0.5 * dc;
+    return (vc > 0) ? ym : yp;
+  }
+  return 0.5 * (H(i, j) + H(i, j - 1));
 }
 
 // x / d rounded to nearest, given r = 1/d rounded to nearest. Markstein's theorem: when q

@@ -771,50 +771,12 @@ __global__ void ez_final_kernel(const double* __restrict__ partials, int nblocks
 inline dim3 grid2(int Nx, int Ny, dim3 b) { return dim3((Nx + b.x - 1) / b.x, (Ny + b.y - 1) / b.y); }
 
 // ---------------------------------------------------------------- corner shadow capture
-// A fill of the work arrays in the reference (pawsim_work_load_state, work.c:538-559, and the
-// face-thickness fills that follow it) leaves in the wall rows next to the periodic seam the
-// values the next fill copies into the corner ghosts. This kernel records them: u, v, h (and
-// b) at the capture, and h_west, h_south as that fill computes them -- by the gathered formula
-// of pawsim_work_calc_face_thickness_no_ghost (work.c:865-1118; the pressure RHS, the
-// divergence norms, the online averages) or by the per-cell formula of
-// calc_face_thickness_layer (work.c:566-684; the tendency), whose HK83 stencil reaches the
-// corner ghosts of the previous fill.
-__device__ inline double face_w_formula(int ts, double sig, double uc, const double* Hm, const double* H0,
-                                        const double* Hp) {
-  // Hm, H0, Hp: h at x-2..x+1 on rows y-1, y, y+1 (index 0 is x-2)
-  if (ts == 1) return (1.0 / 3) * (H0[2] + H0[1] + 0.25 * (Hp[2] + Hp[1] + Hm[2] + Hm[1]));
-  if (ts == 2) {
-    const double d2m = H0[2] - 2 * H0[1] + H0[0];
-    const double d2c = H0[3] - 2 * H0[2] + H0[1];
-    return 0.5 * (H0[2] + H0[1]) - (1 / 6.0) * ((uc > 0) ? d2m : d2c);
-  }
-  if (ts == 3) {
-    const double dm = minmod3(sig * (H0[2] - H0[1]), 0.5 * (H0[2] - H0[0]), sig * (H0[1] - H0[0]));
-    const double dc = minmod3(sig * (H0[3] - H0[2]), 0.5 * (H0[3] - H0[1]), sig * (H0[2] - H0[1]));
-    return (uc > 0) ? H0[1] + 0.5 * dm : H0[2] - 0.5 * dc;
-  }
-  return 0.5 * (H0[2] + H0[1]);
-}
-__device__ inline double face_s_formula(int ts, double sig, double vc, const double* Vm, const double* V0,
-                                        const double* Vp) {
-  // V0: h at y-2..y+1 on column x; Vm, Vp: the same on columns x-1, x+1
-  if (ts == 1) return (1.0 / 3) * (V0[2] + V0[1] + 0.25 * (Vp[2] + Vm[2] + Vp[1] + Vm[1]));
-  if (ts == 2) {
-    const double d2m = V0[2] - 2 * V0[1] + V0[0];
-    const double d2c = V0[3] - 2 * V0[2] + V0[1];
-    return 0.5 * (V0[2] + V0[1]) - (1 / 6.0) * ((vc > 0) ? d2m : d2c);
-  }
-  if (ts == 3) {
-    const double dm = minmod3(sig * (V0[2] - V0[1]), 0.5 * (V0[2] - V0[0]), sig * (V0[1] - V0[0]));
-    const double dc = minmod3(sig * (V0[3] - V0[2]), 0.5 * (V0[3] - V0[1]), sig * (V0[2] - V0[1]));
-    return (vc > 0) ? V0[1] + 0.5 * dm : V0[2] + 0.5 * dc;
-  }
-  return 0.5 * (V0[2] + V0[1]);
-}
-
+// A fill of the work arrays in the reference (pawsim_work_load_state, work.c:538-559) leaves
+// in the wall rows next to the periodic seam the values that the next fill copies into the
+// corner ghosts: the state it copied. This kernel records them (u, v, h, and b when given).
 __global__ void corner_capture_kernel(const Grid2 g, const double* __restrict__ u, const double* __restrict__ v,
                                       const double* __restrict__ h, const double* __restrict__ b,
-                                      const double* __restrict__ prev, double* __restrict__ next, int faces) {
+                                      double* __restrict__ next) {
   const int L = g.L;
   const int per_layer = 2 * CORNER_R * CORNER_C;
   const int total = CORNER_F * L * per_layer;
@@ -825,32 +787,12 @@ __global__ void corner_capture_kernel(const Grid2 g, const double* __restrict__ 
     const int r = (t / CORNER_C) % CORNER_R;
     const int c = t % CORNER_C;
     const int x = corner_x(c, g.Nx), y = corner_y(side, r, g.Ny);
-    const size_t lk = (size_t)k * g.lstride;
-    const size_t o = lk + (size_t)y * g.pitch + x;
+    const size_t o = (size_t)k * g.lstride + (size_t)y * g.pitch + x;
     double val = 0;
     if (f == CF_U) val = u[o];
     else if (f == CF_V) val = v[o];
     else if (f == CF_H) val = h[o];
-    else if (f == CF_B) val = b ? b[o] : 0.0;
-    else if (faces == 2) {
-      val = f == CF_HW ? hw_gathered(g, h + lk, u + lk, x, y) : hs_gathered(g, h + lk, v + lk, x, y);
-    } else {
-      // the per-cell formula on the work copy of h, whose corner ghosts hold the previous fill
-      auto H = [&](int a, int bb) {
-        if (is_corner(a, bb, g.Nx, g.Ny)) return corner_load(prev, CF_H, k, L, a, bb, g.Nx, g.Ny, MAP_S);
-        return load_mapped(h + lk, g.pitch, a, bb, g.Nx, g.Ny, g.wall_ew, g.wall_ns, MAP_S, MAP_S);
-      };
-      double A[3][4];
-      if (f == CF_HW) {
-        for (int dy = -1; dy <= 1; ++dy)
-          for (int dx = -2; dx <= 1; ++dx) A[dy + 1][dx + 2] = H(x + dx, y + dy);
-        val = face_w_formula(g.thick_scheme, g.kt00_sigma, u[o], A[0], A[1], A[2]);
-      } else {
-        for (int dx = -1; dx <= 1; ++dx)
-          for (int dy = -2; dy <= 1; ++dy) A[dx + 1][dy + 2] = H(x + dx, y + dy);
-        val = face_s_formula(g.thick_scheme, g.kt00_sigma, v[o], A[0], A[1], A[2]);
-      }
-    }
+    else val = b ? b[o] : 0.0;
     next[corner_slot(f, k, L, side, r, c)] = val;
   }
 }
@@ -858,8 +800,8 @@ __global__ void corner_capture_kernel(const Grid2 g, const double* __restrict__ 
 }  // namespace
 
 void launch_corner_capture(const Grid2& g, const double* u, const double* v, const double* h, const double* b,
-                           const double* prev, double* next, int faces, cudaStream_t s) {
-  corner_capture_kernel<<<1, 256, 0, s>>>(g, u, v, h, b, prev, next, faces);
+                           double* next, cudaStream_t s) {
+  corner_capture_kernel<<<1, 256, 0, s>>>(g, u, v, h, b, next);
 }
 
 void launch_accumulate_averages(const Grid2& g, const AvgParams& a, cudaStream_t s) {

@@ -22,10 +22,9 @@ int launch_pressure_rhs(const Grid2& g, const double* u, const double* v, const 
                          double* rhs, cudaStream_t s);
 
 // Record the corner shadow (common.cuh) of a work-array fill of the state u, v, h (b nullable)
-// into `next`: faces = 2 forms h_west, h_south by the gathered formula of the pressure path,
-// faces = 1 by the tendency's per-cell formula with the corner ghosts of `prev`.
+// into `next`.
 void launch_corner_capture(const Grid2& g, const double* u, const double* v, const double* h, const double* b,
-                           const double* prev, double* next, int faces, cudaStream_t s);
+                           double* next, cudaStream_t s);
 
 // sum of the owned cells in the reference's serial order (x outer, y inner) or in a fixed
 // pairwise tree; the result is written to *out (device). `partials` needs

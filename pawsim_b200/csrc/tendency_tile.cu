@@ -170,26 +170,47 @@ __device__ inline double face_south(const double* h, const double* v, double sig
   return 0.5 * (AT(h, i, j) + AT(h, i, j - 1));
 }
 
-// kinetic energy of the Bernoulli function (work.c:1437-1499)
-template <int MS, int RW>
-__device__ inline double kinetic(const double* u, const double* v, int i, int j) {
+// kinetic energy of the Bernoulli function (work.c:1437-1499); U(a, b), V(a, b) read the
+// layer's velocities
+template <int MS, typename UF, typename VF>
+__device__ inline double kinetic_f(UF U, VF V, int i, int j) {
   if (MS == 1) {
-    return (sq(AT(u, i + 1, j)) + sq(AT(u, i, j))
-            + 0.25 * (sq(AT(u, i + 1, j + 1)) + sq(AT(u, i, j + 1)) + sq(AT(u, i + 1, j - 1)) + sq(AT(u, i, j - 1)))
-            + sq(AT(v, i, j + 1)) + sq(AT(v, i, j))
-            + 0.25 * (sq(AT(v, i + 1, j + 1)) + sq(AT(v, i + 1, j)) + sq(AT(v, i - 1, j + 1)) + sq(AT(v, i - 1, j)))) / 6;
+    return (sq(U(i + 1, j)) + sq(U(i, j))
+            + 0.25 * (sq(U(i + 1, j + 1)) + sq(U(i, j + 1)) + sq(U(i + 1, j - 1)) + sq(U(i, j - 1)))
+            + sq(V(i, j + 1)) + sq(V(i, j))
+            + 0.25 * (sq(V(i + 1, j + 1)) + sq(V(i + 1, j)) + sq(V(i - 1, j + 1)) + sq(V(i - 1, j)))) / 6;
   }
   if (MS == 3) {
-    return 0.25 * ((2.0 / 3.0) * sq(AT(u, i, j))
-                   + (1.0 / 3.0) * sq(0.5 * (AT(u, i - 1, j) + AT(u, i + 1, j)))
-                   + (2.0 / 3.0) * sq(AT(u, i + 1, j))
-                   + (1.0 / 3.0) * sq(0.5 * (AT(u, i, j) + AT(u, i + 2, j)))
-                   + (2.0 / 3.0) * sq(AT(v, i, j))
-                   + (1.0 / 3.0) * sq(0.5 * (AT(v, i, j - 1) + AT(v, i, j + 1)))
-                   + (2.0 / 3.0) * sq(AT(v, i, j + 1))
-                   + (1.0 / 3.0) * sq(0.5 * (AT(v, i, j) + AT(v, i, j + 2))));
+    return 0.25 * ((2.0 / 3.0) * sq(U(i, j))
+                   + (1.0 / 3.0) * sq(0.5 * (U(i - 1, j) + U(i + 1, j)))
+                   + (2.0 / 3.0) * sq(U(i + 1, j))
+                   + (1.0 / 3.0) * sq(0.5 * (U(i, j) + U(i + 2, j)))
+                   + (2.0 / 3.0) * sq(V(i, j))
+                   + (1.0 / 3.0) * sq(0.5 * (V(i, j - 1) + V(i, j + 1)))
+                   + (2.0 / 3.0) * sq(V(i, j + 1))
+                   + (1.0 / 3.0) * sq(0.5 * (V(i, j) + V(i, j + 2))));
   }
-  return (sq(AT(u, i + 1, j)) + sq(AT(u, i, j))) / 4 + (sq(AT(v, i, j + 1)) + sq(AT(v, i, j))) / 4;
+  return (sq(U(i + 1, j)) + sq(U(i, j))) / 4 + (sq(V(i, j + 1)) + sq(V(i, j))) / 4;
+}
+template <int MS, int RW>
+__device__ inline double kinetic(const double* u, const double* v, int i, int j) {
+  return kinetic_f<MS>([&](int a, int b) { return AT(u, a, b); }, [&](int a, int b) { return AT(v, a, b); }, i, j);
+}
+// the same at raw (x, y) of the serial build's work arrays on an x-periodic, y-walled grid,
+// evaluated at the periodic image of x, with the corner ghosts of the stencil from the shadow
+// (the value the fill copies into a periodic ghost column, common.cuh)
+template <int MS>
+__device__ inline double kinetic_image(const double* uk, const double* vk, int pitch, int Nx, int Ny, const double* sh,
+                                       int k, int L, int x, int y) {
+  auto U = [&](int a, int b) {
+    if (is_corner(a, b, Nx, Ny)) return corner_load(sh, CF_U, k, L, a, b, Nx, Ny, MAP_S);
+    return load_mapped(uk, pitch, a, b, Nx, Ny, false, true, MAP_N, MAP_S);
+  };
+  auto V = [&](int a, int b) {
+    if (is_corner(a, b, Nx, Ny)) return corner_load(sh, CF_V, k, L, a, b, Nx, Ny, MAP_N);
+    return load_mapped(vk, pitch, a, b, Nx, Ny, false, true, MAP_S, MAP_N);
+  };
+  return kinetic_f<MS>(U, V, wrap_index(x, Nx), y);
 }
 
 __device__ inline double gload(const double* f, const TendParams& p, int gi, int gj, int kx, int ky) {
@@ -247,6 +268,23 @@ __device__ inline double gface_south(const TendParams& p, const double* h, const
   return 0.5 * (H(i, j) + H(i, j - 1));
 }
 
+// face thickness of layer k at an owned cell from global memory; on x-periodic, y-walled grids
+// with the serial build's corners the stencil's corner ghosts come from the corner shadow
+template <int TS>
+__device__ inline double face_west_cell(const TendParams& p, int k, int i, int j) {
+  if (p.corners)
+    return corner_face<true>(p.h + k * p.lstride, p.u + k * p.lstride, p.pitch, p.Nx, p.Ny, TS, p.kt00_sigma,
+                             p.corners, k, p.L, i, j);
+  return gface_west<TS>(p, p.h + k * p.lstride, p.u + k * p.lstride, i, j);
+}
+template <int TS>
+__device__ inline double face_south_cell(const TendParams& p, int k, int i, int j) {
+  if (p.corners)
+    return corner_face<false>(p.h + k * p.lstride, p.v + k * p.lstride, p.pitch, p.Nx, p.Ny, TS, p.kt00_sigma,
+                              p.corners, k, p.L, i, j);
+  return gface_south<TS>(p, p.h + k * p.lstride, p.v + k * p.lstride, i, j);
+}
+
 // Surface and bottom layer fractions of every layer at owned cell (gi, gj) (work.c:2151-2340):
 // out(f, k, value) receives f = 0 hFsurf_west, 1 hFsurf_south, 2 hFbot_west, 3 hFbot_south,
 // zeros included. hsml <= 0 puts the whole surface forcing in the top layer, hbbl <= 0 the
@@ -256,8 +294,8 @@ __device__ inline void cell_fractions(const TendParams& p, int gi, int gj, Out o
   const int L = p.L;
   double hwk[LMAX], hsk[LMAX];
   for (int k = 0; k < L; ++k) {
-    hwk[k] = gface_west<TS>(p, p.h + k * p.lstride, p.u + k * p.lstride, gi, gj);
-    hsk[k] = gface_south<TS>(p, p.h + k * p.lstride, p.v + k * p.lstride, gi, gj);
+    hwk[k] = face_west_cell<TS>(p, k, gi, gj);
+    hsk[k] = face_south_cell<TS>(p, k, gi, gj);
   }
   for (int f = 0; f < 4; ++f)
     for (int k = 0; k < L; ++k) out(f, k, 0.0);
@@ -529,9 +567,13 @@ tendency_kernel(const __grid_constant__ TendParams p) {
       int lx = q % RW, ly = q / RW;
       const bool nr = t.near(lx, ly);
       if (lx >= H - 1 && lx <= TX + H && ly >= H - 1 && ly <= TY + H && nr) {
-        if (p.corners && !inner && is_corner(t.gx(lx), t.gy(ly), p.Nx, p.Ny)) {
-          F[F_HW][q] = corner_load(p.corners, CF_HW, k, L, t.gx(lx), t.gy(ly), p.Nx, p.Ny, MAP_S);
-          F[F_HS][q] = corner_load(p.corners, CF_HS, k, L, t.gx(lx), t.gy(ly), p.Nx, p.Ny, MAP_S);
+        // a periodic ghost column (its corners included) receives the values computed at the
+        // image column, whose stencil reads the corner shadow (serial build, common.cuh)
+        if (p.corners && !inner && (t.gx(lx) < 0 || t.gx(lx) >= p.Nx)) {
+          F[F_HW][q] = corner_face<true>(hkp, uk, p.pitch, p.Nx, p.Ny, TS, p.kt00_sigma, p.corners, k, L, t.gx(lx),
+                                         t.gy(ly));
+          F[F_HS][q] = corner_face<false>(hkp, vk, p.pitch, p.Nx, p.Ny, TS, p.kt00_sigma, p.corners, k, L, t.gx(lx),
+                                          t.gy(ly));
         } else {
           int mx = t.mlx(lx), my = t.mly(ly);
           F[F_HW][q] = face_west<TS, RW>(sh, su, p.kt00_sigma, mx, my);
@@ -549,7 +591,10 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         F[F_HQ][q] = hq;
       }
       if (lx >= H - 1 && lx <= TX + H - 1 && ly >= H - 1 && ly <= TY + H - 1) {
-        F[F_KE][q] = nr ? kinetic<MS, RW>(su, sv, t.mlx(lx), t.mly(ly)) : 0.0;
+        if (nr && p.corners && !inner && (t.gx(lx) < 0 || t.gx(lx) >= p.Nx) && t.gy(ly) >= 0 && t.gy(ly) < p.Ny)
+          F[F_KE][q] = kinetic_image<MS>(uk, vk, p.pitch, p.Nx, p.Ny, p.corners, k, L, t.gx(lx), t.gy(ly));
+        else
+          F[F_KE][q] = nr ? kinetic<MS, RW>(su, sv, t.mlx(lx), t.mly(ly)) : 0.0;
       }
       if (p.useA2 || p.useA4) {
         if (lx >= H - 2 && lx <= RW - 2 && ly >= H - 2 && ly <= RH - 2)
@@ -782,10 +827,10 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         for (int s = 0; s < 2; ++s) {
           int kk = k + s;                    // interface kk between layers kk-1 and kk
           if (kk < 1 || kk > L - 1) continue;
-          double hwa = gface_west<TS>(p, p.h + (kk - 1) * p.lstride, p.u + (kk - 1) * p.lstride, gi, gj);
-          double hwb = gface_west<TS>(p, p.h + kk * p.lstride, p.u + kk * p.lstride, gi, gj);
-          double hsa = gface_south<TS>(p, p.h + (kk - 1) * p.lstride, p.v + (kk - 1) * p.lstride, gi, gj);
-          double hsb = gface_south<TS>(p, p.h + kk * p.lstride, p.v + kk * p.lstride, gi, gj);
+          double hwa = face_west_cell<TS>(p, kk - 1, gi, gj);
+          double hwb = face_west_cell<TS>(p, kk, gi, gj);
+          double hsa = face_south_cell<TS>(p, kk - 1, gi, gj);
+          double hsb = face_south_cell<TS>(p, kk, gi, gj);
           double dzu = 0.5 * (hwb + hwa);
           double dzv = 0.5 * (hsb + hsa);
           double nuu = gload(p.nu_u + kk * p.lstride, p, gi, gj, MAP_N, MAP_S);

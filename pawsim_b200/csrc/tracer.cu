@@ -139,9 +139,11 @@ __global__ void __launch_bounds__(TNT) tracer_tile_kernel(const TracerParams p) 
       const int gx = X0 - TH + lx, gy = Y0 - TH + ly;
       const bool nr = gx >= -2 && gx < p.Nx + 2 && gy >= -2 && gy < p.Ny + 2;
       const int mx = mlx(lx), my = mly(ly);
-      if (nr && p.corners && !inner && is_corner(gx, gy, p.Nx, p.Ny)) {
-        S[T_HW][q] = corner_load(p.corners, CF_HW, k, p.L, gx, gy, p.Nx, p.Ny, MAP_S);
-        S[T_HS][q] = corner_load(p.corners, CF_HS, k, p.L, gx, gy, p.Nx, p.Ny, MAP_S);
+      if (nr && p.corners && !inner && (gx < 0 || gx >= p.Nx)) {
+        S[T_HW][q] = corner_face<true>(hk, uk, p.pitch, p.Nx, p.Ny, p.thick_scheme, p.kt00_sigma, p.corners, k, p.L,
+                                       gx, gy);
+        S[T_HS][q] = corner_face<false>(hk, vk, p.pitch, p.Nx, p.Ny, p.thick_scheme, p.kt00_sigma, p.corners, k, p.L,
+                                        gx, gy);
       } else {
         S[T_HW][q] = nr ? face_w(mx, my) : 0.0;
         S[T_HS][q] = nr ? face_s(mx, my) : 0.0;
