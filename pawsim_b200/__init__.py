@@ -244,6 +244,8 @@ class Model:
             shape = (self.Ny + 1, self.Nx + 1)
         elif name == "gg":
             shape = (self.L,)
+        elif name == "corner_shadow":
+            shape = (4 * self.L * 2 * 4, 6)
         else:
             shape = (self.Ny, self.Nx)
         if out is None:

@@ -370,6 +370,11 @@ static bool lookup(Model* m, const std::string& n, FieldRef& f) {
     else if (n == "dt_v") { f.base = m->dtv; f.nk = L; }
     else if (n == "dt_h") { f.base = m->dth; f.nk = L; }
     else if (n == "wdia") { f.base = m->wdia; f.nk = L + 1; }
+    else if (n == "corner_shadow" && m->corner[0]) {
+      // the latest corner shadow: [field u, v, h, b][layer][wall side][row][column] as
+      // CORNER_F * L * 2 * CORNER_R rows of CORNER_C values
+      f.base = m->corner[m->corner_cur]; f.rows = CORNER_F * L * 2 * CORNER_R; f.cols = CORNER_C; f.pitch = CORNER_C;
+    }
     else if (n == "tend_u") { f.base = m->fu[m->h1]; f.nk = L; }
     else if (n == "tend_v") { f.base = m->fv[m->h1]; f.nk = L; }
     else if (n == "tend_h") { f.base = m->fh[m->h1]; f.nk = L; }

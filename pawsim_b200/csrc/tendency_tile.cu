@@ -196,6 +196,28 @@ template <int MS, int RW>
 __device__ inline double kinetic(const double* u, const double* v, int i, int j) {
   return kinetic_f<MS>([&](int a, int b) { return AT(u, a, b); }, [&](int a, int b) { return AT(v, a, b); }, i, j);
 }
+// The work arrays u, v, h of one layer as the serial build holds them around a periodic image
+// column (x-periodic, y-walled grids): the copied values, except the corner ghosts relative to
+// that column, which come from the corner shadow. A field the reference computes and then
+// copies into the seam's ghost columns by its periodic exchange is evaluated with these at the
+// image column wrap(x) (field.c:353-427; common.cuh).
+struct ImageW {
+  const double *u, *v, *h, *sh;
+  int pitch, Nx, Ny, k, L;
+  __device__ double U(int a, int b) const {
+    return is_corner(a, b, Nx, Ny) ? corner_load(sh, CF_U, k, L, a, b, Nx, Ny, MAP_S)
+                                   : load_mapped(u, pitch, a, b, Nx, Ny, false, true, MAP_N, MAP_S);
+  }
+  __device__ double V(int a, int b) const {
+    return is_corner(a, b, Nx, Ny) ? corner_load(sh, CF_V, k, L, a, b, Nx, Ny, MAP_N)
+                                   : load_mapped(v, pitch, a, b, Nx, Ny, false, true, MAP_S, MAP_N);
+  }
+  __device__ double H(int a, int b) const {
+    return is_corner(a, b, Nx, Ny) ? corner_load(sh, CF_H, k, L, a, b, Nx, Ny, MAP_S)
+                                   : load_mapped(h, pitch, a, b, Nx, Ny, false, true, MAP_S, MAP_S);
+  }
+};
+
 // the same at raw (x, y) of the serial build's work arrays on an x-periodic, y-walled grid,
 // evaluated at the periodic image of x, with the corner ghosts of the stencil from the shadow
 // (the value the fill copies into a periodic ghost column, common.cuh)
@@ -580,11 +602,22 @@ tendency_kernel(const __grid_constant__ TendParams p) {
           F[F_HS][q] = face_south<TS, RW>(sh, sv, p.kt00_sigma, mx, my);
         }
       }
+      // at the seam's ghost columns (serial build's corners) zeta, h_q and q are periodic copies
+      // of the image column's (work.c:1231-1288 then an internal exchange); the deformation
+      // rates are computed in place over the ghosted arrays
+      const bool seam = p.corners && !inner && (t.gx(lx) < 0 || t.gx(lx) >= p.Nx);
+      const ImageW iw{uk, vk, hkp, p.corners, p.pitch, p.Nx, p.Ny, k, L};
+      const int ix = wrap_index(t.gx(lx), p.Nx), iy = t.gy(ly);
       if (lx >= H - 1 && ly >= H - 1 && lx <= TX + H + 1 && ly <= TY + H + 1) {
         // zeta, h on the q grid and q itself (work.c:1261-1270)
-        double z = div_rn(AT(su, lx, ly - 1) - AT(su, lx, ly), dy, rdy)
-                 + div_rn(AT(sv, lx, ly) - AT(sv, lx - 1, ly), dx, rdx);
-        double hq = 0.25 * (AT(sh, lx, ly) + AT(sh, lx - 1, ly - 1) + AT(sh, lx - 1, ly) + AT(sh, lx, ly - 1));
+        double z, hq;
+        if (seam) {
+          z = div_rn(iw.U(ix, iy - 1) - iw.U(ix, iy), dy, rdy) + div_rn(iw.V(ix, iy) - iw.V(ix - 1, iy), dx, rdx);
+          hq = 0.25 * (iw.H(ix, iy) + iw.H(ix - 1, iy - 1) + iw.H(ix - 1, iy) + iw.H(ix, iy - 1));
+        } else {
+          z = div_rn(AT(su, lx, ly - 1) - AT(su, lx, ly), dy, rdy) + div_rn(AT(sv, lx, ly) - AT(sv, lx - 1, ly), dx, rdx);
+          hq = 0.25 * (AT(sh, lx, ly) + AT(sh, lx - 1, ly - 1) + AT(sh, lx - 1, ly) + AT(sh, lx, ly - 1));
+        }
         double om = inner ? p.omz[(size_t)t.gy(ly) * p.qpitch + t.gx(lx)]
                           : load_mapped(p.omz, p.qpitch, t.gx(lx), t.gy(ly), p.Nx, p.Ny, p.wall_ew, p.wall_ns, MAP_Q, MAP_Q);
         F[F_QQ][q] = (2 * om + z) / hq;
@@ -646,8 +679,16 @@ tendency_kernel(const __grid_constant__ TendParams p) {
     // ---- mass fluxes and the biharmonic intermediate velocities ----
     for (int q = tid; q < RN; q += NT) {
       int lx = q % RW, ly = q / RW;
-      if (lx >= H - 1 && lx <= TX + H && ly >= H - 1 && ly <= TY + H - 1) F[F_HUU][q] = su[q] * hw[q];
-      if (lx >= H - 1 && lx <= TX + H - 1 && ly >= H - 1 && ly <= TY + H) F[F_HVV][q] = sv[q] * hs[q];
+      // seam ghost columns (serial build's corners): the mass fluxes are periodic copies of the
+      // image column's (work.c:162-186 then an internal exchange); the biharmonic terms are
+      // computed in place over the ghosted arrays
+      const bool seam = p.corners && !inner && (t.gx(lx) < 0 || t.gx(lx) >= p.Nx);
+      const ImageW iw{uk, vk, hkp, p.corners, p.pitch, p.Nx, p.Ny, k, L};
+      const int ix = wrap_index(t.gx(lx), p.Nx), iy = t.gy(ly);
+      auto SU = [&](int a, int b) { return seam ? iw.U(ix + a - lx, iy + b - ly) : AT(su, a, b); };
+      auto SV = [&](int a, int b) { return seam ? iw.V(ix + a - lx, iy + b - ly) : AT(sv, a, b); };
+      if (lx >= H - 1 && lx <= TX + H && ly >= H - 1 && ly <= TY + H - 1) F[F_HUU][q] = SU(lx, ly) * hw[q];
+      if (lx >= H - 1 && lx <= TX + H - 1 && ly >= H - 1 && ly <= TY + H) F[F_HVV][q] = SV(lx, ly) * hs[q];
       if (p.useA4 && lx >= H - 1 && lx <= TX + H && ly >= H - 1 && ly <= TY + H) {
         F[F_U4][q] = (div_rn(A4H(lx, ly) * AT(sh, lx, ly) * AT(DT, lx, ly) - A4H(lx - 1, ly) * AT(sh, lx - 1, ly) * AT(DT, lx - 1, ly), dx, rdx)
                       + div_rn(A4Q(lx, ly + 1) * AT(hq, lx, ly + 1) * AT(DS, lx, ly + 1) - A4Q(lx, ly) * AT(hq, lx, ly) * AT(DS, lx, ly), dy, rdy))
