@@ -24,8 +24,9 @@ SOURCES = ["api.cu", "tendency.cu", "pressure.cu", "mg.cu", "noalloc.cu", "nn.cu
            "tracer.cu"]
 # (object name, source, extra flags): the fused tendency kernel is built for two tile heights
 UNITS = [(s.replace(".cu", ""), s, []) for s in SOURCES] + [
-    ("tendency_ty8", "tendency_tile.cu", ["-DPAWSIM_TEND_TY=8"]),
-    ("tendency_ty16", "tendency_tile.cu", ["-DPAWSIM_TEND_TY=16"]),
+    # one unit per tile height and momentum scheme, so that they compile in parallel
+    *[(f"tendency_ty{ty}_m{ms}", "tendency_tile.cu", [f"-DPAWSIM_TEND_TY={ty}", f"-DPAWSIM_TEND_MS={ms}"])
+      for ty in (8, 16) for ms in range(4)],
     ("tendency_budget", "tendency_tile.cu", ["-DPAWSIM_TEND_TY=8", "-DPAWSIM_TEND_BUD=1", "-DPAWSIM_TEND_MINB=2"]),
 ]
 DRIVER_SRC = os.path.join(HERE, "host", "pawsim_main.c")

@@ -88,14 +88,18 @@ struct Model {
   std::vector<void*> allocs;
   double *u[2], *v[2], *h[2];
   int cur = 0;
-  double *fu[2], *fv[2], *fh[2];
-  int h1 = 0;   // history buffer holding the newest stored tendency
+  // AB history: three tendency buffers per variable; h1 holds the newest stored tendency, h2
+  // the one before, h3 is free and receives the next (so a recomputed tile still reads intact
+  // history)
+  double *fu[3], *fv[3], *fh[3];
+  int h1 = 0, h2 = 1, h3 = 2;
+  int* tile_list = nullptr;   // tiles listed for the fused kernel's exact pass (tendency.cuh)
   double *dtu, *dtv, *dth, *wdia;
   // running averages (allocated by the first accumulation): 9 per-layer sums (u, v, h, M,
   // hu, hv, huu, hvv, huv), then w_dia on L+1 interfaces, then pi
   double* avg = nullptr;
   // tracer (when use_tracer): state b[2] beside u/v/h, tendency history fb[2], restoring
-  double *b[2] = {nullptr, nullptr}, *fb[2] = {nullptr, nullptr}, *bRelax = nullptr, *bTime = nullptr;
+  double *b[2] = {nullptr, nullptr}, *fb[3] = {nullptr, nullptr, nullptr}, *bRelax = nullptr, *bTime = nullptr;
   double *kappa = nullptr, *fsurf = nullptr;   // diapycnal diffusivity (per layer) and surface flux
   double *hhs, *hhb, *Hc, *omz, *taux, *tauy, *fbx, *fby, *uLid, *vLid;
   double *uRelax, *vRelax, *hRelax, *eRelax, *uTime, *vTime, *eTime, *hTime, *wdff, *nu_u, *nu_v;
@@ -220,13 +224,15 @@ static int create(const pawsim_gpu_config* cfg, Model** out) {
   cudaEventCreate(&m->ev1);
   size_t Ls = m->L * m->lstride;
   bool ok = true;
-  for (int b = 0; b < 2; ++b) {
+  for (int b = 0; b < 2; ++b)
     ok &= (m->u[b] = m->alloc<double>(Ls)) && (m->v[b] = m->alloc<double>(Ls)) && (m->h[b] = m->alloc<double>(Ls));
+  for (int b = 0; b < 3; ++b)
     ok &= (m->fu[b] = m->alloc<double>(Ls)) && (m->fv[b] = m->alloc<double>(Ls)) && (m->fh[b] = m->alloc<double>(Ls));
-  }
+  ok &= (m->tile_list = m->alloc<int>(2 + (size_t)((c.Nx + 31) / 32) * ((c.Ny + 7) / 8))) != nullptr;
   ok &= (m->dtu = m->alloc<double>(Ls)) && (m->dtv = m->alloc<double>(Ls)) && (m->dth = m->alloc<double>(Ls));
   if (c.use_tracer) {
-    for (int b = 0; b < 2; ++b) ok &= (m->b[b] = m->alloc<double>(Ls)) && (m->fb[b] = m->alloc<double>(Ls));
+    for (int b = 0; b < 2; ++b) ok &= (m->b[b] = m->alloc<double>(Ls)) != nullptr;
+    for (int b = 0; b < 3; ++b) ok &= (m->fb[b] = m->alloc<double>(Ls)) != nullptr;
     ok &= (m->bRelax = m->alloc<double>(Ls)) && (m->bTime = m->alloc<double>(Ls));
     ok &= (m->kappa = m->alloc<double>(Ls)) && (m->fsurf = m->alloc<double>(m->plane));
   }
@@ -556,6 +562,7 @@ static TendParams base_params(Model* m) {
   p.nonfinite = m->nonfinite;
   p.corners = m->corner[0] ? m->corner[m->corner_cur] : nullptr;
   p.dragv = m->dragv;
+  p.tile_list = m->tile_list;
   p.drag_bot = (c.quad_drag > 0 && c.hbbl > 0) ? 1 : 0;
   p.drag_surf = (c.quad_drag_surf > 0 && c.hsml > 0) ? 1 : 0;
   return p;
@@ -609,9 +616,9 @@ static int tendency_eval(Model* m) {
   TendParams p = base_params(m);
   p.ab_mode = 0;
   p.fu_out = m->dtu; p.fv_out = m->dtv; p.fh_out = m->dth;
-  if (launch_step_kernel(m, p) != 0)
-    return fail(PAWSIM_GPU_EUNSUPPORTED, "scheme combination not available");
-  g_launches += (p.drag_bot || p.drag_surf) ? 2 : 1;   // the drag pre-pass and the fused kernel
+  const int nl = launch_step_kernel(m, p);
+  if (nl < 0) return fail(PAWSIM_GPU_EUNSUPPORTED, "scheme combination not available");
+  g_launches += nl;   // the drag pre-pass, the fused kernel and its exact pass
   corner_fill(m, m->cur);   // the tendency's load_state and face thickness
   PAWSIM_CUDA_OK(cudaGetLastError());
   return 0;
@@ -631,10 +638,10 @@ static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
   } else {
     p.ab_mode = 3; p.c0 = 23 * dt / 12; p.c1 = 4 * dt / 3; p.c2 = 5 * dt / 12;
   }
-  int h2 = 1 - m->h1;
-  p.f1u = m->fu[m->h1]; p.f1v = m->fv[m->h1]; p.f1h = m->fh[m->h1];
+  const int h1 = m->h1, h2 = m->h2, h3 = m->h3;
+  p.f1u = m->fu[h1]; p.f1v = m->fv[h1]; p.f1h = m->fh[h1];
   p.f2u = m->fu[h2]; p.f2v = m->fv[h2]; p.f2h = m->fh[h2];
-  p.fu_out = m->fu[h2]; p.fv_out = m->fv[h2]; p.fh_out = m->fh[h2];
+  p.fu_out = m->fu[h3]; p.fv_out = m->fv[h3]; p.fh_out = m->fh[h3];
   p.write_hist = shift ? 1 : 0;
   int nb = 1 - m->cur;
   p.u_out = m->u[nb]; p.v_out = m->v[nb]; p.h_out = m->h[nb];
@@ -644,9 +651,9 @@ static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
     p.dt = dt;
     p.bud_u = m->bud[0]; p.bud_v = m->bud[1]; p.bud_h = m->bud[2]; p.bud_e = m->bud[3]; p.bud_b = m->bud[4];
   }
-  if (launch_step_kernel(m, p) != 0)
-    return fail(PAWSIM_GPU_EUNSUPPORTED, "scheme combination not available");
-  g_launches += (p.drag_bot || p.drag_surf) ? 2 : 1;   // the drag pre-pass and the fused kernel
+  const int nl = launch_step_kernel(m, p);
+  if (nl < 0) return fail(PAWSIM_GPU_EUNSUPPORTED, "scheme combination not available");
+  g_launches += nl;   // the drag pre-pass, the fused kernel and its exact pass
   if (c.use_tracer) {
     // the tracer reads the state of the start of the step and the w_dia the tendency
     // kernel just wrote; same AB coefficients and history slots
@@ -661,7 +668,7 @@ static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
     tp.u = m->u[m->cur]; tp.v = m->v[m->cur]; tp.h = m->h[m->cur]; tp.b = m->b[m->cur];
     tp.bRelax = m->bRelax; tp.bTime = m->bTime; tp.wdia = m->wdia;
     tp.ab_mode = p.ab_mode; tp.c0 = p.c0; tp.c1 = p.c1; tp.c2 = p.c2; tp.write_hist = p.write_hist;
-    tp.f1b = m->fb[m->h1]; tp.f2b = m->fb[h2]; tp.fb_out = m->fb[h2]; tp.b_out = m->b[nb];
+    tp.f1b = m->fb[h1]; tp.f2b = m->fb[h2]; tp.fb_out = m->fb[h3]; tp.b_out = m->b[nb];
     tp.bud_b = m->bud[4]; tp.dt = dt;
     tp.use_buoy = c.use_buoyancy;
     for (int k = 0; k < m->L; ++k) tp.gg[k] = m->gg[k];
@@ -672,7 +679,11 @@ static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
   }
   corner_fill(m, m->cur);   // the tendency's load_state and face thickness (state of the step start)
   PAWSIM_CUDA_OK(cudaGetLastError());
-  if (shift) m->h1 = h2;
+  if (shift) {   // newest <- the buffer just written, the previous newest moves back one slot
+    m->h1 = h3;
+    m->h2 = h1;
+    m->h3 = h2;
+  }
   m->cur = nb;
   m->prev_h = true;
   m->t += dt;

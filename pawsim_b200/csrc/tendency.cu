@@ -11,9 +11,36 @@ namespace pawsim {
 
 size_t tendency_smem_ty8(const TendParams& p, int ts);
 size_t tendency_smem_ty16(const TendParams& p, int ts);
-int launch_tendency_ty8(const TendParams& p, int ms, int ts, cudaStream_t s);
-int launch_tendency_ty16(const TendParams& p, int ms, int ts, cudaStream_t s);
+// one translation unit per tile height and momentum scheme (compiled in parallel)
+#define PAWSIM_DECL_TEND(TY)                                                   \
+  int launch_tendency_ty##TY##_m0(const TendParams& p, int ms, int ts, cudaStream_t s); \
+  int launch_tendency_ty##TY##_m1(const TendParams& p, int ms, int ts, cudaStream_t s); \
+  int launch_tendency_ty##TY##_m2(const TendParams& p, int ms, int ts, cudaStream_t s); \
+  int launch_tendency_ty##TY##_m3(const TendParams& p, int ms, int ts, cudaStream_t s);
+PAWSIM_DECL_TEND(8)
+PAWSIM_DECL_TEND(16)
+#undef PAWSIM_DECL_TEND
 int launch_tendency_budget_tile(const TendParams& p, int ms, int ts, cudaStream_t s);
+
+static int launch_tendency_ty8(const TendParams& p, int ms, int ts, cudaStream_t s) {
+  switch (ms) {
+    case 0: return launch_tendency_ty8_m0(p, ms, ts, s);
+    case 1: return launch_tendency_ty8_m1(p, ms, ts, s);
+    case 2: return launch_tendency_ty8_m2(p, ms, ts, s);
+    case 3: return launch_tendency_ty8_m3(p, ms, ts, s);
+  }
+  return -1;
+}
+
+static int launch_tendency_ty16(const TendParams& p, int ms, int ts, cudaStream_t s) {
+  switch (ms) {
+    case 0: return launch_tendency_ty16_m0(p, ms, ts, s);
+    case 1: return launch_tendency_ty16_m1(p, ms, ts, s);
+    case 2: return launch_tendency_ty16_m2(p, ms, ts, s);
+    case 3: return launch_tendency_ty16_m3(p, ms, ts, s);
+  }
+  return -1;
+}
 
 int launch_tendency(const TendParams& p, int ms, int ts, cudaStream_t s) {
   // two CTAs per SM: 228 KB of shared memory, 1 KB reserved per CTA

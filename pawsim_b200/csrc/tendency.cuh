@@ -80,6 +80,9 @@ struct TendParams {
   // nullptr when the drag acts on the bottom (top) layer alone
   double* dragv;
   int drag_bot, drag_surf;
+  // tiles for the exact recomputation of the plain build: [0] count, [1] completion counter of
+  // the exact pass (both zero between launches), [2..] tile indices (one slot per tile)
+  int* tile_list;
 };
 
 // budget term indices (work.h:18-91)
@@ -98,6 +101,7 @@ __device__ inline void budget_add(double* fam, int term, int k, int L, size_t ls
   }
 }
 
+// returns the number of kernels launched, or -1 when the combination is not available
 int launch_tendency(const TendParams& p, int momentum_scheme, int thickness_scheme,
                     cudaStream_t stream);
 // the same step with every enabled budget family accumulated and the buoyancy coupling

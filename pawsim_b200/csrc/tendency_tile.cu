@@ -82,10 +82,11 @@ struct Tile {
 __device__ inline double sq(double x) { return x * x; }
 
 // PV interpolation coefficients (work.c:1294-1404) evaluated from qq in shared memory
-template <int MS, int RW> struct Coef {
+template <int MS, int RW, typename DV> struct Coef {
   const double* q;
   double r24;
-  __device__ double D(double x) const { return div_rn(x, 24.0, r24); }
+  DV div;   // the quotient x / d given 1/d (div_rn, or its branch-free pass)
+  __device__ double D(double x) const { return div(x, 24.0, r24); }
   __device__ double Q(int x, int y) const { return AT(q, x, y); }
   __device__ double alpha(int i, int j) const {
     if (MS == 3)
@@ -428,9 +429,28 @@ __device__ inline double drag_load(const double* f, const TendParams& p, int x, 
 #define PAWSIM_TEND_MINB (1024 / NT)
 #endif
 
-template <int MS, int TS, int H>
-__global__ void __launch_bounds__(NT, PAWSIM_TEND_MINB)
-tendency_kernel(const __grid_constant__ TendParams p) {
+// One tile (bx, by) of the fused step; the fused kernel runs one per CTA, the exact pass the
+// tiles listed by it.
+template <int MS, int TS, int H, bool LEAN, bool EXACT>
+__device__ __forceinline__ void tendency_tile(const TendParams& p, int bx, int by) {
+  // LEAN instantiations serve set-ups without w_dia, Smagorinsky, layer fractions, restoring,
+  // diapycnal viscosity, surface or quadratic drag, Fbaro, biharmonic viscosity and corner
+  // shadow: those paths compile away
+  const bool use_wdia = !LEAN && p.use_wdia, use_relax = !LEAN && p.use_relax;
+  const bool use_diavisc = !LEAN && p.use_diavisc, use_fractions = !LEAN && p.use_fractions;
+  const bool use_fbaro = !LEAN && p.use_fbaro, useA4 = !LEAN && p.useA4;
+  const int use_smag = LEAN ? 0 : p.use_smag;
+  const double* const corners = LEAN ? nullptr : p.corners;
+  // Stencil quotients. The plain build's first pass divides without a branch (div_rn_fast) and
+  // flags its tile when an operand fell outside the corrections' range; the EXACT pass then
+  // recomputes only the flagged tiles with div_rn (the budget build always uses div_rn, as it
+  // adds to running sums on the way).
+  constexpr bool SLOWDIV = EXACT || BUD;
+  bool oor = false;
+  auto DIV = [&](double x, double d, double r) {
+    if constexpr (SLOWDIV) return div_rn(x, d, r);
+    else return div_rn_fast(x, d, r, oor);
+  };
   constexpr int RW = Geo<H>::RW, RH = Geo<H>::RH, RN = Geo<H>::RN;
   extern __shared__ double smem[];
   double* F[F_NUM];
@@ -438,13 +458,13 @@ tendency_kernel(const __grid_constant__ TendParams p) {
   for (int f = 0; f < F_NUM; ++f) F[f] = smem + f * RN;
   double* MMall = smem + F_NUM * RN;            // [L][RN]
   double* WDall = MMall + p.L * RN;             // [L+1][RN] when use_wdia
-  double* SM = WDall + (p.use_wdia ? (p.L + 1) * RN : 0);   // [S_NUM][RN] when use_smag
-  double* FR = SM + (p.use_smag ? S_NUM * RN : 0);          // [4][L][NT] when use_fractions
+  double* SM = WDall + (use_wdia ? (p.L + 1) * RN : 0);   // [S_NUM][RN] when use_smag
+  double* FR = SM + (use_smag ? S_NUM * RN : 0);          // [4][L][NT] when use_fractions
 
   const int tid = threadIdx.x;
   Tile<H> t;
-  t.X0 = blockIdx.x * TX;
-  t.Y0 = blockIdx.y * TY;
+  t.X0 = bx * TX;
+  t.Y0 = by * TY;
   t.Nx = p.Nx;
   t.Ny = p.Ny;
   t.wx = p.wall_ew;
@@ -460,7 +480,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
     if (lx < H - 1 || lx > TX + H - 1 || ly < H - 1 || ly > TY + H - 1) continue;
     if (!t.near(lx, ly)) {
       for (int k = 0; k < L; ++k) MMall[k * RN + q] = 0;
-      if (p.use_wdia)
+      if (use_wdia)
         for (int k = 0; k <= L; ++k) WDall[k * RN + q] = 0;
       continue;
     }
@@ -506,7 +526,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         MMall[k * RN + q] = mm;
       }
     }
-    if (p.use_wdia) {
+    if (use_wdia) {
       double* wd = WDall + q;   // interface k at wd[k * RN]
       for (int k = 0; k <= L; ++k) {
         if (p.use_wdia_file) {
@@ -516,7 +536,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
           wd[k * RN] = 0;
         }
       }
-      if (p.use_relax) {
+      if (use_relax) {
         double acc = 0;
         double ht = gload(p.hTime, p, gi, gj, MAP_S, MAP_S);
 #pragma unroll
@@ -547,7 +567,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
 
   // ---- surface and bottom layer fractions at the owned cell (work.c:2151-2340) ----
   // FR[(f * L + k) * NT + tid], f = 0 hFsw, 1 hFss, 2 hFbw, 3 hFbs
-  if (p.use_fractions && valid)
+  if (use_fractions && valid)
     cell_fractions<TS>(p, gi, gj, [&](int f, int k, double v) { FR[(f * L + k) * NT + tid] = v; });
 
   for (int k = 0; k < L; ++k) {
@@ -569,10 +589,10 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         int lx = q % RW, ly = q / RW;
         int gx = t.gx(lx), gy = t.gy(ly);
         bool in = gx >= -H && gx < p.Nx + H && gy >= -H && gy < p.Ny + H;
-        if (in && p.corners && is_corner(gx, gy, p.Nx, p.Ny)) {
-          F[F_U][q] = corner_load(p.corners, CF_U, k, L, gx, gy, p.Nx, p.Ny, MAP_S);
-          F[F_V][q] = corner_load(p.corners, CF_V, k, L, gx, gy, p.Nx, p.Ny, MAP_N);
-          F[F_H][q] = corner_load(p.corners, CF_H, k, L, gx, gy, p.Nx, p.Ny, MAP_S);
+        if (in && corners && is_corner(gx, gy, p.Nx, p.Ny)) {
+          F[F_U][q] = corner_load(corners, CF_U, k, L, gx, gy, p.Nx, p.Ny, MAP_S);
+          F[F_V][q] = corner_load(corners, CF_V, k, L, gx, gy, p.Nx, p.Ny, MAP_N);
+          F[F_H][q] = corner_load(corners, CF_H, k, L, gx, gy, p.Nx, p.Ny, MAP_S);
           continue;
         }
         F[F_U][q] = in ? gload(uk, p, gx, gy, MAP_N, MAP_S) : 0.0;
@@ -591,10 +611,10 @@ tendency_kernel(const __grid_constant__ TendParams p) {
       if (lx >= H - 1 && lx <= TX + H && ly >= H - 1 && ly <= TY + H && nr) {
         // a periodic ghost column (its corners included) receives the values computed at the
         // image column, whose stencil reads the corner shadow (serial build, common.cuh)
-        if (p.corners && !inner && (t.gx(lx) < 0 || t.gx(lx) >= p.Nx)) {
-          F[F_HW][q] = corner_face<true>(hkp, uk, p.pitch, p.Nx, p.Ny, TS, p.kt00_sigma, p.corners, k, L, t.gx(lx),
+        if (corners && !inner && (t.gx(lx) < 0 || t.gx(lx) >= p.Nx)) {
+          F[F_HW][q] = corner_face<true>(hkp, uk, p.pitch, p.Nx, p.Ny, TS, p.kt00_sigma, corners, k, L, t.gx(lx),
                                          t.gy(ly));
-          F[F_HS][q] = corner_face<false>(hkp, vk, p.pitch, p.Nx, p.Ny, TS, p.kt00_sigma, p.corners, k, L, t.gx(lx),
+          F[F_HS][q] = corner_face<false>(hkp, vk, p.pitch, p.Nx, p.Ny, TS, p.kt00_sigma, corners, k, L, t.gx(lx),
                                           t.gy(ly));
         } else {
           int mx = t.mlx(lx), my = t.mly(ly);
@@ -605,17 +625,17 @@ tendency_kernel(const __grid_constant__ TendParams p) {
       // at the seam's ghost columns (serial build's corners) zeta, h_q and q are periodic copies
       // of the image column's (work.c:1231-1288 then an internal exchange); the deformation
       // rates are computed in place over the ghosted arrays
-      const bool seam = p.corners && !inner && (t.gx(lx) < 0 || t.gx(lx) >= p.Nx);
-      const ImageW iw{uk, vk, hkp, p.corners, p.pitch, p.Nx, p.Ny, k, L};
+      const bool seam = corners && !inner && (t.gx(lx) < 0 || t.gx(lx) >= p.Nx);
+      const ImageW iw{uk, vk, hkp, corners, p.pitch, p.Nx, p.Ny, k, L};
       const int ix = wrap_index(t.gx(lx), p.Nx), iy = t.gy(ly);
       if (lx >= H - 1 && ly >= H - 1 && lx <= TX + H + 1 && ly <= TY + H + 1) {
         // zeta, h on the q grid and q itself (work.c:1261-1270)
         double z, hq;
         if (seam) {
-          z = div_rn(iw.U(ix, iy - 1) - iw.U(ix, iy), dy, rdy) + div_rn(iw.V(ix, iy) - iw.V(ix - 1, iy), dx, rdx);
+          z = DIV(iw.U(ix, iy - 1) - iw.U(ix, iy), dy, rdy) + DIV(iw.V(ix, iy) - iw.V(ix - 1, iy), dx, rdx);
           hq = 0.25 * (iw.H(ix, iy) + iw.H(ix - 1, iy - 1) + iw.H(ix - 1, iy) + iw.H(ix, iy - 1));
         } else {
-          z = div_rn(AT(su, lx, ly - 1) - AT(su, lx, ly), dy, rdy) + div_rn(AT(sv, lx, ly) - AT(sv, lx - 1, ly), dx, rdx);
+          z = DIV(AT(su, lx, ly - 1) - AT(su, lx, ly), dy, rdy) + DIV(AT(sv, lx, ly) - AT(sv, lx - 1, ly), dx, rdx);
           hq = 0.25 * (AT(sh, lx, ly) + AT(sh, lx - 1, ly - 1) + AT(sh, lx - 1, ly) + AT(sh, lx, ly - 1));
         }
         double om = inner ? p.omz[(size_t)t.gy(ly) * p.qpitch + t.gx(lx)]
@@ -624,18 +644,18 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         F[F_HQ][q] = hq;
       }
       if (lx >= H - 1 && lx <= TX + H - 1 && ly >= H - 1 && ly <= TY + H - 1) {
-        if (nr && p.corners && !inner && (t.gx(lx) < 0 || t.gx(lx) >= p.Nx) && t.gy(ly) >= 0 && t.gy(ly) < p.Ny)
-          F[F_KE][q] = kinetic_image<MS>(uk, vk, p.pitch, p.Nx, p.Ny, p.corners, k, L, t.gx(lx), t.gy(ly));
+        if (nr && corners && !inner && (t.gx(lx) < 0 || t.gx(lx) >= p.Nx) && t.gy(ly) >= 0 && t.gy(ly) < p.Ny)
+          F[F_KE][q] = kinetic_image<MS>(uk, vk, p.pitch, p.Nx, p.Ny, corners, k, L, t.gx(lx), t.gy(ly));
         else
           F[F_KE][q] = nr ? kinetic<MS, RW>(su, sv, t.mlx(lx), t.mly(ly)) : 0.0;
       }
-      if (p.useA2 || p.useA4) {
+      if (p.useA2 || useA4) {
         if (lx >= H - 2 && lx <= RW - 2 && ly >= H - 2 && ly <= RH - 2)
-          F[F_DT][q] = div_rn(AT(su, lx + 1, ly) - AT(su, lx, ly), dx, rdx)
-                     - div_rn(AT(sv, lx, ly + 1) - AT(sv, lx, ly), dy, rdy);
+          F[F_DT][q] = DIV(AT(su, lx + 1, ly) - AT(su, lx, ly), dx, rdx)
+                     - DIV(AT(sv, lx, ly + 1) - AT(sv, lx, ly), dy, rdy);
         if (lx >= 1 && ly >= 1 && lx >= H - 2 && ly >= H - 2)
-          F[F_DS][q] = div_rn(AT(su, lx, ly) - AT(su, lx, ly - 1), dy, rdy)
-                     + div_rn(AT(sv, lx, ly) - AT(sv, lx - 1, ly), dx, rdx);
+          F[F_DS][q] = DIV(AT(su, lx, ly) - AT(su, lx, ly - 1), dy, rdy)
+                     + DIV(AT(sv, lx, ly) - AT(sv, lx - 1, ly), dx, rdx);
       }
     }
     __syncthreads();
@@ -649,7 +669,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
     const double* A2q = SM + S_A2Q * RN;
     const double* A4h = SM + S_A4H * RN;
     const double* A4q = SM + S_A4Q * RN;
-    if (p.use_smag) {
+    if (use_smag) {
       for (int q = tid; q < RN; q += NT) {
         int lx = q % RW, ly = q / RW;
         // cells: A2 and sqrt(A4) from |D| at the cell centre
@@ -671,7 +691,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
     }
     // without its Smagorinsky term a coefficient is the constant itself (fmax(A, 0) = A and
     // sqrt(fmax(A4, 0)) = sqrt(A4) in the reference)
-    const bool smag2 = (p.use_smag & 1) != 0, smag4 = (p.use_smag & 2) != 0;
+    const bool smag2 = (use_smag & 1) != 0, smag4 = (use_smag & 2) != 0;
     auto A2H = [&](int x, int y) { return smag2 ? AT(A2h, x, y) : p.A2; };
     auto A2Q = [&](int x, int y) { return smag2 ? AT(A2q, x, y) : p.A2; };
     auto A4H = [&](int x, int y) { return smag4 ? AT(A4h, x, y) : p.A4sqrt; };
@@ -682,19 +702,19 @@ tendency_kernel(const __grid_constant__ TendParams p) {
       // seam ghost columns (serial build's corners): the mass fluxes are periodic copies of the
       // image column's (work.c:162-186 then an internal exchange); the biharmonic terms are
       // computed in place over the ghosted arrays
-      const bool seam = p.corners && !inner && (t.gx(lx) < 0 || t.gx(lx) >= p.Nx);
-      const ImageW iw{uk, vk, hkp, p.corners, p.pitch, p.Nx, p.Ny, k, L};
+      const bool seam = corners && !inner && (t.gx(lx) < 0 || t.gx(lx) >= p.Nx);
+      const ImageW iw{uk, vk, hkp, corners, p.pitch, p.Nx, p.Ny, k, L};
       const int ix = wrap_index(t.gx(lx), p.Nx), iy = t.gy(ly);
       auto SU = [&](int a, int b) { return seam ? iw.U(ix + a - lx, iy + b - ly) : AT(su, a, b); };
       auto SV = [&](int a, int b) { return seam ? iw.V(ix + a - lx, iy + b - ly) : AT(sv, a, b); };
       if (lx >= H - 1 && lx <= TX + H && ly >= H - 1 && ly <= TY + H - 1) F[F_HUU][q] = SU(lx, ly) * hw[q];
       if (lx >= H - 1 && lx <= TX + H - 1 && ly >= H - 1 && ly <= TY + H) F[F_HVV][q] = SV(lx, ly) * hs[q];
-      if (p.useA4 && lx >= H - 1 && lx <= TX + H && ly >= H - 1 && ly <= TY + H) {
-        F[F_U4][q] = (div_rn(A4H(lx, ly) * AT(sh, lx, ly) * AT(DT, lx, ly) - A4H(lx - 1, ly) * AT(sh, lx - 1, ly) * AT(DT, lx - 1, ly), dx, rdx)
-                      + div_rn(A4Q(lx, ly + 1) * AT(hq, lx, ly + 1) * AT(DS, lx, ly + 1) - A4Q(lx, ly) * AT(hq, lx, ly) * AT(DS, lx, ly), dy, rdy))
+      if (useA4 && lx >= H - 1 && lx <= TX + H && ly >= H - 1 && ly <= TY + H) {
+        F[F_U4][q] = (DIV(A4H(lx, ly) * AT(sh, lx, ly) * AT(DT, lx, ly) - A4H(lx - 1, ly) * AT(sh, lx - 1, ly) * AT(DT, lx - 1, ly), dx, rdx)
+                      + DIV(A4Q(lx, ly + 1) * AT(hq, lx, ly + 1) * AT(DS, lx, ly + 1) - A4Q(lx, ly) * AT(hq, lx, ly) * AT(DS, lx, ly), dy, rdy))
                      / AT(hw, lx, ly);
-        F[F_V4][q] = (div_rn(A4Q(lx + 1, ly) * AT(hq, lx + 1, ly) * AT(DS, lx + 1, ly) - A4Q(lx, ly) * AT(hq, lx, ly) * AT(DS, lx, ly), dx, rdx)
-                      - div_rn(A4H(lx, ly) * AT(sh, lx, ly) * AT(DT, lx, ly) - A4H(lx, ly - 1) * AT(sh, lx, ly - 1) * AT(DT, lx, ly - 1), dy, rdy))
+        F[F_V4][q] = (DIV(A4Q(lx + 1, ly) * AT(hq, lx + 1, ly) * AT(DS, lx + 1, ly) - A4Q(lx, ly) * AT(hq, lx, ly) * AT(DS, lx, ly), dx, rdx)
+                      - DIV(A4H(lx, ly) * AT(sh, lx, ly) * AT(DT, lx, ly) - A4H(lx, ly - 1) * AT(sh, lx, ly - 1) * AT(DT, lx, ly - 1), dy, rdy))
                      / AT(hs, lx, ly);
       }
     }
@@ -707,7 +727,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
     const double* MM = MMall + k * RN;
     const double* U4 = F[F_U4];
     const double* V4 = F[F_V4];
-    Coef<MS, RW> c{F[F_QQ], r24};
+    Coef<MS, RW, decltype(DIV)> c{F[F_QQ], r24, DIV};
     const double* qq = F[F_QQ];
     const int i = ox, j = oy;
     const double hwest = AT(hw, i, j), hsouth = AT(hs, i, j);
@@ -717,8 +737,8 @@ tendency_kernel(const __grid_constant__ TendParams p) {
     // ---- u momentum (work.c:1667-1752) ----
     double ru;
     {
-      double gM = div_rn(-(AT(MM, i, j) - AT(MM, i - 1, j)), dx, rdx);
-      double gK = div_rn(-(AT(KE, i, j) - AT(KE, i - 1, j)), dx, rdx);
+      double gM = DIV(-(AT(MM, i, j) - AT(MM, i - 1, j)), dx, rdx);
+      double gK = DIV(-(AT(KE, i, j) - AT(KE, i - 1, j)), dx, rdx);
       double rq = 0;
       if (MS == 0 || MS == 1) {
         rq += c.alpha(i, j) * AT(hvv, i, j + 1) + c.beta(i, j) * AT(hvv, i - 1, j + 1)
@@ -735,26 +755,26 @@ tendency_kernel(const __grid_constant__ TendParams p) {
       }
       double a2 = 0, a4 = 0;
       if (p.useA2) {
-        a2 = (div_rn(A2H(i, j) * AT(sh, i, j) * AT(DT, i, j) - A2H(i - 1, j) * AT(sh, i - 1, j) * AT(DT, i - 1, j), dx, rdx)
-              + div_rn(A2Q(i, j + 1) * AT(hq, i, j + 1) * AT(DS, i, j + 1) - A2Q(i, j) * AT(hq, i, j) * AT(DS, i, j), dy, rdy));
+        a2 = (DIV(A2H(i, j) * AT(sh, i, j) * AT(DT, i, j) - A2H(i - 1, j) * AT(sh, i - 1, j) * AT(DT, i - 1, j), dx, rdx)
+              + DIV(A2Q(i, j + 1) * AT(hq, i, j + 1) * AT(DS, i, j + 1) - A2Q(i, j) * AT(hq, i, j) * AT(DS, i, j), dy, rdy));
       }
-      if (p.useA4) {
-        double d4t0 = div_rn(AT(U4, i + 1, j) - AT(U4, i, j), dx, rdx) - div_rn(AT(V4, i, j + 1) - AT(V4, i, j), dy, rdy);
-        double d4tm = div_rn(AT(U4, i, j) - AT(U4, i - 1, j), dx, rdx) - div_rn(AT(V4, i - 1, j + 1) - AT(V4, i - 1, j), dy, rdy);
-        double d4s1 = div_rn(AT(U4, i, j + 1) - AT(U4, i, j), dy, rdy) + div_rn(AT(V4, i, j + 1) - AT(V4, i - 1, j + 1), dx, rdx);
-        double d4s0 = div_rn(AT(U4, i, j) - AT(U4, i, j - 1), dy, rdy) + div_rn(AT(V4, i, j) - AT(V4, i - 1, j), dx, rdx);
-        a4 = -(div_rn(A4H(i, j) * AT(sh, i, j) * d4t0 - A4H(i - 1, j) * AT(sh, i - 1, j) * d4tm, dx, rdx)
-               + div_rn(A4Q(i, j + 1) * AT(hq, i, j + 1) * d4s1 - A4Q(i, j) * AT(hq, i, j) * d4s0, dy, rdy));
+      if (useA4) {
+        double d4t0 = DIV(AT(U4, i + 1, j) - AT(U4, i, j), dx, rdx) - DIV(AT(V4, i, j + 1) - AT(V4, i, j), dy, rdy);
+        double d4tm = DIV(AT(U4, i, j) - AT(U4, i - 1, j), dx, rdx) - DIV(AT(V4, i - 1, j + 1) - AT(V4, i - 1, j), dy, rdy);
+        double d4s1 = DIV(AT(U4, i, j + 1) - AT(U4, i, j), dy, rdy) + DIV(AT(V4, i, j + 1) - AT(V4, i - 1, j + 1), dx, rdx);
+        double d4s0 = DIV(AT(U4, i, j) - AT(U4, i, j - 1), dy, rdy) + DIV(AT(V4, i, j) - AT(V4, i - 1, j), dx, rdx);
+        a4 = -(DIV(A4H(i, j) * AT(sh, i, j) * d4t0 - A4H(i - 1, j) * AT(sh, i - 1, j) * d4tm, dx, rdx)
+               + DIV(A4Q(i, j + 1) * AT(hq, i, j + 1) * d4s1 - A4Q(i, j) * AT(hq, i, j) * d4s0, dy, rdy));
       }
       double buoy = 0;
       if constexpr (BUD) {
         // -0.5 (hz(i) + hz(i-1)) db/dx (work.c:1745-1748)
         if (p.use_buoy && hwest != 0)
           buoy = -0.5 * (buoy_hz(p, k, gi, gj) + buoy_hz(p, k, gi - 1, gj))
-               * div_rn(gload(p.b + k * p.lstride, p, gi, gj, MAP_S, MAP_S)
+               * DIV(gload(p.b + k * p.lstride, p, gi, gj, MAP_S, MAP_S)
                         - gload(p.b + k * p.lstride, p, gi - 1, gj, MAP_S, MAP_S), dx, rdx);
       }
-      ru = gM + gK + rq + ((hwest != 0) ? div_rn(a2 + a4 + buoy, hwest, rhw) : 0);
+      ru = gM + gK + rq + ((hwest != 0) ? DIV(a2 + a4 + buoy, hwest, rhw) : 0);
       if constexpr (BUD) {
         // work.c:1753-1763
         const bool active = !(p.wall_ew && gi == 0);
@@ -774,8 +794,8 @@ tendency_kernel(const __grid_constant__ TendParams p) {
     // ---- v momentum (work.c:1759-1852) ----
     double rv;
     {
-      double gM = div_rn(-(AT(MM, i, j) - AT(MM, i, j - 1)), dy, rdy);
-      double gK = div_rn(-(AT(KE, i, j) - AT(KE, i, j - 1)), dy, rdy);
+      double gM = DIV(-(AT(MM, i, j) - AT(MM, i, j - 1)), dy, rdy);
+      double gK = DIV(-(AT(KE, i, j) - AT(KE, i, j - 1)), dy, rdy);
       double rq = 0;
       if (MS == 0 || MS == 1) {
         rq += c.phi(i, j - 1) * AT(hvv, i, j - 1) - c.phi(i, j) * AT(hvv, i, j + 1)
@@ -792,26 +812,26 @@ tendency_kernel(const __grid_constant__ TendParams p) {
       }
       double a2 = 0, a4 = 0;
       if (p.useA2) {
-        a2 = (div_rn(A2Q(i + 1, j) * AT(hq, i + 1, j) * AT(DS, i + 1, j) - A2Q(i, j) * AT(hq, i, j) * AT(DS, i, j), dx, rdx)
-              - div_rn(A2H(i, j) * AT(sh, i, j) * AT(DT, i, j) - A2H(i, j - 1) * AT(sh, i, j - 1) * AT(DT, i, j - 1), dy, rdy));
+        a2 = (DIV(A2Q(i + 1, j) * AT(hq, i + 1, j) * AT(DS, i + 1, j) - A2Q(i, j) * AT(hq, i, j) * AT(DS, i, j), dx, rdx)
+              - DIV(A2H(i, j) * AT(sh, i, j) * AT(DT, i, j) - A2H(i, j - 1) * AT(sh, i, j - 1) * AT(DT, i, j - 1), dy, rdy));
       }
-      if (p.useA4) {
-        double d4s1 = div_rn(AT(U4, i + 1, j) - AT(U4, i + 1, j - 1), dy, rdy) + div_rn(AT(V4, i + 1, j) - AT(V4, i, j), dx, rdx);
-        double d4s0 = div_rn(AT(U4, i, j) - AT(U4, i, j - 1), dy, rdy) + div_rn(AT(V4, i, j) - AT(V4, i - 1, j), dx, rdx);
-        double d4t0 = div_rn(AT(U4, i + 1, j) - AT(U4, i, j), dx, rdx) - div_rn(AT(V4, i, j + 1) - AT(V4, i, j), dy, rdy);
-        double d4tm = div_rn(AT(U4, i + 1, j - 1) - AT(U4, i, j - 1), dx, rdx) - div_rn(AT(V4, i, j) - AT(V4, i, j - 1), dy, rdy);
-        a4 = -(div_rn(A4Q(i + 1, j) * AT(hq, i + 1, j) * d4s1 - A4Q(i, j) * AT(hq, i, j) * d4s0, dx, rdx)
-               - div_rn(A4H(i, j) * AT(sh, i, j) * d4t0 - A4H(i, j - 1) * AT(sh, i, j - 1) * d4tm, dy, rdy));
+      if (useA4) {
+        double d4s1 = DIV(AT(U4, i + 1, j) - AT(U4, i + 1, j - 1), dy, rdy) + DIV(AT(V4, i + 1, j) - AT(V4, i, j), dx, rdx);
+        double d4s0 = DIV(AT(U4, i, j) - AT(U4, i, j - 1), dy, rdy) + DIV(AT(V4, i, j) - AT(V4, i - 1, j), dx, rdx);
+        double d4t0 = DIV(AT(U4, i + 1, j) - AT(U4, i, j), dx, rdx) - DIV(AT(V4, i, j + 1) - AT(V4, i, j), dy, rdy);
+        double d4tm = DIV(AT(U4, i + 1, j - 1) - AT(U4, i, j - 1), dx, rdx) - DIV(AT(V4, i, j) - AT(V4, i, j - 1), dy, rdy);
+        a4 = -(DIV(A4Q(i + 1, j) * AT(hq, i + 1, j) * d4s1 - A4Q(i, j) * AT(hq, i, j) * d4s0, dx, rdx)
+               - DIV(A4H(i, j) * AT(sh, i, j) * d4t0 - A4H(i, j - 1) * AT(sh, i, j - 1) * d4tm, dy, rdy));
       }
       double buoy = 0;
       if constexpr (BUD) {
         // work.c:1829-1832
         if (p.use_buoy && hsouth != 0)
           buoy = -0.5 * (buoy_hz(p, k, gi, gj) + buoy_hz(p, k, gi, gj - 1))
-               * div_rn(gload(p.b + k * p.lstride, p, gi, gj, MAP_S, MAP_S)
+               * DIV(gload(p.b + k * p.lstride, p, gi, gj, MAP_S, MAP_S)
                         - gload(p.b + k * p.lstride, p, gi, gj - 1, MAP_S, MAP_S), dy, rdy);
       }
-      rv = gM + gK + rq + ((hsouth != 0) ? div_rn(a2 + a4 + buoy, hsouth, rhs) : 0);
+      rv = gM + gK + rq + ((hsouth != 0) ? DIV(a2 + a4 + buoy, hsouth, rhs) : 0);
       if constexpr (BUD) {
         // work.c:1837-1847
         const bool active = !(p.wall_ns && gj == 0);
@@ -829,8 +849,8 @@ tendency_kernel(const __grid_constant__ TendParams p) {
       }
     }
     // ---- diapycnal advection and viscosity (diapycnal.c:203-291) ----
-    if (p.use_wdia || p.use_diavisc) {
-      if (p.use_wdia) {
+    if (use_wdia || use_diavisc) {
+      if (use_wdia) {
         const double* W0 = WDall + k * RN;
         const double* W1 = WDall + (k + 1) * RN;
         double wu0 = 0.5 * (AT(W0, i, j) + AT(W0, i - 1, j));
@@ -848,7 +868,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         double dvm = (wv1 > 0) ? vc - vm : 0;
         if (hwest != 0) {
           const double r = -(wu0 * dup + wu1 * dum);
-          ru += div_rn(r, hwest, rhw);
+          ru += DIV(r, hwest, rhw);
           if constexpr (BUD) {
             budget_add(p.bud_u, BU_WDIA, k, L, p.lstride, cell, r * p.dt);
             budget_add(p.bud_e, BE_WDIAKE, k, L, p.lstride, cell, r * uc * p.dt);
@@ -856,14 +876,14 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         }
         if (hsouth != 0) {
           const double r = -(wv0 * dvp + wv1 * dvm);
-          rv += div_rn(r, hsouth, rhs);
+          rv += DIV(r, hsouth, rhs);
           if constexpr (BUD) {
             budget_add(p.bud_v, BU_WDIA, k, L, p.lstride, cell, r * p.dt);
             budget_add(p.bud_e, BE_WDIAKE, k, L, p.lstride, cell, r * vc * p.dt);
           }
         }
       }
-      if (p.use_diavisc && L >= 2) {
+      if (use_diavisc && L >= 2) {
         double Fu[2] = {0, 0}, Fv[2] = {0, 0};
         for (int s = 0; s < 2; ++s) {
           int kk = k + s;                    // interface kk between layers kk-1 and kk
@@ -898,7 +918,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         }
         if (hwest != 0) {
           const double r = Fu[0] - Fu[1];
-          ru += div_rn(r, hwest, rhw);
+          ru += DIV(r, hwest, rhw);
           if constexpr (BUD) {
             budget_add(p.bud_u, BU_DIAVISC, k, L, p.lstride, cell, r * p.dt);
             budget_add(p.bud_e, BE_DIAVISC, k, L, p.lstride, cell, r * uc * p.dt);
@@ -906,7 +926,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         }
         if (hsouth != 0) {
           const double r = Fv[0] - Fv[1];
-          rv += div_rn(r, hsouth, rhs);
+          rv += DIV(r, hsouth, rhs);
           if constexpr (BUD) {
             budget_add(p.bud_v, BU_DIAVISC, k, L, p.lstride, cell, r * p.dt);
             budget_add(p.bud_e, BE_DIAVISC, k, L, p.lstride, cell, r * vc * p.dt);
@@ -920,7 +940,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
       const bool wface_v = p.wall_ns && gj == 0;
       // layer fractions: computed ones, or all to the top / bottom layer; zero on a wall face
       double fsw, fss, fbw, fbs;
-      if (p.use_fractions) {
+      if (use_fractions) {
         fsw = FR[(0 * L + k) * NT + tid];
         fss = FR[(1 * L + k) * NT + tid];
         fbw = FR[(2 * L + k) * NT + tid];
@@ -935,19 +955,19 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         double tx_ = p.tw0 * p.taux0[cell] + p.tw1 * p.taux1[cell];
         double ty_ = p.tw0 * p.tauy0[cell] + p.tw1 * p.tauy1[cell];
         double r = tx_ * fsw;
-        if (hwest != 0) ru += div_rn(r, hwest, rhw);
+        if (hwest != 0) ru += DIV(r, hwest, rhw);
         if constexpr (BUD) {
           budget_add(p.bud_u, BU_WIND, k, L, p.lstride, cell, r * p.dt);
           budget_add(p.bud_e, BE_WIND, k, L, p.lstride, cell, r * uc * p.dt);
         }
         r = ty_ * fss;
-        if (hsouth != 0) rv += div_rn(r, hsouth, rhs);
+        if (hsouth != 0) rv += DIV(r, hsouth, rhs);
         if constexpr (BUD) {
           budget_add(p.bud_v, BU_WIND, k, L, p.lstride, cell, r * p.dt);
           budget_add(p.bud_e, BE_WIND, k, L, p.lstride, cell, r * vc * p.dt);
         }
       }
-      if (p.use_fbaro) {
+      if (use_fbaro) {
         const double fx = gload(p.fbx, p, gi, gj, MAP_N, MAP_S), fy = gload(p.fby, p, gi, gj, MAP_S, MAP_N);
         ru += fx;
         rv += fy;
@@ -960,7 +980,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
       if (p.lin_drag > 0) {
         if (hwest != 0) {
           const double r = -p.lin_drag * uc * fbw;
-          ru += div_rn(r, hwest, rhw);
+          ru += DIV(r, hwest, rhw);
           if constexpr (BUD) {
             budget_add(p.bud_u, BU_RDRAG, k, L, p.lstride, cell, r * p.dt);
             budget_add(p.bud_e, BE_RDRAG, k, L, p.lstride, cell, r * uc * p.dt);
@@ -968,7 +988,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         }
         if (hsouth != 0) {
           const double r = -p.lin_drag * vc * fbs;
-          rv += div_rn(r, hsouth, rhs);
+          rv += DIV(r, hsouth, rhs);
           if constexpr (BUD) {
             budget_add(p.bud_v, BU_RDRAG, k, L, p.lstride, cell, r * p.dt);
             budget_add(p.bud_e, BE_RDRAG, k, L, p.lstride, cell, r * vc * p.dt);
@@ -984,11 +1004,11 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         double hss = 0.5 * (gload(p.hhs, p, gi, gj, MAP_S, MAP_S) + gload(p.hhs, p, gi, gj - 1, MAP_S, MAP_S));
         return !p.ocean_surf_drag && p.use_rl && hss >= 0;
       };
-      if (p.lin_drag_surf > 0) {
+      if ((!LEAN && p.lin_drag_surf > 0)) {
         if (hwest != 0) {
           double r = -p.lin_drag_surf * (uc - gload(p.uLid, p, gi, gj, MAP_N, MAP_S)) * fsw;
           if (surf_mask_u()) r = 0;
-          ru += div_rn(r, hwest, rhw);
+          ru += DIV(r, hwest, rhw);
           if constexpr (BUD) {
             budget_add(p.bud_u, BU_RSURF, k, L, p.lstride, cell, r * p.dt);
             budget_add(p.bud_e, BE_RSURF, k, L, p.lstride, cell, r * uc * p.dt);
@@ -997,7 +1017,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         if (hsouth != 0) {
           double r = -p.lin_drag_surf * (vc - gload(p.vLid, p, gi, gj, MAP_S, MAP_N)) * fss;
           if (surf_mask_v()) r = 0;
-          rv += div_rn(r, hsouth, rhs);
+          rv += DIV(r, hsouth, rhs);
           if constexpr (BUD) {
             budget_add(p.bud_v, BU_RSURF, k, L, p.lstride, cell, r * p.dt);
             budget_add(p.bud_e, BE_RSURF, k, L, p.lstride, cell, r * vc * p.dt);
@@ -1008,7 +1028,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
       // squared bottom (surface) velocities of the neighbouring faces. Without a fraction
       // depth it acts on the bottom (top) layer alone, whose tile is in shared memory; with one
       // it acts on every layer the fractions reach, from the pre-pass's weighted velocities.
-      if (p.quad_drag > 0 && (p.drag_bot || k == L - 1)) {
+      if ((!LEAN && p.quad_drag > 0) && (p.drag_bot || k == L - 1)) {
         auto uab = [&](int a, int b) {
           if (p.drag_bot) {
             const double* UB = p.dragv;
@@ -1021,7 +1041,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         };
         if (hwest != 0) {
           const double ua = 0.5 * (uab(i, j) + uab(i - 1, j));
-          ru -= div_rn(p.quad_drag * ua * uc * fbw, hwest, rhw);
+          ru -= DIV(p.quad_drag * ua * uc * fbw, hwest, rhw);
           if constexpr (BUD) {
             budget_add(p.bud_u, BU_CDBOT, k, L, p.lstride, cell, -p.quad_drag * ua * uc * fbw * p.dt);
             budget_add(p.bud_e, BE_CDBOT, k, L, p.lstride, cell, -p.quad_drag * ua * sq(uc) * fbw * p.dt);
@@ -1029,14 +1049,14 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         }
         if (hsouth != 0) {
           const double ua = 0.5 * (uab(i, j) + uab(i, j - 1));
-          rv -= div_rn(p.quad_drag * ua * vc * fbs, hsouth, rhs);
+          rv -= DIV(p.quad_drag * ua * vc * fbs, hsouth, rhs);
           if constexpr (BUD) {
             budget_add(p.bud_v, BU_CDBOT, k, L, p.lstride, cell, -p.quad_drag * ua * vc * fbs * p.dt);
             budget_add(p.bud_e, BE_CDBOT, k, L, p.lstride, cell, -p.quad_drag * ua * sq(vc) * fbs * p.dt);
           }
         }
       }
-      if (p.quad_drag_surf > 0 && (p.drag_surf || k == 0)) {
+      if ((!LEAN && p.quad_drag_surf > 0) && (p.drag_surf || k == 0)) {
         const double wf = 1.0 - p.wfb;
         auto lidu = [&](int a, int b) { return gload(p.uLid, p, t.gx(a), t.gy(b), MAP_N, MAP_S); };
         auto lidv = [&](int a, int b) { return gload(p.vLid, p, t.gx(a), t.gy(b), MAP_S, MAP_N); };
@@ -1054,7 +1074,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
           const double ua = 0.5 * (uab(i, j) + uab(i - 1, j));
           double r = -p.quad_drag_surf * ua * (wf * uc - gload(p.uLid, p, gi, gj, MAP_N, MAP_S)) * fsw;
           if (surf_mask_u()) r = 0;
-          ru += div_rn(r, hwest, rhw);
+          ru += DIV(r, hwest, rhw);
           if constexpr (BUD) {
             budget_add(p.bud_u, BU_CDSURF, k, L, p.lstride, cell, r * p.dt);
             budget_add(p.bud_e, BE_CDSURF, k, L, p.lstride, cell, r * uc * p.dt);
@@ -1064,7 +1084,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
           const double ua = 0.5 * (uab(i, j) + uab(i, j - 1));
           double r = -p.quad_drag_surf * ua * (wf * vc - gload(p.vLid, p, gi, gj, MAP_S, MAP_N)) * fss;
           if (surf_mask_v()) r = 0;
-          rv += div_rn(r, hsouth, rhs);
+          rv += DIV(r, hsouth, rhs);
           if constexpr (BUD) {
             budget_add(p.bud_v, BU_CDSURF, k, L, p.lstride, cell, r * p.dt);
             budget_add(p.bud_e, BE_CDSURF, k, L, p.lstride, cell, r * vc * p.dt);
@@ -1073,7 +1093,7 @@ tendency_kernel(const __grid_constant__ TendParams p) {
       }
     }
     // ---- Newtonian velocity restoring (restoring.c:172-220) ----
-    if (p.use_relax) {
+    if (use_relax) {
       double ut = gload(p.uTime + k * p.lstride, p, gi, gj, MAP_N, MAP_S);
       if (ut > 0) {
         const double r = (-(uc - gload(p.uRelax + k * p.lstride, p, gi, gj, MAP_N, MAP_S))) / ut;
@@ -1099,9 +1119,9 @@ tendency_kernel(const __grid_constant__ TendParams p) {
     // ---- thickness tendency (work.c:1875-1885) ----
     double rh;
     {
-      double adv = div_rn(AT(huu, i, j) - AT(huu, i + 1, j), dx, rdx) + div_rn(AT(hvv, i, j) - AT(hvv, i, j + 1), dy, rdy);
+      double adv = DIV(AT(huu, i, j) - AT(huu, i + 1, j), dx, rdx) + DIV(AT(hvv, i, j) - AT(hvv, i, j + 1), dy, rdy);
       double rel = 0;
-      if (p.use_wdia) {
+      if (use_wdia) {
         const double* W0 = WDall + k * RN;
         const double* W1 = WDall + (k + 1) * RN;
         rel = -(AT(W0, i, j) - AT(W1, i, j));
@@ -1113,8 +1133,8 @@ tendency_kernel(const __grid_constant__ TendParams p) {
         // work.c:1891-1906 and the second loop of work.c:1913-1937
         const double hc0 = AT(sh, i, j);
         const double ke2 = 0.5 * (sq(uc) + sq(vc));
-        const double w0 = p.use_wdia ? AT(WDall + k * RN, i, j) : 0.0;
-        const double w1 = p.use_wdia ? AT(WDall + (k + 1) * RN, i, j) : 0.0;
+        const double w0 = use_wdia ? AT(WDall + k * RN, i, j) : 0.0;
+        const double w1 = use_wdia ? AT(WDall + (k + 1) * RN, i, j) : 0.0;
         double eta1 = p.hhb[cell];   // eta_w[k+1] and eta_w[k], built upward as in work.c:1184-1199
         for (int m = L - 1; m > k; --m) eta1 = eta1 + p.h[m * p.lstride + cell];
         const double eta0 = eta1 + hc0;
@@ -1132,12 +1152,12 @@ tendency_kernel(const __grid_constant__ TendParams p) {
           budget_add(p.bud_b, BB_WDIA, k, L, p.lstride, cell, bc * rel * p.dt);
         }
         if (p.bud_u || p.bud_v) {
-          const double adv_w = div_rn(AT(huu, i - 1, j) - AT(huu, i, j), dx, rdx)
-                             + div_rn(AT(hvv, i - 1, j) - AT(hvv, i - 1, j + 1), dy, rdy);
-          const double adv_s = div_rn(AT(huu, i, j - 1) - AT(huu, i + 1, j - 1), dx, rdx)
-                             + div_rn(AT(hvv, i, j - 1) - AT(hvv, i, j), dy, rdy);
+          const double adv_w = DIV(AT(huu, i - 1, j) - AT(huu, i, j), dx, rdx)
+                             + DIV(AT(hvv, i - 1, j) - AT(hvv, i - 1, j + 1), dy, rdy);
+          const double adv_s = DIV(AT(huu, i, j - 1) - AT(huu, i + 1, j - 1), dx, rdx)
+                             + DIV(AT(hvv, i, j - 1) - AT(hvv, i, j), dy, rdy);
           double rel_w = -(0.0 - 0.0), rel_s = -(0.0 - 0.0);
-          if (p.use_wdia) {
+          if (use_wdia) {
             rel_w = -(AT(WDall + k * RN, i - 1, j) - AT(WDall + (k + 1) * RN, i - 1, j));
             rel_s = -(AT(WDall + k * RN, i, j - 1) - AT(WDall + (k + 1) * RN, i, j - 1));
           }
@@ -1195,6 +1215,43 @@ tendency_kernel(const __grid_constant__ TendParams p) {
       p.h_out[o] = p.h_out[o] * (1 - err / htot);
     }
   }
+  // a tile whose quotients met an operand outside the branch-free division's range is listed
+  // for the exact pass (tile_list: count, done counter, tile indices)
+  if constexpr (!SLOWDIV) {
+    if (__syncthreads_or(oor) && tid == 0) {
+      const int e = atomicAdd(&p.tile_list[0], 1);
+      p.tile_list[2 + e] = by * ((p.Nx + TX - 1) / TX) + bx;
+    }
+  }
+}
+
+template <int MS, int TS, int H, bool LEAN>
+__global__ void __launch_bounds__(NT, PAWSIM_TEND_MINB) tendency_kernel(const __grid_constant__ TendParams p) {
+  tendency_tile<MS, TS, H, LEAN, false>(p, blockIdx.x, blockIdx.y);
+}
+
+// The exact pass: the tiles the fused kernel listed, recomputed with div_rn (normally none).
+// The last CTA to finish empties the list for the next launch.
+template <int MS, int TS, int H>
+__global__ void __launch_bounds__(NT, PAWSIM_TEND_MINB) tendency_exact_kernel(const __grid_constant__ TendParams p) {
+  const int n = p.tile_list[0];
+  const int gx = (p.Nx + TX - 1) / TX;
+  for (int e = blockIdx.x; e < n; e += gridDim.x) {
+    const int id = p.tile_list[2 + e];
+    tendency_tile<MS, TS, H, false, true>(p, id % gx, id / gx);
+    __syncthreads();
+  }
+  __shared__ int last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(&p.tile_list[1], 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    p.tile_list[0] = 0;
+    p.tile_list[1] = 0;
+    __threadfence();
+  }
 }
 
 template <int H>
@@ -1204,26 +1261,57 @@ size_t smem_bytes(const TendParams& p) {
        + (p.use_fractions ? (size_t)4 * p.L * NT * sizeof(double) : 0);
 }
 
+constexpr int EXACT_CTAS = 148;   // the exact pass's grid: one CTA per SM
+
+// the set-up needs none of the paths a LEAN instantiation leaves out
+inline bool lean_params(const TendParams& p) {
+  return !p.use_wdia && !p.use_relax && !p.use_diavisc && !p.use_fractions && !p.use_fbaro && !p.useA4 &&
+         !p.use_smag && !p.corners && !(p.quad_drag > 0) && !(p.quad_drag_surf > 0) && !(p.lin_drag_surf > 0) &&
+         !p.drag_bot && !p.drag_surf && !p.use_buoy;
+}
+
+// Launches the step (the drag pre-pass when needed, the fused kernel and, in the plain build,
+// the exact pass over flagged tiles); returns the number of launches, or -1.
 template <int MS, int TS, int H>
 int launch_t(const TendParams& p, cudaStream_t s) {
   const size_t shm = smem_bytes<H>(p);
   static bool attr_done = false;
   if (!attr_done) {
-    cudaFuncSetAttribute(tendency_kernel<MS, TS, H>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(tendency_kernel<MS, TS, H, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if constexpr (!BUD) {
+      cudaFuncSetAttribute(tendency_kernel<MS, TS, H, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      cudaFuncSetAttribute(tendency_exact_kernel<MS, TS, H>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           200 * 1024);
+    }
     attr_done = true;
   }
   if (shm > 200 * 1024) return -1;
+  int pre = 0;
   if (p.drag_bot || p.drag_surf) {
     dim3 b(32, 8), g((p.Nx + 31) / 32, (p.Ny + 7) / 8);
     drag_speed_kernel<TS><<<g, b, 0, s>>>(p);
+    pre = 1;
   }
   dim3 grid((p.Nx + TX - 1) / TX, (p.Ny + TY - 1) / TY);
-  tendency_kernel<MS, TS, H><<<grid, NT, shm, s>>>(p);
-  return 0;
+  if constexpr (BUD) {
+    tendency_kernel<MS, TS, H, false><<<grid, NT, shm, s>>>(p);
+    return pre + 1;
+  } else {
+    if (lean_params(p)) tendency_kernel<MS, TS, H, true><<<grid, NT, shm, s>>>(p);
+    else tendency_kernel<MS, TS, H, false><<<grid, NT, shm, s>>>(p);
+    // the exact recomputation of the listed tiles (one CTA per SM walks the list)
+    tendency_exact_kernel<MS, TS, H><<<EXACT_CTAS, NT, shm, s>>>(p);
+    return pre + 2;
+  }
 }
 
 template <int TS, int H>
 int launch_ms(const TendParams& p, int ms, cudaStream_t s) {
+#ifdef PAWSIM_TEND_MS
+  // this translation unit holds one momentum scheme (the build splits the instantiations)
+  if (ms != PAWSIM_TEND_MS) return -1;
+  return launch_t<PAWSIM_TEND_MS, TS, H>(p, s);
+#else
   switch (ms) {
     case 0: return launch_t<0, TS, H>(p, s);
     case 1: return launch_t<1, TS, H>(p, s);
@@ -1231,6 +1319,7 @@ int launch_ms(const TendParams& p, int ms, cudaStream_t s) {
     case 3: return launch_t<3, TS, H>(p, s);
   }
   return -1;
+#endif
 }
 
 // the upwind thickness schemes and the Smagorinsky biharmonic reach a third halo cell
@@ -1246,12 +1335,15 @@ inline bool wide_halo(const TendParams& p, int ts) { return ts >= 2 || (p.use_sm
 #define PAWSIM_TEND_LAUNCH_FN launch_tendency_budget_tile
 #else
 #define PAWSIM_TEND_SMEM_FN PAWSIM_TEND_CAT(tendency_smem_ty, PAWSIM_TEND_TY)
-#define PAWSIM_TEND_LAUNCH_FN PAWSIM_TEND_CAT(launch_tendency_ty, PAWSIM_TEND_TY)
+#define PAWSIM_TEND_LAUNCH_FN PAWSIM_TEND_CAT(PAWSIM_TEND_CAT(launch_tendency_ty, PAWSIM_TEND_TY), \
+                                              PAWSIM_TEND_CAT(_m, PAWSIM_TEND_MS))
 #endif
 
+#if PAWSIM_TEND_BUD || PAWSIM_TEND_MS == 0
 size_t PAWSIM_TEND_SMEM_FN(const TendParams& p, int ts) {
   return wide_halo(p, ts) ? smem_bytes<3>(p) : smem_bytes<2>(p);
 }
+#endif
 
 int PAWSIM_TEND_LAUNCH_FN(const TendParams& p, int ms, int ts, cudaStream_t s) {
   if (p.L < 1 || p.L > LMAX) return -1;
