@@ -181,8 +181,17 @@ PAWSIM_API int pawsim_gpu_pressure_correct (pawsim_gpu * m, int update_diags, pa
 PAWSIM_API int pawsim_gpu_prelim (pawsim_gpu * m, pawsim_gpu_stats * st);
 /* integrator step n followed by the rigid-lid correction (one pass of pawsim.c:471-492) */
 PAWSIM_API int pawsim_gpu_step (pawsim_gpu * m, unsigned n, pawsim_gpu_stats * st);
-/* nsteps passes starting at step n0; st receives the last step's report */
+/* nsteps passes starting at step n0 (the main loop of pawsim.c:471-511 without its outputs);
+ * st receives the last step's report. Steps whose correction needs no report formed on the
+ * host (SOR or the gathered multigrid once its first solves have tuned it, without
+ * pressure_timing or the learned warm start) are enqueued back to back without a host
+ * synchronisation: their iteration counts go to a device ring read once at the end (st's
+ * solve_ms and norms are 0 for them). check_nonfinite and fail_on_maxiters are evaluated at the
+ * end of the run. */
 PAWSIM_API int pawsim_gpu_run (pawsim_gpu * m, unsigned n0, unsigned nsteps, pawsim_gpu_stats * st);
+/* The iteration count of each step of the last pawsim_gpu_run (n = its nsteps): the numbers of
+ * the reference's per-step "PAWSIM pressure solve" lines (pawsim.c:95-108). */
+PAWSIM_API int pawsim_gpu_run_iterations (pawsim_gpu * m, int * iters, size_t n);
 
 /* Online time averages (diagnostics.c:307-470, the savefreqAvg outputs). accumulate adds
  * avg_fac * dt times the current state to the running sums (call it after each step, with

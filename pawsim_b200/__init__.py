@@ -69,6 +69,7 @@ EXPORTS = (
     "pawsim_gpu_create", "pawsim_gpu_destroy", "pawsim_gpu_set_field", "pawsim_gpu_get_field",
     "pawsim_gpu_init", "pawsim_gpu_tendency_eval", "pawsim_gpu_integrator_step",
     "pawsim_gpu_pressure_correct", "pawsim_gpu_prelim", "pawsim_gpu_step", "pawsim_gpu_run",
+    "pawsim_gpu_run_iterations",
     "pawsim_gpu_solve_mg", "pawsim_gpu_set_stream", "pawsim_gpu_synchronize",
     "pawsim_gpu_time", "pawsim_gpu_launch_count", "pawsim_gpu_last_error",
     "pawsim_nn_conv3x3", "pawsim_nn_conv3x3_wgrad", "pawsim_nn_flip_weights",
@@ -106,6 +107,7 @@ def load_library(path: str = LIB_PATH):
     lib.pawsim_gpu_prelim.argtypes = [P, ctypes.POINTER(GpuStats)]
     lib.pawsim_gpu_step.argtypes = [P, ctypes.c_uint, ctypes.POINTER(GpuStats)]
     lib.pawsim_gpu_run.argtypes = [P, ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(GpuStats)]
+    lib.pawsim_gpu_run_iterations.argtypes = [P, ctypes.POINTER(ctypes.c_int), ctypes.c_size_t]
     lib.pawsim_gpu_solve_mg.argtypes = [P, ctypes.POINTER(GpuStats)]
     lib.pawsim_gpu_accumulate_averages.argtypes = [P, ctypes.c_double]
     lib.pawsim_gpu_scale_averages.argtypes = [P, ctypes.c_double]
@@ -306,9 +308,19 @@ class Model:
         return st.as_dict()
 
     def run(self, n0: int, nsteps: int) -> dict:
+        """nsteps steps from step n0 (enqueued without host synchronisation where the solver
+        allows); the last step's report."""
         st = GpuStats()
         _check(self.lib.pawsim_gpu_run(self._h, n0, nsteps, ctypes.byref(st)))
+        self._last_run = nsteps
         return st.as_dict()
+
+    def run_iterations(self) -> np.ndarray:
+        """The solve iteration count of each step of the last run."""
+        n = getattr(self, "_last_run", 0)
+        out = np.zeros(n, dtype=np.int32)
+        _check(self.lib.pawsim_gpu_run_iterations(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n))
+        return out
 
     def solve_mg(self) -> dict:
         st = GpuStats()

@@ -130,6 +130,12 @@ struct Model {
   double* bud[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   double* pi_prev = nullptr;   // solution before the last one (pi_guess = 1)
   int pi_solves = 0;           // multigrid solves completed, for the extrapolated guess
+  // asynchronous runs (pawsim_gpu_run): each step's solve report in a device ring (iteration
+  // count, final stopping measure), read once at the end of the run
+  int* run_iters = nullptr;
+  double* run_meas = nullptr;
+  int run_cap = 0;
+  std::vector<int> last_run_iters;
   // asynchronous saves: two staging slots (device, packed planes) with page-locked host
   // copies, filled by a copy stream; busy until the caller releases the slot
   struct SaveSlot {
@@ -815,6 +821,64 @@ static int pressure_correct(Model* m, int update_diags, pawsim_gpu_stats* st) {
   return iters;
 }
 
+// Can the rigid-lid correction run without a host synchronisation? (no report the host must
+// form: pressure timing, warm start, the distributed multigrid's host loop, full multigrid)
+static bool async_correct_ok(const Model* m) {
+  const pawsim_gpu_config& c = m->c;
+  if (!c.use_rl) return true;
+  if (c.pressure_timing || (m->ws && m->nn_mode)) return false;
+  if (c.solver == PAWSIM_GPU_SOLVER_SOR) return true;
+  if (c.solver == PAWSIM_GPU_SOLVER_MG) return m->mg && m->mg->async_ready();
+  return false;
+}
+
+// The rigid-lid correction of pressure_correct without a host synchronisation; the solve's
+// iteration count and stopping measure go to the run ring's slot q.
+static int pressure_correct_async(Model* m, int q) {
+  if (!m->c.use_rl) return 0;
+  const int cur = m->cur;
+  Grid2 g = m->grid2();
+  dim3 b(32, 8), gr((m->Nx + 31) / 32, (m->Ny + 7) / 8);
+  if (!m->thickness_fixed) {
+    thickness_fix_kernel<<<gr, b, 0, m->s>>>(m->h[cur], m->Hc, m->Nx, m->Ny, m->pitch, m->lstride, m->L);
+    ++g_launches;
+  }
+  m->thickness_fixed = false;
+  g_launches += launch_pressure_rhs(g, m->u[cur], m->v[cur], m->h[cur], m->rhs, m->s);
+  corner_fill(m, cur);
+  launch_sum(m->rhs, m->Nx, m->Ny, m->pitch, m->serial(), m->scratch, m->dsum, m->s);
+  launch_subtract_mean(m->rhs, m->Nx, m->Ny, m->pitch, m->dsum, m->s);
+  g_launches += m->serial() ? 2 : 3;
+  if (m->c.solver == PAWSIM_GPU_SOLVER_SOR) {
+    if (launch_sor(g, m->pi, m->rhs, m->op, m->c.sor_rp, m->c.pi_tol, m->c.maxiters, m->slots, m->diters, m->s) != 0)
+      return fail(PAWSIM_GPU_ECUDA, "cooperative SOR launch failed");
+    ++g_launches;
+    launch_sum(m->pi, m->Nx, m->Ny, m->pitch, m->serial(), m->scratch, m->dsum, m->s);
+    launch_subtract_mean(m->pi, m->Nx, m->Ny, m->pitch, m->dsum, m->s);
+    g_launches += m->serial() ? 2 : 3;
+    PAWSIM_CUDA_OK(cudaMemcpyAsync(m->run_iters + q, m->diters, sizeof(int), cudaMemcpyDeviceToDevice, m->s));
+  } else {
+    if (m->c.pi_guess == 1) {
+      if (m->pi_solves >= 2) {
+        extrapolate_kernel<<<gr, b, 0, m->s>>>(m->pi, m->pi_prev, m->Nx, m->Ny, m->pitch);
+        ++g_launches;
+      } else if (m->pi_solves == 1) {
+        PAWSIM_CUDA_OK(cudaMemcpyAsync(m->pi_prev, m->pi, (size_t)m->Ny * m->pitch * sizeof(double),
+                                       cudaMemcpyDeviceToDevice, m->s));
+      }
+      ++m->pi_solves;
+    }
+    long long nl = 0;
+    if (m->mg->solve_async(m->pi, m->rhs, m->c.pi_tol, m->c.maxiters, m->run_iters + q, m->run_meas + q, &nl) != 0)
+      return fail(PAWSIM_GPU_ECUDA, "asynchronous multigrid solve failed");
+    g_launches += nl;
+  }
+  launch_projection(g, m->pi, m->u[cur], m->v[cur], m->s);
+  ++g_launches;
+  PAWSIM_CUDA_OK(cudaGetLastError());
+  return 0;
+}
+
 }  // namespace pawsim
 
 using namespace pawsim;
@@ -903,10 +967,68 @@ int pawsim_gpu_step(pawsim_gpu* h, unsigned n, pawsim_gpu_stats* st) {
 
 int pawsim_gpu_run(pawsim_gpu* h, unsigned n0, unsigned nsteps, pawsim_gpu_stats* st) {
   if (!h) return PAWSIM_GPU_EBADCONFIG;
-  for (unsigned n = n0; n < n0 + nsteps; ++n) {
-    int r = pawsim_gpu_step(h, n, st);
-    if (r) return r;
+  Model* m = h->m;
+  m->last_run_iters.assign(nsteps, 0);
+  if (nsteps == 0) return 0;
+  if ((int)nsteps > m->run_cap) {
+    int* ri = m->alloc<int>(nsteps);
+    double* rm = m->alloc<double>(nsteps);
+    if (!ri || !rm) return fail(PAWSIM_GPU_ECUDA, "run report allocation failed");
+    m->run_iters = ri;
+    m->run_meas = rm;
+    m->run_cap = (int)nsteps;
   }
+  // steps whose correction needs the host run synchronously (the first solves tune the
+  // multigrid and build its graph); the others are enqueued back to back and their reports
+  // read once at the end
+  std::vector<char> async(nsteps, 0);
+  pawsim_gpu_stats last;
+  memset(&last, 0, sizeof(last));
+  for (unsigned q = 0; q < nsteps; ++q) {
+    const unsigned n = n0 + q;
+    if (async_correct_ok(m)) {
+      int r = integrator_step(m, n, true);
+      if (r) return r;
+      r = pressure_correct_async(m, (int)q);
+      if (r) return r;
+      async[q] = 1;
+    } else {
+      int r = pawsim_gpu_step(h, n, &last);
+      if (r) return r;
+      m->last_run_iters[q] = last.iters;
+    }
+  }
+  std::vector<int> it(nsteps);
+  std::vector<double> ms(nsteps);
+  PAWSIM_CUDA_OK(cudaMemcpyAsync(it.data(), m->run_iters, nsteps * sizeof(int), cudaMemcpyDeviceToHost, m->s));
+  PAWSIM_CUDA_OK(cudaMemcpyAsync(ms.data(), m->run_meas, nsteps * sizeof(double), cudaMemcpyDeviceToHost, m->s));
+  PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
+  int r = 0;
+  for (unsigned q = 0; q < nsteps; ++q) {
+    if (!async[q]) continue;
+    m->last_run_iters[q] = it[q];
+    if (m->c.use_rl && m->c.solver == PAWSIM_GPU_SOLVER_MG) g_launches += (long long)it[q] * m->mg->body_launches();
+    if (!r) r = check_converged(m, it[q]);
+    if (q == nsteps - 1) {
+      last.iters = it[q];
+      last.stop_measure = m->c.solver == PAWSIM_GPU_SOLVER_MG ? ms[q] : 0;
+      last.mg_omega = m->mg && m->c.solver == PAWSIM_GPU_SOLVER_MG ? m->mg->omega() : 0;
+    }
+  }
+  if (st) *st = last;
+  if (m->nonfinite) {   // the flag raised during the run, read once
+    m->nf_calls = m->c.check_nonfinite - 1;
+    int rf = check_state_finite(m);
+    if (rf) return rf;
+  }
+  return r;
+}
+
+int pawsim_gpu_run_iterations(pawsim_gpu* h, int* iters, size_t n) {
+  if (!h || !iters) return fail(PAWSIM_GPU_EBADCONFIG, "null argument");
+  const std::vector<int>& v = h->m->last_run_iters;
+  if (n != v.size()) return fail(PAWSIM_GPU_EBADCONFIG, "n must equal the last run's step count");
+  if (n) memcpy(iters, v.data(), n * sizeof(int));
   return 0;
 }
 

@@ -786,6 +786,8 @@ struct LoopState {
   int maxiters;
   double tol;
   double maxres;
+  int* iters_out;            // nullable: receives iters and maxres after every cycle (the
+  double* maxres_out;        // asynchronous solves' report slot)
 };
 
 // max |pi - Jacobi(pi)| on the fine level (multigrid.c:1123-1156); NaNs are ignored like fmax
@@ -816,7 +818,9 @@ __global__ void max_residual2_kernel(LV<double> l, const double* pa, const doubl
   block_max_to(mb, &bits[1]);
 }
 
-__global__ void loop_reset_kernel(LoopState* st, int maxiters, double tol) {
+__global__ void loop_reset_kernel(LoopState* st, int maxiters, double tol, int* iters_out, double* maxres_out) {
+  st->iters_out = iters_out;
+  st->maxres_out = maxres_out;
   st->bits = 0;
   st->iters = 0;
   st->maxiters = maxiters;
@@ -831,6 +835,10 @@ __global__ void loop_finalize_kernel(LoopState* st, cudaGraphConditionalHandle h
   st->iters += 1;
   st->maxres = m;
   unsigned cont = (m > st->tol) && (st->iters < st->maxiters);
+  if (st->iters_out) {
+    *st->iters_out = st->iters;
+    *st->maxres_out = m;
+  }
   cudaGraphSetConditional(h, cont);
 }
 
@@ -871,6 +879,18 @@ __global__ void defect_kernel(LV<double> l, double* a, double* b, const int* ite
     if (correct) pout[c] = pc;
   }
   block_max_to(m, bits);
+}
+
+// the asynchronous FP32 solve's end: when the last cycle (index iters - 1) was even it wrote pi
+// to the scratch array, so copy it back; decided on the device from the loop state
+__global__ void commit_if_even_kernel(const LoopState* st, double* dst, const double* src, int Nx, int Ny,
+                                      int pitch) {
+  const int it = st->iters;
+  if (it <= 0 || ((it - 1) & 1) != 0) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= Nx || j >= Ny) return;
+  dst[(size_t)j * pitch + i] = src[(size_t)j * pitch + i];
 }
 
 __global__ void commit_kernel(double* dst, const double* src, int Nx, int Ny, int pitch) {
@@ -1464,7 +1484,7 @@ int Multigrid::solve_once(double* pi, const double* rhs, double tol, int maxiter
     return it;
   }
   if (!g_->exec[prec] && build_graph(prec) != 0) return -1;
-  loop_reset_kernel<<<1, 1, 0, s_>>>(st, maxiters, tol);
+  loop_reset_kernel<<<1, 1, 0, s_>>>(st, maxiters, tol, nullptr, nullptr);
   ++g_launches;
   if (prec == 1) {
     Level& F = lv_.back();
@@ -1488,6 +1508,35 @@ int Multigrid::solve_once(double* pi, const double* rhs, double tol, int maxiter
   g_launches += (long long)h.iters * body_launches_[prec];
   if (maxres_out) *maxres_out = h.maxres;
   return h.iters;
+}
+
+bool Multigrid::async_ready() const {
+  const int prec = opt_.fp32_cycles ? 1 : 0;
+  return g_->exec[prec] != nullptr && !opt_.full_mg && (!opt_.omega_auto || omega_tuned_) &&
+         fine_pi_ != nullptr;
+}
+
+int Multigrid::solve_async(double* pi, const double* rhs, double tol, int maxiters, int* iters_out,
+                           double* maxres_out, long long* launches) {
+  const int prec = opt_.fp32_cycles ? 1 : 0;
+  if (fine_pi_ != pi || fine_rhs_ != rhs || !g_->exec[prec]) return -1;
+  LoopState* st = reinterpret_cast<LoopState*>(dstate_);
+  ++nsolves_;
+  loop_reset_kernel<<<1, 1, 0, s_>>>(st, maxiters, tol, iters_out, maxres_out);
+  *launches = 1;
+  Level& F = lv_.back();
+  if (prec == 1) {
+    LV<double> f = view<double>(F);
+    defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, s_>>>(f, F.e, F.res, nullptr, 0, F.e32, F.pitch, F.rhs32, 0, &st->bits);
+    cudaMemsetAsync(&st->bits, 0, sizeof(unsigned long long), s_);
+    ++*launches;
+  }
+  if (cudaGraphLaunch(g_->exec[prec], s_) != cudaSuccess) return -1;
+  if (prec == 1) {
+    commit_if_even_kernel<<<g2(F.Nx, F.Ny), B2, 0, s_>>>(st, F.e, F.res, F.Nx, F.Ny, F.pitch);
+    ++*launches;
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 template void Multigrid::enqueue_vcycle<double>(cudaStream_t, unsigned long long*, bool, int);

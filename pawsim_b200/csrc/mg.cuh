@@ -47,6 +47,14 @@ class Multigrid {
   // maxres_out receives max |pi - Jacobi(pi)| of the last check.
   int solve(double* pi, int pi_pitch, const double* rhs, int rhs_pitch, double tol, int maxiters,
             double* maxres_out);
+  // Solve without a host synchronisation: the V-cycle count and the final stopping measure go
+  // to the device slots iters_out / maxres_out. Only after a synchronous solve on the same pi
+  // and rhs has built the loop (async_ready); *launches receives the kernels enqueued outside
+  // the V-cycle graph (each executed cycle adds body_launches(), counted by the caller).
+  bool async_ready() const;
+  int solve_async(double* pi, const double* rhs, double tol, int maxiters, int* iters_out, double* maxres_out,
+                  long long* launches);
+  int body_launches() const { return body_launches_[opt_.fp32_cycles ? 1 : 0]; }
   // the weight in use (after the automatic choice, the chosen one)
   double omega() const { return opt_.omega_rb; }
   // one evaluation of the stopping measure (for diagnostics and warm-start decisions)

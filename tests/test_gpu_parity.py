@@ -296,3 +296,29 @@ def test_full_mg_tolerance(tmp_path, oracle_mod, lib, fp32, kind, kw):
     s_o, s_g = o.state(), m.state()
     for var in ("u", "v", "h"):
         assert rel_l2(s_g[var], s_o[var]) < 1e-9, (var, rel_l2(s_g[var], s_o[var]))
+
+
+@pytest.mark.parametrize("fp32", [0, 1], ids=["fp64", "fp32-defect"])
+@pytest.mark.parametrize("kind,kw", [
+    ("gyre", dict(N=128, solver=1, tol=1e-12, dt=900.0)),
+    ("gyre", dict(N=48, Ny=40, solver=0, tol=1e-10, dt=900.0)),
+    ("channel", dict(Nx=128, Ny=64, solver=1, tol=1e-12, dt=150.0)),
+], ids=["gyre128-mg", "gyre48x40-sor", "channel-mg"])
+def test_run_without_host_syncs_matches_steps(tmp_path, lib, fp32, kind, kw):
+    """pawsim_gpu_run enqueues the steps whose correction needs no host report back to back
+    (device-side iteration counts, the FP32 solve's final copy decided on the device): the
+    states and every step's iteration count equal those of pawsim_gpu_step called step by
+    step."""
+    _, cfg, f = make_setup(tmp_path, kind, **kw)
+    a = lib.Model(cfg, f, mg_fp32=fp32)
+    b = lib.Model(cfg, f, mg_fp32=fp32)
+    a.prelim()
+    b.prelim()
+    want = [a.step(n)["iters"] for n in range(1, 13)]
+    st = b.run(1, 12)
+    got = list(b.run_iterations())
+    assert got == want, (got, want)
+    assert st["iters"] == want[-1]
+    for var in ("u", "v", "h"):
+        assert value_equal(a.state()[var], b.state()[var]), var
+    assert value_equal(a.get("pi"), b.get("pi"))
