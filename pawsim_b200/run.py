@@ -6,7 +6,8 @@
                               [--ws-collect S --ws-epochs E] [--tracer SCHEME]
                               [--averages] [--energy] [--budgets]
 
-``--integrator-only`` advances with ``pawsim_gpu_integrator_step`` alone (one fused tendency
+``--run`` advances with one ``pawsim_gpu_run`` call (steps enqueued without a host
+synchronisation). ``--integrator-only`` advances with ``pawsim_gpu_integrator_step`` alone (one fused tendency
 kernel per step, no pressure correction), which isolates the tendency kernel for a profiler.
 ``--param`` runs an existing AWSIM parameter file instead of a synthetic set-up.
 ``--ws-collect S`` first runs S steps that collect warm-start training pairs, trains the
@@ -46,6 +47,7 @@ def main(argv=None):
     ap.add_argument("--mg-pre", type=int, default=1)
     ap.add_argument("--mg-post", type=int, default=1)
     ap.add_argument("--integrator-only", action="store_true")
+    ap.add_argument("--run", action="store_true", help="advance with one pawsim_gpu_run call (no per-step sync)")
     ap.add_argument("--ws-collect", type=int, default=0)
     ap.add_argument("--ws-epochs", type=int, default=2)
     ap.add_argument("--tracer", type=int, default=-1, help="tracer scheme 0..2; negative: no tracer")
@@ -103,11 +105,15 @@ def main(argv=None):
                 m.nn_setup(collect=False, use=True)
             rep = {}
             iters, used = [], 0
-            for n in range(n0, n0 + a.steps):
-                rep = m.step(n)
-                diagnostics()
-                iters.append(rep["iters"])
-                used += rep["warm_start"] == 1
+            if a.run:
+                rep = m.run(n0, a.steps)
+                iters = [int(x) for x in m.run_iterations()]
+            else:
+                for n in range(n0, n0 + a.steps):
+                    rep = m.step(n)
+                    diagnostics()
+                    iters.append(rep["iters"])
+                    used += rep["warm_start"] == 1
             rep["iters_per_step"] = iters
             if ws:
                 rep["warm_start_used"] = used
