@@ -37,6 +37,16 @@ METRIC = "sim-days/s at 2048^2 2-layer (double gyre, rigid lid, AB3, MG pressure
 N_GRID = int(os.environ.get("PAWSIM_BENCH_N", "2048"))
 DT = 60.0
 TOL = 1e-10
+# Stable steps of the other configurations. The channel's biharmonic 1e10 m^4/s on 3.9 km
+# cells limits AB3 to about 200 s (dt 900 s grows without bound); on the 977 m cells of the
+# 4096^2 gyre a biharmonic 5e9 m^4/s would need dt below 2 s and the internal wave limits dt to
+# about 80 s, so that case runs with 1e8 m^4/s and 50 s.
+CHANNEL_DT = 150.0
+FULL_DT = 50.0
+FULL_A4 = 1e8
+# grid spacing of the ensemble's jets members: at dt = 600 s the AB3 limit of the internal
+# gravity wave (about 3 m/s) needs dx above about 7 km
+ENS_DX = 10e3
 FP32_INNER = 4   # FP32 V-cycles per FP64 defect-correction step in the mixed-precision solves
 
 
@@ -264,6 +274,154 @@ def budget_timing(stream, reps):
     return out
 
 
+def config_timing(kind, steps, warmup, stream, peak):
+    """The other stated configurations at their full sizes: steps/s and sim-days/s of the
+    plain FP64 multigrid and of FP32 V-cycles in FP64 defect correction (device-timed runs with
+    the state resident, CUDA events on the model's stream), the fused kernel's time inside
+    complete steps, and whether the state stayed finite.
+      channel: 1024 x 512 x 3 zonally periodic channel with a ridge, biharmonic 1e10
+      full: 4096 x 4096 x 4 closed gyre, random bathymetry, 200 km sponge restoring the
+            interfaces over 30 days, w_dia 1e-7 m/s, biharmonic viscosity
+    The time steps are the largest the AB3 scheme keeps stable on these grids (CHANNEL_DT,
+    FULL_DT, FULL_A4 below)."""
+    import tempfile as _tf
+    import pawsim_b200
+    import torch
+    out = {}
+    with _tf.TemporaryDirectory() as d:
+        if kind == "channel":
+            p = pawsim_b200.inputs.channel(d + "/c", Nx=1024, Ny=512, dt=CHANNEL_DT, A4=1e10, solver=1, tol=TOL)
+            desc = f"1024 x 512 x 3 channel (x-periodic, ridge), biharmonic 1e10 m^4/s, dt {CHANNEL_DT:g} s, AB3"
+        else:
+            p = pawsim_b200.inputs.full_physics(d + "/f", N=4096, dt=FULL_DT, A4=FULL_A4, solver=1, tol=TOL)
+            desc = ("4096 x 4096 x 4 closed gyre, bathymetry, sponge restoring, w_dia 1e-7 m/s, "
+                    f"biharmonic {FULL_A4:g} m^4/s, dt {FULL_DT:g} s, AB3")
+        cfg = pawsim_b200.inputs.read_config(p)
+        fields = pawsim_b200.inputs.load_fields(cfg)
+        out["workload"] = desc
+        L, ncell = cfg.Nlay, cfg.Nx * cfg.Ny
+        dt = cfg.dt
+        for label, fp32 in (("fp64_mg", 0), ("fp32_in_fp64_mg", FP32_INNER)):
+            m = pawsim_b200.Model(cfg, fields, mg_fp32=fp32, check_nonfinite=1)
+            m.set_stream(stream.cuda_stream)
+            with torch.cuda.stream(stream):
+                m.prelim()
+                n = 1
+                for _ in range(warmup):
+                    m.step(n)
+                    n += 1
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                finite = True
+                try:
+                    m.run(n, steps)
+                except pawsim_b200.PawsimError:
+                    finite = False
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1)
+                n += steps
+                res = {"ms_per_step": ms / steps, "sim_days_per_s": steps * dt / 86400.0 / (ms / 1e3),
+                       "gpl_updates_per_s": steps * ncell * L / (ms / 1e3), "finite": finite}
+                if finite:
+                    res["vcycles_per_step"] = float(np.mean(m.run_iterations()))
+                    k_ms = 0.0
+                    for _ in range(5):
+                        k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        k0.record(stream)
+                        m.integrator_step(n)
+                        k1.record(stream)
+                        m.pressure_correct(True)
+                        n += 1
+                        torch.cuda.synchronize()
+                        k_ms += k0.elapsed_time(k1) / 5
+                    alg = ncell * (120 * L + 24)
+                    res["tendency_kernel_ms"] = k_ms
+                    res["tendency_frac_of_measured_hbm"] = alg / (k_ms / 1e3) / 1e9 / peak
+                out[label] = res
+            m.close()
+    out["tendency_bytes_note"] = ("algorithmic bytes N (120 L + 24): state, AB history and outputs; the "
+                                  "feature inputs (restoring fields, w_dia, bathymetry) are not counted")
+    return out
+
+
+def ensemble_timing(steps, warmup, peak):
+    """The batched uneven ensemble: 64 members at 256 x 256 and 16 at 512 x 512 of the
+    doubly periodic 2-layer jets set-up (dx = 10 km, dt = 600 s, distinct noise seeds, plain
+    FP64 multigrid), advanced together (one fused-kernel launch per step over all members'
+    tiles, each member's correction on its own stream), against the same members from the same
+    start advanced one after another with their own runs. Times are host clocks around
+    synchronised runs (the ensemble's streams are its own); the kernel time is CUDA events on
+    the launch stream."""
+    import tempfile as _tf
+    import pawsim_b200
+    import torch
+    specs = [(256, 1000 + i) for i in range(64)] + [(512, 2000 + i) for i in range(16)]
+    dt = 600.0
+    with _tf.TemporaryDirectory() as d:
+        cfgs = []
+        for i, (N, seed) in enumerate(specs):
+            p = pawsim_b200.inputs.jets(f"{d}/m{i}", N=N, Ly=N * ENS_DX, dt=dt, seed=seed, solver=1, tol=TOL)
+            c = pawsim_b200.inputs.read_config(p)
+            cfgs.append((c, pawsim_b200.inputs.load_fields(c)))
+
+        def fresh():
+            ms = []
+            for c, f in cfgs:
+                m = pawsim_b200.Model(c, f, check_nonfinite=1)
+                m.prelim()
+                ms.append(m)
+            return ms
+
+        # the members one after another, each with its own run (its own launch sequence)
+        alone = fresh()
+        for m in alone:
+            m.run(1, warmup)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for m in alone:
+            m.run(1 + warmup, steps)
+        torch.cuda.synchronize()
+        sec_alone = time.perf_counter() - t0
+        iters_alone = np.concatenate([m.run_iterations() for m in alone])
+        for m in alone:
+            m.close()
+        # the same members from the same start, advanced together
+        members = fresh()
+        ens = pawsim_b200.Ensemble(members)
+        ens.run(1, warmup)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ens.run(1 + warmup, steps)
+        sec = time.perf_counter() - t0
+        k_ms = ens.kernel_ms()
+        iters = np.concatenate([m.run_iterations() for m in members])
+        ens.close()
+        for m in members:
+            m.close()
+    L = 2
+    cells = sum(N * N for N, _ in specs)
+    alg = cells * (120 * L + 24)
+    ach = alg / (k_ms / 1e3) / 1e9
+    return {
+        "workload": "64 x 256^2 + 16 x 512^2 jets members, 2 layers, dt 600 s, AB3, FP64 multigrid 1e-10",
+        "members": len(specs), "steps": steps, "warmup": warmup,
+        "ms_per_step": sec / steps * 1e3,
+        "member_steps_per_s": len(specs) * steps / sec,
+        "sim_days_per_s_all_members": len(specs) * steps * dt / 86400.0 / sec,
+        "gpl_updates_per_s": steps * cells * L / sec,
+        "vcycles_per_step": float(np.mean(iters)),
+        "same_vcycles_as_alone": bool(np.array_equal(iters, iters_alone)),
+        "alone_ms_per_step": sec_alone / steps * 1e3,
+        "speedup_vs_members_alone": sec_alone / sec,
+        "timing": "host clock around synchronised runs; inputs (80 x 2 x 3 state planes) above L2",
+        "roofline": {"bound": "hbm", "kernel": "tendency_batch_kernel + tendency_batch_exact_kernel",
+                     "kernel_ms": k_ms, "algorithmic_bytes": alg, "achieved": ach, "peak": peak,
+                     "unit": "GB/s", "frac": ach / peak},
+    }
+
+
 def pressure_comparison(cfg, fields, stream, spin, steps, epochs, pairs):
     """Pressure ms/step and V-cycles/step of the plain FP64 multigrid (started from the
     previous pressure, as the reference's solver is) against FP32 V-cycles in FP64 defect
@@ -331,6 +489,8 @@ def main():
     ap.add_argument("--no-warm-start", action="store_true", help="skip the learned+FP32 pressure comparison")
     ap.add_argument("--ws-spin", type=int, default=160, help="spin-up steps that collect training pairs")
     ap.add_argument("--ws-epochs", type=int, default=30)
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched ensemble sub-line")
+    ap.add_argument("--no-configs", action="store_true", help="skip the channel and full-physics sub-lines")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -528,6 +688,11 @@ def main():
                           "frac": tr_bytes / (tr / 1e3) / 1e9 / peak}
     if ws is not None:
         line["pressure_learned_fp32_vs_plain_fp64"] = ws
+    if not args.no_ensemble:
+        line["ensemble"] = ensemble_timing(min(args.steps, 100), args.warmup, peak)
+    if not args.no_configs:
+        line["channel_1024x512x3"] = config_timing("channel", min(args.steps, 100), args.warmup, stream, peak)
+        line["full_physics_4096x4096x4"] = config_timing("full", min(args.steps, 20), args.warmup, stream, peak)
     if rank == 0 and not args.no_cpu_baseline:
         # a bounded sample in steady state: steps 4 and 5 (after the AB1/AB2 start-up)
         secs, sample = cpu_reference(param, 3, 2)

@@ -193,6 +193,24 @@ PAWSIM_API int pawsim_gpu_run (pawsim_gpu * m, unsigned n0, unsigned nsteps, paw
  * the reference's per-step "PAWSIM pressure solve" lines (pawsim.c:95-108). */
 PAWSIM_API int pawsim_gpu_run_iterations (pawsim_gpu * m, int * iters, size_t n);
 
+/* Batched ensemble (no reference counterpart: the reference runs one model per process, its
+ * multigrid state being file-scope globals, model_code/multigrid.c:54-63; this replaces n such
+ * processes). Members are initialised models of any grid sizes that share Nlay, the momentum
+ * and thickness schemes, use_rl and the fused kernel's feature set, without tracer, budgets or
+ * a quadratic drag over a fraction depth. create moves each member onto its own stream (destroy
+ * gives back the previous one). run advances every member nsteps integrator steps numbered
+ * n0.. : per step one launch of the fused kernel over all members' tiles, then each member's
+ * rigid-lid correction on its own stream, with no host synchronisation until the end; each
+ * member's results equal those of pawsim_gpu_run on that member alone, and its per-step
+ * iteration counts are read with pawsim_gpu_run_iterations. */
+typedef struct pawsim_gpu_ensemble pawsim_gpu_ensemble;
+PAWSIM_API int pawsim_gpu_ensemble_create (pawsim_gpu * const * members, int n, pawsim_gpu_ensemble ** out);
+PAWSIM_API int pawsim_gpu_ensemble_run (pawsim_gpu_ensemble * e, unsigned n0, unsigned nsteps);
+/* Mean device time (ms) of one step's batched fused-kernel launch (with its exact pass) over
+ * the last run, from CUDA events on the ensemble's launch stream. */
+PAWSIM_API double pawsim_gpu_ensemble_kernel_ms (const pawsim_gpu_ensemble * e);
+PAWSIM_API void pawsim_gpu_ensemble_destroy (pawsim_gpu_ensemble * e);
+
 /* Online time averages (diagnostics.c:307-470, the savefreqAvg outputs). accumulate adds
  * avg_fac * dt times the current state to the running sums (call it after each step, with
  * avg_fac = 1, or 1 - (t - t_next_avg) / dt on the step that crosses the window's end, as

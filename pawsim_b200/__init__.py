@@ -70,6 +70,8 @@ EXPORTS = (
     "pawsim_gpu_init", "pawsim_gpu_tendency_eval", "pawsim_gpu_integrator_step",
     "pawsim_gpu_pressure_correct", "pawsim_gpu_prelim", "pawsim_gpu_step", "pawsim_gpu_run",
     "pawsim_gpu_run_iterations",
+    "pawsim_gpu_ensemble_create", "pawsim_gpu_ensemble_run", "pawsim_gpu_ensemble_kernel_ms",
+    "pawsim_gpu_ensemble_destroy",
     "pawsim_gpu_solve_mg", "pawsim_gpu_set_stream", "pawsim_gpu_synchronize",
     "pawsim_gpu_time", "pawsim_gpu_launch_count", "pawsim_gpu_last_error",
     "pawsim_nn_conv3x3", "pawsim_nn_conv3x3_wgrad", "pawsim_nn_flip_weights",
@@ -109,6 +111,12 @@ def load_library(path: str = LIB_PATH):
     lib.pawsim_gpu_run.argtypes = [P, ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(GpuStats)]
     lib.pawsim_gpu_run_iterations.argtypes = [P, ctypes.POINTER(ctypes.c_int), ctypes.c_size_t]
     lib.pawsim_gpu_solve_mg.argtypes = [P, ctypes.POINTER(GpuStats)]
+    lib.pawsim_gpu_ensemble_create.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.POINTER(P)]
+    lib.pawsim_gpu_ensemble_run.argtypes = [P, ctypes.c_uint, ctypes.c_uint]
+    lib.pawsim_gpu_ensemble_kernel_ms.argtypes = [P]
+    lib.pawsim_gpu_ensemble_kernel_ms.restype = ctypes.c_double
+    lib.pawsim_gpu_ensemble_destroy.argtypes = [P]
+    lib.pawsim_gpu_ensemble_destroy.restype = None
     lib.pawsim_gpu_accumulate_averages.argtypes = [P, ctypes.c_double]
     lib.pawsim_gpu_scale_averages.argtypes = [P, ctypes.c_double]
     lib.pawsim_gpu_zero_averages.argtypes = [P]
@@ -406,6 +414,41 @@ class Model:
 
     def launch_count(self) -> int:
         return self.lib.pawsim_gpu_launch_count(self._h)
+
+
+class Ensemble:
+    """Several Models advanced together: per step one fused-kernel launch over all members'
+    tiles, then each member's rigid-lid correction on its own stream (no host synchronisation
+    until the end of a run). Members keep their own state, diagnostics and run report."""
+
+    def __init__(self, members):
+        self.lib = load_library()
+        self.members = list(members)
+        arr = (ctypes.c_void_p * len(self.members))(*[m._h.value for m in self.members])
+        h = ctypes.c_void_p()
+        _check(self.lib.pawsim_gpu_ensemble_create(arr, len(self.members), ctypes.byref(h)))
+        self._h = h
+
+    def run(self, n0: int, nsteps: int) -> None:
+        _check(self.lib.pawsim_gpu_ensemble_run(self._h, n0, nsteps))
+        for m in self.members:
+            m._last_run = nsteps
+
+    def kernel_ms(self) -> float:
+        """Mean device time of one step's batched fused-kernel launch in the last run."""
+        return float(self.lib.pawsim_gpu_ensemble_kernel_ms(self._h))
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self.lib.pawsim_gpu_ensemble_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Net:

@@ -16,6 +16,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpawsim_b200.so")
+OBJDIR = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC,-O3",
@@ -67,11 +68,16 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
     deps.append(os.path.join(os.path.dirname(HERE), "include", "pawsim_b200.h"))
     if not force and not _stale(LIB, deps):
         return LIB
+    # objects are kept in _build/ and a unit recompiles only when its source, a header or the
+    # build flags changed since its object was written (every header counts for every unit)
+    os.makedirs(OBJDIR, exist_ok=True)
+    headers = [d for d in deps if not d.endswith(".cu")] + [os.path.abspath(__file__)]
     cmds, objs = [], []
     for name, src, extra in UNITS:
-        o = os.path.join(CSRC, name + ".o")
-        cmds.append([NVCC, *ARCH, *FLAGS, *extra, "-c", os.path.join(CSRC, src), "-o", o])
+        o = os.path.join(OBJDIR, name + ".o")
         objs.append(o)
+        if force or _stale(o, [os.path.join(CSRC, src), *headers]):
+            cmds.append([NVCC, *ARCH, *FLAGS, *extra, "-c", os.path.join(CSRC, src), "-o", o])
     # translation units compile in parallel (the tendency kernels dominate the build time)
     procs = []
     for cmd in cmds:
@@ -80,13 +86,14 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
         procs.append(subprocess.Popen(cmd))
     failed = [c for c, p in zip(cmds, procs) if p.wait() != 0]
     if failed:
+        for c in failed:   # no half-written object may look up to date next time
+            if os.path.exists(c[-1]):
+                os.remove(c[-1])
         raise subprocess.CalledProcessError(1, failed[0])
     cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
-    for o in objs:
-        os.remove(o)
     return LIB
 
 

@@ -630,8 +630,9 @@ static int tendency_eval(Model* m) {
   return 0;
 }
 
-static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
-  if (!m->ready) return fail(PAWSIM_GPU_EBADCONFIG, "pawsim_gpu_init must follow the uploads");
+// The fused kernel's parameters of integrator step n (AB coefficients of integrator.c:138-198
+// with the AB3 start-up, history slots, output buffers); *shift: the step stores its tendency.
+static TendParams step_params(Model* m, unsigned n, bool fuse_fix, bool* shift_out) {
   const pawsim_gpu_config& c = m->c;
   TendParams p = base_params(m);
   double dt = c.dt;
@@ -657,6 +658,32 @@ static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
     p.dt = dt;
     p.bud_u = m->bud[0]; p.bud_v = m->bud[1]; p.bud_h = m->bud[2]; p.bud_e = m->bud[3]; p.bud_b = m->bud[4];
   }
+  *shift_out = shift;
+  return p;
+}
+
+// The model's bookkeeping after the launches of integrator step (history rotation, state
+// buffers, time).
+static void step_finish(Model* m, const TendParams& p, bool shift) {
+  if (shift) {   // newest <- the buffer just written, the previous newest moves back one slot
+    const int h1 = m->h1, h2 = m->h2, h3 = m->h3;
+    m->h1 = h3;
+    m->h2 = h1;
+    m->h3 = h2;
+  }
+  m->cur = 1 - m->cur;
+  m->prev_h = true;
+  m->t += m->c.dt;
+  m->thickness_fixed = p.fuse_thickness_fix != 0;
+}
+
+static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
+  if (!m->ready) return fail(PAWSIM_GPU_EBADCONFIG, "pawsim_gpu_init must follow the uploads");
+  const pawsim_gpu_config& c = m->c;
+  bool shift = true;
+  const TendParams p = step_params(m, n, fuse_fix, &shift);
+  const double dt = c.dt;
+  const int h1 = m->h1, h2 = m->h2, h3 = m->h3, nb = 1 - m->cur;
   const int nl = launch_step_kernel(m, p);
   if (nl < 0) return fail(PAWSIM_GPU_EUNSUPPORTED, "scheme combination not available");
   g_launches += nl;   // the drag pre-pass, the fused kernel and its exact pass
@@ -685,15 +712,7 @@ static int integrator_step(Model* m, unsigned n, bool fuse_fix) {
   }
   corner_fill(m, m->cur);   // the tendency's load_state and face thickness (state of the step start)
   PAWSIM_CUDA_OK(cudaGetLastError());
-  if (shift) {   // newest <- the buffer just written, the previous newest moves back one slot
-    m->h1 = h3;
-    m->h2 = h1;
-    m->h3 = h2;
-  }
-  m->cur = nb;
-  m->prev_h = true;
-  m->t += dt;
-  m->thickness_fixed = p.fuse_thickness_fix != 0;
+  step_finish(m, p, shift);
   return 0;
 }
 
@@ -821,6 +840,18 @@ static int pressure_correct(Model* m, int update_diags, pawsim_gpu_stats* st) {
   return iters;
 }
 
+// the device ring of per-step solve reports holds at least nsteps entries
+static bool ensure_run_ring(Model* m, unsigned nsteps) {
+  if ((int)nsteps <= m->run_cap) return true;
+  int* ri = m->alloc<int>(nsteps);
+  double* rm = m->alloc<double>(nsteps);
+  if (!ri || !rm) return false;
+  m->run_iters = ri;
+  m->run_meas = rm;
+  m->run_cap = (int)nsteps;
+  return true;
+}
+
 // Can the rigid-lid correction run without a host synchronisation? (no report the host must
 // form: pressure timing, warm start, the distributed multigrid's host loop, full multigrid)
 static bool async_correct_ok(const Model* m) {
@@ -877,6 +908,206 @@ static int pressure_correct_async(Model* m, int q) {
   ++g_launches;
   PAWSIM_CUDA_OK(cudaGetLastError());
   return 0;
+}
+
+// A batched ensemble of models (no reference counterpart: the reference runs one model per
+// process, its multigrid state being file-scope globals, multigrid.c:54-63). Each step the
+// fused kernel of every member runs in one launch over a work-list of all members' tiles,
+// then each member's rigid-lid correction on its own stream; no host synchronisation.
+struct Ensemble {
+  std::vector<Model*> mem;
+  std::vector<cudaStream_t> old_streams, streams;
+  std::vector<cudaEvent_t> ev_p;
+  cudaStream_t s0 = nullptr;
+  cudaEvent_t ev_t = nullptr;
+  TendParams* d_params = nullptr;
+  TendParams* h_params = nullptr;   // page-locked ring of kRing launches' parameters
+  std::vector<cudaEvent_t> ev_ring;
+  std::vector<cudaEvent_t> ev_k;   // timing pairs around each step's batched launch
+  double kernel_ms = 0;            // mean device time of the batched launch in the last run
+  int* d_work = nullptr;
+  int* d_done = nullptr;
+  int nwork = 0;
+  int ring = 0;
+  static constexpr int kRing = 4;
+  ~Ensemble() {
+    if (s0) cudaStreamSynchronize(s0);
+    for (size_t i = 0; i < mem.size() && i < old_streams.size(); ++i) {
+      cudaStreamSynchronize(streams[i]);
+      mem[i]->s = old_streams[i];
+      if (mem[i]->mg) mem[i]->mg->set_stream(old_streams[i]);
+      if (mem[i]->dmg) mem[i]->dmg->set_stream(old_streams[i]);
+    }
+    for (cudaStream_t q : streams) cudaStreamDestroy(q);
+    for (cudaEvent_t e : ev_p) cudaEventDestroy(e);
+    for (cudaEvent_t e : ev_ring) cudaEventDestroy(e);
+    for (cudaEvent_t e : ev_k) cudaEventDestroy(e);
+    if (ev_t) cudaEventDestroy(ev_t);
+    if (s0) cudaStreamDestroy(s0);
+    cudaFree(d_params);
+    cudaFree(d_work);
+    cudaFree(d_done);
+    if (h_params) cudaFreeHost(h_params);
+  }
+};
+
+static int ensemble_create(Model* const* ms, int n, Ensemble** out) {
+  if (n < 1) return fail(PAWSIM_GPU_EBADCONFIG, "an ensemble needs at least one member");
+  const pawsim_gpu_config& c0 = ms[0]->c;
+  for (int i = 0; i < n; ++i) {
+    const Model* m = ms[i];
+    const pawsim_gpu_config& c = m->c;
+    if (!m->ready) return fail(PAWSIM_GPU_EBADCONFIG, "ensemble members must be initialised");
+    if (c.Nlay != c0.Nlay || c.mom_scheme != c0.mom_scheme || c.thick_scheme != c0.thick_scheme ||
+        c.use_rl != c0.use_rl)
+      return fail(PAWSIM_GPU_EUNSUPPORTED, "ensemble members must share Nlay, the schemes and the rigid lid");
+    const bool fraction_drag = base_params(ms[i]).drag_bot || base_params(ms[i]).drag_surf;
+    if (c.use_tracer || c.use_buoyancy || c.budgets || fraction_drag || m->bud[0] || m->bud[1] || m->bud[2] || m->bud[3] || m->bud[4])
+      return fail(PAWSIM_GPU_EUNSUPPORTED, "ensemble members without tracer, budgets or fraction-depth drag");
+    for (int j = 0; j < i; ++j)
+      if (ms[j] == m) return fail(PAWSIM_GPU_EBADCONFIG, "a model appears twice in the ensemble");
+  }
+  // every member must take the same kernel instantiation and shared-memory size
+  const TendParams p0 = base_params(ms[0]);
+  const int ty = tendency_tile_height(p0, c0.thick_scheme);
+  for (int i = 1; i < n; ++i) {
+    const TendParams pi = base_params(ms[i]);
+    if (tendency_tile_height(pi, c0.thick_scheme) != ty || (pi.use_wdia != 0) != (p0.use_wdia != 0) ||
+        pi.use_smag != p0.use_smag || (pi.use_fractions != 0) != (p0.use_fractions != 0) ||
+        (pi.useA4 != 0) != (p0.useA4 != 0) || (pi.corners != nullptr) != (p0.corners != nullptr))
+      return fail(PAWSIM_GPU_EUNSUPPORTED, "ensemble members must share the tendency kernel's feature set");
+  }
+  Ensemble* e = new Ensemble();
+  e->mem.assign(ms, ms + n);
+  std::vector<int> work;
+  for (int i = 0; i < n; ++i) {
+    const int tiles = ((ms[i]->Nx + 31) / 32) * ((ms[i]->Ny + ty - 1) / ty);
+    if (tiles > 0xfffff || i > 2047) {
+      delete e;
+      return fail(PAWSIM_GPU_EUNSUPPORTED, "ensemble too large for the work-list encoding");
+    }
+    for (int t = 0; t < tiles; ++t) work.push_back(i << 20 | t);
+  }
+  e->nwork = (int)work.size();
+  bool ok = cudaStreamCreateWithFlags(&e->s0, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&e->ev_t, cudaEventDisableTiming) == cudaSuccess &&
+            cudaMalloc(&e->d_params, n * sizeof(TendParams)) == cudaSuccess &&
+            cudaMallocHost(&e->h_params, (size_t)Ensemble::kRing * n * sizeof(TendParams)) == cudaSuccess &&
+            cudaMalloc(&e->d_work, work.size() * sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&e->d_done, sizeof(int)) == cudaSuccess &&
+            cudaMemset(e->d_done, 0, sizeof(int)) == cudaSuccess &&
+            cudaMemcpy(e->d_work, work.data(), work.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
+  for (int q = 0; ok && q < Ensemble::kRing; ++q) {
+    cudaEvent_t ev;
+    ok = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess;
+    if (ok) e->ev_ring.push_back(ev);
+  }
+  for (int i = 0; ok && i < n; ++i) {
+    cudaStream_t q;
+    cudaEvent_t ev;
+    ok = cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) break;
+    PAWSIM_CUDA_OK(cudaStreamSynchronize(ms[i]->s));
+    e->streams.push_back(q);
+    e->ev_p.push_back(ev);
+    e->old_streams.push_back(ms[i]->s);
+    ms[i]->s = q;
+    if (ms[i]->mg) ms[i]->mg->set_stream(q);
+    if (ms[i]->dmg) ms[i]->dmg->set_stream(q);
+  }
+  if (!ok) {
+    delete e;
+    return fail(PAWSIM_GPU_ECUDA, "ensemble set-up failed");
+  }
+  *out = e;
+  return 0;
+}
+
+static int ensemble_run(Ensemble* e, unsigned n0, unsigned nsteps) {
+  const int n = (int)e->mem.size();
+  for (Model* m : e->mem) {
+    m->last_run_iters.assign(nsteps, 0);
+    if (!ensure_run_ring(m, nsteps)) return fail(PAWSIM_GPU_ECUDA, "run report allocation failed");
+  }
+  while (e->ev_k.size() < 2 * (size_t)nsteps) {
+    cudaEvent_t ev;
+    PAWSIM_CUDA_OK(cudaEventCreate(&ev));
+    e->ev_k.push_back(ev);
+  }
+  std::vector<std::vector<char>> async(n, std::vector<char>(nsteps, 0));
+  std::vector<TendParams> p(n);
+  std::vector<char> shift(n);
+  for (unsigned q = 0; q < nsteps; ++q) {
+    const unsigned step = n0 + q;
+    // phase 1: the fused kernels of all members in one launch, after their last corrections
+    for (int i = 0; i < n; ++i) PAWSIM_CUDA_OK(cudaStreamWaitEvent(e->s0, e->ev_p[i], 0));
+    const int r = e->ring;
+    e->ring = (e->ring + 1) % Ensemble::kRing;
+    PAWSIM_CUDA_OK(cudaEventSynchronize(e->ev_ring[r]));   // that slot's earlier copy is done
+    TendParams* hp = e->h_params + (size_t)r * n;
+    for (int i = 0; i < n; ++i) {
+      bool sh = true;
+      p[i] = step_params(e->mem[i], step, true, &sh);
+      shift[i] = sh;
+      hp[i] = p[i];
+    }
+    PAWSIM_CUDA_OK(cudaMemcpyAsync(e->d_params, hp, n * sizeof(TendParams), cudaMemcpyHostToDevice, e->s0));
+    PAWSIM_CUDA_OK(cudaEventRecord(e->ev_ring[r], e->s0));
+    PAWSIM_CUDA_OK(cudaEventRecord(e->ev_k[2 * q], e->s0));
+    const int nl = launch_tendency_batch(p[0], e->d_params, e->d_work, e->nwork, n, e->d_done,
+                                         e->mem[0]->c.mom_scheme, e->mem[0]->c.thick_scheme, e->s0);
+    if (nl < 0) return fail(PAWSIM_GPU_EUNSUPPORTED, "batched tendency launch not available");
+    g_launches += nl;
+    PAWSIM_CUDA_OK(cudaEventRecord(e->ev_k[2 * q + 1], e->s0));
+    PAWSIM_CUDA_OK(cudaEventRecord(e->ev_t, e->s0));
+    // phase 2: each member's corner shadow (state of the step start, read-only for the batched
+    // kernel), bookkeeping and rigid-lid correction on its own stream
+    for (int i = 0; i < n; ++i) {
+      Model* m = e->mem[i];
+      corner_fill(m, m->cur);
+      PAWSIM_CUDA_OK(cudaStreamWaitEvent(m->s, e->ev_t, 0));
+      step_finish(m, p[i], shift[i] != 0);
+      if (async_correct_ok(m)) {
+        int rc = pressure_correct_async(m, (int)q);
+        if (rc) return rc;
+        async[i][q] = 1;
+      } else {
+        pawsim_gpu_stats st;
+        const int it = pressure_correct(m, 1, &st);
+        if (it < 0) return it;
+        m->last_run_iters[q] = it;
+      }
+      PAWSIM_CUDA_OK(cudaEventRecord(e->ev_p[i], m->s));
+    }
+  }
+  // the reports of the run, read once; the failure options as pawsim_gpu_run applies them
+  int r = 0;
+  for (int i = 0; i < n; ++i) {
+    Model* m = e->mem[i];
+    std::vector<int> it(nsteps);
+    PAWSIM_CUDA_OK(cudaMemcpyAsync(it.data(), m->run_iters, nsteps * sizeof(int), cudaMemcpyDeviceToHost, m->s));
+    PAWSIM_CUDA_OK(cudaStreamSynchronize(m->s));
+    for (unsigned q = 0; q < nsteps; ++q) {
+      if (!async[i][q]) continue;
+      m->last_run_iters[q] = it[q];
+      if (m->c.use_rl && m->c.solver == PAWSIM_GPU_SOLVER_MG) g_launches += (long long)it[q] * m->mg->body_launches();
+    }
+    for (unsigned q = 0; q < nsteps && !r; ++q) r = check_converged(m, m->last_run_iters[q]);
+    if (!r && m->nonfinite) {
+      m->nf_calls = m->c.check_nonfinite - 1;
+      r = check_state_finite(m);
+    }
+  }
+  PAWSIM_CUDA_OK(cudaStreamSynchronize(e->s0));
+  double tot = 0;
+  for (unsigned q = 0; q < nsteps; ++q) {
+    float ms = 0;
+    PAWSIM_CUDA_OK(cudaEventElapsedTime(&ms, e->ev_k[2 * q], e->ev_k[2 * q + 1]));
+    tot += ms;
+  }
+  e->kernel_ms = nsteps ? tot / nsteps : 0;
+  return r;
 }
 
 }  // namespace pawsim
@@ -970,14 +1201,7 @@ int pawsim_gpu_run(pawsim_gpu* h, unsigned n0, unsigned nsteps, pawsim_gpu_stats
   Model* m = h->m;
   m->last_run_iters.assign(nsteps, 0);
   if (nsteps == 0) return 0;
-  if ((int)nsteps > m->run_cap) {
-    int* ri = m->alloc<int>(nsteps);
-    double* rm = m->alloc<double>(nsteps);
-    if (!ri || !rm) return fail(PAWSIM_GPU_ECUDA, "run report allocation failed");
-    m->run_iters = ri;
-    m->run_meas = rm;
-    m->run_cap = (int)nsteps;
-  }
+  if (!ensure_run_ring(m, nsteps)) return fail(PAWSIM_GPU_ECUDA, "run report allocation failed");
   // steps whose correction needs the host run synchronously (the first solves tune the
   // multigrid and build its graph); the others are enqueued back to back and their reports
   // read once at the end
@@ -1022,6 +1246,39 @@ int pawsim_gpu_run(pawsim_gpu* h, unsigned n0, unsigned nsteps, pawsim_gpu_stats
     if (rf) return rf;
   }
   return r;
+}
+
+struct pawsim_gpu_ensemble {
+  Ensemble* e;
+};
+
+int pawsim_gpu_ensemble_create(pawsim_gpu* const* members, int n, pawsim_gpu_ensemble** out) {
+  if (!members || !out || n < 1) return fail(PAWSIM_GPU_EBADCONFIG, "null argument");
+  std::vector<Model*> ms(n);
+  for (int i = 0; i < n; ++i) {
+    if (!members[i]) return fail(PAWSIM_GPU_EBADCONFIG, "null member");
+    ms[i] = members[i]->m;
+  }
+  Ensemble* e = nullptr;
+  int r = ensemble_create(ms.data(), n, &e);
+  if (r) return r;
+  *out = new pawsim_gpu_ensemble{e};
+  return 0;
+}
+
+int pawsim_gpu_ensemble_run(pawsim_gpu_ensemble* h, unsigned n0, unsigned nsteps) {
+  if (!h) return PAWSIM_GPU_EBADCONFIG;
+  return ensemble_run(h->e, n0, nsteps);
+}
+
+double pawsim_gpu_ensemble_kernel_ms(const pawsim_gpu_ensemble* h) {
+  return h ? h->e->kernel_ms : 0;
+}
+
+void pawsim_gpu_ensemble_destroy(pawsim_gpu_ensemble* h) {
+  if (!h) return;
+  delete h->e;
+  delete h;
 }
 
 int pawsim_gpu_run_iterations(pawsim_gpu* h, int* iters, size_t n) {

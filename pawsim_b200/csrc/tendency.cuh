@@ -104,6 +104,15 @@ __device__ inline void budget_add(double* fam, int term, int k, int L, size_t ls
 // returns the number of kernels launched, or -1 when the combination is not available
 int launch_tendency(const TendParams& p, int momentum_scheme, int thickness_scheme,
                     cudaStream_t stream);
+// tile height (16 or 8 rows) launch_tendency uses for this set-up
+int tendency_tile_height(const TendParams& p, int thickness_scheme);
+// The fused step of several members in one launch (ensemble): ps (device) holds each member's
+// parameters, work (device) the (member << 20 | tile) pairs of nwork tiles, on the tile height
+// tendency_tile_height gives; the members share p0's momentum and thickness schemes, feature
+// set and layer count. Then the exact pass over every member's tile list (done: a device int,
+// zero between launches). Returns the kernels launched, or -1.
+int launch_tendency_batch(const TendParams& p0, const TendParams* ps, const int* work, int nwork, int members,
+                          int* done, int momentum_scheme, int thickness_scheme, cudaStream_t stream);
 // the same step with every enabled budget family accumulated and the buoyancy coupling
 // (32 x 8 tiles)
 int launch_tendency_budget(const TendParams& p, int momentum_scheme, int thickness_scheme,

@@ -1254,6 +1254,57 @@ __global__ void __launch_bounds__(NT, PAWSIM_TEND_MINB) tendency_exact_kernel(co
   }
 }
 
+// Batched ensemble: one launch over a work-list of (member, tile) pairs, member << 20 | tile,
+// with each member's parameters staged in shared memory. Every tile computes exactly what
+// the member's own launch computes.
+template <int MS, int TS, int H, bool LEAN>
+__global__ void __launch_bounds__(NT, PAWSIM_TEND_MINB)
+tendency_batch_kernel(const TendParams* __restrict__ ps, const int* __restrict__ work) {
+  __shared__ TendParams sp;
+  const int w = work[blockIdx.x];
+  const int member = w >> 20, tile = w & 0xfffff;
+  for (int q = threadIdx.x; q < (int)(sizeof(TendParams) / sizeof(int)); q += NT)
+    reinterpret_cast<int*>(&sp)[q] = reinterpret_cast<const int*>(ps + member)[q];
+  __syncthreads();
+  const int gx = (sp.Nx + TX - 1) / TX;
+  tendency_tile<MS, TS, H, LEAN, false>(sp, tile % gx, tile / gx);
+}
+
+// the exact pass of every member's tile list (see tendency_exact_kernel); the last CTA empties
+// all lists
+template <int MS, int TS, int H>
+__global__ void __launch_bounds__(NT, PAWSIM_TEND_MINB)
+tendency_batch_exact_kernel(const TendParams* __restrict__ ps, int members, int* done) {
+  __shared__ TendParams sp;
+  for (int mb = 0; mb < members; ++mb) {
+    for (int q = threadIdx.x; q < (int)(sizeof(TendParams) / sizeof(int)); q += NT)
+      reinterpret_cast<int*>(&sp)[q] = reinterpret_cast<const int*>(ps + mb)[q];
+    __syncthreads();
+    const int n = sp.tile_list[0];
+    const int gx = (sp.Nx + TX - 1) / TX;
+    for (int e = blockIdx.x; e < n; e += gridDim.x) {
+      const int id = sp.tile_list[2 + e];
+      tendency_tile<MS, TS, H, false, true>(sp, id % gx, id / gx);
+      __syncthreads();
+    }
+    __syncthreads();
+  }
+  __shared__ int last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(done, 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last) {
+    for (int mb = threadIdx.x; mb < members; mb += NT) {
+      ps[mb].tile_list[0] = 0;
+      ps[mb].tile_list[1] = 0;
+    }
+    if (threadIdx.x == 0) *done = 0;
+    __threadfence();
+  }
+}
+
 template <int H>
 size_t smem_bytes(const TendParams& p) {
   constexpr int RN = Geo<H>::RN;
@@ -1305,6 +1356,32 @@ int launch_t(const TendParams& p, cudaStream_t s) {
   }
 }
 
+// the batched launch for members sharing p0's scheme, halo, feature set and layer count
+template <int MS, int TS, int H>
+int launch_batch_t(const TendParams& p0, const TendParams* ps, const int* work, int nwork, int members, int* done,
+                   cudaStream_t s) {
+  if constexpr (BUD) {
+    return -1;
+  } else {
+    const size_t shm = smem_bytes<H>(p0);
+    if (shm > 200 * 1024 || p0.drag_bot || p0.drag_surf) return -1;
+    static bool attr_done = false;
+    if (!attr_done) {
+      cudaFuncSetAttribute(tendency_batch_kernel<MS, TS, H, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           200 * 1024);
+      cudaFuncSetAttribute(tendency_batch_kernel<MS, TS, H, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           200 * 1024);
+      cudaFuncSetAttribute(tendency_batch_exact_kernel<MS, TS, H>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           200 * 1024);
+      attr_done = true;
+    }
+    if (lean_params(p0)) tendency_batch_kernel<MS, TS, H, true><<<nwork, NT, shm, s>>>(ps, work);
+    else tendency_batch_kernel<MS, TS, H, false><<<nwork, NT, shm, s>>>(ps, work);
+    tendency_batch_exact_kernel<MS, TS, H><<<EXACT_CTAS, NT, shm, s>>>(ps, members, done);
+    return 2;
+  }
+}
+
 template <int TS, int H>
 int launch_ms(const TendParams& p, int ms, cudaStream_t s) {
 #ifdef PAWSIM_TEND_MS
@@ -1342,6 +1419,30 @@ inline bool wide_halo(const TendParams& p, int ts) { return ts >= 2 || (p.use_sm
 #if PAWSIM_TEND_BUD || PAWSIM_TEND_MS == 0
 size_t PAWSIM_TEND_SMEM_FN(const TendParams& p, int ts) {
   return wide_halo(p, ts) ? smem_bytes<3>(p) : smem_bytes<2>(p);
+}
+#endif
+
+#if !PAWSIM_TEND_BUD
+// batched ensemble launch (tendency.cu dispatches on the momentum scheme and tile height)
+int PAWSIM_TEND_CAT(batch_, PAWSIM_TEND_LAUNCH_FN)(const TendParams& p0, const TendParams* ps, const int* work,
+                                                    int nwork, int members, int* done, int ms, int ts,
+                                                    cudaStream_t s) {
+#ifdef PAWSIM_TEND_MS
+  if (ms != PAWSIM_TEND_MS) return -1;
+#endif
+  if (p0.L < 1 || p0.L > LMAX) return -1;
+  if (!wide_halo(p0, ts)) {
+    if (ts == 0) return launch_batch_t<PAWSIM_TEND_MS, 0, 2>(p0, ps, work, nwork, members, done, s);
+    if (ts == 1) return launch_batch_t<PAWSIM_TEND_MS, 1, 2>(p0, ps, work, nwork, members, done, s);
+    return -1;
+  }
+  switch (ts) {
+    case 0: return launch_batch_t<PAWSIM_TEND_MS, 0, 3>(p0, ps, work, nwork, members, done, s);
+    case 1: return launch_batch_t<PAWSIM_TEND_MS, 1, 3>(p0, ps, work, nwork, members, done, s);
+    case 2: return launch_batch_t<PAWSIM_TEND_MS, 2, 3>(p0, ps, work, nwork, members, done, s);
+    case 3: return launch_batch_t<PAWSIM_TEND_MS, 3, 3>(p0, ps, work, nwork, members, done, s);
+  }
+  return -1;
 }
 #endif
 
