@@ -30,6 +30,11 @@ import time
 
 import numpy as np
 
+# the ensemble sub-line runs 81 streams; more hardware work queues than the default 8 keep
+# unrelated members' kernels from queueing behind one another (read when the CUDA context is
+# created, so it is set before torch or the library touch the GPU)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -395,8 +400,15 @@ def ensemble_timing(steps, warmup, peak):
         t0 = time.perf_counter()
         ens.run(1 + warmup, steps)
         sec = time.perf_counter() - t0
-        k_ms = ens.kernel_ms()
+        graph_steps = ens.graph_steps()
         iters = np.concatenate([m.run_iterations() for m in members])
+        # the batched launch's device time, from a few stream-mode steps after the timed run
+        ens.set_graphs(False)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ens.run(1 + warmup + steps, 10)
+        sec_streams = (time.perf_counter() - t0) / 10
+        k_ms = ens.kernel_ms()
         ens.close()
         for m in members:
             m.close()
@@ -413,6 +425,8 @@ def ensemble_timing(steps, warmup, peak):
         "gpl_updates_per_s": steps * cells * L / sec,
         "vcycles_per_step": float(np.mean(iters)),
         "same_vcycles_as_alone": bool(np.array_equal(iters, iters_alone)),
+        "graph_steps": graph_steps,
+        "stream_mode_ms_per_step": sec_streams * 1e3,
         "alone_ms_per_step": sec_alone / steps * 1e3,
         "speedup_vs_members_alone": sec_alone / sec,
         "timing": "host clock around synchronised runs; inputs (80 x 2 x 3 state planes) above L2",

@@ -207,8 +207,15 @@ typedef struct pawsim_gpu_ensemble pawsim_gpu_ensemble;
 PAWSIM_API int pawsim_gpu_ensemble_create (pawsim_gpu * const * members, int n, pawsim_gpu_ensemble ** out);
 PAWSIM_API int pawsim_gpu_ensemble_run (pawsim_gpu_ensemble * e, unsigned n0, unsigned nsteps);
 /* Mean device time (ms) of one step's batched fused-kernel launch (with its exact pass) over
- * the last run, from CUDA events on the ensemble's launch stream. */
+ * the stream-mode steps of the last run, from CUDA events on the ensemble's launch stream
+ * (0 when every step replayed a graph). */
 PAWSIM_API double pawsim_gpu_ensemble_kernel_ms (const pawsim_gpu_ensemble * e);
+/* Steps whose every member has a fixed form (AB3 with its history shifting, the multigrid
+ * loop built, no host-side warm start) run as replays of CUDA graphs that capture the whole
+ * step, one per arrangement of the members' state buffers; on = 0 keeps every step on streams.
+ * Results are identical either way. graph_steps: how many steps of the last run replayed. */
+PAWSIM_API int pawsim_gpu_ensemble_set_graphs (pawsim_gpu_ensemble * e, int on);
+PAWSIM_API int pawsim_gpu_ensemble_graph_steps (const pawsim_gpu_ensemble * e);
 PAWSIM_API void pawsim_gpu_ensemble_destroy (pawsim_gpu_ensemble * e);
 
 /* Online time averages (diagnostics.c:307-470, the savefreqAvg outputs). accumulate adds

@@ -864,9 +864,13 @@ static bool async_correct_ok(const Model* m) {
 }
 
 // The rigid-lid correction of pressure_correct without a host synchronisation; the solve's
-// iteration count and stopping measure go to the run ring's slot q.
-static int pressure_correct_async(Model* m, int q) {
-  if (!m->c.use_rl) return 0;
+// iteration count and stopping measure go to the device slots it_out / meas_out (0 without
+// the rigid lid).
+static int pressure_correct_async(Model* m, int* it_out, double* meas_out) {
+  if (!m->c.use_rl) {
+    PAWSIM_CUDA_OK(cudaMemsetAsync(it_out, 0, sizeof(int), m->s));
+    return 0;
+  }
   const int cur = m->cur;
   Grid2 g = m->grid2();
   dim3 b(32, 8), gr((m->Nx + 31) / 32, (m->Ny + 7) / 8);
@@ -887,7 +891,7 @@ static int pressure_correct_async(Model* m, int q) {
     launch_sum(m->pi, m->Nx, m->Ny, m->pitch, m->serial(), m->scratch, m->dsum, m->s);
     launch_subtract_mean(m->pi, m->Nx, m->Ny, m->pitch, m->dsum, m->s);
     g_launches += m->serial() ? 2 : 3;
-    PAWSIM_CUDA_OK(cudaMemcpyAsync(m->run_iters + q, m->diters, sizeof(int), cudaMemcpyDeviceToDevice, m->s));
+    PAWSIM_CUDA_OK(cudaMemcpyAsync(it_out, m->diters, sizeof(int), cudaMemcpyDeviceToDevice, m->s));
   } else {
     if (m->c.pi_guess == 1) {
       if (m->pi_solves >= 2) {
@@ -900,7 +904,7 @@ static int pressure_correct_async(Model* m, int q) {
       ++m->pi_solves;
     }
     long long nl = 0;
-    if (m->mg->solve_async(m->pi, m->rhs, m->c.pi_tol, m->c.maxiters, m->run_iters + q, m->run_meas + q, &nl) != 0)
+    if (m->mg->solve_async(m->pi, m->rhs, m->c.pi_tol, m->c.maxiters, it_out, meas_out, &nl) != 0)
       return fail(PAWSIM_GPU_ECUDA, "asynchronous multigrid solve failed");
     g_launches += nl;
   }
@@ -913,7 +917,27 @@ static int pressure_correct_async(Model* m, int q) {
 // A batched ensemble of models (no reference counterpart: the reference runs one model per
 // process, its multigrid state being file-scope globals, multigrid.c:54-63). Each step the
 // fused kernel of every member runs in one launch over a work-list of all members' tiles,
-// then each member's rigid-lid correction on its own stream; no host synchronisation.
+// then each member's rigid-lid correction on its own stream; no host synchronisation. Once
+// every member's step has a fixed form (AB3 history shifting, the multigrid loop built), the
+// whole step -- the batched launch, and per member the correction with its V-cycle loop as a
+// conditional node -- is captured into one CUDA graph per arrangement of the members' state
+// buffers (they rotate with period 6) and replayed with one launch per step.
+struct EnsGraph {
+  std::vector<int> key;               // per member: cur, h1, h2, h3, corner_cur
+  cudaGraphExec_t exec = nullptr;
+  TendParams* d_params = nullptr;     // the parameter blocks the graph's batched launch reads
+  std::vector<TendParams> h_params;   // what d_params holds
+  long long launches = 0;             // kernels per replay outside the V-cycle bodies
+};
+
+__global__ void ring_push_kernel(const int* it, const double* meas, int* ring_it, double* ring_meas,
+                                 const int* pos) {
+  ring_it[*pos] = *it;
+  ring_meas[*pos] = *meas;
+}
+
+__global__ void set_int_kernel(int* p, int v) { *p = v; }
+
 struct Ensemble {
   std::vector<Model*> mem;
   std::vector<cudaStream_t> old_streams, streams;
@@ -923,13 +947,32 @@ struct Ensemble {
   TendParams* d_params = nullptr;
   TendParams* h_params = nullptr;   // page-locked ring of kRing launches' parameters
   std::vector<cudaEvent_t> ev_ring;
-  std::vector<cudaEvent_t> ev_k;   // timing pairs around each step's batched launch
-  double kernel_ms = 0;            // mean device time of the batched launch in the last run
+  std::vector<cudaEvent_t> ev_k;   // timing pairs around each stream-mode step's batched launch
+  double kernel_ms = 0;            // mean device time of the batched launch (stream-mode steps)
   int* d_work = nullptr;
   int* d_done = nullptr;
   int nwork = 0;
   int ring = 0;
   static constexpr int kRing = 4;
+  // captured steps
+  bool use_graphs = true;
+  std::vector<EnsGraph> graphs;
+  std::vector<int*> graph_rings;   // the members' report rings the graphs write
+  int* d_pos = nullptr;            // ring index of the step a replay runs
+  int* d_slot_it = nullptr;        // per member: the captured solve's report slot
+  double* d_slot_meas = nullptr;
+  int graph_steps = 0;             // steps of the last run that ran as graph replays
+  // fork and join events used only inside captures (an event last recorded in a capture may
+  // not be waited on outside it)
+  cudaEvent_t ev_cf = nullptr;
+  std::vector<cudaEvent_t> ev_cj;
+  void drop_graphs() {
+    for (EnsGraph& g : graphs) {
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+      cudaFree(g.d_params);
+    }
+    graphs.clear();
+  }
   ~Ensemble() {
     if (s0) cudaStreamSynchronize(s0);
     for (size_t i = 0; i < mem.size() && i < old_streams.size(); ++i) {
@@ -938,15 +981,21 @@ struct Ensemble {
       if (mem[i]->mg) mem[i]->mg->set_stream(old_streams[i]);
       if (mem[i]->dmg) mem[i]->dmg->set_stream(old_streams[i]);
     }
+    drop_graphs();
     for (cudaStream_t q : streams) cudaStreamDestroy(q);
     for (cudaEvent_t e : ev_p) cudaEventDestroy(e);
     for (cudaEvent_t e : ev_ring) cudaEventDestroy(e);
     for (cudaEvent_t e : ev_k) cudaEventDestroy(e);
+    for (cudaEvent_t e : ev_cj) cudaEventDestroy(e);
+    if (ev_cf) cudaEventDestroy(ev_cf);
     if (ev_t) cudaEventDestroy(ev_t);
     if (s0) cudaStreamDestroy(s0);
     cudaFree(d_params);
     cudaFree(d_work);
     cudaFree(d_done);
+    cudaFree(d_pos);
+    cudaFree(d_slot_it);
+    cudaFree(d_slot_meas);
     if (h_params) cudaFreeHost(h_params);
   }
 };
@@ -991,11 +1040,15 @@ static int ensemble_create(Model* const* ms, int n, Ensemble** out) {
   e->nwork = (int)work.size();
   bool ok = cudaStreamCreateWithFlags(&e->s0, cudaStreamNonBlocking) == cudaSuccess &&
             cudaEventCreateWithFlags(&e->ev_t, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&e->ev_cf, cudaEventDisableTiming) == cudaSuccess &&
             cudaMalloc(&e->d_params, n * sizeof(TendParams)) == cudaSuccess &&
             cudaMallocHost(&e->h_params, (size_t)Ensemble::kRing * n * sizeof(TendParams)) == cudaSuccess &&
             cudaMalloc(&e->d_work, work.size() * sizeof(int)) == cudaSuccess &&
             cudaMalloc(&e->d_done, sizeof(int)) == cudaSuccess &&
             cudaMemset(e->d_done, 0, sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&e->d_pos, sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&e->d_slot_it, n * sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&e->d_slot_meas, n * sizeof(double)) == cudaSuccess &&
             cudaMemcpy(e->d_work, work.data(), work.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
   for (int q = 0; ok && q < Ensemble::kRing; ++q) {
     cudaEvent_t ev;
@@ -1004,13 +1057,15 @@ static int ensemble_create(Model* const* ms, int n, Ensemble** out) {
   }
   for (int i = 0; ok && i < n; ++i) {
     cudaStream_t q;
-    cudaEvent_t ev;
+    cudaEvent_t ev, evj;
     ok = cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking) == cudaSuccess &&
-         cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess;
+         cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&evj, cudaEventDisableTiming) == cudaSuccess;
     if (!ok) break;
     PAWSIM_CUDA_OK(cudaStreamSynchronize(ms[i]->s));
     e->streams.push_back(q);
     e->ev_p.push_back(ev);
+    e->ev_cj.push_back(evj);
     e->old_streams.push_back(ms[i]->s);
     ms[i]->s = q;
     if (ms[i]->mg) ms[i]->mg->set_stream(q);
@@ -1024,11 +1079,76 @@ static int ensemble_create(Model* const* ms, int n, Ensemble** out) {
   return 0;
 }
 
+// Can member m's step run as part of a captured graph? (the history shifts, the correction
+// needs no host and its multigrid loop is built; SOR's cooperative launch stays on streams)
+static bool graph_step_ok(const Model* m, bool shift) {
+  if (!shift || !async_correct_ok(m)) return false;
+  if (!m->c.use_rl) return true;
+  return m->c.solver == PAWSIM_GPU_SOLVER_MG && (m->c.pi_guess != 1 || m->pi_solves >= 2);
+}
+
+// The host-side effects of one replayed step of member m: those the captured step's own
+// enqueue made (integrator bookkeeping, two corner fills, the correction's flags).
+static void replay_member(Model* m, const TendParams& p, bool shift) {
+  step_finish(m, p, shift);
+  m->thickness_fixed = false;
+  if (m->c.use_rl && m->c.solver == PAWSIM_GPU_SOLVER_MG && m->c.pi_guess == 1) ++m->pi_solves;
+}
+
+// One member's part of a step on its own stream, after the batched launch (event ev_t): corner
+// shadow of the step's start state, bookkeeping, correction with its report to (it, meas).
+static int member_step(Ensemble* e, int i, const TendParams& p, bool shift, int* it, double* meas, cudaEvent_t fork) {
+  Model* m = e->mem[i];
+  PAWSIM_CUDA_OK(cudaStreamWaitEvent(m->s, fork, 0));
+  corner_fill(m, m->cur);
+  step_finish(m, p, shift);
+  return pressure_correct_async(m, it, meas);
+}
+
+// Capture one step of every member into graph g (its parameter blocks already in g.d_params).
+static int ensemble_capture(Ensemble* e, EnsGraph& g, const std::vector<TendParams>& p,
+                            const std::vector<char>& shift) {
+  const int n = (int)e->mem.size();
+  const long long g0 = g_launches;
+  PAWSIM_CUDA_OK(cudaStreamBeginCapture(e->s0, cudaStreamCaptureModeRelaxed));
+  int rc = 0;
+  const int nl = launch_tendency_batch(p[0], g.d_params, e->d_work, e->nwork, n, e->d_done,
+                                       e->mem[0]->c.mom_scheme, e->mem[0]->c.thick_scheme, e->s0);
+  if (nl < 0) rc = fail(PAWSIM_GPU_EUNSUPPORTED, "batched tendency launch not available");
+  g_launches += nl > 0 ? nl : 0;
+  if (!rc && cudaEventRecord(e->ev_cf, e->s0) != cudaSuccess) rc = fail(PAWSIM_GPU_ECUDA, "event record failed");
+  for (int i = 0; i < n && !rc; ++i) {
+    Model* m = e->mem[i];
+    rc = member_step(e, i, p[i], shift[i] != 0, e->d_slot_it + i, e->d_slot_meas + i, e->ev_cf);
+    if (rc) break;
+    ring_push_kernel<<<1, 1, 0, m->s>>>(e->d_slot_it + i, e->d_slot_meas + i, m->run_iters, m->run_meas, e->d_pos);
+    ++g_launches;
+    if (cudaEventRecord(e->ev_cj[i], m->s) != cudaSuccess || cudaStreamWaitEvent(e->s0, e->ev_cj[i], 0) != cudaSuccess)
+      rc = fail(PAWSIM_GPU_ECUDA, "capture join failed");
+  }
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(e->s0, &graph);
+  if (!rc && ce != cudaSuccess) rc = fail(PAWSIM_GPU_ECUDA, "ensemble step capture failed");
+  if (!rc && cudaGraphInstantiate(&g.exec, graph, 0) != cudaSuccess) rc = fail(PAWSIM_GPU_ECUDA, "ensemble graph instantiation failed");
+  if (graph) cudaGraphDestroy(graph);
+  g.launches = g_launches - g0;
+  return rc;
+}
+
 static int ensemble_run(Ensemble* e, unsigned n0, unsigned nsteps) {
   const int n = (int)e->mem.size();
-  for (Model* m : e->mem) {
+  // the rings keep their size across runs so that captured graphs stay valid
+  std::vector<int*> rings(n);
+  for (int i = 0; i < n; ++i) {
+    Model* m = e->mem[i];
     m->last_run_iters.assign(nsteps, 0);
-    if (!ensure_run_ring(m, nsteps)) return fail(PAWSIM_GPU_ECUDA, "run report allocation failed");
+    if (!ensure_run_ring(m, nsteps > 1024u ? nsteps : 1024u)) return fail(PAWSIM_GPU_ECUDA, "run report allocation failed");
+    rings[i] = m->run_iters;
+  }
+  if (rings != e->graph_rings) {
+    PAWSIM_CUDA_OK(cudaStreamSynchronize(e->s0));
+    e->drop_graphs();
+    e->graph_rings = rings;
   }
   while (e->ev_k.size() < 2 * (size_t)nsteps) {
     cudaEvent_t ev;
@@ -1036,22 +1156,71 @@ static int ensemble_run(Ensemble* e, unsigned n0, unsigned nsteps) {
     e->ev_k.push_back(ev);
   }
   std::vector<std::vector<char>> async(n, std::vector<char>(nsteps, 0));
+  std::vector<char> timed(nsteps, 0);
   std::vector<TendParams> p(n);
   std::vector<char> shift(n);
+  std::vector<int> key(5 * n);
+  e->graph_steps = 0;
   for (unsigned q = 0; q < nsteps; ++q) {
     const unsigned step = n0 + q;
-    // phase 1: the fused kernels of all members in one launch, after their last corrections
+    bool graph_ok = e->use_graphs;
+    for (int i = 0; i < n; ++i) {
+      Model* m = e->mem[i];
+      bool sh = true;
+      p[i] = step_params(m, step, true, &sh);
+      shift[i] = sh;
+      graph_ok = graph_ok && graph_step_ok(m, sh);
+      key[5 * i] = m->cur; key[5 * i + 1] = m->h1; key[5 * i + 2] = m->h2; key[5 * i + 3] = m->h3;
+      key[5 * i + 4] = m->corner_cur;
+    }
+    // every step waits for the members' last corrections (events of stream-mode steps; after a
+    // replay the launch stream is already ordered behind them)
     for (int i = 0; i < n; ++i) PAWSIM_CUDA_OK(cudaStreamWaitEvent(e->s0, e->ev_p[i], 0));
     const int r = e->ring;
     e->ring = (e->ring + 1) % Ensemble::kRing;
     PAWSIM_CUDA_OK(cudaEventSynchronize(e->ev_ring[r]));   // that slot's earlier copy is done
     TendParams* hp = e->h_params + (size_t)r * n;
-    for (int i = 0; i < n; ++i) {
-      bool sh = true;
-      p[i] = step_params(e->mem[i], step, true, &sh);
-      shift[i] = sh;
-      hp[i] = p[i];
+    for (int i = 0; i < n; ++i) hp[i] = p[i];
+    if (graph_ok) {
+      EnsGraph* g = nullptr;
+      for (EnsGraph& c : e->graphs)
+        if (c.key == key) g = &c;
+      const bool fresh = g == nullptr;
+      if (fresh) {
+        if (e->graphs.size() >= 12) {
+          PAWSIM_CUDA_OK(cudaStreamSynchronize(e->s0));
+          e->drop_graphs();
+        }
+        e->graphs.emplace_back();
+        g = &e->graphs.back();
+        g->key = key;
+        PAWSIM_CUDA_OK(cudaMalloc(&g->d_params, n * sizeof(TendParams)));
+      }
+      if (fresh || memcmp(g->h_params.data(), p.data(), n * sizeof(TendParams)) != 0) {
+        // the blocks change only with time-dependent forcing records
+        PAWSIM_CUDA_OK(cudaMemcpyAsync(g->d_params, hp, n * sizeof(TendParams), cudaMemcpyHostToDevice, e->s0));
+        g->h_params = p;
+      }
+      PAWSIM_CUDA_OK(cudaEventRecord(e->ev_ring[r], e->s0));
+      set_int_kernel<<<1, 1, 0, e->s0>>>(e->d_pos, (int)q);
+      ++g_launches;
+      if (fresh) {
+        const int rc = ensemble_capture(e, *g, p, shift);
+        if (rc) {
+          PAWSIM_CUDA_OK(cudaStreamSynchronize(e->s0));
+          e->drop_graphs();
+          return rc;
+        }
+      } else {
+        g_launches += g->launches;
+        for (int i = 0; i < n; ++i) replay_member(e->mem[i], p[i], shift[i] != 0);
+      }
+      PAWSIM_CUDA_OK(cudaGraphLaunch(g->exec, e->s0));
+      for (int i = 0; i < n; ++i) async[i][q] = 1;
+      ++e->graph_steps;
+      continue;
     }
+    // stream mode. Phase 1: the fused kernels of all members in one launch
     PAWSIM_CUDA_OK(cudaMemcpyAsync(e->d_params, hp, n * sizeof(TendParams), cudaMemcpyHostToDevice, e->s0));
     PAWSIM_CUDA_OK(cudaEventRecord(e->ev_ring[r], e->s0));
     PAWSIM_CUDA_OK(cudaEventRecord(e->ev_k[2 * q], e->s0));
@@ -1060,19 +1229,19 @@ static int ensemble_run(Ensemble* e, unsigned n0, unsigned nsteps) {
     if (nl < 0) return fail(PAWSIM_GPU_EUNSUPPORTED, "batched tendency launch not available");
     g_launches += nl;
     PAWSIM_CUDA_OK(cudaEventRecord(e->ev_k[2 * q + 1], e->s0));
+    timed[q] = 1;
     PAWSIM_CUDA_OK(cudaEventRecord(e->ev_t, e->s0));
-    // phase 2: each member's corner shadow (state of the step start, read-only for the batched
-    // kernel), bookkeeping and rigid-lid correction on its own stream
+    // phase 2: each member's corner shadow, bookkeeping and correction on its own stream
     for (int i = 0; i < n; ++i) {
       Model* m = e->mem[i];
-      corner_fill(m, m->cur);
-      PAWSIM_CUDA_OK(cudaStreamWaitEvent(m->s, e->ev_t, 0));
-      step_finish(m, p[i], shift[i] != 0);
       if (async_correct_ok(m)) {
-        int rc = pressure_correct_async(m, (int)q);
+        int rc = member_step(e, i, p[i], shift[i] != 0, m->run_iters + q, m->run_meas + q, e->ev_t);
         if (rc) return rc;
         async[i][q] = 1;
       } else {
+        PAWSIM_CUDA_OK(cudaStreamWaitEvent(m->s, e->ev_t, 0));
+        corner_fill(m, m->cur);
+        step_finish(m, p[i], shift[i] != 0);
         pawsim_gpu_stats st;
         const int it = pressure_correct(m, 1, &st);
         if (it < 0) return it;
@@ -1082,6 +1251,7 @@ static int ensemble_run(Ensemble* e, unsigned n0, unsigned nsteps) {
     }
   }
   // the reports of the run, read once; the failure options as pawsim_gpu_run applies them
+  PAWSIM_CUDA_OK(cudaStreamSynchronize(e->s0));
   int r = 0;
   for (int i = 0; i < n; ++i) {
     Model* m = e->mem[i];
@@ -1099,14 +1269,16 @@ static int ensemble_run(Ensemble* e, unsigned n0, unsigned nsteps) {
       r = check_state_finite(m);
     }
   }
-  PAWSIM_CUDA_OK(cudaStreamSynchronize(e->s0));
   double tot = 0;
+  int cnt = 0;
   for (unsigned q = 0; q < nsteps; ++q) {
+    if (!timed[q]) continue;
     float ms = 0;
     PAWSIM_CUDA_OK(cudaEventElapsedTime(&ms, e->ev_k[2 * q], e->ev_k[2 * q + 1]));
     tot += ms;
+    ++cnt;
   }
-  e->kernel_ms = nsteps ? tot / nsteps : 0;
+  e->kernel_ms = cnt ? tot / cnt : 0;
   return r;
 }
 
@@ -1213,7 +1385,7 @@ int pawsim_gpu_run(pawsim_gpu* h, unsigned n0, unsigned nsteps, pawsim_gpu_stats
     if (async_correct_ok(m)) {
       int r = integrator_step(m, n, true);
       if (r) return r;
-      r = pressure_correct_async(m, (int)q);
+      r = pressure_correct_async(m, m->run_iters + q, m->run_meas + q);
       if (r) return r;
       async[q] = 1;
     } else {
@@ -1273,6 +1445,16 @@ int pawsim_gpu_ensemble_run(pawsim_gpu_ensemble* h, unsigned n0, unsigned nsteps
 
 double pawsim_gpu_ensemble_kernel_ms(const pawsim_gpu_ensemble* h) {
   return h ? h->e->kernel_ms : 0;
+}
+
+int pawsim_gpu_ensemble_set_graphs(pawsim_gpu_ensemble* h, int on) {
+  if (!h) return PAWSIM_GPU_EBADCONFIG;
+  h->e->use_graphs = on != 0;
+  return 0;
+}
+
+int pawsim_gpu_ensemble_graph_steps(const pawsim_gpu_ensemble* h) {
+  return h ? h->e->graph_steps : 0;
 }
 
 void pawsim_gpu_ensemble_destroy(pawsim_gpu_ensemble* h) {

@@ -1287,7 +1287,6 @@ void Multigrid::set_fine(double* pi, const double* rhs) {
 }
 
 int Multigrid::build_graph(int prec) {
-  LoopState* st = reinterpret_cast<LoopState*>(dstate_);
   cudaGraph_t& G = g_->graph[prec];
   if (cudaGraphCreate(&G, 0) != cudaSuccess) return -1;
   if (cudaGraphConditionalHandleCreate(&g_->handle[prec], G, 1, cudaGraphCondAssignDefault) != cudaSuccess) return -1;
@@ -1297,7 +1296,15 @@ int Multigrid::build_graph(int prec) {
   cp.conditional.size = 1;
   cudaGraphNode_t node;
   if (cudaGraphAddNode(&node, G, nullptr, 0, &cp) != cudaSuccess) return -1;
-  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  if (capture_body(prec, cp.conditional.phGraph_out[0], g_->handle[prec]) != 0) return -1;
+  if (cudaGraphInstantiate(&g_->exec[prec], G, 0) != cudaSuccess) return -1;
+  return 0;
+}
+
+// The loop body (one V-cycle, or the FP32 cycles and the FP64 defect step, then the loop
+// test that sets the conditional handle h) captured into `body`.
+int Multigrid::capture_body(int prec, cudaGraph_t body, cudaGraphConditionalHandle h) {
+  LoopState* st = reinterpret_cast<LoopState*>(dstate_);
   const long long counted = g_launches;   // captured launches are counted per executed cycle
   if (cudaStreamBeginCaptureToGraph(cap_, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
     return -1;
@@ -1311,11 +1318,34 @@ int Multigrid::build_graph(int prec) {
     defect_kernel<<<g2(f.Nx, f.Ny), B2, 0, cap_>>>(f, F.e, F.res, &st->iters, 0, F.e32, F.pitch, F.rhs32, 1,
                                                    &st->bits);
   }
-  loop_finalize_kernel<<<1, 1, 0, cap_>>>(st, g_->handle[prec]);
+  loop_finalize_kernel<<<1, 1, 0, cap_>>>(st, h);
   body_launches_[prec] = (int)(g_launches - counted) + (prec ? 2 : 1);   // + defect, finalize
   g_launches = counted;
   if (cudaStreamEndCapture(cap_, &body) != cudaSuccess) return -1;
-  if (cudaGraphInstantiate(&g_->exec[prec], G, 0) != cudaSuccess) return -1;
+  return 0;
+}
+
+// The V-cycle loop as a conditional node of the graph that s_ is being captured into (a handle
+// of that graph, the body captured afresh), so that a larger captured graph holds whole solves.
+// The same pattern as the loop graph's own; the outer capture continues after the node.
+int Multigrid::add_loop_node(int prec) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t G = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  if (cudaStreamGetCaptureInfo(s_, &cs, nullptr, &G, &deps, &nd) != cudaSuccess || cs != cudaStreamCaptureStatusActive)
+    return -1;
+  std::vector<cudaGraphNode_t> dv(deps, deps + nd);
+  cudaGraphConditionalHandle h;
+  if (cudaGraphConditionalHandleCreate(&h, G, 1, cudaGraphCondAssignDefault) != cudaSuccess) return -1;
+  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (cudaGraphAddNode(&node, G, dv.data(), nd, &cp) != cudaSuccess) return -1;
+  if (capture_body(prec, cp.conditional.phGraph_out[0], h) != 0) return -1;
+  if (cudaStreamUpdateCaptureDependencies(s_, &node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess) return -1;
   return 0;
 }
 
@@ -1531,7 +1561,14 @@ int Multigrid::solve_async(double* pi, const double* rhs, double tol, int maxite
     cudaMemsetAsync(&st->bits, 0, sizeof(unsigned long long), s_);
     ++*launches;
   }
-  if (cudaGraphLaunch(g_->exec[prec], s_) != cudaSuccess) return -1;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s_, &cs) != cudaSuccess) return -1;
+  if (cs == cudaStreamCaptureStatusActive) {
+    // the caller captures a larger graph: the loop becomes one of its nodes
+    if (add_loop_node(prec) != 0) return -1;
+  } else if (cudaGraphLaunch(g_->exec[prec], s_) != cudaSuccess) {
+    return -1;
+  }
   if (prec == 1) {
     commit_if_even_kernel<<<g2(F.Nx, F.Ny), B2, 0, s_>>>(st, F.e, F.res, F.Nx, F.Ny, F.pitch);
     ++*launches;

@@ -50,7 +50,9 @@ class Multigrid {
   // Solve without a host synchronisation: the V-cycle count and the final stopping measure go
   // to the device slots iters_out / maxres_out. Only after a synchronous solve on the same pi
   // and rhs has built the loop (async_ready); *launches receives the kernels enqueued outside
-  // the V-cycle graph (each executed cycle adds body_launches(), counted by the caller).
+  // the V-cycle graph (each executed cycle adds body_launches(), counted by the caller). When
+  // the stream is being captured, the loop is added to the captured graph as its own
+  // conditional node instead of launching the loop graph.
   bool async_ready() const;
   int solve_async(double* pi, const double* rhs, double tol, int maxiters, int* iters_out, double* maxres_out,
                   long long* launches);
@@ -108,6 +110,8 @@ class Multigrid {
   template <typename T> void tune(cudaStream_t s);
   void set_fine(double* pi, const double* rhs);
   int build_graph(int prec);
+  int capture_body(int prec, cudaGraph_t body, cudaGraphConditionalHandle h);
+  int add_loop_node(int prec);
   int body_launches_[2] = {0, 0};   // kernels per executed V-cycle of each graph body
   struct Graphs;
   bool ok_ = false;

@@ -38,10 +38,11 @@ def _check_members(members, alone, iters):
         assert a.t == b.t
 
 
-@pytest.mark.parametrize("solver", [0, 1])
-def test_uneven_jets_members_equal_alone(tmp_path, solver):
+@pytest.mark.parametrize("solver,graphs", [(0, True), (1, True), (1, False)])
+def test_uneven_jets_members_equal_alone(tmp_path, solver, graphs):
     """Three 64^2 and two 128^2 jets members with distinct noise seeds; multigrid (the first
-    solves tune it synchronously, the rest run asynchronously) and red-black SOR."""
+    solves tune it synchronously, then whole steps replay captured graphs, or run on streams
+    with graphs off) and red-black SOR (streams)."""
     import pawsim_b200
 
     specs = [(64, 11), (128, 12), (64, 13), (128, 14), (64, 15)]
@@ -59,12 +60,24 @@ def test_uneven_jets_members_equal_alone(tmp_path, solver):
         m.prelim()
         members.append(m)
     ens = pawsim_b200.Ensemble(members)
+    ens.set_graphs(graphs)
     ens.run(1, 5)
     it1 = [m.run_iterations() for m in members]
     ens.run(6, steps - 5)
     it2 = [m.run_iterations() for m in members]
+    # the multigrid members replay graphs from the first step whose loops are built; the
+    # cooperative SOR launch stays on streams
+    if graphs and solver == 1:
+        assert ens.graph_steps() == steps - 5
+    else:
+        assert ens.graph_steps() == 0
     ens.close()
     _check_members(members, alone, [np.concatenate([a, b]) for a, b in zip(it1, it2)])
+    # closed, the members step on alone exactly like their twins
+    for a, b in zip(members[:2], alone[:2]):
+        a.run(steps + 1, 3)
+        b.run(steps + 1, 3)
+    _check_members(members[:2], alone[:2], [m.run_iterations() for m in members[:2]])
     for m in members + alone:
         m.close()
 
