@@ -9,6 +9,7 @@
 // V-cycle plus the stopping test is a CUDA graph whose body sits in a device-side `while`
 // conditional node: no host round trip per V-cycle.
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -1249,6 +1250,20 @@ void Multigrid::tune(cudaStream_t s) {
       shape = opt_.tile_shape < kNumTileShapes ? opt_.tile_shape : kNumTileShapes - 1;
       continue;
     }
+    if (const char* forced = getenv("PAWSIM_MG_SHAPES")) {
+      // profiling recipes: the shapes of an unprofiled run, finest level first ("4,4,0,0")
+      int k = top, v = 0;
+      const char* c = forced;
+      while (k > n && *c) {
+        while (*c && *c != ',') ++c;
+        if (*c) ++c;
+        --k;
+      }
+      if (sscanf(c, "%d", &v) == 1 && v >= 0 && v < kNumTileShapes) {
+        shape = v;
+        continue;
+      }
+    }
     if (!tile_ok(F.Nx, F.Ny, F.power2, opt_.pre, opt_.post)) continue;
     LV<T> f = view<T>(F), c = view<T>(lv_[n - 1]);
     LV<T> fin = f;
@@ -1276,6 +1291,12 @@ void Multigrid::tune(cudaStream_t s) {
   cudaEventDestroy(ev[0]);
   cudaEventDestroy(ev[1]);
   g_launches = counted;   // tuning runs are not steps of the solve
+  if (getenv("PAWSIM_MG_VERBOSE")) {
+    // the shapes the tuner chose (0..3 tiles, kStripShape strips), for profiling recipes
+    for (int n = ctop_ + 1; n <= top; ++n)
+      fprintf(stderr, "pawsim mg: level %d (%d x %d) %s shape %d\n", n, lv_[n].Nx, lv_[n].Ny,
+              sizeof(T) == 8 ? "fp64" : "fp32", sizeof(T) == 8 ? lv_[n].shape64 : lv_[n].shape32);
+  }
 }
 
 void Multigrid::set_fine(double* pi, const double* rhs) {

@@ -431,6 +431,11 @@ __device__ inline double drag_load(const double* f, const TendParams& p, int x, 
 
 // One tile (bx, by) of the fused step; the fused kernel runs one per CTA, the exact pass the
 // tiles listed by it.
+// an L2 prefetch of the line holding *ptr (no register result, nothing to wait for)
+__device__ __forceinline__ void prefetch_l2(const void* ptr) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
+}
+
 template <int MS, int TS, int H, bool LEAN, bool EXACT>
 __device__ __forceinline__ void tendency_tile(const TendParams& p, int bx, int by) {
   // LEAN instantiations serve set-ups without w_dia, Smagorinsky, layer fractions, restoring,
@@ -474,6 +479,15 @@ __device__ __forceinline__ void tendency_tile(const TendParams& p, int bx, int b
   // tiles whose halo lies inside the domain read global memory without boundary maps
   const bool inner = t.X0 - H >= 0 && t.X0 + TX + H <= p.Nx && t.Y0 - H >= 0 && t.Y0 + TY + H <= p.Ny;
 
+  if (!EXACT) {
+    // the first layer's velocities at this thread's cell, read after the column prologue
+    const int gi0 = t.X0 + tid % TX, gj0 = t.Y0 + tid / TX;
+    if (gi0 < p.Nx && gj0 < p.Ny) {
+      const size_t c0 = (size_t)gj0 * p.pitch + gi0;
+      prefetch_l2(p.u + c0);
+      prefetch_l2(p.v + c0);
+    }
+  }
   // ---- column prologue over the Bernoulli region: eta, pp, Montgomery MM, wdia ----
   for (int q = tid; q < RN; q += NT) {
     int lx = q % RW, ly = q / RW;
@@ -574,6 +588,26 @@ __device__ __forceinline__ void tendency_tile(const TendParams& p, int bx, int b
     const double* uk = p.u + k * p.lstride;
     const double* vk = p.v + k * p.lstride;
     const double* hkp = p.h + k * p.lstride;
+    if (!EXACT && valid) {
+      // this layer's AB history (read in the epilogue) and the next layer's state at this
+      // thread's cell start towards L2 while the layer is computed
+      const size_t o = k * p.lstride + cell;
+      if (p.ab_mode >= 2) {
+        prefetch_l2(p.f1u + o);
+        prefetch_l2(p.f1v + o);
+        prefetch_l2(p.f1h + o);
+      }
+      if (p.ab_mode >= 3) {
+        prefetch_l2(p.f2u + o);
+        prefetch_l2(p.f2v + o);
+        prefetch_l2(p.f2h + o);
+      }
+      if (k + 1 < L) {
+        prefetch_l2(p.u + o + p.lstride);
+        prefetch_l2(p.v + o + p.lstride);
+        prefetch_l2(p.h + o + p.lstride);
+      }
+    }
     __syncthreads();
     // ---- load the layer's u, v, h with the reference's ghost semantics ----
     if (inner) {

@@ -17,6 +17,10 @@ from the network's guess (this exercises the tcgen05 convolution kernels).
 100 days). ``--averages`` accumulates the online averages after every step; ``--energy``
 computes the energy and enstrophy sums after every step; ``--budgets`` turns on the u, v,
 thickness and energy budgets (the budget build of the fused kernel).
+``--ensemble 64x256,16x512`` advances a batched ensemble of jets members instead (count x grid
+size per group, dx 10 km, dt 600 s unless ``--dt``, distinct noise seeds, ``--solver``) for
+``--steps`` steps after 3 warm-up steps; ``--no-graphs`` keeps every step on streams (the
+batched launch is then a kernel of its own for a profiler).
 """
 from __future__ import annotations
 
@@ -25,7 +29,7 @@ import json
 import tempfile
 import time
 
-from . import Model, inputs
+from . import Ensemble, Model, inputs
 
 SETUPS = {"gyre": inputs.gyre, "channel": inputs.channel, "jets": inputs.jets,
           "full": inputs.full_physics}
@@ -54,7 +58,11 @@ def main(argv=None):
     ap.add_argument("--averages", action="store_true")
     ap.add_argument("--energy", action="store_true")
     ap.add_argument("--budgets", action="store_true")
+    ap.add_argument("--ensemble", default=None, help="COUNTxN[,COUNTxN...]: a batched jets ensemble")
+    ap.add_argument("--no-graphs", action="store_true", help="ensemble steps on streams, not graph replays")
     a = ap.parse_args(argv)
+    if a.ensemble:
+        return run_ensemble(a)
     with tempfile.TemporaryDirectory() as d:
         if a.param:
             cfg = inputs.read_config(a.param)
@@ -70,7 +78,7 @@ def main(argv=None):
             if a.dt:
                 kw["dt"] = a.dt
             elif a.setup == "gyre":
-                kw["dt"] = 60.0 * 2048 / a.N if a.N <= 2048 else 60.0
+                kw["dt"] = 50.0 * 2048 / a.N if a.N <= 2048 else 50.0
             p = SETUPS[a.setup](d, **kw)
             if a.tracer >= 0:
                 inputs.add_tracer(p, scheme=a.tracer, relax_days=100.0, K2=100.0)
@@ -122,6 +130,36 @@ def main(argv=None):
         dt = time.perf_counter() - t0
         print(json.dumps({"setup": a.param or a.setup, "N": [cfg.Nx, cfg.Ny, cfg.Nlay], "steps": a.steps,
                           "seconds": dt, "last": rep}))
+        m.close()
+
+
+def run_ensemble(a):
+    groups = []
+    for part in a.ensemble.split(","):
+        count, n = part.lower().split("x")
+        groups.append((int(count), int(n)))
+    dt = a.dt or 600.0
+    members = []
+    with tempfile.TemporaryDirectory() as d:
+        seed = 1000
+        for count, n in groups:
+            for _ in range(count):
+                p = inputs.jets(f"{d}/m{seed}", N=n, Ly=n * 10e3, dt=dt, seed=seed, solver=a.solver)
+                m = Model(inputs.read_config(p))
+                m.prelim()
+                members.append(m)
+                seed += 1
+    ens = Ensemble(members)
+    ens.set_graphs(not a.no_graphs)
+    ens.run(1, 3)
+    t0 = time.perf_counter()
+    ens.run(4, a.steps)
+    sec = time.perf_counter() - t0
+    print(json.dumps({"ensemble": a.ensemble, "members": len(members), "steps": a.steps, "seconds": sec,
+                      "graph_steps": ens.graph_steps(), "kernel_ms": ens.kernel_ms(),
+                      "iters_member0": [int(x) for x in members[0].run_iterations()]}))
+    ens.close()
+    for m in members:
         m.close()
 
 
