@@ -216,6 +216,12 @@ PAWSIM_API double pawsim_gpu_ensemble_kernel_ms (const pawsim_gpu_ensemble * e);
  * Results are identical either way. graph_steps: how many steps of the last run replayed. */
 PAWSIM_API int pawsim_gpu_ensemble_set_graphs (pawsim_gpu_ensemble * e, int on);
 PAWSIM_API int pawsim_gpu_ensemble_graph_steps (const pawsim_gpu_ensemble * e);
+/* 1 when the captured steps solve every member's pressure in one batched multigrid loop (all
+ * members use the multigrid with FP64 cycles, one smoothing sweep each way, no use_fullMG):
+ * per V-cycle one launch per level for all members of a grid size, the loop running until
+ * every member meets its own stopping test; each member's solution and V-cycle count are
+ * those of its own solve. 0 when the members' solves are captured one by one. */
+PAWSIM_API int pawsim_gpu_ensemble_batched_mg (const pawsim_gpu_ensemble * e);
 PAWSIM_API void pawsim_gpu_ensemble_destroy (pawsim_gpu_ensemble * e);
 
 /* Online time averages (diagnostics.c:307-470, the savefreqAvg outputs). accumulate adds

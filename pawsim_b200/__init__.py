@@ -71,7 +71,8 @@ EXPORTS = (
     "pawsim_gpu_pressure_correct", "pawsim_gpu_prelim", "pawsim_gpu_step", "pawsim_gpu_run",
     "pawsim_gpu_run_iterations",
     "pawsim_gpu_ensemble_create", "pawsim_gpu_ensemble_run", "pawsim_gpu_ensemble_kernel_ms",
-    "pawsim_gpu_ensemble_set_graphs", "pawsim_gpu_ensemble_graph_steps", "pawsim_gpu_ensemble_destroy",
+    "pawsim_gpu_ensemble_set_graphs", "pawsim_gpu_ensemble_graph_steps", "pawsim_gpu_ensemble_batched_mg",
+    "pawsim_gpu_ensemble_destroy",
     "pawsim_gpu_solve_mg", "pawsim_gpu_set_stream", "pawsim_gpu_synchronize",
     "pawsim_gpu_time", "pawsim_gpu_launch_count", "pawsim_gpu_last_error",
     "pawsim_nn_conv3x3", "pawsim_nn_conv3x3_wgrad", "pawsim_nn_flip_weights",
@@ -117,6 +118,7 @@ def load_library(path: str = LIB_PATH):
     lib.pawsim_gpu_ensemble_kernel_ms.restype = ctypes.c_double
     lib.pawsim_gpu_ensemble_set_graphs.argtypes = [P, ctypes.c_int]
     lib.pawsim_gpu_ensemble_graph_steps.argtypes = [P]
+    lib.pawsim_gpu_ensemble_batched_mg.argtypes = [P]
     lib.pawsim_gpu_ensemble_destroy.argtypes = [P]
     lib.pawsim_gpu_ensemble_destroy.restype = None
     lib.pawsim_gpu_accumulate_averages.argtypes = [P, ctypes.c_double]
@@ -443,6 +445,10 @@ class Ensemble:
     def graph_steps(self) -> int:
         """Steps of the last run that ran as graph replays."""
         return int(self.lib.pawsim_gpu_ensemble_graph_steps(self._h))
+
+    def batched_mg(self) -> bool:
+        """Whether captured steps solve all members' pressure in one batched multigrid loop."""
+        return bool(self.lib.pawsim_gpu_ensemble_batched_mg(self._h))
 
     def kernel_ms(self) -> float:
         """Mean device time of one step's batched fused-kernel launch over the last run's

@@ -7,6 +7,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <mutex>
@@ -866,11 +867,10 @@ static bool async_correct_ok(const Model* m) {
 // The rigid-lid correction of pressure_correct without a host synchronisation; the solve's
 // iteration count and stopping measure go to the device slots it_out / meas_out (0 without
 // the rigid lid).
-static int pressure_correct_async(Model* m, int* it_out, double* meas_out) {
-  if (!m->c.use_rl) {
-    PAWSIM_CUDA_OK(cudaMemsetAsync(it_out, 0, sizeof(int), m->s));
-    return 0;
-  }
+// The steps of the rigid-lid correction before the solve: thickness constraint (unless the
+// fused step applied it), right-hand side with its corner fill, mean removal, and for the
+// multigrid the extrapolated first guess (pi_guess = 1).
+static int pressure_pre_solve(Model* m) {
   const int cur = m->cur;
   Grid2 g = m->grid2();
   dim3 b(32, 8), gr((m->Nx + 31) / 32, (m->Ny + 7) / 8);
@@ -884,7 +884,35 @@ static int pressure_correct_async(Model* m, int* it_out, double* meas_out) {
   launch_sum(m->rhs, m->Nx, m->Ny, m->pitch, m->serial(), m->scratch, m->dsum, m->s);
   launch_subtract_mean(m->rhs, m->Nx, m->Ny, m->pitch, m->dsum, m->s);
   g_launches += m->serial() ? 2 : 3;
+  if (m->c.solver != PAWSIM_GPU_SOLVER_SOR && m->c.pi_guess == 1) {
+    if (m->pi_solves >= 2) {
+      extrapolate_kernel<<<gr, b, 0, m->s>>>(m->pi, m->pi_prev, m->Nx, m->Ny, m->pitch);
+      ++g_launches;
+    } else if (m->pi_solves == 1) {
+      PAWSIM_CUDA_OK(cudaMemcpyAsync(m->pi_prev, m->pi, (size_t)m->Ny * m->pitch * sizeof(double),
+                                     cudaMemcpyDeviceToDevice, m->s));
+    }
+    ++m->pi_solves;
+  }
+  return 0;
+}
+
+static int pressure_post_solve(Model* m) {
+  launch_projection(m->grid2(), m->pi, m->u[m->cur], m->v[m->cur], m->s);
+  ++g_launches;
+  PAWSIM_CUDA_OK(cudaGetLastError());
+  return 0;
+}
+
+static int pressure_correct_async(Model* m, int* it_out, double* meas_out) {
+  if (!m->c.use_rl) {
+    PAWSIM_CUDA_OK(cudaMemsetAsync(it_out, 0, sizeof(int), m->s));
+    return 0;
+  }
+  int rc = pressure_pre_solve(m);
+  if (rc) return rc;
   if (m->c.solver == PAWSIM_GPU_SOLVER_SOR) {
+    Grid2 g = m->grid2();
     if (launch_sor(g, m->pi, m->rhs, m->op, m->c.sor_rp, m->c.pi_tol, m->c.maxiters, m->slots, m->diters, m->s) != 0)
       return fail(PAWSIM_GPU_ECUDA, "cooperative SOR launch failed");
     ++g_launches;
@@ -893,25 +921,12 @@ static int pressure_correct_async(Model* m, int* it_out, double* meas_out) {
     g_launches += m->serial() ? 2 : 3;
     PAWSIM_CUDA_OK(cudaMemcpyAsync(it_out, m->diters, sizeof(int), cudaMemcpyDeviceToDevice, m->s));
   } else {
-    if (m->c.pi_guess == 1) {
-      if (m->pi_solves >= 2) {
-        extrapolate_kernel<<<gr, b, 0, m->s>>>(m->pi, m->pi_prev, m->Nx, m->Ny, m->pitch);
-        ++g_launches;
-      } else if (m->pi_solves == 1) {
-        PAWSIM_CUDA_OK(cudaMemcpyAsync(m->pi_prev, m->pi, (size_t)m->Ny * m->pitch * sizeof(double),
-                                       cudaMemcpyDeviceToDevice, m->s));
-      }
-      ++m->pi_solves;
-    }
     long long nl = 0;
     if (m->mg->solve_async(m->pi, m->rhs, m->c.pi_tol, m->c.maxiters, it_out, meas_out, &nl) != 0)
       return fail(PAWSIM_GPU_ECUDA, "asynchronous multigrid solve failed");
     g_launches += nl;
   }
-  launch_projection(g, m->pi, m->u[cur], m->v[cur], m->s);
-  ++g_launches;
-  PAWSIM_CUDA_OK(cudaGetLastError());
-  return 0;
+  return pressure_post_solve(m);
 }
 
 // A batched ensemble of models (no reference counterpart: the reference runs one model per
@@ -928,6 +943,7 @@ struct EnsGraph {
   TendParams* d_params = nullptr;     // the parameter blocks the graph's batched launch reads
   std::vector<TendParams> h_params;   // what d_params holds
   long long launches = 0;             // kernels per replay outside the V-cycle bodies
+  bool batched = false;               // the members' solves run as one batched multigrid loop
 };
 
 __global__ void ring_push_kernel(const int* it, const double* meas, int* ring_it, double* ring_meas,
@@ -966,6 +982,10 @@ struct Ensemble {
   // not be waited on outside it)
   cudaEvent_t ev_cf = nullptr;
   std::vector<cudaEvent_t> ev_cj;
+  // the members' multigrid solves batched into one loop (when every member's solver allows)
+  MGBatch* mgb = nullptr;
+  bool mgb_tried = false;
+  cudaStream_t cap = nullptr;   // stream that captures the batched loop's body
   void drop_graphs() {
     for (EnsGraph& g : graphs) {
       if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -982,6 +1002,8 @@ struct Ensemble {
       if (mem[i]->dmg) mem[i]->dmg->set_stream(old_streams[i]);
     }
     drop_graphs();
+    delete mgb;
+    if (cap) cudaStreamDestroy(cap);
     for (cudaStream_t q : streams) cudaStreamDestroy(q);
     for (cudaEvent_t e : ev_p) cudaEventDestroy(e);
     for (cudaEvent_t e : ev_ring) cudaEventDestroy(e);
@@ -1039,6 +1061,7 @@ static int ensemble_create(Model* const* ms, int n, Ensemble** out) {
   }
   e->nwork = (int)work.size();
   bool ok = cudaStreamCreateWithFlags(&e->s0, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&e->cap, cudaStreamNonBlocking) == cudaSuccess &&
             cudaEventCreateWithFlags(&e->ev_t, cudaEventDisableTiming) == cudaSuccess &&
             cudaEventCreateWithFlags(&e->ev_cf, cudaEventDisableTiming) == cudaSuccess &&
             cudaMalloc(&e->d_params, n * sizeof(TendParams)) == cudaSuccess &&
@@ -1105,10 +1128,42 @@ static int member_step(Ensemble* e, int i, const TendParams& p, bool shift, int*
   return pressure_correct_async(m, it, meas);
 }
 
+// The batched multigrid of all members, built once when every member solves with the
+// multigrid and its solver allows batching (MGBatch::ok); nullptr otherwise.
+static MGBatch* ensemble_mg_batch(Ensemble* e) {
+  if (e->mgb_tried) return e->mgb;
+  e->mgb_tried = true;
+  std::vector<Multigrid*> mgs;
+  std::vector<double> tol;
+  std::vector<int> maxit;
+  std::vector<int*> its;
+  std::vector<double*> meas;
+  for (size_t i = 0; i < e->mem.size(); ++i) {
+    Model* m = e->mem[i];
+    if (!m->c.use_rl || m->c.solver != PAWSIM_GPU_SOLVER_MG || !m->mg) return nullptr;
+    mgs.push_back(m->mg);
+    tol.push_back(m->c.pi_tol);
+    maxit.push_back(m->c.maxiters);
+    its.push_back(e->d_slot_it + i);
+    meas.push_back(e->d_slot_meas + i);
+  }
+  MGBatch* b = new MGBatch(mgs, tol, maxit, its, meas);
+  if (!b->ok()) {
+    delete b;
+    cudaGetLastError();
+    return nullptr;
+  }
+  e->mgb = b;
+  return b;
+}
+
 // Capture one step of every member into graph g (its parameter blocks already in g.d_params).
+// With the batched multigrid: each member's pre-solve steps on its stream, the one batched
+// loop on the launch stream, then each member's projection.
 static int ensemble_capture(Ensemble* e, EnsGraph& g, const std::vector<TendParams>& p,
                             const std::vector<char>& shift) {
   const int n = (int)e->mem.size();
+  MGBatch* mgb = ensemble_mg_batch(e);
   const long long g0 = g_launches;
   PAWSIM_CUDA_OK(cudaStreamBeginCapture(e->s0, cudaStreamCaptureModeRelaxed));
   int rc = 0;
@@ -1117,7 +1172,34 @@ static int ensemble_capture(Ensemble* e, EnsGraph& g, const std::vector<TendPara
   if (nl < 0) rc = fail(PAWSIM_GPU_EUNSUPPORTED, "batched tendency launch not available");
   g_launches += nl > 0 ? nl : 0;
   if (!rc && cudaEventRecord(e->ev_cf, e->s0) != cudaSuccess) rc = fail(PAWSIM_GPU_ECUDA, "event record failed");
-  for (int i = 0; i < n && !rc; ++i) {
+  if (mgb) {
+    g.batched = true;
+    for (int i = 0; i < n && !rc; ++i) {
+      Model* m = e->mem[i];
+      if (cudaStreamWaitEvent(m->s, e->ev_cf, 0) != cudaSuccess) rc = fail(PAWSIM_GPU_ECUDA, "capture fork failed");
+      if (rc) break;
+      corner_fill(m, m->cur);
+      step_finish(m, p[i], shift[i] != 0);
+      rc = pressure_pre_solve(m);
+      if (!rc && (cudaEventRecord(e->ev_cj[i], m->s) != cudaSuccess ||
+                  cudaStreamWaitEvent(e->s0, e->ev_cj[i], 0) != cudaSuccess))
+        rc = fail(PAWSIM_GPU_ECUDA, "capture join failed");
+    }
+    if (!rc && mgb->capture(e->s0, e->cap) != 0) rc = fail(PAWSIM_GPU_ECUDA, "batched multigrid capture failed");
+    if (!rc && cudaEventRecord(e->ev_cf, e->s0) != cudaSuccess) rc = fail(PAWSIM_GPU_ECUDA, "event record failed");
+    for (int i = 0; i < n && !rc; ++i) {
+      Model* m = e->mem[i];
+      if (cudaStreamWaitEvent(m->s, e->ev_cf, 0) != cudaSuccess) rc = fail(PAWSIM_GPU_ECUDA, "capture fork failed");
+      if (rc) break;
+      rc = pressure_post_solve(m);
+      if (rc) break;
+      ring_push_kernel<<<1, 1, 0, m->s>>>(e->d_slot_it + i, e->d_slot_meas + i, m->run_iters, m->run_meas, e->d_pos);
+      ++g_launches;
+      if (cudaEventRecord(e->ev_cj[i], m->s) != cudaSuccess || cudaStreamWaitEvent(e->s0, e->ev_cj[i], 0) != cudaSuccess)
+        rc = fail(PAWSIM_GPU_ECUDA, "capture join failed");
+    }
+  }
+  for (int i = 0; i < n && !rc && !mgb; ++i) {
     Model* m = e->mem[i];
     rc = member_step(e, i, p[i], shift[i] != 0, e->d_slot_it + i, e->d_slot_meas + i, e->ev_cf);
     if (rc) break;
@@ -1156,7 +1238,7 @@ static int ensemble_run(Ensemble* e, unsigned n0, unsigned nsteps) {
     e->ev_k.push_back(ev);
   }
   std::vector<std::vector<char>> async(n, std::vector<char>(nsteps, 0));
-  std::vector<char> timed(nsteps, 0);
+  std::vector<char> timed(nsteps, 0), batched(nsteps, 0);
   std::vector<TendParams> p(n);
   std::vector<char> shift(n);
   std::vector<int> key(5 * n);
@@ -1217,6 +1299,7 @@ static int ensemble_run(Ensemble* e, unsigned n0, unsigned nsteps) {
       }
       PAWSIM_CUDA_OK(cudaGraphLaunch(g->exec, e->s0));
       for (int i = 0; i < n; ++i) async[i][q] = 1;
+      batched[q] = g->batched ? 1 : 0;
       ++e->graph_steps;
       continue;
     }
@@ -1253,6 +1336,7 @@ static int ensemble_run(Ensemble* e, unsigned n0, unsigned nsteps) {
   // the reports of the run, read once; the failure options as pawsim_gpu_run applies them
   PAWSIM_CUDA_OK(cudaStreamSynchronize(e->s0));
   int r = 0;
+  std::vector<int> most(nsteps, 0);   // cycles of a batched loop: those of its slowest member
   for (int i = 0; i < n; ++i) {
     Model* m = e->mem[i];
     std::vector<int> it(nsteps);
@@ -1261,7 +1345,8 @@ static int ensemble_run(Ensemble* e, unsigned n0, unsigned nsteps) {
     for (unsigned q = 0; q < nsteps; ++q) {
       if (!async[i][q]) continue;
       m->last_run_iters[q] = it[q];
-      if (m->c.use_rl && m->c.solver == PAWSIM_GPU_SOLVER_MG) g_launches += (long long)it[q] * m->mg->body_launches();
+      if (batched[q]) most[q] = std::max(most[q], it[q]);
+      else if (m->c.use_rl && m->c.solver == PAWSIM_GPU_SOLVER_MG) g_launches += (long long)it[q] * m->mg->body_launches();
     }
     for (unsigned q = 0; q < nsteps && !r; ++q) r = check_converged(m, m->last_run_iters[q]);
     if (!r && m->nonfinite) {
@@ -1269,6 +1354,8 @@ static int ensemble_run(Ensemble* e, unsigned n0, unsigned nsteps) {
       r = check_state_finite(m);
     }
   }
+  for (unsigned q = 0; q < nsteps; ++q)
+    if (batched[q] && e->mgb) g_launches += (long long)most[q] * e->mgb->body_launches();
   double tot = 0;
   int cnt = 0;
   for (unsigned q = 0; q < nsteps; ++q) {
@@ -1455,6 +1542,10 @@ int pawsim_gpu_ensemble_set_graphs(pawsim_gpu_ensemble* h, int on) {
 
 int pawsim_gpu_ensemble_graph_steps(const pawsim_gpu_ensemble* h) {
   return h ? h->e->graph_steps : 0;
+}
+
+int pawsim_gpu_ensemble_batched_mg(const pawsim_gpu_ensemble* h) {
+  return h && h->e->mgb ? 1 : 0;
 }
 
 void pawsim_gpu_ensemble_destroy(pawsim_gpu_ensemble* h) {

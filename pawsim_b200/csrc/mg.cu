@@ -368,12 +368,13 @@ __device__ inline void tile_sweeps(int xy, T omega, const TileBuf<T, OX, OY, H>&
 // pre-smoothing of f.e (or of zero) into `out`, residual and 2x2 restriction into the
 // coarse rhs (the coarse correction starts from zero: the coarse kernels never read it)
 template <typename T, int OX, int OY, int NT, int NU>
-__global__ void __launch_bounds__(NT) down_tile(LV<T> f, LV<T> c, T omega, int zero_e, T* __restrict__ out) {
+__device__ __forceinline__ void down_tile_body(const LV<T>& f, const LV<T>& c, T omega, int zero_e,
+                                               T* __restrict__ out, int bx, int by) {
   constexpr int H = 2 * NU + 1;
   using G = PT<T, OX, OY, H>;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   const TileBuf<T, OX, OY, H> b(reinterpret_cast<T*>(sm_raw));
-  const int X0 = blockIdx.x * OX, Y0 = blockIdx.y * OY;
+  const int X0 = bx * OX, Y0 = by * OY;
   const bool inner = tile_inner<OX, OY, H>(X0, Y0, f.Nx, f.Ny);
   issue_tile<T, OX, OY, H, NT>(f, c, X0, Y0, zero_e != 0, false, b);
   cp_async_wait<0>();
@@ -411,18 +412,23 @@ __global__ void __launch_bounds__(NT) down_tile(LV<T> f, LV<T> c, T omega, int z
   }
 }
 
+template <typename T, int OX, int OY, int NT, int NU>
+__global__ void __launch_bounds__(NT) down_tile(LV<T> f, LV<T> c, T omega, int zero_e, T* __restrict__ out) {
+  down_tile_body<T, OX, OY, NT, NU>(f, c, omega, zero_e, out, blockIdx.x, blockIdx.y);
+}
+
 // prolongation of the coarse correction c.e, correction of f.e and post-smoothing, into
 // `out`. With MEASURE the tile carries one more halo row and the kernel also folds
 // max |e - Jacobi(e)| over its owned cells into *bits: the stopping measure of the
 // finished V-cycle (multigrid.c:1123-1156).
 template <typename T, int OX, int OY, int NT, int NU, bool MEASURE>
-__global__ void __launch_bounds__(NT) up_tile(LV<T> f, LV<T> c, T omega, int wew, int wns,
-                                              unsigned long long* bits, T* __restrict__ out) {
+__device__ __forceinline__ void up_tile_body(const LV<T>& f, const LV<T>& c, T omega, int wew, int wns,
+                                             unsigned long long* bits, T* __restrict__ out, int bx, int by) {
   constexpr int H = 2 * NU + (MEASURE ? 1 : 0);
   using G = PT<T, OX, OY, H>;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   const TileBuf<T, OX, OY, H> b(reinterpret_cast<T*>(sm_raw));
-  const int X0 = blockIdx.x * OX, Y0 = blockIdx.y * OY;
+  const int X0 = bx * OX, Y0 = by * OY;
   const bool inner = tile_inner<OX, OY, H>(X0, Y0, f.Nx, f.Ny);
   issue_tile<T, OX, OY, H, NT>(f, c, X0, Y0, false, true, b);
   cp_async_wait<0>();
@@ -468,6 +474,12 @@ __global__ void __launch_bounds__(NT) up_tile(LV<T> f, LV<T> c, T omega, int wew
     }
   }
   if constexpr (MEASURE) block_max_to(m, bits);
+}
+
+template <typename T, int OX, int OY, int NT, int NU, bool MEASURE>
+__global__ void __launch_bounds__(NT) up_tile(LV<T> f, LV<T> c, T omega, int wew, int wns,
+                                              unsigned long long* bits, T* __restrict__ out) {
+  up_tile_body<T, OX, OY, NT, NU, MEASURE>(f, c, omega, wew, wns, bits, out, blockIdx.x, blockIdx.y);
 }
 
 #include "mg_strip.cuh"
@@ -754,13 +766,13 @@ __global__ void __launch_bounds__(CT) coarse_kernel(const __grid_constant__ Coar
 // memory), instead of one CTA walking the coarse levels phase by phase.
 constexpr int CA_WARPS = 4;
 template <typename T>
-__global__ void __launch_bounds__(CA_WARPS * 32) coarse_apply_kernel(const T* __restrict__ C, int n, int Nx, int pitch,
-                                                                    const T* __restrict__ rhs, T* __restrict__ e) {
+__device__ __forceinline__ void coarse_apply_body(const T* __restrict__ C, int n, int Nx, int pitch,
+                                                  const T* __restrict__ rhs, T* __restrict__ e, int bx) {
   __shared__ T x[1024];
   for (int q = threadIdx.x; q < n; q += CA_WARPS * 32) x[q] = rhs[(size_t)(q / Nx) * pitch + q % Nx];
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int row = blockIdx.x * CA_WARPS + (threadIdx.x >> 5);
+  const int row = bx * CA_WARPS + (threadIdx.x >> 5);
   if (row >= n) return;
   const T* c = C + (size_t)row * n;
   // four independent partial sums so that the loads of a row are all in flight at once
@@ -777,6 +789,12 @@ __global__ void __launch_bounds__(CA_WARPS * 32) coarse_apply_kernel(const T* __
   T acc = (a0 + a1) + (a2 + a3);
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
   if (lane == 0) e[(size_t)(row / Nx) * pitch + row % Nx] = acc;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(CA_WARPS * 32) coarse_apply_kernel(const T* __restrict__ C, int n, int Nx, int pitch,
+                                                                    const T* __restrict__ rhs, T* __restrict__ e) {
+  coarse_apply_body<T>(C, n, Nx, pitch, rhs, e, blockIdx.x);
 }
 
 // ---------------------------------------------------------------- stopping test and loop control
@@ -1594,6 +1612,275 @@ int Multigrid::solve_async(double* pi, const double* rhs, double tol, int maxite
     commit_if_even_kernel<<<g2(F.Nx, F.Ny), B2, 0, s_>>>(st, F.e, F.res, F.Nx, F.Ny, F.pitch);
     ++*launches;
   }
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+// ---------------------------------------------------------------- batched solves (MGBatch)
+
+namespace {
+
+struct BatchLevel {   // one member's arrays for a level kernel of the batched V-cycle
+  LV<double> f, c;
+  double omega;
+  double* out;
+  int zero_e;
+};
+
+struct BatchCoarse {  // one member's tabulated coarse map and its top-level arrays
+  const double* C;
+  const double* rhs;
+  double* e;
+};
+
+struct BatchLoop {    // one member's loop state (the batched LoopState)
+  unsigned long long bits;   // max |pi - Jacobi(pi)| of the cycle, as an integer bit pattern
+  int iters;
+  int active;                // still iterating
+  int maxiters;
+  double tol;
+  double maxres;
+};
+
+constexpr int BOX = 32, BOY = 8, BNT = 256;   // the batched level kernels' tile shape
+
+__global__ void __launch_bounds__(BNT) down_batch_kernel(const BatchLevel* __restrict__ d,
+                                                          const BatchLoop* __restrict__ st) {
+  const int m = blockIdx.z;
+  if (!st[m].active) return;
+  const BatchLevel L = d[m];
+  down_tile_body<double, BOX, BOY, BNT, 1>(L.f, L.c, L.omega, L.zero_e, L.out, blockIdx.x, blockIdx.y);
+}
+
+template <bool MEASURE>
+__global__ void __launch_bounds__(BNT) up_batch_kernel(const BatchLevel* __restrict__ d, BatchLoop* st, int wew,
+                                                        int wns) {
+  const int m = blockIdx.z;
+  if (!st[m].active) return;
+  const BatchLevel L = d[m];
+  up_tile_body<double, BOX, BOY, BNT, 1, MEASURE>(L.f, L.c, L.omega, wew, wns, &st[m].bits, L.out, blockIdx.x,
+                                                  blockIdx.y);
+}
+
+__global__ void __launch_bounds__(CA_WARPS * 32) coarse_batch_kernel(const BatchCoarse* __restrict__ d,
+                                                                      const BatchLoop* __restrict__ st, int n, int Nx,
+                                                                      int pitch) {
+  const int m = blockIdx.y;
+  if (!st[m].active) return;
+  const BatchCoarse B = d[m];
+  coarse_apply_body<double>(B.C, n, Nx, pitch, B.rhs, B.e, blockIdx.x);
+}
+
+__global__ void batch_reset_kernel(BatchLoop* st, int n) {
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+    st[m].bits = 0;
+    st[m].iters = 0;
+    st[m].active = 1;
+    st[m].maxres = st[m].tol + 1;
+  }
+}
+
+// the loop test of every member still iterating (loop_finalize_kernel per member); the loop
+// continues while any member does. One block.
+__global__ void batch_finalize_kernel(BatchLoop* st, int n, int* const* it_out, double* const* meas_out,
+                                      cudaGraphConditionalHandle h) {
+  int any = 0;
+  for (int m = threadIdx.x; m < n; m += blockDim.x) {
+    BatchLoop& s = st[m];
+    if (s.active) {
+      const double v = __longlong_as_double((long long)s.bits);
+      s.bits = 0;
+      s.iters += 1;
+      s.maxres = v;
+      *it_out[m] = s.iters;
+      *meas_out[m] = v;
+      s.active = (v > s.tol) && (s.iters < s.maxiters);
+    }
+    any |= s.active;
+  }
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, any ? 1u : 0u);
+}
+
+}  // namespace
+
+struct MGBatch::Group {
+  int off = 0, count = 0;        // members [off, off + count) of the loop state
+  int top = 0, ctop = 0;         // level indices of the finest level and the coarse block's top
+  int wew = 0, wns = 0;
+  std::vector<int> nx, ny;       // per level
+  std::vector<BatchLevel*> down, up;   // per level (device arrays of count entries)
+  BatchCoarse* coarse = nullptr;
+  int cn = 0, cnx = 0, cpitch = 0;     // the coarse block's top level
+  ~Group() {
+    for (BatchLevel* p : down) cudaFree(p);
+    for (BatchLevel* p : up) cudaFree(p);
+    cudaFree(coarse);
+  }
+};
+
+MGBatch::MGBatch(const std::vector<Multigrid*>& members, const std::vector<double>& tol,
+                 const std::vector<int>& maxiters, const std::vector<int*>& it_out,
+                 const std::vector<double*>& meas_out) {
+  n_ = (int)members.size();
+  if (n_ < 1 || tol.size() != members.size() || maxiters.size() != members.size() ||
+      it_out.size() != members.size() || meas_out.size() != members.size())
+    return;
+  for (const Multigrid* g : members) {
+    const int top = (int)g->lv_.size() - 1;
+    if (!g->async_ready() || g->opt_.fp32_cycles || g->opt_.pre != 1 || g->opt_.post != 1 || g->opt_.full_mg ||
+        !g->cmat_[0] || top <= g->ctop_ || g->lv_[g->ctop_].Nx * g->lv_[g->ctop_].Ny > 1024)
+      return;
+    for (int n = g->ctop_ + 1; n <= top; ++n)
+      if (!tile_ok(g->lv_[n].Nx, g->lv_[n].Ny, g->lv_[n].power2, 1, 1)) return;
+  }
+  // group the members by level hierarchy (finest size and walls), keeping their order
+  std::vector<int> order;
+  std::vector<std::vector<int>> sets;
+  for (int i = 0; i < n_; ++i) {
+    const Multigrid* g = members[i];
+    int found = -1;
+    for (size_t k = 0; k < sets.size(); ++k) {
+      const Multigrid* r = members[sets[k][0]];
+      if (r->Nx_ == g->Nx_ && r->Ny_ == g->Ny_ && r->wew_ == g->wew_ && r->wns_ == g->wns_ &&
+          r->lv_.size() == g->lv_.size() && r->ctop_ == g->ctop_)
+        found = (int)k;
+    }
+    if (found < 0) {
+      sets.emplace_back();
+      found = (int)sets.size() - 1;
+    }
+    sets[found].push_back(i);
+  }
+  // loop state and report slots in group order
+  std::vector<BatchLoop> hl;
+  std::vector<int*> hit;
+  std::vector<double*> hmeas;
+  bool good = true;
+  body_launches_ = 1;   // the loop test
+  for (const std::vector<int>& set : sets) {
+    Group* G = new Group();
+    groups_.push_back(G);
+    const Multigrid* r = members[set[0]];
+    G->off = (int)hl.size();
+    G->count = (int)set.size();
+    G->top = (int)r->lv_.size() - 1;
+    G->ctop = r->ctop_;
+    G->wew = r->wew_ ? 1 : 0;
+    G->wns = r->wns_ ? 1 : 0;
+    G->nx.resize(G->top + 1);
+    G->ny.resize(G->top + 1);
+    G->down.assign(G->top + 1, nullptr);
+    G->up.assign(G->top + 1, nullptr);
+    for (int n = 0; n <= G->top; ++n) {
+      G->nx[n] = r->lv_[n].Nx;
+      G->ny[n] = r->lv_[n].Ny;
+    }
+    for (int n = G->ctop + 1; n <= G->top; ++n) {
+      std::vector<BatchLevel> dn(G->count), upv(G->count);
+      for (int q = 0; q < G->count; ++q) {
+        Multigrid* g = members[set[q]];
+        const LV<double> f = view<double>(g->lv_[n]), c = view<double>(g->lv_[n - 1]);
+        dn[q] = BatchLevel{f, c, g->opt_.omega_rb, f.tmp, n != G->top ? 1 : 0};
+        LV<double> fin = f;
+        fin.e = f.tmp;   // the pre-smoothed correction written by the down kernel
+        upv[q] = BatchLevel{fin, c, g->opt_.omega_rb, f.e, 0};
+      }
+      good = good && cudaMalloc(&G->down[n], G->count * sizeof(BatchLevel)) == cudaSuccess &&
+             cudaMalloc(&G->up[n], G->count * sizeof(BatchLevel)) == cudaSuccess &&
+             cudaMemcpy(G->down[n], dn.data(), G->count * sizeof(BatchLevel), cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemcpy(G->up[n], upv.data(), G->count * sizeof(BatchLevel), cudaMemcpyHostToDevice) == cudaSuccess;
+      body_launches_ += 2;
+    }
+    std::vector<BatchCoarse> cv(G->count);
+    const Multigrid::Level& Lt = r->lv_[G->ctop];
+    G->cn = Lt.Nx * Lt.Ny;
+    G->cnx = Lt.Nx;
+    G->cpitch = Lt.pitch;
+    for (int q = 0; q < G->count; ++q) {
+      Multigrid* g = members[set[q]];
+      const Multigrid::Level& L = g->lv_[g->ctop_];
+      cv[q] = BatchCoarse{static_cast<const double*>(g->cmat_[0]), L.rhs, L.e};
+    }
+    good = good && cudaMalloc(&G->coarse, G->count * sizeof(BatchCoarse)) == cudaSuccess &&
+           cudaMemcpy(G->coarse, cv.data(), G->count * sizeof(BatchCoarse), cudaMemcpyHostToDevice) == cudaSuccess;
+    body_launches_ += 1;
+    for (int q = 0; q < G->count; ++q) {
+      const int i = set[q];
+      BatchLoop b;
+      memset(&b, 0, sizeof(b));
+      b.tol = tol[i];
+      b.maxiters = maxiters[i];
+      hl.push_back(b);
+      hit.push_back(it_out[i]);
+      hmeas.push_back(meas_out[i]);
+    }
+  }
+  good = good && cudaMalloc(&loop_, n_ * sizeof(BatchLoop)) == cudaSuccess &&
+         cudaMalloc(&it_out_, n_ * sizeof(int*)) == cudaSuccess &&
+         cudaMalloc(&meas_out_, n_ * sizeof(double*)) == cudaSuccess &&
+         cudaMemcpy(loop_, hl.data(), n_ * sizeof(BatchLoop), cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(it_out_, hit.data(), n_ * sizeof(int*), cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(meas_out_, hmeas.data(), n_ * sizeof(double*), cudaMemcpyHostToDevice) == cudaSuccess;
+  if (good) {
+    cudaFuncSetAttribute(down_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)tile_bytes<double, BOX, BOY, 3>());
+    cudaFuncSetAttribute(up_batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)tile_bytes<double, BOX, BOY, 3>());
+    cudaFuncSetAttribute(up_batch_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)tile_bytes<double, BOX, BOY, 2>());
+  }
+  ok_ = good && cudaGetLastError() == cudaSuccess;
+}
+
+MGBatch::~MGBatch() {
+  for (Group* g : groups_) delete g;
+  cudaFree(loop_);
+  cudaFree(it_out_);
+  cudaFree(meas_out_);
+}
+
+int MGBatch::capture(cudaStream_t s, cudaStream_t cap) {
+  if (!ok_) return -1;
+  BatchLoop* st = static_cast<BatchLoop*>(loop_);
+  batch_reset_kernel<<<(n_ + 255) / 256, 256, 0, s>>>(st, n_);
+  ++g_launches;
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t G = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  if (cudaStreamGetCaptureInfo(s, &cs, nullptr, &G, &deps, &nd) != cudaSuccess || cs != cudaStreamCaptureStatusActive)
+    return -1;
+  std::vector<cudaGraphNode_t> dv(deps, deps + nd);
+  cudaGraphConditionalHandle h;
+  if (cudaGraphConditionalHandleCreate(&h, G, 1, cudaGraphCondAssignDefault) != cudaSuccess) return -1;
+  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (cudaGraphAddNode(&node, G, dv.data(), nd, &cp) != cudaSuccess) return -1;
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  if (cudaStreamBeginCaptureToGraph(cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+    return -1;
+  for (const Group* g : groups_) {
+    BatchLoop* gs = st + g->off;
+    for (int n = g->top; n > g->ctop; --n) {
+      const dim3 grid((g->nx[n] + BOX - 1) / BOX, (g->ny[n] + BOY - 1) / BOY, g->count);
+      down_batch_kernel<<<grid, BNT, tile_bytes<double, BOX, BOY, 3>(), cap>>>(g->down[n], gs);
+    }
+    coarse_batch_kernel<<<dim3((g->cn + CA_WARPS - 1) / CA_WARPS, g->count), CA_WARPS * 32, 0, cap>>>(
+        g->coarse, gs, g->cn, g->cnx, g->cpitch);
+    for (int n = g->ctop + 1; n <= g->top; ++n) {
+      const dim3 grid((g->nx[n] + BOX - 1) / BOX, (g->ny[n] + BOY - 1) / BOY, g->count);
+      if (n == g->top)
+        up_batch_kernel<true><<<grid, BNT, tile_bytes<double, BOX, BOY, 3>(), cap>>>(g->up[n], gs, g->wew, g->wns);
+      else
+        up_batch_kernel<false><<<grid, BNT, tile_bytes<double, BOX, BOY, 2>(), cap>>>(g->up[n], gs, g->wew, g->wns);
+    }
+  }
+  batch_finalize_kernel<<<1, 256, 0, cap>>>(st, n_, it_out_, meas_out_, h);
+  if (cudaStreamEndCapture(cap, &body) != cudaSuccess) return -1;
+  if (cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess) return -1;
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -36,7 +36,11 @@ struct MGOptions {
 // candidate weights of the automatic choice
 constexpr double kOmegaCandidates[] = {1.0, 1.05, 1.1, 1.15, 1.2, 1.3};
 
+class MGBatch;
+
 class Multigrid {
+  friend class MGBatch;
+
  public:
   // Hc: host array Nx*Ny (x fastest) of the water-column thickness
   Multigrid(int Nx, int Ny, double Lx, double Ly, bool wall_ew, bool wall_ns, const double* Hc_host,
@@ -127,6 +131,40 @@ class Multigrid {
   double* fine_pi_ = nullptr;
   const double* fine_rhs_ = nullptr;
   double *own_e_ = nullptr, *own_rhs_ = nullptr;
+};
+
+// The multigrid solves of several models advanced together (the batched ensemble). Members
+// with the same level hierarchy form a group; per V-cycle one launch per level and group runs
+// the tiles of every member still iterating (blockIdx.z = member), one launch per group applies
+// the tabulated coarse maps, and one conditional loop node repeats the cycle until every member
+// meets its own stopping test. A member's cycles are its own solve's kernels on its own arrays
+// (the same tile arithmetic in the same order), so its iterates, V-cycle count and stopping
+// measure equal those of that member's solve alone.
+class MGBatch {
+ public:
+  // members: solvers whose async_ready() holds, with FP64 cycles, pre = post = 1, no
+  // use_fullMG, a tabulated coarse map and every tiled level 2:1 (ok() is false otherwise);
+  // tol and maxiters per member; it_out[i] / meas_out[i]: device slots that receive member
+  // i's V-cycle count and stopping measure after every cycle
+  MGBatch(const std::vector<Multigrid*>& members, const std::vector<double>& tol, const std::vector<int>& maxiters,
+          const std::vector<int*>& it_out, const std::vector<double*>& meas_out);
+  ~MGBatch();
+  bool ok() const { return ok_; }
+  // enqueue on s, which is being captured into a graph: the loop reset, then the loop as a
+  // conditional node of that graph (its body captured on cap); returns 0 or -1
+  int capture(cudaStream_t s, cudaStream_t cap);
+  // kernels per executed cycle (every group's level launches and the loop test)
+  int body_launches() const { return body_launches_; }
+
+ private:
+  struct Group;
+  std::vector<Group*> groups_;
+  void* loop_ = nullptr;       // per member loop state (device)
+  int** it_out_ = nullptr;     // device arrays of the members' report slots
+  double** meas_out_ = nullptr;
+  int n_ = 0;
+  int body_launches_ = 0;
+  bool ok_ = false;
 };
 
 }  // namespace pawsim

@@ -191,27 +191,48 @@ __global__ void rhs_kernel(const Grid2 g, const double* __restrict__ u, const do
 constexpr int RED_BLOCK = 256;
 constexpr int RED_ROWS = 8;   // rows per partial in the tree sum
 
-// serial order of pressure.c:62-69: x outer, y inner. One thread; loads are batched so
-// that the dependent additions, not the memory latency, set the pace.
-__global__ void serial_sum_kernel(const double* __restrict__ f, int Nx, int Ny, int pitch,
-                                  double* out, int squares) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// serial order of pressure.c:62-69: x outer, y inner (sequence index k = i * Ny + j). The
+// dependent additions are one thread's (thread 0); the other warps stage the sequence into
+// shared memory a chunk ahead, so that the additions read shared memory instead of waiting on
+// strided global loads.
+constexpr int SS_THREADS = 256, SS_CHUNK = 2048;
+__global__ void __launch_bounds__(SS_THREADS) serial_sum_kernel(const double* __restrict__ f, int Nx, int Ny,
+                                                                int pitch, double* out, int squares) {
+  __shared__ double buf[2][SS_CHUNK];
+  const long long n = (long long)Nx * Ny;
+  const long long nchunks = (n + SS_CHUNK - 1) / SS_CHUNK;
+  auto stage = [&](long long c, double* b) {
+    for (int q = threadIdx.x - 32; q < SS_CHUNK; q += SS_THREADS - 32) {
+      const long long k = c * SS_CHUNK + q;
+      if (k < n) {
+        const int i = (int)(k / Ny), j = (int)(k - (long long)i * Ny);
+        b[q] = f[(size_t)j * pitch + i];
+      }
+    }
+  };
+  if (threadIdx.x >= 32) stage(0, buf[0]);
+  __syncthreads();
   double s = 0;
-  for (int i = 0; i < Nx; ++i) {
-    int j = 0;
-    for (; j + 8 <= Ny; j += 8) {
-      double a[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) a[q] = f[(size_t)(j + q) * pitch + i];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) s += squares ? a[q] * a[q] : a[q];
+  for (long long c = 0; c < nchunks; ++c) {
+    if (threadIdx.x >= 32) {
+      if (c + 1 < nchunks) stage(c + 1, buf[(c + 1) & 1]);
+    } else if (threadIdx.x == 0) {
+      const double* b = buf[c & 1];
+      const int m = (int)(n - c * SS_CHUNK < SS_CHUNK ? n - c * SS_CHUNK : SS_CHUNK);
+      if (squares) {
+#pragma unroll 8
+        for (int q = 0; q < m; ++q) {
+          const double a = b[q];
+          s += a * a;
+        }
+      } else {
+#pragma unroll 8
+        for (int q = 0; q < m; ++q) s += b[q];
+      }
     }
-    for (; j < Ny; ++j) {
-      double a = f[(size_t)j * pitch + i];
-      s += squares ? a * a : a;
-    }
+    __syncthreads();
   }
-  out[0] = s;
+  if (threadIdx.x == 0) out[0] = s;
 }
 
 // fixed-shape tree: each block sums RED_ROWS rows (one column per thread, looping over
@@ -869,7 +890,7 @@ size_t reduce_scratch_elems(int Nx, int Ny) { (void)Nx; return (size_t)(Ny + RED
 void launch_sum(const double* f, int Nx, int Ny, int pitch, bool serial, double* partials, double* out,
                 cudaStream_t s) {
   if (serial) {
-    serial_sum_kernel<<<1, 32, 0, s>>>(f, Nx, Ny, pitch, out, 0);
+    serial_sum_kernel<<<1, SS_THREADS, 0, s>>>(f, Nx, Ny, pitch, out, 0);
     return;
   }
   int nb = (Ny + RED_ROWS - 1) / RED_ROWS;
@@ -890,7 +911,7 @@ void launch_norms(const double* f, int Nx, int Ny, int pitch, bool serial, doubl
   max_abs_kernel<<<dim3(1, Ny < 1184 ? Ny : 1184), 256, 0, s>>>(f, Nx, Ny, pitch, bits);
   store_max_kernel<<<1, 1, 0, s>>>(bits, out);
   if (serial) {
-    serial_sum_kernel<<<1, 32, 0, s>>>(f, Nx, Ny, pitch, out + 1, 1);
+    serial_sum_kernel<<<1, SS_THREADS, 0, s>>>(f, Nx, Ny, pitch, out + 1, 1);
   } else {
     int nb = (Ny + RED_ROWS - 1) / RED_ROWS;
     tree_partial_kernel<<<nb, RED_BLOCK, 0, s>>>(f, Nx, Ny, pitch, partials, 1);

@@ -69,6 +69,7 @@ def test_uneven_jets_members_equal_alone(tmp_path, solver, graphs):
     # cooperative SOR launch stays on streams
     if graphs and solver == 1:
         assert ens.graph_steps() == steps - 5
+        assert ens.batched_mg()   # one batched multigrid loop for the 64^2 and 128^2 groups
     else:
         assert ens.graph_steps() == 0
     ens.close()
@@ -113,6 +114,42 @@ def test_walled_gyres_of_two_sizes(tmp_path):
     sa, sb = _state(members[1]), _state(alone[1])
     for k in sa:
         assert np.array_equal(sa[k], sb[k]), k
+    for m in members + alone:
+        m.close()
+
+
+def test_walled_multigrid_members(tmp_path):
+    """Closed-basin gyres with the multigrid (wall faces in every level kernel), two sizes, whole
+    steps as graph replays with the batched multigrid loop; the per-member iteration counts
+    differ between members and each member stops at its own test."""
+    import pawsim_b200
+
+    shapes = [(64, 64), (128, 64), (64, 64), (128, 128)]
+    setups = []
+    for i, (nx, ny) in enumerate(shapes):
+        _, cfg, f = make_setup(tmp_path / f"w{i}", "gyre", N=nx, Ny=ny, solver=1, dt=900.0 * 64 / nx,
+                               seed=i)
+        setups.append((cfg, f))
+    steps = 10
+    alone = []
+    for cfg, f in setups:
+        m = pawsim_b200.Model(cfg, f)
+        m.prelim()
+        m.run(1, steps)
+        alone.append(m)
+    members = []
+    for cfg, f in setups:
+        m = pawsim_b200.Model(cfg, f)
+        m.prelim()
+        members.append(m)
+    ens = pawsim_b200.Ensemble(members)
+    ens.run(1, 4)
+    it1 = [m.run_iterations() for m in members]
+    ens.run(5, steps - 4)
+    it2 = [m.run_iterations() for m in members]
+    assert ens.graph_steps() == steps - 4 and ens.batched_mg()
+    ens.close()
+    _check_members(members, alone, [np.concatenate([a, b]) for a, b in zip(it1, it2)])
     for m in members + alone:
         m.close()
 
