@@ -77,7 +77,9 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
         o = os.path.join(OBJDIR, name + ".o")
         objs.append(o)
         if force or _stale(o, [os.path.join(CSRC, src), *headers]):
-            cmds.append([NVCC, *ARCH, *FLAGS, *extra, "-c", os.path.join(CSRC, src), "-o", o])
+            # written under a temporary name and renamed when the compiler succeeds, so that an
+            # interrupted build leaves no object that looks up to date
+            cmds.append([NVCC, *ARCH, *FLAGS, *extra, "-c", os.path.join(CSRC, src), "-o", o + ".tmp"])
     # translation units compile in parallel (the tendency kernels dominate the build time)
     procs = []
     for cmd in cmds:
@@ -85,10 +87,13 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
             print(" ".join(cmd))
         procs.append(subprocess.Popen(cmd))
     failed = [c for c, p in zip(cmds, procs) if p.wait() != 0]
-    if failed:
-        for c in failed:   # no half-written object may look up to date next time
+    for c in cmds:
+        if c in failed:
             if os.path.exists(c[-1]):
                 os.remove(c[-1])
+        else:
+            os.replace(c[-1], c[-1][: -len(".tmp")])
+    if failed:
         raise subprocess.CalledProcessError(1, failed[0])
     cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
     if verbose:
