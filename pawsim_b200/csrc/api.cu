@@ -5,6 +5,7 @@
 // (integrator.c:138-198), then the rigid-lid correction (pressure.c:2254-2300).
 #include <math.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -986,6 +987,10 @@ struct Ensemble {
   MGBatch* mgb = nullptr;
   bool mgb_tried = false;
   cudaStream_t cap = nullptr;   // stream that captures the batched loop's body
+  // PAWSIM_ENSEMBLE_PHASES=1 (profiling): event nodes between the phases of a captured step
+  // (tendency, the members' pre-solve steps, the solves, the projections); the device times of
+  // the last replay are printed at the end of a run
+  cudaEvent_t ev_ph[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   void drop_graphs() {
     for (EnsGraph& g : graphs) {
       if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -1009,6 +1014,8 @@ struct Ensemble {
     for (cudaEvent_t e : ev_ring) cudaEventDestroy(e);
     for (cudaEvent_t e : ev_k) cudaEventDestroy(e);
     for (cudaEvent_t e : ev_cj) cudaEventDestroy(e);
+    for (cudaEvent_t e : ev_ph)
+      if (e) cudaEventDestroy(e);
     if (ev_cf) cudaEventDestroy(ev_cf);
     if (ev_t) cudaEventDestroy(ev_t);
     if (s0) cudaStreamDestroy(s0);
@@ -1094,6 +1101,8 @@ static int ensemble_create(Model* const* ms, int n, Ensemble** out) {
     if (ms[i]->mg) ms[i]->mg->set_stream(q);
     if (ms[i]->dmg) ms[i]->dmg->set_stream(q);
   }
+  if (ok && getenv("PAWSIM_ENSEMBLE_PHASES"))
+    for (cudaEvent_t& ev : e->ev_ph) ok = ok && cudaEventCreate(&ev) == cudaSuccess;
   if (!ok) {
     delete e;
     return fail(PAWSIM_GPU_ECUDA, "ensemble set-up failed");
@@ -1167,10 +1176,15 @@ static int ensemble_capture(Ensemble* e, EnsGraph& g, const std::vector<TendPara
   const long long g0 = g_launches;
   PAWSIM_CUDA_OK(cudaStreamBeginCapture(e->s0, cudaStreamCaptureModeRelaxed));
   int rc = 0;
+  auto phase = [&](int k) {
+    if (e->ev_ph[k]) cudaEventRecordWithFlags(e->ev_ph[k], e->s0, cudaEventRecordExternal);
+  };
+  phase(0);
   const int nl = launch_tendency_batch(p[0], g.d_params, e->d_work, e->nwork, n, e->d_done,
                                        e->mem[0]->c.mom_scheme, e->mem[0]->c.thick_scheme, e->s0);
   if (nl < 0) rc = fail(PAWSIM_GPU_EUNSUPPORTED, "batched tendency launch not available");
   g_launches += nl > 0 ? nl : 0;
+  phase(1);
   if (!rc && cudaEventRecord(e->ev_cf, e->s0) != cudaSuccess) rc = fail(PAWSIM_GPU_ECUDA, "event record failed");
   if (mgb) {
     g.batched = true;
@@ -1185,7 +1199,9 @@ static int ensemble_capture(Ensemble* e, EnsGraph& g, const std::vector<TendPara
                   cudaStreamWaitEvent(e->s0, e->ev_cj[i], 0) != cudaSuccess))
         rc = fail(PAWSIM_GPU_ECUDA, "capture join failed");
     }
+    phase(2);
     if (!rc && mgb->capture(e->s0, e->cap) != 0) rc = fail(PAWSIM_GPU_ECUDA, "batched multigrid capture failed");
+    phase(3);
     if (!rc && cudaEventRecord(e->ev_cf, e->s0) != cudaSuccess) rc = fail(PAWSIM_GPU_ECUDA, "event record failed");
     for (int i = 0; i < n && !rc; ++i) {
       Model* m = e->mem[i];
@@ -1208,6 +1224,7 @@ static int ensemble_capture(Ensemble* e, EnsGraph& g, const std::vector<TendPara
     if (cudaEventRecord(e->ev_cj[i], m->s) != cudaSuccess || cudaStreamWaitEvent(e->s0, e->ev_cj[i], 0) != cudaSuccess)
       rc = fail(PAWSIM_GPU_ECUDA, "capture join failed");
   }
+  phase(4);
   cudaGraph_t graph = nullptr;
   const cudaError_t ce = cudaStreamEndCapture(e->s0, &graph);
   if (!rc && ce != cudaSuccess) rc = fail(PAWSIM_GPU_ECUDA, "ensemble step capture failed");
@@ -1366,6 +1383,12 @@ static int ensemble_run(Ensemble* e, unsigned n0, unsigned nsteps) {
     ++cnt;
   }
   e->kernel_ms = cnt ? tot / cnt : 0;
+  if (e->ev_ph[0] && e->graph_steps) {
+    float t[4] = {0, 0, 0, 0};
+    for (int k = 0; k < 4; ++k) cudaEventElapsedTime(&t[k], e->ev_ph[k], e->ev_ph[k + 1]);
+    fprintf(stderr, "pawsim ensemble phases (ms, last replay): tendency %.3f pre-solve %.3f solves %.3f post %.3f\n",
+            t[0], t[1], t[2], t[3]);
+  }
   return r;
 }
 

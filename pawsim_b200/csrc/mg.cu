@@ -1641,24 +1641,54 @@ struct BatchLoop {    // one member's loop state (the batched LoopState)
   double maxres;
 };
 
-constexpr int BOX = 32, BOY = 8, BNT = 256;   // the batched level kernels' tile shape
+// the batched level kernels' tile shapes: 64 x 16 tiles (less halo per owned cell) where a
+// level holds at least kBigLevel cells over all members, 32 x 8 tiles below (more CTAs);
+// every shape gives the same values
+constexpr long long kBigLevel = 1 << 20;
 
-__global__ void __launch_bounds__(BNT) down_batch_kernel(const BatchLevel* __restrict__ d,
-                                                          const BatchLoop* __restrict__ st) {
+template <int OX, int OY, int NT>
+__global__ void __launch_bounds__(NT) down_batch_kernel(const BatchLevel* __restrict__ d,
+                                                         const BatchLoop* __restrict__ st) {
   const int m = blockIdx.z;
   if (!st[m].active) return;
   const BatchLevel L = d[m];
-  down_tile_body<double, BOX, BOY, BNT, 1>(L.f, L.c, L.omega, L.zero_e, L.out, blockIdx.x, blockIdx.y);
+  down_tile_body<double, OX, OY, NT, 1>(L.f, L.c, L.omega, L.zero_e, L.out, blockIdx.x, blockIdx.y);
 }
 
-template <bool MEASURE>
-__global__ void __launch_bounds__(BNT) up_batch_kernel(const BatchLevel* __restrict__ d, BatchLoop* st, int wew,
-                                                        int wns) {
+template <int OX, int OY, int NT, bool MEASURE>
+__global__ void __launch_bounds__(NT) up_batch_kernel(const BatchLevel* __restrict__ d, BatchLoop* st, int wew,
+                                                       int wns) {
   const int m = blockIdx.z;
   if (!st[m].active) return;
   const BatchLevel L = d[m];
-  up_tile_body<double, BOX, BOY, BNT, 1, MEASURE>(L.f, L.c, L.omega, wew, wns, &st[m].bits, L.out, blockIdx.x,
-                                                  blockIdx.y);
+  up_tile_body<double, OX, OY, NT, 1, MEASURE>(L.f, L.c, L.omega, wew, wns, &st[m].bits, L.out, blockIdx.x,
+                                               blockIdx.y);
+}
+
+template <int OX, int OY, int NT>
+void set_batch_attrs() {
+  cudaFuncSetAttribute(down_batch_kernel<OX, OY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)tile_bytes<double, OX, OY, 3>());
+  cudaFuncSetAttribute(up_batch_kernel<OX, OY, NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)tile_bytes<double, OX, OY, 3>());
+  cudaFuncSetAttribute(up_batch_kernel<OX, OY, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)tile_bytes<double, OX, OY, 2>());
+}
+
+template <int OX, int OY, int NT>
+void launch_down_batch(int nx, int ny, int count, const BatchLevel* d, const BatchLoop* st, cudaStream_t s) {
+  const dim3 grid((nx + OX - 1) / OX, (ny + OY - 1) / OY, count);
+  down_batch_kernel<OX, OY, NT><<<grid, NT, tile_bytes<double, OX, OY, 3>(), s>>>(d, st);
+}
+
+template <int OX, int OY, int NT>
+void launch_up_batch(int nx, int ny, int count, bool measure, const BatchLevel* d, BatchLoop* st, int wew, int wns,
+                     cudaStream_t s) {
+  const dim3 grid((nx + OX - 1) / OX, (ny + OY - 1) / OY, count);
+  if (measure)
+    up_batch_kernel<OX, OY, NT, true><<<grid, NT, tile_bytes<double, OX, OY, 3>(), s>>>(d, st, wew, wns);
+  else
+    up_batch_kernel<OX, OY, NT, false><<<grid, NT, tile_bytes<double, OX, OY, 2>(), s>>>(d, st, wew, wns);
 }
 
 __global__ void __launch_bounds__(CA_WARPS * 32) coarse_batch_kernel(const BatchCoarse* __restrict__ d,
@@ -1822,12 +1852,8 @@ MGBatch::MGBatch(const std::vector<Multigrid*>& members, const std::vector<doubl
          cudaMemcpy(it_out_, hit.data(), n_ * sizeof(int*), cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(meas_out_, hmeas.data(), n_ * sizeof(double*), cudaMemcpyHostToDevice) == cudaSuccess;
   if (good) {
-    cudaFuncSetAttribute(down_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)tile_bytes<double, BOX, BOY, 3>());
-    cudaFuncSetAttribute(up_batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)tile_bytes<double, BOX, BOY, 3>());
-    cudaFuncSetAttribute(up_batch_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)tile_bytes<double, BOX, BOY, 2>());
+    set_batch_attrs<32, 8, 256>();
+    set_batch_attrs<64, 16, 512>();
   }
   ok_ = good && cudaGetLastError() == cudaSuccess;
 }
@@ -1864,18 +1890,18 @@ int MGBatch::capture(cudaStream_t s, cudaStream_t cap) {
     return -1;
   for (const Group* g : groups_) {
     BatchLoop* gs = st + g->off;
+    auto big = [&](int n) { return (long long)g->count * g->nx[n] * g->ny[n] >= kBigLevel; };
     for (int n = g->top; n > g->ctop; --n) {
-      const dim3 grid((g->nx[n] + BOX - 1) / BOX, (g->ny[n] + BOY - 1) / BOY, g->count);
-      down_batch_kernel<<<grid, BNT, tile_bytes<double, BOX, BOY, 3>(), cap>>>(g->down[n], gs);
+      if (big(n)) launch_down_batch<64, 16, 512>(g->nx[n], g->ny[n], g->count, g->down[n], gs, cap);
+      else launch_down_batch<32, 8, 256>(g->nx[n], g->ny[n], g->count, g->down[n], gs, cap);
     }
     coarse_batch_kernel<<<dim3((g->cn + CA_WARPS - 1) / CA_WARPS, g->count), CA_WARPS * 32, 0, cap>>>(
         g->coarse, gs, g->cn, g->cnx, g->cpitch);
     for (int n = g->ctop + 1; n <= g->top; ++n) {
-      const dim3 grid((g->nx[n] + BOX - 1) / BOX, (g->ny[n] + BOY - 1) / BOY, g->count);
-      if (n == g->top)
-        up_batch_kernel<true><<<grid, BNT, tile_bytes<double, BOX, BOY, 3>(), cap>>>(g->up[n], gs, g->wew, g->wns);
+      if (big(n))
+        launch_up_batch<64, 16, 512>(g->nx[n], g->ny[n], g->count, n == g->top, g->up[n], gs, g->wew, g->wns, cap);
       else
-        up_batch_kernel<false><<<grid, BNT, tile_bytes<double, BOX, BOY, 2>(), cap>>>(g->up[n], gs, g->wew, g->wns);
+        launch_up_batch<32, 8, 256>(g->nx[n], g->ny[n], g->count, n == g->top, g->up[n], gs, g->wew, g->wns, cap);
     }
   }
   batch_finalize_kernel<<<1, 256, 0, cap>>>(st, n_, it_out_, meas_out_, h);

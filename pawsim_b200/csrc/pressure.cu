@@ -198,14 +198,16 @@ constexpr int RED_ROWS = 8;   // rows per partial in the tree sum
 constexpr int SS_THREADS = 256, SS_CHUNK = 2048;
 __global__ void __launch_bounds__(SS_THREADS) serial_sum_kernel(const double* __restrict__ f, int Nx, int Ny,
                                                                 int pitch, double* out, int squares) {
-  __shared__ double buf[2][SS_CHUNK];
-  const long long n = (long long)Nx * Ny;
-  const long long nchunks = (n + SS_CHUNK - 1) / SS_CHUNK;
-  auto stage = [&](long long c, double* b) {
+  __shared__ __align__(16) double buf[2][SS_CHUNK];
+  // grids of the serial order hold far fewer than 2^31 cells (the order is the reference's for
+  // small grids; larger ones take it only when forced), so 32-bit sequence indices suffice
+  const int n = Nx * Ny;
+  const int nchunks = (n + SS_CHUNK - 1) / SS_CHUNK;
+  auto stage = [&](int c, double* b) {
     for (int q = threadIdx.x - 32; q < SS_CHUNK; q += SS_THREADS - 32) {
-      const long long k = c * SS_CHUNK + q;
+      const int k = c * SS_CHUNK + q;
       if (k < n) {
-        const int i = (int)(k / Ny), j = (int)(k - (long long)i * Ny);
+        const int i = k / Ny, j = k - i * Ny;
         b[q] = f[(size_t)j * pitch + i];
       }
     }
@@ -213,22 +215,22 @@ __global__ void __launch_bounds__(SS_THREADS) serial_sum_kernel(const double* __
   if (threadIdx.x >= 32) stage(0, buf[0]);
   __syncthreads();
   double s = 0;
-  for (long long c = 0; c < nchunks; ++c) {
+  for (int c = 0; c < nchunks; ++c) {
     if (threadIdx.x >= 32) {
       if (c + 1 < nchunks) stage(c + 1, buf[(c + 1) & 1]);
     } else if (threadIdx.x == 0) {
       const double* b = buf[c & 1];
-      const int m = (int)(n - c * SS_CHUNK < SS_CHUNK ? n - c * SS_CHUNK : SS_CHUNK);
-      if (squares) {
-#pragma unroll 8
-        for (int q = 0; q < m; ++q) {
-          const double a = b[q];
-          s += a * a;
-        }
-      } else {
-#pragma unroll 8
-        for (int q = 0; q < m; ++q) s += b[q];
+      const int m = n - c * SS_CHUNK < SS_CHUNK ? n - c * SS_CHUNK : SS_CHUNK;
+      int q = 0;
+      // sixteen shared-memory loads in flight ahead of the chain of additions
+      for (; q + 16 <= m; q += 16) {
+        double a[16];
+#pragma unroll
+        for (int r = 0; r < 16; ++r) a[r] = b[q + r];
+#pragma unroll
+        for (int r = 0; r < 16; ++r) s += squares ? a[r] * a[r] : a[r];
       }
+      for (; q < m; ++q) s += squares ? b[q] * b[q] : b[q];
     }
     __syncthreads();
   }
