@@ -1665,6 +1665,38 @@ __global__ void __launch_bounds__(NT) up_batch_kernel(const BatchLevel* __restri
                                                blockIdx.y);
 }
 
+// the streamed strip kernels over every member (blockIdx.y = member) on the big levels
+__global__ void __launch_bounds__(SP_WARPS * 32, SP_CTAS_DOWN)
+down_strip_batch_kernel(const BatchLevel* __restrict__ d, const BatchLoop* __restrict__ st, int S, int nstrips,
+                        int nsegs) {
+  const int m = blockIdx.y;
+  if (!st[m].active) return;
+  const BatchLevel L = d[m];
+  down_strip_body<double>(L.f, L.c, L.omega, L.zero_e, L.out, S, nstrips, nsegs, blockIdx.x);
+}
+
+template <bool MEASURE>
+__global__ void __launch_bounds__(SP_WARPS * 32, SP_CTAS_UP)
+up_strip_batch_kernel(const BatchLevel* __restrict__ d, BatchLoop* st, int wew, int wns, int S, int nstrips,
+                      int nsegs) {
+  const int m = blockIdx.y;
+  if (!st[m].active) return;
+  const BatchLevel L = d[m];
+  up_strip_body<double, MEASURE>(L.f, L.c, L.omega, wew, wns, &st[m].bits, L.out, S, nstrips, nsegs, blockIdx.x);
+}
+
+// strips of one member's level when `count` members share the GPU: longer segments than a
+// single grid takes, so that the members' strips together fill it once
+inline StripGrid strip_grid_batch(int Nx, int Ny, int count) {
+  StripGrid g;
+  const int sms = num_sms() / count;
+  g.S = strip_rows(Nx, Ny, sms < 1 ? 1 : sms);
+  g.nstrips = (Nx + SP_OWN - 1) / SP_OWN;
+  g.nsegs = (Ny + g.S - 1) / g.S;
+  g.blocks = (unsigned)((g.nstrips * g.nsegs + SP_WARPS - 1) / SP_WARPS);
+  return g;
+}
+
 template <int OX, int OY, int NT>
 void set_batch_attrs() {
   cudaFuncSetAttribute(down_batch_kernel<OX, OY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1698,6 +1730,15 @@ __global__ void __launch_bounds__(CA_WARPS * 32) coarse_batch_kernel(const Batch
   if (!st[m].active) return;
   const BatchCoarse B = d[m];
   coarse_apply_body<double>(B.C, n, Nx, pitch, B.rhs, B.e, blockIdx.x);
+}
+
+// flag = 1 when the two arrays differ in any bit (the members' coarse maps are shared when equal)
+__global__ void differ_kernel(const unsigned long long* __restrict__ a, const unsigned long long* __restrict__ b,
+                              size_t n, int* flag) {
+  int d = 0;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+    d |= a[q] != b[q];
+  if (__syncthreads_or(d) && threadIdx.x == 0) *flag = 1;
 }
 
 __global__ void batch_reset_kernel(BatchLoop* st, int n) {
@@ -1826,10 +1867,24 @@ MGBatch::MGBatch(const std::vector<Multigrid*>& members, const std::vector<doubl
     G->cn = Lt.Nx * Lt.Ny;
     G->cnx = Lt.Nx;
     G->cpitch = Lt.pitch;
+    // members whose coarse maps are bit-identical (same depth field and smoother weight, as in
+    // an ensemble over one basin) read one copy, which then stays in L2 across the group
+    int* flags = nullptr;
+    good = good && cudaMalloc(&flags, G->count * sizeof(int)) == cudaSuccess &&
+           cudaMemset(flags, 0, G->count * sizeof(int)) == cudaSuccess;
+    const size_t cwords = (size_t)G->cn * G->cn;
+    const double* C0 = static_cast<const double*>(members[set[0]]->cmat_[0]);
+    for (int q = 1; good && q < G->count; ++q)
+      differ_kernel<<<64, 256>>>(static_cast<const unsigned long long*>(members[set[q]]->cmat_[0]),
+                                 reinterpret_cast<const unsigned long long*>(C0), cwords, flags + q);
+    std::vector<int> differs(G->count, 1);
+    good = good && cudaMemcpy(differs.data(), flags, G->count * sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess;
+    cudaFree(flags);
     for (int q = 0; q < G->count; ++q) {
       Multigrid* g = members[set[q]];
       const Multigrid::Level& L = g->lv_[g->ctop_];
-      cv[q] = BatchCoarse{static_cast<const double*>(g->cmat_[0]), L.rhs, L.e};
+      const double* C = (q > 0 && !differs[q]) ? C0 : static_cast<const double*>(g->cmat_[0]);
+      cv[q] = BatchCoarse{C, L.rhs, L.e};
     }
     good = good && cudaMalloc(&G->coarse, G->count * sizeof(BatchCoarse)) == cudaSuccess &&
            cudaMemcpy(G->coarse, cv.data(), G->count * sizeof(BatchCoarse), cudaMemcpyHostToDevice) == cudaSuccess;
@@ -1854,6 +1909,12 @@ MGBatch::MGBatch(const std::vector<Multigrid*>& members, const std::vector<doubl
   if (good) {
     set_batch_attrs<32, 8, 256>();
     set_batch_attrs<64, 16, 512>();
+    cudaFuncSetAttribute(down_strip_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)strip_smem_bytes<double>(false));
+    cudaFuncSetAttribute(up_strip_batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)strip_smem_bytes<double>(true));
+    cudaFuncSetAttribute(up_strip_batch_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)strip_smem_bytes<double>(true));
   }
   ok_ = good && cudaGetLastError() == cudaSuccess;
 }
@@ -1891,17 +1952,35 @@ int MGBatch::capture(cudaStream_t s, cudaStream_t cap) {
   for (const Group* g : groups_) {
     BatchLoop* gs = st + g->off;
     auto big = [&](int n) { return (long long)g->count * g->nx[n] * g->ny[n] >= kBigLevel; };
+    auto strips = [&](int n) { return big(n) && strip_ok(g->nx[n], g->ny[n]); };
     for (int n = g->top; n > g->ctop; --n) {
-      if (big(n)) launch_down_batch<64, 16, 512>(g->nx[n], g->ny[n], g->count, g->down[n], gs, cap);
-      else launch_down_batch<32, 8, 256>(g->nx[n], g->ny[n], g->count, g->down[n], gs, cap);
+      if (strips(n)) {
+        const StripGrid sg = strip_grid_batch(g->nx[n], g->ny[n], g->count);
+        down_strip_batch_kernel<<<dim3(sg.blocks, g->count), SP_WARPS * 32, strip_smem_bytes<double>(false), cap>>>(
+            g->down[n], gs, sg.S, sg.nstrips, sg.nsegs);
+      } else if (big(n)) {
+        launch_down_batch<64, 16, 512>(g->nx[n], g->ny[n], g->count, g->down[n], gs, cap);
+      } else {
+        launch_down_batch<32, 8, 256>(g->nx[n], g->ny[n], g->count, g->down[n], gs, cap);
+      }
     }
     coarse_batch_kernel<<<dim3((g->cn + CA_WARPS - 1) / CA_WARPS, g->count), CA_WARPS * 32, 0, cap>>>(
         g->coarse, gs, g->cn, g->cnx, g->cpitch);
     for (int n = g->ctop + 1; n <= g->top; ++n) {
-      if (big(n))
+      if (strips(n)) {
+        const StripGrid sg = strip_grid_batch(g->nx[n], g->ny[n], g->count);
+        const dim3 grid(sg.blocks, g->count);
+        if (n == g->top)
+          up_strip_batch_kernel<true><<<grid, SP_WARPS * 32, strip_smem_bytes<double>(true), cap>>>(
+              g->up[n], gs, g->wew, g->wns, sg.S, sg.nstrips, sg.nsegs);
+        else
+          up_strip_batch_kernel<false><<<grid, SP_WARPS * 32, strip_smem_bytes<double>(true), cap>>>(
+              g->up[n], gs, g->wew, g->wns, sg.S, sg.nstrips, sg.nsegs);
+      } else if (big(n)) {
         launch_up_batch<64, 16, 512>(g->nx[n], g->ny[n], g->count, n == g->top, g->up[n], gs, g->wew, g->wns, cap);
-      else
+      } else {
         launch_up_batch<32, 8, 256>(g->nx[n], g->ny[n], g->count, n == g->top, g->up[n], gs, g->wew, g->wns, cap);
+      }
     }
   }
   batch_finalize_kernel<<<1, 256, 0, cap>>>(st, n_, it_out_, meas_out_, h);

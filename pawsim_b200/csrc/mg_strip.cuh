@@ -199,11 +199,11 @@ inline int strip_rows(int Nx, int Ny, int sms) {
 // pre-smoothing (one red-black sweep) of f.e (or of zero) into `out`, residual and 2x2
 // restriction into the coarse rhs: down_tile with NU = 1, streamed
 template <typename T>
-__global__ void __launch_bounds__(SP_WARPS * 32, SP_CTAS_DOWN)
-down_strip(LV<T> f, LV<T> c, T omega, int zero_e, T* __restrict__ out, int S, int nstrips, int nsegs) {
+__device__ __forceinline__ void down_strip_body(const LV<T>& f, const LV<T>& c, T omega, int zero_e,
+                                                T* __restrict__ out, int S, int nstrips, int nsegs, int bx) {
   extern __shared__ __align__(16) unsigned char sp_raw[];
   const int lane = threadIdx.x & 31;
-  const int w = blockIdx.x * SP_WARPS + (threadIdx.x >> 5);
+  const int w = bx * SP_WARPS + (threadIdx.x >> 5);
   if (w >= nstrips * nsegs) return;   // whole warps only: the kernel has no barrier
   T* stage = reinterpret_cast<T*>(sp_raw) + (threadIdx.x >> 5) * (SP_RING * SL_DOWN + SL_SCRATCH);
   T* scratch = stage + SP_RING * SL_DOWN + lane;
@@ -273,12 +273,12 @@ down_strip(LV<T> f, LV<T> c, T omega, int zero_e, T* __restrict__ out, int S, in
 // post-smoothing into `out` and, with MEASURE, the stopping measure max |e - Jacobi(e)|
 // over the owned cells into *bits: up_tile with NU = 1, streamed
 template <typename T, bool MEASURE>
-__global__ void __launch_bounds__(SP_WARPS * 32, SP_CTAS_UP)
-up_strip(LV<T> f, LV<T> c, T omega, int wew, int wns, unsigned long long* bits, T* __restrict__ out, int S,
-         int nstrips, int nsegs) {
+__device__ __forceinline__ void up_strip_body(const LV<T>& f, const LV<T>& c, T omega, int wew, int wns,
+                                              unsigned long long* bits, T* __restrict__ out, int S, int nstrips,
+                                              int nsegs, int bx) {
   extern __shared__ __align__(16) unsigned char sp_raw[];
   const int lane = threadIdx.x & 31;
-  const int w = blockIdx.x * SP_WARPS + (threadIdx.x >> 5);
+  const int w = bx * SP_WARPS + (threadIdx.x >> 5);
   const bool active = w < nstrips * nsegs;   // inactive warps still reach the block reduction
   constexpr bool RCP = kStripRcp<T, true>;
   double m = 0;
@@ -369,4 +369,17 @@ up_strip(LV<T> f, LV<T> c, T omega, int wew, int wns, unsigned long long* bits, 
     cp_async_wait<0>();
   }
   if constexpr (MEASURE) block_max_to(m, bits);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(SP_WARPS * 32, SP_CTAS_DOWN)
+down_strip(LV<T> f, LV<T> c, T omega, int zero_e, T* __restrict__ out, int S, int nstrips, int nsegs) {
+  down_strip_body<T>(f, c, omega, zero_e, out, S, nstrips, nsegs, blockIdx.x);
+}
+
+template <typename T, bool MEASURE>
+__global__ void __launch_bounds__(SP_WARPS * 32, SP_CTAS_UP)
+up_strip(LV<T> f, LV<T> c, T omega, int wew, int wns, unsigned long long* bits, T* __restrict__ out, int S,
+         int nstrips, int nsegs) {
+  up_strip_body<T, MEASURE>(f, c, omega, wew, wns, bits, out, S, nstrips, nsegs, blockIdx.x);
 }
