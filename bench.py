@@ -47,6 +47,8 @@ TOL = 1e-10
 # cells limits AB3 to about 200 s (dt 900 s grows without bound); on the 977 m cells of the
 # 4096^2 gyre a biharmonic 5e9 m^4/s would need dt below 2 s and the internal wave limits dt to
 # about 80 s, so that case runs with 1e8 m^4/s and 50 s.
+FULL_WS_SPIN = 100
+FULL_WS_EPOCHS = 5
 CHANNEL_DT = 150.0
 FULL_DT = 50.0
 FULL_A4 = 1e8
@@ -310,22 +312,43 @@ def config_timing(kind, steps, warmup, stream, peak):
         out["workload"] = desc
         L, ncell = cfg.Nlay, cfg.Nx * cfg.Ny
         dt = cfg.dt
-        for label, fp32 in (("fp64_mg", 0), ("fp32_in_fp64_mg", 1)):
+        variants = [("fp64_mg", 0, False), ("fp32_in_fp64_mg", 1, False)]
+        if kind == "full":
+            # the learned warm start at this size: pairs collected over FULL_WS_SPIN steps,
+            # FULL_WS_EPOCHS epochs on the GPU (untimed)
+            variants.append(("learned_fp32_in_fp64_mg", 1, True))
+        for label, fp32, learn in variants:
             inner = FP32_INNER if fp32 else 1
             m = pawsim_b200.Model(cfg, fields, mg_fp32=fp32, mg_fp32_inner=inner, check_nonfinite=1)
             m.set_stream(stream.cuda_stream)
             with torch.cuda.stream(stream):
+                spin = FULL_WS_SPIN if learn else warmup
+                if learn:
+                    m.nn_setup(collect=True, use=False, max_pairs=spin, batch=8, seed=7)
                 m.prelim()
                 n = 1
-                for _ in range(warmup):
+                for _ in range(spin):
                     m.step(n)
                     n += 1
+                extra = {}
+                if learn:
+                    loss = m.nn_train(epochs=FULL_WS_EPOCHS, lr=1e-3)
+                    extra = {"train_pairs": m.nn_pairs(), "train_epochs": FULL_WS_EPOCHS, "train_loss": loss}
+                    m.nn_setup(collect=False, use=True)
                 torch.cuda.synchronize()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
                 finite = True
+                iters, used = [], 0
                 try:
-                    m.run(n, steps)
+                    if learn:   # the guess is formed and checked on the host's schedule: per-step calls
+                        for q in range(steps):
+                            st = m.step(n + q)
+                            iters.append(st["iters"])
+                            used += st["warm_start"] == 1
+                    else:
+                        m.run(n, steps)
+                        iters = list(m.run_iterations())
                 except pawsim_b200.PawsimError:
                     finite = False
                 e1.record(stream)
@@ -333,9 +356,11 @@ def config_timing(kind, steps, warmup, stream, peak):
                 ms = e0.elapsed_time(e1)
                 n += steps
                 res = {"ms_per_step": ms / steps, "sim_days_per_s": steps * dt / 86400.0 / (ms / 1e3),
-                       "gpl_updates_per_s": steps * ncell * L / (ms / 1e3), "finite": finite}
+                       "gpl_updates_per_s": steps * ncell * L / (ms / 1e3), "finite": finite, **extra}
+                if learn:
+                    res["guess_used_steps"] = int(used)
                 if finite:
-                    res["vcycles_per_step"] = float(np.mean(m.run_iterations())) * inner
+                    res["vcycles_per_step"] = float(np.mean(iters)) * inner
                     k_ms = 0.0
                     for _ in range(5):
                         k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
