@@ -210,8 +210,10 @@ __device__ __forceinline__ double div_rn(double x, double d, double r) {
 // (tiny, huge, infinite or NaN) raises `oor`; the caller then recomputes what used the quotient
 // with div_rn, so every result still equals the IEEE division's.
 __device__ __forceinline__ double div_rn_fast(double x, double d, double r, bool& oor) {
-  const unsigned be = ((unsigned)__double2hiint(x) >> 20) & 0x7ffu;
-  oor |= (be - 124u > 1922u - 124u) & (x != 0);
+  // the exponent field outside [124, 1922], tested on the high word without extracting it:
+  // |hi| < 124 << 20 or |hi| >= 1923 << 20
+  const unsigned ahi = (unsigned)__double2hiint(x) & 0x7fffffffu;
+  oor |= (ahi - (124u << 20) > (1923u << 20) - 1u - (124u << 20)) & (x != 0);
   const double q = x * r;
   double e = fma(-q, d, x);
   const double q1 = fma(e, r, q);
