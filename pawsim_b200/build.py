@@ -28,6 +28,9 @@ UNITS = [(s.replace(".cu", ""), s, []) for s in SOURCES] + [
     # one unit per tile height and momentum scheme, so that they compile in parallel
     *[(f"tendency_ty{ty}_m{ms}", "tendency_tile.cu", [f"-DPAWSIM_TEND_TY={ty}", f"-DPAWSIM_TEND_MS={ms}"])
       for ty in (8, 16) for ms in range(4)],
+    # 32 x 12 tiles of 384 threads, three CTAs per SM
+    *[(f"tendency_ty12_m{ms}", "tendency_tile.cu", ["-DPAWSIM_TEND_TY=12", f"-DPAWSIM_TEND_MS={ms}",
+                                                     "-DPAWSIM_TEND_MINB=3"]) for ms in range(4)],
     ("tendency_budget", "tendency_tile.cu", ["-DPAWSIM_TEND_TY=8", "-DPAWSIM_TEND_BUD=1", "-DPAWSIM_TEND_MINB=2"]),
 ]
 DRIVER_SRC = os.path.join(HERE, "host", "pawsim_main.c")

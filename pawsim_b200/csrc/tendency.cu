@@ -1,8 +1,11 @@
 // tendency.cu -- chooses the tile height of the fused tendency kernel (tendency_tile.cu).
 //
-// Both heights compute the same values; 32 x 16 tiles (512 threads) spend fewer halo
-// evaluations per owned cell than 32 x 8 tiles (256 threads) but hold twice the shared
-// memory. The taller tile is used while two of its CTAs still fit in one SM's shared memory.
+// Every height computes the same values. Tiles are 32 cells wide; 32 x 12 tiles (384 threads)
+// run three CTAs per SM when three fit in its shared memory, 32 x 16 tiles (512 threads) two,
+// and 32 x 8 tiles (256 threads) take the set-ups whose 32 x 16 tile would leave room for one.
+// Taller tiles spend fewer halo evaluations per owned cell; more resident warps hide more
+// latency. Measured on the lean 2048 x 2048 x 2 gyre step: 32 x 12 at three CTAs 0.672 ms,
+// 32 x 16 at two 0.690 ms.
 #include <cuda_runtime.h>
 
 #include "tendency.cuh"
@@ -10,6 +13,7 @@
 namespace pawsim {
 
 size_t tendency_smem_ty8(const TendParams& p, int ts);
+size_t tendency_smem_ty12(const TendParams& p, int ts);
 size_t tendency_smem_ty16(const TendParams& p, int ts);
 // one translation unit per tile height and momentum scheme (compiled in parallel)
 #define PAWSIM_DECL_TEND(TY)                                                   \
@@ -18,59 +22,59 @@ size_t tendency_smem_ty16(const TendParams& p, int ts);
   int launch_tendency_ty##TY##_m2(const TendParams& p, int ms, int ts, cudaStream_t s); \
   int launch_tendency_ty##TY##_m3(const TendParams& p, int ms, int ts, cudaStream_t s);
 PAWSIM_DECL_TEND(8)
+PAWSIM_DECL_TEND(12)
 PAWSIM_DECL_TEND(16)
 #undef PAWSIM_DECL_TEND
 #define PAWSIM_DECL_BATCH(TY, M)                                                                         \
   int batch_launch_tendency_ty##TY##_m##M(const TendParams& p0, const TendParams* ps, const int* work, \
                                            int nwork, int members, int* done, int ms, int ts, cudaStream_t s);
 PAWSIM_DECL_BATCH(8, 0) PAWSIM_DECL_BATCH(8, 1) PAWSIM_DECL_BATCH(8, 2) PAWSIM_DECL_BATCH(8, 3)
+PAWSIM_DECL_BATCH(12, 0) PAWSIM_DECL_BATCH(12, 1) PAWSIM_DECL_BATCH(12, 2) PAWSIM_DECL_BATCH(12, 3)
 PAWSIM_DECL_BATCH(16, 0) PAWSIM_DECL_BATCH(16, 1) PAWSIM_DECL_BATCH(16, 2) PAWSIM_DECL_BATCH(16, 3)
 #undef PAWSIM_DECL_BATCH
 int launch_tendency_budget_tile(const TendParams& p, int ms, int ts, cudaStream_t s);
 
-static int launch_tendency_ty8(const TendParams& p, int ms, int ts, cudaStream_t s) {
-  switch (ms) {
-    case 0: return launch_tendency_ty8_m0(p, ms, ts, s);
-    case 1: return launch_tendency_ty8_m1(p, ms, ts, s);
-    case 2: return launch_tendency_ty8_m2(p, ms, ts, s);
-    case 3: return launch_tendency_ty8_m3(p, ms, ts, s);
-  }
-  return -1;
-}
-
-static int launch_tendency_ty16(const TendParams& p, int ms, int ts, cudaStream_t s) {
-  switch (ms) {
-    case 0: return launch_tendency_ty16_m0(p, ms, ts, s);
-    case 1: return launch_tendency_ty16_m1(p, ms, ts, s);
-    case 2: return launch_tendency_ty16_m2(p, ms, ts, s);
-    case 3: return launch_tendency_ty16_m3(p, ms, ts, s);
-  }
-  return -1;
+int tendency_tile_height(const TendParams& p, int ts) {
+  // 228 KB of shared memory per SM, 1 KB reserved per CTA
+  constexpr size_t kThreePerSM = 74 * 1024, kTwoPerSM = 113 * 1024;
+  if (tendency_smem_ty12(p, ts) <= kThreePerSM) return 12;
+  if (tendency_smem_ty16(p, ts) <= kTwoPerSM) return 16;
+  return 8;
 }
 
 int launch_tendency(const TendParams& p, int ms, int ts, cudaStream_t s) {
-  // two CTAs per SM: 228 KB of shared memory, 1 KB reserved per CTA
-  constexpr size_t kTwoPerSM = 113 * 1024;
-  if (tendency_smem_ty16(p, ts) <= kTwoPerSM) return launch_tendency_ty16(p, ms, ts, s);
-  return launch_tendency_ty8(p, ms, ts, s);
+#define PAWSIM_TEND_CASE(M)                                           \
+  case M:                                                             \
+    switch (ty) {                                                     \
+      case 12: return launch_tendency_ty12_m##M(p, ms, ts, s);        \
+      case 16: return launch_tendency_ty16_m##M(p, ms, ts, s);        \
+      default: return launch_tendency_ty8_m##M(p, ms, ts, s);         \
+    }
+  const int ty = tendency_tile_height(p, ts);
+  switch (ms) {
+    PAWSIM_TEND_CASE(0)
+    PAWSIM_TEND_CASE(1)
+    PAWSIM_TEND_CASE(2)
+    PAWSIM_TEND_CASE(3)
+  }
+#undef PAWSIM_TEND_CASE
+  return -1;
 }
 
 int launch_tendency_budget(const TendParams& p, int ms, int ts, cudaStream_t s) {
   return launch_tendency_budget_tile(p, ms, ts, s);
 }
 
-int tendency_tile_height(const TendParams& p, int ts) {
-  constexpr size_t kTwoPerSM = 113 * 1024;
-  return tendency_smem_ty16(p, ts) <= kTwoPerSM ? 16 : 8;
-}
-
 int launch_tendency_batch(const TendParams& p0, const TendParams* ps, const int* work, int nwork, int members,
                           int* done, int ms, int ts, cudaStream_t s) {
-  const bool tall = tendency_tile_height(p0, ts) == 16;
-#define PAWSIM_BATCH_CASE(M)                                                                         \
-  case M:                                                                                            \
-    return tall ? batch_launch_tendency_ty16_m##M(p0, ps, work, nwork, members, done, ms, ts, s)   \
-                : batch_launch_tendency_ty8_m##M(p0, ps, work, nwork, members, done, ms, ts, s);
+  const int ty = tendency_tile_height(p0, ts);
+#define PAWSIM_BATCH_CASE(M)                                                                               \
+  case M:                                                                                                  \
+    switch (ty) {                                                                                          \
+      case 12: return batch_launch_tendency_ty12_m##M(p0, ps, work, nwork, members, done, ms, ts, s);      \
+      case 16: return batch_launch_tendency_ty16_m##M(p0, ps, work, nwork, members, done, ms, ts, s);      \
+      default: return batch_launch_tendency_ty8_m##M(p0, ps, work, nwork, members, done, ms, ts, s);       \
+    }
   switch (ms) {
     PAWSIM_BATCH_CASE(0)
     PAWSIM_BATCH_CASE(1)

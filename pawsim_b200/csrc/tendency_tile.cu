@@ -1,8 +1,8 @@
 // tendency_tile.cu -- fused layer tendency + Adams-Bashforth step (the K-tend kernel).
 //
-// Compiled twice, with PAWSIM_TEND_TY = 8 (256 threads) and 16 (512 threads): the taller
-// tile computes fewer halo cells per owned cell but needs more shared memory, so
-// tendency.cu picks it when its footprint still lets two CTAs share an SM.
+// Compiled for three tile heights, PAWSIM_TEND_TY = 8, 12 and 16 (256, 384 and 512 threads):
+// a taller tile computes fewer halo cells per owned cell but needs more shared memory, and
+// tendency.cu picks the height by how many CTAs then share an SM.
 //
 // One CTA owns a TX x TY tile of cells for every layer. It replaces, for that tile, the
 // reference's whole derivative evaluation and state update:
