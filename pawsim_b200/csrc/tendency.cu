@@ -2,7 +2,7 @@
 //
 // Every height computes the same values. Tiles are 32 cells wide; 32 x 12 tiles (384 threads)
 // run three CTAs per SM when three fit in its shared memory, 32 x 16 tiles (512 threads) two,
-// and 32 x 8 tiles (256 threads) take the set-ups whose 32 x 16 tile would leave room for one.
+// then 32 x 12 tiles two, and 32 x 8 tiles (256 threads) take what is left.
 // Taller tiles spend fewer halo evaluations per owned cell; more resident warps hide more
 // latency. Measured on the lean 2048 x 2048 x 2 gyre step: 32 x 12 at three CTAs 0.672 ms,
 // 32 x 16 at two 0.690 ms.
@@ -39,6 +39,9 @@ int tendency_tile_height(const TendParams& p, int ts) {
   constexpr size_t kThreePerSM = 74 * 1024, kTwoPerSM = 113 * 1024;
   if (tendency_smem_ty12(p, ts) <= kThreePerSM) return 12;
   if (tendency_smem_ty16(p, ts) <= kTwoPerSM) return 16;
+  // 32 x 12 at two CTAs (24 warps) beats 32 x 8 at two (16 warps): 0.82 against 1.07 ms on
+  // the 1024 x 1024 x 4 full-physics set-up (A4, w_dia, restoring)
+  if (tendency_smem_ty12(p, ts) <= kTwoPerSM) return 12;
   return 8;
 }
 
