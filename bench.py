@@ -677,8 +677,11 @@ def main():
     d2h = sum(t.numel() * 8 for t in pinned_out.values()) + args.steps * (4 + 8)
     e2e_value = job_throughput(world, args.steps, max_over_ranks(e2e_s, dist))
 
+    # the sub-lines after the headline run on rank 0 only (its JSON line carries them; the
+    # other ranks' replicas add nothing to them)
+    extras = rank == 0
     ws = None
-    if not args.no_warm_start:
+    if extras and not args.no_warm_start:
         ws = pressure_comparison(cfg, fields, stream, args.ws_spin, args.ws_steps, args.ws_epochs, args.ws_spin)
 
     peak, peak_kind = peaks()
@@ -707,7 +710,7 @@ def main():
     }
     # the passive tracer (a set-up with useTracer: KT00 advection, K2, relaxation) on the same
     # grid, not part of the headline step
-    tr = tracer_timing(cfg, stream, args.steps)
+    tr = tracer_timing(cfg, stream, args.steps) if extras else None
     # bytes per cell: read u, v, h and pi, hhb, w_dia; read and write the 10 L + 2 sums
     avg_bytes = ncell * (24 * L + 8 * (L + 3) + 16 * (10 * L + 2))
     line["averages"] = {"kernel": "accumulate_averages_kernel", "ms_per_step": avg_ms,
@@ -720,14 +723,16 @@ def main():
     line["energy"] = {"kernel": "ez_partial_kernel + ez_final_kernel", "ms_per_call": ez_ms,
                       "algorithmic_bytes": ez_bytes, "achieved_gbs": ez_bytes / (ez_ms / 1e3) / 1e9,
                       "frac": ez_bytes / (ez_ms / 1e3) / 1e9 / peak}
-    bt = budget_timing(stream, min(args.steps, 20))
-    # budget sums read and written once per step: 16 + 16 + 2 + 15 terms per layer; the kernel
-    # itself as in the roofline line
-    bud_bytes = ncell * L * 16 * (16 + 16 + 2 + 15)
-    line["budgets"] = {"kernel": "tendency_kernel budget build (32 x 8 tiles)", "families": "UMom VMom Thic Energy",
-                       "ms_per_step": bt[1], "plain_ms_per_step": bt[0], "extra_ms": bt[1] - bt[0],
-                       "budget_bytes": bud_bytes,
-                       "budget_gbs": bud_bytes / ((bt[1] - bt[0]) / 1e3) / 1e9 if bt[1] > bt[0] else None}
+    if extras:
+        bt = budget_timing(stream, min(args.steps, 20))
+        # budget sums read and written once per step: 16 + 16 + 2 + 15 terms per layer; the
+        # kernel itself as in the roofline line
+        bud_bytes = ncell * L * 16 * (16 + 16 + 2 + 15)
+        line["budgets"] = {"kernel": "tendency_kernel budget build (32 x 8 tiles)",
+                           "families": "UMom VMom Thic Energy",
+                           "ms_per_step": bt[1], "plain_ms_per_step": bt[0], "extra_ms": bt[1] - bt[0],
+                           "budget_bytes": bud_bytes,
+                           "budget_gbs": bud_bytes / ((bt[1] - bt[0]) / 1e3) / 1e9 if bt[1] > bt[0] else None}
     if tr is not None:
         tr_bytes = ncell * L * 88   # read u, v, h, b, bRelax, bTime, f1, f2, w_dia; write b, f
         line["tracer"] = {"kernel": "tracer_tile_kernel (KT00, K2, relaxation)", "ms_per_step": tr,
@@ -735,9 +740,9 @@ def main():
                           "frac": tr_bytes / (tr / 1e3) / 1e9 / peak}
     if ws is not None:
         line["pressure_learned_fp32_vs_plain_fp64"] = ws
-    if not args.no_ensemble:
+    if extras and not args.no_ensemble:
         line["ensemble"] = ensemble_timing(min(args.steps, 100), max(args.warmup, ENS_WARMUP), peak)
-    if not args.no_configs:
+    if extras and not args.no_configs:
         line["channel_1024x512x3"] = config_timing("channel", min(args.steps, 100), args.warmup, stream, peak)
         line["full_physics_4096x4096x4"] = config_timing("full", min(args.steps, 20), args.warmup, stream, peak)
     if rank == 0 and not args.no_cpu_baseline:
