@@ -1052,7 +1052,8 @@ static int ensemble_create(Model* const* ms, int n, Ensemble** out) {
     const TendParams pi = base_params(ms[i]);
     if (tendency_tile_height(pi, c0.thick_scheme) != ty || (pi.use_wdia != 0) != (p0.use_wdia != 0) ||
         pi.use_smag != p0.use_smag || (pi.use_fractions != 0) != (p0.use_fractions != 0) ||
-        (pi.useA4 != 0) != (p0.useA4 != 0) || (pi.corners != nullptr) != (p0.corners != nullptr))
+        (pi.useA4 != 0) != (p0.useA4 != 0) || (pi.corners != nullptr) != (p0.corners != nullptr) ||
+        tendency_lean(pi) != tendency_lean(p0))
       return fail(PAWSIM_GPU_EUNSUPPORTED, "ensemble members must share the tendency kernel's feature set");
   }
   Ensemble* e = new Ensemble();

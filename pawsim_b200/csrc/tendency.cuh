@@ -106,6 +106,15 @@ int launch_tendency(const TendParams& p, int momentum_scheme, int thickness_sche
                     cudaStream_t stream);
 // tile height (16 or 8 rows) launch_tendency uses for this set-up
 int tendency_tile_height(const TendParams& p, int thickness_scheme);
+
+// The set-up needs none of the paths the lean instantiation of the fused kernel leaves out
+// (w_dia, restoring, diapycnal viscosity, fractions, Fbaro, A4, Smagorinsky, corner shadow,
+// quadratic and surface drag, buoyancy); the launch then takes the lean build.
+inline bool tendency_lean(const TendParams& p) {
+  return !p.use_wdia && !p.use_relax && !p.use_diavisc && !p.use_fractions && !p.use_fbaro && !p.useA4 &&
+         !p.use_smag && !p.corners && !(p.quad_drag > 0) && !(p.quad_drag_surf > 0) && !(p.lin_drag_surf > 0) &&
+         !p.drag_bot && !p.drag_surf && !p.use_buoy;
+}
 // The fused step of several members in one launch (ensemble): ps (device) holds each member's
 // parameters, work (device) the (member << 20 | tile) pairs of nwork tiles, on the tile height
 // tendency_tile_height gives; the members share p0's momentum and thickness schemes, feature

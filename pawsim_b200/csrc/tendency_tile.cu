@@ -458,10 +458,12 @@ __device__ __forceinline__ void tendency_tile(const TendParams& p, int bx, int b
   };
   constexpr int RW = Geo<H>::RW, RH = Geo<H>::RH, RN = Geo<H>::RN;
   extern __shared__ double smem[];
+  // the lean build has no biharmonic intermediates (U4, V4): their planes are not allocated
+  constexpr int FP = LEAN ? F_U4 : F_NUM;
   double* F[F_NUM];
 #pragma unroll
-  for (int f = 0; f < F_NUM; ++f) F[f] = smem + f * RN;
-  double* MMall = smem + F_NUM * RN;            // [L][RN]
+  for (int f = 0; f < F_NUM; ++f) F[f] = smem + (f < FP ? f : 0) * RN;
+  double* MMall = smem + FP * RN;               // [L][RN]
   double* WDall = MMall + p.L * RN;             // [L+1][RN] when use_wdia
   double* SM = WDall + (use_wdia ? (p.L + 1) * RN : 0);   // [S_NUM][RN] when use_smag
   double* FR = SM + (use_smag ? S_NUM * RN : 0);          // [4][L][NT] when use_fractions
@@ -1339,21 +1341,18 @@ tendency_batch_exact_kernel(const TendParams* __restrict__ ps, int members, int*
   }
 }
 
+// dynamic shared memory of a tile (lean: the lean instantiation's, without the U4, V4 planes)
 template <int H>
-size_t smem_bytes(const TendParams& p) {
+size_t smem_bytes(const TendParams& p, bool lean = false) {
   constexpr int RN = Geo<H>::RN;
-  return (size_t)(F_NUM + p.L + (p.use_wdia ? p.L + 1 : 0) + (p.use_smag ? S_NUM : 0)) * RN * sizeof(double)
+  const int planes = lean ? F_U4 : F_NUM;
+  return (size_t)(planes + p.L + (p.use_wdia ? p.L + 1 : 0) + (p.use_smag ? S_NUM : 0)) * RN * sizeof(double)
        + (p.use_fractions ? (size_t)4 * p.L * NT * sizeof(double) : 0);
 }
 
 constexpr int EXACT_CTAS = 148;   // the exact pass's grid: one CTA per SM
 
-// the set-up needs none of the paths a LEAN instantiation leaves out
-inline bool lean_params(const TendParams& p) {
-  return !p.use_wdia && !p.use_relax && !p.use_diavisc && !p.use_fractions && !p.use_fbaro && !p.useA4 &&
-         !p.use_smag && !p.corners && !(p.quad_drag > 0) && !(p.quad_drag_surf > 0) && !(p.lin_drag_surf > 0) &&
-         !p.drag_bot && !p.drag_surf && !p.use_buoy;
-}
+inline bool lean_params(const TendParams& p) { return tendency_lean(p); }
 
 // Launches the step (the drag pre-pass when needed, the fused kernel and, in the plain build,
 // the exact pass over flagged tiles); returns the number of launches, or -1.
@@ -1382,9 +1381,10 @@ int launch_t(const TendParams& p, cudaStream_t s) {
     tendency_kernel<MS, TS, H, false><<<grid, NT, shm, s>>>(p);
     return pre + 1;
   } else {
-    if (lean_params(p)) tendency_kernel<MS, TS, H, true><<<grid, NT, shm, s>>>(p);
+    if (lean_params(p)) tendency_kernel<MS, TS, H, true><<<grid, NT, smem_bytes<H>(p, true), s>>>(p);
     else tendency_kernel<MS, TS, H, false><<<grid, NT, shm, s>>>(p);
-    // the exact recomputation of the listed tiles (one CTA per SM walks the list)
+    // the exact recomputation of the listed tiles (one CTA per SM walks the list; the full
+    // build, so the full shared memory)
     tendency_exact_kernel<MS, TS, H><<<EXACT_CTAS, NT, shm, s>>>(p);
     return pre + 2;
   }
@@ -1409,7 +1409,7 @@ int launch_batch_t(const TendParams& p0, const TendParams* ps, const int* work, 
                            200 * 1024);
       attr_done = true;
     }
-    if (lean_params(p0)) tendency_batch_kernel<MS, TS, H, true><<<nwork, NT, shm, s>>>(ps, work);
+    if (lean_params(p0)) tendency_batch_kernel<MS, TS, H, true><<<nwork, NT, smem_bytes<H>(p0, true), s>>>(ps, work);
     else tendency_batch_kernel<MS, TS, H, false><<<nwork, NT, shm, s>>>(ps, work);
     tendency_batch_exact_kernel<MS, TS, H><<<EXACT_CTAS, NT, shm, s>>>(ps, members, done);
     return 2;
