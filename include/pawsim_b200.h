@@ -202,7 +202,9 @@ PAWSIM_API int pawsim_gpu_run_iterations (pawsim_gpu * m, int * iters, size_t n)
  * n0.. : per step one launch of the fused kernel over all members' tiles, then each member's
  * rigid-lid correction on its own stream, with no host synchronisation until the end; each
  * member's results equal those of pawsim_gpu_run on that member alone, and its per-step
- * iteration counts are read with pawsim_gpu_run_iterations. */
+ * iteration counts are read with pawsim_gpu_run_iterations. Members must outlive the
+ * ensemble and are not stepped on their own while it exists; after an error return of run
+ * the members' states are unspecified. */
 typedef struct pawsim_gpu_ensemble pawsim_gpu_ensemble;
 PAWSIM_API int pawsim_gpu_ensemble_create (pawsim_gpu * const * members, int n, pawsim_gpu_ensemble ** out);
 PAWSIM_API int pawsim_gpu_ensemble_run (pawsim_gpu_ensemble * e, unsigned n0, unsigned nsteps);
